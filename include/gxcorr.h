@@ -1,0 +1,186 @@
+/*
+ * gxcorr -- B200-native FX correlation for DiFX's Mode/Core hot path.
+ *
+ * C ABI.  Plain structs, pointers and sizes; no C++ or CUDA types cross it.
+ * One handle = one correlation configuration on one GPU, with its own CUDA
+ * stream; calls on one handle are serialised by the caller (the reference
+ * gives each Core process thread its own Mode objects in the same way,
+ * mpifxcorr/src/core.cpp:2186-2193).  Every call returns a gx_status; no
+ * exceptions cross the ABI; gx_last_error() gives the message of the last
+ * failure on a handle.
+ *
+ * What each entry point replaces in the reference:
+ *
+ *   gx_open            Configuration::getMode for every datastream plus the
+ *                      result-layout computation Core relies on
+ *                      (configuration.cpp:932-998, populateResultLengths
+ *                      2348-2630, setStrides 2701-2734).
+ *   gx_open_input      new Configuration(file) (non-MPI ctor,
+ *                      configuration.cpp:98) + Model(.calc/.im)
+ *                      (model.cpp:20-76) + the same as gx_open.
+ *   gx_interpolator    Model::calculateDelayInterpolator as called from
+ *                      Mode::setOffsets (model.cpp:219-289, mode.cpp:1502-1532).
+ *   gx_subint          one Core slot through Core::processdata (core.cpp:657-1129):
+ *                      for every datastream setValidFlags/setData/setOffsets
+ *                      (mode.cpp:1534-1550) and Mode::process on every FFT
+ *                      block (mode.cpp:634-1374, Mk5Mode::unpack
+ *                      mk5mode.cpp:94-174), then the baseline XMAC
+ *                      (core.cpp:816-982), baseline weights (core.cpp:1005-1052),
+ *                      autocorrelation copy (core.cpp:1166-1376) and
+ *                      visibility copy (core.cpp:1605-1884), writing the Core
+ *                      result array (procslots[].results) layout.
+ *   gx_subint_device   the same with every buffer already in device memory.
+ *   gx_spectra         Mode::getFreqs (mode.h:138) for one block, for
+ *                      incremental adoption behind a GpuMode.
+ */
+#ifndef GXCORR_H
+#define GXCORR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GX_VERSION_MAJOR 0
+#define GX_VERSION_MINOR 1
+
+#define GX_MAX_LOCAL_FREQS 64
+#define GX_MAX_BANDS 128
+#define GX_MAX_POLPRODUCTS 4
+
+typedef enum gx_status {
+  GX_OK = 0,
+  GX_ERR_ARG = 1,          /* invalid argument or descriptor */
+  GX_ERR_UNSUPPORTED = 2,  /* a configuration feature this build does not implement */
+  GX_ERR_CUDA = 3,         /* CUDA runtime failure (message has the CUDA error string) */
+  GX_ERR_NOMEM = 4,        /* device or host allocation failed */
+  GX_ERR_IO = 5,           /* could not read or parse a setup file */
+  GX_ERR_MODEL = 6,        /* no delay model for the requested time (Mode torches the subint) */
+  GX_ERR_TIMEOUT = 7,      /* a bounded device wait gave up */
+  GX_ERR_STATE = 8         /* call out of order */
+} gx_status;
+
+/* X-step forms */
+typedef enum gx_xstep {
+  GX_XSTEP_FP32 = 0,       /* plain FP32 Hermitian cross-multiply-accumulate */
+  GX_XSTEP_TC_FP16 = 1,    /* tcgen05 tensor cores, FP16 spectra, FP32 accumulation */
+  GX_XSTEP_TC_FP16_HILO = 2 /* as above with a split hi+lo FP16 product (3 MMAs) */
+} gx_xstep;
+
+/* One frequency-table entry (FREQ TABLE, configuration.cpp:1970-2022). */
+typedef struct gx_freq_desc {
+  double freq_mhz;         /* FREQ (MHZ): band edge / LO frequency */
+  double bw_mhz;           /* BW (MHZ) */
+  int lower_sideband;      /* SIDEBAND L */
+  int nchan;               /* NUM CHANNELS */
+} gx_freq_desc;
+
+/* One datastream (DATASTREAM TABLE, configuration.cpp:1397-1850).  Only
+ * single-thread VDIF is decoded on the device. */
+typedef struct gx_station_desc {
+  int nbits;               /* QUANTISATION BITS: 1, 2, 4 or 8 */
+  int is_complex;          /* DATA SAMPLING: 0 REAL, 1 COMPLEX (single sideband) */
+  int framebytes;          /* DATA FRAME SIZE including the 32-byte VDIF header */
+  int nrecfreqs;           /* NUM RECORDED FREQS */
+  int recfreq[GX_MAX_LOCAL_FREQS];                 /* REC FREQ INDEX -> freq table */
+  double clock_offset_us[GX_MAX_LOCAL_FREQS];      /* CLK OFFSET (us) */
+  double clock_offset_delta_us[GX_MAX_LOCAL_FREQS];/* second field of CLK OFFSET a:b */
+  double lo_offset_hz[GX_MAX_LOCAL_FREQS];         /* FREQ OFFSET (Hz) */
+  int nbands;              /* recorded bands = sum of NUM REC POLS */
+  int band_localfreq[GX_MAX_BANDS];                /* REC BAND i INDEX */
+  char band_pol[GX_MAX_BANDS];                     /* REC BAND i POL */
+  int clock_int_seconds;   /* floor(CLOCK COEFF 0 / 1e6 + 0.5), subtracted from the delay (mode.cpp:68,1526) */
+} gx_station_desc;
+
+/* One baseline (BASELINE TABLE, configuration.cpp:1033-1180). */
+typedef struct gx_baseline_desc {
+  int ds1, ds2;            /* datastream indices (ds1 is the unconjugated one) */
+  int nfreqs;              /* NUM FREQS */
+  int freq[GX_MAX_LOCAL_FREQS];                            /* freq-table index of each */
+  int npolprod[GX_MAX_LOCAL_FREQS];                        /* POL PRODUCTS */
+  int band1[GX_MAX_LOCAL_FREQS][GX_MAX_POLPRODUCTS];       /* D/STREAM A BAND */
+  int band2[GX_MAX_LOCAL_FREQS][GX_MAX_POLPRODUCTS];       /* D/STREAM B BAND */
+} gx_baseline_desc;
+
+/* One correlation configuration (CONFIGURATIONS section, configuration.cpp:1315). */
+typedef struct gx_job_desc {
+  int nstations;
+  const gx_station_desc *stations;
+  int nfreqs;
+  const gx_freq_desc *freqs;
+  int nbaselines;
+  const gx_baseline_desc *baselines;
+  int subint_ns;           /* SUBINT NANOSECONDS */
+  int guard_ns;            /* GUARD NANOSECONDS */
+  int fringe_rotation_order; /* FRINGE ROTN ORDER (1 supported) */
+  int array_stride;        /* ARRAY STRIDE LEN, 0 = automatic */
+  int xmac_stride;         /* XMAC STRIDE LEN, 0 = automatic */
+  int write_autocorrs;     /* WRITE AUTOCORRS (also enables cross-pol autocorrelations) */
+  int64_t max_data_bytes;  /* largest per-station data buffer one subint will pass */
+  int xstep;               /* gx_xstep */
+  int block_chunk;         /* FFT blocks per device pass, 0 = automatic */
+} gx_job_desc;
+
+/* One subint: the contents of one Core processslot (core.h:76-98). */
+typedef struct gx_subint_desc {
+  int scan, sec, ns;       /* procslots[].offsets: subint start, relative to scan start */
+  double scan_start_sec;   /* Model::getScanStartSec(scan, startmjd, startseconds): wall-clock base */
+  const double *interp;    /* [nstations][3] delay interpolators, us, as Mode::setOffsets leaves them
+                              (intclockseconds already removed); NULL: use the handle's own model */
+  const uint8_t *const *data;    /* [nstations] raw buffers (whole VDIF frames) */
+  const int64_t *datalen;        /* [nstations] bytes */
+  const int32_t *const *control; /* [nstations] control words: [0]=scan [1]=sec [2]=ns of the
+                                    first sample, [3..] valid flags, 30 per word (FLAGS_PER_INT) */
+  int controllen;                /* words per control buffer */
+} gx_subint_desc;
+
+typedef struct gx_handle gx_handle;
+
+/* Layout summary of the Core result array (configuration.cpp:2348-2630). */
+typedef struct gx_layout_info {
+  int64_t result_length;   /* complex floats */
+  int nfreqs, nbaselines, nstations;
+  int blocks_per_send;
+  int xmac_stride;
+  int array_stride;
+  int fftchannels;
+  int nchan;
+} gx_layout_info;
+
+gx_status gx_open(const gx_job_desc *desc, int device, gx_handle **out);
+gx_status gx_open_input(const char *inputfile, int device, int xstep, gx_handle **out);
+gx_status gx_close(gx_handle *h);
+const char *gx_last_error(const gx_handle *h);
+const char *gx_status_string(gx_status s);
+
+gx_status gx_get_layout(const gx_handle *h, gx_layout_info *info);
+/* offsets in complex-float units; arrays sized [nfreqs*nbaselines] and [nstations]; -1 = absent */
+gx_status gx_get_offsets(const gx_handle *h, int *baseline_offsets, int *bweight_offsets,
+                         int *autocorr_offsets, int *acweight_offsets);
+
+gx_status gx_interpolator(gx_handle *h, int station, int scan, int sec, int ns, double out[3]);
+gx_status gx_scan_start_sec(gx_handle *h, int scan, double *out);
+
+/* Host buffers in, host results out (results: result_length complex floats, overwritten). */
+gx_status gx_subint(gx_handle *h, const gx_subint_desc *sub, float *results);
+/* Device buffers in, device results out, on the handle's stream (or `stream` if non-NULL:
+   a cudaStream_t passed as void*).  Does not synchronise. */
+gx_status gx_subint_device(gx_handle *h, const gx_subint_desc *sub, float *dev_results, void *stream);
+gx_status gx_synchronize(gx_handle *h);
+
+/* Spectra of one FFT block of one datastream after the last gx_subint* call
+   (nbands x nchan complex floats, after fractional-sample correction), and its weight. */
+gx_status gx_spectra(gx_handle *h, int station, int block, float *out, float *weight);
+
+/* Device time of the last gx_subint* call per stage, milliseconds: [0] unpack+F, [1] X, [2] finalise. */
+gx_status gx_stage_times(gx_handle *h, float ms[3]);
+
+/* Number of kernel launches issued by the last gx_subint* call. */
+gx_status gx_launch_count(const gx_handle *h, int *count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GXCORR_H */

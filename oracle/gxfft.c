@@ -5,6 +5,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+static const double GX_PI = 3.14159265358979323846264338327950288;
+
 static int is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 
 void gxfft_c2c_f64(double *d, int n, int sign)
@@ -16,7 +18,7 @@ void gxfft_c2c_f64(double *d, int n, int sign)
       double sr = 0, si = 0;
       for (int j = 0; j < n; j++) {
         long long m = ((long long)j * k) % n;
-        double a = sign * 2.0 * M_PI * (double)m / (double)n;
+        double a = sign * 2.0 * GX_PI * (double)m / (double)n;
         double c = cos(a), s = sin(a);
         sr += d[2*j] * c - d[2*j+1] * s;
         si += d[2*j] * s + d[2*j+1] * c;
@@ -42,7 +44,7 @@ void gxfft_c2c_f64(double *d, int n, int sign)
     int half = len >> 1;
     for (int k = 0; k < half; k++) {
       /* twiddle evaluated directly (no recurrence) for accuracy */
-      double a = sign * 2.0 * M_PI * (double)k / (double)len;
+      double a = sign * 2.0 * GX_PI * (double)k / (double)len;
       double wr = cos(a), wi = sin(a);
       for (int s = 0; s < n; s += len) {
         int p = s + k, q = p + half;

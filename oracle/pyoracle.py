@@ -1,0 +1,154 @@
+"""Python access to the oracle (TEST INFRASTRUCTURE ONLY).
+
+* :class:`Oracle` -- the C restatement in gxoracle.c (``_ref/libgxoracle.so``).
+* :class:`Reference` -- the reference correlator's own hot path compiled from
+  its sources with the harness in ref_harness.cpp (``_ref/libdifxref.so``).
+
+Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` use this module, as the checker.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from typing import Optional
+
+import numpy as np
+
+from difx_b200 import capi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+ORACLE_LIB = os.path.join(REF_DIR, "libgxoracle.so")
+REFERENCE_LIB = os.path.join(REF_DIR, "libdifxref.so")
+REFERENCE_SRC = "/root/reference"
+
+
+def build(reference: bool = True) -> None:
+    """Build the oracle (and, where the reference tree exists, the reference harness)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    if reference and os.path.isdir(REFERENCE_SRC):
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "-j8"], check=True)
+
+
+def reference_available() -> bool:
+    return os.path.exists(REFERENCE_LIB)
+
+
+class gxo_params(C.Structure):
+    _fields_ = [("precision", C.c_int), ("nthreads", C.c_int), ("num_buffered_ffts", C.c_int),
+                ("xc_avg_ns", C.c_longlong), ("ac_avg_ns", C.c_longlong)]
+
+
+FP32_REF = 0
+FP64 = 1
+
+
+class Oracle:
+    def __init__(self):
+        if not os.path.exists(ORACLE_LIB):
+            build(reference=False)
+        self.lib = C.CDLL(ORACLE_LIB)
+        self.lib.gxo_layout.restype = C.c_longlong
+        self.lib.gxo_unpack.restype = C.c_int
+
+    def layout(self, jd: capi.JobDesc):
+        d = jd.desc
+        nfb = max(1, d.nfreqs * d.nbaselines)
+        bl = np.zeros(nfb, np.int32)
+        bw = np.zeros(nfb, np.int32)
+        ac = np.zeros(d.nstations, np.int32)
+        acw = np.zeros(d.nstations, np.int32)
+        rl = self.lib.gxo_layout(jd.ptr(), bl.ctypes.data_as(C.c_void_p), bw.ctypes.data_as(C.c_void_p),
+                                 ac.ctypes.data_as(C.c_void_p), acw.ctypes.data_as(C.c_void_p))
+        return int(rl), bl, bw, ac, acw
+
+    def params(self, precision=FP32_REF, nthreads=1, num_buffered_ffts=10,
+               xc_avg_ns=2_000_000_000, ac_avg_ns=2_000_000_000):
+        return gxo_params(precision, nthreads, num_buffered_ffts, xc_avg_ns, ac_avg_ns)
+
+    def subint(self, jd: capi.JobDesc, sd: capi.SubintDesc, params: gxo_params) -> np.ndarray:
+        rl = self.layout(jd)[0]
+        out = np.zeros(2 * rl, np.float64)
+        self.lib.gxo_subint(jd.ptr(), sd.ptr(), C.byref(params), out.ctypes.data_as(C.c_void_p))
+        return out[0::2] + 1j * out[1::2]
+
+    def station_block(self, jd: capi.JobDesc, sd: capi.SubintDesc, station: int, block: int,
+                      params: gxo_params):
+        st = jd.desc.stations[station]
+        n = jd.desc.freqs[st.recfreq[0]].nchan
+        out = np.zeros(2 * st.nbands * n, np.float64)
+        w = C.c_double(0)
+        self.lib.gxo_station_block(jd.ptr(), sd.ptr(), station, block, C.byref(params),
+                                   out.ctypes.data_as(C.c_void_p), C.byref(w))
+        return (out[0::2] + 1j * out[1::2]).reshape(st.nbands, n), w.value
+
+    def unpack(self, jd: capi.JobDesc, station: int, data: np.ndarray, offset: int, nsamp: int):
+        st = jd.desc.stations[station]
+        fs = (st.framebytes - 32) * 8 // (st.nbits * st.nbands)
+        if st.is_complex:
+            fs //= 2
+        per = nsamp * (2 if st.is_complex else 1)
+        out = np.zeros(st.nbands * per, np.float32)
+        good = self.lib.gxo_unpack(C.byref(st), fs, data.ctypes.data_as(C.c_void_p), C.c_longlong(len(data)),
+                                   offset, nsamp, out.ctypes.data_as(C.c_void_p))
+        return out.reshape(st.nbands, per), good
+
+
+class Reference:
+    """The reference's own Configuration/Mode/Core, driven through ref_harness.cpp."""
+
+    def __init__(self, inputfile: str):
+        if not os.path.exists(REFERENCE_LIB):
+            raise RuntimeError("reference harness not built (oracle/_ref/libdifxref.so)")
+        self.lib = C.CDLL(REFERENCE_LIB)
+        self.lib.ref_open.restype = C.c_void_p
+        h = self.lib.ref_open(inputfile.encode())
+        if not h:
+            raise RuntimeError(f"reference could not open {inputfile}")
+        self.h = C.c_void_p(h)
+        self.result_length = self.lib.ref_result_length(self.h)
+        self.blocks_per_send = self.lib.ref_blocks_per_send(self.h)
+        self.nthreads = self.lib.ref_num_threads(self.h)
+
+    def layout(self, nfreqs: int, nbaselines: int, nstations: int):
+        bl = np.zeros(max(1, nfreqs * nbaselines), np.int32)
+        bw = np.zeros_like(bl)
+        ac = np.zeros(nstations, np.int32)
+        acw = np.zeros(nstations, np.int32)
+        self.lib.ref_layout(self.h, bl.ctypes.data_as(C.c_void_p), bw.ctypes.data_as(C.c_void_p),
+                            ac.ctypes.data_as(C.c_void_p), acw.ctypes.data_as(C.c_void_p))
+        return self.result_length, bl, bw, ac, acw
+
+    def interpolator(self, station: int, scan: int, sec: int, ns: int) -> np.ndarray:
+        out = np.zeros(3, np.float64)
+        self.lib.ref_interpolator(self.h, station, scan, sec, ns, out.ctypes.data_as(C.c_void_p))
+        return out
+
+    def process(self, si) -> np.ndarray:
+        n = len(si.data)
+        datap = (C.c_void_p * n)(*[d.ctypes.data for d in si.data])
+        lens = (C.c_int * n)(*[len(d) for d in si.data])
+        ctrl = (C.c_void_p * n)(*[c.ctypes.data for c in si.control])
+        res = np.zeros(2 * self.result_length, np.float32)
+        self.lib.ref_process(self.h, si.scan, si.sec, si.ns, datap, lens, ctrl, len(si.control[0]),
+                             res.ctypes.data_as(C.c_void_p))
+        return res[0::2] + 1j * res[1::2]
+
+    def mode_block(self, si, station: int, block: int, nbands: int, nchan: int):
+        sp = np.zeros(2 * nbands * nchan, np.float32)
+        w = C.c_float(0)
+        self.lib.ref_mode_block(self.h, station, si.data[station].ctypes.data_as(C.c_void_p),
+                                len(si.data[station]), si.control[station].ctypes.data_as(C.c_void_p),
+                                len(si.control[station]), si.scan, si.sec, si.ns, block,
+                                sp.ctypes.data_as(C.c_void_p), C.byref(w))
+        return (sp[0::2] + 1j * sp[1::2]).reshape(nbands, nchan), w.value
+
+    def unpack(self, station: int, data: np.ndarray, offset: int, nbands: int, per: int):
+        out = np.zeros(nbands * per * 2, np.float32)
+        w = C.c_float(0)
+        us = C.c_int(0)
+        n = self.lib.ref_unpack(self.h, station, data.ctypes.data_as(C.c_void_p), len(data), offset,
+                                out.ctypes.data_as(C.c_void_p), C.byref(w), C.byref(us))
+        return out, w.value, us.value, n
