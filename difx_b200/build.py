@@ -1,0 +1,71 @@
+"""Build libgxcorr.so in-tree (nvcc, sm_100a).
+
+    python -m difx_b200.build            # builds difx_b200/libgxcorr.so
+
+The host C++ is compiled by the system g++ (``-ccbin``) so the library links
+the system libstdc++ dynamically, like every other extension loaded into the
+Python process.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libgxcorr.so")
+BUILD = os.path.join(HERE, "_build")
+
+SOURCES = ["gx_fstep.cu", "gx_xstep.cu", "gx_tcxmac.cu", "gx_api.cpp", "gx_input.cpp"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+    for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if c and os.path.exists(c):
+            return c
+    raise RuntimeError("nvcc not found")
+
+
+def host_cxx() -> str:
+    return "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else (shutil.which("g++") or "g++")
+
+
+def build(verbose: bool = False, force: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    srcs = [s for s in SOURCES if os.path.exists(os.path.join(CSRC, s))]
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(HERE, "..", "include", "gxcorr.h")]
+    newest = max(os.path.getmtime(p) for p in deps)
+    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= newest:
+        return LIB
+    objs = []
+    common = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-ccbin", host_cxx(),
+              "-I" + os.path.join(HERE, "..", "include")]
+    for s in srcs:
+        o = os.path.join(BUILD, s + ".o")
+        cmd = [nvcc()] + ARCH + common + ["-c", os.path.join(CSRC, s), "-o", o]
+        if s.endswith(".cu"):
+            cmd += ["-Xptxas", "-v"] if verbose else []
+        if verbose:
+            print(" ".join(cmd))
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            sys.stderr.write(r.stdout + r.stderr)
+            raise RuntimeError(f"nvcc failed on {s}")
+        if verbose and r.stderr:
+            sys.stderr.write(r.stderr)
+        objs.append(o)
+    tmp = LIB + ".tmp"
+    cmd = [nvcc()] + ARCH + ["-shared", "-ccbin", host_cxx(), "-o", tmp] + objs + ["-lcudart"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("link failed")
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv, force=True))

@@ -1,0 +1,770 @@
+// gxcorr host driver: the C ABI of include/gxcorr.h.
+//
+// gx_open derives, from a gx_job_desc, what Configuration::getMode and
+// Configuration::populateResultLengths derive from the .input tables
+// (mpifxcorr/src/configuration.cpp:932-998, 2348-2630, setStrides 2701-2734,
+// calcstridelength 38-50, calcgoodxmacstridelength 2653-2698), allocates the
+// device buffers once, and precomputes the tables that map the X-step
+// accumulators onto the Core result array.  gx_subint[_device] then runs one
+// Core slot: F-step and X-step over chunks of FFT blocks, then one
+// finalising pass writing the result array.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+#include "../../include/gxcorr.h"
+#include "gx_dev.h"
+#include "gx_xstep.h"
+#include "gx_host.h"
+
+using namespace gx;
+
+namespace {
+
+int stride_length(int n)  // calcstridelength, configuration.cpp:38-50
+{
+  if (n <= 16) return n;
+  for (unsigned int g = (unsigned int)std::sqrt(n + 0.1);; --g)
+    if (n % g == 0) return n / (int)g;
+}
+
+long gcdl(long a, long b)
+{
+  while (b) { long t = a % b; a = b; b = t; }
+  return a;
+}
+
+}  // namespace
+
+struct gx_handle {
+  std::string err;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = true;
+
+  std::vector<gx_station_desc> st;
+  std::vector<gx_freq_desc> fr;
+  std::vector<gx_baseline_desc> bl;
+  gx_job_desc jd{};
+
+  DevJob J{};
+  int maxnrf = 1, nslots = 1, chunk = 0, ks = 1, xmac_stride = 0, maxprod = 0;
+  XmacShape xs{};
+  long long rl = 0;
+  std::vector<int> blofs, bwofs, acofs, acwofs;
+  std::vector<std::vector<int>> band_input;  // [station][band]
+  std::vector<ProdEntry> prods;
+  std::vector<WeightEntry> wents;
+  std::vector<int2> pairs;
+
+  DevStation *d_st = nullptr;
+  float2 *d_tw = nullptr, *d_spec = nullptr, *d_acc = nullptr, *d_results = nullptr, *d_spec1 = nullptr;
+  float *d_w = nullptr, *d_wacc = nullptr, *d_w1 = nullptr;
+  size_t acc_slice = 0;  // float2 per K-split slice
+  int2 *d_pairs = nullptr;
+  ProdEntry *d_prods = nullptr;
+  WeightEntry *d_went = nullptr;
+  const uint8_t **d_dataptrs = nullptr;
+  int64_t *d_datalen = nullptr;
+  int32_t *d_ctrl = nullptr;
+  int ctrlstride = 0;
+  double *d_interp = nullptr;
+  std::vector<uint8_t *> d_data;
+  std::vector<int64_t> data_cap;
+
+  SubintArrays last{};
+  bool have_last = false;
+  std::vector<cudaEvent_t> evs;  // pairs per launch: [start, end]
+  std::vector<int> ev_stage;
+  int launches = 0;
+
+  std::unique_ptr<HostModel> model;  // only for gx_open_input
+
+  gx_status fail(gx_status s, const std::string &m)
+  {
+    err = m;
+    return s;
+  }
+  gx_status cuda(cudaError_t e, const char *what)
+  {
+    if (e == cudaSuccess) return GX_OK;
+    err = std::string(what) + ": " + cudaGetErrorString(e);
+    return GX_ERR_CUDA;
+  }
+};
+
+#define CKR(h, call)                                         \
+  do {                                                       \
+    gx_status _s = (h)->cuda((call), #call);                 \
+    if (_s != GX_OK) return _s;                              \
+  } while (0)
+
+static void free_all(gx_handle *h)
+{
+  if (h->device < 0) return;
+  void *ptrs[] = {h->d_st, h->d_tw, h->d_spec, h->d_acc, h->d_results, h->d_spec1, h->d_w, h->d_wacc, h->d_w1,
+                  h->d_pairs, h->d_prods, h->d_went, (void *)h->d_dataptrs, h->d_datalen, h->d_ctrl, h->d_interp};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  for (auto p : h->d_data)
+    if (p) cudaFree(p);
+  for (auto e : h->evs) cudaEventDestroy(e);
+  h->evs.clear();
+  if (h->stream && h->own_stream) cudaStreamDestroy(h->stream);
+}
+
+static int bl_localfreq(const gx_baseline_desc &b, int f)
+{
+  int r = -1;
+  for (int j = 0; j < b.nfreqs; j++)
+    if (b.freq[j] == f) r = j;
+  return r;
+}
+
+static gx_status setup(gx_handle *h)
+{
+  const gx_job_desc &d = h->jd;
+  if (d.nstations < 1 || !d.stations || d.nfreqs < 1 || !d.freqs || d.nbaselines < 0)
+    return h->fail(GX_ERR_ARG, "job descriptor: missing stations or freqs");
+  if (d.fringe_rotation_order != 1)
+    return h->fail(GX_ERR_UNSUPPORTED, "only FRINGE ROTN ORDER 1 is implemented");
+  const gx_station_desc &s0 = d.stations[0];
+  for (int s = 0; s < d.nstations; s++) {
+    const gx_station_desc &x = d.stations[s];
+    if (x.nbits != s0.nbits || x.is_complex != s0.is_complex || x.framebytes != s0.framebytes ||
+        x.nbands != s0.nbands)
+      return h->fail(GX_ERR_UNSUPPORTED, "all datastreams must share bits, sampling, frame size and band count");
+    if (x.nrecfreqs < 1 || x.nrecfreqs > GX_MAX_LOCAL_FREQS || x.nbands < 1 || x.nbands > GX_MAX_BANDS)
+      return h->fail(GX_ERR_ARG, "datastream freq/band count out of range");
+    for (int i = 0; i < x.nrecfreqs; i++)
+      if (x.recfreq[i] < 0 || x.recfreq[i] >= d.nfreqs) return h->fail(GX_ERR_ARG, "REC FREQ INDEX out of range");
+    for (int b = 0; b < x.nbands; b++)
+      if (x.band_localfreq[b] < 0 || x.band_localfreq[b] >= x.nrecfreqs)
+        return h->fail(GX_ERR_ARG, "REC BAND INDEX out of range");
+  }
+  if (s0.nbits != 1 && s0.nbits != 2 && s0.nbits != 4 && s0.nbits != 8)
+    return h->fail(GX_ERR_UNSUPPORTED, "QUANTISATION BITS must be 1, 2, 4 or 8");
+  const gx_freq_desc &f0 = d.freqs[s0.recfreq[0]];
+  for (int f = 0; f < d.nfreqs; f++)
+    if (d.freqs[f].nchan != f0.nchan || d.freqs[f].bw_mhz != f0.bw_mhz)
+      return h->fail(GX_ERR_UNSUPPORTED, "all freqs must share bandwidth and channel count");
+  const int cplx = s0.is_complex ? 1 : 0;
+  const int bits_ts = s0.nbands * s0.nbits * (cplx ? 2 : 1);
+  if (bits_ts % 8 != 0)
+    return h->fail(GX_ERR_UNSUPPORTED, "a time sample of all bands must fill whole bytes (sample granularity 1)");
+  const int payload = s0.framebytes - 32;
+  if (payload <= 0 || (payload * 8) % bits_ts != 0 || payload % 8 != 0)
+    return h->fail(GX_ERR_ARG, "DATA FRAME SIZE is not a whole number of time samples");
+
+  DevJob &J = h->J;
+  J.nstations = d.nstations;
+  J.nbands = s0.nbands;
+  J.nbits = s0.nbits;
+  J.cplx = cplx;
+  J.framebytes = s0.framebytes;
+  J.framesamples = payload * 8 / (s0.nbits * s0.nbands);
+  if (cplx) J.framesamples /= 2;
+  J.bytespersample = bits_ts / 8;
+  J.nchan = f0.nchan;
+  J.fftlen = cplx ? f0.nchan : 2 * f0.nchan;
+  if (J.fftlen & (J.fftlen - 1)) return h->fail(GX_ERR_UNSUPPORTED, "FFT length must be a power of two");
+  if (J.fftlen < 16 || J.fftlen > 8192) return h->fail(GX_ERR_UNSUPPORTED, "FFT length must be in [16, 8192]");
+  J.stride = d.array_stride > 0 ? d.array_stride : stride_length(f0.nchan);
+  if (J.fftlen % J.stride) return h->fail(GX_ERR_ARG, "array stride does not divide the FFT length");
+  J.nfr = J.fftlen / J.stride;
+  J.half = (cplx ? 2 * J.nfr : J.nfr) / 2;
+  J.unpacksamples = cplx ? f0.nchan : 2 * f0.nchan;
+  J.sampletime = 1.0 / (2.0 * f0.bw_mhz);
+  if (cplx) J.sampletime *= 2.0;
+  J.bw = f0.bw_mhz;
+  J.nfreqs = d.nfreqs;
+  {
+    double ffttime = 1000.0 * f0.nchan / f0.bw_mhz;
+    double b = d.subint_ns / ffttime;
+    J.blocks_per_send = (int)(b + 0.5);
+    if (std::fabs(b - J.blocks_per_send) > 1e-9 || J.blocks_per_send < 1)
+      return h->fail(GX_ERR_ARG, "SUBINT NANOSECONDS is not a whole number of FFT blocks");
+  }
+  J.flaglen = J.blocks_per_send / 30 + (J.blocks_per_send % 30 ? 1 : 0);
+  if ((J.unpacksamples + J.framesamples - 1) / J.framesamples + 1 > kMaxFramesPerBlock)
+    return h->fail(GX_ERR_UNSUPPORTED, "an FFT block spans too many frames");
+
+  // xmac stride (does not change results; reported for layout parity)
+  {
+    int g = 0;
+    for (int j = 0; j < d.nbaselines; j++)
+      for (int k = 0; k < d.baselines[j].nfreqs; k++) {
+        int n = d.freqs[d.baselines[j].freq[k]].nchan;
+        g = g ? (int)gcdl(g, n) : n;
+      }
+    if (d.xmac_stride > 0) h->xmac_stride = d.xmac_stride;
+    else {
+      double err = 1e12;
+      for (int guess = g; guess > 0; --guess) {
+        if (g % guess) continue;
+        double e = std::fabs((double)guess - 150);
+        if (e < err) { err = e; h->xmac_stride = guess; }
+      }
+    }
+  }
+
+  // spectra rows: every (station, band) of a freq gets one input row
+  std::vector<int> count(d.nfreqs, 0);
+  h->band_input.assign(d.nstations, std::vector<int>(s0.nbands, -1));
+  h->maxnrf = 1;
+  std::vector<DevStation> dst(d.nstations);
+  for (int s = 0; s < d.nstations; s++) {
+    const gx_station_desc &x = d.stations[s];
+    DevStation &D = dst[s];
+    memset(&D, 0, sizeof(D));
+    D.nrecfreqs = x.nrecfreqs;
+    if (x.nrecfreqs > h->maxnrf) h->maxnrf = x.nrecfreqs;
+    for (int i = 0; i < x.nrecfreqs; i++) {
+      const gx_freq_desc &fq = d.freqs[x.recfreq[i]];
+      double lo = fq.freq_mhz;
+      if (std::fabs(lo - (int)(lo + 0.5)) > (double)0.000000001f) D.fractional_lo = 1;
+      if (x.clock_offset_delta_us[i] != 0.0) D.deltapol = 1;
+      D.lofreq[i] = (cplx && fq.lower_sideband) ? -lo : lo;
+      D.lsb[i] = fq.lower_sideband ? 1 : 0;
+      D.freq_index[i] = x.recfreq[i];
+      D.clk[i] = x.clock_offset_us[i];
+      D.clkdelta[i] = x.clock_offset_delta_us[i];
+      D.looff[i] = x.lo_offset_hz[i];
+    }
+    for (int b = 0; b < x.nbands; b++) {
+      int f = x.recfreq[x.band_localfreq[b]];
+      D.band_localfreq[b] = x.band_localfreq[b];
+      D.band_input[b] = count[f]++;
+      h->band_input[s][b] = D.band_input[b];
+    }
+    for (int b = 0; b < x.nbands; b++) D.band_polb[b] = (D.deltapol && x.band_pol[b] != 'R') ? 1 : 0;
+  }
+  int ni = 0;
+  for (int f = 0; f < d.nfreqs; f++) ni = count[f] > ni ? count[f] : ni;
+  h->xs = xmac_shape(ni);
+  J.ninputs = h->xs.nsuper * h->xs.ST;
+  h->xs = xmac_shape(J.ninputs);
+
+  // Core result layout (populateResultLengths, one phase centre, no bins, no averaging)
+  const int nbl = d.nbaselines;
+  auto freq_used = [&](int f) {
+    for (int j = 0; j < nbl; j++)
+      if (bl_localfreq(d.baselines[j], f) >= 0) return true;
+    return false;
+  };
+  h->maxprod = 0;
+  for (int j = 0; j < nbl; j++)
+    for (int k = 0; k < d.baselines[j].nfreqs; k++) {
+      if (d.baselines[j].npolprod[k] > h->maxprod) h->maxprod = d.baselines[j].npolprod[k];
+      if (d.baselines[j].npolprod[k] < 1 || d.baselines[j].npolprod[k] > GX_MAX_POLPRODUCTS)
+        return h->fail(GX_ERR_ARG, "POL PRODUCTS out of range");
+    }
+  const int bpa = h->maxprod > 2 ? 2 : 1;
+  h->blofs.assign(d.nfreqs * (nbl ? nbl : 1), -1);
+  h->bwofs.assign(d.nfreqs * (nbl ? nbl : 1), -1);
+  h->acofs.assign(d.nstations, 0);
+  h->acwofs.assign(d.nstations, 0);
+  long long idx = 0;
+  for (int f = 0; f < d.nfreqs; f++) {
+    if (!freq_used(f)) continue;
+    for (int j = 0; j < nbl; j++) {
+      int lf = bl_localfreq(d.baselines[j], f);
+      if (lf < 0) continue;
+      h->blofs[f * nbl + j] = (int)idx;
+      idx += (long long)d.baselines[j].npolprod[lf] * d.freqs[f].nchan;
+    }
+  }
+  for (int f = 0; f < d.nfreqs; f++) {
+    if (!freq_used(f)) continue;
+    for (int j = 0; j < nbl; j++) {
+      int lf = bl_localfreq(d.baselines[j], f);
+      if (lf < 0) continue;
+      h->bwofs[f * nbl + j] = (int)idx;
+      int np = d.baselines[j].npolprod[lf];
+      idx += np / 2 + np % 2;
+    }
+  }
+  for (int s = 0; s < d.nstations; s++) {
+    h->acofs[s] = (int)idx;
+    const gx_station_desc &x = d.stations[s];
+    for (int b = 0; b < x.nbands; b++)
+      if (freq_used(x.recfreq[x.band_localfreq[b]])) idx += (long long)bpa * J.nchan;
+  }
+  for (int s = 0; s < d.nstations; s++) {
+    h->acwofs[s] = (int)idx;
+    const gx_station_desc &x = d.stations[s];
+    int add = 0;
+    for (int b = 0; b < x.nbands; b++)
+      if (freq_used(x.recfreq[x.band_localfreq[b]])) add += bpa;
+    add = (add + 1) / 2;
+    if (add == 0) add = 1;
+    idx += add;
+  }
+  h->rl = idx;
+
+  // accumulator index of the Hermitian entry (a, b) of freq f
+  const XmacShape &xs = h->xs;
+  auto acc_index = [&](int f, int a, int b, int &conj) -> long long {
+    conj = 0;
+    if (a / xs.T > b / xs.T) { int t = a; a = b; b = t; conj = 1; }
+    int SI = a / xs.ST, SJ = b / xs.ST;
+    long long stp = 0;
+    for (int i = 0; i < SI; i++) stp += xs.nsuper - i;
+    stp += SJ - SI;
+    return (((long long)f * xs.npairs + stp) * xs.ST * xs.ST + (long long)(a % xs.ST) * xs.ST + (b % xs.ST)) *
+           J.nchan;
+  };
+  h->prods.clear();
+  h->wents.clear();
+  h->pairs.clear();
+  for (int j = 0; j < nbl; j++) {
+    const gx_baseline_desc &B = d.baselines[j];
+    if (B.ds1 < 0 || B.ds1 >= d.nstations || B.ds2 < 0 || B.ds2 >= d.nstations)
+      return h->fail(GX_ERR_ARG, "baseline datastream index out of range");
+    h->pairs.push_back(make_int2(B.ds1, B.ds2));
+  }
+  for (int f = 0; f < d.nfreqs; f++) {
+    for (int j = 0; j < nbl; j++) {
+      const gx_baseline_desc &B = d.baselines[j];
+      int lf = bl_localfreq(B, f);
+      if (lf < 0) continue;
+      for (int p = 0; p < B.npolprod[lf]; p++) {
+        int b1 = B.band1[lf][p], b2 = B.band2[lf][p];
+        if (b1 < 0 || b1 >= d.stations[B.ds1].nbands || b2 < 0 || b2 >= d.stations[B.ds2].nbands)
+          return h->fail(GX_ERR_UNSUPPORTED, "baseline band index out of range (zoom bands are not implemented)");
+        int a = h->band_input[B.ds1][b1], bb = h->band_input[B.ds2][b2];
+        ProdEntry e{};
+        e.result_offset = h->blofs[f * nbl + j] + (long long)p * J.nchan;
+        e.acc_index = acc_index(f, a, bb, e.conj);
+        h->prods.push_back(e);
+        WeightEntry w{};
+        w.float_index = 2LL * h->bwofs[f * nbl + j] + p;
+        w.source = d.nstations + j;
+        h->wents.push_back(w);
+      }
+    }
+  }
+  const bool writecross = d.write_autocorrs && h->maxprod > 2;
+  for (int s = 0; s < d.nstations; s++) {
+    const gx_station_desc &x = d.stations[s];
+    long long ro = h->acofs[s];
+    long long wo = 2LL * h->acwofs[s];
+    std::vector<int> used;
+    for (int b = 0; b < x.nbands; b++)
+      if (freq_used(x.recfreq[x.band_localfreq[b]])) used.push_back(b);
+    for (int b : used) {
+      int f = x.recfreq[x.band_localfreq[b]];
+      int a = h->band_input[s][b];
+      ProdEntry e{};
+      e.result_offset = ro;
+      e.acc_index = acc_index(f, a, a, e.conj);
+      h->prods.push_back(e);
+      ro += J.nchan;
+      WeightEntry w{};
+      w.float_index = wo++;
+      w.source = s;
+      h->wents.push_back(w);
+    }
+    if (writecross) {
+      for (int b : used) {
+        int lf = x.band_localfreq[b];
+        int f = x.recfreq[lf];
+        // partner: indices[0], indices[1] of this freq (mode.cpp:1124-1129, 1333-1351)
+        int i0 = -1, i1 = -1;
+        for (int q = 0; q < x.nbands; q++)
+          if (x.band_localfreq[q] == lf) {
+            if (i0 < 0) i0 = q;
+            else if (i1 < 0) i1 = q;
+          }
+        int partner = (b == i0) ? i1 : ((b == i1) ? i0 : -1);
+        WeightEntry w{};
+        w.float_index = wo++;
+        w.source = partner >= 0 ? s : -1;
+        h->wents.push_back(w);
+        if (partner >= 0) {
+          ProdEntry e{};
+          e.result_offset = ro;
+          e.acc_index = acc_index(f, h->band_input[s][b], h->band_input[s][partner], e.conj);
+          h->prods.push_back(e);
+        }
+        ro += J.nchan;
+      }
+    }
+  }
+
+  // chunking and K-split
+  const size_t per_block = (size_t)d.nfreqs * J.ninputs * J.nchan * sizeof(float2);
+  int chunk = d.block_chunk > 0 ? d.block_chunk : (int)std::min<size_t>(4096, std::max<size_t>(64, (size_t)(2u << 30) / per_block));
+  if (chunk > J.blocks_per_send) chunk = J.blocks_per_send;
+  chunk = std::max(1, chunk);
+  h->chunk = chunk;
+  {
+    long long base = (long long)((J.nchan + xs.CT - 1) / xs.CT) * xs.npairs * d.nfreqs;
+    int ks = (int)((296 + base - 1) / base);
+    ks = std::max(1, std::min(ks, 16));
+    ks = std::max(1, std::min(ks, chunk / 16 > 0 ? chunk / 16 : 1));
+    h->ks = ks;
+  }
+  // F-step concurrency: FFT slots per CTA
+  {
+    int ns = std::min(J.nbands, 32);
+    while (ns > 1 && (fstep_smem_bytes(J, h->maxnrf, ns) > 200 * 1024 || kFThreads % ns)) ns--;
+    h->nslots = ns;
+    if (fstep_smem_bytes(J, h->maxnrf, ns) > 227 * 1024)
+      return h->fail(GX_ERR_UNSUPPORTED, "F-step shared memory exceeds 227 KB");
+  }
+
+  // ---------------------------------------------------------- device state
+  if (h->device < 0) return GX_OK;  // host-only handle: layout and model queries
+  CKR(h, cudaSetDevice(h->device));
+  if (!h->stream) CKR(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  CKR(h, cudaMalloc(&h->d_st, sizeof(DevStation) * d.nstations));
+  CKR(h, cudaMemcpy(h->d_st, dst.data(), sizeof(DevStation) * d.nstations, cudaMemcpyHostToDevice));
+  {
+    std::vector<float2> tw(J.fftlen);
+    for (int m = 0; m < J.fftlen; m++) {
+      double a = -2.0 * M_PI * (double)m / (double)J.fftlen;
+      tw[m] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    CKR(h, cudaMalloc(&h->d_tw, sizeof(float2) * J.fftlen));
+    CKR(h, cudaMemcpy(h->d_tw, tw.data(), sizeof(float2) * J.fftlen, cudaMemcpyHostToDevice));
+    J.twiddle = h->d_tw;
+  }
+  {
+    // decode tables (format_vdif.c:66-146): 2-bit {-HiMag,-1,1,HiMag}, 1-bit {-1,1},
+    // 4-bit (l-7.5)/2.95, 8-bit (b-128)/3.3 or (b-127.5)/3.3 with SYMMETRIC_8_BIT_VDIF
+    float lut[256];
+    memset(lut, 0, sizeof(lut));
+    const float himag = 3.3359f;
+    if (J.nbits == 1) { lut[0] = -1.0f; lut[1] = 1.0f; }
+    else if (J.nbits == 2) { lut[0] = -himag; lut[1] = -1.0f; lut[2] = 1.0f; lut[3] = himag; }
+    else if (J.nbits == 4) { for (int l = 0; l < 16; l++) lut[l] = (float)((l - 7.5) / (double)2.95f); }
+    else {
+      double off = getenv("SYMMETRIC_8_BIT_VDIF") ? 127.5 : 128.0;
+      for (int b = 0; b < 256; b++) lut[b] = (float)((b - off) / 3.3);
+    }
+    CKR(h, fstep_set_lut(lut, h->stream));
+  }
+  const size_t spec_elems = (size_t)d.nfreqs * chunk * J.ninputs * J.nchan;
+  CKR(h, cudaMalloc(&h->d_spec, sizeof(float2) * spec_elems));
+  CKR(h, cudaMemsetAsync(h->d_spec, 0, sizeof(float2) * spec_elems, h->stream));
+  CKR(h, cudaMalloc(&h->d_spec1, sizeof(float2) * (size_t)d.nfreqs * J.ninputs * J.nchan));
+  CKR(h, cudaMemsetAsync(h->d_spec1, 0, sizeof(float2) * (size_t)d.nfreqs * J.ninputs * J.nchan, h->stream));
+  CKR(h, cudaMalloc(&h->d_w, sizeof(float) * (size_t)d.nstations * chunk));
+  CKR(h, cudaMalloc(&h->d_w1, sizeof(float) * (size_t)d.nstations));
+  h->acc_slice = (size_t)d.nfreqs * xs.npairs * xs.ST * xs.ST * J.nchan;
+  CKR(h, cudaMalloc(&h->d_acc, sizeof(float2) * h->acc_slice * h->ks));
+  CKR(h, cudaMalloc(&h->d_wacc, sizeof(float) * (d.nstations + nbl)));
+  if (nbl) {
+    CKR(h, cudaMalloc(&h->d_pairs, sizeof(int2) * nbl));
+    CKR(h, cudaMemcpy(h->d_pairs, h->pairs.data(), sizeof(int2) * nbl, cudaMemcpyHostToDevice));
+  }
+  CKR(h, cudaMalloc(&h->d_prods, sizeof(ProdEntry) * std::max<size_t>(1, h->prods.size())));
+  if (!h->prods.empty())
+    CKR(h, cudaMemcpy(h->d_prods, h->prods.data(), sizeof(ProdEntry) * h->prods.size(), cudaMemcpyHostToDevice));
+  CKR(h, cudaMalloc(&h->d_went, sizeof(WeightEntry) * std::max<size_t>(1, h->wents.size())));
+  if (!h->wents.empty())
+    CKR(h, cudaMemcpy(h->d_went, h->wents.data(), sizeof(WeightEntry) * h->wents.size(), cudaMemcpyHostToDevice));
+  CKR(h, cudaMalloc(&h->d_results, sizeof(float2) * h->rl));
+  CKR(h, cudaMalloc((void **)&h->d_dataptrs, sizeof(uint8_t *) * d.nstations));
+  CKR(h, cudaMalloc(&h->d_datalen, sizeof(int64_t) * d.nstations));
+  h->ctrlstride = 3 + J.flaglen;
+  CKR(h, cudaMalloc(&h->d_ctrl, sizeof(int32_t) * h->ctrlstride * d.nstations));
+  CKR(h, cudaMalloc(&h->d_interp, sizeof(double) * 3 * d.nstations));
+  h->d_data.assign(d.nstations, nullptr);
+  h->data_cap.assign(d.nstations, 0);
+  if (d.max_data_bytes > 0) {
+    for (int s = 0; s < d.nstations; s++) {
+      CKR(h, cudaMalloc(&h->d_data[s], d.max_data_bytes));
+      h->data_cap[s] = d.max_data_bytes;
+    }
+  }
+  CKR(h, cudaStreamSynchronize(h->stream));
+  return GX_OK;
+}
+
+extern "C" {
+
+const char *gx_status_string(gx_status s)
+{
+  switch (s) {
+    case GX_OK: return "ok";
+    case GX_ERR_ARG: return "invalid argument";
+    case GX_ERR_UNSUPPORTED: return "unsupported configuration";
+    case GX_ERR_CUDA: return "CUDA error";
+    case GX_ERR_NOMEM: return "out of memory";
+    case GX_ERR_IO: return "I/O or parse error";
+    case GX_ERR_MODEL: return "no delay model";
+    case GX_ERR_TIMEOUT: return "device wait timed out";
+    case GX_ERR_STATE: return "call out of order";
+  }
+  return "unknown";
+}
+
+gx_status gx_open(const gx_job_desc *desc, int device, gx_handle **out)
+{
+  if (!desc || !out) return GX_ERR_ARG;
+  *out = nullptr;
+  gx_handle *h = new gx_handle();
+  h->device = device;
+  h->jd = *desc;
+  if (desc->stations && desc->nstations > 0) h->st.assign(desc->stations, desc->stations + desc->nstations);
+  if (desc->freqs && desc->nfreqs > 0) h->fr.assign(desc->freqs, desc->freqs + desc->nfreqs);
+  if (desc->baselines && desc->nbaselines > 0)
+    h->bl.assign(desc->baselines, desc->baselines + desc->nbaselines);
+  h->jd.stations = h->st.data();
+  h->jd.freqs = h->fr.data();
+  h->jd.baselines = h->bl.data();
+  gx_status s = setup(h);
+  if (s != GX_OK) {
+    fprintf(stderr, "gx_open: %s\n", h->err.c_str());
+    free_all(h);
+    delete h;
+    return s;
+  }
+  *out = h;
+  return GX_OK;
+}
+
+gx_status gx_close(gx_handle *h)
+{
+  if (!h) return GX_ERR_ARG;
+  if (h->device >= 0) {
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+  }
+  free_all(h);
+  delete h;
+  return GX_OK;
+}
+
+const char *gx_last_error(const gx_handle *h) { return h ? h->err.c_str() : "null handle"; }
+
+gx_status gx_get_layout(const gx_handle *h, gx_layout_info *info)
+{
+  if (!h || !info) return GX_ERR_ARG;
+  info->result_length = h->rl;
+  info->nfreqs = h->jd.nfreqs;
+  info->nbaselines = h->jd.nbaselines;
+  info->nstations = h->jd.nstations;
+  info->blocks_per_send = h->J.blocks_per_send;
+  info->xmac_stride = h->xmac_stride;
+  info->array_stride = h->J.stride;
+  info->fftchannels = h->J.fftlen;
+  info->nchan = h->J.nchan;
+  return GX_OK;
+}
+
+gx_status gx_get_offsets(const gx_handle *h, int *blofs, int *bwofs, int *acofs, int *acwofs)
+{
+  if (!h) return GX_ERR_ARG;
+  if (blofs) memcpy(blofs, h->blofs.data(), sizeof(int) * h->blofs.size());
+  if (bwofs) memcpy(bwofs, h->bwofs.data(), sizeof(int) * h->bwofs.size());
+  if (acofs) memcpy(acofs, h->acofs.data(), sizeof(int) * h->acofs.size());
+  if (acwofs) memcpy(acwofs, h->acwofs.data(), sizeof(int) * h->acwofs.size());
+  return GX_OK;
+}
+
+static gx_status record(gx_handle *h, cudaStream_t st, int stage, bool start)
+{
+  cudaEvent_t e;
+  CKR(h, cudaEventCreate(&e));
+  CKR(h, cudaEventRecord(e, st));
+  h->evs.push_back(e);
+  if (start) h->ev_stage.push_back(stage);
+  return GX_OK;
+}
+
+// Runs one subint whose data buffers are already device pointers.
+static gx_status run_device(gx_handle *h, const gx_subint_desc *sub, const uint8_t *const *devdata,
+                            float2 *dev_results, cudaStream_t st)
+{
+  const gx_job_desc &d = h->jd;
+  const DevJob &J = h->J;
+  for (auto e : h->evs) cudaEventDestroy(e);
+  h->evs.clear();
+  h->ev_stage.clear();
+  h->launches = 0;
+  if (sub->controllen < 3 + J.flaglen) return h->fail(GX_ERR_ARG, "control buffer shorter than 3 + flag words");
+  // small per-subint tables
+  std::vector<int32_t> ctrl((size_t)h->ctrlstride * d.nstations, 0);
+  std::vector<int64_t> lens(d.nstations);
+  std::vector<double> interp(3 * d.nstations);
+  for (int s = 0; s < d.nstations; s++) {
+    if (!sub->control[s]) return h->fail(GX_ERR_ARG, "missing control buffer");
+    memcpy(&ctrl[(size_t)s * h->ctrlstride], sub->control[s], sizeof(int32_t) * h->ctrlstride);
+    lens[s] = sub->datalen[s];
+  }
+  if (sub->interp) {
+    memcpy(interp.data(), sub->interp, sizeof(double) * 3 * d.nstations);
+  } else {
+    if (!h->model) return h->fail(GX_ERR_ARG, "no interpolators given and the handle has no delay model");
+    for (int s = 0; s < d.nstations; s++) {
+      gx_status r = h->model->interpolator(s, sub->scan, sub->sec, sub->ns, &interp[3 * s]);
+      if (r != GX_OK) return h->fail(r, "no delay model for this subint");
+    }
+  }
+  CKR(h, cudaMemcpyAsync(h->d_ctrl, ctrl.data(), sizeof(int32_t) * ctrl.size(), cudaMemcpyHostToDevice, st));
+  CKR(h, cudaMemcpyAsync(h->d_datalen, lens.data(), sizeof(int64_t) * lens.size(), cudaMemcpyHostToDevice, st));
+  CKR(h, cudaMemcpyAsync(h->d_interp, interp.data(), sizeof(double) * interp.size(), cudaMemcpyHostToDevice, st));
+  CKR(h, cudaMemcpyAsync(h->d_dataptrs, devdata, sizeof(uint8_t *) * d.nstations, cudaMemcpyHostToDevice, st));
+  SubintArrays S{};
+  S.sec = sub->sec;
+  S.ns = sub->ns;
+  S.scan_start_sec = sub->scan_start_sec;
+  S.data = h->d_dataptrs;
+  S.datalen = h->d_datalen;
+  S.control = h->d_ctrl;
+  S.controlstride = h->ctrlstride;
+  S.interp = h->d_interp;
+  h->last = S;
+  h->have_last = true;
+
+  const int nbl = d.nbaselines;
+  CKR(h, cudaMemsetAsync(h->d_acc, 0, sizeof(float2) * h->acc_slice * h->ks, st));
+  CKR(h, cudaMemsetAsync(h->d_wacc, 0, sizeof(float) * (d.nstations + nbl), st));
+  for (int b0 = 0; b0 < J.blocks_per_send; b0 += h->chunk) {
+    const int nb = std::min(h->chunk, J.blocks_per_send - b0);
+    gx_status r;
+    if ((r = record(h, st, 0, true)) != GX_OK) return r;
+    CKR(h, fstep_launch(J, h->d_st, h->maxnrf, S, b0, nb, h->nslots, h->d_spec, h->d_w, st));
+    if ((r = record(h, st, 0, false)) != GX_OK) return r;
+    if ((r = record(h, st, 1, true)) != GX_OK) return r;
+    CKR(h, xmac_fp32_launch(h->d_spec, nb, J.ninputs, J.nchan, d.nfreqs, h->ks, h->d_acc, st));
+    CKR(h, weights_launch(h->d_w, nb, d.nstations, h->d_pairs, nbl, h->d_wacc, st));
+    if ((r = record(h, st, 1, false)) != GX_OK) return r;
+    h->launches += 3;
+  }
+  gx_status r;
+  if ((r = record(h, st, 2, true)) != GX_OK) return r;
+  CKR(h, cudaMemsetAsync(dev_results, 0, sizeof(float2) * h->rl, st));
+  CKR(h, finalise_launch(h->d_prods, (int)h->prods.size(), h->d_acc, h->ks, h->acc_slice, J.nchan, h->d_went,
+                         (int)h->wents.size(), h->d_wacc, dev_results, st));
+  h->launches += (h->prods.empty() ? 0 : 1) + (h->wents.empty() ? 0 : 1);
+  if ((r = record(h, st, 2, false)) != GX_OK) return r;
+  return GX_OK;
+}
+
+gx_status gx_subint_device(gx_handle *h, const gx_subint_desc *sub, float *dev_results, void *stream)
+{
+  if (!h || !sub || !dev_results || !sub->data || !sub->datalen || !sub->control) return GX_ERR_ARG;
+  if (h->device < 0) return h->fail(GX_ERR_STATE, "host-only handle (opened with device -1)");
+  CKR(h, cudaSetDevice(h->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+  return run_device(h, sub, sub->data, reinterpret_cast<float2 *>(dev_results), st);
+}
+
+gx_status gx_subint(gx_handle *h, const gx_subint_desc *sub, float *results)
+{
+  if (!h || !sub || !results || !sub->data || !sub->datalen || !sub->control) return GX_ERR_ARG;
+  if (h->device < 0) return h->fail(GX_ERR_STATE, "host-only handle (opened with device -1)");
+  CKR(h, cudaSetDevice(h->device));
+  const gx_job_desc &d = h->jd;
+  std::vector<const uint8_t *> dptr(d.nstations);
+  for (int s = 0; s < d.nstations; s++) {
+    if (sub->datalen[s] < 0) return h->fail(GX_ERR_ARG, "negative data length");
+    if (sub->datalen[s] > h->data_cap[s]) {
+      if (h->d_data[s]) CKR(h, cudaFree(h->d_data[s]));
+      h->d_data[s] = nullptr;
+      CKR(h, cudaMalloc(&h->d_data[s], sub->datalen[s] + 64));
+      h->data_cap[s] = sub->datalen[s];
+    }
+    if (sub->datalen[s] > 0)
+      CKR(h, cudaMemcpyAsync(h->d_data[s], sub->data[s], sub->datalen[s], cudaMemcpyHostToDevice, h->stream));
+    dptr[s] = h->d_data[s];
+  }
+  gx_status r = run_device(h, sub, dptr.data(), h->d_results, h->stream);
+  if (r != GX_OK) return r;
+  CKR(h, cudaMemcpyAsync(results, h->d_results, sizeof(float2) * h->rl, cudaMemcpyDeviceToHost, h->stream));
+  CKR(h, cudaStreamSynchronize(h->stream));
+  return GX_OK;
+}
+
+gx_status gx_synchronize(gx_handle *h)
+{
+  if (!h) return GX_ERR_ARG;
+  CKR(h, cudaStreamSynchronize(h->stream));
+  return GX_OK;
+}
+
+gx_status gx_stage_times(gx_handle *h, float ms[3])
+{
+  if (!h || !ms) return GX_ERR_ARG;
+  ms[0] = ms[1] = ms[2] = 0.f;
+  for (size_t i = 0; i + 1 < h->evs.size(); i += 2) {
+    CKR(h, cudaEventSynchronize(h->evs[i + 1]));
+    float t = 0;
+    CKR(h, cudaEventElapsedTime(&t, h->evs[i], h->evs[i + 1]));
+    int stg = h->ev_stage[i / 2];
+    if (stg >= 0 && stg < 3) ms[stg] += t;
+  }
+  return GX_OK;
+}
+
+gx_status gx_launch_count(const gx_handle *h, int *count)
+{
+  if (!h || !count) return GX_ERR_ARG;
+  *count = h->launches;
+  return GX_OK;
+}
+
+gx_status gx_spectra(gx_handle *h, int station, int block, float *out, float *weight)
+{
+  if (!h || !out || !weight) return GX_ERR_ARG;
+  if (h->device < 0 || !h->have_last) return h->fail(GX_ERR_STATE, "no subint has been processed yet");
+  const DevJob &J = h->J;
+  if (station < 0 || station >= J.nstations || block < 0 || block >= J.blocks_per_send)
+    return h->fail(GX_ERR_ARG, "station or block out of range");
+  CKR(h, cudaSetDevice(h->device));
+  CKR(h, fstep_launch(J, h->d_st, h->maxnrf, h->last, block, 1, h->nslots, h->d_spec1, h->d_w1, h->stream));
+  const gx_station_desc &x = h->jd.stations[station];
+  for (int b = 0; b < x.nbands; b++) {
+    int f = x.recfreq[x.band_localfreq[b]];
+    const float2 *src = h->d_spec1 + ((size_t)f * J.ninputs + h->band_input[station][b]) * J.nchan;
+    CKR(h, cudaMemcpyAsync(out + 2 * (size_t)b * J.nchan, src, sizeof(float2) * J.nchan, cudaMemcpyDeviceToHost,
+                           h->stream));
+  }
+  CKR(h, cudaMemcpyAsync(weight, h->d_w1 + station, sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  CKR(h, cudaStreamSynchronize(h->stream));
+  return GX_OK;
+}
+
+gx_status gx_interpolator(gx_handle *h, int station, int scan, int sec, int ns, double out[3])
+{
+  if (!h || !out) return GX_ERR_ARG;
+  if (!h->model) return h->fail(GX_ERR_STATE, "handle has no delay model (open it with gx_open_input)");
+  return h->model->interpolator(station, scan, sec, ns, out);
+}
+
+gx_status gx_scan_start_sec(gx_handle *h, int scan, double *out)
+{
+  if (!h || !out) return GX_ERR_ARG;
+  if (!h->model) return h->fail(GX_ERR_STATE, "handle has no delay model");
+  *out = h->model->scan_start_sec(scan);
+  return GX_OK;
+}
+
+gx_status gx_open_input(const char *inputfile, int device, int xstep, gx_handle **out)
+{
+  if (!inputfile || !out) return GX_ERR_ARG;
+  *out = nullptr;
+  std::string err;
+  std::unique_ptr<InputJob> job(read_input_job(inputfile, err));
+  if (!job) {
+    fprintf(stderr, "gx_open_input: %s\n", err.c_str());
+    return GX_ERR_IO;
+  }
+  job->desc.xstep = xstep;
+  gx_handle *h = nullptr;
+  gx_status s = gx_open(&job->desc, device, &h);
+  if (s != GX_OK) return s;
+  h->model = std::move(job->model);
+  *out = h;
+  return GX_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,65 @@
+// Device-side job and subint descriptions shared by the gxcorr kernels and
+// the host driver.  All stations of one job share the sampling setup (bits,
+// sampling type, frame size, bands, channels); the per-station parts are the
+// recorded-frequency tables and the data buffers.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "../../include/gxcorr.h"
+
+namespace gx {
+
+constexpr int kMaxFramesPerBlock = 256;  // frames one FFT block may span
+constexpr int kFThreads = 256;           // threads per F-step CTA
+constexpr int kMaxFreqsPerStation = GX_MAX_LOCAL_FREQS;
+
+// Per-station constants (device copy lives in global memory).
+struct DevStation {
+  int nrecfreqs;
+  int fractional_lo;      // Mode::fractionalLoFreq (mode.cpp:86-102)
+  int deltapol;           // any CLK OFFSET delta != 0 (mode.cpp:335-343)
+  int pad_;
+  double lofreq[kMaxFreqsPerStation];      // LO used for fringe rotation (mode.cpp:872-880)
+  int lsb[kMaxFreqsPerStation];
+  int freq_index[kMaxFreqsPerStation];     // job freq table index
+  double clk[kMaxFreqsPerStation];
+  double clkdelta[kMaxFreqsPerStation];
+  double looff[kMaxFreqsPerStation];       // Hz
+  int band_localfreq[GX_MAX_BANDS];
+  int band_input[GX_MAX_BANDS];            // row of this band in its freq's spectra block
+  int band_polb[GX_MAX_BANDS];             // uses fracsamprotatorB (mode.cpp:1257-1261)
+};
+
+// Job-wide constants (passed by value to kernels).
+struct DevJob {
+  int nstations;
+  int nbands;             // recorded bands per station
+  int nbits, cplx;
+  int framebytes, framesamples, bytespersample;
+  int nchan;              // N: channels per band
+  int fftlen;             // F: fftchannels (2N real, N complex)
+  int stride;             // S: arraystridelength
+  int nfr;                // F / S
+  int half;               // numfracstrides / 2
+  int unpacksamples;
+  int ninputs;            // NI: padded spectra rows per freq
+  int nfreqs;
+  int blocks_per_send;
+  int flaglen;
+  double sampletime;      // us
+  double bw;              // MHz
+  const float2 *twiddle;  // exp(-2 pi i m / F), m in [0, F)
+};
+
+// One subint: device pointers to its buffers.
+struct SubintArrays {
+  int sec, ns;
+  double scan_start_sec;
+  const uint8_t *const *data;    // [nstations] device pointers
+  const int64_t *datalen;        // [nstations]
+  const int32_t *control;        // [nstations][controlstride]
+  int controlstride;
+  const double *interp;          // [nstations][3]
+};
+
+}  // namespace gx

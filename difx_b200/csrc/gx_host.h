@@ -1,0 +1,61 @@
+// Host-side setup readers: .input / .calc / .im and the delay model.
+#pragma once
+#include <memory>
+#include <string>
+#include <vector>
+#include "../../include/gxcorr.h"
+
+namespace gx {
+
+// Per-scan delay polynomials (Model's scantable, mpifxcorr/src/model.h).
+struct ModelScan {
+  int offsetseconds = 0;      // SCAN n START (S)
+  int durationseconds = 0;
+  int numphasecentres = 1;
+  int nsamples = 0;
+  int polystartmjd = 0, polystartseconds = 0;
+  // delay[sample][source][station][order+1], us; source 0 = pointing centre
+  std::vector<double> delay;
+};
+
+// Model::calculateDelayInterpolator and Mode::setOffsets (model.cpp:219-289,
+// mode.cpp:1502-1532), with the clock terms folded in as Model::addClockTerms
+// does (model.cpp:291-352).
+class HostModel {
+ public:
+  int polyorder = 0, modelincsecs = 0;
+  int modelmjd = 0, modelstartseconds = 0;
+  int jobmjd = 0, jobseconds = 0;
+  int nstations = 0;
+  std::vector<ModelScan> scans;
+  std::vector<int> station_of_datastream;   // model antenna index per datastream
+  std::vector<int> intclockseconds;         // per datastream
+  double timespan_s = 0;                    // blockspersend * fftchannels * sampletime / 1e6
+  int blocks_per_send = 0;
+
+  double delay_at(const ModelScan &sc, int sample, int src, int ant, int l) const
+  {
+    return sc.delay[(((size_t)sample * (sc.numphasecentres + 1) + src) * nstations + ant) * (polyorder + 1) + l];
+  }
+  gx_status interpolator(int datastream, int scan, int sec, int ns, double out[3]) const;
+  double scan_start_sec(int scan) const;
+};
+
+struct InputJob {
+  gx_job_desc desc{};
+  std::vector<gx_station_desc> stations;
+  std::vector<gx_freq_desc> freqs;
+  std::vector<gx_baseline_desc> baselines;
+  std::unique_ptr<HostModel> model;
+  int start_mjd = 0, start_seconds = 0, execute_seconds = 0;
+  double int_time = 0;
+  std::vector<std::string> datafiles;   // first file of each datastream
+};
+
+InputJob *read_input_job(const char *inputfile, std::string &err);
+
+}  // namespace gx
+
+using gx::HostModel;
+using gx::InputJob;
+using gx::read_input_job;

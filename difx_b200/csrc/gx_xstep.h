@@ -1,0 +1,43 @@
+// Kernel entry points and tables shared between the gxcorr kernels and the host driver.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "gx_dev.h"
+
+namespace gx {
+
+// One visibility row of the Core result array: result_offset + c <- acc[acc_index + c] (conj if set).
+struct ProdEntry {
+  long long result_offset;  // complex-float index into the result array
+  long long acc_index;      // complex-float index into the ks = 0 accumulator slice
+  int conj;
+  int pad_;
+};
+
+// One float slot of the result array that holds a weight.
+struct WeightEntry {
+  long long float_index;    // float index into the result array
+  int source;               // index into the weight accumulators (-1: zero)
+  int pad_;
+};
+
+struct XmacShape {
+  int T, ST, CT;
+  int nsuper, npairs;
+};
+
+XmacShape xmac_shape(int NI);
+
+cudaError_t fstep_set_lut(const float *lut, cudaStream_t st);
+size_t fstep_smem_bytes(const DevJob &J, int nrf, int nslots);
+cudaError_t fstep_launch(const DevJob &J, const DevStation *stations, int maxnrf, const SubintArrays &S,
+                         int blk0, int nblk, int nslots, float2 *spec, float *weights, cudaStream_t st);
+cudaError_t xmac_fp32_launch(const float2 *spec, int nblk, int NI, int N, int nfreqs, int ks, float2 *acc,
+                             cudaStream_t st);
+cudaError_t weights_launch(const float *w, int nblk, int nstations, const int2 *pairs, int npairs, float *wacc,
+                           cudaStream_t st);
+cudaError_t finalise_launch(const ProdEntry *prods, int nprods, const float2 *acc, int ks, size_t ks_stride, int N,
+                            const WeightEntry *we, int nw, const float *wacc, float2 *results, cudaStream_t st);
+
+}  // namespace gx

@@ -1,0 +1,151 @@
+"""Python binding of the gxcorr C ABI (include/gxcorr.h) via ctypes.
+
+``Correlator`` mirrors the reference's Core-slot contract: one call per
+subint with the raw datastream buffers and control words, returning the Core
+result array (complex64, the layout of ``procslots[].results``,
+mpifxcorr/src/configuration.cpp:2348-2630).
+
+The CUDA library ``difx_b200/libgxcorr.so`` must be built (``python -m
+difx_b200.build``); there is no CPU fallback -- loading fails loudly if it is
+missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import capi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(_HERE, "libgxcorr.so")
+_lib = None
+
+
+class GxError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{capi.STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def lib():
+    """The loaded libgxcorr.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBPATH):
+            raise RuntimeError(f"{LIBPATH} is missing: build it with `python -m difx_b200.build`")
+        L = C.CDLL(LIBPATH)
+        L.gx_last_error.restype = C.c_char_p
+        L.gx_status_string.restype = C.c_char_p
+        for name in ("gx_open", "gx_open_input", "gx_close", "gx_get_layout", "gx_get_offsets", "gx_interpolator",
+                     "gx_scan_start_sec", "gx_subint", "gx_subint_device", "gx_synchronize", "gx_spectra",
+                     "gx_stage_times", "gx_launch_count"):
+            getattr(L, name).restype = C.c_int
+        _lib = L
+    return _lib
+
+
+EXPORTED_SYMBOLS = ("gx_open", "gx_open_input", "gx_close", "gx_last_error", "gx_status_string",
+                    "gx_get_layout", "gx_get_offsets", "gx_interpolator", "gx_scan_start_sec", "gx_subint",
+                    "gx_subint_device", "gx_synchronize", "gx_spectra", "gx_stage_times", "gx_launch_count")
+
+
+class Correlator:
+    """One correlation configuration on one GPU."""
+
+    def __init__(self, handle: C.c_void_p, keepalive=None):
+        self.h = handle
+        self._keep = keepalive
+        info = capi.gx_layout_info()
+        self._check(lib().gx_get_layout(self.h, C.byref(info)))
+        self.info = info
+        self.result_length = int(info.result_length)
+
+    # ------------------------------------------------------------- opening
+    @classmethod
+    def from_desc(cls, jd: capi.JobDesc, device: int = 0) -> "Correlator":
+        h = C.c_void_p()
+        st = lib().gx_open(jd.ptr(), device, C.byref(h))
+        if st != 0:
+            raise GxError(st, "gx_open failed (see stderr)")
+        return cls(h, jd)
+
+    @classmethod
+    def from_input(cls, inputfile: str, device: int = 0, xstep: int = capi.GX_XSTEP_FP32) -> "Correlator":
+        h = C.c_void_p()
+        st = lib().gx_open_input(inputfile.encode(), device, xstep, C.byref(h))
+        if st != 0:
+            raise GxError(st, f"gx_open_input({inputfile}) failed (see stderr)")
+        return cls(h)
+
+    def close(self):
+        if self.h:
+            lib().gx_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int):
+        if st != 0:
+            msg = lib().gx_last_error(self.h).decode() if self.h else ""
+            raise GxError(st, msg)
+
+    # ------------------------------------------------------------- queries
+    def offsets(self):
+        i = self.info
+        nfb = max(1, i.nfreqs * i.nbaselines)
+        bl = np.zeros(nfb, np.int32)
+        bw = np.zeros(nfb, np.int32)
+        ac = np.zeros(i.nstations, np.int32)
+        acw = np.zeros(i.nstations, np.int32)
+        self._check(lib().gx_get_offsets(self.h, bl.ctypes.data_as(C.c_void_p), bw.ctypes.data_as(C.c_void_p),
+                                         ac.ctypes.data_as(C.c_void_p), acw.ctypes.data_as(C.c_void_p)))
+        return self.result_length, bl, bw, ac, acw
+
+    def interpolator(self, station: int, scan: int, sec: int, ns: int) -> np.ndarray:
+        out = np.zeros(3, np.float64)
+        self._check(lib().gx_interpolator(self.h, station, scan, sec, ns, out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def scan_start_sec(self, scan: int) -> float:
+        v = C.c_double(0)
+        self._check(lib().gx_scan_start_sec(self.h, scan, C.byref(v)))
+        return v.value
+
+    def stage_times(self) -> np.ndarray:
+        ms = (C.c_float * 3)()
+        self._check(lib().gx_stage_times(self.h, ms))
+        return np.array(list(ms))
+
+    def launch_count(self) -> int:
+        n = C.c_int(0)
+        self._check(lib().gx_launch_count(self.h, C.byref(n)))
+        return n.value
+
+    # ------------------------------------------------------------- work
+    def subint(self, sd: capi.SubintDesc, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Host buffers in, Core result array (complex64) out."""
+        if out is None:
+            out = np.zeros(self.result_length, np.complex64)
+        self._check(lib().gx_subint(self.h, sd.ptr(), out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def subint_device(self, sd: capi.SubintDesc, dev_results_ptr: int, stream_ptr: int = 0):
+        """Device buffers in (sd holds device pointers), device results out; asynchronous."""
+        self._check(lib().gx_subint_device(self.h, sd.ptr(), C.c_void_p(dev_results_ptr),
+                                           C.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def synchronize(self):
+        self._check(lib().gx_synchronize(self.h))
+
+    def spectra(self, station: int, block: int, nbands: int):
+        out = np.zeros(nbands * self.info.nchan, np.complex64)
+        w = C.c_float(0)
+        self._check(lib().gx_spectra(self.h, station, block, out.ctypes.data_as(C.c_void_p), C.byref(w)))
+        return out.reshape(nbands, self.info.nchan), w.value

@@ -182,7 +182,7 @@ def make_station_stream(spec: JobSpec, station: int, first_frame: int, nframes: 
         out[f, VDIF_HEADER_BYTES:] = payload[f]
         if fillflags[f]:
             out[f, VDIF_HEADER_BYTES:VDIF_HEADER_BYTES + 8] = np.frombuffer(
-                np.uint64(0x4433221144332211).tobytes(), dtype=np.uint8)
+                np.uint64(0x1122334411223344).tobytes(), dtype=np.uint8)
     return StationStream(station, first_frame, nframes, out.reshape(-1), invalid | fillflags)
 
 

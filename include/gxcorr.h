@@ -149,6 +149,8 @@ typedef struct gx_layout_info {
   int nchan;
 } gx_layout_info;
 
+/* device < 0 opens a host-only handle: layout, offsets and delay-model
+   queries work, no CUDA call is made, and gx_subint* return GX_ERR_STATE. */
 gx_status gx_open(const gx_job_desc *desc, int device, gx_handle **out);
 gx_status gx_open_input(const char *inputfile, int device, int xstep, gx_handle **out);
 gx_status gx_close(gx_handle *h);

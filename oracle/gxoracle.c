@@ -14,7 +14,7 @@
 #define FLAGS_PER_INT 30                          /* mpifxcorr.h:29 */
 #define INVALID_SUBINT (-99999999)                /* mode.h:222 */
 static const float MODE_TINY = 0.000000001f;      /* mode.cpp:26 */
-#define FILL_WORD64 0x4433221144332211ULL         /* blanker_mark5.c:33 (little endian) */
+#define FILL_WORD64 0x1122334411223344ULL         /* blanker_mark5.c:35 (little-endian hosts) */
 
 typedef struct { float re, im; } cf;
 typedef struct { double re, im; } cd;

@@ -62,6 +62,9 @@ void *ref_open(const char *inputfile)
     fprintf(stderr, "ref_open: configuration inconsistent\n");
     return 0;
   }
+  // mpifxcorr's main() sets this flag (default off) right after constructing
+  // the Configuration (mpifxcorr.cpp:262, 370); the constructor leaves it unset.
+  config->setVGOSComplexVDIFHack(false);
   RefJob *j = new RefJob();
   j->config = config;
   j->nds = config->getNumDataStreams();

@@ -1,0 +1,141 @@
+"""The oracle pinned against the reference correlator itself (CPU).
+
+The reference's own hot path (Configuration, Mk5Mode/Mode, Core::processdata,
+mark5access) is compiled from its sources into oracle/_ref/libdifxref.so; the
+C restatement in oracle/gxoracle.c must reproduce it bit for bit when the
+reference runs one process thread (a deterministic accumulation order)."""
+import numpy as np
+import pytest
+
+from oracle import pyoracle
+from tests import jobs
+
+needs_ref = pytest.mark.skipif(not pyoracle.reference_available(), reason="reference harness not built")
+
+
+def _params(orc, spec, precision=pyoracle.FP32_REF):
+    return orc.params(precision=precision, nthreads=1, num_buffered_ffts=spec.num_buffered_ffts,
+                      xc_avg_ns=spec.uvshift_interval_ns, ac_avg_ns=spec.ac_avg_interval_ns)
+
+
+CASES = {
+    "c1": lambda: (jobs.spec_c1(), dict()),
+    "c1_invalid_fill": lambda: (jobs.spec_c1(name="c1bad", seed=21), dict(invalid_frac=0.05, fill_frac=0.03)),
+    "lsb": lambda: (jobs.spec_lsb(), dict()),
+    "cplx8": lambda: (jobs.spec_cplx8(), dict()),
+    "cplx8_invalid": lambda: (jobs.spec_cplx8(name="cx8bad", seed=23), dict(invalid_frac=0.08)),
+    "c1_flush": lambda: (jobs.spec_c1(name="c1fl", uvshift_interval_ns=1_000_000, ac_avg_interval_ns=2_000_000,
+                                      num_buffered_ffts=7), dict()),
+}
+
+
+@needs_ref
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_oracle_bitexact_vs_reference(case, oracle_lib):
+    spec, kw = CASES[case]()
+    prep = jobs.prepare(spec, [100_000_000], **kw)
+    ref = jobs.reference_for(prep.paths["input"])
+    assert ref.nthreads == 1
+    r = ref.process(prep.subs[0])
+    o = oracle_lib.subint(prep.jd, prep.sds[0], _params(oracle_lib, spec))
+    assert r.shape == o.shape
+    np.testing.assert_array_equal(o.astype(np.complex64), r)
+
+
+@needs_ref
+@pytest.mark.parametrize("case", ["c1", "lsb", "cplx8", "c1_invalid_fill"])
+def test_layout_matches_reference(case, oracle_lib):
+    spec, _ = CASES[case]()
+    prep = jobs.prepare(spec, [100_000_000])
+    ref = jobs.reference_for(prep.paths["input"])
+    nbl = spec.nstations * (spec.nstations - 1) // 2
+    rl, *lr = ref.layout(len(spec.subbands), nbl, spec.nstations)
+    ol, *lo = oracle_lib.layout(prep.jd)
+    assert rl == ol
+    for a, b in zip(lr, lo):
+        np.testing.assert_array_equal(a, b)
+
+
+@needs_ref
+@pytest.mark.parametrize("case", ["c1", "lsb", "cplx8"])
+def test_host_reader_matches_reference(case):
+    """libgxcorr's own .input/.calc/.im reader and delay model (host-only
+    handle) against Configuration and Model::calculateDelayInterpolator."""
+    from difx_b200.gxcorr import Correlator
+    spec, _ = CASES[case]()
+    prep = jobs.prepare(spec, [100_000_000, 1_300_000_000])
+    ref = jobs.reference_for(prep.paths["input"])
+    c = Correlator.from_input(prep.paths["input"], device=-1)
+    nbl = spec.nstations * (spec.nstations - 1) // 2
+    rl, *lr = ref.layout(len(spec.subbands), nbl, spec.nstations)
+    gl, *lg = c.offsets()
+    assert rl == gl
+    for a, b in zip(lr, lg):
+        np.testing.assert_array_equal(a, b)
+    assert c.info.blocks_per_send == ref.blocks_per_send
+    for si in prep.subs:
+        for s in range(spec.nstations):
+            np.testing.assert_array_equal(c.interpolator(s, 0, si.sec, si.ns), ref.interpolator(s, 0, si.sec, si.ns))
+    c.close()
+
+
+@needs_ref
+@pytest.mark.parametrize("case", ["c1_invalid_fill", "cplx8_invalid"])
+def test_unpack_bitexact_vs_reference(case, oracle_lib):
+    """Mk5Mode::unpack (samples and weight) at many offsets across invalid and fill-pattern frames."""
+    spec, kw = CASES[case]()
+    prep = jobs.prepare(spec, [100_000_000], **kw)
+    ref = jobs.reference_for(prep.paths["input"])
+    data = prep.subs[0].data[1]
+    per = spec.fftchannels * (2 if spec.is_complex else 1)
+    nframes = len(data) // spec.framebytes
+    rng = np.random.default_rng(0)
+    offs = list(rng.integers(0, (nframes - 2) * spec.frame_samples, 40))
+    offs += [f * spec.frame_samples - 3 for f in range(1, min(nframes - 2, 12))]
+    for off in offs:
+        out, w, us, n = ref.unpack(1, data, int(off), spec.nbands, per)
+        o, good = oracle_lib.unpack(prep.jd, 1, data, int(off), spec.fftchannels)
+        assert us == off
+        np.testing.assert_array_equal(o.reshape(-1), out[:spec.nbands * per].reshape(spec.nbands, per).reshape(-1))
+        assert np.float32(good) / np.float32(spec.fftchannels) == np.float32(w)
+
+
+@needs_ref
+def test_mode_block_vs_oracle(oracle_lib):
+    """Mode::process spectra of single blocks (after fractional-sample correction)."""
+    spec, kw = CASES["c1_invalid_fill"]()
+    prep = jobs.prepare(spec, [100_000_000], **kw)
+    ref = jobs.reference_for(prep.paths["input"])
+    p = _params(oracle_lib, spec)
+    for st in range(spec.nstations):
+        for blk in (0, 1, 17, 500, spec.blocks_per_send - 1):
+            rs, rw = ref.mode_block(prep.subs[0], st, blk, spec.nbands, spec.nchan)
+            os_, ow = oracle_lib.station_block(prep.jd, prep.sds[0], st, blk, p)
+            assert np.float32(ow) == np.float32(rw)
+            np.testing.assert_array_equal(os_.astype(np.complex64), rs)
+
+
+def test_fp64_oracle_agrees_with_fp32(oracle_lib):
+    """The FP64 precision oracle and the FP32 reference-order restatement agree
+    to FP32 rounding (per-record mean |diff| / mean |value| < 1e-5)."""
+    spec, _ = CASES["c1"]()
+    prep = jobs.prepare(spec, [100_000_000])
+    o32 = oracle_lib.subint(prep.jd, prep.sds[0], _params(oracle_lib, spec))
+    o64 = oracle_lib.subint(prep.jd, prep.sds[0], _params(oracle_lib, spec, pyoracle.FP64))
+    rl, bl, bw, ac, acw = oracle_lib.layout(prep.jd)
+    offs = jobs.record_offsets(prep.jd, bl, ac, spec)
+    assert jobs.record_metric(o32, o64, offs, spec.nchan) < 1e-5
+
+
+def test_correlation_is_detected(oracle_lib):
+    """The synthetic signal model gives a coherent correlation (flat phase across
+    channels) on every parallel-hand baseline after delay/fringe correction."""
+    spec, _ = CASES["c1"]()
+    prep = jobs.prepare(spec, [100_000_000], rho=0.2)
+    o = oracle_lib.subint(prep.jd, prep.sds[0], _params(oracle_lib, spec, pyoracle.FP64))
+    rl, bl, bw, ac, acw = oracle_lib.layout(prep.jd)
+    nbl = prep.jd.desc.nbaselines
+    for j in range(nbl):
+        v = o[bl[j]: bl[j] + spec.nchan]   # freq 0, RR
+        coh = abs(v.mean()) / np.abs(v).mean()
+        assert coh > 0.8, (j, coh)
