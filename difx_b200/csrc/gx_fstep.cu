@@ -403,11 +403,13 @@ cudaError_t fstep_launch(const DevJob &J, const DevStation *stations, int maxnrf
   const int bpc = 4;
   dim3 grid((nblk + bpc - 1) / bpc, J.nstations);
   size_t sm = fstep_smem_bytes(J, maxnrf, nslots);
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(fstep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+  // opt in to the dynamic shared memory this launch needs (the kernel's
+  // static shared memory counts against the same 227 KB per block)
+  static size_t attr_bytes = 48 * 1024;
+  if (sm > attr_bytes) {
+    cudaError_t e = cudaFuncSetAttribute(fstep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
-    attr_set = true;
+    attr_bytes = sm;
   }
   fstep_kernel<<<grid, kFThreads, sm, st>>>(J, stations, S, blk0, nblk, bpc, nslots, spec, weights);
   return cudaGetLastError();

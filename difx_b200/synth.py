@@ -228,7 +228,7 @@ def valid_flags(spec: JobSpec, bad_blocks: Optional[np.ndarray] = None) -> np.nd
     w = np.zeros(nwords, dtype=np.int64)
     ok = np.ones(nb, dtype=bool)
     if bad_blocks is not None:
-        ok[bad_blocks] = False
+        ok[np.asarray(bad_blocks, dtype=np.int64)] = False
     for b in range(nb):
         if ok[b]:
             w[b // 30] |= (1 << (b % 30))
@@ -265,3 +265,27 @@ def streams_for_job(spec: JobSpec, sub_starts_ns: List[int], rho: float = 0.05, 
         out.append(make_station_stream(spec, s, lo, hi - lo, rho=rho, seed=seed,
                                        invalid_frac=invalid_frac, fill_frac=fill_frac))
     return out
+
+
+def make_station_stream_tiled(spec: JobSpec, station: int, first_frame: int, nframes: int, tile_frames: int,
+                              rho: float = 0.05, seed: int = 1, invalid_frac: float = 0.0) -> StationStream:
+    """Like make_station_stream, but only the first `tile_frames` frames are
+    synthesised from the signal model; their payloads repeat over the rest of
+    the window.  Headers (seconds, frame number, invalid bit per absolute
+    frame) are written for every frame.  Used for benchmark-size inputs,
+    where the throughput does not depend on the sample values."""
+    tile_frames = max(1, min(tile_frames, nframes))
+    base = make_station_stream(spec, station, first_frame, tile_frames, rho=rho, seed=seed, invalid_frac=0.0)
+    fb = spec.framebytes
+    tile = base.data.reshape(tile_frames, fb)
+    reps = (nframes + tile_frames - 1) // tile_frames
+    out = np.tile(tile, (reps, 1))[:nframes].copy()
+    fps = int(round(spec.frames_per_second))
+    af = first_frame + np.arange(nframes, dtype=np.int64)
+    rng = np.random.default_rng([seed, 13, station])
+    invalid = rng.random(first_frame + nframes)[first_frame:] < invalid_frac
+    hdr = out[:, :VDIF_HEADER_BYTES].view(np.uint32).reshape(nframes, 8)
+    sec = (spec.start_seconds + af // fps).astype(np.uint32)
+    hdr[:, 0] = (sec & np.uint32(0x3FFFFFFF)) | np.where(invalid, np.uint32(1 << 31), np.uint32(0))
+    hdr[:, 1] = (af % fps).astype(np.uint32) & np.uint32(0xFFFFFF)
+    return StationStream(station, first_frame, nframes, out.reshape(-1), invalid)

@@ -1,0 +1,154 @@
+"""CUDA path (libgxcorr through its C ABI) against the oracle and the reference.
+
+Tolerances: visibility and autocorrelation records within 1e-5 by the
+per-record metric of utilities/vis2screen/diffDiFX.py:146-151
+(mean |gpu - ref| / mean |ref|); weights within 1e-6 relative; per-block
+data weights bit-exact."""
+import numpy as np
+import pytest
+
+from oracle import pyoracle
+from tests import jobs
+
+pytestmark = pytest.mark.gpu
+
+REC_TOL = 1e-5
+W_TOL = 1e-6
+
+
+def _params(orc, spec, precision=pyoracle.FP32_REF):
+    return orc.params(precision=precision, nthreads=1, num_buffered_ffts=spec.num_buffered_ffts,
+                      xc_avg_ns=spec.uvshift_interval_ns, ac_avg_ns=spec.ac_avg_interval_ns)
+
+
+def _weight_slots(jd, bw, acw, spec):
+    """Float indices of every weight in the result array."""
+    d = jd.desc
+    idx = []
+    nbl = d.nbaselines
+    for f in range(d.nfreqs):
+        for j in range(nbl):
+            o = bw[f * nbl + j]
+            if o < 0:
+                continue
+            for p in range(d.baselines[j].npolprod[0]):
+                idx.append(2 * o + p)
+    nw = spec.nbands * (2 if spec.full_pol and len(spec.pols) > 1 else 1)
+    for s in range(d.nstations):
+        idx += [2 * acw[s] + k for k in range(nw)]
+    return np.array(idx)
+
+
+def _compare(gpu, ref, jd, spec, orc):
+    rl, bl, bw, ac, acw = orc.layout(jd)
+    offs = jobs.record_offsets(jd, bl, ac, spec)
+    m = jobs.record_metric(gpu, ref, offs, spec.nchan)
+    wi = _weight_slots(jd, bw, acw, spec)
+    gf = gpu.view(np.float32) if gpu.dtype == np.complex64 else gpu.astype(np.complex64).view(np.float32)
+    rf = ref.astype(np.complex64).view(np.float32)
+    wrel = np.max(np.abs(gf[wi] - rf[wi]) / np.maximum(np.abs(rf[wi]), 1e-30))
+    return m, wrel
+
+
+CASES = {
+    "c1": lambda: (jobs.spec_c1(), dict()),
+    "c1_invalid_fill": lambda: (jobs.spec_c1(name="c1bad", seed=21), dict(invalid_frac=0.05, fill_frac=0.03)),
+    "lsb": lambda: (jobs.spec_lsb(), dict()),
+    "cplx8": lambda: (jobs.spec_cplx8(), dict()),
+    "cplx8_invalid": lambda: (jobs.spec_cplx8(name="cx8bad", seed=23), dict(invalid_frac=0.08)),
+    "c2small": lambda: (jobs.spec_c2small(), dict(invalid_frac=0.01)),
+}
+
+
+@pytest.fixture(scope="module")
+def gx():
+    from difx_b200 import gxcorr
+    return gxcorr
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_gpu_matches_oracle(case, gx, oracle_lib):
+    spec, kw = CASES[case]()
+    prep = jobs.prepare(spec, [100_000_000], **kw)
+    c = gx.Correlator.from_desc(prep.jd)
+    g = c.subint(prep.sds[0])
+    o = oracle_lib.subint(prep.jd, prep.sds[0], _params(oracle_lib, spec))
+    m, wrel = _compare(g, o, prep.jd, spec, oracle_lib)
+    assert m < REC_TOL, m
+    assert wrel < W_TOL, wrel
+    c.close()
+
+
+@pytest.mark.skipif(not pyoracle.reference_available(), reason="reference harness not built")
+@pytest.mark.parametrize("case", ["c1", "cplx8_invalid"])
+def test_gpu_matches_reference(case, gx, oracle_lib):
+    spec, kw = CASES[case]()
+    prep = jobs.prepare(spec, [100_000_000], **kw)
+    c = gx.Correlator.from_desc(prep.jd)
+    g = c.subint(prep.sds[0])
+    r = jobs.reference_for(prep.paths["input"]).process(prep.subs[0])
+    m, wrel = _compare(g, r, prep.jd, spec, oracle_lib)
+    assert m < REC_TOL, m
+    assert wrel < W_TOL, wrel
+    c.close()
+
+
+@pytest.mark.parametrize("case", ["c1_invalid_fill", "cplx8_invalid", "lsb"])
+def test_gpu_block_spectra_and_weights(case, gx, oracle_lib):
+    """Station-stage output of single blocks (Mode::getFreqs after process())."""
+    spec, kw = CASES[case]()
+    prep = jobs.prepare(spec, [100_000_000], **kw)
+    c = gx.Correlator.from_desc(prep.jd)
+    c.subint(prep.sds[0])
+    p = _params(oracle_lib, spec)
+    for st in range(spec.nstations):
+        for blk in (0, 3, 101, spec.blocks_per_send // 2, spec.blocks_per_send - 1):
+            gs, gw = c.spectra(st, blk, spec.nbands)
+            os_, ow = oracle_lib.station_block(prep.jd, prep.sds[0], st, blk, p)
+            assert np.float32(gw) == np.float32(ow)          # data weight bit-exact
+            scale = np.sqrt(np.mean(np.abs(os_) ** 2)) if ow > 0 else 1.0
+            assert np.max(np.abs(gs - os_)) <= 1e-5 * max(scale, 1e-30) * np.sqrt(spec.fftchannels), (st, blk)
+    c.close()
+
+
+def test_gpu_bad_blocks_and_host_model(gx, oracle_lib):
+    """Per-block valid flags (mode.cpp:656-669) and the handle's own delay model
+    (gx_open_input, interpolators from its .im reader) on two subints."""
+    spec = jobs.spec_c1(name="c1flags", seed=31)
+    nb = spec.blocks_per_send
+    bad = [np.array([0, 5, 6, 7, nb - 1]), np.array([]), np.arange(100, 160), np.array([999])]
+    prep = jobs.prepare(spec, [100_000_000, 108_000_000], bad_blocks=bad)
+    c = gx.Correlator.from_input(prep.paths["input"])
+    c2 = gx.Correlator.from_desc(prep.jd)
+    from difx_b200 import capi
+    for i, si in enumerate(prep.subs):
+        own = capi.subint_desc_host(si, None)          # handle computes the interpolators
+        g_own = c.subint(own)
+        g_exp = c2.subint(prep.sds[i])
+        np.testing.assert_array_equal(g_own, g_exp)
+        o = oracle_lib.subint(prep.jd, prep.sds[i], _params(oracle_lib, spec))
+        m, wrel = _compare(g_own, o, prep.jd, spec, oracle_lib)
+        assert m < REC_TOL and wrel < W_TOL, (m, wrel)
+    c.close()
+    c2.close()
+
+
+def test_gpu_device_entry_point(gx, oracle_lib):
+    """gx_subint_device on device-resident buffers equals the host entry point."""
+    import torch
+    from difx_b200 import capi
+    spec = jobs.spec_c1(name="c1dev", seed=41)
+    prep = jobs.prepare(spec, [100_000_000])
+    c = gx.Correlator.from_desc(prep.jd)
+    g_host = c.subint(prep.sds[0])
+    si = prep.subs[0]
+    dev = [torch.from_numpy(d).cuda() for d in si.data]
+    torch.cuda.synchronize()
+    sd = capi.SubintDesc(si.scan, si.sec, si.ns, 0.0, [t.data_ptr() for t in dev], [len(d) for d in si.data],
+                         [x.ctypes.data for x in si.control], len(si.control[0]), prep.interps[0])
+    out = torch.zeros(2 * c.result_length, dtype=torch.float32, device="cuda")
+    c.subint_device(sd, out.data_ptr())
+    c.synchronize()
+    g_dev = out.cpu().numpy().view(np.complex64)
+    np.testing.assert_array_equal(g_dev, g_host)
+    c.close()
