@@ -418,6 +418,21 @@ static gx_status setup(gx_handle *h)
       return h->fail(GX_ERR_UNSUPPORTED, "F-step shared memory exceeds 227 KB");
   }
 
+  {
+    // decode tables (format_vdif.c:66-146): 2-bit {-HiMag,-1,1,HiMag}, 1-bit {-1,1},
+    // 4-bit (l-7.5)/2.95, 8-bit (b-128)/3.3 or (b-127.5)/3.3 with SYMMETRIC_8_BIT_VDIF
+    float *lut = J.lut;
+    memset(lut, 0, sizeof(J.lut));
+    const float himag = 3.3359f;
+    if (J.nbits == 1) { lut[0] = -1.0f; lut[1] = 1.0f; }
+    else if (J.nbits == 2) { lut[0] = -himag; lut[1] = -1.0f; lut[2] = 1.0f; lut[3] = himag; }
+    else if (J.nbits == 4) { for (int l = 0; l < 16; l++) lut[l] = (float)((l - 7.5) / (double)2.95f); }
+    else {
+      double off = getenv("SYMMETRIC_8_BIT_VDIF") ? 127.5 : 128.0;
+      for (int b = 0; b < 256; b++) lut[b] = (float)((b - off) / 3.3);
+    }
+  }
+
   // ---------------------------------------------------------- device state
   if (h->device < 0) return GX_OK;  // host-only handle: layout and model queries
   CKR(h, cudaSetDevice(h->device));
@@ -433,21 +448,6 @@ static gx_status setup(gx_handle *h)
     CKR(h, cudaMalloc(&h->d_tw, sizeof(float2) * J.fftlen));
     CKR(h, cudaMemcpy(h->d_tw, tw.data(), sizeof(float2) * J.fftlen, cudaMemcpyHostToDevice));
     J.twiddle = h->d_tw;
-  }
-  {
-    // decode tables (format_vdif.c:66-146): 2-bit {-HiMag,-1,1,HiMag}, 1-bit {-1,1},
-    // 4-bit (l-7.5)/2.95, 8-bit (b-128)/3.3 or (b-127.5)/3.3 with SYMMETRIC_8_BIT_VDIF
-    float lut[256];
-    memset(lut, 0, sizeof(lut));
-    const float himag = 3.3359f;
-    if (J.nbits == 1) { lut[0] = -1.0f; lut[1] = 1.0f; }
-    else if (J.nbits == 2) { lut[0] = -himag; lut[1] = -1.0f; lut[2] = 1.0f; lut[3] = himag; }
-    else if (J.nbits == 4) { for (int l = 0; l < 16; l++) lut[l] = (float)((l - 7.5) / (double)2.95f); }
-    else {
-      double off = getenv("SYMMETRIC_8_BIT_VDIF") ? 127.5 : 128.0;
-      for (int b = 0; b < 256; b++) lut[b] = (float)((b - off) / 3.3);
-    }
-    CKR(h, fstep_set_lut(lut, h->stream));
   }
   const size_t spec_elems = (size_t)d.nfreqs * chunk * J.ninputs * J.nchan;
   CKR(h, cudaMalloc(&h->d_spec, sizeof(float2) * spec_elems));

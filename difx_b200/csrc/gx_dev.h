@@ -49,6 +49,7 @@ struct DevJob {
   double sampletime;      // us
   double bw;              // MHz
   const float2 *twiddle;  // exp(-2 pi i m / F), m in [0, F)
+  float lut[256];         // level of each sample code (VDIF decode table), staged to shared memory
 };
 
 // One subint: device pointers to its buffers.

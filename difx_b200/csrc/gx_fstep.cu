@@ -22,8 +22,6 @@
 
 namespace gx {
 
-__constant__ float c_lut[256];   // level of each sample code (VDIF decode tables)
-
 #define GX_TWO_PI 6.283185307179586476925286766559
 
 struct BlockParams {
@@ -168,6 +166,7 @@ fstep_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays S,
   int *fvalid = reinterpret_cast<int *>(fstep + 2 * nrf * (half > 0 ? half : 1));  // kMaxFramesPerBlock
   __shared__ BlockParams P;
   __shared__ int good_acc;
+  __shared__ float s_lut[256];   // decode table
 
   const int tps = kFThreads / nslots;
   const int myslot = tid / tps;
@@ -177,6 +176,8 @@ fstep_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays S,
   const int64_t datalen = S.datalen[s];
   const int32_t *ctrl = S.control + (size_t)s * S.controlstride;
   const double *ip = S.interp + 3 * s;
+  for (int i = tid; i < 256; i += blockDim.x) s_lut[i] = J.lut[i];
+  __syncthreads();
 
   for (int bi = blockIdx.x * blocks_per_cta; bi < min(nblk, (blockIdx.x + 1) * blocks_per_cta); bi++) {
     const int blk = blk0 + bi;
@@ -338,11 +339,11 @@ fstep_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays S,
             const uint8_t *payload = data + ((long long)P.fr0 + q) * J.framebytes + 32;
             const long long bit0 = (long long)(smp % J.framesamples) * bits_per_ts + (long long)bd * sub * J.nbits;
             const int c0 = (payload[bit0 >> 3] >> (bit0 & 7)) & mask;
-            u.x = c_lut[c0];
+            u.x = s_lut[c0];
             if (J.cplx) {
               const long long bit1 = bit0 + J.nbits;
               const int c1 = (payload[bit1 >> 3] >> (bit1 & 7)) & mask;
-              u.y = c_lut[c1];
+              u.y = s_lut[c1];
             }
           }
           const int k = n % Sd, j = n / Sd;
@@ -390,11 +391,6 @@ size_t fstep_smem_bytes(const DevJob &J, int nrf, int nslots)
   b += (size_t)2 * nrf * (J.stride + (J.half > 0 ? J.half : 1)) * sizeof(float2);
   b += kMaxFramesPerBlock * sizeof(int);
   return b;
-}
-
-cudaError_t fstep_set_lut(const float *lut, cudaStream_t st)
-{
-  return cudaMemcpyToSymbolAsync(c_lut, lut, 256 * sizeof(float), 0, cudaMemcpyHostToDevice, st);
 }
 
 cudaError_t fstep_launch(const DevJob &J, const DevStation *stations, int maxnrf, const SubintArrays &S,

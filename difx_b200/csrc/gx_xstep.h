@@ -29,7 +29,6 @@ struct XmacShape {
 
 XmacShape xmac_shape(int NI);
 
-cudaError_t fstep_set_lut(const float *lut, cudaStream_t st);
 size_t fstep_smem_bytes(const DevJob &J, int nrf, int nslots);
 cudaError_t fstep_launch(const DevJob &J, const DevStation *stations, int maxnrf, const SubintArrays &S,
                          int blk0, int nblk, int nslots, float2 *spec, float *weights, cudaStream_t st);

@@ -1,0 +1,90 @@
+"""The C-ABI library loads and exports every entry point include/gxcorr.h
+declares; host-only handles work without a GPU; descriptor errors are
+reported as status codes, not crashes."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from difx_b200 import capi, gxcorr
+from tests import jobs
+
+HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "gxcorr.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(gx_[a-z_]+)\s*\(", src)))
+
+
+def test_header_and_binding_agree():
+    decl = declared_functions()
+    assert decl, "no declarations parsed"
+    assert sorted(gxcorr.EXPORTED_SYMBOLS) == decl
+
+
+def test_library_exports_every_declared_symbol():
+    lib = gxcorr.lib()
+    for name in declared_functions():
+        assert hasattr(lib, name), name
+
+
+@pytest.mark.skipif(not os.path.exists("/usr/bin/gcc"), reason="no C compiler")
+def test_struct_layout_matches_c_compiler(tmp_path):
+    """ctypes mirrors of the ABI structs have the C compiler's sizes and offsets."""
+    import subprocess
+    structs = {"gx_freq_desc": capi.gx_freq_desc, "gx_station_desc": capi.gx_station_desc,
+               "gx_baseline_desc": capi.gx_baseline_desc, "gx_job_desc": capi.gx_job_desc,
+               "gx_subint_desc": capi.gx_subint_desc, "gx_layout_info": capi.gx_layout_info}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
+    for name, cls in structs.items():
+        lines.append(f'printf("{name} %zu\\n", sizeof({name}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'printf("{name}.{fname} %zu\\n", offsetof({name}, {fname}));')
+    lines.append("return 0;}")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["/usr/bin/gcc", str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = dict(l.split() for l in out if l.strip())
+    for name, cls in structs.items():
+        assert int(got[name]) == C.sizeof(cls), name
+        for fname, _ in cls._fields_:
+            assert int(got[f"{name}.{fname}"]) == getattr(cls, fname).offset, (name, fname)
+
+
+def test_host_only_handle_layout():
+    spec = jobs.spec_c1()
+    jd = capi.job_desc_from_spec(spec)
+    c = gxcorr.Correlator.from_desc(jd, device=-1)
+    assert c.info.nchan == spec.nchan
+    assert c.info.fftchannels == 2 * spec.nchan
+    assert c.info.blocks_per_send == spec.blocks_per_send
+    assert c.info.array_stride == 16 and c.info.xmac_stride == 128
+    with pytest.raises(gxcorr.GxError) as ei:
+        c.subint(capi.SubintDesc(0, 0, 0, 0.0, [0] * 4, [0] * 4, [0] * 4, 3))
+    assert ei.value.status == 8   # GX_ERR_STATE: host-only handle
+    c.close()
+
+
+@pytest.mark.parametrize("mutate,status", [
+    (lambda d: setattr(d.desc, "fringe_rotation_order", 2), 2),
+    (lambda d: setattr(d.desc, "subint_ns", 8_000_001), 1),
+    (lambda d: setattr(d._st[1], "nbits", 8), 2),
+])
+def test_bad_descriptors_are_rejected(mutate, status):
+    jd = capi.job_desc_from_spec(jobs.spec_c1())
+    mutate(jd)
+    with pytest.raises(gxcorr.GxError) as ei:
+        gxcorr.Correlator.from_desc(jd, device=-1)
+    assert ei.value.status == status
+
+
+def test_missing_input_file_is_an_io_error():
+    with pytest.raises(gxcorr.GxError) as ei:
+        gxcorr.Correlator.from_input("/nonexistent/job.input", device=-1)
+    assert ei.value.status == 5
