@@ -20,6 +20,7 @@
 #include "gx_dev.h"
 #include "gx_xstep.h"
 #include "gx_host.h"
+#include "gx_plan.h"
 
 using namespace gx;
 
@@ -83,6 +84,7 @@ struct gx_handle {
   int launches = 0;
 
   std::unique_ptr<HostModel> model;  // only for gx_open_input
+  std::vector<DevStation> dst;       // host copy of the per-station device constants
 
   gx_status fail(gx_status s, const std::string &m)
   {
@@ -248,6 +250,7 @@ static gx_status setup(gx_handle *h)
   h->xs = xmac_shape(ni);
   J.ninputs = h->xs.nsuper * h->xs.ST;
   h->xs = xmac_shape(J.ninputs);
+  h->dst = dst;
 
   // Core result layout (populateResultLengths, one phase centre, no bins, no averaging)
   const int nbl = d.nbaselines;
@@ -486,6 +489,46 @@ static gx_status setup(gx_handle *h)
   CKR(h, cudaStreamSynchronize(h->stream));
   return GX_OK;
 }
+
+namespace gx {
+
+// The tables of a host-only open (device -1), handed to callers that place
+// them in their own device memory.
+gx_status plan_job(const gx_job_desc *desc, JobPlan *plan, std::string &err)
+{
+  if (!desc || !plan) { err = "null descriptor or plan"; return GX_ERR_ARG; }
+  gx_handle h;
+  h.device = -1;
+  h.jd = *desc;
+  if (desc->stations && desc->nstations > 0) h.st.assign(desc->stations, desc->stations + desc->nstations);
+  if (desc->freqs && desc->nfreqs > 0) h.fr.assign(desc->freqs, desc->freqs + desc->nfreqs);
+  if (desc->baselines && desc->nbaselines > 0) h.bl.assign(desc->baselines, desc->baselines + desc->nbaselines);
+  h.jd.stations = h.st.data();
+  h.jd.freqs = h.fr.data();
+  h.jd.baselines = h.bl.data();
+  gx_status s = setup(&h);
+  if (s != GX_OK) { err = h.err; return s; }
+  plan->J = h.J;
+  plan->J.twiddle = nullptr;
+  plan->maxnrf = h.maxnrf;
+  plan->nslots = h.nslots;
+  plan->ks = h.ks;
+  plan->xs = h.xs;
+  plan->result_length = h.rl;
+  plan->ctrlstride = 3 + h.J.flaglen;
+  plan->stations = h.dst;
+  plan->prods = h.prods;
+  plan->wents = h.wents;
+  plan->pairs = h.pairs;
+  plan->twiddle.resize(h.J.fftlen);
+  for (int m = 0; m < h.J.fftlen; m++) {
+    double a = -2.0 * M_PI * (double)m / (double)h.J.fftlen;
+    plan->twiddle[m] = make_float2((float)std::cos(a), (float)std::sin(a));
+  }
+  return GX_OK;
+}
+
+}  // namespace gx
 
 extern "C" {
 

@@ -41,7 +41,7 @@ def lib():
         L.gx_status_string.restype = C.c_char_p
         for name in ("gx_open", "gx_open_input", "gx_close", "gx_get_layout", "gx_get_offsets", "gx_interpolator",
                      "gx_scan_start_sec", "gx_subint", "gx_subint_device", "gx_synchronize", "gx_spectra",
-                     "gx_stage_times", "gx_launch_count"):
+                     "gx_stage_times", "gx_launch_count", "gx_subint_device_noalloc"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -49,7 +49,23 @@ def lib():
 
 EXPORTED_SYMBOLS = ("gx_open", "gx_open_input", "gx_close", "gx_last_error", "gx_status_string",
                     "gx_get_layout", "gx_get_offsets", "gx_interpolator", "gx_scan_start_sec", "gx_subint",
-                    "gx_subint_device", "gx_synchronize", "gx_spectra", "gx_stage_times", "gx_launch_count")
+                    "gx_subint_device", "gx_synchronize", "gx_spectra", "gx_stage_times", "gx_launch_count",
+                    "gx_subint_device_noalloc")
+
+
+def subint_device_noalloc(jd: capi.JobDesc, sd: capi.SubintDesc, dev_results_ptr: int, stream_ptr: int = 0) -> None:
+    """One subint without any device allocation (gx_subint_device_noalloc).
+
+    For callers that cannot allocate device memory: sd holds device data
+    pointers (host control words and interpolators); results go to the
+    caller's device buffer.  Work runs on `stream_ptr` (0 = legacy default
+    stream) and is not synchronised.  Calls share one library-wide scratch
+    array, so calls must not overlap on the GPU."""
+    err = C.create_string_buffer(512)
+    st = lib().gx_subint_device_noalloc(jd.ptr(), sd.ptr(), C.c_void_p(dev_results_ptr),
+                                        C.c_void_p(stream_ptr) if stream_ptr else None, err, len(err))
+    if st != 0:
+        raise GxError(st, err.value.decode(errors="replace"))
 
 
 class Correlator:

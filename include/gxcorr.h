@@ -172,6 +172,24 @@ gx_status gx_subint(gx_handle *h, const gx_subint_desc *sub, float *results);
 gx_status gx_subint_device(gx_handle *h, const gx_subint_desc *sub, float *dev_results, void *stream);
 gx_status gx_synchronize(gx_handle *h);
 
+/* No counterpart in the reference.  The same subint work as gx_subint_device
+   for callers that cannot allocate device memory (code inside CUDA stream
+   capture, real-time threads that must not take cudaMalloc's implicit
+   synchronisation, host frameworks that own all device memory and only pass
+   buffers in).  No handle: desc is planned on every call; sub->data are
+   device pointers, sub->control and sub->interp host pointers (interp is
+   required).  Everything besides the caller's inputs and dev_results lives in
+   one library-wide scratch array of GX_NOALLOC_SCRATCH_BYTES in device global
+   memory, which every GPU that loads the library holds until exit; jobs that
+   do not fit return GX_ERR_UNSUPPORTED with the bytes needed in err.  The
+   call allocates no device memory.  All calls share the array: calls whose
+   work overlaps on the GPU race, so order them on one stream.  Only the FP32
+   X-step form is available on this path.  err (may be NULL) receives a
+   message of at most errlen bytes. */
+#define GX_NOALLOC_SCRATCH_BYTES (64u << 20)
+gx_status gx_subint_device_noalloc(const gx_job_desc *desc, const gx_subint_desc *sub, float *dev_results,
+                                   void *stream, char *err, int errlen);
+
 /* Spectra of one FFT block of one datastream after the last gx_subint* call
    (nbands x nchan complex floats, after fractional-sample correction), and its weight. */
 gx_status gx_spectra(gx_handle *h, int station, int block, float *out, float *weight);
