@@ -204,6 +204,8 @@ def main():
     ap.add_argument("--config", default="c2", choices=["c2", "c1"])
     ap.add_argument("--xstep", default="fp32", choices=["fp32", "tc"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--subint-ms", type=float, default=200.0,
+                    help="subint length (default 200 ms); smaller values give small profiling cases")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
@@ -221,7 +223,7 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
 
-    spec = workload_spec(args.config)
+    spec = workload_spec(args.config, subint_ns=int(round(args.subint_ms * 1e6)))
     xstep = capi.GX_XSTEP_FP32 if args.xstep == "fp32" else capi.GX_XSTEP_TC_FP16
     d = tempfile.mkdtemp(prefix=f"gxbench{rank}_")
     paths = write_job(spec, d)

@@ -65,6 +65,7 @@ struct gx_handle {
   DevStation *d_st = nullptr;
   float2 *d_tw = nullptr, *d_spec = nullptr, *d_acc = nullptr, *d_results = nullptr, *d_spec1 = nullptr;
   float *d_w = nullptr, *d_wacc = nullptr, *d_w1 = nullptr;
+  BlockParam *d_bp = nullptr, *d_bp1 = nullptr;
   size_t acc_slice = 0;  // float2 per K-split slice
   int2 *d_pairs = nullptr;
   ProdEntry *d_prods = nullptr;
@@ -109,7 +110,8 @@ static void free_all(gx_handle *h)
 {
   if (h->device < 0) return;
   void *ptrs[] = {h->d_st, h->d_tw, h->d_spec, h->d_acc, h->d_results, h->d_spec1, h->d_w, h->d_wacc, h->d_w1,
-                  h->d_pairs, h->d_prods, h->d_went, (void *)h->d_dataptrs, h->d_datalen, h->d_ctrl, h->d_interp};
+                  h->d_pairs, h->d_prods, h->d_went, (void *)h->d_dataptrs, h->d_datalen, h->d_ctrl, h->d_interp,
+                  h->d_bp, h->d_bp1};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   for (auto p : h->d_data)
@@ -178,6 +180,9 @@ static gx_status setup(gx_handle *h)
   J.stride = d.array_stride > 0 ? d.array_stride : stride_length(f0.nchan);
   if (J.fftlen % J.stride) return h->fail(GX_ERR_ARG, "array stride does not divide the FFT length");
   J.nfr = J.fftlen / J.stride;
+  if (J.stride & (J.stride - 1)) return h->fail(GX_ERR_UNSUPPORTED, "array stride must be a power of two");
+  J.lgstride = 0;
+  while ((1 << J.lgstride) < J.stride) J.lgstride++;
   J.half = (cplx ? 2 * J.nfr : J.nfr) / 2;
   J.unpacksamples = cplx ? f0.nchan : 2 * f0.nchan;
   J.sampletime = 1.0 / (2.0 * f0.bw_mhz);
@@ -407,10 +412,19 @@ static gx_status setup(gx_handle *h)
   h->chunk = chunk;
   {
     long long base = (long long)((J.nchan + xs.CT - 1) / xs.CT) * xs.npairs * d.nfreqs;
-    int ks = (int)((296 + base - 1) / base);
-    ks = std::max(1, std::min(ks, 16));
-    ks = std::max(1, std::min(ks, chunk / 16 > 0 ? chunk / 16 : 1));
-    h->ks = ks;
+    // K-split: enough CTAs for at least two per SM, rounded to whole waves of
+    // 148 SMs where possible, keeping at least 64 blocks per slice
+    const int kmax = std::max(1, std::min(16, chunk / 64));
+    int best = 1;
+    double best_score = -1;
+    for (int ks = 1; ks <= kmax; ks++) {
+      const long long ctas = base * ks;
+      const double waves = std::ceil(ctas / 148.0);
+      const double eff = ctas / (waves * 148.0);
+      const double score = eff * std::min(1.0, ctas / 296.0);
+      if (score > best_score + 1e-9) { best_score = score; best = ks; }
+    }
+    h->ks = best;
   }
   // F-step concurrency: FFT slots per CTA
   {
@@ -459,6 +473,8 @@ static gx_status setup(gx_handle *h)
   CKR(h, cudaMemsetAsync(h->d_spec1, 0, sizeof(float2) * (size_t)d.nfreqs * J.ninputs * J.nchan, h->stream));
   CKR(h, cudaMalloc(&h->d_w, sizeof(float) * (size_t)d.nstations * chunk));
   CKR(h, cudaMalloc(&h->d_w1, sizeof(float) * (size_t)d.nstations));
+  CKR(h, cudaMalloc(&h->d_bp, sizeof(BlockParam) * (size_t)d.nstations * chunk));
+  CKR(h, cudaMalloc(&h->d_bp1, sizeof(BlockParam) * (size_t)d.nstations));
   h->acc_slice = (size_t)d.nfreqs * xs.npairs * xs.ST * xs.ST * J.nchan;
   CKR(h, cudaMalloc(&h->d_acc, sizeof(float2) * h->acc_slice * h->ks));
   CKR(h, cudaMalloc(&h->d_wacc, sizeof(float) * (d.nstations + nbl)));
@@ -674,7 +690,7 @@ static gx_status run_device(gx_handle *h, const gx_subint_desc *sub, const uint8
     const int nb = std::min(h->chunk, J.blocks_per_send - b0);
     gx_status r;
     if ((r = record(h, st, 0, true)) != GX_OK) return r;
-    CKR(h, fstep_launch(J, h->d_st, h->maxnrf, S, b0, nb, h->nslots, h->d_spec, h->d_w, st));
+    CKR(h, fstep_launch(J, h->d_st, h->maxnrf, S, b0, nb, h->nslots, h->d_spec, h->d_w, h->d_bp, st));
     if ((r = record(h, st, 0, false)) != GX_OK) return r;
     if ((r = record(h, st, 1, true)) != GX_OK) return r;
     CKR(h, xmac_fp32_launch(h->d_spec, nb, J.ninputs, J.nchan, d.nfreqs, h->ks, h->d_acc, st));
@@ -763,7 +779,8 @@ gx_status gx_spectra(gx_handle *h, int station, int block, float *out, float *we
   if (station < 0 || station >= J.nstations || block < 0 || block >= J.blocks_per_send)
     return h->fail(GX_ERR_ARG, "station or block out of range");
   CKR(h, cudaSetDevice(h->device));
-  CKR(h, fstep_launch(J, h->d_st, h->maxnrf, h->last, block, 1, h->nslots, h->d_spec1, h->d_w1, h->stream));
+  CKR(h, fstep_launch(J, h->d_st, h->maxnrf, h->last, block, 1, h->nslots, h->d_spec1, h->d_w1, h->d_bp1,
+                      h->stream));
   const gx_station_desc &x = h->jd.stations[station];
   for (int b = 0; b < x.nbands; b++) {
     int f = x.recfreq[x.band_localfreq[b]];

@@ -9,7 +9,7 @@
 
 namespace gx {
 
-constexpr int kMaxFramesPerBlock = 256;  // frames one FFT block may span
+constexpr int kMaxFramesPerBlock = 64;   // frames one FFT block may span (bits of BlockParam::validmask)
 constexpr int kFThreads = 256;           // threads per F-step CTA
 constexpr int kMaxFreqsPerStation = GX_MAX_LOCAL_FREQS;
 
@@ -46,10 +46,22 @@ struct DevJob {
   int nfreqs;
   int blocks_per_send;
   int flaglen;
+  int lgstride;           // log2(stride): FFT length, channels and stride are powers of two
   double sampletime;      // us
   double bw;              // MHz
   const float2 *twiddle;  // exp(-2 pi i m / F), m in [0, F)
   float lut[256];         // level of each sample code (VDIF decode table), staged to shared memory
+};
+
+// Per (station, FFT block) parameters, computed in FP64 by blockparams_kernel
+// (mode.cpp:656-757, 782-799; mk5mode.cpp:94-174) and read by the F-step.
+struct __align__(16) BlockParam {
+  double a, b;                    // linear delay interpolation over the block (us), b without integer part
+  double fracwalltime;
+  unsigned long long validmask;   // bit q: frame fr0+q is valid
+  int nearestsample, fr0, integerdelay, intwalltime;
+  float fracsampleerror, weight;
+  int state, nframes;             // state 0: zeroed block
 };
 
 // One subint: device pointers to its buffers.

@@ -3,9 +3,17 @@
 // fractional-sample correction, writing spectra in the layout the X-step
 // reads: spec[freq][block][input][channel] (float2).
 //
-// One CTA processes a run of consecutive FFT blocks of one station; the
-// recorded bands of a block are transformed concurrently in "slots" (one
-// FFT per slot, ping-pong buffers in shared memory).
+// Two kernels per pass of blocks:
+//   blockparams_kernel  one thread per (station, block): FP64 delay, nearest
+//                       sample, fractional-sample error, linear interpolation
+//                       coefficients, frame-validity mask and data weight.
+//   fstep_warp_kernel   (FFT length <= 1024) one warp per (block, band): the
+//                       warp builds its rotator tables, decodes and rotates
+//                       its samples into warp-private shared memory, runs the
+//                       FFT with warp-level synchronisation only and writes
+//                       the corrected spectrum row.
+//   fstep_cta_kernel    (longer FFTs) the bands of a block are transformed
+//                       concurrently in slots of one CTA.
 //
 // Reference semantics followed (mpifxcorr/src):
 //   block validity / delay / nearest sample      mode.cpp:656-701
@@ -23,19 +31,6 @@
 namespace gx {
 
 #define GX_TWO_PI 6.283185307179586476925286766559
-
-struct BlockParams {
-  int state;             // 0 zero block, 1 process
-  int nearestsample;
-  int fr0, nframes;
-  int integerdelay;
-  int intwalltime;
-  float fracsampleerror;
-  float weight;
-  double a, b;
-  double fracwalltime;
-  int good;
-};
 
 __device__ __forceinline__ float2 cmul_exact(float2 a, float2 b)
 {
@@ -80,10 +75,10 @@ __device__ __forceinline__ void dft8(float2 *v)
   v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
 }
 
-// One Stockham radix-R pass over one slot's buffer: in -> out.
+// One Stockham radix-R pass: in -> out, butterflies j = lt, lt+nt, ...
 template <int R>
 __device__ __forceinline__ void stockham_pass(const float2 *in, float2 *out, int F, int Ns,
-                                              const float2 *tw, int lt, int nt)
+                                              const float2 *__restrict__ tw, int lt, int nt)
 {
   const int nb = F / R;
   const int twstep = F / (Ns * R);
@@ -109,26 +104,6 @@ __device__ __forceinline__ void stockham_pass(const float2 *in, float2 *out, int
   }
 }
 
-// Whole forward FFT of one slot (bufA holds the input); returns the buffer holding the result.
-__device__ float2 *slot_fft(float2 *bufA, float2 *bufB, int F, const float2 *tw, int lt, int nt,
-                            int slot_threads_first, int nslots_active)
-{
-  float2 *in = bufA, *out = bufB;
-  int Ns = 1;
-  while (Ns < F) {
-    int R = (Ns * 8 <= F) ? 8 : ((Ns * 4 <= F) ? 4 : 2);
-    if (lt >= 0) {
-      if (R == 8) stockham_pass<8>(in, out, F, Ns, tw, lt, nt);
-      else if (R == 4) stockham_pass<4>(in, out, F, Ns, tw, lt, nt);
-      else stockham_pass<2>(in, out, F, Ns, tw, lt, nt);
-    }
-    __syncthreads();
-    float2 *t = in; in = out; out = t;
-    Ns *= R;
-  }
-  return in;
-}
-
 __device__ __forceinline__ int frame_ok(const uint8_t *frame, int framebytes, int check_header)
 {
   const uint32_t *h = reinterpret_cast<const uint32_t *>(frame);
@@ -145,179 +120,376 @@ __device__ __forceinline__ int frame_ok(const uint8_t *frame, int framebytes, in
   return 1;
 }
 
+// --------------------------------------------------------------------------
+// Per-block parameters (FP64): mode.cpp:656-757 and 782-799, mk5mode.cpp:94-174.
+__global__ void blockparams_kernel(DevJob J, SubintArrays S, int blk0, int nblk, BlockParam *__restrict__ bp,
+                                   float *__restrict__ weights)
+{
+  const int bi = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (bi >= nblk) return;
+  const int blk = blk0 + bi;
+  const int F = J.fftlen;
+  BlockParam P;
+  P.state = 0;
+  P.weight = 0.0f;
+  P.a = P.b = P.fracwalltime = 0.0;
+  P.validmask = 0ull;
+  P.nearestsample = P.fr0 = P.integerdelay = P.intwalltime = P.nframes = 0;
+  P.fracsampleerror = 0.0f;
+  const uint8_t *data = S.data[s];
+  const int64_t datalen = S.datalen[s];
+  const int32_t *ctrl = S.control + (size_t)s * S.controlstride;
+  const double *ip = S.interp + 3 * s;
+  const int datasec = ctrl[1], datans = ctrl[2];
+  const int flagword = ctrl[3 + blk / 30];
+  if (datalen > 1 && ((flagword >> (blk % 30)) & 1) != 0) {
+    const double fftcentre = blk + 0.5;
+    const double averagedelay = ip[0] * fftcentre * fftcentre + ip[1] * fftcentre + ip[2];
+    const double fftstartmicrosec = (blk * F) * J.sampletime;
+    const double starttime = (S.sec - datasec) * 1000000.0 +
+                             ((long long)S.ns - (long long)datans) / 1000.0 + fftstartmicrosec - averagedelay;
+    int ns = (int)(starttime / J.sampletime + 0.5);
+    const double walltimesecs = (double)((long long)S.scan_start_sec + S.sec) + S.ns / 1.0e9 +
+                                fftstartmicrosec / 1.0e6;
+    P.intwalltime = (int)walltimesecs;
+    P.fracwalltime = walltimesecs - P.intwalltime;
+    if (!(ns < -1 || (long long)(ns + F) * J.bytespersample > datalen)) {
+      if (ns == -1) ns = 0;
+      P.nearestsample = ns;
+      P.fr0 = ns / J.framesamples;
+      P.nframes = (ns + J.unpacksamples - 1) / J.framesamples - P.fr0 + 1;
+      if (P.nframes <= kMaxFramesPerBlock) {
+        int good = 0;
+        for (int q = 0; q < P.nframes; q++) {
+          const long long fr = (long long)P.fr0 + q;
+          int ok = 0;
+          if ((fr + 1) * J.framebytes <= datalen)
+            ok = frame_ok(data + fr * J.framebytes, J.framebytes, !(J.cplx && q == 0));
+          if (ok) {
+            P.validmask |= (1ull << q);
+            const long long lo = max((long long)ns, fr * J.framesamples);
+            const long long hi = min((long long)ns + J.unpacksamples, (fr + 1) * J.framesamples);
+            good += (int)(hi - lo);
+          }
+        }
+        P.weight = (float)good / (float)J.unpacksamples;
+        if (P.weight > 0.0f) {
+          P.state = 1;
+          P.fracsampleerror = (float)(starttime - ns * J.sampletime);
+          const double d0 = ip[0] * blk * blk + ip[1] * blk + ip[2];
+          const double d1 = ip[0] * (blk + 0.5) * (blk + 0.5) + ip[1] * (blk + 0.5) + ip[2];
+          const double d2 = ip[0] * (blk + 1) * (blk + 1) + ip[1] * (blk + 1) + ip[2];
+          const double a = d2 - d0;
+          double b = d0 + (d1 - (a * 0.5 + d0)) / 3.0;
+          const int idelay = (int)b;
+          b -= idelay;
+          P.a = a;
+          P.b = b;
+          P.integerdelay = idelay;
+        } else {
+          P.weight = 0.0f;
+        }
+      }
+    }
+  }
+  bp[(size_t)s * nblk + bi] = P;
+  weights[(size_t)s * nblk + bi] = P.state ? P.weight : 0.0f;
+}
+
+// Fringe-rotator table entry e of local freq fi: e < S -> sub[e], else step[e - S]
+// (mode.cpp:882-955: FP64 phases, FP32 argument, sincos).
+__device__ __forceinline__ float2 fringe_entry(const DevJob &J, const DevStation &st, int fi, int e,
+                                               const BlockParam &P)
+{
+  const int Sd = J.stride, F = J.fftlen;
+  const double lofreq = st.lofreq[fi];
+  const double looffset = st.looff[fi];
+  const bool looff = (looffset > 0.0 || looffset < 0.0);
+  double ph;
+  if (e < Sd) {
+    double x = ((double)e / (double)F) * P.a;
+    x += P.b;
+    ph = x * lofreq;
+    if (st.fractional_lo) ph += (lofreq - (int)lofreq) * (double)P.integerdelay;
+    if (looff) {
+      ph += ((e * J.sampletime) / 1e6) * -looffset;
+      ph += -looffset * P.fracwalltime;
+      double fl = fabs(looffset) - (int)fabs(looffset);
+      const bool isfrac = fl > (double)0.000000001f;
+      if (looffset < 0) fl = -fl;
+      if (isfrac) ph += -fl * P.intwalltime;
+    }
+  } else {
+    const int j = e - Sd;
+    const double x = ((double)(j * Sd) / (double)F) * P.a;
+    ph = x * lofreq;
+    if (looff) ph += ((j * Sd * J.sampletime) / 1e6) * -looffset;
+  }
+  const float arg = (float)(-GX_TWO_PI * (ph - (int)ph));
+  float sn, cs;
+  sincosf(arg, &sn, &cs);
+  return make_float2(cs, sn);
+}
+
+// Fractional-sample rotator entry e of local freq fi, polarisation set ps
+// (0: A, 1: B): e < S -> sub[e], else step[e - S] (mode.cpp:1029-1122).
+__device__ __forceinline__ float2 frac_entry(const DevJob &J, const DevStation &st, int fi, int ps, int e,
+                                             const BlockParam &P)
+{
+  const int Sd = J.stride, N = J.nchan, half = J.half;
+  const double sgn = ps == 0 ? 1.0 : -1.0;
+  const float val = (float)((double)P.fracsampleerror - st.clk[fi] + sgn * st.clkdelta[fi] / 2);
+  float cfreq;
+  if (e < Sd) {
+    cfreq = (float)((GX_TWO_PI * (e) * J.bw) / N);
+  } else {
+    const int j = e - Sd;
+    cfreq = st.lsb[fi] ? (float)((-GX_TWO_PI * ((half - j) * Sd) * J.bw) / N)
+                       : (float)((GX_TWO_PI * j * Sd * J.bw) / N);
+  }
+  const float arg = __fmul_rn(cfreq, val);
+  float sn, cs;
+  sincosf(arg, &sn, &cs);
+  return make_float2(cs, sn);
+}
+
+// Decoded sample n of band bd (real in .x, imaginary in .y for complex data).
+__device__ __forceinline__ float2 decode_sample(const DevJob &J, const uint8_t *__restrict__ data,
+                                                const BlockParam &P, int bd, int n, const float *lut)
+{
+  const int smp = P.nearestsample + n;
+  const int q = smp / J.framesamples - P.fr0;
+  float2 u = make_float2(0.f, 0.f);
+  if ((P.validmask >> q) & 1ull) {
+    const int sub = J.cplx ? 2 : 1;
+    const int mask = (1 << J.nbits) - 1;
+    const uint8_t *payload = data + ((long long)P.fr0 + q) * J.framebytes + 32;
+    const long long bit0 = (long long)(smp % J.framesamples) * (J.nbands * J.nbits * sub) +
+                           (long long)bd * sub * J.nbits;
+    u.x = lut[(__ldg(payload + (bit0 >> 3)) >> (bit0 & 7)) & mask];
+    if (J.cplx) {
+      const long long bit1 = bit0 + J.nbits;
+      u.y = lut[(__ldg(payload + (bit1 >> 3)) >> (bit1 & 7)) & mask];
+    }
+  }
+  return u;
+}
+
+// Sideband selection (mode.cpp:1185-1217) of output channel c from FFT result res.
+__device__ __forceinline__ float2 select_channel(const DevJob &J, const float2 *res, int lsb, int c)
+{
+  const int N = J.nchan, F = J.fftlen;
+  if (!J.cplx) return res[lsb ? N + c : c];
+  if (!lsb) return res[c];
+  if (c == 0) return res[0];
+  float2 v = res[F - c];
+  v.y = -v.y;
+  return v;
+}
+
+// --------------------------------------------------------------------------
+// One compile-time Stockham pass (FL points, stride NS, radix R) over one
+// warp's buffer; every index is a shift or mask.
+template <int FL, int NS, int R>
+__device__ __forceinline__ void warp_pass(const float2 *in, float2 *out, const float2 *__restrict__ tw, int lane)
+{
+  constexpr int NB = FL / R;
+  constexpr int TWSTEP = FL / (NS * R);
+#pragma unroll
+  for (int j0 = 0; j0 < NB; j0 += 32) {
+    const int j = j0 + lane;
+    if (NB % 32 != 0 && j >= NB) break;
+    float2 v[R];
+    const int k = j & (NS - 1);
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      float2 x = in[j + r * NB];
+      if (r > 0 && NS > 1) x = cmul(x, __ldg(&tw[r * k * TWSTEP]));
+      v[r] = x;
+    }
+    if (R == 8) dft8(v);
+    else if (R == 4) dft4(v[0], v[1], v[2], v[3]);
+    else {
+      float2 t = v[0];
+      v[0] = cadd(t, v[1]);
+      v[1] = csub(t, v[1]);
+    }
+    const int idxD = (j - k) * R + k;   // (j / NS) * NS * R + k
+#pragma unroll
+    for (int r = 0; r < R; r++) out[idxD + r * NS] = v[r];
+  }
+}
+
+// All passes of an FL-point forward FFT: radix 8 while it fits, then 4 or 2.
+template <int FL, int NS>
+__device__ __forceinline__ float2 *warp_fft(float2 *in, float2 *out, const float2 *__restrict__ tw, int lane)
+{
+  if constexpr (NS >= FL) {
+    return in;
+  } else {
+    constexpr int R = (NS * 8 <= FL) ? 8 : ((NS * 4 <= FL) ? 4 : 2);
+    warp_pass<FL, NS, R>(in, out, tw, lane);
+    __syncwarp();
+    return warp_fft<FL, NS * R>(out, in, tw, lane);
+  }
+}
+
+// Warp-per-(block, band) F-step for FFT lengths up to 1024 (FL points,
+// complex sampling CPLX).
+template <int FL, int CPLX>
 __global__ void __launch_bounds__(kFThreads)
-fstep_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays S,
-             int blk0, int nblk, int blocks_per_cta, int nslots,
-             float2 *__restrict__ spec, float *__restrict__ weights)
+fstep_warp_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays S,
+                  const BlockParam *__restrict__ bp, int nblk, int blocks_per_cta, int wstride,
+                  float2 *__restrict__ spec)
+{
+  constexpr int NCH = CPLX ? FL : FL / 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ float s_lut[256];
+  const int s = blockIdx.y;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  const DevStation &st = stations[s];
+  const int Sd = J.stride, lgS = J.lgstride, nfr = J.nfr, half = J.half;
+  for (int i = tid; i < 256; i += blockDim.x) s_lut[i] = J.lut[i];
+  __syncthreads();
+
+  float2 *A = reinterpret_cast<float2 *>(smem_raw) + (size_t)warp * wstride;
+  float2 *B = A + FL;
+  float2 *rs = B + FL;         // S
+  float2 *rp = rs + Sd;        // nfr
+  float2 *fs = rp + nfr;       // S
+  float2 *fp = fs + Sd;        // half
+
+  const uint8_t *data = S.data[s];
+  const int fsamp = J.framesamples;
+  const int bits_ts = J.nbands * J.nbits * (CPLX ? 2 : 1);
+  const int cmask = (1 << J.nbits) - 1;
+  const int b0 = blockIdx.x * blocks_per_cta;
+  const int nbk = min(blocks_per_cta, nblk - b0);
+  const int nitems = nbk * J.nbands;
+  for (int it = warp; it < nitems; it += nwarps) {
+    const int bi = b0 + it / J.nbands;
+    const int bd = it % J.nbands;
+    const BlockParam P = bp[(size_t)s * nblk + bi];
+    const int lf = st.band_localfreq[bd];
+    const int f = st.freq_index[lf];
+    float2 *dst = spec + (((size_t)f * nblk + bi) * J.ninputs + st.band_input[bd]) * NCH;
+    if (P.state == 0) {
+#pragma unroll
+      for (int c = lane; c < NCH; c += 32) dst[c] = make_float2(0.f, 0.f);
+      continue;
+    }
+    const int ps = st.band_polb[bd] ? 1 : 0;
+    for (int e = lane; e < Sd + nfr; e += 32) {
+      const float2 v = fringe_entry(J, st, lf, e, P);
+      if (e < Sd) rs[e] = v;
+      else rp[e - Sd] = v;
+    }
+    for (int e = lane; e < Sd + half; e += 32) {
+      const float2 v = frac_entry(J, st, lf, ps, e, P);
+      if (e < Sd) fs[e] = v;
+      else fp[e - Sd] = v;
+    }
+    __syncwarp();
+    // decode + rotate: frame q and in-frame sample r advance incrementally
+    {
+      const int smp0 = P.nearestsample + lane;
+      int q = smp0 / fsamp;
+      int r = smp0 - q * fsamp;
+      q -= P.fr0;
+      const int bitband = bd * (CPLX ? 2 : 1) * J.nbits;
+#pragma unroll 4
+      for (int n = lane; n < FL; n += 32) {
+        float2 u = make_float2(0.f, 0.f);
+        if ((P.validmask >> q) & 1ull) {
+          const uint8_t *payload = data + ((long long)P.fr0 + q) * J.framebytes + 32;
+          const long long bit0 = (long long)r * bits_ts + bitband;
+          u.x = s_lut[(__ldg(payload + (bit0 >> 3)) >> (bit0 & 7)) & cmask];
+          if (CPLX) {
+            const long long bit1 = bit0 + J.nbits;
+            u.y = s_lut[(__ldg(payload + (bit1 >> 3)) >> (bit1 & 7)) & cmask];
+          }
+        }
+        const int k = n & (Sd - 1), j = n >> lgS;
+        const float2 rot = (j == 0) ? rs[k] : cmul_exact(rs[k], rp[j]);
+        A[n] = CPLX ? cmul(rot, u) : make_float2(u.x * rot.x, u.x * rot.y);
+        r += 32;
+        while (r >= fsamp) { r -= fsamp; q++; }
+      }
+    }
+    __syncwarp();
+    const float2 *res = warp_fft<FL, 1>(A, B, J.twiddle, lane);
+    const int lsb = st.lsb[lf];
+#pragma unroll 4
+    for (int c = lane; c < NCH; c += 32) {
+      float2 v;
+      if (!CPLX) v = res[lsb ? NCH + c : c];
+      else if (!lsb) v = res[c];
+      else if (c == 0) v = res[0];
+      else { v = res[FL - c]; v.y = -v.y; }
+      dst[c] = cmul(v, cmul_exact(fs[c & (Sd - 1)], fp[c >> lgS]));
+    }
+    __syncwarp();
+  }
+}
+
+// --------------------------------------------------------------------------
+// Slot-per-band F-step for long FFTs: the bands of a block in waves of
+// nslots concurrent FFTs, each over kFThreads / nslots threads.
+__global__ void __launch_bounds__(kFThreads)
+fstep_cta_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays S,
+                 const BlockParam *__restrict__ bp, int nblk, int blocks_per_cta, int nslots,
+                 float2 *__restrict__ spec)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ float s_lut[256];
+  __shared__ BlockParam P;
   const int s = blockIdx.y;
   const int tid = threadIdx.x;
   const DevStation &st = stations[s];
   const int F = J.fftlen, N = J.nchan, Sd = J.stride, nfr = J.nfr, half = J.half;
   const int nrf = st.nrecfreqs;
+  for (int i = tid; i < 256; i += blockDim.x) s_lut[i] = J.lut[i];
 
-  // shared memory carve-up
-  float2 *slotbuf = reinterpret_cast<float2 *>(smem_raw);                 // nslots * 2F
-  float2 *rsub = slotbuf + (size_t)nslots * 2 * F;                        // nrf * S
-  float2 *rstep = rsub + nrf * Sd;                                         // nrf * nfr
-  float2 *fsub = rstep + nrf * nfr;                                        // 2 * nrf * S
-  float2 *fstep = fsub + 2 * nrf * Sd;                                     // 2 * nrf * half
-  int *fvalid = reinterpret_cast<int *>(fstep + 2 * nrf * (half > 0 ? half : 1));  // kMaxFramesPerBlock
-  __shared__ BlockParams P;
-  __shared__ int good_acc;
-  __shared__ float s_lut[256];   // decode table
+  float2 *slotbuf = reinterpret_cast<float2 *>(smem_raw);   // nslots * 2F
+  float2 *rsub = slotbuf + (size_t)nslots * 2 * F;          // nrf * S
+  float2 *rstep = rsub + nrf * Sd;                           // nrf * nfr
+  float2 *fsub = rstep + nrf * nfr;                          // 2 * nrf * S
+  float2 *fstep = fsub + 2 * nrf * Sd;                       // 2 * nrf * half
 
   const int tps = kFThreads / nslots;
   const int myslot = tid / tps;
   const int lt = (myslot < nslots) ? (tid % tps) : -1;
-
   const uint8_t *data = S.data[s];
-  const int64_t datalen = S.datalen[s];
-  const int32_t *ctrl = S.control + (size_t)s * S.controlstride;
-  const double *ip = S.interp + 3 * s;
-  for (int i = tid; i < 256; i += blockDim.x) s_lut[i] = J.lut[i];
-  __syncthreads();
 
   for (int bi = blockIdx.x * blocks_per_cta; bi < min(nblk, (blockIdx.x + 1) * blocks_per_cta); bi++) {
-    const int blk = blk0 + bi;
-    if (tid == 0) {
-      P.state = 0;
-      P.weight = 0.0f;
-      good_acc = 0;
-      const int datasec = ctrl[1], datans = ctrl[2];
-      const int flagword = ctrl[3 + blk / 30];
-      if (datalen > 1 && ((flagword >> (blk % 30)) & 1) != 0) {
-        const double fftcentre = blk + 0.5;
-        const double averagedelay = ip[0] * fftcentre * fftcentre + ip[1] * fftcentre + ip[2];
-        const double fftstartmicrosec = (blk * F) * J.sampletime;
-        const double starttime = (S.sec - datasec) * 1000000.0 +
-                                 ((long long)S.ns - (long long)datans) / 1000.0 + fftstartmicrosec - averagedelay;
-        int ns = (int)(starttime / J.sampletime + 0.5);
-        const double walltimesecs = (double)((long long)S.scan_start_sec + S.sec) + S.ns / 1.0e9 +
-                                    fftstartmicrosec / 1.0e6;
-        P.intwalltime = (int)walltimesecs;
-        P.fracwalltime = walltimesecs - P.intwalltime;
-        if (!(ns < -1 || (long long)(ns + F) * J.bytespersample > datalen)) {
-          if (ns == -1) ns = 0;
-          P.nearestsample = ns;
-          P.fr0 = ns / J.framesamples;
-          P.nframes = (ns + J.unpacksamples - 1) / J.framesamples - P.fr0 + 1;
-          if (P.nframes <= kMaxFramesPerBlock) {
-            P.state = 1;
-            P.fracsampleerror = (float)(starttime - ns * J.sampletime);
-            const double d0 = ip[0] * blk * blk + ip[1] * blk + ip[2];
-            const double d1 = ip[0] * (blk + 0.5) * (blk + 0.5) + ip[1] * (blk + 0.5) + ip[2];
-            const double d2 = ip[0] * (blk + 1) * (blk + 1) + ip[1] * (blk + 1) + ip[2];
-            const double a = d2 - d0;
-            double b = d0 + (d1 - (a * 0.5 + d0)) / 3.0;
-            const int idelay = (int)b;
-            b -= idelay;
-            P.a = a;
-            P.b = b;
-            P.integerdelay = idelay;
-          }
-        }
-      }
-    }
     __syncthreads();
-    if (P.state == 1) {
-      // frame validity and good-sample count
-      for (int q = tid; q < P.nframes; q += blockDim.x) {
-        const long long fr = (long long)P.fr0 + q;
-        int ok = 0;
-        if ((fr + 1) * J.framebytes <= datalen)
-          ok = frame_ok(data + fr * J.framebytes, J.framebytes, !(J.cplx && q == 0));
-        fvalid[q] = ok;
-        if (ok) {
-          const long long lo = max((long long)P.nearestsample, fr * J.framesamples);
-          const long long hi = min((long long)P.nearestsample + J.unpacksamples, (fr + 1) * J.framesamples);
-          atomicAdd(&good_acc, (int)(hi - lo));
-        }
-      }
-      __syncthreads();
-      if (tid == 0) {
-        P.good = good_acc;
-        P.weight = (float)good_acc / (float)J.unpacksamples;
-        if (!(P.weight > 0.0f)) P.state = 0;
-      }
-      __syncthreads();
-    }
+    if (tid == 0) P = bp[(size_t)s * nblk + bi];
+    __syncthreads();
     if (P.state == 0) {
-      // zeroed block (mode.cpp:656-669, 688-701, 743-754)
       for (int bd = 0; bd < J.nbands; bd++) {
-        const int lf = st.band_localfreq[bd];
-        const int f = st.freq_index[lf];
+        const int f = st.freq_index[st.band_localfreq[bd]];
         float2 *dst = spec + (((size_t)f * nblk + bi) * J.ninputs + st.band_input[bd]) * N;
         for (int c = tid; c < N; c += blockDim.x) dst[c] = make_float2(0.f, 0.f);
       }
-      if (tid == 0) weights[(size_t)s * nblk + bi] = 0.0f;
-      __syncthreads();
       continue;
     }
-
-    // fringe-rotator and fractional-sample tables for every recorded freq (FP64 phases -> FP32 sincos)
     for (int idx = tid; idx < nrf * (Sd + nfr); idx += blockDim.x) {
-      const int fi = idx / (Sd + nfr);
-      const int e = idx % (Sd + nfr);
-      const double lofreq = st.lofreq[fi];
-      const double looffset = st.looff[fi];
-      const bool looff = (looffset > 0.0 || looffset < 0.0);
-      double ph;
-      if (e < Sd) {
-        const int k = e;
-        double x = ((double)k / (double)F) * P.a;
-        x += P.b;
-        ph = x * lofreq;
-        if (st.fractional_lo) ph += (lofreq - (int)lofreq) * (double)P.integerdelay;
-        if (looff) {
-          ph += ((k * J.sampletime) / 1e6) * -looffset;
-          ph += -looffset * P.fracwalltime;
-          double fl = fabs(looffset) - (int)fabs(looffset);
-          const bool isfrac = fl > (double)0.000000001f;
-          if (looffset < 0) fl = -fl;
-          if (isfrac) ph += -fl * P.intwalltime;
-        }
-        const float arg = (float)(-GX_TWO_PI * (ph - (int)ph));
-        float sn, cs;
-        sincosf(arg, &sn, &cs);
-        rsub[fi * Sd + k] = make_float2(cs, sn);
-      } else {
-        const int j = e - Sd;
-        const double x = ((double)(j * Sd) / (double)F) * P.a;
-        ph = x * lofreq;
-        if (looff) ph += ((j * Sd * J.sampletime) / 1e6) * -looffset;
-        const float arg = (float)(-GX_TWO_PI * (ph - (int)ph));
-        float sn, cs;
-        sincosf(arg, &sn, &cs);
-        rstep[fi * nfr + j] = make_float2(cs, sn);
-      }
+      const int fi = idx / (Sd + nfr), e = idx % (Sd + nfr);
+      const float2 v = fringe_entry(J, st, fi, e, P);
+      if (e < Sd) rsub[fi * Sd + e] = v;
+      else rstep[fi * nfr + e - Sd] = v;
     }
     const int npolsets = st.deltapol ? 2 : 1;
     for (int idx = tid; idx < npolsets * nrf * (Sd + half); idx += blockDim.x) {
       const int ps = idx / (nrf * (Sd + half));
       const int r = idx % (nrf * (Sd + half));
-      const int fi = r / (Sd + half);
-      const int e = r % (Sd + half);
-      const double sgn = ps == 0 ? 1.0 : -1.0;
-      const float val = (float)((double)P.fracsampleerror - st.clk[fi] + sgn * st.clkdelta[fi] / 2);
-      float cfreq;
-      if (e < Sd) {
-        cfreq = (float)((GX_TWO_PI * (e) * J.bw) / N);
-      } else {
-        const int j = e - Sd;
-        cfreq = st.lsb[fi] ? (float)((-GX_TWO_PI * ((half - j) * Sd) * J.bw) / N)
-                           : (float)((GX_TWO_PI * j * Sd * J.bw) / N);
-      }
-      const float arg = __fmul_rn(cfreq, val);
-      float sn, cs;
-      sincosf(arg, &sn, &cs);
-      if (e < Sd) fsub[(ps * nrf + fi) * Sd + e] = make_float2(cs, sn);
-      else fstep[(ps * nrf + fi) * half + (e - Sd)] = make_float2(cs, sn);
+      const int fi = r / (Sd + half), e = r % (Sd + half);
+      const float2 v = frac_entry(J, st, fi, ps, e, P);
+      if (e < Sd) fsub[(ps * nrf + fi) * Sd + e] = v;
+      else fstep[(ps * nrf + fi) * half + (e - Sd)] = v;
     }
     __syncthreads();
-
-    // bands in waves of nslots concurrent FFTs
     for (int wave0 = 0; wave0 < J.nbands; wave0 += nslots) {
       const int bd = wave0 + myslot;
       const bool active = (lt >= 0) && (bd < J.nbands);
@@ -328,34 +500,26 @@ fstep_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays S,
         lf = st.band_localfreq[bd];
         const float2 *rs = rsub + lf * Sd;
         const float2 *rp = rstep + lf * nfr;
-        const int sub = J.cplx ? 2 : 1;
-        const int bits_per_ts = J.nbands * J.nbits * sub;
-        const int mask = (1 << J.nbits) - 1;
         for (int n = lt; n < F; n += tps) {
-          const int smp = P.nearestsample + n;
-          const int q = smp / J.framesamples - P.fr0;
-          float2 u = make_float2(0.f, 0.f);
-          if (fvalid[q]) {
-            const uint8_t *payload = data + ((long long)P.fr0 + q) * J.framebytes + 32;
-            const long long bit0 = (long long)(smp % J.framesamples) * bits_per_ts + (long long)bd * sub * J.nbits;
-            const int c0 = (payload[bit0 >> 3] >> (bit0 & 7)) & mask;
-            u.x = s_lut[c0];
-            if (J.cplx) {
-              const long long bit1 = bit0 + J.nbits;
-              const int c1 = (payload[bit1 >> 3] >> (bit1 & 7)) & mask;
-              u.y = s_lut[c1];
-            }
-          }
+          const float2 u = decode_sample(J, data, P, bd, n, s_lut);
           const int k = n % Sd, j = n / Sd;
           const float2 rot = (j == 0) ? rs[k] : cmul_exact(rs[k], rp[j]);
-          float2 v;
-          if (J.cplx) v = cmul(rot, u);
-          else v = make_float2(u.x * rot.x, u.x * rot.y);
-          bufA[n] = v;
+          bufA[n] = J.cplx ? cmul(rot, u) : make_float2(u.x * rot.x, u.x * rot.y);
         }
       }
       __syncthreads();
-      float2 *res = slot_fft(bufA, bufB, F, J.twiddle, active ? lt : -1, tps, 0, nslots);
+      float2 *in = bufA, *out = bufB;
+      for (int Ns = 1; Ns < F;) {
+        const int R = (Ns * 8 <= F) ? 8 : ((Ns * 4 <= F) ? 4 : 2);
+        if (active) {
+          if (R == 8) stockham_pass<8>(in, out, F, Ns, J.twiddle, lt, tps);
+          else if (R == 4) stockham_pass<4>(in, out, F, Ns, J.twiddle, lt, tps);
+          else stockham_pass<2>(in, out, F, Ns, J.twiddle, lt, tps);
+        }
+        __syncthreads();
+        float2 *t = in; in = out; out = t;
+        Ns *= R;
+      }
       if (active) {
         const int f = st.freq_index[lf];
         const int lsb = st.lsb[lf];
@@ -364,50 +528,76 @@ fstep_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays S,
         const float2 *fp = fstep + (ps * nrf + lf) * half;
         float2 *dst = spec + (((size_t)f * nblk + bi) * J.ninputs + st.band_input[bd]) * N;
         for (int c = lt; c < N; c += tps) {
-          float2 v;
-          if (!J.cplx) {
-            v = res[lsb ? N + c : c];
-          } else if (!lsb) {
-            v = res[c];
-          } else {
-            v = (c == 0) ? res[0] : res[F - c];
-            if (c != 0) v.y = -v.y;
-          }
-          const float2 fr = cmul_exact(fs[c % Sd], fp[c / Sd]);
-          dst[c] = cmul(v, fr);
+          const float2 v = select_channel(J, in, lsb, c);
+          dst[c] = cmul(v, cmul_exact(fs[c % Sd], fp[c / Sd]));
         }
       }
       __syncthreads();
     }
-    if (tid == 0) weights[(size_t)s * nblk + bi] = P.weight;
-    __syncthreads();
   }
+}
+
+// --------------------------------------------------------------------------
+static bool use_warp_kernel(const DevJob &J) { return J.fftlen >= 128 && J.fftlen <= 1024; }
+
+static int warp_stride(const DevJob &J)
+{
+  int w = 2 * J.fftlen + 2 * J.stride + J.nfr + (J.half > 0 ? J.half : 1);
+  return (w + 1) & ~1;   // keep each warp's region 16-byte aligned
 }
 
 size_t fstep_smem_bytes(const DevJob &J, int nrf, int nslots)
 {
+  if (use_warp_kernel(J)) return (size_t)(kFThreads / 32) * warp_stride(J) * sizeof(float2);
   size_t b = (size_t)nslots * 2 * J.fftlen * sizeof(float2);
   b += (size_t)nrf * (J.stride + J.nfr) * sizeof(float2);
   b += (size_t)2 * nrf * (J.stride + (J.half > 0 ? J.half : 1)) * sizeof(float2);
-  b += kMaxFramesPerBlock * sizeof(int);
   return b;
 }
 
-cudaError_t fstep_launch(const DevJob &J, const DevStation *stations, int maxnrf, const SubintArrays &S,
-                         int blk0, int nblk, int nslots, float2 *spec, float *weights, cudaStream_t st)
+template <typename K>
+static cudaError_t opt_in(K kernel, size_t bytes, size_t &have)
 {
-  const int bpc = 4;
-  dim3 grid((nblk + bpc - 1) / bpc, J.nstations);
-  size_t sm = fstep_smem_bytes(J, maxnrf, nslots);
-  // opt in to the dynamic shared memory this launch needs (the kernel's
-  // static shared memory counts against the same 227 KB per block)
-  static size_t attr_bytes = 48 * 1024;
-  if (sm > attr_bytes) {
-    cudaError_t e = cudaFuncSetAttribute(fstep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    attr_bytes = sm;
+  if (bytes <= have) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) have = bytes;
+  return e;
+}
+
+cudaError_t fstep_launch(const DevJob &J, const DevStation *stations, int maxnrf, const SubintArrays &S,
+                         int blk0, int nblk, int nslots, float2 *spec, float *weights, BlockParam *bp,
+                         cudaStream_t st)
+{
+  {
+    dim3 grid((nblk + 127) / 128, J.nstations);
+    blockparams_kernel<<<grid, 128, 0, st>>>(J, S, blk0, nblk, bp, weights);
   }
-  fstep_kernel<<<grid, kFThreads, sm, st>>>(J, stations, S, blk0, nblk, bpc, nslots, spec, weights);
+  const size_t sm = fstep_smem_bytes(J, maxnrf, nslots);
+  if (use_warp_kernel(J)) {
+    // enough items per CTA that each warp has several (block, band) items
+    const int bpc = (J.nbands >= 8) ? 4 : 16;
+    dim3 grid((nblk + bpc - 1) / bpc, J.nstations);
+    const int ws = warp_stride(J);
+#define GX_WARP_CASE(FLV, CX)                                                                         \
+    if (J.fftlen == FLV && J.cplx == CX) {                                                            \
+      static size_t have = 48 * 1024;                                                                 \
+      cudaError_t e = opt_in(fstep_warp_kernel<FLV, CX>, sm, have);                                   \
+      if (e != cudaSuccess) return e;                                                                 \
+      fstep_warp_kernel<FLV, CX><<<grid, kFThreads, sm, st>>>(J, stations, S, bp, nblk, bpc, ws, spec); \
+      return cudaGetLastError();                                                                      \
+    }
+    GX_WARP_CASE(128, 0) GX_WARP_CASE(256, 0) GX_WARP_CASE(512, 0) GX_WARP_CASE(1024, 0)
+    GX_WARP_CASE(128, 1) GX_WARP_CASE(256, 1) GX_WARP_CASE(512, 1) GX_WARP_CASE(1024, 1)
+#undef GX_WARP_CASE
+  }
+  {
+    static size_t have = 48 * 1024;
+    cudaError_t e = opt_in(fstep_cta_kernel, sm, have);
+    if (e != cudaSuccess) return e;
+    const int bpc = 2;
+    dim3 grid((nblk + bpc - 1) / bpc, J.nstations);
+    fstep_cta_kernel<<<grid, kFThreads, sm, st>>>(J, stations, S, bp, nblk, bpc, nslots, spec);
+  }
   return cudaGetLastError();
 }
 

@@ -116,7 +116,8 @@ extern "C" gx_status gx_subint_device_noalloc(const gx_job_desc *desc, const gx_
   const size_t o_wacc = take(sizeof(float) * (nst + nbl));
   const size_t acc_slice = (size_t)J0.nfreqs * plan.xs.npairs * plan.xs.ST * plan.xs.ST * J0.nchan;
   int ks = plan.ks;
-  const size_t per_block = sizeof(float2) * (size_t)J0.nfreqs * J0.ninputs * J0.nchan + sizeof(float) * nst;
+  const size_t per_block = sizeof(float2) * (size_t)J0.nfreqs * J0.ninputs * J0.nchan +
+                           (sizeof(float) + sizeof(BlockParam)) * nst + 512;
   size_t fixed = off + align256(sizeof(float2) * acc_slice * ks);
   if (fixed + per_block + 512 > kScratchBytes && ks > 1) {
     ks = 1;
@@ -134,6 +135,7 @@ extern "C" gx_status gx_subint_device_noalloc(const gx_job_desc *desc, const gx_
   ks = std::max(1, std::min(ks, chunk / 16 > 0 ? chunk / 16 : 1));
   const size_t o_acc = take(sizeof(float2) * acc_slice * ks);
   const size_t o_w = take(sizeof(float) * (size_t)nst * chunk);
+  const size_t o_bp = take(sizeof(BlockParam) * (size_t)nst * chunk);
   const size_t spec_bytes = sizeof(float2) * (size_t)J0.nfreqs * chunk * J0.ninputs * J0.nchan;
   const size_t o_spec = take(spec_bytes);
   if (off > kScratchBytes) {
@@ -163,6 +165,7 @@ extern "C" gx_status gx_subint_device_noalloc(const gx_job_desc *desc, const gx_
   float *d_wacc = reinterpret_cast<float *>(base + o_wacc);
   float2 *d_acc = reinterpret_cast<float2 *>(base + o_acc);
   float *d_w = reinterpret_cast<float *>(base + o_w);
+  BlockParam *d_bp = reinterpret_cast<BlockParam *>(base + o_bp);
   float2 *d_spec = reinterpret_cast<float2 *>(base + o_spec);
 
   // per-call tables (host sources are staged by the copy calls before they return)
@@ -209,7 +212,7 @@ extern "C" gx_status gx_subint_device_noalloc(const gx_job_desc *desc, const gx_
   S.interp = d_interp;
   for (int b0 = 0; b0 < J.blocks_per_send; b0 += chunk) {
     const int nb = std::min(chunk, J.blocks_per_send - b0);
-    NA_CK(fstep_launch(J, d_st, plan.maxnrf, S, b0, nb, plan.nslots, d_spec, d_w, st));
+    NA_CK(fstep_launch(J, d_st, plan.maxnrf, S, b0, nb, plan.nslots, d_spec, d_w, d_bp, st));
     NA_CK(xmac_fp32_launch(d_spec, nb, J.ninputs, J.nchan, J.nfreqs, ks, d_acc, st));
     NA_CK(weights_launch(d_w, nb, nst, d_pairs, nbl, d_wacc, st));
   }

@@ -21,6 +21,15 @@
 
 namespace gx {
 
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes)
+{
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
 template <int T, int ST, int CT, int KB>
 __global__ void __launch_bounds__(CT *(ST / T) * (ST / T))
 xmac_fp32_kernel(const float2 *__restrict__ spec, int nblk, int NI, int N, int nsuper,
@@ -28,8 +37,10 @@ xmac_fp32_kernel(const float2 *__restrict__ spec, int nblk, int NI, int N, int n
 {
   constexpr int NT = ST / T;            // register tiles per super-tile side
   constexpr int NTHREADS = CT * NT * NT;
-  __shared__ __align__(16) float2 sI[KB][ST][CT];
-  __shared__ __align__(16) float2 sJ[KB][ST][CT];
+  constexpr int STAGE = KB * ST * CT;   // float2 per stage per operand
+  extern __shared__ __align__(16) float2 xsm[];
+  float2 *sI = xsm;                     // [2][KB][ST][CT]
+  float2 *sJ = xsm + 2 * STAGE;         // [2][KB][ST][CT]
 
   const int tid = threadIdx.x;
   const int c = tid % CT;
@@ -39,14 +50,36 @@ xmac_fp32_kernel(const float2 *__restrict__ spec, int nblk, int NI, int N, int n
   const int stp = blockIdx.y;           // super-tile pair index (upper triangle, row-major)
   const int f = blockIdx.z / ks_count;
   const int ks = blockIdx.z % ks_count;
-  // decode (SI, SJ) from the upper-triangle index
   int SI = 0, rem = stp;
   while (rem >= nsuper - SI) { rem -= nsuper - SI; SI++; }
   const int SJ = SI + rem;
   const int I0 = SI * ST, J0 = SJ * ST;
+  const bool diag = (SI == SJ);
+  const float2 *sJread = diag ? sI : sJ;
 
   const int kper = (nblk + ks_count - 1) / ks_count;
   const int kb0 = ks * kper, kb1 = min(nblk, kb0 + kper);
+  const int nstages = (kb1 > kb0) ? (kb1 - kb0 + KB - 1) / KB : 0;
+
+  // one stage: rows [I0, I0+ST) (and [J0, J0+ST) off the diagonal) x CT channels x KB blocks,
+  // 16-byte (two-channel) pieces; missing blocks/channels are zero-filled
+  auto load_stage = [&](int st, int buf) {
+    const int k = kb0 + st * KB;
+    constexpr int PIECES = KB * ST * (CT / 2);
+    for (int e = tid; e < PIECES * (diag ? 1 : 2); e += NTHREADS) {
+      const int opnd = e / PIECES;
+      const int q = e % PIECES;
+      const int kk = q / (ST * (CT / 2));
+      const int r = (q / (CT / 2)) % ST;
+      const int cc = (q % (CT / 2)) * 2;
+      const int row = (opnd ? J0 : I0) + r;
+      const bool ok = (k + kk < kb1) && (c0 + cc < N) && (row < NI);
+      const float2 *src = ok ? spec + (((size_t)f * nblk + (k + kk)) * NI + row) * N + c0 + cc : spec;
+      float2 *dst = (opnd ? sJ : sI) + buf * STAGE + (kk * ST + r) * CT + cc;
+      cp_async16(dst, src, ok ? 16 : 0);
+    }
+    cp_async_commit();
+  };
 
   float ar[T][T], ai[T][T];
 #pragma unroll
@@ -54,30 +87,29 @@ xmac_fp32_kernel(const float2 *__restrict__ spec, int nblk, int NI, int N, int n
 #pragma unroll
     for (int b = 0; b < T; b++) { ar[a][b] = 0.f; ai[a][b] = 0.f; }
 
-  const bool compute = (SI < SJ) || (ti <= tj);   // lower tiles of diagonal super-tiles are redundant
+  const bool compute = !diag || (ti <= tj);   // lower tiles of diagonal super-tiles are redundant
 
-  for (int k = kb0; k < kb1; k += KB) {
-    const int kn = min(KB, kb1 - k);
-    // stage rows [I0, I0+ST) and [J0, J0+ST) x channels [c0, c0+CT) of kn blocks
-    for (int e = tid; e < KB * ST * CT; e += NTHREADS) {
-      const int kk = e / (ST * CT);
-      const int r = (e / CT) % ST;
-      const int cc = e % CT;
-      float2 vi = make_float2(0.f, 0.f), vj = make_float2(0.f, 0.f);
-      if (kk < kn && c0 + cc < N) {
-        const size_t rowbase = ((size_t)f * nblk + (k + kk)) * NI;
-        if (I0 + r < NI) vi = spec[(rowbase + I0 + r) * N + c0 + cc];
-        if (J0 + r < NI) vj = spec[(rowbase + J0 + r) * N + c0 + cc];
-      }
-      sI[kk][r][cc] = vi;
-      sJ[kk][r][cc] = vj;
+  if (nstages > 0) load_stage(0, 0);
+  for (int st = 0; st < nstages; st++) {
+    const int buf = st & 1;
+    if (st + 1 < nstages) {
+      load_stage(st + 1, buf ^ 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
     __syncthreads();
     if (compute) {
-      for (int kk = 0; kk < kn; kk++) {
+      const float2 *bi_ = sI + buf * STAGE;
+      const float2 *bj_ = sJread + buf * STAGE;
+#pragma unroll 2
+      for (int kk = 0; kk < KB; kk++) {
         float2 xi[T], xj[T];
 #pragma unroll
-        for (int r = 0; r < T; r++) { xi[r] = sI[kk][ti * T + r][c]; xj[r] = sJ[kk][tj * T + r][c]; }
+        for (int r = 0; r < T; r++) {
+          xi[r] = bi_[(kk * ST + ti * T + r) * CT + c];
+          xj[r] = bj_[(kk * ST + tj * T + r) * CT + c];
+        }
 #pragma unroll
         for (int a = 0; a < T; a++)
 #pragma unroll
@@ -93,7 +125,8 @@ xmac_fp32_kernel(const float2 *__restrict__ spec, int nblk, int NI, int N, int n
     __syncthreads();
   }
   if (!compute || c0 + c >= N) return;
-  const size_t base = (((size_t)ks * gridDim.z / ks_count + f) * gridDim.y + stp) * (size_t)ST * ST;
+  const int nfreqs = gridDim.z / ks_count;
+  const size_t base = (((size_t)ks * nfreqs + f) * gridDim.y + stp) * (size_t)ST * ST;
 #pragma unroll
   for (int a = 0; a < T; a++)
 #pragma unroll
@@ -166,8 +199,16 @@ static cudaError_t launch_t(const float2 *spec, int nblk, int NI, int N, int nfr
 {
   const int nsuper = (NI + ST - 1) / ST;
   const int npairs = nsuper * (nsuper + 1) / 2;
+  const size_t sm = sizeof(float2) * 4 * KB * ST * CT;
+  static size_t have = 48 * 1024;
+  if (sm > have) {
+    cudaError_t e = cudaFuncSetAttribute(xmac_fp32_kernel<T, ST, CT, KB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    have = sm;
+  }
   dim3 grid((N + CT - 1) / CT, npairs, nfreqs * ks);
-  xmac_fp32_kernel<T, ST, CT, KB><<<grid, CT *(ST / T) * (ST / T), 0, st>>>(spec, nblk, NI, N, nsuper, ks, acc);
+  xmac_fp32_kernel<T, ST, CT, KB><<<grid, CT *(ST / T) * (ST / T), sm, st>>>(spec, nblk, NI, N, nsuper, ks, acc);
   return cudaGetLastError();
 }
 

@@ -31,7 +31,8 @@ XmacShape xmac_shape(int NI);
 
 size_t fstep_smem_bytes(const DevJob &J, int nrf, int nslots);
 cudaError_t fstep_launch(const DevJob &J, const DevStation *stations, int maxnrf, const SubintArrays &S,
-                         int blk0, int nblk, int nslots, float2 *spec, float *weights, cudaStream_t st);
+                         int blk0, int nblk, int nslots, float2 *spec, float *weights, BlockParam *bp,
+                         cudaStream_t st);
 cudaError_t xmac_fp32_launch(const float2 *spec, int nblk, int NI, int N, int nfreqs, int ks, float2 *acc,
                              cudaStream_t st);
 cudaError_t weights_launch(const float *w, int nblk, int nstations, const int2 *pairs, int npairs, float *wacc,
