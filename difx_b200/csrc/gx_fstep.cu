@@ -289,56 +289,71 @@ __device__ __forceinline__ float2 select_channel(const DevJob &J, const float2 *
 }
 
 // --------------------------------------------------------------------------
-// One compile-time Stockham pass (FL points, stride NS, radix R) over one
-// warp's buffer; every index is a shift or mask.
+// Warp-private FFT buffers are padded by one element every eight so that the
+// strided Stockham stores spread over the shared-memory banks.
+__device__ __forceinline__ int pidx(int i) { return i + (i >> 3); }
+
+// One compile-time Stockham pass (FL points, stride NS, radix R), in place in
+// one warp's buffer: every lane loads all of its butterflies' inputs, the warp
+// synchronises, then every lane stores its outputs.  Indices are shifts/masks.
 template <int FL, int NS, int R>
-__device__ __forceinline__ void warp_pass(const float2 *in, float2 *out, const float2 *__restrict__ tw, int lane)
+__device__ __forceinline__ void warp_pass(float2 *buf, const float2 *tw, int lane)
 {
   constexpr int NB = FL / R;
+  constexpr int PER = (NB + 31) / 32;
   constexpr int TWSTEP = FL / (NS * R);
+  float2 v[PER][R];
 #pragma unroll
-  for (int j0 = 0; j0 < NB; j0 += 32) {
-    const int j = j0 + lane;
-    if (NB % 32 != 0 && j >= NB) break;
-    float2 v[R];
-    const int k = j & (NS - 1);
+  for (int p = 0; p < PER; p++) {
+    const int j = lane + 32 * p;
+    if (NB % 32 == 0 || j < NB) {
+      const int k = j & (NS - 1);
 #pragma unroll
-    for (int r = 0; r < R; r++) {
-      float2 x = in[j + r * NB];
-      if (r > 0 && NS > 1) x = cmul(x, __ldg(&tw[r * k * TWSTEP]));
-      v[r] = x;
+      for (int r = 0; r < R; r++) {
+        float2 x = buf[pidx(j + r * NB)];
+        if (r > 0 && NS > 1) x = cmul(x, tw[r * k * TWSTEP]);
+        v[p][r] = x;
+      }
+      if (R == 8) dft8(v[p]);
+      else if (R == 4) dft4(v[p][0], v[p][1], v[p][2], v[p][3]);
+      else {
+        float2 t = v[p][0];
+        v[p][0] = cadd(t, v[p][1]);
+        v[p][1] = csub(t, v[p][1]);
+      }
     }
-    if (R == 8) dft8(v);
-    else if (R == 4) dft4(v[0], v[1], v[2], v[3]);
-    else {
-      float2 t = v[0];
-      v[0] = cadd(t, v[1]);
-      v[1] = csub(t, v[1]);
-    }
-    const int idxD = (j - k) * R + k;   // (j / NS) * NS * R + k
-#pragma unroll
-    for (int r = 0; r < R; r++) out[idxD + r * NS] = v[r];
   }
+  __syncwarp();
+#pragma unroll
+  for (int p = 0; p < PER; p++) {
+    const int j = lane + 32 * p;
+    if (NB % 32 == 0 || j < NB) {
+      const int k = j & (NS - 1);
+      const int idxD = (j - k) * R + k;   // (j / NS) * NS * R + k
+#pragma unroll
+      for (int r = 0; r < R; r++) buf[pidx(idxD + r * NS)] = v[p][r];
+    }
+  }
+  __syncwarp();
 }
 
-// All passes of an FL-point forward FFT: radix 8 while it fits, then 4 or 2.
+// All passes of an FL-point forward FFT in place: radix 8 while it fits, then 4 or 2.
 template <int FL, int NS>
-__device__ __forceinline__ float2 *warp_fft(float2 *in, float2 *out, const float2 *__restrict__ tw, int lane)
+__device__ __forceinline__ void warp_fft(float2 *buf, const float2 *tw, int lane)
 {
-  if constexpr (NS >= FL) {
-    return in;
-  } else {
+  if constexpr (NS < FL) {
     constexpr int R = (NS * 8 <= FL) ? 8 : ((NS * 4 <= FL) ? 4 : 2);
-    warp_pass<FL, NS, R>(in, out, tw, lane);
-    __syncwarp();
-    return warp_fft<FL, NS * R>(out, in, tw, lane);
+    warp_pass<FL, NS, R>(buf, tw, lane);
+    warp_fft<FL, NS * R>(buf, tw, lane);
   }
 }
 
 // Warp-per-(block, band) F-step for FFT lengths up to 1024 (FL points,
 // complex sampling CPLX).
+constexpr int kWarpKernelThreads = 128;
+
 template <int FL, int CPLX>
-__global__ void __launch_bounds__(kFThreads)
+__global__ void __launch_bounds__(kWarpKernelThreads)
 fstep_warp_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays S,
                   const BlockParam *__restrict__ bp, int nblk, int blocks_per_cta, int wstride,
                   float2 *__restrict__ spec)
@@ -346,16 +361,17 @@ fstep_warp_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArray
   constexpr int NCH = CPLX ? FL : FL / 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ float s_lut[256];
+  __shared__ float2 s_tw[FL];
   const int s = blockIdx.y;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
   const DevStation &st = stations[s];
   const int Sd = J.stride, lgS = J.lgstride, nfr = J.nfr, half = J.half;
   for (int i = tid; i < 256; i += blockDim.x) s_lut[i] = J.lut[i];
+  for (int i = tid; i < FL; i += blockDim.x) s_tw[i] = J.twiddle[i];
   __syncthreads();
 
-  float2 *A = reinterpret_cast<float2 *>(smem_raw) + (size_t)warp * wstride;
-  float2 *B = A + FL;
-  float2 *rs = B + FL;         // S
+  float2 *A = reinterpret_cast<float2 *>(smem_raw) + (size_t)warp * wstride;   // FL + FL/8 (padded)
+  float2 *rs = A + FL + FL / 8;   // S
   float2 *rp = rs + Sd;        // nfr
   float2 *fs = rp + nfr;       // S
   float2 *fp = fs + Sd;        // half
@@ -403,30 +419,30 @@ fstep_warp_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArray
         float2 u = make_float2(0.f, 0.f);
         if ((P.validmask >> q) & 1ull) {
           const uint8_t *payload = data + ((long long)P.fr0 + q) * J.framebytes + 32;
-          const long long bit0 = (long long)r * bits_ts + bitband;
+          const int bit0 = r * bits_ts + bitband;   // < 8 * payload bytes
           u.x = s_lut[(__ldg(payload + (bit0 >> 3)) >> (bit0 & 7)) & cmask];
           if (CPLX) {
-            const long long bit1 = bit0 + J.nbits;
+            const int bit1 = bit0 + J.nbits;
             u.y = s_lut[(__ldg(payload + (bit1 >> 3)) >> (bit1 & 7)) & cmask];
           }
         }
         const int k = n & (Sd - 1), j = n >> lgS;
         const float2 rot = (j == 0) ? rs[k] : cmul_exact(rs[k], rp[j]);
-        A[n] = CPLX ? cmul(rot, u) : make_float2(u.x * rot.x, u.x * rot.y);
+        A[pidx(n)] = CPLX ? cmul(rot, u) : make_float2(u.x * rot.x, u.x * rot.y);
         r += 32;
         while (r >= fsamp) { r -= fsamp; q++; }
       }
     }
     __syncwarp();
-    const float2 *res = warp_fft<FL, 1>(A, B, J.twiddle, lane);
+    warp_fft<FL, 1>(A, s_tw, lane);
     const int lsb = st.lsb[lf];
 #pragma unroll 4
     for (int c = lane; c < NCH; c += 32) {
       float2 v;
-      if (!CPLX) v = res[lsb ? NCH + c : c];
-      else if (!lsb) v = res[c];
-      else if (c == 0) v = res[0];
-      else { v = res[FL - c]; v.y = -v.y; }
+      if (!CPLX) v = A[pidx(lsb ? NCH + c : c)];
+      else if (!lsb) v = A[pidx(c)];
+      else if (c == 0) v = A[0];
+      else { v = A[pidx(FL - c)]; v.y = -v.y; }
       dst[c] = cmul(v, cmul_exact(fs[c & (Sd - 1)], fp[c >> lgS]));
     }
     __syncwarp();
@@ -542,13 +558,13 @@ static bool use_warp_kernel(const DevJob &J) { return J.fftlen >= 128 && J.fftle
 
 static int warp_stride(const DevJob &J)
 {
-  int w = 2 * J.fftlen + 2 * J.stride + J.nfr + (J.half > 0 ? J.half : 1);
+  int w = J.fftlen + J.fftlen / 8 + 2 * J.stride + J.nfr + (J.half > 0 ? J.half : 1);
   return (w + 1) & ~1;   // keep each warp's region 16-byte aligned
 }
 
 size_t fstep_smem_bytes(const DevJob &J, int nrf, int nslots)
 {
-  if (use_warp_kernel(J)) return (size_t)(kFThreads / 32) * warp_stride(J) * sizeof(float2);
+  if (use_warp_kernel(J)) return (size_t)(kWarpKernelThreads / 32) * warp_stride(J) * sizeof(float2);
   size_t b = (size_t)nslots * 2 * J.fftlen * sizeof(float2);
   b += (size_t)nrf * (J.stride + J.nfr) * sizeof(float2);
   b += (size_t)2 * nrf * (J.stride + (J.half > 0 ? J.half : 1)) * sizeof(float2);
@@ -575,7 +591,7 @@ cudaError_t fstep_launch(const DevJob &J, const DevStation *stations, int maxnrf
   const size_t sm = fstep_smem_bytes(J, maxnrf, nslots);
   if (use_warp_kernel(J)) {
     // enough items per CTA that each warp has several (block, band) items
-    const int bpc = (J.nbands >= 8) ? 4 : 16;
+    const int bpc = (J.nbands >= 8) ? 2 : 8;
     dim3 grid((nblk + bpc - 1) / bpc, J.nstations);
     const int ws = warp_stride(J);
 #define GX_WARP_CASE(FLV, CX)                                                                         \
@@ -583,7 +599,7 @@ cudaError_t fstep_launch(const DevJob &J, const DevStation *stations, int maxnrf
       static size_t have = 48 * 1024;                                                                 \
       cudaError_t e = opt_in(fstep_warp_kernel<FLV, CX>, sm, have);                                   \
       if (e != cudaSuccess) return e;                                                                 \
-      fstep_warp_kernel<FLV, CX><<<grid, kFThreads, sm, st>>>(J, stations, S, bp, nblk, bpc, ws, spec); \
+      fstep_warp_kernel<FLV, CX><<<grid, kWarpKernelThreads, sm, st>>>(J, stations, S, bp, nblk, bpc, ws, spec); \
       return cudaGetLastError();                                                                      \
     }
     GX_WARP_CASE(128, 0) GX_WARP_CASE(256, 0) GX_WARP_CASE(512, 0) GX_WARP_CASE(1024, 0)

@@ -30,7 +30,7 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-template <int T, int ST, int CT, int KB>
+template <int T, int ST, int CT, int KB, int NSTAGE>
 __global__ void __launch_bounds__(CT *(ST / T) * (ST / T))
 xmac_fp32_kernel(const float2 *__restrict__ spec, int nblk, int NI, int N, int nsuper,
                  int ks_count, float2 *__restrict__ acc)
@@ -39,8 +39,8 @@ xmac_fp32_kernel(const float2 *__restrict__ spec, int nblk, int NI, int N, int n
   constexpr int NTHREADS = CT * NT * NT;
   constexpr int STAGE = KB * ST * CT;   // float2 per stage per operand
   extern __shared__ __align__(16) float2 xsm[];
-  float2 *sI = xsm;                     // [2][KB][ST][CT]
-  float2 *sJ = xsm + 2 * STAGE;         // [2][KB][ST][CT]
+  float2 *sI = xsm;                     // [NSTAGE][KB][ST][CT]
+  float2 *sJ = xsm + NSTAGE * STAGE;    // [NSTAGE][KB][ST][CT]
 
   const int tid = threadIdx.x;
   const int c = tid % CT;
@@ -89,15 +89,17 @@ xmac_fp32_kernel(const float2 *__restrict__ spec, int nblk, int NI, int N, int n
 
   const bool compute = !diag || (ti <= tj);   // lower tiles of diagonal super-tiles are redundant
 
-  if (nstages > 0) load_stage(0, 0);
+  // NSTAGE-deep cp.async pipeline (one commit group per stage, empty groups at the tail)
+#pragma unroll
+  for (int s0 = 0; s0 < NSTAGE - 1; s0++) {
+    if (s0 < nstages) load_stage(s0, s0);
+    else cp_async_commit();
+  }
   for (int st = 0; st < nstages; st++) {
-    const int buf = st & 1;
-    if (st + 1 < nstages) {
-      load_stage(st + 1, buf ^ 1);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
+    const int buf = st % NSTAGE;
+    if (st + NSTAGE - 1 < nstages) load_stage(st + NSTAGE - 1, (st + NSTAGE - 1) % NSTAGE);
+    else cp_async_commit();
+    cp_async_wait<NSTAGE - 1>();
     __syncthreads();
     if (compute) {
       const float2 *bi_ = sI + buf * STAGE;
@@ -193,22 +195,23 @@ __global__ void finalise_weights_kernel(const WeightEntry *__restrict__ we, int 
 
 // ------------------------------------------------------------------ launchers
 
-template <int T, int ST, int CT, int KB>
+template <int T, int ST, int CT, int KB, int NSTAGE>
 static cudaError_t launch_t(const float2 *spec, int nblk, int NI, int N, int nfreqs, int ks, float2 *acc,
                             cudaStream_t st)
 {
   const int nsuper = (NI + ST - 1) / ST;
   const int npairs = nsuper * (nsuper + 1) / 2;
-  const size_t sm = sizeof(float2) * 4 * KB * ST * CT;
+  const size_t sm = sizeof(float2) * 2 * NSTAGE * KB * ST * CT;
   static size_t have = 48 * 1024;
   if (sm > have) {
-    cudaError_t e = cudaFuncSetAttribute(xmac_fp32_kernel<T, ST, CT, KB>,
+    cudaError_t e = cudaFuncSetAttribute(xmac_fp32_kernel<T, ST, CT, KB, NSTAGE>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     have = sm;
   }
   dim3 grid((N + CT - 1) / CT, npairs, nfreqs * ks);
-  xmac_fp32_kernel<T, ST, CT, KB><<<grid, CT *(ST / T) * (ST / T), sm, st>>>(spec, nblk, NI, N, nsuper, ks, acc);
+  xmac_fp32_kernel<T, ST, CT, KB, NSTAGE>
+      <<<grid, CT *(ST / T) * (ST / T), sm, st>>>(spec, nblk, NI, N, nsuper, ks, acc);
   return cudaGetLastError();
 }
 
@@ -227,9 +230,9 @@ cudaError_t xmac_fp32_launch(const float2 *spec, int nblk, int NI, int N, int nf
                              cudaStream_t st)
 {
   XmacShape s = xmac_shape(NI);
-  if (s.ST == 8) return launch_t<4, 8, 32, 8>(spec, nblk, NI, N, nfreqs, ks, acc, st);
-  if (s.ST == 16) return launch_t<4, 16, 16, 8>(spec, nblk, NI, N, nfreqs, ks, acc, st);
-  return launch_t<8, 32, 16, 4>(spec, nblk, NI, N, nfreqs, ks, acc, st);
+  if (s.ST == 8) return launch_t<4, 8, 32, 8, 3>(spec, nblk, NI, N, nfreqs, ks, acc, st);
+  if (s.ST == 16) return launch_t<4, 16, 16, 8, 3>(spec, nblk, NI, N, nfreqs, ks, acc, st);
+  return launch_t<8, 32, 16, 8, 3>(spec, nblk, NI, N, nfreqs, ks, acc, st);
 }
 
 cudaError_t weights_launch(const float *w, int nblk, int nstations, const int2 *pairs, int npairs, float *wacc,
