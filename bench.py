@@ -1,20 +1,29 @@
 #!/usr/bin/env python
-"""Benchmark: Gsamp/s correlated through the FX hot path.
+"""Benchmark: Gsamp/s correlated through the FX hot path, tensor-core X-step
+against the FP32 plain X-step.
 
-Workload (default): 16 stations; 2-bit real VDIF at 2 Gbps/station
-(2 pol x 8 subbands x 32 MHz, 16 bands); 256 channels per subband (512-point
-FFTs); 1% seeded invalid frames per station; seeded quadratic delay models
-(|tau| <= 20 ms, rates <= 3 us/s); fringe rotation order 1; all four polarisation
-products on all 120 baselines plus autocorrelations.  One step = one 0.2 s
-subint (25 000 FFT blocks per station, 3.28 Gsamples = station x band time
-samples).  The input (0.8 GB of VDIF per step) is larger than L2, so no L2
-flush is needed between steps.
+Workloads (--config):
+  c3 (default)  64 stations x 2 pol; 8-bit complex VDIF (sigma = 16 counts,
+                rho = 0.01 common component); 4 subbands x 64 MHz; 4096
+                channels per subband (4096-point complex FFTs); 1% seeded
+                invalid frames; seeded quadratic delay models (|tau| <= 20 ms,
+                rates <= 3 us/s); all four polarisation products on all 2016
+                baselines plus autocorrelations.  One step = one 128 ms subint
+                (2000 FFT blocks per station, 4.19 Gsamples = station x band
+                complex time samples, 8.4 GB of VDIF).
+  c2            16 stations; 2-bit real VDIF at 2 Gbps/station (2 pol x 8
+                subbands x 32 MHz); 256 channels; 1% invalid frames; one step =
+                one 200 ms subint (3.28 Gsamples).
+Inputs are larger than L2, so no L2 flush is needed between steps.
 
 Arms:
-  default            gxcorr: value = device-resident gx_subint_device steps timed
+  default            gxcorr with the X-step of --xstep (c3: split-FP16 tensor
+                     cores, the form that keeps every visibility within 1e-3 of
+                     FP64).  value = device-resident gx_subint_device steps timed
                      with CUDA events; e2e = gx_subint with pinned host buffers
                      (H2D of the raw VDIF and D2H of the result array inside the
-                     timed region).
+                     timed region).  On c3 the FP32 plain and single-FP16 X-steps
+                     are timed in the same run ("compare").
   --impl reference   the reference correlator's own CPU path (oracle/_ref, compiled
                      from its sources: Configuration/Mode/Core::processdata) on
                      every host core, on a bounded sample of the same workload.
@@ -26,7 +35,6 @@ samples / max-over-ranks time (weak scaling).
 from __future__ import annotations
 
 import argparse
-import ctypes as C
 import json
 import os
 import statistics
@@ -46,9 +54,20 @@ from difx_b200.jobfiles import JobSpec, Subband, write_job  # noqa: E402
 
 METRIC = "Gsamp/s correlated"
 UNIT = "Gsamp/s"
+XSTEPS = {"fp32": capi.GX_XSTEP_FP32, "tc": capi.GX_XSTEP_TC_FP16, "tc_hilo": capi.GX_XSTEP_TC_FP16_HILO}
+DEFAULT_SUBINT_MS = {"c3": 128.0, "c2": 200.0, "c1": 200.0}
+DEFAULT_XSTEP = {"c3": "tc_hilo", "c2": "fp32", "c1": "fp32"}
+RHO = {"c3": 0.01, "c2": 0.02, "c1": 0.05}
 
 
-def workload_spec(name="c2", subint_ns=200_000_000, threads=1) -> JobSpec:
+def workload_spec(name="c3", subint_ns=None) -> JobSpec:
+    if subint_ns is None:
+        subint_ns = int(round(DEFAULT_SUBINT_MS[name] * 1e6))
+    if name == "c3":
+        return JobSpec(name=f"bench_{name}", nstations=64,
+                       subbands=[Subband(6000.0 + 64 * i, 64.0, "U", 4096) for i in range(4)],
+                       nbits=8, sampling="COMPLEX", payload_bytes=8000, subint_ns=subint_ns, execute_seconds=20,
+                       int_time=1.0, max_delay_us=20000.0, max_rate_us_per_s=3.0, seed=2027)
     if name == "c2":
         return JobSpec(name=f"bench_{name}", nstations=16,
                        subbands=[Subband(8200.0 + 32 * i, 32.0, "U", 256) for i in range(8)],
@@ -130,19 +149,23 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# subint of the bounded CPU sample per workload (whole FFT blocks)
+REF_SAMPLE_NS = {"c3": 2_048_000, "c2": 4_000_000, "c1": 8_000_000}
+
+
 def reference_rate(spec_name: str, target_s: float = 15.0, max_subints: int = 50):
     """The reference's own CPU path on every host core over a bounded sample."""
     from oracle import pyoracle
     if not pyoracle.reference_available():
         return None, "reference harness not built (oracle/_ref/libdifxref.so)"
     ncores = os.cpu_count() or 1
-    spec = workload_spec(spec_name, subint_ns=4_000_000 if spec_name == "c2" else 8_000_000)
+    spec = workload_spec(spec_name, subint_ns=REF_SAMPLE_NS[spec_name])
     d = tempfile.mkdtemp(prefix="gxref_")
     paths = write_job(spec, d)
     with open(paths["threads"], "w") as f:
         f.write(f"{'NUMBER OF CORES:':<20}1\n{ncores}\n")
     ref = pyoracle.Reference(paths["input"])
-    si = build_input(spec, 100_000_000, tile_ms=2.0)
+    si = build_input(spec, 100_000_000, rho=RHO[spec_name], tile_ms=2.0)
     ref.process(si)  # warm-up
     t0 = time.perf_counter()
     n = 0
@@ -174,7 +197,7 @@ def run_reference_arm(args):
         return 0
     v = statistics.median(steps)
     base["value"] = v
-    spec = workload_spec(args.config)
+    spec = workload_spec(args.config, subint_ns=int(round(args.subint_ms * 1e6)))
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": samples_per_subint(spec) / (v * 1e9) * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -186,7 +209,8 @@ def run_reference_arm(args):
 
 
 def config_dict(spec: JobSpec, args):
-    return {"workload": f"{args.config.upper()}: {spec.nstations} stations, {spec.nbits}-bit real VDIF, "
+    kind = f"{spec.nbits}-bit {'complex' if spec.is_complex else 'real'} VDIF"
+    return {"workload": f"{args.config.upper()}: {spec.nstations} stations, {kind}, "
                         f"{len(spec.subbands)} subbands x {len(spec.pols)} pol x {spec.bw_mhz:g} MHz, "
                         f"{spec.nchan} ch/subband, 1% invalid frames, {spec.subint_ns / 1e6:g} ms subints",
             "stations": spec.nstations, "bands_per_station": spec.nbands, "nchan": spec.nchan,
@@ -195,18 +219,103 @@ def config_dict(spec: JobSpec, args):
             "l2": "inputs larger than L2 (no flush)", "parallelism": f"subint-parallel x{args.gpus}"}
 
 
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def x_flops(spec: JobSpec) -> float:
+    """Hermitian-unique X-step flops of one subint: 8 x NI (NI + 1) / 2 x nchan x blocks per subband."""
+    ni = spec.nstations * len(spec.pols)
+    return 8.0 * ni * (ni + 1) / 2 * spec.nchan * spec.blocks_per_send * len(spec.subbands)
+
+
+def time_device(corr, sd_dev, dres, stream, steps, warmup, local, dist=None, clocks=False):
+    """Device-resident steps on one stream: (ms for all steps, stage ms of the last step, launches, clocks)."""
+    import torch
+    sptr = stream.cuda_stream
+    for _ in range(warmup):
+        corr.subint_device(sd_dev, dres.data_ptr(), sptr)
+    corr.synchronize()
+    stream.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches = 0
+    clk = ClockSampler(local) if clocks else None
+    if clk:
+        clk.__enter__()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        corr.subint_device(sd_dev, dres.data_ptr(), sptr)
+        launches += corr.launch_count()
+    ev1.record(stream)
+    ev1.synchronize()
+    if clk:
+        clk.__exit__()
+    corr.synchronize()
+    dev_ms = ev0.elapsed_time(ev1)
+    stage = corr.stage_times()
+    torch.cuda.synchronize()
+    return dev_ms, stage, launches, (clk.summary() if clk else None)
+
+
+def roofline(spec: JobSpec, xstep: str, stage, peaks):
+    f_ms, x_ms, fin_ms = float(stage[0]), float(stage[1]), float(stage[2])
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    src = "of measured" if "hbm_gbs" in peaks else "of fallback"
+    nblk = spec.blocks_per_send
+    in_bytes = nblk * spec.nstations * spec.fftchannels * (spec.bits_per_timesample // 8)
+    spec_bytes = nblk * spec.nstations * spec.nbands * spec.nchan * 8
+    stages = {"F": f_ms, "X": x_ms, "finalise": fin_ms}
+    if f_ms >= x_ms:
+        k = "fstep_cta_kernel" if spec.fftchannels > 1024 else "fstep_warp_kernel"
+        a = (in_bytes + spec_bytes) / (f_ms * 1e-3) / 1e9
+        return {"kernel": k, "bound": "hbm", "achieved": a, "peak": hbm_peak, "unit": "GB/s", "frac": a / hbm_peak,
+                "traffic": None, "peak_source": src, "algorithmic_bytes_per_step": in_bytes + spec_bytes,
+                "stage_ms": stages}
+    if xstep == "fp32":
+        a = x_flops(spec) / (x_ms * 1e-3) / 1e12
+        p = 148 * 128 * 2 * (peaks.get("sm_max_mhz", 1965.0) * 1e6) / 1e12
+        return {"kernel": "xmac_fp32_kernel", "bound": "fp32-core", "achieved": a, "peak": p, "unit": "TFLOP/s",
+                "frac": a / p, "traffic": None,
+                "peak_source": "nominal FP32 CUDA-core peak (148 SM x 128 FMA/clk x max SM clock)",
+                "stage_ms": stages}
+    # tensor-core X-step: HBM-bound on the FP32 spectra it reads; tensor pipe reported beside
+    a = spec_bytes / (x_ms * 1e-3) / 1e9
+    nprod = 9 if xstep == "tc_hilo" else 3          # 128x128 real products per channel and block
+    tflops = nprod * 2 * 128 * 128 * spec.nchan * nblk * len(spec.subbands) / (x_ms * 1e-3) / 1e12
+    tpk = peaks.get("bf16_tflops", 1590.0)
+    return {"kernel": "xmac_tc_kernel", "bound": "hbm", "achieved": a, "peak": hbm_peak, "unit": "GB/s",
+            "frac": a / hbm_peak, "traffic": None, "peak_source": src, "algorithmic_bytes_per_step": spec_bytes,
+            "tensor": {"executed_tflops": tflops, "peak": tpk, "frac": tflops / tpk,
+                       "useful_tflops": x_flops(spec) / (x_ms * 1e-3) / 1e12,
+                       "peak_source": "measured dense bf16 (FP16 runs at the same rate)"},
+            "stage_ms": stages}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gxcorr", choices=["gxcorr", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c2", "c1"])
-    ap.add_argument("--xstep", default="fp32", choices=["fp32", "tc"])
+    ap.add_argument("--config", default="c3", choices=["c3", "c2", "c1"])
+    ap.add_argument("--xstep", default=None, choices=sorted(XSTEPS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--subint-ms", type=float, default=200.0,
-                    help="subint length (default 200 ms); smaller values give small profiling cases")
+    ap.add_argument("--no-compare", action="store_true", help="skip the other X-step forms")
+    ap.add_argument("--subint-ms", type=float, default=None,
+                    help="subint length; smaller values give small profiling cases")
     args = ap.parse_args()
+    if args.xstep is None:
+        args.xstep = DEFAULT_XSTEP[args.config]
+    if args.subint_ms is None:
+        args.subint_ms = DEFAULT_SUBINT_MS[args.config]
     if args.impl == "reference":
         return run_reference_arm(args)
 
@@ -224,55 +333,56 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
 
     spec = workload_spec(args.config, subint_ns=int(round(args.subint_ms * 1e6)))
-    xstep = capi.GX_XSTEP_FP32 if args.xstep == "fp32" else capi.GX_XSTEP_TC_FP16
     d = tempfile.mkdtemp(prefix=f"gxbench{rank}_")
     paths = write_job(spec, d)
     # each rank correlates its own subint of the job
     t_sub = 200_000_000 + rank * spec.subint_ns
-    si = build_input(spec, t_sub)
-    jd = capi.job_desc_from_spec(spec, xstep=xstep, max_data_bytes=max(len(x) for x in si.data))
-    corr = Correlator.from_desc(jd, device=local)
+    si = build_input(spec, t_sub, rho=RHO[args.config])
     model = Correlator.from_input(paths["input"], device=-1)
     interp = np.array([model.interpolator(s, 0, si.sec, si.ns) for s in range(spec.nstations)])
     model.close()
+    maxbytes = max(len(x) for x in si.data)
 
     # device-resident inputs
     dev = [torch.from_numpy(x).to(f"cuda:{local}") for x in si.data]
-    dres = torch.zeros(2 * corr.result_length, dtype=torch.float32, device=f"cuda:{local}")
     sd_dev = capi.SubintDesc(si.scan, si.sec, si.ns, 0.0, [t.data_ptr() for t in dev], [len(x) for x in si.data],
                              [x.ctypes.data for x in si.control], len(si.control[0]), interp)
     stream = torch.cuda.Stream(device=local)
-    sptr = stream.cuda_stream
-    torch.cuda.synchronize()
-    for _ in range(args.warmup):
-        corr.subint_device(sd_dev, dres.data_ptr(), sptr)
-    stream.synchronize()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    launches = 0
-    stage = np.zeros(3)
-    with ClockSampler(local) as clk:
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        for _ in range(args.steps):
-            corr.subint_device(sd_dev, dres.data_ptr(), sptr)
-            launches += corr.launch_count()
-        ev1.record(stream)
-        ev1.synchronize()
-        dev_ms = ev0.elapsed_time(ev1)
-        stage = corr.stage_times()     # last step's per-stage device time
-    torch.cuda.synchronize()
+    peaks = load_peaks()
+    samples = samples_per_subint(spec)
+
+    # the other X-step forms first (device-resident timing only), then the headline arm
+    compare = {}
+    if args.config == "c3" and not args.no_compare:
+        for name in sorted(XSTEPS):
+            if name == args.xstep:
+                continue
+            c = Correlator.from_desc(capi.job_desc_from_spec(spec, xstep=XSTEPS[name]), device=local)
+            dres = torch.zeros(2 * c.result_length, dtype=torch.float32, device=f"cuda:{local}")
+            ms, stage, _, _ = time_device(c, sd_dev, dres, stream, max(2, args.steps // 2), 2, local, dist)
+            c.close()
+            del dres
+            compare[name] = {"value": samples * max(2, args.steps // 2) * world / (ms * 1e-3) / 1e9,
+                             "ms_per_step": ms / max(2, args.steps // 2),
+                             "stage_ms": {"F": float(stage[0]), "X": float(stage[1]), "finalise": float(stage[2])}}
+        torch.cuda.empty_cache()
+
+    jd = capi.job_desc_from_spec(spec, xstep=XSTEPS[args.xstep], max_data_bytes=maxbytes)
+    corr = Correlator.from_desc(jd, device=local)
+    dres = torch.zeros(2 * corr.result_length, dtype=torch.float32, device=f"cuda:{local}")
+    dev_ms, stage, launches, clocks = time_device(corr, sd_dev, dres, stream, args.steps, args.warmup, local, dist,
+                                                  clocks=True)
     if dist:
         dist.barrier()
         t = torch.tensor([dev_ms], device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dev_ms = float(t.item())
-    total_samples = samples_per_subint(spec) * args.steps * world
+    total_samples = samples * args.steps * world
     value = total_samples / (dev_ms * 1e-3) / 1e9
 
     # end to end through the public host-buffer entry point, pinned host memory
+    del dev, dres
+    torch.cuda.empty_cache()
     pinned = [torch.from_numpy(x).pin_memory() for x in si.data]
     res_host = torch.zeros(2 * corr.result_length, dtype=torch.float32).pin_memory()
     sd_host = capi.SubintDesc(si.scan, si.sec, si.ns, 0.0, [t.data_ptr() for t in pinned],
@@ -296,48 +406,28 @@ def main():
         e2e_s = float(t.item())
     e2e = total_samples / e2e_s / 1e9
 
-    # roofline of the dominant kernel (from the last device step's stage times)
-    info = corr.info
-    chunks = -(-spec.blocks_per_send // 4096)
-    nblk_total = spec.blocks_per_send
-    f_ms, x_ms = float(stage[0]), float(stage[1])
-    peaks = {}
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            peaks = json.load(f)
-    except Exception:
-        pass
-    hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    in_bytes = nblk_total * spec.nstations * spec.fftchannels * (spec.bits_per_timesample // 8)
-    spec_bytes = nblk_total * spec.nstations * spec.nbands * spec.nchan * 8
-    f_bytes = in_bytes + spec_bytes
-    if f_ms >= x_ms:
-        achieved = f_bytes / (f_ms * 1e-3) / 1e9
-        roof = {"kernel": "fstep_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
-                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None, "peak_source": peak_src,
-                "algorithmic_bytes_per_subint": f_bytes, "stage_ms": {"F": f_ms, "X": x_ms, "finalise": float(stage[2])}}
-    else:
-        ncross = spec.nstations * spec.nbands
-        cmacs = nblk_total * len(spec.subbands) * spec.nchan * (ncross // len(spec.subbands)) * \
-            (ncross // len(spec.subbands) + 1) / 2
-        achieved = 8 * cmacs / (x_ms * 1e-3) / 1e12
-        fp32_peak = 148 * 128 * 2 * (peaks.get("sm_max_mhz", 1965.0) * 1e6) / 1e12
-        roof = {"kernel": "xmac_fp32_kernel", "bound": "fp32-core", "achieved": achieved, "peak": fp32_peak,
-                "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
-                "peak_source": "nominal FP32 CUDA-core peak (148 SM x 128 FMA/clk x 1965 MHz)",
-                "stage_ms": {"F": f_ms, "X": x_ms, "finalise": float(stage[2])}}
-
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded correlated VDIF, 2 ms correlated segment repeated; random-init delay models)",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": {"fp32": "f32", "tc": "f16 operands, f32 accumulation",
+                      "tc_hilo": "f16 hi+lo operands, f32 accumulation"}[args.xstep],
+            "data": "synthetic (seeded correlated VDIF, 2 ms correlated segment repeated; seeded delay models)",
             "config": config_dict(spec, args),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(sum(len(x) for x in si.data)),
                     "d2h_bytes_per_step": int(corr.result_length * 8)},
             "latency_ms": {"p50": statistics.median(lat), "p99": float(np.percentile(lat, 99)),
                            "subint_ms": spec.subint_ns / 1e6},
-            "gpu_launches": int(launches), "roofline": roof, "clocks": clk.summary()}
+            "gpu_launches": int(launches), "roofline": roofline(spec, args.xstep, stage, peaks), "clocks": clocks}
+    if compare:
+        compare[args.xstep] = {"value": value, "ms_per_step": dev_ms / args.steps,
+                               "stage_ms": {"F": float(stage[0]), "X": float(stage[1]), "finalise": float(stage[2])}}
+        fp = compare.get("fp32")
+        if fp:
+            line["tc_vs_fp32"] = {
+                k: {"whole_path": compare[k]["value"] / fp["value"],
+                    "x_step": fp["stage_ms"]["X"] / compare[k]["stage_ms"]["X"]}
+                for k in compare if k != "fp32"}
+        line["compare"] = compare
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base, err = reference_rate(args.config)
         line["cpu_baseline"] = base if base else {"unavailable": err}

@@ -59,8 +59,16 @@ struct gx_handle {
   std::vector<int> blofs, bwofs, acofs, acwofs;
   std::vector<std::vector<int>> band_input;  // [station][band]
   std::vector<ProdEntry> prods;
+  std::vector<TcProdEntry> tcprods;
   std::vector<WeightEntry> wents;
   std::vector<int2> pairs;
+  bool tc = false, hilo = false;   // tensor-core X-step (split FP16 product)
+  float tc_scale0 = 1.0f;          // default power-of-two operand scale
+  float *d_scale = nullptr;        // [freq][128][nchan] operand scales
+  TcProdEntry *d_tcprods = nullptr;
+  int *d_err = nullptr;            // kernel status (bounded waits that expired)
+  int *h_err = nullptr;            // pinned copy of *d_err after each subint
+  cudaStream_t last_stream = nullptr;  // stream of the last gx_subint_device
 
   DevStation *d_st = nullptr;
   float2 *d_tw = nullptr, *d_spec = nullptr, *d_acc = nullptr, *d_results = nullptr, *d_spec1 = nullptr;
@@ -111,9 +119,11 @@ static void free_all(gx_handle *h)
   if (h->device < 0) return;
   void *ptrs[] = {h->d_st, h->d_tw, h->d_spec, h->d_acc, h->d_results, h->d_spec1, h->d_w, h->d_wacc, h->d_w1,
                   h->d_pairs, h->d_prods, h->d_went, (void *)h->d_dataptrs, h->d_datalen, h->d_ctrl, h->d_interp,
-                  h->d_bp, h->d_bp1};
+                  h->d_bp, h->d_bp1, h->d_scale, h->d_tcprods, h->d_err};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  if (h->h_err) cudaFreeHost(h->h_err);
+  h->h_err = nullptr;
   for (auto p : h->d_data)
     if (p) cudaFree(p);
   for (auto e : h->evs) cudaEventDestroy(e);
@@ -183,6 +193,8 @@ static gx_status setup(gx_handle *h)
   if (J.stride & (J.stride - 1)) return h->fail(GX_ERR_UNSUPPORTED, "array stride must be a power of two");
   J.lgstride = 0;
   while ((1 << J.lgstride) < J.stride) J.lgstride++;
+  J.lgcgroup = 0;
+  while ((1 << J.lgcgroup) < J.nchan) J.lgcgroup++;
   J.half = (cplx ? 2 * J.nfr : J.nfr) / 2;
   J.unpacksamples = cplx ? f0.nchan : 2 * f0.nchan;
   J.sampletime = 1.0 / (2.0 * f0.bw_mhz);
@@ -252,8 +264,19 @@ static gx_status setup(gx_handle *h)
   }
   int ni = 0;
   for (int f = 0; f < d.nfreqs; f++) ni = count[f] > ni ? count[f] : ni;
-  h->xs = xmac_shape(ni);
-  J.ninputs = h->xs.nsuper * h->xs.ST;
+  if (d.xstep < GX_XSTEP_FP32 || d.xstep > GX_XSTEP_TC_FP16_HILO) return h->fail(GX_ERR_ARG, "unknown xstep");
+  h->tc = d.xstep != GX_XSTEP_FP32;
+  h->hilo = d.xstep == GX_XSTEP_TC_FP16_HILO;
+  if (h->tc) {
+    if (ni > kTcInputs)
+      return h->fail(GX_ERR_UNSUPPORTED, "the tensor-core X-step takes at most 128 inputs (station bands) per freq");
+    if (J.nchan < 2) return h->fail(GX_ERR_UNSUPPORTED, "the tensor-core X-step needs at least 2 channels");
+    J.ninputs = kTcInputs;   // rows beyond the job's inputs stay zero
+    J.lgcgroup = 1;          // channel pairs interleaved: [chan/2][input][2]
+  } else {
+    h->xs = xmac_shape(ni);
+    J.ninputs = h->xs.nsuper * h->xs.ST;
+  }
   h->xs = xmac_shape(J.ninputs);
   h->dst = dst;
 
@@ -327,8 +350,22 @@ static gx_status setup(gx_handle *h)
            J.nchan;
   };
   h->prods.clear();
+  h->tcprods.clear();
   h->wents.clear();
   h->pairs.clear();
+  // one visibility row: result offset ro <- input pair (a, b) of freq f
+  auto add_prod = [&](long long ro, int f, int a, int b) {
+    ProdEntry e{};
+    e.result_offset = ro;
+    e.acc_index = acc_index(f, a, b, e.conj);
+    h->prods.push_back(e);
+    TcProdEntry t{};
+    t.result_offset = ro;
+    t.freq = f;
+    t.a = a;
+    t.b = b;
+    h->tcprods.push_back(t);
+  };
   for (int j = 0; j < nbl; j++) {
     const gx_baseline_desc &B = d.baselines[j];
     if (B.ds1 < 0 || B.ds1 >= d.nstations || B.ds2 < 0 || B.ds2 >= d.nstations)
@@ -345,10 +382,7 @@ static gx_status setup(gx_handle *h)
         if (b1 < 0 || b1 >= d.stations[B.ds1].nbands || b2 < 0 || b2 >= d.stations[B.ds2].nbands)
           return h->fail(GX_ERR_UNSUPPORTED, "baseline band index out of range (zoom bands are not implemented)");
         int a = h->band_input[B.ds1][b1], bb = h->band_input[B.ds2][b2];
-        ProdEntry e{};
-        e.result_offset = h->blofs[f * nbl + j] + (long long)p * J.nchan;
-        e.acc_index = acc_index(f, a, bb, e.conj);
-        h->prods.push_back(e);
+        add_prod(h->blofs[f * nbl + j] + (long long)p * J.nchan, f, a, bb);
         WeightEntry w{};
         w.float_index = 2LL * h->bwofs[f * nbl + j] + p;
         w.source = d.nstations + j;
@@ -367,10 +401,7 @@ static gx_status setup(gx_handle *h)
     for (int b : used) {
       int f = x.recfreq[x.band_localfreq[b]];
       int a = h->band_input[s][b];
-      ProdEntry e{};
-      e.result_offset = ro;
-      e.acc_index = acc_index(f, a, a, e.conj);
-      h->prods.push_back(e);
+      add_prod(ro, f, a, a);
       ro += J.nchan;
       WeightEntry w{};
       w.float_index = wo++;
@@ -393,12 +424,7 @@ static gx_status setup(gx_handle *h)
         w.float_index = wo++;
         w.source = partner >= 0 ? s : -1;
         h->wents.push_back(w);
-        if (partner >= 0) {
-          ProdEntry e{};
-          e.result_offset = ro;
-          e.acc_index = acc_index(f, h->band_input[s][b], h->band_input[s][partner], e.conj);
-          h->prods.push_back(e);
-        }
+        if (partner >= 0) add_prod(ro, f, h->band_input[s][b], h->band_input[s][partner]);
         ro += J.nchan;
       }
     }
@@ -406,11 +432,33 @@ static gx_status setup(gx_handle *h)
 
   // chunking and K-split
   const size_t per_block = (size_t)d.nfreqs * J.ninputs * J.nchan * sizeof(float2);
-  int chunk = d.block_chunk > 0 ? d.block_chunk : (int)std::min<size_t>(4096, std::max<size_t>(64, (size_t)(2u << 30) / per_block));
+  // The tensor-core X-step moves its accumulators through HBM once per chunk
+  // (128 x 128 x 2 floats per channel), so it gets longer chunks.
+  const size_t spec_budget = h->tc ? (size_t(16) << 30) : (size_t(2) << 30);
+  int chunk = d.block_chunk > 0 ? d.block_chunk
+                                : (int)std::min<size_t>(4096, std::max<size_t>(64, spec_budget / per_block));
   if (chunk > J.blocks_per_send) chunk = J.blocks_per_send;
   chunk = std::max(1, chunk);
+  if (d.block_chunk <= 0) {
+    // equal chunks: no short tail pass
+    const int nch = (J.blocks_per_send + chunk - 1) / chunk;
+    chunk = (J.blocks_per_send + nch - 1) / nch;
+  }
   h->chunk = chunk;
-  {
+  if (h->tc) {
+    // one CTA per SM (all 512 tensor-memory columns); at least 4 K-tiles per slice
+    const long long base = (long long)(J.nchan / 2) * d.nfreqs;
+    const int kmax = std::max(1, std::min(16, chunk / 64));
+    int best = 1;
+    double best_score = -1;
+    for (int ks = 1; ks <= kmax; ks++) {
+      const long long ctas = base * ks;
+      const double waves = std::ceil(ctas / 148.0);
+      const double score = (ctas / (waves * 148.0)) * std::min(1.0, ctas / 148.0);
+      if (score > best_score + 1e-9) { best_score = score; best = ks; }
+    }
+    h->ks = best;
+  } else {
     long long base = (long long)((J.nchan + xs.CT - 1) / xs.CT) * xs.npairs * d.nfreqs;
     // K-split: enough CTAs for at least two per SM, rounded to whole waves of
     // 148 SMs where possible, keeping at least 64 blocks per slice
@@ -448,6 +496,15 @@ static gx_status setup(gx_handle *h)
       double off = getenv("SYMMETRIC_8_BIT_VDIF") ? 127.5 : 128.0;
       for (int b = 0; b < 256; b++) lut[b] = (float)((b - off) / 3.3);
     }
+    // Tensor-core operands: a power-of-two scale that brings the spectrum of
+    // noise with the r.m.s. level of the decode table to an r.m.s. near 8, so
+    // that the FP16 values and their split remainders stay in the normal range.
+    double ms = 0;
+    const int ncode = 1 << J.nbits;
+    for (int l = 0; l < ncode; l++) ms += (double)lut[l] * lut[l];
+    ms /= ncode;
+    const double rms_spec = std::sqrt(ms * J.fftlen * (J.cplx ? 2.0 : 1.0));
+    h->tc_scale0 = (float)std::ldexp(1.0, (int)std::lround(std::log2(8.0 / rms_spec)));
   }
 
   // ---------------------------------------------------------- device state
@@ -475,8 +532,25 @@ static gx_status setup(gx_handle *h)
   CKR(h, cudaMalloc(&h->d_w1, sizeof(float) * (size_t)d.nstations));
   CKR(h, cudaMalloc(&h->d_bp, sizeof(BlockParam) * (size_t)d.nstations * chunk));
   CKR(h, cudaMalloc(&h->d_bp1, sizeof(BlockParam) * (size_t)d.nstations));
-  h->acc_slice = (size_t)d.nfreqs * xs.npairs * xs.ST * xs.ST * J.nchan;
+  if (h->tc) {
+    // Re and P arrays of [freq][chan/2][128][128][2] floats per K-split slice
+    h->acc_slice = (size_t)d.nfreqs * J.nchan * kTcInputs * kTcInputs;
+    const size_t nsc = (size_t)d.nfreqs * kTcInputs * J.nchan;
+    std::vector<float> sc(nsc, h->tc_scale0);
+    CKR(h, cudaMalloc(&h->d_scale, sizeof(float) * nsc));
+    CKR(h, cudaMemcpy(h->d_scale, sc.data(), sizeof(float) * nsc, cudaMemcpyHostToDevice));
+    CKR(h, cudaMalloc(&h->d_tcprods, sizeof(TcProdEntry) * std::max<size_t>(1, h->tcprods.size())));
+    if (!h->tcprods.empty())
+      CKR(h, cudaMemcpy(h->d_tcprods, h->tcprods.data(), sizeof(TcProdEntry) * h->tcprods.size(),
+                        cudaMemcpyHostToDevice));
+  } else {
+    h->acc_slice = (size_t)d.nfreqs * xs.npairs * xs.ST * xs.ST * J.nchan;
+  }
   CKR(h, cudaMalloc(&h->d_acc, sizeof(float2) * h->acc_slice * h->ks));
+  CKR(h, cudaMalloc(&h->d_err, sizeof(int)));
+  CKR(h, cudaMemset(h->d_err, 0, sizeof(int)));
+  CKR(h, cudaMallocHost(&h->h_err, sizeof(int)));
+  *h->h_err = 0;
   CKR(h, cudaMalloc(&h->d_wacc, sizeof(float) * (d.nstations + nbl)));
   if (nbl) {
     CKR(h, cudaMalloc(&h->d_pairs, sizeof(int2) * nbl));
@@ -684,8 +758,12 @@ static gx_status run_device(gx_handle *h, const gx_subint_desc *sub, const uint8
   h->have_last = true;
 
   const int nbl = d.nbaselines;
-  CKR(h, cudaMemsetAsync(h->d_acc, 0, sizeof(float2) * h->acc_slice * h->ks, st));
+  float *acc_re = reinterpret_cast<float *>(h->d_acc);
+  float *acc_p = acc_re + h->acc_slice * h->ks;
+  // the tensor-core X-step stores its first chunk instead of adding to it
+  if (!h->tc) CKR(h, cudaMemsetAsync(h->d_acc, 0, sizeof(float2) * h->acc_slice * h->ks, st));
   CKR(h, cudaMemsetAsync(h->d_wacc, 0, sizeof(float) * (d.nstations + nbl), st));
+  CKR(h, cudaMemsetAsync(h->d_err, 0, sizeof(int), st));
   for (int b0 = 0; b0 < J.blocks_per_send; b0 += h->chunk) {
     const int nb = std::min(h->chunk, J.blocks_per_send - b0);
     gx_status r;
@@ -693,7 +771,11 @@ static gx_status run_device(gx_handle *h, const gx_subint_desc *sub, const uint8
     CKR(h, fstep_launch(J, h->d_st, h->maxnrf, S, b0, nb, h->nslots, h->d_spec, h->d_w, h->d_bp, st));
     if ((r = record(h, st, 0, false)) != GX_OK) return r;
     if ((r = record(h, st, 1, true)) != GX_OK) return r;
-    CKR(h, xmac_fp32_launch(h->d_spec, nb, J.ninputs, J.nchan, d.nfreqs, h->ks, h->d_acc, st));
+    if (h->tc)
+      CKR(h, xmac_tc_launch(h->d_spec, nb, J.nchan, d.nfreqs, h->ks, h->hilo, h->d_scale, acc_re, acc_p,
+                            h->acc_slice, b0 > 0 ? 1 : 0, h->d_err, st));
+    else
+      CKR(h, xmac_fp32_launch(h->d_spec, nb, J.ninputs, J.nchan, d.nfreqs, h->ks, h->d_acc, st));
     CKR(h, weights_launch(h->d_w, nb, d.nstations, h->d_pairs, nbl, h->d_wacc, st));
     if ((r = record(h, st, 1, false)) != GX_OK) return r;
     h->launches += 3;
@@ -701,10 +783,26 @@ static gx_status run_device(gx_handle *h, const gx_subint_desc *sub, const uint8
   gx_status r;
   if ((r = record(h, st, 2, true)) != GX_OK) return r;
   CKR(h, cudaMemsetAsync(dev_results, 0, sizeof(float2) * h->rl, st));
-  CKR(h, finalise_launch(h->d_prods, (int)h->prods.size(), h->d_acc, h->ks, h->acc_slice, J.nchan, h->d_went,
-                         (int)h->wents.size(), h->d_wacc, dev_results, st));
+  if (h->tc) {
+    CKR(h, finalise_tc_launch(h->d_tcprods, (int)h->tcprods.size(), acc_re, acc_p, h->ks, h->acc_slice, J.nchan,
+                              h->d_scale, dev_results, st));
+    CKR(h, finalise_launch(nullptr, 0, h->d_acc, h->ks, h->acc_slice, J.nchan, h->d_went, (int)h->wents.size(),
+                           h->d_wacc, dev_results, st));
+  } else {
+    CKR(h, finalise_launch(h->d_prods, (int)h->prods.size(), h->d_acc, h->ks, h->acc_slice, J.nchan, h->d_went,
+                           (int)h->wents.size(), h->d_wacc, dev_results, st));
+  }
   h->launches += (h->prods.empty() ? 0 : 1) + (h->wents.empty() ? 0 : 1);
   if ((r = record(h, st, 2, false)) != GX_OK) return r;
+  CKR(h, cudaMemcpyAsync(h->h_err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  return GX_OK;
+}
+
+// Status the kernels of the last subint left in *d_err (read after a synchronise).
+static gx_status kernel_status(gx_handle *h)
+{
+  if (h->h_err && *h->h_err != 0)
+    return h->fail(GX_ERR_TIMEOUT, "a tensor-core X-step wait expired (status " + std::to_string(*h->h_err) + ")");
   return GX_OK;
 }
 
@@ -714,6 +812,7 @@ gx_status gx_subint_device(gx_handle *h, const gx_subint_desc *sub, float *dev_r
   if (h->device < 0) return h->fail(GX_ERR_STATE, "host-only handle (opened with device -1)");
   CKR(h, cudaSetDevice(h->device));
   cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+  h->last_stream = st;
   return run_device(h, sub, sub->data, reinterpret_cast<float2 *>(dev_results), st);
 }
 
@@ -740,14 +839,16 @@ gx_status gx_subint(gx_handle *h, const gx_subint_desc *sub, float *results)
   if (r != GX_OK) return r;
   CKR(h, cudaMemcpyAsync(results, h->d_results, sizeof(float2) * h->rl, cudaMemcpyDeviceToHost, h->stream));
   CKR(h, cudaStreamSynchronize(h->stream));
-  return GX_OK;
+  return kernel_status(h);
 }
 
 gx_status gx_synchronize(gx_handle *h)
 {
   if (!h) return GX_ERR_ARG;
+  if (h->device < 0) return GX_OK;
   CKR(h, cudaStreamSynchronize(h->stream));
-  return GX_OK;
+  if (h->last_stream && h->last_stream != h->stream) CKR(h, cudaStreamSynchronize(h->last_stream));
+  return kernel_status(h);
 }
 
 gx_status gx_stage_times(gx_handle *h, float ms[3])
@@ -779,7 +880,10 @@ gx_status gx_spectra(gx_handle *h, int station, int block, float *out, float *we
   if (station < 0 || station >= J.nstations || block < 0 || block >= J.blocks_per_send)
     return h->fail(GX_ERR_ARG, "station or block out of range");
   CKR(h, cudaSetDevice(h->device));
-  CKR(h, fstep_launch(J, h->d_st, h->maxnrf, h->last, block, 1, h->nslots, h->d_spec1, h->d_w1, h->d_bp1,
+  DevJob Jrow = J;   // one contiguous row per (freq, input), whatever layout the X-step reads
+  Jrow.lgcgroup = 0;
+  while ((1 << Jrow.lgcgroup) < J.nchan) Jrow.lgcgroup++;
+  CKR(h, fstep_launch(Jrow, h->d_st, h->maxnrf, h->last, block, 1, h->nslots, h->d_spec1, h->d_w1, h->d_bp1,
                       h->stream));
   const gx_station_desc &x = h->jd.stations[station];
   for (int b = 0; b < x.nbands; b++) {
@@ -828,3 +932,25 @@ gx_status gx_open_input(const char *inputfile, int device, int xstep, gx_handle 
 }
 
 }  // extern "C"
+
+gx_status gx_set_tc_scales(gx_handle *h, int station, int band, const float *scales)
+{
+  if (!h || !scales) return GX_ERR_ARG;
+  if (!h->tc || h->device < 0) return h->fail(GX_ERR_STATE, "handle has no tensor-core X-step on a device");
+  if (station < 0 || station >= h->jd.nstations || band < 0 || band >= h->jd.stations[station].nbands)
+    return h->fail(GX_ERR_ARG, "station or band out of range");
+  const int N = h->J.nchan;
+  std::vector<float> row(N);
+  for (int c = 0; c < N; c++) {
+    const float s = scales[c];
+    if (!(s > 0.0f) || !std::isfinite(s)) return h->fail(GX_ERR_ARG, "scales must be finite and positive");
+    row[c] = (float)std::ldexp(1.0, (int)std::lround(std::log2((double)s)));
+  }
+  const gx_station_desc &x = h->jd.stations[station];
+  const int f = x.recfreq[x.band_localfreq[band]];
+  const size_t off = ((size_t)f * kTcInputs + h->band_input[station][band]) * N;
+  CKR(h, cudaSetDevice(h->device));
+  CKR(h, cudaMemcpyAsync(h->d_scale + off, row.data(), sizeof(float) * N, cudaMemcpyHostToDevice, h->stream));
+  CKR(h, cudaStreamSynchronize(h->stream));
+  return GX_OK;
+}

@@ -1,7 +1,9 @@
 // F-step: VDIF unpack + validity/weights, FP64 per-block delay evaluation,
 // FP32 fringe rotation, shared-memory Stockham FFT, sideband selection and
 // fractional-sample correction, writing spectra in the layout the X-step
-// reads: spec[freq][block][input][channel] (float2).
+// reads: spec[freq][block][...] (float2) with (input, channel) placed by
+// spec_offset — [input][channel] for the FP32 X-step, channel pairs
+// interleaved ([channel/2][input][2]) for the tensor-core X-step.
 //
 // Two kernels per pass of blocks:
 //   blockparams_kernel  one thread per (station, block): FP64 delay, nearest
@@ -389,10 +391,11 @@ fstep_warp_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArray
     const BlockParam P = bp[(size_t)s * nblk + bi];
     const int lf = st.band_localfreq[bd];
     const int f = st.freq_index[lf];
-    float2 *dst = spec + (((size_t)f * nblk + bi) * J.ninputs + st.band_input[bd]) * NCH;
+    float2 *dst = spec + ((size_t)f * nblk + bi) * J.ninputs * NCH;
+    const int row = st.band_input[bd];
     if (P.state == 0) {
 #pragma unroll
-      for (int c = lane; c < NCH; c += 32) dst[c] = make_float2(0.f, 0.f);
+      for (int c = lane; c < NCH; c += 32) dst[spec_offset(J, row, c)] = make_float2(0.f, 0.f);
       continue;
     }
     const int ps = st.band_polb[bd] ? 1 : 0;
@@ -443,7 +446,7 @@ fstep_warp_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArray
       else if (!lsb) v = A[pidx(c)];
       else if (c == 0) v = A[0];
       else { v = A[pidx(FL - c)]; v.y = -v.y; }
-      dst[c] = cmul(v, cmul_exact(fs[c & (Sd - 1)], fp[c >> lgS]));
+      dst[spec_offset(J, row, c)] = cmul(v, cmul_exact(fs[c & (Sd - 1)], fp[c >> lgS]));
     }
     __syncwarp();
   }
@@ -485,8 +488,9 @@ fstep_cta_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays
     if (P.state == 0) {
       for (int bd = 0; bd < J.nbands; bd++) {
         const int f = st.freq_index[st.band_localfreq[bd]];
-        float2 *dst = spec + (((size_t)f * nblk + bi) * J.ninputs + st.band_input[bd]) * N;
-        for (int c = tid; c < N; c += blockDim.x) dst[c] = make_float2(0.f, 0.f);
+        float2 *dst = spec + ((size_t)f * nblk + bi) * J.ninputs * N;
+        const int row = st.band_input[bd];
+        for (int c = tid; c < N; c += blockDim.x) dst[spec_offset(J, row, c)] = make_float2(0.f, 0.f);
       }
       continue;
     }
@@ -542,10 +546,11 @@ fstep_cta_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays
         const int ps = st.band_polb[bd] ? 1 : 0;
         const float2 *fs = fsub + (ps * nrf + lf) * Sd;
         const float2 *fp = fstep + (ps * nrf + lf) * half;
-        float2 *dst = spec + (((size_t)f * nblk + bi) * J.ninputs + st.band_input[bd]) * N;
+        float2 *dst = spec + ((size_t)f * nblk + bi) * J.ninputs * N;
+        const int row = st.band_input[bd];
         for (int c = lt; c < N; c += tps) {
           const float2 v = select_channel(J, in, lsb, c);
-          dst[c] = cmul(v, cmul_exact(fs[c % Sd], fp[c / Sd]));
+          dst[spec_offset(J, row, c)] = cmul(v, cmul_exact(fs[c % Sd], fp[c / Sd]));
         }
       }
       __syncthreads();

@@ -87,6 +87,10 @@ extern "C" gx_status gx_subint_device_noalloc(const gx_job_desc *desc, const gx_
     set_err(err, errlen, "interpolators are required (there is no delay model without a handle)");
     return GX_ERR_ARG;
   }
+  if (desc->xstep != GX_XSTEP_FP32) {
+    set_err(err, errlen, "the no-allocation entry point runs the FP32 X-step only");
+    return GX_ERR_UNSUPPORTED;
+  }
   JobPlan plan;
   std::string perr;
   gx_status ps = plan_job(desc, &plan, perr);

@@ -1,0 +1,453 @@
+// Tensor-core X-step: the cross-multiply-accumulate of Core::processdata
+// (mpifxcorr/src/core.cpp:784-1053; the product vis1 * conj(vis2) of
+// vectorAddProduct_cf32 at core.cpp:963, summed over the FFT blocks of a
+// subint) on the 5th-generation tensor cores: tcgen05.mma with FP16 operands
+// and FP32 accumulators in tensor memory.
+//
+// For one frequency and one channel the blocks of a chunk form the NI x K
+// complex matrix X = Xr + i Xi (row a: input a, column k: FFT block k), and the
+// visibilities of every input pair are V = X X^H:
+//     Re V = Xr Xr^T + Xi Xi^T,    Im V(a, b) = P(a, b) - P(b, a),  P = Xi Xr^T.
+// Each CTA owns one frequency and one pair of channels and keeps, per channel, a
+// 128-lane x 256-column FP32 accumulator in tensor memory: columns 0..127 hold
+// Re V, columns 128..255 hold P.  Per step of 16 FFT blocks and channel:
+//     D[:, 0:256) += Xi [Xi ; Xr]^T      (M = 128, N = 256, K = 16)
+//     D[:, 0:128) += Xr Xr^T             (M = 128, N = 128, K = 16)
+// i.e. three 128x128x16 real products per complex 128x128 Hermitian update
+// (the fourth, Xr Xi^T, is P transposed and is formed in the finalising pass).
+//
+// Data path per CTA: the spectra of its channel pair are stored as one
+// contiguous 2 KB row per block (layout [freq][block][chan/2][input][2] float2,
+// written so by the F-step), fetched by bulk copies (cp.async.bulk, no
+// multicast) into a 4-stage FP32 ring; all threads scale each value by a power
+// of two per (input, channel), round it to FP16 and store it, transposed to
+// K-major, into the canonical no-swizzle core-matrix layout of the MMA operand
+// [Xi ; Xr] (256 rows x 16 blocks); one thread issues the MMAs and commits them
+// to an mbarrier that frees the operand stage.  In the split form the FP16
+// remainder lo = fp16(x*s - hi) is kept too and the products hi*hi + hi*lo +
+// lo*hi are accumulated (lo*lo, below 2^-22 relative, is dropped).
+//
+// The accumulators leave tensor memory once per chunk: each thread reads its
+// lane (row a) and adds 16-column slices into acc[freq][chan/2][a][b][2]
+// (Re and P arrays), so partial sums across chunks and K-split slices stay FP32.
+//
+// Every wait on an mbarrier is bounded in time; on expiry the kernel records a
+// nonzero status in *err, drains its own copies and MMAs (again bounded),
+// releases its tensor memory and returns.
+#include <cstdint>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include "gx_xstep.h"
+
+namespace gx {
+namespace {
+
+constexpr int kNI = 128;                     // inputs per frequency = MMA M
+constexpr int kKT = 16;                      // FFT blocks per K-tile = one MMA K step for FP16
+constexpr int kStages = 4;                   // FP32 staging ring depth (bulk copies in flight)
+constexpr int kOpStages = 2;                 // FP16 operand stages
+constexpr int kThreads = 256;
+constexpr uint32_t kTmemCols = 512;          // 2 channels x (128 Re + 128 P) FP32 columns
+constexpr uint32_t kRowBytes = kNI * 16;     // one block of a channel pair: 128 inputs x 2 channels x float2
+constexpr uint32_t kStageBytes = kKT * kRowBytes;         // 32 KB
+constexpr uint32_t kLBO = 128;               // byte step between the two 8-block core matrices of a row group
+constexpr uint32_t kSBO = (kKT / 8) * 128;   // byte step between 8-row groups
+constexpr uint32_t kOpChanBytes = 2 * kNI * kKT * 2;      // [Xi ; Xr]: 256 rows x 16 FP16 = 8 KB
+constexpr uint32_t kXrOffset = (kNI / 8) * kSBO;          // rows 128.. (Xr) start here
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
+{
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Waits for the phase of the given parity to complete; false after kWaitLimitNs.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  while (!mbar_try_wait(bar, parity))
+    if (global_ns() - t0 > kWaitLimitNs) return false;
+  return true;
+}
+
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
+{
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_alloc(uint32_t dst_smem, uint32_t ncols)
+{
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst_smem), "r"(ncols)
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_relinquish()
+{
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols)
+{
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+// D[tmem] (+)= A[smem] * B[smem]^T, FP16 operands, FP32 accumulator.
+__device__ __forceinline__ void mma_f16(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate)
+{
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar)
+{
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+// 32 lanes x 16 consecutive FP32 columns: thread i of the warp gets lane (base lane + i).
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
+{
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Shared-memory operand descriptor, K-major without swizzle: 8-row x 16-byte
+// core matrices, kLBO between the two core matrices of a K step, kSBO between
+// 8-row groups; version 1 (bits 46-47) as tcgen05 requires.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr)
+{
+  return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)(kLBO >> 4) << 16) | ((uint64_t)(kSBO >> 4) << 32) |
+         (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator (bits 4-5 = 1), FP16 A
+// and B (formats 0), both K-major, N >> 3 at bit 17, M >> 4 at bit 24 (M = 128).
+__host__ __device__ constexpr uint32_t idesc_f16(int n)
+{
+  return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kNI >> 4) << 24);
+}
+
+__device__ __forceinline__ uint32_t pack_half2(float a, float b)
+{
+  const __half2 h = __floats2half2_rn(a, b);
+  return *reinterpret_cast<const uint32_t *>(&h);
+}
+
+// hi = fp16(a), lo = fp16(a - hi): a - hi is exact in FP32.
+__device__ __forceinline__ void split2(float a, float b, uint32_t &hi, uint32_t &lo)
+{
+  const __half2 h = __floats2half2_rn(a, b);
+  const float2 hf = __half22float2(h);
+  const __half2 l = __floats2half2_rn(a - hf.x, b - hf.y);
+  hi = *reinterpret_cast<const uint32_t *>(&h);
+  lo = *reinterpret_cast<const uint32_t *>(&l);
+}
+
+template <bool HILO>
+__global__ void __launch_bounds__(kThreads, 1)
+xmac_tc_kernel(const float2 *__restrict__ spec, int nblk, int NP, int ks, const float *__restrict__ scale,
+               float *__restrict__ acc_re, float *__restrict__ acc_p, size_t slice_floats, int accumulate,
+               int *__restrict__ err)
+{
+  constexpr uint32_t kParts = HILO ? 2 : 1;
+  constexpr uint32_t kOpStageBytes = kParts * 2 * kOpChanBytes;
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char *staging = smem;
+  unsigned char *ops = smem + kStages * kStageBytes;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(ops + kOpStages * kOpStageBytes);  // [kStages] full, [kOpStages] MMA done
+  uint32_t *s_tmem = reinterpret_cast<uint32_t *>(bars + kStages + kOpStages);
+  volatile int *s_abort = reinterpret_cast<volatile int *>(s_tmem + 1);
+
+  const int p = blockIdx.x, f = blockIdx.y, z = blockIdx.z;
+  const int N = 2 * NP;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ntile_all = (nblk + kKT - 1) / kKT;
+  const int t0 = (int)((long long)ntile_all * z / ks);
+  const int nt = (int)((long long)ntile_all * (z + 1) / ks) - t0;
+
+  if (tid == 0) {
+    for (int i = 0; i < kStages + kOpStages; i++) mbar_init(smem_u32(bars + i), 1);
+    *s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    tmem_alloc(smem_u32(s_tmem), kTmemCols);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *s_tmem;
+
+  // conversion role: row r of the operand, block group g (blocks 8g .. 8g+7 of a tile)
+  const int r = tid & (kNI - 1), g = tid >> 7;
+  const float s0 = scale[((size_t)f * kNI + r) * N + 2 * p];
+  const float s1 = scale[((size_t)f * kNI + r) * N + 2 * p + 1];
+  const uint32_t row_off = (uint32_t)(r >> 3) * kSBO + (uint32_t)g * kLBO + (uint32_t)(r & 7) * 16;
+
+  // tile u of this slice into staging stage u % kStages (thread 0 only)
+  auto issue = [&](int u) {
+    const int st = u % kStages;
+    const int kb0 = (t0 + u) * kKT;
+    const int kv = min(kKT, nblk - kb0);
+    const uint32_t bar = smem_u32(bars + st);
+    mbar_expect_tx(bar, (uint32_t)kv * kRowBytes);
+    for (int k = 0; k < kv; k++) {
+      const float2 *src = spec + (((size_t)f * nblk + kb0 + k) * NP + p) * (size_t)(2 * kNI);
+      bulk_load(smem_u32(staging + st * kStageBytes + k * kRowBytes), src, kRowBytes, bar);
+    }
+  };
+
+  int issued = 0, t = 0;
+  if (tid == 0)
+    for (; issued < nt && issued < kStages - 1; issued++) issue(issued);
+
+  for (; t < nt; t++) {
+    if (tid == 0 && issued < nt) issue(issued++);
+    const int st = t % kStages, o = t % kOpStages;
+    bool good = mbar_wait(smem_u32(bars + st), (uint32_t)(t / kStages) & 1u);
+    if (good && t >= kOpStages) good = mbar_wait(smem_u32(bars + kStages + o), (uint32_t)(t / kOpStages - 1) & 1u);
+    if (!good) {
+      *s_abort = 1;
+      atomicExch(err, 1);
+    } else {
+      const int kv = min(kKT, nblk - (t0 + t) * kKT);
+      const float4 *stg = reinterpret_cast<const float4 *>(staging + st * kStageBytes);
+      uint32_t re0[4], im0[4], re1[4], im1[4];
+      uint32_t lre0[4], lim0[4], lre1[4], lim1[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int k = g * 8 + 2 * j;
+        const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 a = (k < kv) ? stg[k * kNI + r] : zero;          // (c0.re, c0.im, c1.re, c1.im) at block k
+        const float4 b = (k + 1 < kv) ? stg[(k + 1) * kNI + r] : zero;
+        if (HILO) {
+          split2(a.x * s0, b.x * s0, re0[j], lre0[j]);
+          split2(a.y * s0, b.y * s0, im0[j], lim0[j]);
+          split2(a.z * s1, b.z * s1, re1[j], lre1[j]);
+          split2(a.w * s1, b.w * s1, im1[j], lim1[j]);
+        } else {
+          re0[j] = pack_half2(a.x * s0, b.x * s0);
+          im0[j] = pack_half2(a.y * s0, b.y * s0);
+          re1[j] = pack_half2(a.z * s1, b.z * s1);
+          im1[j] = pack_half2(a.w * s1, b.w * s1);
+        }
+      }
+      unsigned char *op = ops + o * kOpStageBytes;
+      // channel e, part q at op + (q * 2 + e) * kOpChanBytes; Xi rows 0..127, Xr rows 128..255
+      *reinterpret_cast<uint4 *>(op + row_off) = make_uint4(im0[0], im0[1], im0[2], im0[3]);
+      *reinterpret_cast<uint4 *>(op + row_off + kXrOffset) = make_uint4(re0[0], re0[1], re0[2], re0[3]);
+      *reinterpret_cast<uint4 *>(op + kOpChanBytes + row_off) = make_uint4(im1[0], im1[1], im1[2], im1[3]);
+      *reinterpret_cast<uint4 *>(op + kOpChanBytes + row_off + kXrOffset) = make_uint4(re1[0], re1[1], re1[2], re1[3]);
+      if (HILO) {
+        unsigned char *lo = op + 2 * kOpChanBytes;
+        *reinterpret_cast<uint4 *>(lo + row_off) = make_uint4(lim0[0], lim0[1], lim0[2], lim0[3]);
+        *reinterpret_cast<uint4 *>(lo + row_off + kXrOffset) = make_uint4(lre0[0], lre0[1], lre0[2], lre0[3]);
+        *reinterpret_cast<uint4 *>(lo + kOpChanBytes + row_off) = make_uint4(lim1[0], lim1[1], lim1[2], lim1[3]);
+        *reinterpret_cast<uint4 *>(lo + kOpChanBytes + row_off + kXrOffset) =
+            make_uint4(lre1[0], lre1[1], lre1[2], lre1[3]);
+      }
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (*s_abort) break;
+    if (tid == 0) {
+      tc_fence_after();
+      const uint32_t opb = smem_u32(ops + o * kOpStageBytes);
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const uint32_t d = tmem + (uint32_t)e * 256u;
+        const uint32_t hb = opb + (uint32_t)e * kOpChanBytes;
+        const uint64_t xi = smem_desc(hb), xr = smem_desc(hb + kXrOffset);
+        mma_f16(d, xi, xi, idesc_f16(256), t > 0 ? 1u : 0u);
+        mma_f16(d, xr, xr, idesc_f16(128), 1u);
+        if (HILO) {
+          const uint32_t lb = opb + (2u + (uint32_t)e) * kOpChanBytes;
+          const uint64_t li = smem_desc(lb), lr = smem_desc(lb + kXrOffset);
+          mma_f16(d, xi, li, idesc_f16(256), 1u);
+          mma_f16(d, li, xi, idesc_f16(256), 1u);
+          mma_f16(d, xr, lr, idesc_f16(128), 1u);
+          mma_f16(d, lr, xr, idesc_f16(128), 1u);
+        }
+      }
+      mma_commit(smem_u32(bars + kStages + o));
+    }
+  }
+
+  // all MMAs of the slice have completed once the last commit has arrived
+  if (!*s_abort && nt > 0) {
+    const int tl = nt - 1;
+    if (!mbar_wait(smem_u32(bars + kStages + tl % kOpStages), (uint32_t)(tl / kOpStages) & 1u)) {
+      *s_abort = 1;
+      atomicExch(err, 2);
+    }
+  }
+  __syncthreads();
+  tc_fence_after();
+
+  if (!*s_abort) {
+    // warp w reads lanes 32 (w % 4) .. +31 (rows a); warps 0-3 the Re columns, 4-7 the P columns
+    const int q = warp & 3, h = warp >> 2;
+    const int a = 32 * q + lane;
+    float *out = (h == 0 ? acc_re : acc_p) + (size_t)z * slice_floats +
+                 (((size_t)f * NP + p) * kNI + a) * (size_t)(2 * kNI);
+    const uint32_t lane_addr = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)h * 128u;
+#pragma unroll 1
+    for (int cb = 0; cb < kNI / 16; cb++) {
+      float v0[16], v1[16];
+      if (nt > 0) {
+        tmem_ld16(lane_addr + (uint32_t)cb * 16u, v0);
+        tmem_ld16(lane_addr + 256u + (uint32_t)cb * 16u, v1);
+        tmem_ld_wait();
+      } else {
+#pragma unroll
+        for (int i = 0; i < 16; i++) v0[i] = v1[i] = 0.f;
+      }
+      if (nt == 0 && accumulate) continue;
+      float4 *o4 = reinterpret_cast<float4 *>(out + cb * 32);
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        float4 w = make_float4(v0[2 * i], v1[2 * i], v0[2 * i + 1], v1[2 * i + 1]);
+        if (accumulate) {
+          const float4 old = o4[i];
+          w.x += old.x;
+          w.y += old.y;
+          w.z += old.z;
+          w.w += old.w;
+        }
+        o4[i] = w;
+      }
+    }
+  } else if (tid == 0) {
+    // drain: copies issued but not consumed, then the MMAs last committed
+    for (int u = t; u < issued; u++) mbar_wait(smem_u32(bars + u % kStages), (uint32_t)(u / kStages) & 1u);
+    if (t > 0) mbar_wait(smem_u32(bars + kStages + (t - 1) % kOpStages), (uint32_t)((t - 1) / kOpStages) & 1u);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tmem_dealloc(tmem, kTmemCols);
+}
+
+// One thread per (entry, channel): Re and Im of input pair (a, b) from the Re
+// and P accumulators summed over the K-split slices, unscaled.
+__global__ void finalise_tc_kernel(const TcProdEntry *__restrict__ prods, int nprods, const float *__restrict__ acc_re,
+                                   const float *__restrict__ acc_p, int ks, size_t slice_floats, int N,
+                                   const float *__restrict__ scale, float2 *__restrict__ results)
+{
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)nprods * N) return;
+  const int e = (int)(i / N), c = (int)(i % N);
+  const TcProdEntry P = prods[e];
+  const int NP = N / 2, cp = c >> 1, ce = c & 1;
+  const size_t base = ((size_t)P.freq * NP + cp) * kNI * kNI * 2;
+  const size_t iab = base + ((size_t)P.a * kNI + P.b) * 2 + ce;
+  const size_t iba = base + ((size_t)P.b * kNI + P.a) * 2 + ce;
+  float re = 0.f, pab = 0.f, pba = 0.f;
+  for (int z = 0; z < ks; z++) {
+    re += acc_re[z * slice_floats + iab];
+    pab += acc_p[z * slice_floats + iab];
+    pba += acc_p[z * slice_floats + iba];
+  }
+  const float sa = scale[((size_t)P.freq * kNI + P.a) * N + c];
+  const float sb = scale[((size_t)P.freq * kNI + P.b) * N + c];
+  const float inv = 1.0f / (sa * sb);
+  results[P.result_offset + c] = make_float2(re * inv, (pab - pba) * inv);
+}
+
+}  // namespace
+
+size_t xmac_tc_smem_bytes(bool hilo)
+{
+  const size_t ops = (size_t)kOpStages * (hilo ? 2 : 1) * 2 * kOpChanBytes;
+  return (size_t)kStages * kStageBytes + ops + (kStages + kOpStages) * 8 + 16;
+}
+
+cudaError_t xmac_tc_launch(const float2 *spec, int nblk, int N, int nfreqs, int ks, bool hilo, const float *scale,
+                           float *acc_re, float *acc_p, size_t slice_floats, int accumulate, int *err,
+                           cudaStream_t st)
+{
+  if (nblk <= 0) return cudaSuccess;
+  const size_t sm = xmac_tc_smem_bytes(hilo);
+  dim3 grid(N / 2, nfreqs, ks);
+  if (hilo) {
+    static bool opted = false;
+    if (!opted) {
+      cudaError_t e = cudaFuncSetAttribute(xmac_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      if (e != cudaSuccess) return e;
+      opted = true;
+    }
+    xmac_tc_kernel<true><<<grid, kThreads, sm, st>>>(spec, nblk, N / 2, ks, scale, acc_re, acc_p, slice_floats,
+                                                      accumulate, err);
+  } else {
+    static bool opted = false;
+    if (!opted) {
+      cudaError_t e = cudaFuncSetAttribute(xmac_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      if (e != cudaSuccess) return e;
+      opted = true;
+    }
+    xmac_tc_kernel<false><<<grid, kThreads, sm, st>>>(spec, nblk, N / 2, ks, scale, acc_re, acc_p, slice_floats,
+                                                       accumulate, err);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t finalise_tc_launch(const TcProdEntry *prods, int nprods, const float *acc_re, const float *acc_p, int ks,
+                               size_t slice_floats, int N, const float *scale, float2 *results, cudaStream_t st)
+{
+  if (nprods <= 0) return cudaSuccess;
+  const long long n = (long long)nprods * N;
+  finalise_tc_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(prods, nprods, acc_re, acc_p, ks, slice_floats, N,
+                                                                  scale, results);
+  return cudaGetLastError();
+}
+
+}  // namespace gx

@@ -41,7 +41,7 @@ def lib():
         L.gx_status_string.restype = C.c_char_p
         for name in ("gx_open", "gx_open_input", "gx_close", "gx_get_layout", "gx_get_offsets", "gx_interpolator",
                      "gx_scan_start_sec", "gx_subint", "gx_subint_device", "gx_synchronize", "gx_spectra",
-                     "gx_stage_times", "gx_launch_count", "gx_subint_device_noalloc"):
+                     "gx_stage_times", "gx_launch_count", "gx_subint_device_noalloc", "gx_set_tc_scales"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -50,7 +50,7 @@ def lib():
 EXPORTED_SYMBOLS = ("gx_open", "gx_open_input", "gx_close", "gx_last_error", "gx_status_string",
                     "gx_get_layout", "gx_get_offsets", "gx_interpolator", "gx_scan_start_sec", "gx_subint",
                     "gx_subint_device", "gx_synchronize", "gx_spectra", "gx_stage_times", "gx_launch_count",
-                    "gx_subint_device_noalloc")
+                    "gx_subint_device_noalloc", "gx_set_tc_scales")
 
 
 def subint_device_noalloc(jd: capi.JobDesc, sd: capi.SubintDesc, dev_results_ptr: int, stream_ptr: int = 0) -> None:
@@ -159,6 +159,12 @@ class Correlator:
 
     def synchronize(self):
         self._check(lib().gx_synchronize(self.h))
+
+    def set_tc_scales(self, station: int, band: int, scales) -> None:
+        """Per-channel operand scales of the tensor-core X-step for one station band
+        (rounded to powers of two by the library)."""
+        a = np.ascontiguousarray(scales, dtype=np.float32)
+        self._check(lib().gx_set_tc_scales(self.h, station, band, a.ctypes.data_as(C.c_void_p)))
 
     def spectra(self, station: int, block: int, nbands: int):
         out = np.zeros(nbands * self.info.nchan, np.complex64)

@@ -200,6 +200,16 @@ gx_status gx_stage_times(gx_handle *h, float ms[3]);
 /* Number of kernel launches issued by the last gx_subint* call. */
 gx_status gx_launch_count(const gx_handle *h, int *count);
 
+/* Operand scales of the tensor-core X-step for one band of one datastream:
+   scales[c] multiplies channel c of that band's spectra before they are
+   rounded to FP16 and is divided out of every visibility.  Each value is
+   rounded to the nearest power of two, so scaling and unscaling are exact.
+   The defaults bring noise spectra to an r.m.s. near 8.  Returns GX_ERR_STATE
+   for a handle without the tensor-core X-step, GX_ERR_ARG for a value that is
+   not finite and positive.  No counterpart in the reference (its X-step is
+   FP32 throughout). */
+gx_status gx_set_tc_scales(gx_handle *h, int station, int band, const float *scales);
+
 #ifdef __cplusplus
 }
 #endif

@@ -84,6 +84,28 @@ def test_bad_descriptors_are_rejected(mutate, status):
     assert ei.value.status == status
 
 
+def test_tensor_core_xstep_limits():
+    """The tensor-core X-step takes at most 128 station bands per freq
+    (GX_ERR_UNSUPPORTED beyond), an unknown xstep is GX_ERR_ARG, and
+    gx_set_tc_scales needs a device handle with that X-step (GX_ERR_STATE)."""
+    from difx_b200.jobfiles import Subband
+    big = jobs.JobSpec(name="tcbig", nstations=65, subbands=[Subband(6000.0, 16.0, "U", 64)], nbits=8,
+                       sampling="COMPLEX", subint_ns=1_024_000, execute_seconds=2, max_delay_us=150.0, seed=1)
+    with pytest.raises(gxcorr.GxError) as ei:
+        gxcorr.Correlator.from_desc(capi.job_desc_from_spec(big, xstep=capi.GX_XSTEP_TC_FP16), device=-1)
+    assert ei.value.status == 2
+    ok = capi.job_desc_from_spec(jobs.spec_c1(), xstep=capi.GX_XSTEP_TC_FP16_HILO)
+    c = gxcorr.Correlator.from_desc(ok, device=-1)
+    with pytest.raises(gxcorr.GxError) as ei:
+        c.set_tc_scales(0, 0, [1.0] * jobs.spec_c1().nchan)
+    assert ei.value.status == 8
+    c.close()
+    bad = capi.job_desc_from_spec(jobs.spec_c1(), xstep=7)
+    with pytest.raises(gxcorr.GxError) as ei:
+        gxcorr.Correlator.from_desc(bad, device=-1)
+    assert ei.value.status == 1
+
+
 def test_missing_input_file_is_an_io_error():
     with pytest.raises(gxcorr.GxError) as ei:
         gxcorr.Correlator.from_input("/nonexistent/job.input", device=-1)
