@@ -274,7 +274,7 @@ def roofline(spec: JobSpec, xstep: str, stage, peaks):
     spec_bytes = nblk * spec.nstations * spec.nbands * spec.nchan * 8
     stages = {"F": f_ms, "X": x_ms, "finalise": fin_ms}
     if f_ms >= x_ms:
-        k = "fstep_cta_kernel" if spec.fftchannels > 1024 else "fstep_warp_kernel"
+        k = "fstep_r16_kernel" if spec.fftchannels >= 2048 else "fstep_warp_kernel"
         a = (in_bytes + spec_bytes) / (f_ms * 1e-3) / 1e9
         return {"kernel": k, "bound": "hbm", "achieved": a, "peak": hbm_peak, "unit": "GB/s", "frac": a / hbm_peak,
                 "traffic": None, "peak_source": src, "algorithmic_bytes_per_step": in_bytes + spec_bytes,

@@ -8,6 +8,7 @@
 // accumulators onto the Core result array.  gx_subint[_device] then runs one
 // Core slot: F-step and X-step over chunks of FFT blocks, then one
 // finalising pass writing the result array.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -59,13 +60,15 @@ struct gx_handle {
   std::vector<int> blofs, bwofs, acofs, acwofs;
   std::vector<std::vector<int>> band_input;  // [station][band]
   std::vector<ProdEntry> prods;
-  std::vector<TcProdEntry> tcprods;
+  std::vector<TcProdEntry> tcprods;   // sorted by (freq, a)
+  std::vector<TcRowEntry> tcrows;
   std::vector<WeightEntry> wents;
   std::vector<int2> pairs;
   bool tc = false, hilo = false;   // tensor-core X-step (split FP16 product)
   float tc_scale0 = 1.0f;          // default power-of-two operand scale
   float *d_scale = nullptr;        // [freq][128][nchan] operand scales
   TcProdEntry *d_tcprods = nullptr;
+  TcRowEntry *d_tcrows = nullptr;
   int *d_err = nullptr;            // kernel status (bounded waits that expired)
   int *h_err = nullptr;            // pinned copy of *d_err after each subint
   cudaStream_t last_stream = nullptr;  // stream of the last gx_subint_device
@@ -119,7 +122,7 @@ static void free_all(gx_handle *h)
   if (h->device < 0) return;
   void *ptrs[] = {h->d_st, h->d_tw, h->d_spec, h->d_acc, h->d_results, h->d_spec1, h->d_w, h->d_wacc, h->d_w1,
                   h->d_pairs, h->d_prods, h->d_went, (void *)h->d_dataptrs, h->d_datalen, h->d_ctrl, h->d_interp,
-                  h->d_bp, h->d_bp1, h->d_scale, h->d_tcprods, h->d_err};
+                  h->d_bp, h->d_bp1, h->d_scale, h->d_tcprods, h->d_tcrows, h->d_err};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->h_err) cudaFreeHost(h->h_err);
@@ -193,8 +196,6 @@ static gx_status setup(gx_handle *h)
   if (J.stride & (J.stride - 1)) return h->fail(GX_ERR_UNSUPPORTED, "array stride must be a power of two");
   J.lgstride = 0;
   while ((1 << J.lgstride) < J.stride) J.lgstride++;
-  J.lgcgroup = 0;
-  while ((1 << J.lgcgroup) < J.nchan) J.lgcgroup++;
   J.half = (cplx ? 2 * J.nfr : J.nfr) / 2;
   J.unpacksamples = cplx ? f0.nchan : 2 * f0.nchan;
   J.sampletime = 1.0 / (2.0 * f0.bw_mhz);
@@ -272,7 +273,6 @@ static gx_status setup(gx_handle *h)
       return h->fail(GX_ERR_UNSUPPORTED, "the tensor-core X-step takes at most 128 inputs (station bands) per freq");
     if (J.nchan < 2) return h->fail(GX_ERR_UNSUPPORTED, "the tensor-core X-step needs at least 2 channels");
     J.ninputs = kTcInputs;   // rows beyond the job's inputs stay zero
-    J.lgcgroup = 1;          // channel pairs interleaved: [chan/2][input][2]
   } else {
     h->xs = xmac_shape(ni);
     J.ninputs = h->xs.nsuper * h->xs.ST;
@@ -430,11 +430,35 @@ static gx_status setup(gx_handle *h)
     }
   }
 
+  // tensor-core finalising pass: entries grouped by (freq, a) row
+  h->tcrows.clear();
+  if (h->tc) {
+    std::stable_sort(h->tcprods.begin(), h->tcprods.end(), [](const TcProdEntry &x, const TcProdEntry &y) {
+      return x.freq != y.freq ? x.freq < y.freq : x.a < y.a;
+    });
+    for (size_t i = 0; i < h->tcprods.size();) {
+      TcRowEntry r{h->tcprods[i].freq, h->tcprods[i].a, kTcInputs, (int)i, (int)i};
+      while (i < h->tcprods.size() && h->tcprods[i].freq == r.freq && h->tcprods[i].a == r.a) {
+        r.bmin = std::min(r.bmin, h->tcprods[i].b);
+        i++;
+      }
+      r.end = (int)i;
+      h->tcrows.push_back(r);
+    }
+  }
+
   // chunking and K-split
   const size_t per_block = (size_t)d.nfreqs * J.ninputs * J.nchan * sizeof(float2);
-  // The tensor-core X-step moves its accumulators through HBM once per chunk
-  // (128 x 128 x 2 floats per channel), so it gets longer chunks.
-  const size_t spec_budget = h->tc ? (size_t(16) << 30) : (size_t(2) << 30);
+  // The tensor-core X-step moves its accumulators (128 x 128 complex per
+  // channel) through HBM once per chunk, so it gets long chunks: up to 40 GB of
+  // spectra, at most 30% of the device memory free at open.
+  size_t spec_budget = size_t(2) << 30;
+  if (h->tc) {
+    spec_budget = size_t(40) << 30;
+    size_t fr = 0, tot = 0;
+    if (h->device >= 0 && cudaSetDevice(h->device) == cudaSuccess && cudaMemGetInfo(&fr, &tot) == cudaSuccess)
+      spec_budget = std::max(size_t(1) << 30, std::min(spec_budget, fr / 10 * 3));
+  }
   int chunk = d.block_chunk > 0 ? d.block_chunk
                                 : (int)std::min<size_t>(4096, std::max<size_t>(64, spec_budget / per_block));
   if (chunk > J.blocks_per_send) chunk = J.blocks_per_send;
@@ -533,7 +557,7 @@ static gx_status setup(gx_handle *h)
   CKR(h, cudaMalloc(&h->d_bp, sizeof(BlockParam) * (size_t)d.nstations * chunk));
   CKR(h, cudaMalloc(&h->d_bp1, sizeof(BlockParam) * (size_t)d.nstations));
   if (h->tc) {
-    // Re and P arrays of [freq][chan/2][128][128][2] floats per K-split slice
+    // [freq][chan/2][128][128] float4 (both channels of a pair) per K-split slice
     h->acc_slice = (size_t)d.nfreqs * J.nchan * kTcInputs * kTcInputs;
     const size_t nsc = (size_t)d.nfreqs * kTcInputs * J.nchan;
     std::vector<float> sc(nsc, h->tc_scale0);
@@ -542,6 +566,10 @@ static gx_status setup(gx_handle *h)
     CKR(h, cudaMalloc(&h->d_tcprods, sizeof(TcProdEntry) * std::max<size_t>(1, h->tcprods.size())));
     if (!h->tcprods.empty())
       CKR(h, cudaMemcpy(h->d_tcprods, h->tcprods.data(), sizeof(TcProdEntry) * h->tcprods.size(),
+                        cudaMemcpyHostToDevice));
+    CKR(h, cudaMalloc(&h->d_tcrows, sizeof(TcRowEntry) * std::max<size_t>(1, h->tcrows.size())));
+    if (!h->tcrows.empty())
+      CKR(h, cudaMemcpy(h->d_tcrows, h->tcrows.data(), sizeof(TcRowEntry) * h->tcrows.size(),
                         cudaMemcpyHostToDevice));
   } else {
     h->acc_slice = (size_t)d.nfreqs * xs.npairs * xs.ST * xs.ST * J.nchan;
@@ -758,8 +786,7 @@ static gx_status run_device(gx_handle *h, const gx_subint_desc *sub, const uint8
   h->have_last = true;
 
   const int nbl = d.nbaselines;
-  float *acc_re = reinterpret_cast<float *>(h->d_acc);
-  float *acc_p = acc_re + h->acc_slice * h->ks;
+  float4 *acc4 = reinterpret_cast<float4 *>(h->d_acc);
   // the tensor-core X-step stores its first chunk instead of adding to it
   if (!h->tc) CKR(h, cudaMemsetAsync(h->d_acc, 0, sizeof(float2) * h->acc_slice * h->ks, st));
   CKR(h, cudaMemsetAsync(h->d_wacc, 0, sizeof(float) * (d.nstations + nbl), st));
@@ -772,8 +799,8 @@ static gx_status run_device(gx_handle *h, const gx_subint_desc *sub, const uint8
     if ((r = record(h, st, 0, false)) != GX_OK) return r;
     if ((r = record(h, st, 1, true)) != GX_OK) return r;
     if (h->tc)
-      CKR(h, xmac_tc_launch(h->d_spec, nb, J.nchan, d.nfreqs, h->ks, h->hilo, h->d_scale, acc_re, acc_p,
-                            h->acc_slice, b0 > 0 ? 1 : 0, h->d_err, st));
+      CKR(h, xmac_tc_launch(h->d_spec, nb, J.nchan, d.nfreqs, h->ks, h->hilo, h->d_scale, acc4, b0 > 0 ? 1 : 0,
+                            h->d_err, st));
     else
       CKR(h, xmac_fp32_launch(h->d_spec, nb, J.ninputs, J.nchan, d.nfreqs, h->ks, h->d_acc, st));
     CKR(h, weights_launch(h->d_w, nb, d.nstations, h->d_pairs, nbl, h->d_wacc, st));
@@ -784,8 +811,8 @@ static gx_status run_device(gx_handle *h, const gx_subint_desc *sub, const uint8
   if ((r = record(h, st, 2, true)) != GX_OK) return r;
   CKR(h, cudaMemsetAsync(dev_results, 0, sizeof(float2) * h->rl, st));
   if (h->tc) {
-    CKR(h, finalise_tc_launch(h->d_tcprods, (int)h->tcprods.size(), acc_re, acc_p, h->ks, h->acc_slice, J.nchan,
-                              h->d_scale, dev_results, st));
+    CKR(h, finalise_tc_launch(h->d_tcprods, h->d_tcrows, (int)h->tcrows.size(), acc4, d.nfreqs, J.nchan, h->ks,
+                              dev_results, st));
     CKR(h, finalise_launch(nullptr, 0, h->d_acc, h->ks, h->acc_slice, J.nchan, h->d_went, (int)h->wents.size(),
                            h->d_wacc, dev_results, st));
   } else {
@@ -880,10 +907,7 @@ gx_status gx_spectra(gx_handle *h, int station, int block, float *out, float *we
   if (station < 0 || station >= J.nstations || block < 0 || block >= J.blocks_per_send)
     return h->fail(GX_ERR_ARG, "station or block out of range");
   CKR(h, cudaSetDevice(h->device));
-  DevJob Jrow = J;   // one contiguous row per (freq, input), whatever layout the X-step reads
-  Jrow.lgcgroup = 0;
-  while ((1 << Jrow.lgcgroup) < J.nchan) Jrow.lgcgroup++;
-  CKR(h, fstep_launch(Jrow, h->d_st, h->maxnrf, h->last, block, 1, h->nslots, h->d_spec1, h->d_w1, h->d_bp1,
+  CKR(h, fstep_launch(J, h->d_st, h->maxnrf, h->last, block, 1, h->nslots, h->d_spec1, h->d_w1, h->d_bp1,
                       h->stream));
   const gx_station_desc &x = h->jd.stations[station];
   for (int b = 0; b < x.nbands; b++) {

@@ -47,7 +47,6 @@ struct DevJob {
   int blocks_per_send;
   int flaglen;
   int lgstride;           // log2(stride): FFT length, channels and stride are powers of two
-  int lgcgroup;           // log2(channels per spectra group), see spec_offset
   double sampletime;      // us
   double bw;              // MHz
   const float2 *twiddle;  // exp(-2 pi i m / F), m in [0, F)
@@ -55,14 +54,10 @@ struct DevJob {
 };
 
 // Offset of (input row, channel c) inside the spectra of one (freq, block):
-// channels in groups of G = 1 << lgcgroup, each group holding every row
-// ([c / G][row][c % G]).  G = nchan is the plain [row][channel] layout of the
-// FP32 X-step; G = 2 gives the tensor-core X-step one contiguous row of
-// ninputs x 2 channels per block.
+// spec[freq][block][row][channel].
 __host__ __device__ __forceinline__ size_t spec_offset(const DevJob &J, int row, int c)
 {
-  const int G = 1 << J.lgcgroup;
-  return ((size_t)(c >> J.lgcgroup) * J.ninputs + row) * G + (c & (G - 1));
+  return (size_t)row * J.nchan + c;
 }
 
 // Per (station, FFT block) parameters, computed in FP64 by blockparams_kernel

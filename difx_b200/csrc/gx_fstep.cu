@@ -1,9 +1,7 @@
 // F-step: VDIF unpack + validity/weights, FP64 per-block delay evaluation,
 // FP32 fringe rotation, shared-memory Stockham FFT, sideband selection and
-// fractional-sample correction, writing spectra in the layout the X-step
-// reads: spec[freq][block][...] (float2) with (input, channel) placed by
-// spec_offset — [input][channel] for the FP32 X-step, channel pairs
-// interleaved ([channel/2][input][2]) for the tensor-core X-step.
+// fractional-sample correction, writing spectra in the layout both X-steps
+// read: spec[freq][block][input][channel] (float2).
 //
 // Two kernels per pass of blocks:
 //   blockparams_kernel  one thread per (station, block): FP64 delay, nearest
@@ -14,8 +12,11 @@
 //                       its samples into warp-private shared memory, runs the
 //                       FFT with warp-level synchronisation only and writes
 //                       the corrected spectrum row.
-//   fstep_cta_kernel    (longer FFTs) the bands of a block are transformed
-//                       concurrently in slots of one CTA.
+//   fstep_r16_kernel    (FFT length >= 2048) a group of F / 16 threads per
+//                       (block, band), 16 samples per thread in registers,
+//                       radix-16 passes with padded shared-memory exchanges.
+//   fstep_cta_kernel    (longer FFTs not covered above) the bands of a block
+//                       are transformed concurrently in slots of one CTA.
 //
 // Reference semantics followed (mpifxcorr/src):
 //   block validity / delay / nearest sample      mode.cpp:656-701
@@ -28,7 +29,9 @@
 //   real->complex, rotate, FFT, sideband copy     mode.cpp:1160-1217
 //   fractional-sample correction                  mode.cpp:1256-1261
 #include <cstdint>
+#include <cstdlib>
 #include "gx_dev.h"
+#include "gx_fft16.h"
 
 namespace gx {
 
@@ -559,6 +562,163 @@ fstep_cta_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays
 }
 
 // --------------------------------------------------------------------------
+// Register-resident F-step for long transforms: a group of NT = F / 16 threads
+// per (block, band) item, 16 samples per thread (x[j + NT t]) decoded and
+// fringe-rotated straight into registers, transformed by the radix-16 passes of
+// gx_fft16.h with padded shared-memory exchanges, and written from registers
+// after the sideband selection and fractional-sample correction.  A CTA holds
+// G = CTA / NT groups; groups synchronise on their own named barrier.
+#ifndef GX_R16_MINB
+#define GX_R16_MINB 3
+#endif
+template <int F>
+struct R16Launch {
+  static constexpr int NT = F / 16;
+  static constexpr int CTA = NT >= 256 ? NT : 256;
+  static constexpr int G = CTA / NT;
+  static constexpr int MINB = GX_R16_MINB * 256 / CTA;   // resident CTAs per SM the registers are sized for
+};
+
+template <int NT, int CTA>
+__device__ __forceinline__ void group_sync(int g)
+{
+  if constexpr (NT == 32) __syncwarp();
+  else if constexpr (NT == CTA) __syncthreads();
+  else asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(NT) : "memory");
+}
+
+template <int F, int CPLX>
+__global__ void __launch_bounds__(R16Launch<F>::CTA, R16Launch<F>::MINB)
+fstep_r16_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays S,
+                 const BlockParam *__restrict__ bp, int nblk, int blocks_per_cta, int tabstride,
+                 float2 *__restrict__ spec)
+{
+  using Pl = r16::Plan<F>;
+  constexpr int NT = Pl::NT, CTA = R16Launch<F>::CTA, G = R16Launch<F>::G;
+  constexpr int NCH = CPLX ? F : F / 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ float s_lut[256];
+  const int s = blockIdx.y;
+  const int tid = threadIdx.x, g = tid / NT, j = tid % NT;
+  const DevStation &st = stations[s];
+  const int Sd = J.stride, lgS = J.lgstride, nfr = J.nfr, half = J.half;
+  for (int i = tid; i < 256; i += CTA) s_lut[i] = J.lut[i];
+  __syncthreads();
+
+  float2 *sm = reinterpret_cast<float2 *>(smem_raw) + (size_t)g * (Pl::SMEM + tabstride);
+  float2 *rs = sm + Pl::SMEM;  // S
+  float2 *rp = rs + Sd;        // nfr
+  float2 *fs = rp + nfr;       // S
+  float2 *fp = fs + Sd;        // half
+  const float2 *__restrict__ twg = J.twiddle;
+  auto tw = [twg](int m) { return __ldg(&twg[m]); };
+
+  const uint8_t *data = S.data[s];
+  const int fsamp = J.framesamples;
+  const int bits_ts = J.nbands * J.nbits * (CPLX ? 2 : 1);
+  const int cmask = (1 << J.nbits) - 1;
+  const bool byte_pairs = CPLX && J.nbits == 8;   // (re, im) = one 16-bit word
+  const int b0 = blockIdx.x * blocks_per_cta;
+  const int nbk = min(blocks_per_cta, nblk - b0);
+  const int nitems = nbk * J.nbands;
+  for (int it = g; it < nitems; it += G) {
+    const int bi = b0 + it / J.nbands;
+    const int bd = it % J.nbands;
+    const BlockParam P = bp[(size_t)s * nblk + bi];
+    const int lf = st.band_localfreq[bd];
+    const int f = st.freq_index[lf];
+    const int row = st.band_input[bd];
+    float2 *dst = spec + ((size_t)f * nblk + bi) * J.ninputs * NCH;
+    if (P.state == 0) {
+      for (int c = j; c < NCH; c += NT) dst[spec_offset(J, row, c)] = make_float2(0.f, 0.f);
+      continue;
+    }
+    const int ps = st.band_polb[bd] ? 1 : 0;
+    group_sync<NT, CTA>(g);   // the group's previous item is done with the tables and the exchange buffer
+    for (int e = j; e < Sd + nfr; e += NT) {
+      const float2 v = fringe_entry(J, st, lf, e, P);
+      if (e < Sd) rs[e] = v;
+      else rp[e - Sd] = v;
+    }
+    for (int e = j; e < Sd + half; e += NT) {
+      const float2 v = frac_entry(J, st, lf, ps, e, P);
+      if (e < Sd) fs[e] = v;
+      else fp[e - Sd] = v;
+    }
+    group_sync<NT, CTA>(g);
+
+    // decode + rotate: sample n = j + NT t of the block; frame q and in-frame sample r advance incrementally
+    float2 v[16];
+    {
+      const int smp0 = P.nearestsample + j;
+      int q = smp0 / fsamp;
+      int r = smp0 - q * fsamp;
+      q -= P.fr0;
+      const int bitband = bd * (CPLX ? 2 : 1) * J.nbits;
+#pragma unroll
+      for (int t = 0; t < 16; t++) {
+        const int n = j + NT * t;
+        float2 u = make_float2(0.f, 0.f);
+        if ((P.validmask >> q) & 1ull) {
+          const uint8_t *payload = data + ((long long)P.fr0 + q) * J.framebytes + 32;
+          const int bit0 = r * bits_ts + bitband;   // < 8 * payload bytes
+          if (byte_pairs) {
+            const unsigned int w = __ldg(reinterpret_cast<const unsigned short *>(payload + (bit0 >> 3)));
+            u.x = s_lut[w & 255u];
+            u.y = s_lut[w >> 8];
+          } else {
+            u.x = s_lut[(__ldg(payload + (bit0 >> 3)) >> (bit0 & 7)) & cmask];
+            if (CPLX) {
+              const int bit1 = bit0 + J.nbits;
+              u.y = s_lut[(__ldg(payload + (bit1 >> 3)) >> (bit1 & 7)) & cmask];
+            }
+          }
+        }
+        const int k = n & (Sd - 1), jj = n >> lgS;
+        const float2 rot = (jj == 0) ? rs[k] : cmul_exact(rs[k], rp[jj]);
+        v[t] = CPLX ? cmul(rot, u) : make_float2(u.x * rot.x, u.x * rot.y);
+        r += NT;
+        while (r >= fsamp) { r -= fsamp; q++; }
+      }
+    }
+
+    // FFT: radix-16 passes, exchanges through the padded buffer, then the final radix
+    int Ns = 1;
+#pragma unroll
+    for (int pass = 0; pass < Pl::L; pass++) {
+      r16::pass16<F>(v, j, Ns, tw);
+      if (!(pass == Pl::L - 1 && Pl::R0 == 1)) {
+        group_sync<NT, CTA>(g);
+        r16::store16(v, j, Ns, sm);
+        group_sync<NT, CTA>(g);
+        r16::load16<F>(v, j, sm);
+      }
+      Ns *= 16;
+    }
+    if constexpr (Pl::R0 > 1) r16::final_pass<F, Pl::R0>(v, j, tw);
+
+    // register t holds bin j + NT t: sideband selection (mode.cpp:1185-1217) and correction
+    const int lsb = st.lsb[lf];
+#pragma unroll
+    for (int t = 0; t < 16; t++) {
+      const int bin = j + NT * t;
+      float2 val = v[t];
+      int c;
+      if (!CPLX) {
+        if (lsb ? (t < 8) : (t >= 8)) continue;   // NT * 8 = F / 2 = NCH
+        c = lsb ? bin - NCH : bin;
+      } else if (!lsb) {
+        c = bin;
+      } else {
+        c = bin == 0 ? 0 : F - bin;
+        if (bin != 0) val.y = -val.y;
+      }
+      dst[spec_offset(J, row, c)] = cmul(val, cmul_exact(fs[c & (Sd - 1)], fp[c >> lgS]));
+    }
+  }
+}
+
+// --------------------------------------------------------------------------
 static bool use_warp_kernel(const DevJob &J) { return J.fftlen >= 128 && J.fftlen <= 1024; }
 
 static int warp_stride(const DevJob &J)
@@ -567,8 +727,29 @@ static int warp_stride(const DevJob &J)
   return (w + 1) & ~1;   // keep each warp's region 16-byte aligned
 }
 
+// Register-resident radix-16 kernel for the transform lengths it is built for.
+static bool use_r16_kernel(const DevJob &J)
+{
+  const char *e = getenv("GX_FSTEP_R16_MIN");   // smallest length routed to it (tuning runs)
+  const int fmin = e ? atoi(e) : 2048;
+  return J.fftlen >= fmin && J.fftlen >= 512 && J.fftlen <= 8192;
+}
+
+static int r16_tabstride(const DevJob &J)
+{
+  return (2 * J.stride + J.nfr + (J.half > 0 ? J.half : 1) + 1) & ~1;
+}
+
+static int r16_groups(const DevJob &J)
+{
+  const int nt = J.fftlen / 16;
+  return nt >= 256 ? 1 : 256 / nt;
+}
+
 size_t fstep_smem_bytes(const DevJob &J, int nrf, int nslots)
 {
+  if (use_r16_kernel(J))
+    return (size_t)r16_groups(J) * (J.fftlen + J.fftlen / 16 + r16_tabstride(J)) * sizeof(float2);
   if (use_warp_kernel(J)) return (size_t)(kWarpKernelThreads / 32) * warp_stride(J) * sizeof(float2);
   size_t b = (size_t)nslots * 2 * J.fftlen * sizeof(float2);
   b += (size_t)nrf * (J.stride + J.nfr) * sizeof(float2);
@@ -594,6 +775,24 @@ cudaError_t fstep_launch(const DevJob &J, const DevStation *stations, int maxnrf
     blockparams_kernel<<<grid, 128, 0, st>>>(J, S, blk0, nblk, bp, weights);
   }
   const size_t sm = fstep_smem_bytes(J, maxnrf, nslots);
+  if (use_r16_kernel(J)) {
+    const int G = r16_groups(J);
+    // at least four items per group, so that groups overlap their barriers
+    const int bpc = std::max(1, (4 * G + J.nbands - 1) / J.nbands);
+    dim3 grid((nblk + bpc - 1) / bpc, J.nstations);
+    const int ts = r16_tabstride(J);
+#define GX_R16_CASE(FLV, CX)                                                                          \
+    if (J.fftlen == FLV && J.cplx == CX) {                                                            \
+      static size_t have = 48 * 1024;                                                                 \
+      cudaError_t e = opt_in(fstep_r16_kernel<FLV, CX>, sm, have);                                    \
+      if (e != cudaSuccess) return e;                                                                 \
+      fstep_r16_kernel<FLV, CX><<<grid, R16Launch<FLV>::CTA, sm, st>>>(J, stations, S, bp, nblk, bpc, ts, spec); \
+      return cudaGetLastError();                                                                      \
+    }
+    GX_R16_CASE(512, 0) GX_R16_CASE(1024, 0) GX_R16_CASE(2048, 0) GX_R16_CASE(4096, 0) GX_R16_CASE(8192, 0)
+    GX_R16_CASE(512, 1) GX_R16_CASE(1024, 1) GX_R16_CASE(2048, 1) GX_R16_CASE(4096, 1) GX_R16_CASE(8192, 1)
+#undef GX_R16_CASE
+  }
   if (use_warp_kernel(J)) {
     // enough items per CTA that each warp has several (block, band) items
     const int bpc = (J.nbands >= 8) ? 2 : 8;

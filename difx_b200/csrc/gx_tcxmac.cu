@@ -16,10 +16,11 @@
 // i.e. three 128x128x16 real products per complex 128x128 Hermitian update
 // (the fourth, Xr Xi^T, is P transposed and is formed in the finalising pass).
 //
-// Data path per CTA: the spectra of its channel pair are stored as one
-// contiguous 2 KB row per block (layout [freq][block][chan/2][input][2] float2,
-// written so by the F-step), fetched by bulk copies (cp.async.bulk, no
-// multicast) into a 4-stage FP32 ring; all threads scale each value by a power
+// Data path per CTA: the spectra spec[freq][block][input][chan] (float2, as the
+// F-step writes them) are read as a 4-D FP32 tensor; one TMA tile load (no
+// multicast) per 16 blocks fetches the 4 floats of the CTA's channel pair for
+// all 128 inputs ([block][input][16 bytes], blocks past the chunk read as
+// zeros) into a 4-stage FP32 ring; all threads scale each value by a power
 // of two per (input, channel), round it to FP16 and store it, transposed to
 // K-major, into the canonical no-swizzle core-matrix layout of the MMA operand
 // [Xi ; Xr] (256 rows x 16 blocks); one thread issues the MMAs and commits them
@@ -27,14 +28,20 @@
 // remainder lo = fp16(x*s - hi) is kept too and the products hi*hi + hi*lo +
 // lo*hi are accumulated (lo*lo, below 2^-22 relative, is dropped).
 //
-// The accumulators leave tensor memory once per chunk: each thread reads its
-// lane (row a) and adds 16-column slices into acc[freq][chan/2][a][b][2]
-// (Re and P arrays), so partial sums across chunks and K-split slices stay FP32.
+// The accumulators leave tensor memory once per chunk.  P of both channels is
+// parked in shared memory (rows padded to 129 floats, conflict-free by row and
+// by column), so that each thread, holding row a of Re, forms
+// Im V(a, b) = P(a, b) - P(b, a), divides out the operand scales and adds the
+// complex visibilities of both channels, one float4 per (a, b), into
+// acc[freq][chan/2][a][b]; partial sums across chunks and K-split slices stay
+// FP32 and the finalising pass reads whole rows.
 //
 // Every wait on an mbarrier is bounded in time; on expiry the kernel records a
 // nonzero status in *err, drains its own copies and MMAs (again bounded),
 // releases its tensor memory and returns.
 #include <cstdint>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include "gx_xstep.h"
@@ -44,7 +51,7 @@ namespace {
 
 constexpr int kNI = 128;                     // inputs per frequency = MMA M
 constexpr int kKT = 16;                      // FFT blocks per K-tile = one MMA K step for FP16
-constexpr int kStages = 4;                   // FP32 staging ring depth (bulk copies in flight)
+constexpr int kStages = 4;                   // FP32 staging ring depth (tile loads in flight)
 constexpr int kOpStages = 2;                 // FP16 operand stages
 constexpr int kThreads = 256;
 constexpr uint32_t kTmemCols = 512;          // 2 channels x (128 Re + 128 P) FP32 columns
@@ -54,6 +61,9 @@ constexpr uint32_t kLBO = 128;               // byte step between the two 8-bloc
 constexpr uint32_t kSBO = (kKT / 8) * 128;   // byte step between 8-row groups
 constexpr uint32_t kOpChanBytes = 2 * kNI * kKT * 2;      // [Xi ; Xr]: 256 rows x 16 FP16 = 8 KB
 constexpr uint32_t kXrOffset = (kNI / 8) * kSBO;          // rows 128.. (Xr) start here
+constexpr int kPRow = kNI + 1;               // padded row of the P matrices parked in shared memory
+static_assert((2 * kNI * kPRow + 2 * kNI) * 4 <= kStages * kStageBytes + kOpStages * 2 * kOpChanBytes,
+              "epilogue tables must fit in the staging ring and operand stages");
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
@@ -101,10 +111,14 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
   return true;
 }
 
-__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
+// One tile of a 4-D tensor map (no multicast) into shared memory; coordinates innermost first.
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap *map, int x, int y, int zc, int w,
+                                            uint32_t bar)
 {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-               "l"(src), "r"(bytes), "r"(bar)
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(zc), "r"(w), "r"(bar)
                : "memory");
 }
 
@@ -194,9 +208,8 @@ __device__ __forceinline__ void split2(float a, float b, uint32_t &hi, uint32_t 
 
 template <bool HILO>
 __global__ void __launch_bounds__(kThreads, 1)
-xmac_tc_kernel(const float2 *__restrict__ spec, int nblk, int NP, int ks, const float *__restrict__ scale,
-               float *__restrict__ acc_re, float *__restrict__ acc_p, size_t slice_floats, int accumulate,
-               int *__restrict__ err)
+xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, int nfreqs, int ks,
+               const float *__restrict__ scale, float4 *__restrict__ acc, int accumulate, int *__restrict__ err)
 {
   constexpr uint32_t kParts = HILO ? 2 : 1;
   constexpr uint32_t kOpStageBytes = kParts * 2 * kOpChanBytes;
@@ -234,17 +247,14 @@ xmac_tc_kernel(const float2 *__restrict__ spec, int nblk, int NP, int ks, const 
   const float s1 = scale[((size_t)f * kNI + r) * N + 2 * p + 1];
   const uint32_t row_off = (uint32_t)(r >> 3) * kSBO + (uint32_t)g * kLBO + (uint32_t)(r & 7) * 16;
 
-  // tile u of this slice into staging stage u % kStages (thread 0 only)
+  // tile u of this slice into staging stage u % kStages (thread 0 only): channels 2p, 2p+1
+  // (4 floats) of all 128 rows of kKT blocks; blocks past the chunk read as zeros
   auto issue = [&](int u) {
     const int st = u % kStages;
     const int kb0 = (t0 + u) * kKT;
-    const int kv = min(kKT, nblk - kb0);
     const uint32_t bar = smem_u32(bars + st);
-    mbar_expect_tx(bar, (uint32_t)kv * kRowBytes);
-    for (int k = 0; k < kv; k++) {
-      const float2 *src = spec + (((size_t)f * nblk + kb0 + k) * NP + p) * (size_t)(2 * kNI);
-      bulk_load(smem_u32(staging + st * kStageBytes + k * kRowBytes), src, kRowBytes, bar);
-    }
+    mbar_expect_tx(bar, kStageBytes);
+    tma_load_4d(smem_u32(staging + st * kStageBytes), &spec_map, 4 * p, 0, kb0, f, bar);
   };
 
   int issued = 0, t = 0;
@@ -335,36 +345,61 @@ xmac_tc_kernel(const float2 *__restrict__ spec, int nblk, int NP, int ks, const 
   tc_fence_after();
 
   if (!*s_abort) {
-    // warp w reads lanes 32 (w % 4) .. +31 (rows a); warps 0-3 the Re columns, 4-7 the P columns
+    // warp w reads lanes 32 (w % 4) .. +31, i.e. row a of both accumulators
     const int q = warp & 3, h = warp >> 2;
     const int a = 32 * q + lane;
-    float *out = (h == 0 ? acc_re : acc_p) + (size_t)z * slice_floats +
-                 (((size_t)f * NP + p) * kNI + a) * (size_t)(2 * kNI);
-    const uint32_t lane_addr = tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)h * 128u;
+    const uint32_t lane_addr = tmem + ((uint32_t)(32 * q) << 16);
+    float4 *orow = acc + (((size_t)z * nfreqs + f) * NP + p) * kNI * kNI + (size_t)a * kNI;
+    if (nt == 0) {
+      // empty slice: its share is zero
+      if (!accumulate)
+        for (int b = h * 64; b < h * 64 + 64; b++) orow[b] = make_float4(0.f, 0.f, 0.f, 0.f);
+    } else {
+      // the staging ring and operand stages are idle now: P of both channels, then 1 / scale per (b, channel)
+      float *sP = reinterpret_cast<float *>(staging);             // [2][128][kPRow]
+      float *sInv = sP + 2 * kNI * kPRow;                          // [2][128]
+      if (h == 1) {
 #pragma unroll 1
-    for (int cb = 0; cb < kNI / 16; cb++) {
-      float v0[16], v1[16];
-      if (nt > 0) {
-        tmem_ld16(lane_addr + (uint32_t)cb * 16u, v0);
-        tmem_ld16(lane_addr + 256u + (uint32_t)cb * 16u, v1);
-        tmem_ld_wait();
-      } else {
+        for (int cb = 0; cb < kNI / 16; cb++) {
+          float v0[16], v1[16];
+          tmem_ld16(lane_addr + 128u + (uint32_t)cb * 16u, v0);
+          tmem_ld16(lane_addr + 384u + (uint32_t)cb * 16u, v1);
+          tmem_ld_wait();
 #pragma unroll
-        for (int i = 0; i < 16; i++) v0[i] = v1[i] = 0.f;
-      }
-      if (nt == 0 && accumulate) continue;
-      float4 *o4 = reinterpret_cast<float4 *>(out + cb * 32);
-#pragma unroll
-      for (int i = 0; i < 8; i++) {
-        float4 w = make_float4(v0[2 * i], v1[2 * i], v0[2 * i + 1], v1[2 * i + 1]);
-        if (accumulate) {
-          const float4 old = o4[i];
-          w.x += old.x;
-          w.y += old.y;
-          w.z += old.z;
-          w.w += old.w;
+          for (int i = 0; i < 16; i++) {
+            sP[a * kPRow + cb * 16 + i] = v0[i];
+            sP[(kNI + a) * kPRow + cb * 16 + i] = v1[i];
+          }
         }
-        o4[i] = w;
+      } else {
+        sInv[a] = 1.0f / s0;          // operand scales are powers of two: exact
+        sInv[kNI + a] = 1.0f / s1;
+      }
+      __syncthreads();
+      const float ia0 = 1.0f / s0, ia1 = 1.0f / s1;
+#pragma unroll 1
+      for (int cb = 0; cb < 4; cb++) {
+        const int b0 = h * 64 + cb * 16;
+        float r0[16], r1[16];
+        tmem_ld16(lane_addr + (uint32_t)b0, r0);
+        tmem_ld16(lane_addr + 256u + (uint32_t)b0, r1);
+        tmem_ld_wait();
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+          const int b = b0 + i;
+          const float i0 = ia0 * sInv[b], i1 = ia1 * sInv[kNI + b];
+          const float im0 = sP[a * kPRow + b] - sP[b * kPRow + a];
+          const float im1 = sP[(kNI + a) * kPRow + b] - sP[(kNI + b) * kPRow + a];
+          float4 w = make_float4(r0[i] * i0, im0 * i0, r1[i] * i1, im1 * i1);
+          if (accumulate) {
+            const float4 old = orow[b];
+            w.x += old.x;
+            w.y += old.y;
+            w.z += old.z;
+            w.w += old.w;
+          }
+          orow[b] = w;
+        }
       }
     }
   } else if (tid == 0) {
@@ -377,30 +412,46 @@ xmac_tc_kernel(const float2 *__restrict__ spec, int nblk, int NP, int ks, const 
   if (warp == 0) tmem_dealloc(tmem, kTmemCols);
 }
 
-// One thread per (entry, channel): Re and Im of input pair (a, b) from the Re
-// and P accumulators summed over the K-split slices, unscaled.
-__global__ void finalise_tc_kernel(const TcProdEntry *__restrict__ prods, int nprods, const float *__restrict__ acc_re,
-                                   const float *__restrict__ acc_p, int ks, size_t slice_floats, int N,
-                                   const float *__restrict__ scale, float2 *__restrict__ results)
+// One CTA per (freq, a) row that has visibility rows: passes of kFinPairs
+// channel pairs stage acc[z][freq][p][a][bmin..127] (contiguous, summed over
+// the K-split slices) in shared memory, then every entry (a, b) of the row
+// writes its 2 kFinPairs channels as one contiguous run of the result array.
+constexpr int kFinPairs = 16;
+
+__global__ void __launch_bounds__(256)
+finalise_tc_kernel(const TcProdEntry *__restrict__ prods, const TcRowEntry *__restrict__ rows,
+                   const float4 *__restrict__ acc, int nfreqs, int NP, int ks, float2 *__restrict__ results)
 {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (long long)nprods * N) return;
-  const int e = (int)(i / N), c = (int)(i % N);
-  const TcProdEntry P = prods[e];
-  const int NP = N / 2, cp = c >> 1, ce = c & 1;
-  const size_t base = ((size_t)P.freq * NP + cp) * kNI * kNI * 2;
-  const size_t iab = base + ((size_t)P.a * kNI + P.b) * 2 + ce;
-  const size_t iba = base + ((size_t)P.b * kNI + P.a) * 2 + ce;
-  float re = 0.f, pab = 0.f, pba = 0.f;
-  for (int z = 0; z < ks; z++) {
-    re += acc_re[z * slice_floats + iab];
-    pab += acc_p[z * slice_floats + iab];
-    pba += acc_p[z * slice_floats + iba];
+  __shared__ float4 sV[kFinPairs][kNI];
+  const TcRowEntry R = rows[blockIdx.x];
+  const size_t slice = (size_t)nfreqs * NP * kNI * kNI;
+  const int nb = kNI - R.bmin;
+  const int ne = R.end - R.start;
+  for (int p0 = 0; p0 < NP; p0 += kFinPairs) {
+    const int np = min(kFinPairs, NP - p0);
+    for (int i = threadIdx.x; i < np * nb; i += blockDim.x) {
+      const int pp = i / nb, b = R.bmin + i % nb;
+      const size_t off = (((size_t)R.freq * NP + p0 + pp) * kNI + R.a) * kNI + b;
+      float4 v = acc[off];
+      for (int z = 1; z < ks; z++) {
+        const float4 u = acc[z * slice + off];
+        v.x += u.x;
+        v.y += u.y;
+        v.z += u.z;
+        v.w += u.w;
+      }
+      sV[pp][b] = v;
+    }
+    __syncthreads();
+    const int nc = 2 * np;
+    for (int i = threadIdx.x; i < ne * nc; i += blockDim.x) {
+      const TcProdEntry P = prods[R.start + i / nc];
+      const int cc = i % nc;
+      const float4 v = sV[cc >> 1][P.b];
+      results[P.result_offset + 2 * p0 + cc] = (cc & 1) ? make_float2(v.z, v.w) : make_float2(v.x, v.y);
+    }
+    __syncthreads();
   }
-  const float sa = scale[((size_t)P.freq * kNI + P.a) * N + c];
-  const float sb = scale[((size_t)P.freq * kNI + P.b) * N + c];
-  const float inv = 1.0f / (sa * sb);
-  results[P.result_offset + c] = make_float2(re * inv, (pab - pba) * inv);
 }
 
 }  // namespace
@@ -412,10 +463,30 @@ size_t xmac_tc_smem_bytes(bool hilo)
 }
 
 cudaError_t xmac_tc_launch(const float2 *spec, int nblk, int N, int nfreqs, int ks, bool hilo, const float *scale,
-                           float *acc_re, float *acc_p, size_t slice_floats, int accumulate, int *err,
-                           cudaStream_t st)
+                           float4 *acc, int accumulate, int *err, cudaStream_t st)
 {
   if (nblk <= 0) return cudaSuccess;
+  // spec[freq][block][row][channel] float2 as a 4-D FP32 tensor (innermost first):
+  // {2N floats, 128 rows, nblk blocks, nfreqs}; box {4 floats, 128 rows, kKT blocks, 1}
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess) return e;
+    if (q != cudaDriverEntryPointSuccess || !fn) return cudaErrorNotSupported;
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  CUtensorMap map;
+  const cuuint64_t dims[4] = {(cuuint64_t)(2 * N), (cuuint64_t)kNI, (cuuint64_t)nblk, (cuuint64_t)nfreqs};
+  const cuuint64_t strides[3] = {(cuuint64_t)(2 * N) * 4, (cuuint64_t)(2 * N) * 4 * kNI,
+                                 (cuuint64_t)(2 * N) * 4 * kNI * nblk};
+  const cuuint32_t box[4] = {4, (cuuint32_t)kNI, (cuuint32_t)kKT, 1};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult cr = encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float2 *>(spec), dims, strides, box, estr,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (cr != CUDA_SUCCESS) return cudaErrorInvalidValue;
   const size_t sm = xmac_tc_smem_bytes(hilo);
   dim3 grid(N / 2, nfreqs, ks);
   if (hilo) {
@@ -425,8 +496,7 @@ cudaError_t xmac_tc_launch(const float2 *spec, int nblk, int N, int nfreqs, int 
       if (e != cudaSuccess) return e;
       opted = true;
     }
-    xmac_tc_kernel<true><<<grid, kThreads, sm, st>>>(spec, nblk, N / 2, ks, scale, acc_re, acc_p, slice_floats,
-                                                      accumulate, err);
+    xmac_tc_kernel<true><<<grid, kThreads, sm, st>>>(map, nblk, N / 2, nfreqs, ks, scale, acc, accumulate, err);
   } else {
     static bool opted = false;
     if (!opted) {
@@ -434,19 +504,16 @@ cudaError_t xmac_tc_launch(const float2 *spec, int nblk, int N, int nfreqs, int 
       if (e != cudaSuccess) return e;
       opted = true;
     }
-    xmac_tc_kernel<false><<<grid, kThreads, sm, st>>>(spec, nblk, N / 2, ks, scale, acc_re, acc_p, slice_floats,
-                                                       accumulate, err);
+    xmac_tc_kernel<false><<<grid, kThreads, sm, st>>>(map, nblk, N / 2, nfreqs, ks, scale, acc, accumulate, err);
   }
   return cudaGetLastError();
 }
 
-cudaError_t finalise_tc_launch(const TcProdEntry *prods, int nprods, const float *acc_re, const float *acc_p, int ks,
-                               size_t slice_floats, int N, const float *scale, float2 *results, cudaStream_t st)
+cudaError_t finalise_tc_launch(const TcProdEntry *prods, const TcRowEntry *rows, int nrows, const float4 *acc,
+                               int nfreqs, int N, int ks, float2 *results, cudaStream_t st)
 {
-  if (nprods <= 0) return cudaSuccess;
-  const long long n = (long long)nprods * N;
-  finalise_tc_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(prods, nprods, acc_re, acc_p, ks, slice_floats, N,
-                                                                  scale, results);
+  if (nrows <= 0) return cudaSuccess;
+  finalise_tc_kernel<<<nrows, 256, 0, st>>>(prods, rows, acc, nfreqs, N / 2, ks, results);
   return cudaGetLastError();
 }
 

@@ -44,15 +44,20 @@ cudaError_t xmac_fp32_launch(const float2 *spec, int nblk, int NI, int N, int nf
                              cudaStream_t st);
 cudaError_t weights_launch(const float *w, int nblk, int nstations, const int2 *pairs, int npairs, float *wacc,
                            cudaStream_t st);
+// Entries [start, end) of the tensor-core product table (sorted by freq, then a)
+// share row a of freq; bmin is their smallest b.
+struct TcRowEntry {
+  int freq, a, bmin, start, end;
+};
+
 // Tensor-core X-step over spectra in the channel-pair layout
-// [freq][block][N/2][128 inputs][2]; acc_re / acc_p hold [freq][N/2][128][128][2]
-// floats per K-split slice (slice_floats apart).
+// [freq][block][N/2][128 inputs][2]; acc holds, per K-split slice,
+// [freq][N/2][a][b] float4 = (Re, Im) of both channels of the pair, unscaled.
 size_t xmac_tc_smem_bytes(bool hilo);
 cudaError_t xmac_tc_launch(const float2 *spec, int nblk, int N, int nfreqs, int ks, bool hilo, const float *scale,
-                           float *acc_re, float *acc_p, size_t slice_floats, int accumulate, int *err,
-                           cudaStream_t st);
-cudaError_t finalise_tc_launch(const TcProdEntry *prods, int nprods, const float *acc_re, const float *acc_p, int ks,
-                               size_t slice_floats, int N, const float *scale, float2 *results, cudaStream_t st);
+                           float4 *acc, int accumulate, int *err, cudaStream_t st);
+cudaError_t finalise_tc_launch(const TcProdEntry *prods, const TcRowEntry *rows, int nrows, const float4 *acc,
+                               int nfreqs, int N, int ks, float2 *results, cudaStream_t st);
 constexpr int kTcInputs = 128;   // inputs per frequency of the tensor-core X-step (the MMA M)
 
 cudaError_t finalise_launch(const ProdEntry *prods, int nprods, const float2 *acc, int ks, size_t ks_stride, int N,

@@ -48,6 +48,19 @@ def spec_c2small(**kw) -> JobSpec:
     return JobSpec(**base)
 
 
+def spec_long(name: str, nbits: int, sampling: str, sideband: str, nchan: int, seed: int, **kw) -> JobSpec:
+    """Long transforms (2048- to 8192-point FFTs): 3 stations, 2 x 16 MHz subbands, 2 pols, 64 FFT blocks."""
+    f0 = 6000.0 if sampling == "COMPLEX" else 8400.0
+    if sideband == "L":
+        f0 += 16.0
+    fft_us = nchan / 16.0 if sampling == "COMPLEX" else 2 * nchan / 32.0
+    base = dict(name=name, nstations=3, subbands=[Subband(f0 + 16 * i, 16.0, sideband, nchan) for i in range(2)],
+                nbits=nbits, sampling=sampling, subint_ns=int(64 * fft_us * 1000), execute_seconds=2,
+                max_delay_us=200.0, seed=seed)
+    base.update(kw)
+    return JobSpec(**base)
+
+
 @dataclasses.dataclass
 class Prepared:
     spec: JobSpec

@@ -57,6 +57,11 @@ CASES = {
     "cplx8": lambda: (jobs.spec_cplx8(), dict()),
     "cplx8_invalid": lambda: (jobs.spec_cplx8(name="cx8bad", seed=23), dict(invalid_frac=0.08)),
     "c2small": lambda: (jobs.spec_c2small(), dict(invalid_frac=0.01)),
+    # long transforms (register-resident radix-16 F-step)
+    "cplx8_4096": lambda: (jobs.spec_long("cx8l", 8, "COMPLEX", "U", 4096, 41), dict(invalid_frac=0.03)),
+    "cplx8_4096_lsb": lambda: (jobs.spec_long("cx8ll", 8, "COMPLEX", "L", 4096, 43), dict(invalid_frac=0.03)),
+    "real2_8192": lambda: (jobs.spec_long("r2x", 2, "REAL", "U", 4096, 47), dict(invalid_frac=0.03)),
+    "real2_2048_lsb": lambda: (jobs.spec_long("r2m", 2, "REAL", "L", 1024, 53), dict(invalid_frac=0.03)),
 }
 
 
