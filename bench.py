@@ -97,7 +97,11 @@ def build_input(spec: JobSpec, sub_start_ns: int, rho=0.02, invalid_frac=0.01, t
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """nvidia-smi clocks and throttle reasons during the timed region.
+
+    Started before the warm-up (so that nvidia-smi's start-up does not fall in
+    the timed region); mark() brackets the timed region and summary() keeps
+    the samples taken inside it (at least the first three from its start)."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
@@ -105,22 +109,29 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
-        self.lines = []
+        self.lines = []      # (monotonic time, csv line)
+        self.window = [None, None]
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.monotonic()
+            while not self.lines and time.monotonic() - t0 < 10.0:
+                time.sleep(0.05)
         except Exception:
             self.proc = None
         return self
 
+    def mark(self, which: int):
+        self.window[which] = time.monotonic()
+
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
 
     def __exit__(self, *a):
         if self.proc:
@@ -133,7 +144,13 @@ class ClockSampler:
     def summary(self):
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in self.lines:
+        t0, t1 = self.window
+        lines = self.lines
+        if t0 is not None:
+            after = [x for x in lines if x[0] >= t0]
+            inside = [x for x in after if t1 is None or x[0] <= t1 + 0.1]
+            lines = inside if len(inside) >= 3 else after[:3]
+        for _, l in lines:
             p = [x.strip() for x in l.split(",")]
             if len(p) < 9:
                 continue
@@ -237,6 +254,9 @@ def time_device(corr, sd_dev, dres, stream, steps, warmup, local, dist=None, clo
     """Device-resident steps on one stream: (ms for all steps, stage ms of the last step, launches, clocks)."""
     import torch
     sptr = stream.cuda_stream
+    clk = ClockSampler(local) if clocks else None
+    if clk:
+        clk.__enter__()
     for _ in range(warmup):
         corr.subint_device(sd_dev, dres.data_ptr(), sptr)
     corr.synchronize()
@@ -245,11 +265,10 @@ def time_device(corr, sd_dev, dres, stream, steps, warmup, local, dist=None, clo
         dist.barrier()
     torch.cuda.synchronize()
     launches = 0
-    clk = ClockSampler(local) if clocks else None
-    if clk:
-        clk.__enter__()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    if clk:
+        clk.mark(0)
     ev0.record(stream)
     for _ in range(steps):
         corr.subint_device(sd_dev, dres.data_ptr(), sptr)
@@ -257,6 +276,7 @@ def time_device(corr, sd_dev, dres, stream, steps, warmup, local, dist=None, clo
     ev1.record(stream)
     ev1.synchronize()
     if clk:
+        clk.mark(1)
         clk.__exit__()
     corr.synchronize()
     dev_ms = ev0.elapsed_time(ev1)

@@ -113,15 +113,32 @@ struct Plan {
 };
 
 // Radix-16 pass of stride Ns: twiddle (Ns > 1) and transform in registers.
-// tw[m] = exp(-2 pi i m / F).
+// tw[m] = exp(-2 pi i m / F).  The twiddles w^r, r = 1..15, of a thread come
+// from four table entries (w, w^2, w^4, w^8) and at most three products each.
 template <int F, typename TW>
 __host__ __device__ __forceinline__ void pass16(float2 (&v)[16], int j, int Ns, TW tw)
 {
   if (Ns > 1) {
     const int m = j & (Ns - 1);
-    const int step = F / (16 * Ns);
+    const int step = m * (F / (16 * Ns));
+    float2 w[16];
+    w[1] = tw(step);
+    w[2] = tw(2 * step);
+    w[4] = tw(4 * step);
+    w[8] = tw(8 * step);
+    w[3] = mul(w[2], w[1]);
+    w[5] = mul(w[4], w[1]);
+    w[6] = mul(w[4], w[2]);
+    w[7] = mul(w[4], w[3]);
+    w[9] = mul(w[8], w[1]);
+    w[10] = mul(w[8], w[2]);
+    w[11] = mul(w[8], w[3]);
+    w[12] = mul(w[8], w[4]);
+    w[13] = mul(w[8], w[5]);
+    w[14] = mul(w[8], w[6]);
+    w[15] = mul(w[8], w[7]);
 #pragma unroll
-    for (int r = 1; r < 16; r++) v[r] = mul(v[r], tw(m * r * step));
+    for (int r = 1; r < 16; r++) v[r] = mul(v[r], w[r]);
   }
   dft16(v);
 }

@@ -569,7 +569,7 @@ fstep_cta_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays
 // after the sideband selection and fractional-sample correction.  A CTA holds
 // G = CTA / NT groups; groups synchronise on their own named barrier.
 #ifndef GX_R16_MINB
-#define GX_R16_MINB 3
+#define GX_R16_MINB 4
 #endif
 template <int F>
 struct R16Launch {
@@ -585,6 +585,101 @@ __device__ __forceinline__ void group_sync(int g)
   if constexpr (NT == 32) __syncwarp();
   else if constexpr (NT == CTA) __syncthreads();
   else asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(NT) : "memory");
+}
+
+// Samples x[j + NT t] (t = 0..15) of band bd of the block described by P,
+// decoded and fringe-rotated (mode.cpp:1160-1183): frame q and in-frame
+// sample r advance incrementally; all 16 raw loads are issued before use.
+template <int F, int CPLX>
+__device__ __forceinline__ void r16_decode_rotate(const DevJob &J, const uint8_t *__restrict__ data,
+                                                  const BlockParam &P, int bd, int j, const float2 *rs,
+                                                  const float2 *rp, const float *s_lut, float2 (&v)[16])
+{
+  constexpr int NT = F / 16;
+  const int fsamp = J.framesamples;
+  const int bits_ts = J.nbands * J.nbits * (CPLX ? 2 : 1);
+  const int cmask = (1 << J.nbits) - 1;
+  const bool byte_pairs = CPLX && J.nbits == 8;   // (re, im) = one 16-bit word
+  const int smp0 = P.nearestsample + j;
+  int q = smp0 / fsamp;
+  int r = smp0 - q * fsamp;
+  q -= P.fr0;
+  const int bitband = bd * (CPLX ? 2 : 1) * J.nbits;
+  unsigned int raw[16];
+#pragma unroll
+  for (int t = 0; t < 16; t++) {
+    raw[t] = 0xFFFFFFFFu;   // invalid frame: decodes to zero
+    if ((P.validmask >> q) & 1ull) {
+      const uint8_t *payload = data + ((long long)P.fr0 + q) * J.framebytes + 32;
+      const int bit0 = r * bits_ts + bitband;   // < 8 * payload bytes
+      if (byte_pairs) {
+        raw[t] = __ldg(reinterpret_cast<const unsigned short *>(payload + (bit0 >> 3)));
+      } else {
+        unsigned int w = (__ldg(payload + (bit0 >> 3)) >> (bit0 & 7)) & cmask;
+        if (CPLX) {
+          const int bit1 = bit0 + J.nbits;
+          w |= ((__ldg(payload + (bit1 >> 3)) >> (bit1 & 7)) & cmask) << 8;
+        }
+        raw[t] = w;
+      }
+    }
+    r += NT;
+    while (r >= fsamp) { r -= fsamp; q++; }
+  }
+  const int Sd = J.stride, lgS = J.lgstride;
+#pragma unroll
+  for (int t = 0; t < 16; t++) {
+    float2 u = make_float2(0.f, 0.f);
+    if (raw[t] != 0xFFFFFFFFu) {
+      u.x = s_lut[raw[t] & 255u];
+      if (CPLX) u.y = s_lut[(raw[t] >> 8) & 255u];
+    }
+    const int n = j + NT * t;
+    const int k = n & (Sd - 1), jj = n >> lgS;
+    const float2 rot = (jj == 0) ? rs[k] : cmul_exact(rs[k], rp[jj]);
+    v[t] = CPLX ? cmul(rot, u) : make_float2(u.x * rot.x, u.x * rot.y);
+  }
+}
+
+// Forward FFT of the group's transform: radix-16 passes with exchanges through
+// the padded buffer sm, then the final radix; register t ends with bin j + NT t.
+template <int F, int CTA, typename TW>
+__device__ __forceinline__ void r16_fft(float2 (&v)[16], int j, int g, float2 *sm, TW tw)
+{
+  using Pl = r16::Plan<F>;
+  constexpr int NT = Pl::NT;
+  int Ns = 1;
+#pragma unroll
+  for (int pass = 0; pass < Pl::L; pass++) {
+    r16::pass16<F>(v, j, Ns, tw);
+    if (!(pass == Pl::L - 1 && Pl::R0 == 1)) {
+      group_sync<NT, CTA>(g);
+      r16::store16(v, j, Ns, sm);
+      group_sync<NT, CTA>(g);
+      r16::load16<F>(v, j, sm);
+    }
+    Ns *= 16;
+  }
+  if constexpr (Pl::R0 > 1) r16::final_pass<F, Pl::R0>(v, j, tw);
+}
+
+// Sideband selection (mode.cpp:1185-1217) for bin j + NT t: false when the bin
+// is not kept; otherwise its channel c (val conjugated for complex LSB).
+template <int F, int CPLX>
+__device__ __forceinline__ bool r16_channel(int t, int j, int lsb, float2 &val, int &c)
+{
+  constexpr int NT = F / 16, NCH = CPLX ? F : F / 2;
+  const int bin = j + NT * t;
+  if (!CPLX) {
+    if (lsb ? (t < 8) : (t >= 8)) return false;   // NT * 8 = F / 2 = NCH
+    c = lsb ? bin - NCH : bin;
+  } else if (!lsb) {
+    c = bin;
+  } else {
+    c = bin == 0 ? 0 : F - bin;
+    if (bin != 0) val.y = -val.y;
+  }
+  return true;
 }
 
 template <int F, int CPLX>
@@ -614,10 +709,6 @@ fstep_r16_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays
   auto tw = [twg](int m) { return __ldg(&twg[m]); };
 
   const uint8_t *data = S.data[s];
-  const int fsamp = J.framesamples;
-  const int bits_ts = J.nbands * J.nbits * (CPLX ? 2 : 1);
-  const int cmask = (1 << J.nbits) - 1;
-  const bool byte_pairs = CPLX && J.nbits == 8;   // (re, im) = one 16-bit word
   const int b0 = blockIdx.x * blocks_per_cta;
   const int nbk = min(blocks_per_cta, nblk - b0);
   const int nitems = nbk * J.nbands;
@@ -647,72 +738,16 @@ fstep_r16_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays
     }
     group_sync<NT, CTA>(g);
 
-    // decode + rotate: sample n = j + NT t of the block; frame q and in-frame sample r advance incrementally
     float2 v[16];
-    {
-      const int smp0 = P.nearestsample + j;
-      int q = smp0 / fsamp;
-      int r = smp0 - q * fsamp;
-      q -= P.fr0;
-      const int bitband = bd * (CPLX ? 2 : 1) * J.nbits;
-#pragma unroll
-      for (int t = 0; t < 16; t++) {
-        const int n = j + NT * t;
-        float2 u = make_float2(0.f, 0.f);
-        if ((P.validmask >> q) & 1ull) {
-          const uint8_t *payload = data + ((long long)P.fr0 + q) * J.framebytes + 32;
-          const int bit0 = r * bits_ts + bitband;   // < 8 * payload bytes
-          if (byte_pairs) {
-            const unsigned int w = __ldg(reinterpret_cast<const unsigned short *>(payload + (bit0 >> 3)));
-            u.x = s_lut[w & 255u];
-            u.y = s_lut[w >> 8];
-          } else {
-            u.x = s_lut[(__ldg(payload + (bit0 >> 3)) >> (bit0 & 7)) & cmask];
-            if (CPLX) {
-              const int bit1 = bit0 + J.nbits;
-              u.y = s_lut[(__ldg(payload + (bit1 >> 3)) >> (bit1 & 7)) & cmask];
-            }
-          }
-        }
-        const int k = n & (Sd - 1), jj = n >> lgS;
-        const float2 rot = (jj == 0) ? rs[k] : cmul_exact(rs[k], rp[jj]);
-        v[t] = CPLX ? cmul(rot, u) : make_float2(u.x * rot.x, u.x * rot.y);
-        r += NT;
-        while (r >= fsamp) { r -= fsamp; q++; }
-      }
-    }
-
-    // FFT: radix-16 passes, exchanges through the padded buffer, then the final radix
-    int Ns = 1;
-#pragma unroll
-    for (int pass = 0; pass < Pl::L; pass++) {
-      r16::pass16<F>(v, j, Ns, tw);
-      if (!(pass == Pl::L - 1 && Pl::R0 == 1)) {
-        group_sync<NT, CTA>(g);
-        r16::store16(v, j, Ns, sm);
-        group_sync<NT, CTA>(g);
-        r16::load16<F>(v, j, sm);
-      }
-      Ns *= 16;
-    }
-    if constexpr (Pl::R0 > 1) r16::final_pass<F, Pl::R0>(v, j, tw);
-
-    // register t holds bin j + NT t: sideband selection (mode.cpp:1185-1217) and correction
+    r16_decode_rotate<F, CPLX>(J, data, P, bd, j, rs, rp, s_lut, v);
+    r16_fft<F, CTA>(v, j, g, sm, tw);
+    // register t holds bin j + NT t: sideband selection and fractional-sample correction
     const int lsb = st.lsb[lf];
 #pragma unroll
     for (int t = 0; t < 16; t++) {
-      const int bin = j + NT * t;
       float2 val = v[t];
       int c;
-      if (!CPLX) {
-        if (lsb ? (t < 8) : (t >= 8)) continue;   // NT * 8 = F / 2 = NCH
-        c = lsb ? bin - NCH : bin;
-      } else if (!lsb) {
-        c = bin;
-      } else {
-        c = bin == 0 ? 0 : F - bin;
-        if (bin != 0) val.y = -val.y;
-      }
+      if (!r16_channel<F, CPLX>(t, j, lsb, val, c)) continue;
       dst[spec_offset(J, row, c)] = cmul(val, cmul_exact(fs[c & (Sd - 1)], fp[c >> lgS]));
     }
   }

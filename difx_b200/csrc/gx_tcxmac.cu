@@ -62,7 +62,10 @@ constexpr uint32_t kSBO = (kKT / 8) * 128;   // byte step between 8-row groups
 constexpr uint32_t kOpChanBytes = 2 * kNI * kKT * 2;      // [Xi ; Xr]: 256 rows x 16 FP16 = 8 KB
 constexpr uint32_t kXrOffset = (kNI / 8) * kSBO;          // rows 128.. (Xr) start here
 constexpr int kPRow = kNI + 1;               // padded row of the P matrices parked in shared memory
-static_assert((2 * kNI * kPRow + 2 * kNI) * 4 <= kStages * kStageBytes + kOpStages * 2 * kOpChanBytes,
+constexpr int kVCols = 8;                    // columns of V per epilogue slice (one 128-byte line per row)
+constexpr int kVRow = kVCols + 1;            // padded slice row, float4
+static_assert((2 * kNI * kPRow + 2 * kNI) * 4 + kNI * kVRow * 16 <=
+                  kStages * kStageBytes + kOpStages * 2 * kOpChanBytes,
               "epilogue tables must fit in the staging ring and operand stages");
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;
 
@@ -170,6 +173,17 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
       : "r"(taddr));
 #pragma unroll
   for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// 32 lanes x 4 consecutive FP32 columns.
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, float (&v)[4])
+{
+  uint32_t r[4];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 4; i++) v[i] = __uint_as_float(r[i]);
 }
 
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
@@ -344,20 +358,18 @@ xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, i
   __syncthreads();
   tc_fence_after();
 
-  if (!*s_abort) {
+  if (!*s_abort && !(nt == 0 && accumulate)) {   // an empty slice adds nothing
     // warp w reads lanes 32 (w % 4) .. +31, i.e. row a of both accumulators
     const int q = warp & 3, h = warp >> 2;
     const int a = 32 * q + lane;
     const uint32_t lane_addr = tmem + ((uint32_t)(32 * q) << 16);
-    float4 *orow = acc + (((size_t)z * nfreqs + f) * NP + p) * kNI * kNI + (size_t)a * kNI;
-    if (nt == 0) {
-      // empty slice: its share is zero
-      if (!accumulate)
-        for (int b = h * 64; b < h * 64 + 64; b++) orow[b] = make_float4(0.f, 0.f, 0.f, 0.f);
-    } else {
-      // the staging ring and operand stages are idle now: P of both channels, then 1 / scale per (b, channel)
-      float *sP = reinterpret_cast<float *>(staging);             // [2][128][kPRow]
-      float *sInv = sP + 2 * kNI * kPRow;                          // [2][128]
+    float4 *oblk = acc + (((size_t)z * nfreqs + f) * NP + p) * kNI * kNI;   // [a][b]
+    // the staging ring and operand stages are idle now: P of both channels,
+    // 1 / scale per (b, channel), and one 8-column slice of V
+    float *sP = reinterpret_cast<float *>(staging);                 // [2][128][kPRow]
+    float *sInv = sP + 2 * kNI * kPRow;                              // [2][128]
+    float4 *sV = reinterpret_cast<float4 *>(sInv + 2 * kNI);         // [128][kVRow]
+    if (nt > 0) {
       if (h == 1) {
 #pragma unroll 1
         for (int cb = 0; cb < kNI / 16; cb++) {
@@ -375,34 +387,51 @@ xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, i
         sInv[a] = 1.0f / s0;          // operand scales are powers of two: exact
         sInv[kNI + a] = 1.0f / s1;
       }
-      __syncthreads();
-      const float ia0 = 1.0f / s0, ia1 = 1.0f / s1;
+    }
+    __syncthreads();
+    const float ia0 = 1.0f / s0, ia1 = 1.0f / s1;
 #pragma unroll 1
-      for (int cb = 0; cb < 4; cb++) {
-        const int b0 = h * 64 + cb * 16;
-        float r0[16], r1[16];
-        tmem_ld16(lane_addr + (uint32_t)b0, r0);
-        tmem_ld16(lane_addr + 256u + (uint32_t)b0, r1);
+    for (int cb = 0; cb < kNI / kVCols; cb++) {
+      // thread (a, h) forms columns b = 8 cb + 4 h + i of row a
+      const int b0 = cb * kVCols + h * 4;
+      float r0[4] = {0.f, 0.f, 0.f, 0.f}, r1[4] = {0.f, 0.f, 0.f, 0.f};
+      if (nt > 0) {
+        tmem_ld4(lane_addr + (uint32_t)b0, r0);
+        tmem_ld4(lane_addr + 256u + (uint32_t)b0, r1);
         tmem_ld_wait();
+      }
 #pragma unroll
-        for (int i = 0; i < 16; i++) {
-          const int b = b0 + i;
+      for (int i = 0; i < 4; i++) {
+        const int b = b0 + i;
+        float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (nt > 0) {
           const float i0 = ia0 * sInv[b], i1 = ia1 * sInv[kNI + b];
           const float im0 = sP[a * kPRow + b] - sP[b * kPRow + a];
           const float im1 = sP[(kNI + a) * kPRow + b] - sP[(kNI + b) * kPRow + a];
-          float4 w = make_float4(r0[i] * i0, im0 * i0, r1[i] * i1, im1 * i1);
-          if (accumulate) {
-            const float4 old = orow[b];
-            w.x += old.x;
-            w.y += old.y;
-            w.z += old.z;
-            w.w += old.w;
-          }
-          orow[b] = w;
+          w = make_float4(r0[i] * i0, im0 * i0, r1[i] * i1, im1 * i1);
         }
+        sV[a * kVRow + h * 4 + i] = w;
       }
+      __syncthreads();
+      // write the slice back as whole 128-byte lines: 8 consecutive threads per row
+#pragma unroll
+      for (int m = 0; m < kNI * kVCols / kThreads; m++) {
+        const int i = tid + kThreads * m;
+        const int row = i / kVCols, col = i % kVCols;
+        float4 w = sV[row * kVRow + col];
+        float4 *dst = oblk + (size_t)row * kNI + cb * kVCols + col;
+        if (accumulate) {
+          const float4 old = *dst;
+          w.x += old.x;
+          w.y += old.y;
+          w.z += old.z;
+          w.w += old.w;
+        }
+        *dst = w;
+      }
+      __syncthreads();
     }
-  } else if (tid == 0) {
+  } else if (*s_abort && tid == 0) {
     // drain: copies issued but not consumed, then the MMAs last committed
     for (int u = t; u < issued; u++) mbar_wait(smem_u32(bars + u % kStages), (uint32_t)(u / kStages) & 1u);
     if (t > 0) mbar_wait(smem_u32(bars + kStages + (t - 1) % kOpStages), (uint32_t)((t - 1) / kOpStages) & 1u);
@@ -427,8 +456,11 @@ finalise_tc_kernel(const TcProdEntry *__restrict__ prods, const TcRowEntry *__re
   const size_t slice = (size_t)nfreqs * NP * kNI * kNI;
   const int nb = kNI - R.bmin;
   const int ne = R.end - R.start;
-  for (int p0 = 0; p0 < NP; p0 += kFinPairs) {
-    const int np = min(kFinPairs, NP - p0);
+  // channel pairs [pb, pe) of this CTA (blockIdx.y of gridDim.y slices)
+  const int per = ((NP + gridDim.y - 1) / gridDim.y + kFinPairs - 1) / kFinPairs * kFinPairs;
+  const int pb = blockIdx.y * per, pe = min(NP, pb + per);
+  for (int p0 = pb; p0 < pe; p0 += kFinPairs) {
+    const int np = min(kFinPairs, pe - p0);
     for (int i = threadIdx.x; i < np * nb; i += blockDim.x) {
       const int pp = i / nb, b = R.bmin + i % nb;
       const size_t off = (((size_t)R.freq * NP + p0 + pp) * kNI + R.a) * kNI + b;
@@ -489,31 +521,32 @@ cudaError_t xmac_tc_launch(const float2 *spec, int nblk, int N, int nfreqs, int 
   if (cr != CUDA_SUCCESS) return cudaErrorInvalidValue;
   const size_t sm = xmac_tc_smem_bytes(hilo);
   dim3 grid(N / 2, nfreqs, ks);
-  if (hilo) {
-    static bool opted = false;
-    if (!opted) {
-      cudaError_t e = cudaFuncSetAttribute(xmac_tc_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      if (e != cudaSuccess) return e;
-      opted = true;
-    }
-    xmac_tc_kernel<true><<<grid, kThreads, sm, st>>>(map, nblk, N / 2, nfreqs, ks, scale, acc, accumulate, err);
-  } else {
-    static bool opted = false;
-    if (!opted) {
-      cudaError_t e = cudaFuncSetAttribute(xmac_tc_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      if (e != cudaSuccess) return e;
-      opted = true;
-    }
-    xmac_tc_kernel<false><<<grid, kThreads, sm, st>>>(map, nblk, N / 2, nfreqs, ks, scale, acc, accumulate, err);
+#define GX_TC_CASE(H)                                                                                       \
+  if (hilo == H) {                                                                                          \
+    static bool opted = false;                                                                              \
+    if (!opted) {                                                                                           \
+      cudaError_t e = cudaFuncSetAttribute(xmac_tc_kernel<H>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
+                                           (int)sm);                                                        \
+      if (e != cudaSuccess) return e;                                                                       \
+      opted = true;                                                                                         \
+    }                                                                                                       \
+    xmac_tc_kernel<H><<<grid, kThreads, sm, st>>>(map, nblk, N / 2, nfreqs, ks, scale, acc, accumulate, err); \
+    return cudaGetLastError();                                                                              \
   }
-  return cudaGetLastError();
+  GX_TC_CASE(true) GX_TC_CASE(false)
+#undef GX_TC_CASE
+  return cudaErrorInvalidValue;
 }
 
 cudaError_t finalise_tc_launch(const TcProdEntry *prods, const TcRowEntry *rows, int nrows, const float4 *acc,
                                int nfreqs, int N, int ks, float2 *results, cudaStream_t st)
 {
   if (nrows <= 0) return cudaSuccess;
-  finalise_tc_kernel<<<nrows, 256, 0, st>>>(prods, rows, acc, nfreqs, N / 2, ks, results);
+  // enough CTAs for several waves: slices of the channel pairs per row
+  const int NP = N / 2;
+  int slices = 1;
+  while ((long long)nrows * slices < 8 * 148 && (slices * 2) * kFinPairs <= NP) slices *= 2;
+  finalise_tc_kernel<<<dim3(nrows, slices), 256, 0, st>>>(prods, rows, acc, nfreqs, NP, ks, results);
   return cudaGetLastError();
 }
 

@@ -36,8 +36,7 @@ struct XmacShape {
 
 XmacShape xmac_shape(int NI);
 
-size_t fstep_smem_bytes(const DevJob &J, int nrf, int nslots);
-cudaError_t fstep_launch(const DevJob &J, const DevStation *stations, int maxnrf, const SubintArrays &S,
+size_t fstep_smem_bytes(const DevJob &J, int nrf, int nslots);cudaError_t fstep_launch(const DevJob &J, const DevStation *stations, int maxnrf, const SubintArrays &S,
                          int blk0, int nblk, int nslots, float2 *spec, float *weights, BlockParam *bp,
                          cudaStream_t st);
 cudaError_t xmac_fp32_launch(const float2 *spec, int nblk, int NI, int N, int nfreqs, int ks, float2 *acc,
@@ -50,9 +49,9 @@ struct TcRowEntry {
   int freq, a, bmin, start, end;
 };
 
-// Tensor-core X-step over spectra in the channel-pair layout
-// [freq][block][N/2][128 inputs][2]; acc holds, per K-split slice,
-// [freq][N/2][a][b] float4 = (Re, Im) of both channels of the pair, unscaled.
+// Tensor-core X-step over 128-row spectra [freq][block][128 inputs][N]; acc
+// holds, per K-split slice, [freq][N/2][a][b] float4 = (Re, Im) of both
+// channels of a channel pair, unscaled.
 size_t xmac_tc_smem_bytes(bool hilo);
 cudaError_t xmac_tc_launch(const float2 *spec, int nblk, int N, int nfreqs, int ks, bool hilo, const float *scale,
                            float4 *acc, int accumulate, int *err, cudaStream_t st);

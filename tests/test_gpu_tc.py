@@ -54,6 +54,15 @@ CASES = {
     "c1_padded_chunked": (jobs.spec_c1, dict(), 40),
     "lsb_ksplit_chunked": (jobs.spec_lsb, dict(invalid_frac=0.03), 200),
     "cplx8": (jobs.spec_cplx8, dict(invalid_frac=0.05), 0),
+    # FFT lengths of the register-resident F-step
+    "cplx8_4096": (lambda: jobs.spec_long("tcx4k", 8, "COMPLEX", "U", 4096, 61), dict(invalid_frac=0.03), 0),
+    "real2_8192_lsb": (lambda: jobs.spec_long("tcr8k", 2, "REAL", "L", 4096, 67), dict(invalid_frac=0.03), 0),
+    # 64 stations x 2 pols at 512 channels, chunks of 24 blocks (partial K-tiles, accumulation over chunks)
+    "c3_512_chunked": (lambda: spec_c3small(name="c3p", subbands=[Subband(6000.0, 16.0, "U", 512)],
+                                            subint_ns=2_048_000, seed=71), dict(rho=0.01), 24),
+    # single polarisation
+    "cplx8_2048_singlepol": (lambda: jobs.spec_long("tcsp", 8, "COMPLEX", "U", 2048, 73, pols=("R",)),
+                             dict(invalid_frac=0.03), 0),
 }
 
 _prepared = {}
