@@ -1,0 +1,91 @@
+// The gx_handle behind the C ABI of include/gxcorr.h (host driver state),
+// shared by the translation units of the host driver.
+#pragma once
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+#include "../../include/gxcorr.h"
+#include "gx_dev.h"
+#include "gx_host.h"
+#include "gx_xstep.h"
+
+struct gx_handle {
+  std::string err;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = true;
+
+  std::vector<gx_station_desc> st;
+  std::vector<gx_freq_desc> fr;
+  std::vector<gx_baseline_desc> bl;
+  gx_job_desc jd{};
+
+  gx::DevJob J{};
+  int maxnrf = 1, nslots = 1, chunk = 0, ks = 1, xmac_stride = 0, maxprod = 0;
+  gx::XmacShape xs{};
+  long long rl = 0;
+  std::vector<int> blofs, bwofs, acofs, acwofs;
+  std::vector<std::vector<int>> band_input;  // [station][band]
+  std::vector<gx::ProdEntry> prods;
+  std::vector<gx::TcProdEntry> tcprods;   // sorted by (freq, a)
+  std::vector<gx::TcRowEntry> tcrows;
+  std::vector<gx::WeightEntry> wents;
+  std::vector<int2> pairs;
+  bool tc = false, hilo = false;   // tensor-core X-step (split FP16 product)
+  float tc_scale0 = 1.0f;          // default power-of-two operand scale
+  float *d_scale = nullptr;        // [freq][128][nchan] operand scales
+  gx::TcProdEntry *d_tcprods = nullptr;
+  gx::TcRowEntry *d_tcrows = nullptr;
+  int *d_err = nullptr;            // kernel status (bounded waits that expired)
+  int *h_err = nullptr;            // pinned copy of *d_err after each subint
+  cudaStream_t last_stream = nullptr;  // stream of the last gx_subint_device
+
+  gx::DevStation *d_st = nullptr;
+  float2 *d_tw = nullptr, *d_spec = nullptr, *d_acc = nullptr, *d_results = nullptr, *d_spec1 = nullptr;
+  float *d_w = nullptr, *d_wacc = nullptr, *d_w1 = nullptr;
+  gx::BlockParam *d_bp = nullptr, *d_bp1 = nullptr;
+  size_t acc_slice = 0;  // float2 per K-split slice
+  int2 *d_pairs = nullptr;
+  gx::ProdEntry *d_prods = nullptr;
+  gx::WeightEntry *d_went = nullptr;
+  const uint8_t **d_dataptrs = nullptr;
+  int64_t *d_datalen = nullptr;
+  int32_t *d_ctrl = nullptr;
+  int ctrlstride = 0;
+  double *d_interp = nullptr;
+  std::vector<uint8_t *> d_data;
+  std::vector<int64_t> data_cap;
+
+  gx::SubintArrays last{};
+  bool have_last = false;
+  std::vector<cudaEvent_t> evs;  // pairs per launch: [start, end]
+  std::vector<int> ev_stage;
+  int launches = 0;
+
+  std::unique_ptr<HostModel> model;  // only for gx_open_input
+  std::unique_ptr<gx::JobMeta> meta; // only for gx_open_input
+  std::vector<gx::DevStation> dst;   // host copy of the per-station device constants
+
+  gx_status fail(gx_status s, const std::string &m)
+  {
+    err = m;
+    return s;
+  }
+  gx_status cuda(cudaError_t e, const char *what)
+  {
+    if (e == cudaSuccess) return GX_OK;
+    err = std::string(what) + ": " + cudaGetErrorString(e);
+    return GX_ERR_CUDA;
+  }
+};
+
+#define CKR(h, call)                                         \
+  do {                                                       \
+    gx_status _s = (h)->cuda((call), #call);                 \
+    if (_s != GX_OK) return _s;                              \
+  } while (0)
+
+// local freq index of job freq f on baseline b (-1: not correlated)
+int gx_bl_localfreq(const gx_baseline_desc &b, int f);

@@ -14,8 +14,10 @@ struct ModelScan {
   int numphasecentres = 1;
   int nsamples = 0;
   int polystartmjd = 0, polystartseconds = 0;
+  int phase_centre_source = 0;   // .calc SCAN n PHS CTR 0: source table index of the phase centre
   // delay[sample][source][station][order+1], us; source 0 = pointing centre
   std::vector<double> delay;
+  std::vector<double> u, v, w;   // same indexing, metres
 };
 
 // Model::calculateDelayInterpolator and Mode::setOffsets (model.cpp:219-289,
@@ -39,6 +41,18 @@ class HostModel {
   }
   gx_status interpolator(int datastream, int scan, int sec, int ns, double out[3]) const;
   double scan_start_sec(int scan) const;
+  // Model::interpolateUVW (model.cpp:177-217): baseline (u, v, w) of model
+  // antennas ant1 - ant2 at offsettime seconds after the scan start, source
+  // src of the scan's table (1: first phase centre).
+  bool uvw(int scan, double offsettime, int ant1, int ant2, int src, double out[3]) const;
+};
+
+// Job-level .input facts the visibility writer needs (Configuration).
+struct JobMeta {
+  int start_mjd = 0, start_seconds = 0, execute_seconds = 0;
+  double int_time = 0;                 // INT TIME (SEC)
+  std::vector<int> telescope;          // TELESCOPE INDEX per datastream
+  std::vector<double> tsys;            // TSYS per datastream
 };
 
 struct InputJob {
@@ -50,6 +64,7 @@ struct InputJob {
   int start_mjd = 0, start_seconds = 0, execute_seconds = 0;
   double int_time = 0;
   std::vector<std::string> datafiles;   // first file of each datastream
+  JobMeta meta;
 };
 
 InputJob *read_input_job(const char *inputfile, std::string &err);

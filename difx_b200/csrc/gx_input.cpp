@@ -148,6 +148,36 @@ double HostModel::scan_start_sec(int scan) const
   return (double)((modelmjd - jobmjd) * 86400 + (modelstartseconds - jobseconds) + scans[scan].offsetseconds);
 }
 
+bool HostModel::uvw(int scanindex, double offsettime, int ant1, int ant2, int src, double out[3]) const
+{
+  if (scanindex < 0 || scanindex >= (int)scans.size()) return false;
+  const ModelScan &sc = scans[scanindex];
+  if (sc.u.empty() || ant1 < 0 || ant2 < 0 || ant1 >= nstations || ant2 >= nstations || src < 0 ||
+      src > sc.numphasecentres)
+    return false;
+  const int polyoffset = (modelmjd - sc.polystartmjd) * 86400 + modelstartseconds + sc.offsetseconds - sc.polystartseconds;
+  int scansample = int((offsettime + polyoffset) / double(modelincsecs));
+  if (scansample == sc.nsamples && ((offsettime + polyoffset - scansample * modelincsecs) < modelincsecs / 1000000.0))
+    scansample--;
+  if (scansample < 0 || scansample >= sc.nsamples) return false;
+  const double deltat = offsettime + polyoffset - scansample * modelincsecs;
+  double tp[16];
+  tp[0] = 1.0;
+  for (int i = 0; i < polyorder; i++) tp[i + 1] = tp[i] * deltat;
+  const std::vector<double> *tabs[3] = {&sc.u, &sc.v, &sc.w};
+  for (int c = 0; c < 3; c++) {
+    const double *c1 = &(*tabs[c])[(((size_t)scansample * (sc.numphasecentres + 1) + src) * nstations + ant1) *
+                                    (polyorder + 1)];
+    const double *c2 = &(*tabs[c])[(((size_t)scansample * (sc.numphasecentres + 1) + src) * nstations + ant2) *
+                                    (polyorder + 1)];
+    double a = 0, b = 0;   // dot products in index order (genericDotProduct_64f)
+    for (int i = 0; i <= polyorder; i++) a += tp[i] * c1[i];
+    for (int i = 0; i <= polyorder; i++) b += tp[i] * c2[i];
+    out[c] = a - b;
+  }
+  return true;
+}
+
 gx_status HostModel::interpolator(int ds, int scanindex, int sec, int ns, double out[3]) const
 {
   if (scanindex < 0 || scanindex >= (int)scans.size()) return GX_ERR_MODEL;
@@ -271,11 +301,12 @@ InputJob *read_input_job(const char *inputfile, std::string &err)
   NEED(in, "NUM DATA SEGMENTS", v);
   std::vector<gx_station_desc> dstab(nds_table);
   std::vector<int> dstel(nds_table);
+  std::vector<double> dstsys(nds_table, 0.0);
   for (int i = 0; i < nds_table; i++) {
     gx_station_desc &s = dstab[i];
     memset(&s, 0, sizeof(s));
     NEED(in, "TELESCOPE INDEX", v); dstel[i] = atoi(v.c_str());
-    NEED(in, "TSYS", v);
+    NEED(in, "TSYS", v); dstsys[i] = atof(v.c_str());
     NEED(in, "DATA FORMAT", v);
     if (strip(v) != "VDIF") { err = "DATA FORMAT " + strip(v) + " is not implemented (single-thread VDIF only)"; return nullptr; }
     NEED(in, "QUANTISATION BITS", v); s.nbits = atoi(v.c_str());
@@ -432,6 +463,7 @@ InputJob *read_input_job(const char *inputfile, std::string &err)
     if (!cget(pre + "DUR (S)", v)) return nullptr; m->scans[i].durationseconds = atoi(v.c_str());
     if (!cget(pre + "NUM PHS CTRS", v)) return nullptr; m->scans[i].numphasecentres = atoi(v.c_str());
     if (m->scans[i].numphasecentres != 1) { err = "multiple phase centres are not implemented"; return nullptr; }
+    if (!cget(pre + "PHS CTR 0", v)) return nullptr; m->scans[i].phase_centre_source = atoi(v.c_str());
   }
   if (!cget("NUM SPACECRAFT", v)) return nullptr;
   if (atoi(v.c_str()) != 0) { err = "spacecraft models are not implemented"; return nullptr; }
@@ -463,20 +495,28 @@ InputJob *read_input_job(const char *inputfile, std::string &err)
         ModelScan &sc = m->scans[a];
         sc.nsamples = atoi(it.val.c_str());
         sc.delay.assign((size_t)sc.nsamples * (sc.numphasecentres + 1) * m->nstations * np1, 0.0);
+        sc.u = sc.v = sc.w = sc.delay;
       } else if (sscanf(k.c_str(), "SCAN %d POLY %d %63s", &a, &b, tail) == 3) {
         if (a != curscan) { err = "IM: polynomial outside its scan"; return nullptr; }
         curpoly = b;
         if (!strcmp(tail, "MJD") && b == 0) m->scans[a].polystartmjd = atoi(it.val.c_str());
         if (!strcmp(tail, "SEC") && b == 0) m->scans[a].polystartseconds = atoi(it.val.c_str());
-      } else if (sscanf(k.c_str(), "SRC %d ANT %d", &a, &b) == 2 && k.find("DELAY (us)") != std::string::npos) {
-        if (curscan < 0 || curpoly < 0) { err = "IM: delay row before its scan/poly"; return nullptr; }
+      } else if (sscanf(k.c_str(), "SRC %d ANT %d", &a, &b) == 2) {
+        int which = -1;   // 0 delay, 1-3 u, v, w
+        if (k.find("DELAY (us)") != std::string::npos) which = 0;
+        else if (k.find("U (m)") != std::string::npos) which = 1;
+        else if (k.find("V (m)") != std::string::npos) which = 2;
+        else if (k.find("W (m)") != std::string::npos) which = 3;
+        if (which < 0) continue;
+        if (curscan < 0 || curpoly < 0) { err = "IM: polynomial row before its scan/poly"; return nullptr; }
         ModelScan &sc = m->scans[curscan];
+        std::vector<double> *tab = which == 0 ? &sc.delay : which == 1 ? &sc.u : which == 2 ? &sc.v : &sc.w;
         if (curpoly >= sc.nsamples || a > sc.numphasecentres || b >= m->nstations) { err = "IM: index"; return nullptr; }
         std::istringstream iss(it.val);
         for (int i = 0; i < np1; i++) {
           std::string tok;
           if (!(iss >> tok)) { err = "IM: short polynomial row"; return nullptr; }
-          sc.delay[(((size_t)curpoly * (sc.numphasecentres + 1) + a) * m->nstations + b) * np1 + i] = atof(tok.c_str());
+          (*tab)[(((size_t)curpoly * (sc.numphasecentres + 1) + a) * m->nstations + b) * np1 + i] = atof(tok.c_str());
         }
       }
     }
@@ -533,6 +573,14 @@ InputJob *read_input_job(const char *inputfile, std::string &err)
     m->timespan_s = timespan;
   }
   job->model = std::move(m);
+  job->meta.start_mjd = job->start_mjd;
+  job->meta.start_seconds = job->start_seconds;
+  job->meta.execute_seconds = job->execute_seconds;
+  job->meta.int_time = job->int_time;
+  for (int i = 0; i < numds; i++) {
+    job->meta.telescope.push_back(tel_of_cfgds[i]);
+    job->meta.tsys.push_back(dstsys[dsidx[i]]);
+  }
   return job.release();
 }
 

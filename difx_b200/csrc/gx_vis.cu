@@ -1,0 +1,334 @@
+// Visibility output: the integration and SWIN writing of mpifxcorr's
+// Visibility (mpifxcorr/src/visibility.cpp) for one job handle.
+//
+//   gx_vis_add    Visibility::addData (visibility.cpp:192-205): the subint's
+//                 Core result array is added into a device-resident
+//                 integration buffer (results[i] += subint[i], FP32).
+//   gx_vis_write  Visibility::writedata (353-690) + writeSWIN (781-960):
+//                 baseline and autocorrelation weights are read back (a few
+//                 KB), each record's normalisation 1 / (weight * subints per
+//                 integration * blocks per send * 2 * nchan) is formed with the
+//                 reference's float/double expression, the records are scaled
+//                 on the device, the buffer comes back once, and every record
+//                 with a positive weight is appended as a 74-byte SWIN header
+//                 (appendSWINHeaderBuffered, 1205-1234) plus nchan complex
+//                 floats to <outdir>/DIFX_<mjd>_<sec>.s0000.b0000
+//                 (flushBuffersToDisk, 1056-1091): cross-correlations first in
+//                 baseline / freq / polarisation-product order, then the
+//                 autocorrelations per datastream.
+//
+// Covered: one configuration, one phase centre, no pulsar bins, no channel
+// averaging or output bands, TSYS 0 (normalised correlation coefficients).
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <vector>
+#include "gx_handle.h"
+
+using namespace gx;
+
+namespace {
+
+struct VisScale {
+  long long offset;   // complex-float index of the record's first channel
+  float scale;
+  int pad_;
+};
+
+__global__ void vis_add4_kernel(float4 *__restrict__ acc, const float4 *__restrict__ r, size_t n)
+{
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    float4 a = acc[i];
+    const float4 b = r[i];
+    a.x += b.x;
+    a.y += b.y;
+    a.z += b.z;
+    a.w += b.w;
+    acc[i] = a;
+  }
+}
+
+__global__ void vis_add_kernel(float *__restrict__ acc, const float *__restrict__ r, size_t n)
+{
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    acc[i] += r[i];
+}
+
+__global__ void vis_scale_kernel(float2 *__restrict__ acc, const VisScale *__restrict__ recs, int nchan)
+{
+  const VisScale R = recs[blockIdx.y];
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nchan; c += gridDim.x * blockDim.x) {
+    float2 v = acc[R.offset + c];
+    v.x *= R.scale;
+    v.y *= R.scale;
+    acc[R.offset + c] = v;
+  }
+}
+
+char opposite_pol(char p)
+{
+  switch (p) {
+    case 'R': return 'L';
+    case 'L': return 'R';
+    case 'X': return 'Y';
+    case 'Y': return 'X';
+    default: return p;
+  }
+}
+
+template <typename T>
+void put(std::vector<char> &b, const T &v)
+{
+  const char *p = reinterpret_cast<const char *>(&v);
+  b.insert(b.end(), p, p + sizeof(T));
+}
+
+}  // namespace
+
+struct gx_vis {
+  gx_handle *h = nullptr;
+  std::string outdir;
+  float2 *d_int = nullptr;   // integration buffer, result_length complex floats
+  float2 *h_buf = nullptr;   // pinned copy for the writer
+  VisScale *d_rec = nullptr;
+  int maxrec = 0;
+  int nsub = 0;
+  cudaStream_t st = nullptr;
+};
+
+extern "C" {
+
+gx_status gx_vis_open(gx_handle *h, const char *outdir, gx_vis **out)
+{
+  if (!h || !outdir || !out) return GX_ERR_ARG;
+  *out = nullptr;
+  if (h->device < 0) return h->fail(GX_ERR_STATE, "host-only handle (opened with device -1)");
+  if (!h->model || !h->meta) return h->fail(GX_ERR_STATE, "the visibility writer needs a handle opened with gx_open_input");
+  for (double t : h->meta->tsys)
+    if (t > 0.0) return h->fail(GX_ERR_UNSUPPORTED, "TSYS > 0 (a-priori amplitude calibration) is not implemented");
+  std::unique_ptr<gx_vis> v(new gx_vis());
+  v->h = h;
+  v->outdir = outdir;
+  v->st = h->stream;
+  const gx_job_desc &d = h->jd;
+  int nrec = 0;
+  for (int i = 0; i < d.nbaselines; i++)
+    for (int k = 0; k < d.baselines[i].nfreqs; k++) nrec += d.baselines[i].npolprod[k];
+  for (int s = 0; s < d.nstations; s++) nrec += 2 * d.stations[s].nbands;
+  v->maxrec = nrec > 0 ? nrec : 1;
+  CKR(h, cudaSetDevice(h->device));
+  CKR(h, cudaMalloc(&v->d_int, sizeof(float2) * h->rl));
+  CKR(h, cudaMemsetAsync(v->d_int, 0, sizeof(float2) * h->rl, v->st));
+  CKR(h, cudaMallocHost(&v->h_buf, sizeof(float2) * h->rl));
+  CKR(h, cudaMalloc(&v->d_rec, sizeof(VisScale) * v->maxrec));
+  CKR(h, cudaStreamSynchronize(v->st));
+  *out = v.release();
+  return GX_OK;
+}
+
+gx_status gx_vis_add(gx_vis *v, const float *dev_results, void *stream)
+{
+  if (!v || !dev_results) return GX_ERR_ARG;
+  gx_handle *h = v->h;
+  CKR(h, cudaSetDevice(h->device));
+  cudaStream_t st = stream ? (cudaStream_t)stream : v->st;
+  const size_t nfl = 2 * (size_t)h->rl;
+  const int blocks = 148 * 8;
+  if (((uintptr_t)dev_results & 15) == 0 && nfl % 4 == 0)
+    vis_add4_kernel<<<blocks, 256, 0, st>>>(reinterpret_cast<float4 *>(v->d_int),
+                                            reinterpret_cast<const float4 *>(dev_results), nfl / 4);
+  else
+    vis_add_kernel<<<blocks, 256, 0, st>>>(reinterpret_cast<float *>(v->d_int), dev_results, nfl);
+  CKR(h, cudaGetLastError());
+  if (st != v->st) {   // later work on the handle's stream sees the sum
+    cudaEvent_t e;
+    CKR(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    CKR(h, cudaEventRecord(e, st));
+    CKR(h, cudaStreamWaitEvent(v->st, e, 0));
+    CKR(h, cudaEventDestroy(e));
+  }
+  v->nsub++;
+  return GX_OK;
+}
+
+gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
+{
+  if (!v) return GX_ERR_ARG;
+  if (nrecords) *nrecords = 0;
+  gx_handle *h = v->h;
+  const gx_job_desc &d = h->jd;
+  const JobMeta &M = *h->meta;
+  const HostModel &model = *h->model;
+  CKR(h, cudaSetDevice(h->device));
+  if (scan < 0 || scan >= (int)model.scans.size()) return GX_OK;               // past the last scan
+  const int scanstart = (int)model.scan_start_sec(scan);
+  if (sec + scanstart >= M.execute_seconds || v->nsub == 0) return GX_OK;      // writedata's early exits
+  const int nbl = d.nbaselines, N = h->J.nchan;
+
+  // weights: the baseline-weight and autocorrelation-weight regions of the summed array
+  std::vector<float> fr(2 * (size_t)h->rl);
+  {
+    long long bw0 = h->rl, bw1 = 0, aw0 = h->rl;
+    for (int x : h->bwofs)
+      if (x >= 0) bw0 = std::min<long long>(bw0, x), bw1 = std::max<long long>(bw1, x + 2);
+    for (int x : h->acwofs) aw0 = std::min<long long>(aw0, x);
+    if (bw1 > bw0)
+      CKR(h, cudaMemcpyAsync(&fr[2 * bw0], v->d_int + bw0, sizeof(float2) * (bw1 - bw0), cudaMemcpyDeviceToHost,
+                             v->st));
+    if (h->rl > aw0)
+      CKR(h, cudaMemcpyAsync(&fr[2 * aw0], v->d_int + aw0, sizeof(float2) * (h->rl - aw0), cudaMemcpyDeviceToHost,
+                             v->st));
+    CKR(h, cudaStreamSynchronize(v->st));
+  }
+  // Visibility::changeConfig (visibility.cpp:1314-1316)
+  const double meansub = M.int_time / (((double)d.subint_ns) / 1000000000.0);
+  const double ffts = meansub * h->J.blocks_per_send;
+  const float chanfactor = (float)(h->J.blocks_per_send * 2 * N * 1);   // blocks per send * 2 * nchan * chanavg
+  auto weight_and_scale = [&](long long widx, float &w, float &scale) {
+    w = (float)(fr[widx] / ffts);
+    scale = w > 0.0f ? (float)(1.0 / ((double)w * meansub * (double)chanfactor)) : 0.0f;
+  };
+  auto freq_used = [&](int f) {
+    for (int j = 0; j < nbl; j++)
+      if (gx_bl_localfreq(d.baselines[j], f) >= 0) return true;
+    return false;
+  };
+
+  // record table, in writeSWIN order
+  struct Rec {
+    int baseline, freq;
+    char pol[2];
+    float weight;
+    double uvw[3];
+    long long offset;
+  };
+  std::vector<Rec> recs;
+  std::vector<VisScale> scales;
+  const int srcindex = model.scans[scan].phase_centre_source;
+  const double scanoffset = sec + ((double)ns) / 1e9 + M.int_time / 2.0;
+  for (int i = 0; i < nbl; i++) {
+    const gx_baseline_desc &B = d.baselines[i];
+    Rec r{};
+    r.baseline = (M.telescope[B.ds1] + 1) * 256 + (M.telescope[B.ds2] + 1);
+    if (!model.uvw(scan, scanoffset, model.station_of_datastream[B.ds1], model.station_of_datastream[B.ds2], 1, r.uvw))
+      return h->fail(GX_ERR_MODEL, "no (u, v, w) model for this integration");
+    for (int f = 0; f < d.nfreqs; f++) {
+      const int lf = gx_bl_localfreq(B, f);
+      if (lf < 0) continue;
+      for (int k = 0; k < B.npolprod[lf]; k++) {
+        float w, scale;
+        weight_and_scale(2LL * h->bwofs[f * nbl + i] + k, w, scale);
+        if (scale > 0.0f) scales.push_back(VisScale{h->blofs[f * nbl + i] + (long long)k * N, scale, 0});
+        if (w > 0.0f) {
+          r.freq = f;
+          r.pol[0] = d.stations[B.ds1].band_pol[B.band1[lf][k]];
+          r.pol[1] = d.stations[B.ds2].band_pol[B.band2[lf][k]];
+          r.weight = w;
+          r.offset = h->blofs[f * nbl + i] + (long long)k * N;
+          recs.push_back(r);
+        }
+      }
+    }
+  }
+  if (d.write_autocorrs) {
+    const int acwidth = h->maxprod > 2 ? 2 : 1;
+    for (int s = 0; s < d.nstations; s++) {
+      const gx_station_desc &x = d.stations[s];
+      long long off = h->acofs[s], widx = 2LL * h->acwofs[s];
+      for (int j = 0; j < acwidth; j++)
+        for (int b = 0; b < x.nbands; b++) {
+          const int f = x.recfreq[x.band_localfreq[b]];
+          if (!freq_used(f)) continue;
+          float w, scale;
+          weight_and_scale(widx++, w, scale);
+          if (scale > 0.0f) scales.push_back(VisScale{off, scale, 0});
+          if (w > 0.0f) {
+            Rec r{};
+            r.baseline = 257 * (M.telescope[s] + 1);
+            r.freq = f;
+            r.pol[0] = x.band_pol[b];
+            r.pol[1] = j == 0 ? r.pol[0] : opposite_pol(r.pol[0]);
+            r.weight = w;
+            r.offset = off;
+            recs.push_back(r);
+          }
+          off += N;
+        }
+    }
+  }
+
+  // normalise on the device, then one copy back
+  if (!scales.empty()) {
+    if ((int)scales.size() > v->maxrec) return h->fail(GX_ERR_ARG, "record table overflow");
+    CKR(h, cudaMemcpyAsync(v->d_rec, scales.data(), sizeof(VisScale) * scales.size(), cudaMemcpyHostToDevice, v->st));
+    dim3 grid((N + 255) / 256, (unsigned)scales.size());
+    vis_scale_kernel<<<grid, 256, 0, v->st>>>(v->d_int, v->d_rec, N);
+    CKR(h, cudaGetLastError());
+  }
+  CKR(h, cudaMemcpyAsync(v->h_buf, v->d_int, sizeof(float2) * h->rl, cudaMemcpyDeviceToHost, v->st));
+  CKR(h, cudaStreamSynchronize(v->st));
+
+  // SWIN records (appendSWINHeaderBuffered): 74-byte header + nchan complex floats
+  const int intsec = M.start_seconds + scanstart + sec;
+  const int dumpmjd = M.start_mjd + intsec / 86400;
+  const double dumpseconds = double(intsec % 86400) + ((double)ns) / 1000000000.0 + M.int_time / 2.0;
+  std::vector<char> buf;
+  buf.reserve(recs.size() * (74 + sizeof(float2) * (size_t)N));
+  for (const Rec &r : recs) {
+    put(buf, (uint32_t)0xFF00FF00u);   // sync word
+    put(buf, (int32_t)1);              // binary header version
+    put(buf, (int32_t)r.baseline);
+    put(buf, (int32_t)dumpmjd);
+    put(buf, dumpseconds);
+    put(buf, (int32_t)0);              // configuration index
+    put(buf, (int32_t)srcindex);
+    put(buf, (int32_t)r.freq);
+    buf.push_back(r.pol[0]);
+    buf.push_back(r.pol[1]);
+    put(buf, (int32_t)0);              // pulsar bin
+    put(buf, (double)r.weight);
+    put(buf, r.uvw[0]);
+    put(buf, r.uvw[1]);
+    put(buf, r.uvw[2]);
+    const char *p = reinterpret_cast<const char *>(v->h_buf + r.offset);
+    buf.insert(buf.end(), p, p + sizeof(float2) * (size_t)N);
+  }
+  char name[64];
+  snprintf(name, sizeof(name), "/DIFX_%05d_%06d.s%04d.b%04d", M.start_mjd, M.start_seconds, 0, 0);
+  std::ofstream of(v->outdir + name, std::ios::app | std::ios::binary);
+  if (!of) return h->fail(GX_ERR_IO, "cannot open " + v->outdir + name);
+  of.write(buf.data(), (std::streamsize)buf.size());
+  of.close();
+  if (!of) return h->fail(GX_ERR_IO, "write failed: " + v->outdir + name);
+
+  CKR(h, cudaMemsetAsync(v->d_int, 0, sizeof(float2) * h->rl, v->st));
+  v->nsub = 0;
+  if (nrecords) *nrecords = (int)recs.size();
+  return GX_OK;
+}
+
+gx_status gx_vis_close(gx_vis *v)
+{
+  if (!v) return GX_ERR_ARG;
+  if (v->h && v->h->device >= 0) cudaSetDevice(v->h->device);
+  if (v->st) cudaStreamSynchronize(v->st);
+  if (v->d_int) cudaFree(v->d_int);
+  if (v->d_rec) cudaFree(v->d_rec);
+  if (v->h_buf) cudaFreeHost(v->h_buf);
+  delete v;
+  return GX_OK;
+}
+
+gx_status gx_uvw(gx_handle *h, int scan, double offset, int ds1, int ds2, double out[3])
+{
+  if (!h || !out) return GX_ERR_ARG;
+  if (!h->model) return h->fail(GX_ERR_STATE, "handle has no delay model (open it with gx_open_input)");
+  if (ds1 < 0 || ds2 < 0 || ds1 >= h->jd.nstations || ds2 >= h->jd.nstations)
+    return h->fail(GX_ERR_ARG, "datastream out of range");
+  if (!h->model->uvw(scan, offset, h->model->station_of_datastream[ds1], h->model->station_of_datastream[ds2], 1, out))
+    return h->fail(GX_ERR_MODEL, "no (u, v, w) model at this time");
+  return GX_OK;
+}
+
+}  // extern "C"

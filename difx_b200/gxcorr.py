@@ -39,10 +39,9 @@ def lib():
         L = C.CDLL(LIBPATH)
         L.gx_last_error.restype = C.c_char_p
         L.gx_status_string.restype = C.c_char_p
-        for name in ("gx_open", "gx_open_input", "gx_close", "gx_get_layout", "gx_get_offsets", "gx_interpolator",
-                     "gx_scan_start_sec", "gx_subint", "gx_subint_device", "gx_synchronize", "gx_spectra",
-                     "gx_stage_times", "gx_launch_count", "gx_subint_device_noalloc", "gx_set_tc_scales"):
-            getattr(L, name).restype = C.c_int
+        for name in EXPORTED_SYMBOLS:
+            if name not in ("gx_last_error", "gx_status_string"):
+                getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
 
@@ -50,7 +49,8 @@ def lib():
 EXPORTED_SYMBOLS = ("gx_open", "gx_open_input", "gx_close", "gx_last_error", "gx_status_string",
                     "gx_get_layout", "gx_get_offsets", "gx_interpolator", "gx_scan_start_sec", "gx_subint",
                     "gx_subint_device", "gx_synchronize", "gx_spectra", "gx_stage_times", "gx_launch_count",
-                    "gx_subint_device_noalloc", "gx_set_tc_scales")
+                    "gx_subint_device_noalloc", "gx_set_tc_scales", "gx_vis_open", "gx_vis_add", "gx_vis_write",
+                    "gx_vis_close", "gx_uvw")
 
 
 def subint_device_noalloc(jd: capi.JobDesc, sd: capi.SubintDesc, dev_results_ptr: int, stream_ptr: int = 0) -> None:
@@ -129,6 +129,12 @@ class Correlator:
         self._check(lib().gx_interpolator(self.h, station, scan, sec, ns, out.ctypes.data_as(C.c_void_p)))
         return out
 
+    def uvw(self, scan: int, offset_s: float, ds1: int, ds2: int) -> np.ndarray:
+        """(u, v, w) in metres of baseline ds1 - ds2, offset_s after the scan start (gx_uvw)."""
+        out = np.zeros(3, np.float64)
+        self._check(lib().gx_uvw(self.h, scan, C.c_double(offset_s), ds1, ds2, out.ctypes.data_as(C.c_void_p)))
+        return out
+
     def scan_start_sec(self, scan: int) -> float:
         v = C.c_double(0)
         self._check(lib().gx_scan_start_sec(self.h, scan, C.byref(v)))
@@ -171,3 +177,36 @@ class Correlator:
         w = C.c_float(0)
         self._check(lib().gx_spectra(self.h, station, block, out.ctypes.data_as(C.c_void_p), C.byref(w)))
         return out.reshape(nbands, self.info.nchan), w.value
+
+
+class Visibility:
+    """Device integration buffer and DIFX/SWIN writer of one Correlator
+    (gx_vis_*, mpifxcorr's Visibility).  The Correlator must come from
+    ``Correlator.from_input``."""
+
+    def __init__(self, corr: Correlator, outdir: str):
+        self.corr = corr
+        self.v = C.c_void_p()
+        corr._check(lib().gx_vis_open(corr.h, outdir.encode(), C.byref(self.v)))
+
+    def add(self, dev_results_ptr: int, stream_ptr: int = 0) -> None:
+        """Adds one subint's Core result array (device pointer) to the integration."""
+        self.corr._check(lib().gx_vis_add(self.v, C.c_void_p(dev_results_ptr),
+                                          C.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def write(self, scan: int, sec: int, ns: int) -> int:
+        """Normalises and appends the integration that started at (scan, sec, ns); returns the records written."""
+        n = C.c_int(0)
+        self.corr._check(lib().gx_vis_write(self.v, scan, sec, ns, C.byref(n)))
+        return n.value
+
+    def close(self) -> None:
+        if self.v:
+            lib().gx_vis_close(self.v)
+            self.v = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -165,6 +165,24 @@ class JobSpec:
         return c
 
 
+def uvw_poly_rows(spec: JobSpec, nsamp: int) -> np.ndarray:
+    """Seeded (u, v, w) polynomials per model sample and station, metres, order 5 in
+    seconds from the sample start: a position of up to 6000 km drifting at up to
+    450 m/s with a small quadratic term.  Shape [nsamp, nstations, 3, 6]."""
+    rng = np.random.default_rng(spec.seed * 104729 + 3)
+    out = np.zeros((nsamp, spec.nstations, 3, 6))
+    for s in range(spec.nstations):
+        p0 = rng.uniform(-6.0e6, 6.0e6, 3)
+        rate = rng.uniform(-450.0, 450.0, 3)
+        acc = rng.uniform(-0.03, 0.03, 3)
+        for k in range(nsamp):
+            t0 = k * spec.poly_interval_s
+            out[k, s, :, 0] = p0 + rate * t0 + acc * t0 * t0
+            out[k, s, :, 1] = rate + 2 * acc * t0
+            out[k, s, :, 2] = acc
+    return out
+
+
 def _stname(i: int) -> str:
     a = "ABCDEFGHIJKLMNOPQRSTUVWXYZ"
     return a[(i // 26) % 26] + a[i % 26]
@@ -421,7 +439,7 @@ def write_job(spec: JobSpec, outdir: str) -> dict:
     I.append(_kv("SCAN 0 NUM PHS CTRS", 1))
     I.append(_kv("SCAN 0 PHS CTR 0 SRC", "SYNTH"))
     I.append(_kv("SCAN 0 NUM POLY", nsamp))
-    zero = "\t".join(["0.0000000000000000e+00"] * 6)
+    uvw = uvw_poly_rows(spec, nsamp)
     for k in range(nsamp):
         t = spec.start_seconds + k * spec.poly_interval_s
         I.append(_kv(f"SCAN 0 POLY {k} MJD", spec.start_mjd + t // 86400))
@@ -430,9 +448,8 @@ def write_job(spec: JobSpec, outdir: str) -> dict:
             for s in range(nst):
                 vals = "\t ".join(f"{v:.16e}" for v in rows[k, s])
                 I.append(_kv(f"SRC {src} ANT {s} DELAY (us)", vals))
-                I.append(_kv(f"SRC {src} ANT {s} U (m)", zero))
-                I.append(_kv(f"SRC {src} ANT {s} V (m)", zero))
-                I.append(_kv(f"SRC {src} ANT {s} W (m)", zero))
+                for c, name in enumerate("UVW"):
+                    I.append(_kv(f"SRC {src} ANT {s} {name} (m)", "\t ".join(f"{v:.16e}" for v in uvw[k, s, c])))
     with open(paths["im"], "w") as f:
         f.write("".join(I))
     return paths

@@ -200,6 +200,38 @@ gx_status gx_stage_times(gx_handle *h, float ms[3]);
 /* Number of kernel launches issued by the last gx_subint* call. */
 gx_status gx_launch_count(const gx_handle *h, int *count);
 
+/* ---- Visibility output (mpifxcorr/src/visibility.cpp) -------------------- */
+
+/* An integration buffer and SWIN writer on the handle's device (Visibility,
+   visibility.cpp:33-103).  Needs a handle opened with gx_open_input (job
+   start, integration time, telescope indices and the .im (u, v, w) model).
+   Records are appended to <outdir>/DIFX_<start mjd>_<start seconds>.s0000.b0000
+   as Visibility::flushBuffersToDisk names them (visibility.cpp:1056-1091).
+   GX_ERR_STATE without a .input job, GX_ERR_UNSUPPORTED for TSYS > 0. */
+typedef struct gx_vis gx_vis;
+gx_status gx_vis_open(gx_handle *h, const char *outdir, gx_vis **out);
+
+/* Visibility::addData (visibility.cpp:192-205): adds one subint's Core result
+   array (device memory, gx_layout_info.result_length complex floats) into the
+   integration, on stream (NULL: the handle's stream). */
+gx_status gx_vis_add(gx_vis *v, const float *dev_results, void *stream);
+
+/* Visibility::writedata and writeSWIN (visibility.cpp:353-690, 781-960) for
+   the integration that started at scan, sec (seconds after the scan start),
+   ns: normalises every record by 1 / (weight x subints per integration x
+   blocks per send x 2 x nchan), writes the records with positive weight
+   (74-byte header + nchan complex floats; cross-correlations, then
+   autocorrelations) and clears the buffer.  *nrecords (may be NULL) returns
+   the number of records written.  Nothing is written for an integration
+   past the end of the job or with no subints added. */
+gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords);
+gx_status gx_vis_close(gx_vis *v);
+
+/* Model::interpolateUVW (model.cpp:177-217): (u, v, w) in metres of the
+   baseline datastream ds1 - datastream ds2, offset seconds after the start
+   of scan, first phase centre. */
+gx_status gx_uvw(gx_handle *h, int scan, double offset, int ds1, int ds2, double out[3]);
+
 /* Operand scales of the tensor-core X-step for one band of one datastream:
    scales[c] multiplies channel c of that band's spectra before they are
    rounded to FP16 and is divided out of every visibility.  Each value is

@@ -136,6 +136,22 @@ class Reference:
                              res.ctypes.data_as(C.c_void_p))
         return res[0::2] + 1j * res[1::2]
 
+    def vis_write(self, results, scan: int, sec: int, ns: int, outdir: str) -> None:
+        """The reference's Visibility integrating `results` (complex64 Core result
+        arrays) for the integration starting at (scan, sec, ns), written to outdir."""
+        arrs = [np.ascontiguousarray(r, dtype=np.complex64) for r in results]
+        ptrs = (C.c_void_p * len(arrs))(*[a.ctypes.data for a in arrs])
+        os.makedirs(outdir, exist_ok=True)
+        st = self.lib.ref_vis_write(self.h, len(arrs), ptrs, scan, sec, ns, outdir.encode())
+        if st != 0:
+            raise RuntimeError(f"ref_vis_write failed ({st})")
+
+    def uvw(self, scan: int, offset_s: float, ds1: int, ds2: int) -> np.ndarray:
+        out = np.zeros(3, np.float64)
+        if self.lib.ref_uvw(self.h, scan, C.c_double(offset_s), ds1, ds2, out.ctypes.data_as(C.c_void_p)) != 0:
+            raise RuntimeError("no (u, v, w) model at this time")
+        return out
+
     def mode_block(self, si, station: int, block: int, nbands: int, nchan: int):
         sp = np.zeros(2 * nbands * nchan, np.float32)
         w = C.c_float(0)

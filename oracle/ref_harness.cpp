@@ -22,6 +22,7 @@
 #include "mode.h"
 #include "mk5mode.h"
 #include "model.h"
+#include "visibility.h"
 
 namespace {
 struct RefJob {
@@ -217,6 +218,46 @@ int ref_unpack(void *h, int station, const unsigned char *data, int datalen, int
   int per = m->unpacksamples * (m->usecomplex ? 2 : 1);
   for (int b = 0; b < m->numrecordedbands; b++) memcpy(out + b * per, m->unpackedarrays[b], sizeof(f32) * per);
   return m->unpacksamples;
+}
+
+// Visibility (visibility.cpp:33-103, addData 192-205, writedata 353-690,
+// writeSWIN 781-960) integrating nsub Core result arrays (host, each of the
+// configuration's result length) into the integration that started at scan,
+// sec (seconds after the scan start), ns; the records go to
+// <outdir>/DIFX_<mjd>_<sec>.s0000.b0000 (the .input's OUTPUT FILENAME is
+// replaced by outdir, which must exist).
+int ref_vis_write(void *h, int nsub, const float *const *results, int scan, int sec, int ns, const char *outdir)
+{
+  RefJob *j = (RefJob *)h;
+  Configuration *config = j->config;
+  config->outputfilename = outdir;
+  const long long maxlen = config->getMaxCoreResultLength();
+  const long long rl = config->getCoreResultLength(0);
+  const long long buflen = maxlen * 8 + (64LL << 20);
+  if (buflen > 0x7fffffffLL) return -1;
+  char *buf = new char[buflen];
+  static const string polnames[] = {"R", "L", "X", "Y"};
+  Visibility *v = new Visibility(config, 0, 1, buf, (int)buflen, config->getExecuteSeconds(), scan, sec, ns, polnames);
+  cf32 *tmp = vectorAlloc_cf32(maxlen);
+  for (int i = 0; i < nsub; i++) {
+    vectorZero_cf32(tmp, maxlen);
+    memcpy(tmp, results[i], sizeof(cf32) * rl);
+    v->addData(tmp);
+  }
+  v->writedata();
+  delete v;
+  vectorFree(tmp);
+  delete[] buf;
+  return 0;
+}
+
+// Model::interpolateUVW (model.cpp:177-217) for datastreams ds1, ds2.
+int ref_uvw(void *h, int scan, double offset, int ds1, int ds2, double *out3)
+{
+  RefJob *j = (RefJob *)h;
+  Configuration *config = j->config;
+  const int a1 = config->getDModelFileIndex(0, ds1), a2 = config->getDModelFileIndex(0, ds2);
+  return config->getModel()->interpolateUVW(scan, offset, a1, a2, 1, out3) ? 0 : -1;
 }
 
 void ref_close(void *h)
