@@ -146,10 +146,11 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         t0, t1 = self.window
         lines = self.lines
-        if t0 is not None:
-            after = [x for x in lines if x[0] >= t0]
-            inside = [x for x in after if t1 is None or x[0] <= t1 + 0.1]
-            lines = inside if len(inside) >= 3 else after[:3]
+        if t0 is not None and lines:
+            t1 = t0 if t1 is None else t1
+            inside = [x for x in lines if t0 <= x[0] <= t1 + 0.1]
+            mid = 0.5 * (t0 + t1)
+            lines = inside if len(inside) >= 3 else sorted(lines, key=lambda x: abs(x[0] - mid))[:3]
         for _, l in lines:
             p = [x.strip() for x in l.split(",")]
             if len(p) < 9:

@@ -399,17 +399,14 @@ static gx_status setup(gx_handle *h)
   }
   h->chunk = chunk;
   if (h->tc) {
-    // one CTA per SM (all 512 tensor-memory columns); at least 4 K-tiles per slice
+    // One CTA per SM (all 512 tensor-memory columns).  Every K-split slice
+    // adds a full accumulator write and finalise read, so the K dimension is
+    // split only while the grid is under two waves of 148 SMs (at least 4
+    // K-tiles per slice).
     const long long base = (long long)(J.nchan / 2) * d.nfreqs;
     const int kmax = std::max(1, std::min(16, chunk / 64));
     int best = 1;
-    double best_score = -1;
-    for (int ks = 1; ks <= kmax; ks++) {
-      const long long ctas = base * ks;
-      const double waves = std::ceil(ctas / 148.0);
-      const double score = (ctas / (waves * 148.0)) * std::min(1.0, ctas / 148.0);
-      if (score > best_score + 1e-9) { best_score = score; best = ks; }
-    }
+    while (best < kmax && base * best < 2 * 148) best++;
     h->ks = best;
   } else {
     long long base = (long long)((J.nchan + xs.CT - 1) / xs.CT) * xs.npairs * d.nfreqs;
