@@ -461,7 +461,7 @@ static gx_status setup(gx_handle *h)
   if (h->device < 0) return GX_OK;  // host-only handle: layout and model queries
   CKR(h, cudaSetDevice(h->device));
   if (!h->stream) CKR(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
-  CKR(h, cudaMalloc(&h->d_st, sizeof(DevStation) * d.nstations));
+  CKR(h, h->dalloc(&h->d_st, sizeof(DevStation) * d.nstations));
   CKR(h, cudaMemcpy(h->d_st, dst.data(), sizeof(DevStation) * d.nstations, cudaMemcpyHostToDevice));
   {
     std::vector<float2> tw(J.fftlen);
@@ -469,65 +469,67 @@ static gx_status setup(gx_handle *h)
       double a = -2.0 * M_PI * (double)m / (double)J.fftlen;
       tw[m] = make_float2((float)std::cos(a), (float)std::sin(a));
     }
-    CKR(h, cudaMalloc(&h->d_tw, sizeof(float2) * J.fftlen));
+    CKR(h, h->dalloc(&h->d_tw, sizeof(float2) * J.fftlen));
     CKR(h, cudaMemcpy(h->d_tw, tw.data(), sizeof(float2) * J.fftlen, cudaMemcpyHostToDevice));
     J.twiddle = h->d_tw;
   }
   const size_t spec_elems = (size_t)d.nfreqs * chunk * J.ninputs * J.nchan;
-  CKR(h, cudaMalloc(&h->d_spec, sizeof(float2) * spec_elems));
+  CKR(h, h->dalloc(&h->d_spec, sizeof(float2) * spec_elems));
   CKR(h, cudaMemsetAsync(h->d_spec, 0, sizeof(float2) * spec_elems, h->stream));
-  CKR(h, cudaMalloc(&h->d_spec1, sizeof(float2) * (size_t)d.nfreqs * J.ninputs * J.nchan));
+  CKR(h, h->dalloc(&h->d_spec1, sizeof(float2) * (size_t)d.nfreqs * J.ninputs * J.nchan));
   CKR(h, cudaMemsetAsync(h->d_spec1, 0, sizeof(float2) * (size_t)d.nfreqs * J.ninputs * J.nchan, h->stream));
-  CKR(h, cudaMalloc(&h->d_w, sizeof(float) * (size_t)d.nstations * chunk));
-  CKR(h, cudaMalloc(&h->d_w1, sizeof(float) * (size_t)d.nstations));
-  CKR(h, cudaMalloc(&h->d_bp, sizeof(BlockParam) * (size_t)d.nstations * chunk));
-  CKR(h, cudaMalloc(&h->d_bp1, sizeof(BlockParam) * (size_t)d.nstations));
+  CKR(h, h->dalloc(&h->d_w, sizeof(float) * (size_t)d.nstations * chunk));
+  CKR(h, h->dalloc(&h->d_w1, sizeof(float) * (size_t)d.nstations));
+  CKR(h, h->dalloc(&h->d_bp, sizeof(BlockParam) * (size_t)d.nstations * chunk));
+  CKR(h, h->dalloc(&h->d_bp1, sizeof(BlockParam) * (size_t)d.nstations));
   if (h->tc) {
     // [freq][chan/2][128][128] float4 (both channels of a pair) per K-split slice
     h->acc_slice = (size_t)d.nfreqs * J.nchan * kTcInputs * kTcInputs;
     const size_t nsc = (size_t)d.nfreqs * kTcInputs * J.nchan;
     std::vector<float> sc(nsc, h->tc_scale0);
-    CKR(h, cudaMalloc(&h->d_scale, sizeof(float) * nsc));
+    CKR(h, h->dalloc(&h->d_scale, sizeof(float) * nsc));
     CKR(h, cudaMemcpy(h->d_scale, sc.data(), sizeof(float) * nsc, cudaMemcpyHostToDevice));
-    CKR(h, cudaMalloc(&h->d_tcprods, sizeof(TcProdEntry) * std::max<size_t>(1, h->tcprods.size())));
+    CKR(h, h->dalloc(&h->d_tcprods, sizeof(TcProdEntry) * std::max<size_t>(1, h->tcprods.size())));
     if (!h->tcprods.empty())
       CKR(h, cudaMemcpy(h->d_tcprods, h->tcprods.data(), sizeof(TcProdEntry) * h->tcprods.size(),
                         cudaMemcpyHostToDevice));
-    CKR(h, cudaMalloc(&h->d_tcrows, sizeof(TcRowEntry) * std::max<size_t>(1, h->tcrows.size())));
+    CKR(h, h->dalloc(&h->d_tcrows, sizeof(TcRowEntry) * std::max<size_t>(1, h->tcrows.size())));
     if (!h->tcrows.empty())
       CKR(h, cudaMemcpy(h->d_tcrows, h->tcrows.data(), sizeof(TcRowEntry) * h->tcrows.size(),
                         cudaMemcpyHostToDevice));
   } else {
     h->acc_slice = (size_t)d.nfreqs * xs.npairs * xs.ST * xs.ST * J.nchan;
   }
-  CKR(h, cudaMalloc(&h->d_acc, sizeof(float2) * h->acc_slice * h->ks));
-  CKR(h, cudaMalloc(&h->d_err, sizeof(int)));
+  CKR(h, h->dalloc(&h->d_acc, sizeof(float2) * h->acc_slice * h->ks));
+  CKR(h, h->dalloc(&h->d_err, sizeof(int)));
   CKR(h, cudaMemset(h->d_err, 0, sizeof(int)));
   CKR(h, cudaMallocHost(&h->h_err, sizeof(int)));
   *h->h_err = 0;
-  CKR(h, cudaMalloc(&h->d_wacc, sizeof(float) * (d.nstations + nbl)));
+  CKR(h, h->dalloc(&h->d_wacc, sizeof(float) * (d.nstations + nbl)));
   if (nbl) {
-    CKR(h, cudaMalloc(&h->d_pairs, sizeof(int2) * nbl));
+    CKR(h, h->dalloc(&h->d_pairs, sizeof(int2) * nbl));
     CKR(h, cudaMemcpy(h->d_pairs, h->pairs.data(), sizeof(int2) * nbl, cudaMemcpyHostToDevice));
   }
-  CKR(h, cudaMalloc(&h->d_prods, sizeof(ProdEntry) * std::max<size_t>(1, h->prods.size())));
+  CKR(h, h->dalloc(&h->d_prods, sizeof(ProdEntry) * std::max<size_t>(1, h->prods.size())));
   if (!h->prods.empty())
     CKR(h, cudaMemcpy(h->d_prods, h->prods.data(), sizeof(ProdEntry) * h->prods.size(), cudaMemcpyHostToDevice));
-  CKR(h, cudaMalloc(&h->d_went, sizeof(WeightEntry) * std::max<size_t>(1, h->wents.size())));
+  CKR(h, h->dalloc(&h->d_went, sizeof(WeightEntry) * std::max<size_t>(1, h->wents.size())));
   if (!h->wents.empty())
     CKR(h, cudaMemcpy(h->d_went, h->wents.data(), sizeof(WeightEntry) * h->wents.size(), cudaMemcpyHostToDevice));
-  CKR(h, cudaMalloc(&h->d_results, sizeof(float2) * h->rl));
-  CKR(h, cudaMalloc((void **)&h->d_dataptrs, sizeof(uint8_t *) * d.nstations));
-  CKR(h, cudaMalloc(&h->d_datalen, sizeof(int64_t) * d.nstations));
+  CKR(h, h->dalloc(&h->d_results, sizeof(float2) * h->rl));
+  CKR(h, h->dalloc((void **)&h->d_dataptrs, sizeof(uint8_t *) * d.nstations));
+  CKR(h, h->dalloc(&h->d_datalen, sizeof(int64_t) * d.nstations));
   h->ctrlstride = 3 + J.flaglen;
-  CKR(h, cudaMalloc(&h->d_ctrl, sizeof(int32_t) * h->ctrlstride * d.nstations));
-  CKR(h, cudaMalloc(&h->d_interp, sizeof(double) * 3 * d.nstations));
+  CKR(h, h->dalloc(&h->d_ctrl, sizeof(int32_t) * h->ctrlstride * d.nstations));
+  CKR(h, h->dalloc(&h->d_interp, sizeof(double) * 3 * d.nstations));
   h->d_data.assign(d.nstations, nullptr);
   h->data_cap.assign(d.nstations, 0);
+  h->data_alloc.assign(d.nstations, 0);
   if (d.max_data_bytes > 0) {
     for (int s = 0; s < d.nstations; s++) {
-      CKR(h, cudaMalloc(&h->d_data[s], d.max_data_bytes));
+      CKR(h, h->dalloc(&h->d_data[s], d.max_data_bytes));
       h->data_cap[s] = d.max_data_bytes;
+      h->data_alloc[s] = d.max_data_bytes;
     }
   }
   CKR(h, cudaStreamSynchronize(h->stream));
@@ -779,9 +781,13 @@ gx_status gx_subint(gx_handle *h, const gx_subint_desc *sub, float *results)
   for (int s = 0; s < d.nstations; s++) {
     if (sub->datalen[s] < 0) return h->fail(GX_ERR_ARG, "negative data length");
     if (sub->datalen[s] > h->data_cap[s]) {
-      if (h->d_data[s]) CKR(h, cudaFree(h->d_data[s]));
+      if (h->d_data[s]) {
+        CKR(h, cudaFree(h->d_data[s]));
+        h->dev_bytes -= h->data_alloc[s];
+      }
       h->d_data[s] = nullptr;
-      CKR(h, cudaMalloc(&h->d_data[s], sub->datalen[s] + 64));
+      CKR(h, h->dalloc(&h->d_data[s], sub->datalen[s] + 64));
+      h->data_alloc[s] = sub->datalen[s] + 64;
       h->data_cap[s] = sub->datalen[s];
     }
     if (sub->datalen[s] > 0)

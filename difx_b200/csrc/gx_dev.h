@@ -82,4 +82,10 @@ struct SubintArrays {
   const double *interp;          // [nstations][3]
 };
 
+// Raises `kernel`'s dynamic shared-memory limit on the current device to at
+// least `bytes`.  Safe from several host threads at once: the limit only ever
+// grows, so a launch that opted in for its size cannot be undercut by another
+// thread opting in for a smaller one.
+cudaError_t smem_opt_in(const void *kernel, size_t bytes);
+
 }  // namespace gx

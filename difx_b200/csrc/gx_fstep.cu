@@ -7,14 +7,14 @@
 //   blockparams_kernel  one thread per (station, block): FP64 delay, nearest
 //                       sample, fractional-sample error, linear interpolation
 //                       coefficients, frame-validity mask and data weight.
-//   fstep_warp_kernel   (FFT length <= 1024) one warp per (block, band): the
+//   fstep_r16_kernel    (FFT length 512-8192) a group of F / 16 threads per
+//                       (block, band), 16 samples per thread in registers,
+//                       radix-16 passes with padded shared-memory exchanges.
+//   fstep_warp_kernel   (FFT length 128-256) one warp per (block, band): the
 //                       warp builds its rotator tables, decodes and rotates
 //                       its samples into warp-private shared memory, runs the
 //                       FFT with warp-level synchronisation only and writes
 //                       the corrected spectrum row.
-//   fstep_r16_kernel    (FFT length >= 2048) a group of F / 16 threads per
-//                       (block, band), 16 samples per thread in registers,
-//                       radix-16 passes with padded shared-memory exchanges.
 //   fstep_cta_kernel    (longer FFTs not covered above) the bands of a block
 //                       are transformed concurrently in slots of one CTA.
 //
@@ -30,6 +30,9 @@
 //   fractional-sample correction                  mode.cpp:1256-1261
 #include <cstdint>
 #include <cstdlib>
+#include <map>
+#include <mutex>
+#include <utility>
 #include "gx_dev.h"
 #include "gx_fft16.h"
 
@@ -766,7 +769,7 @@ static int warp_stride(const DevJob &J)
 static bool use_r16_kernel(const DevJob &J)
 {
   const char *e = getenv("GX_FSTEP_R16_MIN");   // smallest length routed to it (tuning runs)
-  const int fmin = e ? atoi(e) : 2048;
+  const int fmin = e ? atoi(e) : 512;
   return J.fftlen >= fmin && J.fftlen >= 512 && J.fftlen <= 8192;
 }
 
@@ -792,11 +795,18 @@ size_t fstep_smem_bytes(const DevJob &J, int nrf, int nslots)
   return b;
 }
 
-template <typename K>
-static cudaError_t opt_in(K kernel, size_t bytes, size_t &have)
+cudaError_t smem_opt_in(const void *kernel, size_t bytes)
 {
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  static std::mutex mu;
+  static std::map<std::pair<const void *, int>, size_t> limits;   // (kernel, device) -> limit set
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  size_t &have = limits[{kernel, dev}];
   if (bytes <= have) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   if (e == cudaSuccess) have = bytes;
   return e;
 }
@@ -818,8 +828,7 @@ cudaError_t fstep_launch(const DevJob &J, const DevStation *stations, int maxnrf
     const int ts = r16_tabstride(J);
 #define GX_R16_CASE(FLV, CX)                                                                          \
     if (J.fftlen == FLV && J.cplx == CX) {                                                            \
-      static size_t have = 48 * 1024;                                                                 \
-      cudaError_t e = opt_in(fstep_r16_kernel<FLV, CX>, sm, have);                                    \
+      cudaError_t e = smem_opt_in((const void *)fstep_r16_kernel<FLV, CX>, sm);                       \
       if (e != cudaSuccess) return e;                                                                 \
       fstep_r16_kernel<FLV, CX><<<grid, R16Launch<FLV>::CTA, sm, st>>>(J, stations, S, bp, nblk, bpc, ts, spec); \
       return cudaGetLastError();                                                                      \
@@ -835,8 +844,7 @@ cudaError_t fstep_launch(const DevJob &J, const DevStation *stations, int maxnrf
     const int ws = warp_stride(J);
 #define GX_WARP_CASE(FLV, CX)                                                                         \
     if (J.fftlen == FLV && J.cplx == CX) {                                                            \
-      static size_t have = 48 * 1024;                                                                 \
-      cudaError_t e = opt_in(fstep_warp_kernel<FLV, CX>, sm, have);                                   \
+      cudaError_t e = smem_opt_in((const void *)fstep_warp_kernel<FLV, CX>, sm);                      \
       if (e != cudaSuccess) return e;                                                                 \
       fstep_warp_kernel<FLV, CX><<<grid, kWarpKernelThreads, sm, st>>>(J, stations, S, bp, nblk, bpc, ws, spec); \
       return cudaGetLastError();                                                                      \
@@ -846,8 +854,7 @@ cudaError_t fstep_launch(const DevJob &J, const DevStation *stations, int maxnrf
 #undef GX_WARP_CASE
   }
   {
-    static size_t have = 48 * 1024;
-    cudaError_t e = opt_in(fstep_cta_kernel, sm, have);
+    cudaError_t e = smem_opt_in((const void *)fstep_cta_kernel, sm);
     if (e != cudaSuccess) return e;
     const int bpc = 2;
     dim3 grid((nblk + bpc - 1) / bpc, J.nstations);

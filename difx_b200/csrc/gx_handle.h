@@ -56,7 +56,8 @@ struct gx_handle {
   int ctrlstride = 0;
   double *d_interp = nullptr;
   std::vector<uint8_t *> d_data;
-  std::vector<int64_t> data_cap;
+  std::vector<int64_t> data_cap;     // usable bytes of d_data[s]
+  std::vector<long long> data_alloc; // allocated bytes of d_data[s]
 
   gx::SubintArrays last{};
   bool have_last = false;
@@ -67,6 +68,16 @@ struct gx_handle {
   std::unique_ptr<HostModel> model;  // only for gx_open_input
   std::unique_ptr<gx::JobMeta> meta; // only for gx_open_input
   std::vector<gx::DevStation> dst;   // host copy of the per-station device constants
+
+  long long dev_bytes = 0;           // device memory held by the handle
+
+  template <typename T>
+  cudaError_t dalloc(T **p, size_t bytes)
+  {
+    cudaError_t e = cudaMalloc(reinterpret_cast<void **>(p), bytes);
+    if (e == cudaSuccess) dev_bytes += (long long)bytes;
+    return e;
+  }
 
   gx_status fail(gx_status s, const std::string &m)
   {

@@ -1,0 +1,288 @@
+// Request loop over resident correlation jobs on one GPU (continuous batching).
+//
+// Jobs are opened handles (their delay models, twiddles, tables and
+// accumulators stay on the device between requests) attached to the server;
+// the device memory they hold counts against the server's HBM budget.
+// Requests -- one subint of one job -- are queued as they arrive and admitted
+// in arrival order by `slots` worker threads as soon as (a) a slot is free,
+// (b) no other request of the same job is on the GPU (a job's device buffers
+// serve one subint at a time), and (c) the memory the request adds keeps the
+// total within the budget (a request is always admitted when nothing else
+// is in flight, so an oversized request cannot stall the loop).  Requests of
+// different jobs therefore run concurrently, each on its job's stream, and a
+// request that arrives while others are on the GPU starts as soon as a slot
+// and memory free up.  Each request's latency runs from submission to the
+// moment its results are in the caller's buffer.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+#include "gx_handle.h"
+
+using Clock = std::chrono::steady_clock;
+
+namespace {
+
+struct Request {
+  long long ticket;
+  int job;
+  gx_subint_desc sub;
+  float *results;
+  long long bytes;
+  Clock::time_point t_submit;
+  gx_status status = GX_OK;
+  double latency_ms = 0;
+  bool done = false;
+};
+
+struct Job {
+  gx_handle *h;
+  long long resident;
+  bool busy = false;
+};
+
+// The default executors: host buffers through gx_subint, or device buffers
+// through gx_subint_device with the result array copied to the caller.
+gx_status run_host(void *, gx_handle *h, int, const gx_subint_desc *sub, float *results)
+{
+  return gx_subint(h, sub, results);
+}
+
+gx_status run_device_inputs(void *, gx_handle *h, int, const gx_subint_desc *sub, float *results)
+{
+  gx_status s = gx_subint_device(h, sub, reinterpret_cast<float *>(h->d_results), nullptr);
+  if (s != GX_OK) return s;
+  CKR(h, cudaMemcpyAsync(results, h->d_results, sizeof(float2) * h->rl, cudaMemcpyDeviceToHost, h->stream));
+  return gx_synchronize(h);
+}
+
+}  // namespace
+
+struct gx_server {
+  int slots = 1;
+  long long budget = 0;
+  bool device_inputs = false;
+  gx_server_executor exec = run_host;
+  void *exec_ctx = nullptr;
+  bool started = false;
+
+  std::vector<Job> jobs;
+  long long resident_total = 0, inflight_bytes = 0;
+  int inflight = 0;
+  std::deque<Request *> queue;
+  std::unordered_map<long long, Request *> reqs;
+  long long next_ticket = 1;
+  std::vector<double> latencies;
+  long long completed = 0, failed = 0;
+  std::string last_error;       // message of the last failed request
+  std::string last_error_copy;  // the copy gx_server_last_error hands out
+
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::vector<std::thread> workers;
+  bool stopping = false;
+
+  // first queued request that can start now (arrival order among the admissible)
+  std::deque<Request *>::iterator pick()
+  {
+    for (auto it = queue.begin(); it != queue.end(); ++it) {
+      const Request *r = *it;
+      if (jobs[r->job].busy) continue;
+      if (inflight > 0 && resident_total + inflight_bytes + r->bytes > budget) continue;
+      return it;
+    }
+    return queue.end();
+  }
+
+  void worker()
+  {
+    std::unique_lock<std::mutex> lk(mu);
+    for (;;) {
+      std::deque<Request *>::iterator it;
+      cv_work.wait(lk, [&] { return (it = pick()) != queue.end() || (stopping && queue.empty()); });
+      if (it == queue.end()) return;   // stopping, and everything queued has been taken
+      Request *r = *it;
+      queue.erase(it);
+      Job &J = jobs[r->job];
+      J.busy = true;
+      inflight++;
+      inflight_bytes += r->bytes;
+      lk.unlock();
+      const gx_status st = exec(exec_ctx, J.h, r->job, &r->sub, r->results);
+      const double ms = std::chrono::duration<double, std::milli>(Clock::now() - r->t_submit).count();
+      lk.lock();
+      J.busy = false;
+      inflight--;
+      inflight_bytes -= r->bytes;
+      r->status = st;
+      r->latency_ms = ms;
+      r->done = true;
+      if (st == GX_OK) {
+        latencies.push_back(ms);
+        completed++;
+      } else {
+        failed++;
+        last_error = "job " + std::to_string(r->job) + ": " + (J.h ? J.h->err : std::string("executor failed"));
+      }
+      cv_done.notify_all();
+      cv_work.notify_all();
+    }
+  }
+
+  void start()
+  {
+    if (started) return;
+    started = true;
+    for (int i = 0; i < slots; i++) workers.emplace_back([this] { worker(); });
+  }
+};
+
+extern "C" {
+
+gx_status gx_server_open(int slots, long long hbm_budget_bytes, int device_inputs, gx_server **out)
+{
+  if (!out || slots < 1 || slots > 64 || hbm_budget_bytes <= 0) return GX_ERR_ARG;
+  gx_server *s = new gx_server();
+  s->slots = slots;
+  s->budget = hbm_budget_bytes;
+  s->device_inputs = device_inputs != 0;
+  s->exec = s->device_inputs ? run_device_inputs : run_host;
+  *out = s;
+  return GX_OK;
+}
+
+gx_status gx_server_set_executor(gx_server *s, gx_server_executor fn, void *ctx)
+{
+  if (!s || !fn) return GX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->started) return GX_ERR_STATE;
+  s->exec = fn;
+  s->exec_ctx = ctx;
+  return GX_OK;
+}
+
+gx_status gx_server_attach(gx_server *s, gx_handle *h, long long resident_bytes, int *job)
+{
+  if (!s || !job) return GX_ERR_ARG;
+  if (!h && resident_bytes < 0) return GX_ERR_ARG;
+  const long long res = resident_bytes >= 0 ? resident_bytes : h->dev_bytes;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (s->resident_total + res > s->budget) return GX_ERR_NOMEM;
+  s->jobs.push_back(Job{h, res});
+  s->resident_total += res;
+  *job = (int)s->jobs.size() - 1;
+  return GX_OK;
+}
+
+gx_status gx_server_submit(gx_server *s, int job, const gx_subint_desc *sub, float *results, long long request_bytes,
+                           long long *ticket)
+{
+  if (!s || !sub || !ticket) return GX_ERR_ARG;
+  std::unique_lock<std::mutex> lk(s->mu);
+  if (job < 0 || job >= (int)s->jobs.size()) return GX_ERR_ARG;
+  long long bytes = request_bytes;
+  if (bytes < 0) {   // what the request adds: growth of the job's input buffers (host inputs only)
+    bytes = 0;
+    const gx_handle *h = s->jobs[job].h;
+    if (h && !s->device_inputs && sub->datalen)
+      for (int i = 0; i < h->jd.nstations && i < (int)h->data_cap.size(); i++)
+        bytes += std::max<long long>(0, (long long)sub->datalen[i] - (long long)h->data_cap[i]);
+  }
+  if (s->resident_total + bytes > s->budget) return GX_ERR_NOMEM;
+  Request *r = new Request();
+  r->ticket = s->next_ticket++;
+  r->job = job;
+  r->sub = *sub;
+  r->results = results;
+  r->bytes = bytes;
+  r->t_submit = Clock::now();
+  s->queue.push_back(r);
+  s->reqs[r->ticket] = r;
+  *ticket = r->ticket;
+  s->start();
+  s->cv_work.notify_one();
+  return GX_OK;
+}
+
+gx_status gx_server_wait(gx_server *s, long long ticket, double *latency_ms)
+{
+  if (!s) return GX_ERR_ARG;
+  std::unique_lock<std::mutex> lk(s->mu);
+  auto it = s->reqs.find(ticket);
+  if (it == s->reqs.end()) return GX_ERR_ARG;
+  Request *r = it->second;
+  s->cv_done.wait(lk, [&] { return r->done; });
+  const gx_status st = r->status;
+  if (latency_ms) *latency_ms = r->latency_ms;
+  s->reqs.erase(it);
+  delete r;
+  return st;
+}
+
+gx_status gx_server_stats(gx_server *s, int reset, gx_latency_stats *out)
+{
+  if (!s || !out) return GX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  memset(out, 0, sizeof(*out));
+  out->completed = s->completed;
+  out->failed = s->failed;
+  std::vector<double> v = s->latencies;
+  if (!v.empty()) {
+    std::sort(v.begin(), v.end());
+    // percentile with linear interpolation between order statistics
+    auto pct = [&](double p) {
+      const double x = p / 100.0 * (double)(v.size() - 1);
+      const size_t i = (size_t)x;
+      const double f = x - (double)i;
+      return i + 1 < v.size() ? v[i] * (1 - f) + v[i + 1] * f : v[i];
+    };
+    out->p50_ms = pct(50);
+    out->p95_ms = pct(95);
+    out->p99_ms = pct(99);
+    double sum = 0;
+    for (double x : v) sum += x;
+    out->mean_ms = sum / (double)v.size();
+    out->max_ms = v.back();
+  }
+  if (reset) {
+    s->latencies.clear();
+    s->completed = s->failed = 0;
+  }
+  return GX_OK;
+}
+
+gx_status gx_server_close(gx_server *s)
+{
+  if (!s) return GX_ERR_ARG;
+  {
+    std::unique_lock<std::mutex> lk(s->mu);
+    s->stopping = true;
+    s->cv_work.notify_all();
+  }
+  for (auto &t : s->workers) t.join();
+  for (auto &kv : s->reqs) delete kv.second;
+  delete s;
+  return GX_OK;
+}
+
+const char *gx_server_last_error(gx_server *s)
+{
+  if (!s) return "null server";
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->last_error_copy = s->last_error;
+  return s->last_error_copy.c_str();
+}
+
+gx_status gx_device_bytes(const gx_handle *h, long long *bytes)
+{
+  if (!h || !bytes) return GX_ERR_ARG;
+  *bytes = h->dev_bytes;
+  return GX_OK;
+}
+
+}  // extern "C"

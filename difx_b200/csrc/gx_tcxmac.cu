@@ -523,13 +523,8 @@ cudaError_t xmac_tc_launch(const float2 *spec, int nblk, int N, int nfreqs, int 
   dim3 grid(N / 2, nfreqs, ks);
 #define GX_TC_CASE(H)                                                                                       \
   if (hilo == H) {                                                                                          \
-    static bool opted = false;                                                                              \
-    if (!opted) {                                                                                           \
-      cudaError_t e = cudaFuncSetAttribute(xmac_tc_kernel<H>, cudaFuncAttributeMaxDynamicSharedMemorySize,   \
-                                           (int)sm);                                                        \
-      if (e != cudaSuccess) return e;                                                                       \
-      opted = true;                                                                                         \
-    }                                                                                                       \
+    cudaError_t e = smem_opt_in((const void *)xmac_tc_kernel<H>, sm);                                       \
+    if (e != cudaSuccess) return e;                                                                         \
     xmac_tc_kernel<H><<<grid, kThreads, sm, st>>>(map, nblk, N / 2, nfreqs, ks, scale, acc, accumulate, err); \
     return cudaGetLastError();                                                                              \
   }

@@ -202,13 +202,8 @@ static cudaError_t launch_t(const float2 *spec, int nblk, int NI, int N, int nfr
   const int nsuper = (NI + ST - 1) / ST;
   const int npairs = nsuper * (nsuper + 1) / 2;
   const size_t sm = sizeof(float2) * 2 * NSTAGE * KB * ST * CT;
-  static size_t have = 48 * 1024;
-  if (sm > have) {
-    cudaError_t e = cudaFuncSetAttribute(xmac_fp32_kernel<T, ST, CT, KB, NSTAGE>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    have = sm;
-  }
+  cudaError_t e = smem_opt_in((const void *)xmac_fp32_kernel<T, ST, CT, KB, NSTAGE>, sm);
+  if (e != cudaSuccess) return e;
   dim3 grid((N + CT - 1) / CT, npairs, nfreqs * ks);
   xmac_fp32_kernel<T, ST, CT, KB, NSTAGE>
       <<<grid, CT *(ST / T) * (ST / T), sm, st>>>(spec, nblk, NI, N, nsuper, ks, acc);

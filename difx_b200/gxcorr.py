@@ -39,8 +39,9 @@ def lib():
         L = C.CDLL(LIBPATH)
         L.gx_last_error.restype = C.c_char_p
         L.gx_status_string.restype = C.c_char_p
+        L.gx_server_last_error.restype = C.c_char_p
         for name in EXPORTED_SYMBOLS:
-            if name not in ("gx_last_error", "gx_status_string"):
+            if name not in ("gx_last_error", "gx_status_string", "gx_server_last_error"):
                 getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -50,7 +51,9 @@ EXPORTED_SYMBOLS = ("gx_open", "gx_open_input", "gx_close", "gx_last_error", "gx
                     "gx_get_layout", "gx_get_offsets", "gx_interpolator", "gx_scan_start_sec", "gx_subint",
                     "gx_subint_device", "gx_synchronize", "gx_spectra", "gx_stage_times", "gx_launch_count",
                     "gx_subint_device_noalloc", "gx_set_tc_scales", "gx_vis_open", "gx_vis_add", "gx_vis_write",
-                    "gx_vis_close", "gx_uvw")
+                    "gx_vis_close", "gx_uvw", "gx_server_open", "gx_server_set_executor", "gx_server_attach",
+                    "gx_server_submit", "gx_server_wait", "gx_server_stats", "gx_server_close", "gx_device_bytes",
+                    "gx_server_last_error")
 
 
 def subint_device_noalloc(jd: capi.JobDesc, sd: capi.SubintDesc, dev_results_ptr: int, stream_ptr: int = 0) -> None:
@@ -145,6 +148,12 @@ class Correlator:
         self._check(lib().gx_stage_times(self.h, ms))
         return np.array(list(ms))
 
+    def device_bytes(self) -> int:
+        """Device memory the handle holds (gx_device_bytes)."""
+        n = C.c_longlong(0)
+        self._check(lib().gx_device_bytes(self.h, C.byref(n)))
+        return n.value
+
     def launch_count(self) -> int:
         n = C.c_int(0)
         self._check(lib().gx_launch_count(self.h, C.byref(n)))
@@ -204,6 +213,74 @@ class Visibility:
         if self.v:
             lib().gx_vis_close(self.v)
             self.v = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class LatencyStats(C.Structure):
+    _fields_ = [("completed", C.c_longlong), ("failed", C.c_longlong), ("p50_ms", C.c_double),
+                ("p95_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("max_ms", C.c_double)]
+
+
+EXECUTOR = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p)
+
+
+class Server:
+    """Request loop over resident jobs on one GPU (gx_server_*): continuous
+    batching of subint requests under an HBM budget, with latency statistics."""
+
+    def __init__(self, slots: int, hbm_budget_bytes: int, device_inputs: bool = False):
+        self.s = C.c_void_p()
+        self._check(lib().gx_server_open(int(slots), C.c_longlong(int(hbm_budget_bytes)), 1 if device_inputs else 0,
+                                         C.byref(self.s)))
+        self._keep = []   # descriptors and buffers of requests in flight
+
+    def _check(self, st: int):
+        if st != 0:
+            msg = lib().gx_server_last_error(self.s).decode() if getattr(self, "s", None) else ""
+            raise GxError(st, msg or "gx_server call failed")
+
+    def set_executor(self, fn) -> None:
+        """fn(job, sub_ptr, results_ptr) -> status; replaces the default executor."""
+        cb = EXECUTOR(lambda ctx, h, job, sub, res: int(fn(job, sub, res)))
+        self._cb = cb
+        self._check(lib().gx_server_set_executor(self.s, cb, None))
+
+    def attach(self, corr: Optional[Correlator] = None, resident_bytes: int = -1) -> int:
+        job = C.c_int(-1)
+        self._check(lib().gx_server_attach(self.s, corr.h if corr else None, C.c_longlong(int(resident_bytes)),
+                                           C.byref(job)))
+        return job.value
+
+    def submit(self, job: int, sd: capi.SubintDesc, results_ptr: int = 0, request_bytes: int = -1,
+               keep=None) -> int:
+        t = C.c_longlong(0)
+        self._check(lib().gx_server_submit(self.s, job, sd.ptr(), C.c_void_p(results_ptr) if results_ptr else None,
+                                           C.c_longlong(int(request_bytes)), C.byref(t)))
+        self._keep.append((t.value, sd, keep))
+        return t.value
+
+    def wait(self, ticket: int) -> float:
+        ms = C.c_double(0)
+        st = lib().gx_server_wait(self.s, C.c_longlong(ticket), C.byref(ms))
+        self._keep = [k for k in self._keep if k[0] != ticket]
+        self._check(st)
+        return ms.value
+
+    def stats(self, reset: bool = False) -> LatencyStats:
+        out = LatencyStats()
+        self._check(lib().gx_server_stats(self.s, 1 if reset else 0, C.byref(out)))
+        return out
+
+    def close(self) -> None:
+        if self.s:
+            lib().gx_server_close(self.s)
+            self.s = None
+            self._keep = []
 
     def __del__(self):
         try:

@@ -232,6 +232,55 @@ gx_status gx_vis_close(gx_vis *v);
    of scan, first phase centre. */
 gx_status gx_uvw(gx_handle *h, int scan, double offset, int ds1, int ds2, double out[3]);
 
+/* ---- Request loop (continuous batching of subints of resident jobs) ------ */
+
+/* Opened handles are attached as jobs; their device memory (delay model,
+   twiddles, tables, accumulators, input buffers) stays resident and counts
+   against the server's HBM budget.  Submitted requests -- one subint of one
+   job -- are admitted in arrival order by `slots` worker threads as soon as a
+   slot is free, no other request of the same job is on the GPU, and the
+   memory the request adds keeps the total within the budget (a request is
+   always admitted when nothing else is in flight).  Requests of different jobs
+   run concurrently, each on its job's stream.  Latency runs from submission to
+   results in the caller's buffer.  The buffers a submission points to must
+   stay valid until gx_server_wait returns for it.  No counterpart in the
+   reference, whose FxManager (fxmanager.cpp:301-529) hands subints to Core
+   processes over MPI. */
+typedef struct gx_server gx_server;
+
+/* Runs one request; the default is gx_subint (host buffers) or, with
+   device_inputs, gx_subint_device followed by a copy of the result array to
+   `results`.  h is the attached handle (may be NULL for a custom executor). */
+typedef gx_status (*gx_server_executor)(void *ctx, gx_handle *h, int job, const gx_subint_desc *sub,
+                                        float *results);
+
+typedef struct gx_latency_stats {
+  long long completed, failed;
+  double p50_ms, p95_ms, p99_ms, mean_ms, max_ms;   /* latency of completed requests */
+} gx_latency_stats;
+
+gx_status gx_server_open(int slots, long long hbm_budget_bytes, int device_inputs, gx_server **out);
+/* Replaces the executor (before the first submission). */
+gx_status gx_server_set_executor(gx_server *s, gx_server_executor fn, void *ctx);
+/* resident_bytes < 0: the handle's own device memory (gx_device_bytes).
+   GX_ERR_NOMEM when the resident total would exceed the budget. */
+gx_status gx_server_attach(gx_server *s, gx_handle *h, long long resident_bytes, int *job);
+/* request_bytes < 0: the growth of the job's input buffers a host-buffer
+   request needs (0 with device inputs).  GX_ERR_NOMEM if it can never fit. */
+gx_status gx_server_submit(gx_server *s, int job, const gx_subint_desc *sub, float *results, long long request_bytes,
+                           long long *ticket);
+/* Blocks until the request has completed; returns its status and latency. */
+gx_status gx_server_wait(gx_server *s, long long ticket, double *latency_ms);
+/* Latency percentiles of the requests completed so far (reset: start over). */
+gx_status gx_server_stats(gx_server *s, int reset, gx_latency_stats *out);
+/* Finishes every queued request, then stops the workers. */
+gx_status gx_server_close(gx_server *s);
+/* Message of the last request that failed (its job and the handle's error). */
+const char *gx_server_last_error(gx_server *s);
+
+/* Device memory a handle holds, bytes. */
+gx_status gx_device_bytes(const gx_handle *h, long long *bytes);
+
 /* Operand scales of the tensor-core X-step for one band of one datastream:
    scales[c] multiplies channel c of that band's spectra before they are
    rounded to FP16 and is divided out of every visibility.  Each value is

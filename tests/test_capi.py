@@ -17,7 +17,8 @@ HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))
 def declared_functions():
     src = open(HEADER).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(gx_[a-z_]+)\s*\(", src)))
+    # function declarations: a return type at the start of a line, then the name and "("
+    return sorted(set(re.findall(r"^\s*(?:gx_status|const\s+char\s*\*)\s*(gx_[a-z_]+)\s*\(", src, re.M)))
 
 
 def test_header_and_binding_agree():

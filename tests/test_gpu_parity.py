@@ -157,3 +157,20 @@ def test_gpu_device_entry_point(gx, oracle_lib):
     g_dev = out.cpu().numpy().view(np.complex64)
     np.testing.assert_array_equal(g_dev, g_host)
     c.close()
+
+
+@pytest.mark.parametrize("case", ["c2small", "real2_2048_lsb"])
+def test_gpu_fstep_kernel_choices_agree(case, gx, oracle_lib, monkeypatch):
+    """Each F-step kernel a transform length can be routed to (radix-16
+    register kernel, warp kernel for <= 1024 points, CTA-slot kernel above)
+    matches the oracle on the same subint."""
+    spec, kw = CASES[case]()
+    prep = jobs.prepare(spec, [100_000_000], **kw)
+    o = oracle_lib.subint(prep.jd, prep.sds[0], _params(oracle_lib, spec))
+    for r16_min in ("512", "1000000"):
+        monkeypatch.setenv("GX_FSTEP_R16_MIN", r16_min)
+        c = gx.Correlator.from_desc(prep.jd)
+        g = c.subint(prep.sds[0])
+        c.close()
+        m, wrel = _compare(g, o, prep.jd, spec, oracle_lib)
+        assert m < REC_TOL and wrel < W_TOL, (r16_min, m, wrel)
