@@ -55,8 +55,8 @@ from difx_b200.jobfiles import JobSpec, Subband, write_job  # noqa: E402
 METRIC = "Gsamp/s correlated"
 UNIT = "Gsamp/s"
 XSTEPS = {"fp32": capi.GX_XSTEP_FP32, "tc": capi.GX_XSTEP_TC_FP16, "tc_hilo": capi.GX_XSTEP_TC_FP16_HILO}
-DEFAULT_SUBINT_MS = {"c3": 128.0, "c2": 200.0, "c1": 200.0, "c5": 0.0}
-DEFAULT_XSTEP = {"c3": "tc_hilo", "c2": "fp32", "c1": "fp32", "c5": "tc_hilo"}
+DEFAULT_SUBINT_MS = {"c3": 128.0, "c2": 200.0, "c1": 200.0, "c4": 0.0, "c5": 0.0}
+DEFAULT_XSTEP = {"c3": "tc_hilo", "c2": "fp32", "c1": "fp32", "c4": "tc_hilo", "c5": "tc_hilo"}
 RHO = {"c3": 0.01, "c2": 0.02, "c1": 0.05}
 
 
@@ -295,7 +295,7 @@ def roofline(spec: JobSpec, xstep: str, stage, peaks):
     spec_bytes = nblk * spec.nstations * spec.nbands * spec.nchan * 8
     stages = {"F": f_ms, "X": x_ms, "finalise": fin_ms}
     if f_ms >= x_ms:
-        k = "fstep_r16_kernel" if spec.fftchannels >= 2048 else "fstep_warp_kernel"
+        k = "fstep_r16_kernel" if spec.fftchannels >= 512 else "fstep_warp_kernel"
         a = (in_bytes + spec_bytes) / (f_ms * 1e-3) / 1e9
         return {"kernel": k, "bound": "hbm", "achieved": a, "peak": hbm_peak, "unit": "GB/s", "frac": a / hbm_peak,
                 "traffic": None, "peak_source": src, "algorithmic_bytes_per_step": in_bytes + spec_bytes,
@@ -338,6 +338,134 @@ def c5_jobs(njobs=12, seed=2030):
                            nbits=2, payload_bytes=8000, subint_ns=subint_ns, execute_seconds=20, int_time=1.0,
                            max_delay_us=100.0, max_rate_us_per_s=3.0, seed=3000 + j))
     return out
+
+
+def c4_jobs(njobs=200, seed=4040):
+    """Uneven batch: 200 jobs of U{3..32} stations, 64/256/1024/4096 channels,
+    1-, 2- or 8-bit samples (8-bit real or complex), 1-16 recorded bands
+    (subbands x polarisations, a power of two as VDIF requires, and enough of
+    them that a time sample fills whole bytes) at 8-64 MHz,
+    0.1-1 s subints (whole FFT blocks), correlation coefficient 0.005-0.1."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for j in range(njobs):
+        nst = int(rng.integers(3, 33))
+        nchan = int(rng.choice([64, 256, 1024, 4096]))
+        nbits = int(rng.choice([1, 2, 8]))
+        # a time sample of all bands fills whole bytes: 1-bit >= 8 bands, 2-bit >= 4
+        nbands = int(rng.choice([b for b in (1, 2, 4, 8, 16) if b * nbits >= 8]))
+        bw = float(rng.choice([8.0, 16.0, 32.0, 64.0]))
+        cplx = nbits == 8 and rng.random() < 0.5
+        pols = ("R", "L") if nbands > 1 and rng.random() < 0.5 else ("R",)
+        nsub = nbands // len(pols)
+        sub = float(rng.uniform(0.1, 1.0))
+        rho = float(rng.uniform(0.005, 0.1))
+        block_ns = nchan / bw * 1000   # N channels from N complex or 2N real samples
+        subint_ns = max(1, int(round(sub * 1e9 / block_ns))) * int(round(block_ns))
+        out.append((JobSpec(name=f"c4_{j}", nstations=nst, pols=pols,
+                            subbands=[Subband(4000.0 + bw * i, bw, "U", nchan) for i in range(nsub)],
+                            nbits=nbits, sampling="COMPLEX" if cplx else "REAL", payload_bytes=8000,
+                            subint_ns=subint_ns, execute_seconds=4, int_time=1.0, max_delay_us=100.0,
+                            max_rate_us_per_s=3.0, seed=5000 + j), rho))
+    return out
+
+
+def run_c4(args):
+    """One subint of each of 200 uneven resident jobs per step (gx_batch):
+    per-job launches on one stream against the branch-stream schedule
+    replayed as one CUDA graph (branch count tuned on the first steps)."""
+    import torch
+    from difx_b200.gxcorr import Batch, Correlator
+    t_setup = time.perf_counter()
+    staged = []
+    for spec, rho in c4_jobs():
+        d = tempfile.mkdtemp(prefix="gxc4_")
+        paths = write_job(spec, d)
+        # one synthesised station stream, shared by every station of the job
+        one = JobSpec(**{**spec.__dict__, "nstations": 1})
+        si = build_input(one, 200_000_000, rho=rho)
+        m = Correlator.from_input(paths["input"], device=-1)
+        interp = np.array([m.interpolator(s, 0, si.sec, si.ns) for s in range(spec.nstations)])
+        m.close()
+        dev = torch.from_numpy(si.data[0]).cuda()
+        n = spec.nstations
+        sd = capi.SubintDesc(si.scan, si.sec, si.ns, 0.0, [dev.data_ptr()] * n, [len(si.data[0])] * n,
+                             [si.control[0].ctypes.data] * n, len(si.control[0]), interp)
+        staged.append((spec, sd, dev, si))
+    torch.cuda.synchronize()
+    corrs, res = [], []
+    for spec, *_ in staged:
+        # spectra buffer of about 256 MB per job (the tensor-core form pads a freq to 128 inputs)
+        row = len(spec.subbands) * 128 * spec.nchan * 8
+        chunk = int(max(16, min(spec.blocks_per_send, (256 << 20) // row)))
+        c = Correlator.from_desc(capi.job_desc_from_spec(spec, xstep=capi.GX_XSTEP_AUTO, block_chunk=chunk))
+        corrs.append(c)
+        res.append(torch.empty(2 * c.result_length, dtype=torch.float32, device="cuda"))
+    subs = [sd for _, sd, _, _ in staged]
+    ptrs = [r.data_ptr() for r in res]
+    setup_s = time.perf_counter() - t_setup
+    samples = sum(samples_per_subint(s) for s, *_ in staged)
+    steps = max(1, args.c4_steps)
+
+    def timed(b, nsteps, clk=None):
+        dev_ms, wall = [], time.perf_counter()
+        if clk:
+            clk.mark(0)
+        for _ in range(nsteps):
+            b.run(subs)
+            dev_ms.append(b.synchronize())
+        if clk:
+            clk.mark(1)
+        return float(np.sum(dev_ms)), (time.perf_counter() - wall) * 1e3
+
+    modes = {}
+    # per-job launches: one job after another on one stream
+    b = Batch(corrs, ptrs, mode="serial")
+    timed(b, 1)
+    ms, wall = timed(b, steps)
+    modes["per_job_launches"] = {"gsamp_s": samples * steps / (ms * 1e-3) / 1e9, "device_ms_per_step": ms / steps,
+                                 "wall_ms_per_step": wall / steps, "gpu_launches_per_step": b.info()[2]}
+    b.close()
+    # branch streams replayed as one graph; the branch count is tuned on the first steps
+    with ClockSampler(0) as clk:
+        b = Batch(corrs, ptrs, mode="graph", nstreams=0)
+        tune = []
+        while b.info()[1]:
+            b.run(subs)
+            tune.append(b.synchronize())
+        k = b.info()[0]
+        ms, wall = timed(b, steps, clk)
+        launches = b.info()[2]
+        b.close()
+    clocks = clk.summary()
+    modes["graph"] = {"gsamp_s": samples * steps / (ms * 1e-3) / 1e9, "device_ms_per_step": ms / steps,
+                      "wall_ms_per_step": wall / steps, "branches": k, "tuning_ms": tune,
+                      "gpu_launches_per_step": launches, "host_launches_per_step": 1}
+    # the same schedule issued stream by stream (no graph)
+    b = Batch(corrs, ptrs, mode="streams", nstreams=k)
+    timed(b, 1)
+    ms_s, wall_s = timed(b, steps)
+    modes["streams"] = {"gsamp_s": samples * steps / (ms_s * 1e-3) / 1e9, "device_ms_per_step": ms_s / steps,
+                        "wall_ms_per_step": wall_s / steps, "branches": k}
+    b.close()
+    forms = {}
+    for c in corrs:
+        forms[c.info.xstep] = forms.get(c.info.xstep, 0) + 1
+        c.close()
+    value = modes["graph"]["gsamp_s"]
+    line = {"metric": "C4 batch: Gsamp/s correlated over 200 uneven jobs (one subint each per step)", "value": value,
+            "unit": "Gsamp/s", "n_gpus": 1, "steps": steps, "warmup": len(tune), "ms_per_step": ms / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "per job: f32, or f16 hi+lo operands with f32 accumulation (GX_XSTEP_AUTO)",
+            "data": "synthetic (seeded VDIF, one stream per job shared by its stations), inputs device-resident",
+            "config": {"workload": "C4: 200 jobs, U{3..32} stations, 64/256/1024/4096 ch, 1/2/8-bit, 1-16 bands "
+                                   "at 8-64 MHz, 0.1-1 s subints", "samples_per_step": samples,
+                       "xstep_forms": {{0: "fp32", 2: "tc_hilo"}.get(f, str(f)): n for f, n in forms.items()},
+                       "l2": "inputs larger than L2 (no flush)", "setup_s": setup_s},
+            "modes": modes, "graph_vs_per_job_launches": value / modes["per_job_launches"]["gsamp_s"],
+            "gpu_launches": launches, "clocks": clocks}
+    print(json.dumps(line))
+    return 0
 
 
 def run_c5(args):
@@ -440,7 +568,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gxcorr", choices=["gxcorr", "reference"])
-    ap.add_argument("--config", default="c3", choices=["c3", "c2", "c1", "c5"])
+    ap.add_argument("--config", default="c3", choices=["c3", "c2", "c1", "c4", "c5"])
+    ap.add_argument("--c4-steps", type=int, default=1, help="timed batch steps per mode (C4)")
     ap.add_argument("--c5-slots", type=int, default=4)
     ap.add_argument("--c5-seconds", type=float, default=20.0)
     ap.add_argument("--c5-rate", type=float, default=0.0, help="requests per second (0: 70%% of capacity)")
@@ -458,6 +587,8 @@ def main():
         return run_reference_arm(args)
     if args.config == "c5":
         return run_c5(args)
+    if args.config == "c4":
+        return run_c4(args)
 
     import torch
     from difx_b200.gxcorr import Correlator

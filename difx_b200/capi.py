@@ -22,6 +22,7 @@ GX_MAX_POLPRODUCTS = 4
 GX_XSTEP_FP32 = 0
 GX_XSTEP_TC_FP16 = 1
 GX_XSTEP_TC_FP16_HILO = 2
+GX_XSTEP_AUTO = 3
 
 STATUS_NAMES = {0: "GX_OK", 1: "GX_ERR_ARG", 2: "GX_ERR_UNSUPPORTED", 3: "GX_ERR_CUDA", 4: "GX_ERR_NOMEM",
                 5: "GX_ERR_IO", 6: "GX_ERR_MODEL", 7: "GX_ERR_TIMEOUT", 8: "GX_ERR_STATE"}
@@ -76,7 +77,7 @@ class gx_subint_desc(C.Structure):
 class gx_layout_info(C.Structure):
     _fields_ = [("result_length", C.c_int64), ("nfreqs", C.c_int), ("nbaselines", C.c_int),
                 ("nstations", C.c_int), ("blocks_per_send", C.c_int), ("xmac_stride", C.c_int),
-                ("array_stride", C.c_int), ("fftchannels", C.c_int), ("nchan", C.c_int)]
+                ("array_stride", C.c_int), ("fftchannels", C.c_int), ("nchan", C.c_int), ("xstep", C.c_int)]
 
 
 class JobDesc:

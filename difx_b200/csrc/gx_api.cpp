@@ -48,12 +48,16 @@ static void free_all(gx_handle *h)
 {
   if (h->device < 0) return;
   void *ptrs[] = {h->d_st, h->d_tw, h->d_spec, h->d_acc, h->d_results, h->d_spec1, h->d_w, h->d_wacc, h->d_w1,
-                  h->d_pairs, h->d_prods, h->d_went, (void *)h->d_dataptrs, h->d_datalen, h->d_ctrl, h->d_interp,
-                  h->d_bp, h->d_bp1, h->d_scale, h->d_tcprods, h->d_tcrows, h->d_err};
+                  h->d_pairs, h->d_prods, h->d_went, h->d_sub, h->d_bp, h->d_bp1, h->d_scale, h->d_tcprods,
+                  h->d_tcrows, h->d_err};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->h_err) cudaFreeHost(h->h_err);
   h->h_err = nullptr;
+  if (h->h_sub) cudaFreeHost(h->h_sub);
+  h->h_sub = nullptr;
+  if (h->ev_sub) cudaEventDestroy(h->ev_sub);
+  h->ev_sub = nullptr;
   for (auto p : h->d_data)
     if (p) cudaFree(p);
   for (auto e : h->evs) cudaEventDestroy(e);
@@ -194,9 +198,15 @@ static gx_status setup(gx_handle *h)
   }
   int ni = 0;
   for (int f = 0; f < d.nfreqs; f++) ni = count[f] > ni ? count[f] : ni;
-  if (d.xstep < GX_XSTEP_FP32 || d.xstep > GX_XSTEP_TC_FP16_HILO) return h->fail(GX_ERR_ARG, "unknown xstep");
-  h->tc = d.xstep != GX_XSTEP_FP32;
-  h->hilo = d.xstep == GX_XSTEP_TC_FP16_HILO;
+  if (d.xstep < GX_XSTEP_FP32 || d.xstep > GX_XSTEP_AUTO) return h->fail(GX_ERR_ARG, "unknown xstep");
+  h->xstep = d.xstep;
+  if (d.xstep == GX_XSTEP_AUTO) {
+    const char *e = getenv("GX_XSTEP_AUTO_MIN_INPUTS");
+    const int nmin = e ? atoi(e) : 48;
+    h->xstep = (ni >= nmin && ni <= kTcInputs && J.nchan >= 2) ? GX_XSTEP_TC_FP16_HILO : GX_XSTEP_FP32;
+  }
+  h->tc = h->xstep != GX_XSTEP_FP32;
+  h->hilo = h->xstep == GX_XSTEP_TC_FP16_HILO;
   if (h->tc) {
     if (ni > kTcInputs)
       return h->fail(GX_ERR_UNSUPPORTED, "the tensor-core X-step takes at most 128 inputs (station bands) per freq");
@@ -517,11 +527,16 @@ static gx_status setup(gx_handle *h)
   if (!h->wents.empty())
     CKR(h, cudaMemcpy(h->d_went, h->wents.data(), sizeof(WeightEntry) * h->wents.size(), cudaMemcpyHostToDevice));
   CKR(h, h->dalloc(&h->d_results, sizeof(float2) * h->rl));
-  CKR(h, h->dalloc((void **)&h->d_dataptrs, sizeof(uint8_t *) * d.nstations));
-  CKR(h, h->dalloc(&h->d_datalen, sizeof(int64_t) * d.nstations));
   h->ctrlstride = 3 + J.flaglen;
-  CKR(h, h->dalloc(&h->d_ctrl, sizeof(int32_t) * h->ctrlstride * d.nstations));
-  CKR(h, h->dalloc(&h->d_interp, sizeof(double) * 3 * d.nstations));
+  h->o_len = sizeof(SubintClock);
+  h->o_ptr = h->o_len + sizeof(int64_t) * d.nstations;
+  h->o_interp = h->o_ptr + sizeof(uint8_t *) * d.nstations;
+  h->o_ctrl = h->o_interp + sizeof(double) * 3 * d.nstations;
+  h->sub_bytes = h->o_ctrl + sizeof(int32_t) * h->ctrlstride * d.nstations;
+  CKR(h, h->dalloc(&h->d_sub, h->sub_bytes));
+  CKR(h, cudaMallocHost(&h->h_sub, h->sub_bytes));
+  memset(h->h_sub, 0, h->sub_bytes);
+  CKR(h, cudaEventCreateWithFlags(&h->ev_sub, cudaEventDisableTiming));
   h->d_data.assign(d.nstations, nullptr);
   h->data_cap.assign(d.nstations, 0);
   h->data_alloc.assign(d.nstations, 0);
@@ -645,6 +660,7 @@ gx_status gx_get_layout(const gx_handle *h, gx_layout_info *info)
   info->array_stride = h->J.stride;
   info->fftchannels = h->J.fftlen;
   info->nchan = h->J.nchan;
+  info->xstep = h->xstep;
   return GX_OK;
 }
 
@@ -668,75 +684,99 @@ static gx_status record(gx_handle *h, cudaStream_t st, int stage, bool start)
   return GX_OK;
 }
 
-// Runs one subint whose data buffers are already device pointers.
-static gx_status run_device(gx_handle *h, const gx_subint_desc *sub, const uint8_t *const *devdata,
-                            float2 *dev_results, cudaStream_t st)
+}  // extern "C"
+
+// Writes the per-subint tables of `sub` (data in device buffers `devdata`)
+// into the handle's pinned block.
+static gx_status stage_subint(gx_handle *h, const gx_subint_desc *sub, const uint8_t *const *devdata)
 {
   const gx_job_desc &d = h->jd;
-  const DevJob &J = h->J;
-  for (auto e : h->evs) cudaEventDestroy(e);
-  h->evs.clear();
-  h->ev_stage.clear();
-  h->launches = 0;
-  if (sub->controllen < 3 + J.flaglen) return h->fail(GX_ERR_ARG, "control buffer shorter than 3 + flag words");
-  // small per-subint tables
-  std::vector<int32_t> ctrl((size_t)h->ctrlstride * d.nstations, 0);
-  std::vector<int64_t> lens(d.nstations);
-  std::vector<double> interp(3 * d.nstations);
-  for (int s = 0; s < d.nstations; s++) {
+  if (sub->controllen < h->ctrlstride) return h->fail(GX_ERR_ARG, "control buffer shorter than 3 + flag words");
+  for (int s = 0; s < d.nstations; s++)
     if (!sub->control[s]) return h->fail(GX_ERR_ARG, "missing control buffer");
-    memcpy(&ctrl[(size_t)s * h->ctrlstride], sub->control[s], sizeof(int32_t) * h->ctrlstride);
+  if (!sub->interp && !h->model)
+    return h->fail(GX_ERR_ARG, "no interpolators given and the handle has no delay model");
+  // the previous subint's copy of the block must have left it
+  if (h->ev_sub_pending) {
+    CKR(h, cudaEventSynchronize(h->ev_sub));
+    h->ev_sub_pending = false;
+  }
+  unsigned char *b = h->h_sub;
+  *reinterpret_cast<SubintClock *>(b) = SubintClock{sub->sec, sub->ns, sub->scan_start_sec};
+  int64_t *lens = reinterpret_cast<int64_t *>(b + h->o_len);
+  const uint8_t **ptrs = reinterpret_cast<const uint8_t **>(b + h->o_ptr);
+  double *interp = reinterpret_cast<double *>(b + h->o_interp);
+  int32_t *ctrl = reinterpret_cast<int32_t *>(b + h->o_ctrl);
+  for (int s = 0; s < d.nstations; s++) {
+    memcpy(ctrl + (size_t)s * h->ctrlstride, sub->control[s], sizeof(int32_t) * h->ctrlstride);
     lens[s] = sub->datalen[s];
+    ptrs[s] = devdata[s];
   }
   if (sub->interp) {
-    memcpy(interp.data(), sub->interp, sizeof(double) * 3 * d.nstations);
+    memcpy(interp, sub->interp, sizeof(double) * 3 * d.nstations);
   } else {
-    if (!h->model) return h->fail(GX_ERR_ARG, "no interpolators given and the handle has no delay model");
     for (int s = 0; s < d.nstations; s++) {
       gx_status r = h->model->interpolator(s, sub->scan, sub->sec, sub->ns, &interp[3 * s]);
       if (r != GX_OK) return h->fail(r, "no delay model for this subint");
     }
   }
-  CKR(h, cudaMemcpyAsync(h->d_ctrl, ctrl.data(), sizeof(int32_t) * ctrl.size(), cudaMemcpyHostToDevice, st));
-  CKR(h, cudaMemcpyAsync(h->d_datalen, lens.data(), sizeof(int64_t) * lens.size(), cudaMemcpyHostToDevice, st));
-  CKR(h, cudaMemcpyAsync(h->d_interp, interp.data(), sizeof(double) * interp.size(), cudaMemcpyHostToDevice, st));
-  CKR(h, cudaMemcpyAsync(h->d_dataptrs, devdata, sizeof(uint8_t *) * d.nstations, cudaMemcpyHostToDevice, st));
+  return GX_OK;
+}
+
+// Enqueues the device work of the staged subint on `st`: the tables' copy,
+// F-step, X-step and finalisation into dev_results.  Nothing here waits on
+// the host, so the sequence can be captured into a CUDA graph (h->untimed:
+// no events recorded; the graph's copy reads the pinned block at replay).
+gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
+{
+  const gx_job_desc &d = h->jd;
+  const DevJob &J = h->J;
+  const bool timed = !h->untimed;
+  if (timed) {
+    for (auto e : h->evs) cudaEventDestroy(e);
+    h->evs.clear();
+    h->ev_stage.clear();
+  }
+  h->launches = 0;
+  CKR(h, cudaMemcpyAsync(h->d_sub, h->h_sub, h->sub_bytes, cudaMemcpyHostToDevice, st));
+  if (timed) {
+    CKR(h, cudaEventRecord(h->ev_sub, st));
+    h->ev_sub_pending = true;
+  }
   SubintArrays S{};
-  S.sec = sub->sec;
-  S.ns = sub->ns;
-  S.scan_start_sec = sub->scan_start_sec;
-  S.data = h->d_dataptrs;
-  S.datalen = h->d_datalen;
-  S.control = h->d_ctrl;
+  S.clock = reinterpret_cast<const SubintClock *>(h->d_sub);
+  S.data = reinterpret_cast<const uint8_t *const *>(h->d_sub + h->o_ptr);
+  S.datalen = reinterpret_cast<const int64_t *>(h->d_sub + h->o_len);
+  S.control = reinterpret_cast<const int32_t *>(h->d_sub + h->o_ctrl);
   S.controlstride = h->ctrlstride;
-  S.interp = h->d_interp;
+  S.interp = reinterpret_cast<const double *>(h->d_sub + h->o_interp);
   h->last = S;
   h->have_last = true;
 
   const int nbl = d.nbaselines;
   float4 *acc4 = reinterpret_cast<float4 *>(h->d_acc);
+  auto mark = [&](int stage, bool start) -> gx_status { return timed ? record(h, st, stage, start) : GX_OK; };
   // the tensor-core X-step stores its first chunk instead of adding to it
   if (!h->tc) CKR(h, cudaMemsetAsync(h->d_acc, 0, sizeof(float2) * h->acc_slice * h->ks, st));
   CKR(h, cudaMemsetAsync(h->d_wacc, 0, sizeof(float) * (d.nstations + nbl), st));
   CKR(h, cudaMemsetAsync(h->d_err, 0, sizeof(int), st));
+  gx_status r;
   for (int b0 = 0; b0 < J.blocks_per_send; b0 += h->chunk) {
     const int nb = std::min(h->chunk, J.blocks_per_send - b0);
-    gx_status r;
-    if ((r = record(h, st, 0, true)) != GX_OK) return r;
+    if ((r = mark(0, true)) != GX_OK) return r;
     CKR(h, fstep_launch(J, h->d_st, h->maxnrf, S, b0, nb, h->nslots, h->d_spec, h->d_w, h->d_bp, st));
-    if ((r = record(h, st, 0, false)) != GX_OK) return r;
-    if ((r = record(h, st, 1, true)) != GX_OK) return r;
+    if ((r = mark(0, false)) != GX_OK) return r;
+    if ((r = mark(1, true)) != GX_OK) return r;
     if (h->tc)
       CKR(h, xmac_tc_launch(h->d_spec, nb, J.nchan, d.nfreqs, h->ks, h->hilo, h->d_scale, acc4, b0 > 0 ? 1 : 0,
                             h->d_err, st));
     else
       CKR(h, xmac_fp32_launch(h->d_spec, nb, J.ninputs, J.nchan, d.nfreqs, h->ks, h->d_acc, st));
     CKR(h, weights_launch(h->d_w, nb, d.nstations, h->d_pairs, nbl, h->d_wacc, st));
-    if ((r = record(h, st, 1, false)) != GX_OK) return r;
+    if ((r = mark(1, false)) != GX_OK) return r;
     h->launches += 3;
   }
-  gx_status r;
-  if ((r = record(h, st, 2, true)) != GX_OK) return r;
+  if ((r = mark(2, true)) != GX_OK) return r;
   CKR(h, cudaMemsetAsync(dev_results, 0, sizeof(float2) * h->rl, st));
   if (h->tc) {
     CKR(h, finalise_tc_launch(h->d_tcprods, h->d_tcrows, (int)h->tcrows.size(), acc4, d.nfreqs, J.nchan, h->ks,
@@ -748,9 +788,25 @@ static gx_status run_device(gx_handle *h, const gx_subint_desc *sub, const uint8
                            (int)h->wents.size(), h->d_wacc, dev_results, st));
   }
   h->launches += (h->prods.empty() ? 0 : 1) + (h->wents.empty() ? 0 : 1);
-  if ((r = record(h, st, 2, false)) != GX_OK) return r;
+  if ((r = mark(2, false)) != GX_OK) return r;
   CKR(h, cudaMemcpyAsync(h->h_err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
   return GX_OK;
+}
+
+gx_status gx_stage_subint(gx_handle *h, const gx_subint_desc *sub, const uint8_t *const *devdata)
+{
+  return stage_subint(h, sub, devdata);
+}
+
+extern "C" {
+
+// Runs one subint whose data buffers are already device pointers.
+static gx_status run_device(gx_handle *h, const gx_subint_desc *sub, const uint8_t *const *devdata,
+                            float2 *dev_results, cudaStream_t st)
+{
+  gx_status r = stage_subint(h, sub, devdata);
+  if (r != GX_OK) return r;
+  return gx_enqueue_subint(h, dev_results, st);
 }
 
 // Status the kernels of the last subint left in *d_err (read after a synchronise).

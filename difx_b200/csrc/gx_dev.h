@@ -71,10 +71,16 @@ struct __align__(16) BlockParam {
   int state, nframes;             // state 0: zeroed block
 };
 
-// One subint: device pointers to its buffers.
-struct SubintArrays {
+// Start of the subint (read from device memory, so that a replayed CUDA
+// graph sees each call's value).
+struct SubintClock {
   int sec, ns;
   double scan_start_sec;
+};
+
+// One subint: device pointers to its buffers.
+struct SubintArrays {
+  const SubintClock *clock;
   const uint8_t *const *data;    // [nstations] device pointers
   const int64_t *datalen;        // [nstations]
   const int32_t *control;        // [nstations][controlstride]

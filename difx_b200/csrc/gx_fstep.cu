@@ -155,10 +155,11 @@ __global__ void blockparams_kernel(DevJob J, SubintArrays S, int blk0, int nblk,
     const double fftcentre = blk + 0.5;
     const double averagedelay = ip[0] * fftcentre * fftcentre + ip[1] * fftcentre + ip[2];
     const double fftstartmicrosec = (blk * F) * J.sampletime;
-    const double starttime = (S.sec - datasec) * 1000000.0 +
-                             ((long long)S.ns - (long long)datans) / 1000.0 + fftstartmicrosec - averagedelay;
+    const SubintClock clk = *S.clock;
+    const double starttime = (clk.sec - datasec) * 1000000.0 +
+                             ((long long)clk.ns - (long long)datans) / 1000.0 + fftstartmicrosec - averagedelay;
     int ns = (int)(starttime / J.sampletime + 0.5);
-    const double walltimesecs = (double)((long long)S.scan_start_sec + S.sec) + S.ns / 1.0e9 +
+    const double walltimesecs = (double)((long long)clk.scan_start_sec + clk.sec) + clk.ns / 1.0e9 +
                                 fftstartmicrosec / 1.0e6;
     P.intwalltime = (int)walltimesecs;
     P.fracwalltime = walltimesecs - P.intwalltime;

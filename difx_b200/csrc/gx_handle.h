@@ -33,6 +33,7 @@ struct gx_handle {
   std::vector<gx::TcRowEntry> tcrows;
   std::vector<gx::WeightEntry> wents;
   std::vector<int2> pairs;
+  int xstep = 0;                   // X-step form in use (GX_XSTEP_AUTO resolved at open)
   bool tc = false, hilo = false;   // tensor-core X-step (split FP16 product)
   float tc_scale0 = 1.0f;          // default power-of-two operand scale
   float *d_scale = nullptr;        // [freq][128][nchan] operand scales
@@ -50,11 +51,16 @@ struct gx_handle {
   int2 *d_pairs = nullptr;
   gx::ProdEntry *d_prods = nullptr;
   gx::WeightEntry *d_went = nullptr;
-  const uint8_t **d_dataptrs = nullptr;
-  int64_t *d_datalen = nullptr;
-  int32_t *d_ctrl = nullptr;
+  // Per-subint tables, one block written on the host (pinned) and copied to
+  // the device with one copy per subint:
+  //   SubintClock | datalen[nst] (int64) | data pointers[nst] | interp[nst][3]
+  //   (double) | control words[nst][ctrlstride] (int32)
+  unsigned char *h_sub = nullptr, *d_sub = nullptr;
+  size_t sub_bytes = 0, o_len = 0, o_ptr = 0, o_interp = 0, o_ctrl = 0;
+  cudaEvent_t ev_sub = nullptr;    // recorded after the block's copy (host may rewrite it once passed)
+  bool ev_sub_pending = false;
   int ctrlstride = 0;
-  double *d_interp = nullptr;
+  bool untimed = false;            // no events recorded (batch runs, CUDA-graph capture)
   std::vector<uint8_t *> d_data;
   std::vector<int64_t> data_cap;     // usable bytes of d_data[s]
   std::vector<long long> data_alloc; // allocated bytes of d_data[s]
@@ -100,3 +106,10 @@ struct gx_handle {
 
 // local freq index of job freq f on baseline b (-1: not correlated)
 int gx_bl_localfreq(const gx_baseline_desc &b, int f);
+
+// The two halves of one subint, shared with the batch runner: the host half
+// writes the subint's tables into the handle's pinned block; the device half
+// enqueues the tables' copy and all kernels on `st` without waiting on the
+// host (capturable into a CUDA graph when h->untimed is set).
+gx_status gx_stage_subint(gx_handle *h, const gx_subint_desc *sub, const uint8_t *const *devdata);
+gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st);

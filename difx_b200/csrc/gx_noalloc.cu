@@ -114,6 +114,7 @@ extern "C" gx_status gx_subint_device_noalloc(const gx_job_desc *desc, const gx_
   const size_t o_len = take(sizeof(int64_t) * nst);
   const size_t o_ptr = take(sizeof(uint8_t *) * nst);
   const size_t o_interp = take(sizeof(double) * 3 * nst);
+  const size_t o_clock = take(sizeof(SubintClock));
   const size_t o_pairs = take(sizeof(int2) * (nbl > 0 ? nbl : 1));
   const size_t o_prods = take(sizeof(ProdEntry) * (plan.prods.empty() ? 1 : plan.prods.size()));
   const size_t o_went = take(sizeof(WeightEntry) * (plan.wents.empty() ? 1 : plan.wents.size()));
@@ -163,6 +164,7 @@ extern "C" gx_status gx_subint_device_noalloc(const gx_job_desc *desc, const gx_
   int64_t *d_len = reinterpret_cast<int64_t *>(base + o_len);
   const uint8_t **d_ptr = reinterpret_cast<const uint8_t **>(base + o_ptr);
   double *d_interp = reinterpret_cast<double *>(base + o_interp);
+  SubintClock *d_clock = reinterpret_cast<SubintClock *>(base + o_clock);
   int2 *d_pairs = reinterpret_cast<int2 *>(base + o_pairs);
   ProdEntry *d_prods = reinterpret_cast<ProdEntry *>(base + o_prods);
   WeightEntry *d_went = reinterpret_cast<WeightEntry *>(base + o_went);
@@ -193,6 +195,8 @@ extern "C" gx_status gx_subint_device_noalloc(const gx_job_desc *desc, const gx_
   NA_CK(cudaMemcpyAsync(d_len, lens.data(), sizeof(int64_t) * nst, cudaMemcpyHostToDevice, st));
   NA_CK(cudaMemcpyAsync(d_ptr, sub->data, sizeof(uint8_t *) * nst, cudaMemcpyHostToDevice, st));
   NA_CK(cudaMemcpyAsync(d_interp, sub->interp, sizeof(double) * 3 * nst, cudaMemcpyHostToDevice, st));
+  const SubintClock clock{sub->sec, sub->ns, sub->scan_start_sec};
+  NA_CK(cudaMemcpyAsync(d_clock, &clock, sizeof(clock), cudaMemcpyHostToDevice, st));
   if (nbl > 0) NA_CK(cudaMemcpyAsync(d_pairs, plan.pairs.data(), sizeof(int2) * nbl, cudaMemcpyHostToDevice, st));
   if (!plan.prods.empty())
     NA_CK(cudaMemcpyAsync(d_prods, plan.prods.data(), sizeof(ProdEntry) * plan.prods.size(), cudaMemcpyHostToDevice, st));
@@ -206,9 +210,7 @@ extern "C" gx_status gx_subint_device_noalloc(const gx_job_desc *desc, const gx_
   NA_CK(cudaMemsetAsync(dev_results, 0, sizeof(float2) * plan.result_length, st));
 
   SubintArrays S{};
-  S.sec = sub->sec;
-  S.ns = sub->ns;
-  S.scan_start_sec = sub->scan_start_sec;
+  S.clock = d_clock;
   S.data = d_ptr;
   S.datalen = d_len;
   S.control = d_ctrl;

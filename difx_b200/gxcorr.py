@@ -40,8 +40,9 @@ def lib():
         L.gx_last_error.restype = C.c_char_p
         L.gx_status_string.restype = C.c_char_p
         L.gx_server_last_error.restype = C.c_char_p
+        L.gx_batch_last_error.restype = C.c_char_p
         for name in EXPORTED_SYMBOLS:
-            if name not in ("gx_last_error", "gx_status_string", "gx_server_last_error"):
+            if name not in ("gx_last_error", "gx_status_string", "gx_server_last_error", "gx_batch_last_error"):
                 getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -53,7 +54,8 @@ EXPORTED_SYMBOLS = ("gx_open", "gx_open_input", "gx_close", "gx_last_error", "gx
                     "gx_subint_device_noalloc", "gx_set_tc_scales", "gx_vis_open", "gx_vis_add", "gx_vis_write",
                     "gx_vis_close", "gx_uvw", "gx_server_open", "gx_server_set_executor", "gx_server_attach",
                     "gx_server_submit", "gx_server_wait", "gx_server_stats", "gx_server_close", "gx_device_bytes",
-                    "gx_server_last_error")
+                    "gx_server_last_error", "gx_batch_open", "gx_batch_run", "gx_batch_synchronize",
+                    "gx_batch_info", "gx_batch_last_error", "gx_batch_close")
 
 
 def subint_device_noalloc(jd: capi.JobDesc, sd: capi.SubintDesc, dev_results_ptr: int, stream_ptr: int = 0) -> None:
@@ -281,6 +283,62 @@ class Server:
             lib().gx_server_close(self.s)
             self.s = None
             self._keep = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+BATCH_MODES = {"serial": 0, "streams": 1, "graph": 2}
+
+
+class Batch:
+    """One subint of each of several resident jobs per step (gx_batch_*):
+    per-job launches on one stream ("serial"), jobs spread over branch
+    streams ("streams") or that schedule replayed as one CUDA graph
+    ("graph"); nstreams 0 tunes the branch count on the first steps."""
+
+    def __init__(self, corrs: Sequence[Correlator], dev_results_ptrs: Sequence[int], mode: str = "graph",
+                 nstreams: int = 0):
+        n = len(corrs)
+        hs = (C.c_void_p * n)(*[c.h for c in corrs])
+        rs = (C.c_void_p * n)(*[int(p) for p in dev_results_ptrs])
+        self.b = C.c_void_p()
+        self.n = n
+        self._corrs = list(corrs)
+        st = lib().gx_batch_open(hs, rs, n, BATCH_MODES[mode], int(nstreams), C.byref(self.b))
+        if st != 0:
+            raise GxError(st, "gx_batch_open failed")
+        self._subs = None
+
+    def _check(self, st: int):
+        if st != 0:
+            raise GxError(st, lib().gx_batch_last_error(self.b).decode() if self.b else "")
+
+    def run(self, subs: Sequence[capi.SubintDesc]) -> None:
+        """Starts one step: subs[j] is job j's subint (device data pointers)."""
+        arr = (C.c_void_p * self.n)(*[C.addressof(sd.desc) for sd in subs])
+        self._subs = (list(subs), arr)   # alive until the step has been staged and run
+        self._check(lib().gx_batch_run(self.b, arr))
+
+    def synchronize(self) -> float:
+        """Waits for the step; returns its device time in ms."""
+        ms = C.c_float(0)
+        self._check(lib().gx_batch_synchronize(self.b, C.byref(ms)))
+        return ms.value
+
+    def info(self):
+        """(branch streams in use (0 while tuning), tuning, kernel launches of the last step)."""
+        k, t, l = C.c_int(0), C.c_int(0), C.c_int(0)
+        self._check(lib().gx_batch_info(self.b, C.byref(k), C.byref(t), C.byref(l)))
+        return k.value, bool(t.value), l.value
+
+    def close(self) -> None:
+        if self.b:
+            lib().gx_batch_close(self.b)
+            self.b = None
 
     def __del__(self):
         try:

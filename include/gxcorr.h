@@ -66,7 +66,11 @@ typedef enum gx_status {
 typedef enum gx_xstep {
   GX_XSTEP_FP32 = 0,       /* plain FP32 Hermitian cross-multiply-accumulate */
   GX_XSTEP_TC_FP16 = 1,    /* tcgen05 tensor cores, FP16 spectra, FP32 accumulation */
-  GX_XSTEP_TC_FP16_HILO = 2 /* as above with a split hi+lo FP16 product (3 MMAs) */
+  GX_XSTEP_TC_FP16_HILO = 2, /* as above with a split hi+lo FP16 product (3 MMAs) */
+  GX_XSTEP_AUTO = 3          /* TC_FP16_HILO when a freq has at least 48 inputs (station
+                                bands; env GX_XSTEP_AUTO_MIN_INPUTS) and at most 128, else FP32:
+                                the tensor-core tile costs the same for any input count up to
+                                128, the FP32 X-step grows with its square */
 } gx_xstep;
 
 /* One frequency-table entry (FREQ TABLE, configuration.cpp:1970-2022). */
@@ -147,6 +151,7 @@ typedef struct gx_layout_info {
   int array_stride;
   int fftchannels;
   int nchan;
+  int xstep;               /* X-step form in use (GX_XSTEP_AUTO resolved) */
 } gx_layout_info;
 
 /* device < 0 opens a host-only handle: layout, offsets and delay-model
@@ -277,6 +282,41 @@ gx_status gx_server_stats(gx_server *s, int reset, gx_latency_stats *out);
 gx_status gx_server_close(gx_server *s);
 /* Message of the last request that failed (its job and the handle's error). */
 const char *gx_server_last_error(gx_server *s);
+
+/* ---- Batches of uneven jobs (one subint of every job per step) ---------- */
+
+/* A batch is a fixed set of opened handles on one device, each with a device
+   result array.  Every gx_batch_run correlates one subint of each job, with
+   device-resident inputs (sub->data are device pointers, as for
+   gx_subint_device), and returns without waiting; gx_batch_synchronize waits.
+   Each job's results are bit-identical to what gx_subint_device gives it
+   alone.  Modes:
+     GX_BATCH_SERIAL   one job after another on one stream (per-job launches)
+     GX_BATCH_STREAMS  jobs spread over branch streams, longest first onto the
+                       least-loaded branch
+     GX_BATCH_GRAPH    that schedule captured once into one CUDA graph and
+                       replayed each step (one host launch per step)
+   nstreams 0 (STREAMS, GRAPH): the branch count is tuned on the first steps
+   (1, 2, 4, 8, 16 branches, two steps each; every step still delivers its
+   results).  A handle may be in one batch at a time and must not be used
+   elsewhere while a step is in flight.  No counterpart in the reference,
+   which runs one job per correlator process. */
+typedef struct gx_batch gx_batch;
+#define GX_BATCH_SERIAL 0
+#define GX_BATCH_STREAMS 1
+#define GX_BATCH_GRAPH 2
+
+gx_status gx_batch_open(gx_handle *const *jobs, float *const *dev_results, int njobs, int mode, int nstreams,
+                        gx_batch **out);
+/* subs[j]: the subint of job j (all njobs entries). */
+gx_status gx_batch_run(gx_batch *b, const gx_subint_desc *const *subs);
+/* Waits for the step in flight; device_ms (may be NULL) = its device time. */
+gx_status gx_batch_synchronize(gx_batch *b, float *device_ms);
+/* Branch count in use (0 while tuning), whether tuning is still on, and the
+   kernel launches of the last step. */
+gx_status gx_batch_info(const gx_batch *b, int *nstreams, int *tuning, int *launches);
+const char *gx_batch_last_error(const gx_batch *b);
+gx_status gx_batch_close(gx_batch *b);
 
 /* Device memory a handle holds, bytes. */
 gx_status gx_device_bytes(const gx_handle *h, long long *bytes);
