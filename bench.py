@@ -395,10 +395,9 @@ def run_c4(args):
     torch.cuda.synchronize()
     corrs, res = [], []
     for spec, *_ in staged:
-        # spectra buffer of about 256 MB per job (the tensor-core form pads a freq to 128 inputs)
-        row = len(spec.subbands) * 128 * spec.nchan * 8
-        chunk = int(max(16, min(spec.blocks_per_send, (256 << 20) // row)))
-        c = Correlator.from_desc(capi.job_desc_from_spec(spec, xstep=capi.GX_XSTEP_AUTO, block_chunk=chunk))
+        # spectra buffers sized for efficient passes, at most 2 GB per job
+        c = Correlator.from_desc(capi.job_desc_from_spec(spec, xstep=capi.GX_XSTEP_AUTO,
+                                                         spectra_budget_bytes=2 << 30))
         corrs.append(c)
         res.append(torch.empty(2 * c.result_length, dtype=torch.float32, device="cuda"))
     subs = [sd for _, sd, _, _ in staged]

@@ -61,7 +61,8 @@ class gx_job_desc(C.Structure):
                 ("subint_ns", C.c_int), ("guard_ns", C.c_int),
                 ("fringe_rotation_order", C.c_int), ("array_stride", C.c_int),
                 ("xmac_stride", C.c_int), ("write_autocorrs", C.c_int),
-                ("max_data_bytes", C.c_int64), ("xstep", C.c_int), ("block_chunk", C.c_int)]
+                ("max_data_bytes", C.c_int64), ("xstep", C.c_int), ("block_chunk", C.c_int),
+                ("spectra_budget_bytes", C.c_int64)]
 
 
 class gx_subint_desc(C.Structure):
@@ -77,7 +78,8 @@ class gx_subint_desc(C.Structure):
 class gx_layout_info(C.Structure):
     _fields_ = [("result_length", C.c_int64), ("nfreqs", C.c_int), ("nbaselines", C.c_int),
                 ("nstations", C.c_int), ("blocks_per_send", C.c_int), ("xmac_stride", C.c_int),
-                ("array_stride", C.c_int), ("fftchannels", C.c_int), ("nchan", C.c_int), ("xstep", C.c_int)]
+                ("array_stride", C.c_int), ("fftchannels", C.c_int), ("nchan", C.c_int), ("xstep", C.c_int),
+                ("block_chunk", C.c_int)]
 
 
 class JobDesc:
@@ -103,7 +105,7 @@ class JobDesc:
 
 
 def job_desc_from_spec(spec: JobSpec, xstep: int = GX_XSTEP_FP32, max_data_bytes: int = 0,
-                       block_chunk: int = 0) -> JobDesc:
+                       block_chunk: int = 0, spectra_budget_bytes: int = 0) -> JobDesc:
     """gx_job_desc for a JobSpec (all stations share the same recorded bands)."""
     spec.validate()
     freqs = []
@@ -162,7 +164,8 @@ def job_desc_from_spec(spec: JobSpec, xstep: int = GX_XSTEP_FP32, max_data_bytes
                    subint_ns=spec.subint_ns, guard_ns=spec.guard_ns,
                    fringe_rotation_order=spec.fringe_rot_order, array_stride=spec.array_stride,
                    xmac_stride=spec.xmac_stride, write_autocorrs=1 if spec.write_autocorrs else 0,
-                   max_data_bytes=max_data_bytes, xstep=xstep, block_chunk=block_chunk)
+                   max_data_bytes=max_data_bytes, xstep=xstep, block_chunk=block_chunk,
+                   spectra_budget_bytes=spectra_budget_bytes)
 
 
 class SubintDesc:

@@ -211,7 +211,7 @@ static gx_status setup(gx_handle *h)
     if (ni > kTcInputs)
       return h->fail(GX_ERR_UNSUPPORTED, "the tensor-core X-step takes at most 128 inputs (station bands) per freq");
     if (J.nchan < 2) return h->fail(GX_ERR_UNSUPPORTED, "the tensor-core X-step needs at least 2 channels");
-    J.ninputs = kTcInputs;   // rows beyond the job's inputs stay zero
+    J.ninputs = ni;   // the X-step reads the rows up to 128 beyond these as zeros
   } else {
     h->xs = xmac_shape(ni);
     J.ninputs = h->xs.nsuper * h->xs.ST;
@@ -388,18 +388,36 @@ static gx_status setup(gx_handle *h)
 
   // chunking and K-split
   const size_t per_block = (size_t)d.nfreqs * J.ninputs * J.nchan * sizeof(float2);
-  // The tensor-core X-step moves its accumulators (128 x 128 complex per
-  // channel) through HBM once per chunk, so it gets long chunks: up to 40 GB of
-  // spectra, at most 30% of the device memory free at open.
-  size_t spec_budget = size_t(2) << 30;
+  // Every pass reads and writes the accumulators once; the spectra of a block
+  // are written and read once.  Passes of at least `efficient` blocks keep the
+  // accumulator traffic under a quarter of the spectra traffic.
+  size_t acc_pass;
   if (h->tc) {
-    spec_budget = size_t(40) << 30;
-    size_t fr = 0, tot = 0;
-    if (h->device >= 0 && cudaSetDevice(h->device) == cudaSuccess && cudaMemGetInfo(&fr, &tot) == cudaSuccess)
-      spec_budget = std::max(size_t(1) << 30, std::min(spec_budget, fr / 10 * 3));
+    const size_t cols = (size_t)(ni + 7) / 8 * 8;   // written in 8-column slices
+    acc_pass = 2 * (size_t)d.nfreqs * (J.nchan / 2) * ni * cols * sizeof(float4);
+  } else {
+    acc_pass = 2 * (size_t)d.nfreqs * xs.npairs * xs.ST * xs.ST * J.nchan * sizeof(float2);
   }
-  int chunk = d.block_chunk > 0 ? d.block_chunk
-                                : (int)std::min<size_t>(4096, std::max<size_t>(64, spec_budget / per_block));
+  const size_t efficient = std::max<size_t>(64, (4 * acc_pass + 2 * per_block - 1) / (2 * per_block));
+  int chunk;
+  if (d.block_chunk > 0) {
+    chunk = d.block_chunk;
+  } else if (d.spectra_budget_bytes > 0) {
+    // memory is shared with other jobs: the efficient length, within the budget
+    chunk = (int)std::min<size_t>({8192, efficient, std::max<size_t>(16, (size_t)d.spectra_budget_bytes / per_block)});
+  } else {
+    // The tensor-core X-step moves its accumulators (128 x 128 complex per
+    // channel) through HBM once per chunk, so it gets long chunks: up to 40 GB
+    // of spectra, at most 30% of the device memory free at open.
+    size_t spec_budget = size_t(2) << 30;
+    if (h->tc) {
+      spec_budget = size_t(40) << 30;
+      size_t fr = 0, tot = 0;
+      if (h->device >= 0 && cudaSetDevice(h->device) == cudaSuccess && cudaMemGetInfo(&fr, &tot) == cudaSuccess)
+        spec_budget = std::max(size_t(1) << 30, std::min(spec_budget, fr / 10 * 3));
+    }
+    chunk = (int)std::min<size_t>(4096, std::max<size_t>(64, spec_budget / per_block));
+  }
   if (chunk > J.blocks_per_send) chunk = J.blocks_per_send;
   chunk = std::max(1, chunk);
   if (d.block_chunk <= 0) {
@@ -661,6 +679,7 @@ gx_status gx_get_layout(const gx_handle *h, gx_layout_info *info)
   info->fftchannels = h->J.fftlen;
   info->nchan = h->J.nchan;
   info->xstep = h->xstep;
+  info->block_chunk = h->chunk;
   return GX_OK;
 }
 
@@ -768,8 +787,8 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
     if ((r = mark(0, false)) != GX_OK) return r;
     if ((r = mark(1, true)) != GX_OK) return r;
     if (h->tc)
-      CKR(h, xmac_tc_launch(h->d_spec, nb, J.nchan, d.nfreqs, h->ks, h->hilo, h->d_scale, acc4, b0 > 0 ? 1 : 0,
-                            h->d_err, st));
+      CKR(h, xmac_tc_launch(h->d_spec, nb, J.nchan, d.nfreqs, J.ninputs, h->ks, h->hilo, h->d_scale, acc4,
+                            b0 > 0 ? 1 : 0, h->d_err, st));
     else
       CKR(h, xmac_fp32_launch(h->d_spec, nb, J.ninputs, J.nchan, d.nfreqs, h->ks, h->d_acc, st));
     CKR(h, weights_launch(h->d_w, nb, d.nstations, h->d_pairs, nbl, h->d_wacc, st));
@@ -779,8 +798,8 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
   if ((r = mark(2, true)) != GX_OK) return r;
   CKR(h, cudaMemsetAsync(dev_results, 0, sizeof(float2) * h->rl, st));
   if (h->tc) {
-    CKR(h, finalise_tc_launch(h->d_tcprods, h->d_tcrows, (int)h->tcrows.size(), acc4, d.nfreqs, J.nchan, h->ks,
-                              dev_results, st));
+    CKR(h, finalise_tc_launch(h->d_tcprods, h->d_tcrows, (int)h->tcrows.size(), acc4, d.nfreqs, J.nchan,
+                              J.ninputs, h->ks, dev_results, st));
     CKR(h, finalise_launch(nullptr, 0, h->d_acc, h->ks, h->acc_slice, J.nchan, h->d_went, (int)h->wents.size(),
                            h->d_wacc, dev_results, st));
   } else {

@@ -222,7 +222,7 @@ __device__ __forceinline__ void split2(float a, float b, uint32_t &hi, uint32_t 
 
 template <bool HILO>
 __global__ void __launch_bounds__(kThreads, 1)
-xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, int nfreqs, int ks,
+xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, int nfreqs, int ks, int ninputs,
                const float *__restrict__ scale, float4 *__restrict__ acc, int accumulate, int *__restrict__ err)
 {
   constexpr uint32_t kParts = HILO ? 2 : 1;
@@ -390,8 +390,10 @@ xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, i
     }
     __syncthreads();
     const float ia0 = 1.0f / s0, ia1 = 1.0f / s1;
+    // only the job's inputs: rows and 8-column slices beyond them are never read
+    const int ncb = (ninputs + kVCols - 1) / kVCols;
 #pragma unroll 1
-    for (int cb = 0; cb < kNI / kVCols; cb++) {
+    for (int cb = 0; cb < ncb; cb++) {
       // thread (a, h) forms columns b = 8 cb + 4 h + i of row a
       const int b0 = cb * kVCols + h * 4;
       float r0[4] = {0.f, 0.f, 0.f, 0.f}, r1[4] = {0.f, 0.f, 0.f, 0.f};
@@ -418,6 +420,7 @@ xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, i
       for (int m = 0; m < kNI * kVCols / kThreads; m++) {
         const int i = tid + kThreads * m;
         const int row = i / kVCols, col = i % kVCols;
+        if (row >= ninputs) continue;
         float4 w = sV[row * kVRow + col];
         float4 *dst = oblk + (size_t)row * kNI + cb * kVCols + col;
         if (accumulate) {
@@ -449,12 +452,13 @@ constexpr int kFinPairs = 16;
 
 __global__ void __launch_bounds__(256)
 finalise_tc_kernel(const TcProdEntry *__restrict__ prods, const TcRowEntry *__restrict__ rows,
-                   const float4 *__restrict__ acc, int nfreqs, int NP, int ks, float2 *__restrict__ results)
+                   const float4 *__restrict__ acc, int nfreqs, int NP, int ks, int ninputs,
+                   float2 *__restrict__ results)
 {
   __shared__ float4 sV[kFinPairs][kNI];
   const TcRowEntry R = rows[blockIdx.x];
   const size_t slice = (size_t)nfreqs * NP * kNI * kNI;
-  const int nb = kNI - R.bmin;
+  const int nb = ninputs - R.bmin;
   const int ne = R.end - R.start;
   // channel pairs [pb, pe) of this CTA (blockIdx.y of gridDim.y slices)
   const int per = ((NP + gridDim.y - 1) / gridDim.y + kFinPairs - 1) / kFinPairs * kFinPairs;
@@ -494,12 +498,15 @@ size_t xmac_tc_smem_bytes(bool hilo)
   return (size_t)kStages * kStageBytes + ops + (kStages + kOpStages) * 8 + 16;
 }
 
-cudaError_t xmac_tc_launch(const float2 *spec, int nblk, int N, int nfreqs, int ks, bool hilo, const float *scale,
-                           float4 *acc, int accumulate, int *err, cudaStream_t st)
+cudaError_t xmac_tc_launch(const float2 *spec, int nblk, int N, int nfreqs, int ninputs, int ks, bool hilo,
+                           const float *scale, float4 *acc, int accumulate, int *err, cudaStream_t st)
 {
   if (nblk <= 0) return cudaSuccess;
+  if (ninputs < 1 || ninputs > kNI) return cudaErrorInvalidValue;
   // spec[freq][block][row][channel] float2 as a 4-D FP32 tensor (innermost first):
-  // {2N floats, 128 rows, nblk blocks, nfreqs}; box {4 floats, 128 rows, kKT blocks, 1}
+  // {2N floats, ninputs rows, nblk blocks, nfreqs}; box {4 floats, 128 rows, kKT
+  // blocks, 1}: the rows beyond the job's inputs (and blocks beyond nblk) are
+  // out of bounds, so the copy fills them with zeros without reading memory
   static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
   if (!encode) {
     void *fn = nullptr;
@@ -510,9 +517,9 @@ cudaError_t xmac_tc_launch(const float2 *spec, int nblk, int N, int nfreqs, int 
     encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
   }
   CUtensorMap map;
-  const cuuint64_t dims[4] = {(cuuint64_t)(2 * N), (cuuint64_t)kNI, (cuuint64_t)nblk, (cuuint64_t)nfreqs};
-  const cuuint64_t strides[3] = {(cuuint64_t)(2 * N) * 4, (cuuint64_t)(2 * N) * 4 * kNI,
-                                 (cuuint64_t)(2 * N) * 4 * kNI * nblk};
+  const cuuint64_t dims[4] = {(cuuint64_t)(2 * N), (cuuint64_t)ninputs, (cuuint64_t)nblk, (cuuint64_t)nfreqs};
+  const cuuint64_t strides[3] = {(cuuint64_t)(2 * N) * 4, (cuuint64_t)(2 * N) * 4 * ninputs,
+                                 (cuuint64_t)(2 * N) * 4 * ninputs * nblk};
   const cuuint32_t box[4] = {4, (cuuint32_t)kNI, (cuuint32_t)kKT, 1};
   const cuuint32_t estr[4] = {1, 1, 1, 1};
   CUresult cr = encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float2 *>(spec), dims, strides, box, estr,
@@ -525,7 +532,8 @@ cudaError_t xmac_tc_launch(const float2 *spec, int nblk, int N, int nfreqs, int 
   if (hilo == H) {                                                                                          \
     cudaError_t e = smem_opt_in((const void *)xmac_tc_kernel<H>, sm);                                       \
     if (e != cudaSuccess) return e;                                                                         \
-    xmac_tc_kernel<H><<<grid, kThreads, sm, st>>>(map, nblk, N / 2, nfreqs, ks, scale, acc, accumulate, err); \
+    xmac_tc_kernel<H><<<grid, kThreads, sm, st>>>(map, nblk, N / 2, nfreqs, ks, ninputs, scale, acc, accumulate, \
+                                                  err);                                                     \
     return cudaGetLastError();                                                                              \
   }
   GX_TC_CASE(true) GX_TC_CASE(false)
@@ -534,14 +542,14 @@ cudaError_t xmac_tc_launch(const float2 *spec, int nblk, int N, int nfreqs, int 
 }
 
 cudaError_t finalise_tc_launch(const TcProdEntry *prods, const TcRowEntry *rows, int nrows, const float4 *acc,
-                               int nfreqs, int N, int ks, float2 *results, cudaStream_t st)
+                               int nfreqs, int N, int ninputs, int ks, float2 *results, cudaStream_t st)
 {
   if (nrows <= 0) return cudaSuccess;
   // enough CTAs for several waves: slices of the channel pairs per row
   const int NP = N / 2;
   int slices = 1;
   while ((long long)nrows * slices < 8 * 148 && (slices * 2) * kFinPairs <= NP) slices *= 2;
-  finalise_tc_kernel<<<dim3(nrows, slices), 256, 0, st>>>(prods, rows, acc, nfreqs, NP, ks, results);
+  finalise_tc_kernel<<<dim3(nrows, slices), 256, 0, st>>>(prods, rows, acc, nfreqs, NP, ks, ninputs, results);
   return cudaGetLastError();
 }
 

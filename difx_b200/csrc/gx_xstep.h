@@ -49,14 +49,15 @@ struct TcRowEntry {
   int freq, a, bmin, start, end;
 };
 
-// Tensor-core X-step over 128-row spectra [freq][block][128 inputs][N]; acc
-// holds, per K-split slice, [freq][N/2][a][b] float4 = (Re, Im) of both
-// channels of a channel pair, unscaled.
+// Tensor-core X-step over spectra [freq][block][ninputs][N] (ninputs <= 128,
+// the MMA tile's M; missing rows are zeros); acc holds, per K-split slice,
+// [freq][N/2][128][128] float4 = (Re, Im) of both channels of a channel pair,
+// unscaled, of which rows and columns below ninputs are written.
 size_t xmac_tc_smem_bytes(bool hilo);
-cudaError_t xmac_tc_launch(const float2 *spec, int nblk, int N, int nfreqs, int ks, bool hilo, const float *scale,
-                           float4 *acc, int accumulate, int *err, cudaStream_t st);
+cudaError_t xmac_tc_launch(const float2 *spec, int nblk, int N, int nfreqs, int ninputs, int ks, bool hilo,
+                           const float *scale, float4 *acc, int accumulate, int *err, cudaStream_t st);
 cudaError_t finalise_tc_launch(const TcProdEntry *prods, const TcRowEntry *rows, int nrows, const float4 *acc,
-                               int nfreqs, int N, int ks, float2 *results, cudaStream_t st);
+                               int nfreqs, int N, int ninputs, int ks, float2 *results, cudaStream_t st);
 constexpr int kTcInputs = 128;   // inputs per frequency of the tensor-core X-step (the MMA M)
 
 cudaError_t finalise_launch(const ProdEntry *prods, int nprods, const float2 *acc, int ks, size_t ks_stride, int N,

@@ -125,6 +125,10 @@ typedef struct gx_job_desc {
   int64_t max_data_bytes;  /* largest per-station data buffer one subint will pass */
   int xstep;               /* gx_xstep */
   int block_chunk;         /* FFT blocks per device pass, 0 = automatic */
+  int64_t spectra_budget_bytes; /* with block_chunk 0: > 0 caps the spectra buffer and makes passes only as
+                                   long as keeps accumulator traffic under a quarter of the spectra
+                                   traffic (for many resident jobs); 0 = as long as 2 GB (FP32) or up to
+                                   40 GB (tensor cores) allow */
 } gx_job_desc;
 
 /* One subint: the contents of one Core processslot (core.h:76-98). */
@@ -152,6 +156,7 @@ typedef struct gx_layout_info {
   int fftchannels;
   int nchan;
   int xstep;               /* X-step form in use (GX_XSTEP_AUTO resolved) */
+  int block_chunk;         /* FFT blocks per device pass in use */
 } gx_layout_info;
 
 /* device < 0 opens a host-only handle: layout, offsets and delay-model

@@ -111,3 +111,22 @@ def test_missing_input_file_is_an_io_error():
     with pytest.raises(gxcorr.GxError) as ei:
         gxcorr.Correlator.from_input("/nonexistent/job.input", device=-1)
     assert ei.value.status == 5
+
+
+def test_spectra_budget_sets_pass_length():
+    """With a spectra budget the pass (block chunk) is the efficient length
+    within the budget; an explicit block_chunk wins; the default fills 2 GB."""
+    spec = jobs.spec_c2small()
+    per_block = len(spec.subbands) * spec.nchan * 8
+    lens = {}
+    for budget in (0, 1 << 20, 64 << 20, 1 << 34):
+        c = gxcorr.Correlator.from_desc(capi.job_desc_from_spec(spec, spectra_budget_bytes=budget), device=-1)
+        lens[budget] = c.info.block_chunk
+        c.close()
+    assert lens[0] == spec.blocks_per_send                      # 2 GB holds the whole subint
+    assert 16 <= lens[1 << 20] <= max(16, (1 << 20) // (per_block * spec.nstations * len(spec.pols)))
+    assert lens[1 << 20] <= lens[64 << 20] <= lens[1 << 34] <= spec.blocks_per_send
+    c = gxcorr.Correlator.from_desc(capi.job_desc_from_spec(spec, block_chunk=50, spectra_budget_bytes=1 << 20),
+                                    device=-1)
+    assert c.info.block_chunk == 50
+    c.close()
