@@ -308,6 +308,32 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
   return GX_OK;
 }
 
+gx_status gx_vis_buffer(gx_vis *v, float **dev, long long *nfloats, int *nsub)
+{
+  if (!v || !dev || !nfloats) return GX_ERR_ARG;
+  *dev = reinterpret_cast<float *>(v->d_int);
+  *nfloats = 2 * (long long)v->h->rl;
+  if (nsub) *nsub = v->nsub;
+  return GX_OK;
+}
+
+gx_status gx_vis_set_subints(gx_vis *v, int nsub)
+{
+  if (!v || nsub < 0) return GX_ERR_ARG;
+  v->nsub = nsub;
+  return GX_OK;
+}
+
+gx_status gx_vis_clear(gx_vis *v)
+{
+  if (!v) return GX_ERR_ARG;
+  gx_handle *h = v->h;
+  CKR(h, cudaSetDevice(h->device));
+  CKR(h, cudaMemsetAsync(v->d_int, 0, sizeof(float2) * h->rl, v->st));
+  v->nsub = 0;
+  return GX_OK;
+}
+
 gx_status gx_vis_close(gx_vis *v)
 {
   if (!v) return GX_ERR_ARG;

@@ -55,7 +55,8 @@ EXPORTED_SYMBOLS = ("gx_open", "gx_open_input", "gx_close", "gx_last_error", "gx
                     "gx_vis_close", "gx_uvw", "gx_server_open", "gx_server_set_executor", "gx_server_attach",
                     "gx_server_submit", "gx_server_wait", "gx_server_stats", "gx_server_close", "gx_device_bytes",
                     "gx_server_last_error", "gx_batch_open", "gx_batch_run", "gx_batch_synchronize",
-                    "gx_batch_info", "gx_batch_last_error", "gx_batch_close")
+                    "gx_batch_info", "gx_batch_last_error", "gx_batch_close", "gx_vis_buffer",
+                    "gx_vis_set_subints", "gx_vis_clear")
 
 
 def subint_device_noalloc(jd: capi.JobDesc, sd: capi.SubintDesc, dev_results_ptr: int, stream_ptr: int = 0) -> None:
@@ -210,6 +211,18 @@ class Visibility:
         n = C.c_int(0)
         self.corr._check(lib().gx_vis_write(self.v, scan, sec, ns, C.byref(n)))
         return n.value
+
+    def buffer(self):
+        """(device pointer, float count, subints added) of the integration buffer (gx_vis_buffer)."""
+        p, n, k = C.c_void_p(), C.c_longlong(0), C.c_int(0)
+        self.corr._check(lib().gx_vis_buffer(self.v, C.byref(p), C.byref(n), C.byref(k)))
+        return p.value, n.value, k.value
+
+    def set_subints(self, nsub: int) -> None:
+        self.corr._check(lib().gx_vis_set_subints(self.v, int(nsub)))
+
+    def clear(self) -> None:
+        self.corr._check(lib().gx_vis_clear(self.v))
 
     def close(self) -> None:
         if self.v:

@@ -237,6 +237,17 @@ gx_status gx_vis_add(gx_vis *v, const float *dev_results, void *stream);
 gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords);
 gx_status gx_vis_close(gx_vis *v);
 
+/* Partial integrations on several GPUs (subints shared out over ranks, as the
+   FxManager shares them over Cores, fxmanager.cpp:331-336): the device
+   integration buffer (2 x result_length floats, on the handle's device) and
+   the subints added to it, so that the partial buffers can be summed into the
+   writing rank's buffer by a collective (the caller synchronises the
+   handle's stream first); gx_vis_set_subints then records how many subints
+   the sum holds, and gx_vis_clear empties a buffer without writing it. */
+gx_status gx_vis_buffer(gx_vis *v, float **dev, long long *nfloats, int *nsub);
+gx_status gx_vis_set_subints(gx_vis *v, int nsub);
+gx_status gx_vis_clear(gx_vis *v);
+
 /* Model::interpolateUVW (model.cpp:177-217): (u, v, w) in metres of the
    baseline datastream ds1 - datastream ds2, offset seconds after the start
    of scan, first phase centre. */

@@ -97,3 +97,50 @@ def test_gx_vis_end_to_end_matches_reference(tmp_path):
         assert abs(float(ha["weight"]) - float(hb["weight"])) <= 1e-6 * float(hb["weight"])
         worst = max(worst, float(np.mean(np.abs(da - db)) / np.mean(np.abs(db))))
     assert worst < 1e-5, worst
+
+
+def test_integration_over_ranks_single_gpu(tmp_path):
+    """difx_b200.dist.correlate_integration with one rank writes the same file
+    as the sequential use of gx_vis, and the integration buffer seen through
+    torch (gx_vis_buffer) holds the sum of the subints' result arrays."""
+    import torch
+    from difx_b200 import dist as gxdist
+    from difx_b200.gxcorr import Correlator, Visibility
+    spec = CASES["c1"]()
+    nsub = int(round(spec.int_time * 1e9 / spec.subint_ns))
+    starts = [100_000_000 + k * spec.subint_ns for k in range(nsub)]
+    prep = jobs.prepare(spec, starts, invalid_frac=0.03)
+    seq = str(tmp_path / "seq")
+    os.makedirs(seq)
+    _, host = _run_gpu(prep, seq)
+    c = Correlator.from_input(prep.paths["input"], device=0)
+    v = Visibility(c, str(tmp_path))
+    keep, subs = [], []
+    for si, ip in zip(prep.subs, prep.interps):
+        data = [torch.from_numpy(x).cuda() for x in si.data]
+        keep.append(data)
+        subs.append(capi.SubintDesc(si.scan, si.sec, si.ns, 0.0, [t.data_ptr() for t in data],
+                                    [len(x) for x in si.data], [x.ctypes.data for x in si.control],
+                                    len(si.control[0]), ip))
+    res = torch.zeros(2 * c.result_length, dtype=torch.float32, device="cuda")
+    # the buffer view: add two subints, compare with their sum
+    for i in range(2):
+        c.subint_device(subs[i], res.data_ptr())
+        v.add(res.data_ptr())
+    c.synchronize()
+    buf = gxdist.integration_tensor(v)
+    want = host[0].view(np.float32).astype(np.float64) + host[1].view(np.float32)
+    np.testing.assert_allclose(buf.cpu().numpy(), want, rtol=1e-6, atol=1e-6)
+    assert v.buffer()[2] == 2
+    v.clear()
+    assert v.buffer()[2] == 0 and float(buf.abs().max()) == 0.0
+    outdir = str(tmp_path / "ranks")
+    os.makedirs(outdir)
+    v.close()
+    v = Visibility(c, outdir)
+    s0 = prep.subs[0]
+    n = gxdist.correlate_integration(c, v, subs, res, s0.scan, s0.sec, s0.ns)
+    assert n > 0
+    assert np.array_equal(np.fromfile(_file(outdir), np.uint8), np.fromfile(_file(seq), np.uint8))
+    v.close()
+    c.close()
