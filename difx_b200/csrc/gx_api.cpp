@@ -54,12 +54,18 @@ static void free_all(gx_handle *h)
     if (p) cudaFree(p);
   if (h->h_err) cudaFreeHost(h->h_err);
   h->h_err = nullptr;
-  if (h->h_sub) cudaFreeHost(h->h_sub);
-  h->h_sub = nullptr;
-  if (h->ev_sub) cudaEventDestroy(h->ev_sub);
-  h->ev_sub = nullptr;
-  for (auto p : h->d_data)
-    if (p) cudaFree(p);
+  for (int k = 0; k < gx_handle::kSlots; k++) {
+    if (h->h_sub[k]) cudaFreeHost(h->h_sub[k]);
+    h->h_sub[k] = nullptr;
+    if (h->ev_sub[k]) cudaEventDestroy(h->ev_sub[k]);
+    if (h->ev_copied[k]) cudaEventDestroy(h->ev_copied[k]);
+    if (h->ev_done[k]) cudaEventDestroy(h->ev_done[k]);
+    h->ev_sub[k] = h->ev_copied[k] = h->ev_done[k] = nullptr;
+    for (auto p : h->d_data[k])
+      if (p) cudaFree(p);
+  }
+  if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
+  h->copy_stream = nullptr;
   for (auto e : h->evs) cudaEventDestroy(e);
   h->evs.clear();
   if (h->stream && h->own_stream) cudaStreamDestroy(h->stream);
@@ -531,8 +537,8 @@ static gx_status setup(gx_handle *h)
   CKR(h, h->dalloc(&h->d_acc, sizeof(float2) * h->acc_slice * h->ks));
   CKR(h, h->dalloc(&h->d_err, sizeof(int)));
   CKR(h, cudaMemset(h->d_err, 0, sizeof(int)));
-  CKR(h, cudaMallocHost(&h->h_err, sizeof(int)));
-  *h->h_err = 0;
+  CKR(h, cudaMallocHost(&h->h_err, sizeof(int) * gx_handle::kSlots));
+  for (int k = 0; k < gx_handle::kSlots; k++) h->h_err[k] = 0;
   CKR(h, h->dalloc(&h->d_wacc, sizeof(float) * (d.nstations + nbl)));
   if (nbl) {
     CKR(h, h->dalloc(&h->d_pairs, sizeof(int2) * nbl));
@@ -552,17 +558,21 @@ static gx_status setup(gx_handle *h)
   h->o_ctrl = h->o_interp + sizeof(double) * 3 * d.nstations;
   h->sub_bytes = h->o_ctrl + sizeof(int32_t) * h->ctrlstride * d.nstations;
   CKR(h, h->dalloc(&h->d_sub, h->sub_bytes));
-  CKR(h, cudaMallocHost(&h->h_sub, h->sub_bytes));
-  memset(h->h_sub, 0, h->sub_bytes);
-  CKR(h, cudaEventCreateWithFlags(&h->ev_sub, cudaEventDisableTiming));
-  h->d_data.assign(d.nstations, nullptr);
-  h->data_cap.assign(d.nstations, 0);
-  h->data_alloc.assign(d.nstations, 0);
-  if (d.max_data_bytes > 0) {
+  for (int k = 0; k < gx_handle::kSlots; k++) {
+    CKR(h, cudaMallocHost(&h->h_sub[k], h->sub_bytes));
+    memset(h->h_sub[k], 0, h->sub_bytes);
+    CKR(h, cudaEventCreateWithFlags(&h->ev_sub[k], cudaEventDisableTiming));
+    CKR(h, cudaEventCreateWithFlags(&h->ev_copied[k], cudaEventDisableTiming));
+    CKR(h, cudaEventCreateWithFlags(&h->ev_done[k], cudaEventDisableTiming));
+    h->d_data[k].assign(d.nstations, nullptr);
+    h->data_cap[k].assign(d.nstations, 0);
+    h->data_alloc[k].assign(d.nstations, 0);
+  }
+  if (d.max_data_bytes > 0) {   // slot 0 only; slot 1 grows on the first gx_subint_async
     for (int s = 0; s < d.nstations; s++) {
-      CKR(h, h->dalloc(&h->d_data[s], d.max_data_bytes));
-      h->data_cap[s] = d.max_data_bytes;
-      h->data_alloc[s] = d.max_data_bytes;
+      CKR(h, h->dalloc(&h->d_data[0][s], d.max_data_bytes));
+      h->data_cap[0][s] = d.max_data_bytes;
+      h->data_alloc[0][s] = d.max_data_bytes;
     }
   }
   CKR(h, cudaStreamSynchronize(h->stream));
@@ -715,12 +725,13 @@ static gx_status stage_subint(gx_handle *h, const gx_subint_desc *sub, const uin
     if (!sub->control[s]) return h->fail(GX_ERR_ARG, "missing control buffer");
   if (!sub->interp && !h->model)
     return h->fail(GX_ERR_ARG, "no interpolators given and the handle has no delay model");
-  // the previous subint's copy of the block must have left it
-  if (h->ev_sub_pending) {
-    CKR(h, cudaEventSynchronize(h->ev_sub));
-    h->ev_sub_pending = false;
+  // the previous copy of this slot's block must have left it
+  const int k = h->slot;
+  if (h->ev_sub_pending[k]) {
+    CKR(h, cudaEventSynchronize(h->ev_sub[k]));
+    h->ev_sub_pending[k] = false;
   }
-  unsigned char *b = h->h_sub;
+  unsigned char *b = h->h_sub[k];
   *reinterpret_cast<SubintClock *>(b) = SubintClock{sub->sec, sub->ns, sub->scan_start_sec};
   int64_t *lens = reinterpret_cast<int64_t *>(b + h->o_len);
   const uint8_t **ptrs = reinterpret_cast<const uint8_t **>(b + h->o_ptr);
@@ -757,10 +768,11 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
     h->ev_stage.clear();
   }
   h->launches = 0;
-  CKR(h, cudaMemcpyAsync(h->d_sub, h->h_sub, h->sub_bytes, cudaMemcpyHostToDevice, st));
+  const int k = h->slot;
+  CKR(h, cudaMemcpyAsync(h->d_sub, h->h_sub[k], h->sub_bytes, cudaMemcpyHostToDevice, st));
   if (timed) {
-    CKR(h, cudaEventRecord(h->ev_sub, st));
-    h->ev_sub_pending = true;
+    CKR(h, cudaEventRecord(h->ev_sub[k], st));
+    h->ev_sub_pending[k] = true;
   }
   SubintArrays S{};
   S.clock = reinterpret_cast<const SubintClock *>(h->d_sub);
@@ -808,7 +820,7 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
   }
   h->launches += (h->prods.empty() ? 0 : 1) + (h->wents.empty() ? 0 : 1);
   if ((r = mark(2, false)) != GX_OK) return r;
-  CKR(h, cudaMemcpyAsync(h->h_err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CKR(h, cudaMemcpyAsync(h->h_err + k, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
   return GX_OK;
 }
 
@@ -829,10 +841,10 @@ static gx_status run_device(gx_handle *h, const gx_subint_desc *sub, const uint8
 }
 
 // Status the kernels of the last subint left in *d_err (read after a synchronise).
-static gx_status kernel_status(gx_handle *h)
+static gx_status kernel_status(gx_handle *h, int k = 0)
 {
-  if (h->h_err && *h->h_err != 0)
-    return h->fail(GX_ERR_TIMEOUT, "a tensor-core X-step wait expired (status " + std::to_string(*h->h_err) + ")");
+  if (h->h_err && h->h_err[k] != 0)
+    return h->fail(GX_ERR_TIMEOUT, "a tensor-core X-step wait expired (status " + std::to_string(h->h_err[k]) + ")");
   return GX_OK;
 }
 
@@ -840,40 +852,97 @@ gx_status gx_subint_device(gx_handle *h, const gx_subint_desc *sub, float *dev_r
 {
   if (!h || !sub || !dev_results || !sub->data || !sub->datalen || !sub->control) return GX_ERR_ARG;
   if (h->device < 0) return h->fail(GX_ERR_STATE, "host-only handle (opened with device -1)");
+  if (!h->inflight.empty()) return h->fail(GX_ERR_STATE, "subints of gx_subint_async not yet waited for");
   CKR(h, cudaSetDevice(h->device));
   cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
   h->last_stream = st;
+  h->slot = 0;
   return run_device(h, sub, sub->data, reinterpret_cast<float2 *>(dev_results), st);
+}
+
+// Device buffers of slot k large enough for the subint's station data.
+static gx_status ensure_data(gx_handle *h, int k, const gx_subint_desc *sub)
+{
+  for (int s = 0; s < h->jd.nstations; s++) {
+    if (sub->datalen[s] < 0) return h->fail(GX_ERR_ARG, "negative data length");
+    if (sub->datalen[s] > h->data_cap[k][s]) {
+      if (h->d_data[k][s]) {
+        CKR(h, cudaFree(h->d_data[k][s]));
+        h->dev_bytes -= h->data_alloc[k][s];
+      }
+      h->d_data[k][s] = nullptr;
+      CKR(h, h->dalloc(&h->d_data[k][s], sub->datalen[s] + 64));
+      h->data_alloc[k][s] = sub->datalen[s] + 64;
+      h->data_cap[k][s] = sub->datalen[s];
+    }
+  }
+  return GX_OK;
 }
 
 gx_status gx_subint(gx_handle *h, const gx_subint_desc *sub, float *results)
 {
   if (!h || !sub || !results || !sub->data || !sub->datalen || !sub->control) return GX_ERR_ARG;
   if (h->device < 0) return h->fail(GX_ERR_STATE, "host-only handle (opened with device -1)");
+  if (!h->inflight.empty()) return h->fail(GX_ERR_STATE, "subints of gx_subint_async not yet waited for");
   CKR(h, cudaSetDevice(h->device));
+  gx_status r = ensure_data(h, 0, sub);
+  if (r != GX_OK) return r;
   const gx_job_desc &d = h->jd;
-  std::vector<const uint8_t *> dptr(d.nstations);
-  for (int s = 0; s < d.nstations; s++) {
-    if (sub->datalen[s] < 0) return h->fail(GX_ERR_ARG, "negative data length");
-    if (sub->datalen[s] > h->data_cap[s]) {
-      if (h->d_data[s]) {
-        CKR(h, cudaFree(h->d_data[s]));
-        h->dev_bytes -= h->data_alloc[s];
-      }
-      h->d_data[s] = nullptr;
-      CKR(h, h->dalloc(&h->d_data[s], sub->datalen[s] + 64));
-      h->data_alloc[s] = sub->datalen[s] + 64;
-      h->data_cap[s] = sub->datalen[s];
-    }
+  for (int s = 0; s < d.nstations; s++)
     if (sub->datalen[s] > 0)
-      CKR(h, cudaMemcpyAsync(h->d_data[s], sub->data[s], sub->datalen[s], cudaMemcpyHostToDevice, h->stream));
-    dptr[s] = h->d_data[s];
-  }
-  gx_status r = run_device(h, sub, dptr.data(), h->d_results, h->stream);
+      CKR(h, cudaMemcpyAsync(h->d_data[0][s], sub->data[s], sub->datalen[s], cudaMemcpyHostToDevice, h->stream));
+  h->slot = 0;
+  r = run_device(h, sub, h->d_data[0].data(), h->d_results, h->stream);
   if (r != GX_OK) return r;
   CKR(h, cudaMemcpyAsync(results, h->d_results, sizeof(float2) * h->rl, cudaMemcpyDeviceToHost, h->stream));
   CKR(h, cudaStreamSynchronize(h->stream));
   return kernel_status(h);
+}
+
+gx_status gx_subint_async(gx_handle *h, const gx_subint_desc *sub, float *results)
+{
+  if (!h || !sub || !results || !sub->data || !sub->datalen || !sub->control) return GX_ERR_ARG;
+  if (h->device < 0) return h->fail(GX_ERR_STATE, "host-only handle (opened with device -1)");
+  if ((int)h->inflight.size() >= gx_handle::kSlots)
+    return h->fail(GX_ERR_STATE, "two subints in flight: gx_subint_wait for one first");
+  CKR(h, cudaSetDevice(h->device));
+  if (!h->copy_stream) CKR(h, cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+  // the other slot than the one in flight; its last subint has been waited for,
+  // so its kernels no longer read its data buffers
+  const int k = h->inflight.empty() ? 0 : 1 - h->inflight.back();
+  gx_status r = ensure_data(h, k, sub);
+  if (r != GX_OK) return r;
+  const gx_job_desc &d = h->jd;
+  for (int s = 0; s < d.nstations; s++)
+    if (sub->datalen[s] > 0)
+      CKR(h, cudaMemcpyAsync(h->d_data[k][s], sub->data[s], sub->datalen[s], cudaMemcpyHostToDevice,
+                             h->copy_stream));
+  CKR(h, cudaEventRecord(h->ev_copied[k], h->copy_stream));
+  h->slot = k;
+  r = stage_subint(h, sub, h->d_data[k].data());
+  if (r == GX_OK) {
+    // the kernels start once this subint's data is in and the previous subint's work is done
+    r = h->cuda(cudaStreamWaitEvent(h->stream, h->ev_copied[k], 0), "cudaStreamWaitEvent");
+    if (r == GX_OK) r = gx_enqueue_subint(h, h->d_results, h->stream);
+  }
+  h->slot = 0;
+  if (r != GX_OK) return r;
+  CKR(h, cudaMemcpyAsync(results, h->d_results, sizeof(float2) * h->rl, cudaMemcpyDeviceToHost, h->stream));
+  CKR(h, cudaEventRecord(h->ev_done[k], h->stream));
+  h->last_stream = h->stream;
+  h->inflight.push_back(k);
+  return GX_OK;
+}
+
+gx_status gx_subint_wait(gx_handle *h)
+{
+  if (!h) return GX_ERR_ARG;
+  if (h->inflight.empty()) return h->fail(GX_ERR_STATE, "no subint of gx_subint_async in flight");
+  const int k = h->inflight.front();
+  h->inflight.pop_front();
+  CKR(h, cudaSetDevice(h->device));
+  CKR(h, cudaEventSynchronize(h->ev_done[k]));
+  return kernel_status(h, k);
 }
 
 gx_status gx_synchronize(gx_handle *h)

@@ -159,7 +159,7 @@ struct gx_batch {
     if (r != GX_OK) return r;
     if ((r = cuda(cudaEventElapsedTime(&last_ms, ev0, ev1), "cudaEventElapsedTime")) != GX_OK) return r;
     for (size_t j = 0; j < jobs.size(); j++)
-      if (jobs[j]->h_err && *jobs[j]->h_err != 0)
+      if (jobs[j]->h_err && jobs[j]->h_err[0] != 0)
         return fail(GX_ERR_TIMEOUT, "job " + std::to_string(j) + ": a tensor-core X-step wait expired");
     if (tuning) {
       const int ci = cand_index(run_branches);

@@ -2,6 +2,7 @@
 // shared by the translation units of the host driver.
 #pragma once
 #include <cstdint>
+#include <deque>
 #include <memory>
 #include <string>
 #include <vector>
@@ -40,7 +41,7 @@ struct gx_handle {
   gx::TcProdEntry *d_tcprods = nullptr;
   gx::TcRowEntry *d_tcrows = nullptr;
   int *d_err = nullptr;            // kernel status (bounded waits that expired)
-  int *h_err = nullptr;            // pinned copy of *d_err after each subint
+  int *h_err = nullptr;            // pinned copies of *d_err after each subint, one per slot
   cudaStream_t last_stream = nullptr;  // stream of the last gx_subint_device
 
   gx::DevStation *d_st = nullptr;
@@ -55,15 +56,22 @@ struct gx_handle {
   // the device with one copy per subint:
   //   SubintClock | datalen[nst] (int64) | data pointers[nst] | interp[nst][3]
   //   (double) | control words[nst][ctrlstride] (int32)
-  unsigned char *h_sub = nullptr, *d_sub = nullptr;
+  // Two slots, so that gx_subint_async can stage and upload one subint while
+  // the previous one computes; every other entry point uses slot 0.
+  static constexpr int kSlots = 2;
+  int slot = 0;                    // slot of the subint being staged and enqueued
+  unsigned char *h_sub[kSlots] = {}, *d_sub = nullptr;
   size_t sub_bytes = 0, o_len = 0, o_ptr = 0, o_interp = 0, o_ctrl = 0;
-  cudaEvent_t ev_sub = nullptr;    // recorded after the block's copy (host may rewrite it once passed)
-  bool ev_sub_pending = false;
+  cudaEvent_t ev_sub[kSlots] = {}; // recorded after a block's copy (host may rewrite it once passed)
+  bool ev_sub_pending[kSlots] = {};
   int ctrlstride = 0;
   bool untimed = false;            // no events recorded (batch runs, CUDA-graph capture)
-  std::vector<uint8_t *> d_data;
-  std::vector<int64_t> data_cap;     // usable bytes of d_data[s]
-  std::vector<long long> data_alloc; // allocated bytes of d_data[s]
+  std::vector<uint8_t *> d_data[kSlots];     // host-buffer entry points: device copies of the station data
+  std::vector<int64_t> data_cap[kSlots];     // usable bytes of d_data[k][s]
+  std::vector<long long> data_alloc[kSlots]; // allocated bytes of d_data[k][s]
+  cudaStream_t copy_stream = nullptr;        // uploads of gx_subint_async
+  cudaEvent_t ev_copied[kSlots] = {}, ev_done[kSlots] = {};
+  std::deque<int> inflight;                  // slots of gx_subint_async calls not yet waited for
 
   gx::SubintArrays last{};
   bool have_last = false;

@@ -190,8 +190,8 @@ gx_status gx_server_submit(gx_server *s, int job, const gx_subint_desc *sub, flo
     bytes = 0;
     const gx_handle *h = s->jobs[job].h;
     if (h && !s->device_inputs && sub->datalen)
-      for (int i = 0; i < h->jd.nstations && i < (int)h->data_cap.size(); i++)
-        bytes += std::max<long long>(0, (long long)sub->datalen[i] - (long long)h->data_cap[i]);
+      for (int i = 0; i < h->jd.nstations && i < (int)h->data_cap[0].size(); i++)
+        bytes += std::max<long long>(0, (long long)sub->datalen[i] - (long long)h->data_cap[0][i]);
   }
   if (s->resident_total + bytes > s->budget) return GX_ERR_NOMEM;
   Request *r = new Request();

@@ -56,7 +56,7 @@ EXPORTED_SYMBOLS = ("gx_open", "gx_open_input", "gx_close", "gx_last_error", "gx
                     "gx_server_submit", "gx_server_wait", "gx_server_stats", "gx_server_close", "gx_device_bytes",
                     "gx_server_last_error", "gx_batch_open", "gx_batch_run", "gx_batch_synchronize",
                     "gx_batch_info", "gx_batch_last_error", "gx_batch_close", "gx_vis_buffer",
-                    "gx_vis_set_subints", "gx_vis_clear")
+                    "gx_vis_set_subints", "gx_vis_clear", "gx_subint_async", "gx_subint_wait")
 
 
 def subint_device_noalloc(jd: capi.JobDesc, sd: capi.SubintDesc, dev_results_ptr: int, stream_ptr: int = 0) -> None:
@@ -177,6 +177,22 @@ class Correlator:
 
     def synchronize(self):
         self._check(lib().gx_synchronize(self.h))
+
+    def subint_async(self, sd: capi.SubintDesc, out: np.ndarray) -> None:
+        """Pipelined gx_subint: returns once the subint is enqueued (at most two in
+        flight); `sd`'s buffers and `out` (complex64, pinned for overlap) must stay
+        alive until the matching wait()."""
+        self._check(lib().gx_subint_async(self.h, sd.ptr(), out.ctypes.data_as(C.c_void_p)))
+        if not hasattr(self, "_inflight"):
+            self._inflight = []
+        self._inflight.append((sd, out))
+
+    def wait(self) -> np.ndarray:
+        """Waits for the oldest gx_subint_async call; returns its result array."""
+        st = lib().gx_subint_wait(self.h)
+        sd, out = self._inflight.pop(0) if getattr(self, "_inflight", None) else (None, None)
+        self._check(st)
+        return out
 
     def set_tc_scales(self, station: int, band: int, scales) -> None:
         """Per-channel operand scales of the tensor-core X-step for one station band

@@ -182,6 +182,18 @@ gx_status gx_subint(gx_handle *h, const gx_subint_desc *sub, float *results);
 gx_status gx_subint_device(gx_handle *h, const gx_subint_desc *sub, float *dev_results, void *stream);
 gx_status gx_synchronize(gx_handle *h);
 
+/* Pipelined form of gx_subint (no counterpart in the reference, whose Core
+   threads block on each slot): copies the station data to the device on the
+   handle's copy stream, enqueues the subint's kernels behind that copy and
+   the result copy into `results`, and returns.  gx_subint_wait waits for the
+   oldest subint in flight and returns its status.  At most two are in flight
+   (GX_ERR_STATE for a third), so one subint's upload overlaps the other's
+   kernels; `sub`'s buffers and `results` must stay valid (and be pinned for
+   the copies to overlap) until its wait returns.  gx_subint and
+   gx_subint_device return GX_ERR_STATE while any is in flight. */
+gx_status gx_subint_async(gx_handle *h, const gx_subint_desc *sub, float *results);
+gx_status gx_subint_wait(gx_handle *h);
+
 /* No counterpart in the reference.  The same subint work as gx_subint_device
    for callers that cannot allocate device memory (code inside CUDA stream
    capture, real-time threads that must not take cudaMalloc's implicit

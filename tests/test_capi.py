@@ -130,3 +130,15 @@ def test_spectra_budget_sets_pass_length():
                                     device=-1)
     assert c.info.block_chunk == 50
     c.close()
+
+
+def test_async_needs_a_device_handle():
+    c = gxcorr.Correlator.from_desc(capi.job_desc_from_spec(jobs.spec_c1()), device=-1)
+    out = np.zeros(c.result_length, np.complex64)
+    with pytest.raises(gxcorr.GxError) as ei:
+        c.subint_async(capi.SubintDesc(0, 0, 0, 0.0, [0] * 4, [0] * 4, [0] * 4, 3), out)
+    assert ei.value.status == 8
+    with pytest.raises(gxcorr.GxError) as ei:
+        c.wait()
+    assert ei.value.status == 8
+    c.close()

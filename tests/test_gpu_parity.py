@@ -174,3 +174,45 @@ def test_gpu_fstep_kernel_choices_agree(case, gx, oracle_lib, monkeypatch):
         c.close()
         m, wrel = _compare(g, o, prep.jd, spec, oracle_lib)
         assert m < REC_TOL and wrel < W_TOL, (r16_min, m, wrel)
+
+
+def test_gpu_async_pipeline_matches_sync(gx):
+    """gx_subint_async / gx_subint_wait (two subints in flight, uploads on a
+    copy stream) give the same result arrays as gx_subint, in order; a third
+    subint in flight and a blocking call meanwhile are refused."""
+    import torch
+    from difx_b200 import capi
+    spec = jobs.spec_c1(name="c1async", seed=43)
+    starts = [100_000_000 + k * spec.subint_ns for k in range(4)]
+    prep = jobs.prepare(spec, starts)
+    c = gx.Correlator.from_desc(prep.jd)
+    want = [c.subint(sd).copy() for sd in prep.sds]
+    pinned = []
+    sds = []
+    for si, ip in zip(prep.subs, prep.interps):
+        data = [torch.from_numpy(x).pin_memory() for x in si.data]
+        pinned.append(data)
+        sds.append(capi.SubintDesc(si.scan, si.sec, si.ns, 0.0, [t.data_ptr() for t in data],
+                                   [len(x) for x in si.data], [x.ctypes.data for x in si.control],
+                                   len(si.control[0]), ip))
+    outs = [torch.zeros(2 * c.result_length, dtype=torch.float32).pin_memory().numpy().view(np.complex64)
+            for _ in range(4)]
+    c.subint_async(sds[0], outs[0])
+    c.subint_async(sds[1], outs[1])
+    with pytest.raises(gx.GxError) as ei:
+        c.subint_async(sds[2], outs[2])
+    assert ei.value.status == 8
+    with pytest.raises(gx.GxError) as ei:
+        c.subint(prep.sds[0])
+    assert ei.value.status == 8
+    np.testing.assert_array_equal(c.wait(), want[0])
+    c.subint_async(sds[2], outs[2])
+    np.testing.assert_array_equal(c.wait(), want[1])
+    c.subint_async(sds[3], outs[3])
+    np.testing.assert_array_equal(c.wait(), want[2])
+    np.testing.assert_array_equal(c.wait(), want[3])
+    with pytest.raises(gx.GxError) as ei:
+        c.wait()
+    assert ei.value.status == 8
+    np.testing.assert_array_equal(c.subint(prep.sds[1]), want[1])   # blocking calls work again
+    c.close()
