@@ -29,12 +29,37 @@ __host__ __device__ __forceinline__ float2 mul_mi(float2 a) { return make_float2
 // shared-memory position of element i: one pad element per 16
 __host__ __device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
 
-// 4-point forward DFT in place, natural order
+// Paired FP32 add and subtract (one f32x2 instruction on sm_100, same
+// rounding as the two scalar operations); plain float2 arithmetic on the host.
+__host__ __device__ __forceinline__ float2 add2(float2 a, float2 b)
+{
+#ifdef __CUDA_ARCH__
+  return __fadd2_rn(a, b);
+#else
+  return add(a, b);
+#endif
+}
+__host__ __device__ __forceinline__ float2 sub2(float2 a, float2 b)
+{
+#ifdef __CUDA_ARCH__
+  float2 r;
+  asm("{\n\t.reg .b64 pa, pb, pd;\n\tmov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+      "sub.rn.f32x2 pd, pa, pb;\n\tmov.b64 {%0, %1}, pd;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+#else
+  return sub(a, b);
+#endif
+}
+
+// 4-point forward DFT in place, natural order (the +-i terms stay scalar:
+// their operands are swapped lanes)
 __host__ __device__ __forceinline__ void dft4(float2 &a, float2 &b, float2 &c, float2 &d)
 {
-  const float2 s0 = add(a, c), s1 = sub(a, c), s2 = add(b, d), s3 = mul_mi(sub(b, d));
-  a = add(s0, s2);
-  c = sub(s0, s2);
+  const float2 s0 = add2(a, c), s1 = sub2(a, c), s2 = add2(b, d), s3 = mul_mi(sub2(b, d));
+  a = add2(s0, s2);
+  c = sub2(s0, s2);
   b = add(s1, s3);
   d = sub(s1, s3);
 }
@@ -143,21 +168,28 @@ __host__ __device__ __forceinline__ void pass16(float2 (&v)[16], int j, int Ns, 
   dft16(v);
 }
 
-// Outputs of a radix-16 pass of stride Ns into the padded exchange buffer.
+// Outputs of a radix-16 pass of stride Ns (a power of 16) into the padded
+// exchange buffer: element base + Ns r sits at pad(base) + r (Ns + Ns / 16)
+// (Ns r is a multiple of 16, so the pad of the sum is the sum of the pads), and
+// for Ns = 1 (base = 16 j) at 17 j + r: one base index, then constant offsets.
 __host__ __device__ __forceinline__ void store16(const float2 (&v)[16], int j, int Ns, float2 *sm)
 {
   const int m = j & (Ns - 1);
-  const int base = (j - m) * 16 + m;
+  const int p0 = Ns == 1 ? 17 * j : pad((j - m) * 16 + m);
+  const int step = Ns == 1 ? 1 : Ns + (Ns >> 4);
 #pragma unroll
-  for (int r = 0; r < 16; r++) sm[pad(base + Ns * r)] = v[r];
+  for (int r = 0; r < 16; r++) sm[p0 + step * r] = v[r];
 }
 
-// Inputs x[j + NT t] of the next pass from the padded exchange buffer.
+// Inputs x[j + NT t] of the next pass from the padded exchange buffer
+// (NT = F / 16 is a multiple of 16: pad(j + NT t) = pad(j) + t (NT + NT / 16)).
 template <int F>
 __host__ __device__ __forceinline__ void load16(float2 (&v)[16], int j, const float2 *sm)
 {
+  constexpr int NT = F / 16, step = NT + NT / 16;
+  const int p0 = pad(j);
 #pragma unroll
-  for (int t = 0; t < 16; t++) v[t] = sm[pad(j + (F / 16) * t)];
+  for (int t = 0; t < 16; t++) v[t] = sm[p0 + step * t];
 }
 
 // Final radix-R0 pass (stride F / R0) in registers: 16 / R0 transforms per thread.

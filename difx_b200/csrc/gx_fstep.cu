@@ -594,6 +594,10 @@ __device__ __forceinline__ void group_sync(int g)
 // Samples x[j + NT t] (t = 0..15) of band bd of the block described by P,
 // decoded and fringe-rotated (mode.cpp:1160-1183): frame q and in-frame
 // sample r advance incrementally; all 16 raw loads are issued before use.
+// When a time sample of all bands is whole bytes and a step of NT samples
+// crosses at most one frame boundary (NT <= samples per frame), the byte
+// offset advances by a constant with one predicated correction per boundary;
+// otherwise each sample's bit offset is formed from (q, r).
 template <int F, int CPLX>
 __device__ __forceinline__ void r16_decode_rotate(const DevJob &J, const uint8_t *__restrict__ data,
                                                   const BlockParam &P, int bd, int j, const float2 *rs,
@@ -610,27 +614,55 @@ __device__ __forceinline__ void r16_decode_rotate(const DevJob &J, const uint8_t
   q -= P.fr0;
   const int bitband = bd * (CPLX ? 2 : 1) * J.nbits;
   unsigned int raw[16];
+  if ((bits_ts & 7) == 0 && NT <= fsamp && (byte_pairs || !CPLX)) {
+    const int bpts = bits_ts >> 3, sh = bitband & 7;
+    const uint8_t *fr = data + ((long long)P.fr0 + q) * J.framebytes + 32 + (bitband >> 3);
+    int off = r * bpts;
+    bool ok = (P.validmask >> q) & 1ull;
 #pragma unroll
-  for (int t = 0; t < 16; t++) {
-    raw[t] = 0xFFFFFFFFu;   // invalid frame: decodes to zero
-    if ((P.validmask >> q) & 1ull) {
-      const uint8_t *payload = data + ((long long)P.fr0 + q) * J.framebytes + 32;
-      const int bit0 = r * bits_ts + bitband;   // < 8 * payload bytes
-      if (byte_pairs) {
-        raw[t] = __ldg(reinterpret_cast<const unsigned short *>(payload + (bit0 >> 3)));
-      } else {
-        unsigned int w = (__ldg(payload + (bit0 >> 3)) >> (bit0 & 7)) & cmask;
-        if (CPLX) {
-          const int bit1 = bit0 + J.nbits;
-          w |= ((__ldg(payload + (bit1 >> 3)) >> (bit1 & 7)) & cmask) << 8;
-        }
-        raw[t] = w;
+    for (int t = 0; t < 16; t++) {
+      if (byte_pairs)
+        raw[t] = ok ? (unsigned int)__ldg(reinterpret_cast<const unsigned short *>(fr + off)) : 0xFFFFFFFFu;
+      else
+        raw[t] = ok ? ((unsigned int)(__ldg(fr + off) >> sh) & cmask) : 0xFFFFFFFFu;
+      r += NT;
+      off += NT * bpts;
+      if (r >= fsamp) {   // next frame: skip its header
+        r -= fsamp;
+        off -= fsamp * bpts;
+        q++;
+        fr += J.framebytes;
+        ok = (P.validmask >> q) & 1ull;
       }
     }
-    r += NT;
-    while (r >= fsamp) { r -= fsamp; q++; }
+  } else {
+#pragma unroll
+    for (int t = 0; t < 16; t++) {
+      raw[t] = 0xFFFFFFFFu;   // invalid frame: decodes to zero
+      if ((P.validmask >> q) & 1ull) {
+        const uint8_t *payload = data + ((long long)P.fr0 + q) * J.framebytes + 32;
+        const int bit0 = r * bits_ts + bitband;   // < 8 * payload bytes
+        if (byte_pairs) {
+          raw[t] = __ldg(reinterpret_cast<const unsigned short *>(payload + (bit0 >> 3)));
+        } else {
+          unsigned int w = (__ldg(payload + (bit0 >> 3)) >> (bit0 & 7)) & cmask;
+          if (CPLX) {
+            const int bit1 = bit0 + J.nbits;
+            w |= ((__ldg(payload + (bit1 >> 3)) >> (bit1 & 7)) & cmask) << 8;
+          }
+          raw[t] = w;
+        }
+      }
+      r += NT;
+      while (r >= fsamp) { r -= fsamp; q++; }
+    }
   }
+  // rotator x[n] = sub[n mod S] * step[n / S]; with S dividing NT the sub entry
+  // is the same for all 16 samples of the thread
   const int Sd = J.stride, lgS = J.lgstride;
+  const bool kfix = (NT & (Sd - 1)) == 0;
+  const float2 rsk = rs[j & (Sd - 1)];
+  const int jj0 = j >> lgS, jstep = NT >> lgS;
 #pragma unroll
   for (int t = 0; t < 16; t++) {
     float2 u = make_float2(0.f, 0.f);
@@ -638,9 +670,15 @@ __device__ __forceinline__ void r16_decode_rotate(const DevJob &J, const uint8_t
       u.x = s_lut[raw[t] & 255u];
       if (CPLX) u.y = s_lut[(raw[t] >> 8) & 255u];
     }
-    const int n = j + NT * t;
-    const int k = n & (Sd - 1), jj = n >> lgS;
-    const float2 rot = (jj == 0) ? rs[k] : cmul_exact(rs[k], rp[jj]);
+    float2 rot;
+    if (kfix) {
+      const int jj = jj0 + jstep * t;
+      rot = (jj == 0) ? rsk : cmul_exact(rsk, rp[jj]);
+    } else {
+      const int n = j + NT * t;
+      const int k = n & (Sd - 1), jj = n >> lgS;
+      rot = (jj == 0) ? rs[k] : cmul_exact(rs[k], rp[jj]);
+    }
     v[t] = CPLX ? cmul(rot, u) : make_float2(u.x * rot.x, u.x * rot.y);
   }
 }
@@ -746,13 +784,18 @@ fstep_r16_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays
     r16_decode_rotate<F, CPLX>(J, data, P, bd, j, rs, rp, s_lut, v);
     r16_fft<F, CTA>(v, j, g, sm, tw);
     // register t holds bin j + NT t: sideband selection and fractional-sample correction
+    // (with S dividing NT, channel c mod S is the same for all the thread's bins:
+    // j mod S, or -j mod S for complex lower sideband)
     const int lsb = st.lsb[lf];
+    const bool kfix = (NT & (Sd - 1)) == 0;
+    const float2 fsk = fs[((CPLX && lsb) ? -j : j) & (Sd - 1)];
+    float2 *drow = dst + spec_offset(J, row, 0);
 #pragma unroll
     for (int t = 0; t < 16; t++) {
       float2 val = v[t];
       int c;
       if (!r16_channel<F, CPLX>(t, j, lsb, val, c)) continue;
-      dst[spec_offset(J, row, c)] = cmul(val, cmul_exact(fs[c & (Sd - 1)], fp[c >> lgS]));
+      drow[c] = cmul(val, cmul_exact(kfix ? fsk : fs[c & (Sd - 1)], fp[c >> lgS]));
     }
   }
 }
