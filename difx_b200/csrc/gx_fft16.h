@@ -139,7 +139,9 @@ struct Plan {
 
 // Radix-16 pass of stride Ns: twiddle (Ns > 1) and transform in registers.
 // tw[m] = exp(-2 pi i m / F).  The twiddles w^r, r = 1..15, of a thread come
-// from four table entries (w, w^2, w^4, w^8) and at most three products each.
+// from four table entries (w, w^2, w^4, w^8) and at most three products each:
+// the table gathers of a warp touch many cache lines, so fifteen loads per
+// pass cost more L1 throughput than eleven products cost issue slots.
 template <int F, typename TW>
 __host__ __device__ __forceinline__ void pass16(float2 (&v)[16], int j, int Ns, TW tw)
 {

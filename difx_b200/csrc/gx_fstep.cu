@@ -790,12 +790,24 @@ fstep_r16_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays
     const bool kfix = (NT & (Sd - 1)) == 0;
     const float2 fsk = fs[((CPLX && lsb) ? -j : j) & (Sd - 1)];
     float2 *drow = dst + spec_offset(J, row, 0);
-#pragma unroll
-    for (int t = 0; t < 16; t++) {
-      float2 val = v[t];
-      int c;
-      if (!r16_channel<F, CPLX>(t, j, lsb, val, c)) continue;
+    auto emit = [&](int c, float2 val) {
       drow[c] = cmul(val, cmul_exact(kfix ? fsk : fs[c & (Sd - 1)], fp[c >> lgS]));
+    };
+    // one unrolled loop per sideband, so that every channel index is j plus a constant
+    if (lsb) {
+#pragma unroll
+      for (int t = 0; t < 16; t++) {
+        float2 val = v[t];
+        int c;
+        if (r16_channel<F, CPLX>(t, j, 1, val, c)) emit(c, val);
+      }
+    } else {
+#pragma unroll
+      for (int t = 0; t < 16; t++) {
+        float2 val = v[t];
+        int c;
+        if (r16_channel<F, CPLX>(t, j, 0, val, c)) emit(c, val);
+      }
     }
   }
 }
