@@ -41,8 +41,10 @@ def lib():
         L.gx_status_string.restype = C.c_char_p
         L.gx_server_last_error.restype = C.c_char_p
         L.gx_batch_last_error.restype = C.c_char_p
+        L.gx_vdifmux_last_error.restype = C.c_char_p
         for name in EXPORTED_SYMBOLS:
-            if name not in ("gx_last_error", "gx_status_string", "gx_server_last_error", "gx_batch_last_error"):
+            if name not in ("gx_last_error", "gx_status_string", "gx_server_last_error", "gx_batch_last_error",
+                            "gx_vdifmux_last_error"):
                 getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -56,7 +58,9 @@ EXPORTED_SYMBOLS = ("gx_open", "gx_open_input", "gx_close", "gx_last_error", "gx
                     "gx_server_submit", "gx_server_wait", "gx_server_stats", "gx_server_close", "gx_device_bytes",
                     "gx_server_last_error", "gx_batch_open", "gx_batch_run", "gx_batch_synchronize",
                     "gx_batch_info", "gx_batch_last_error", "gx_batch_close", "gx_vis_buffer",
-                    "gx_vis_set_subints", "gx_vis_clear", "gx_subint_async", "gx_subint_wait")
+                    "gx_vis_set_subints", "gx_vis_clear", "gx_subint_async", "gx_subint_wait", "gx_vdifmux_open",
+                    "gx_vdifmux_info", "gx_vdifmux_run", "gx_vdifmux_reset_stats", "gx_vdifmux_last_error",
+                    "gx_vdifmux_close")
 
 
 def subint_device_noalloc(jd: capi.JobDesc, sd: capi.SubintDesc, dev_results_ptr: int, stream_ptr: int = 0) -> None:
@@ -368,6 +372,54 @@ class Batch:
         if self.b:
             lib().gx_batch_close(self.b)
             self.b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class VdifMuxStats(C.Structure):
+    _fields_ = [(n, C.c_longlong) for n in (
+        "valid_frames", "invalid_frames", "discarded_frames", "wrong_thread_frames", "skipped_bytes", "fill_bytes",
+        "duplicate_frames", "bytes_processed", "good_output_frames", "partial_output_frames", "filler_output_frames",
+        "calls", "src_bytes", "src_used", "dest_bytes", "dest_used", "output_frames", "start_frame",
+        "returned_bytes")] + [("epoch", C.c_int)]
+
+
+class VdifMux:
+    """Multi-thread VDIF -> multi-channel single-thread VDIF on the device (gx_vdifmux_*)."""
+
+    def __init__(self, frame_bytes: int, frames_per_second: int, bits: int, thread_ids: Sequence[int],
+                 nsort: int = 32, ngap: int = 1000, flags: int = 0, channels_per_thread: int = 1, device: int = 0):
+        ids = (C.c_int * len(thread_ids))(*thread_ids)
+        self.m = C.c_void_p()
+        st = lib().gx_vdifmux_open(frame_bytes, frames_per_second, bits, len(thread_ids), ids, channels_per_thread,
+                                   nsort, ngap, flags, device, C.byref(self.m))
+        if st != 0:
+            raise GxError(st, "gx_vdifmux_open failed")
+        ofb, nch, gran = C.c_int(0), C.c_int(0), C.c_int(0)
+        lib().gx_vdifmux_info(self.m, C.byref(ofb), C.byref(nch), C.byref(gran))
+        self.output_frame_bytes, self.output_channels, self.frame_granularity = ofb.value, nch.value, gran.value
+
+    def run(self, src_ptr: int, src_bytes: int, dest_ptr: int, dest_bytes: int, start_frame: int = -1,
+            stream_ptr: int = 0) -> VdifMuxStats:
+        stats = VdifMuxStats()
+        st = lib().gx_vdifmux_run(self.m, C.c_void_p(src_ptr), C.c_longlong(src_bytes), C.c_void_p(dest_ptr),
+                                  C.c_longlong(dest_bytes), C.c_longlong(start_frame), C.byref(stats),
+                                  C.c_void_p(stream_ptr) if stream_ptr else None)
+        if st != 0:
+            raise GxError(st, lib().gx_vdifmux_last_error(self.m).decode())
+        return stats
+
+    def reset_stats(self) -> None:
+        lib().gx_vdifmux_reset_stats(self.m)
+
+    def close(self) -> None:
+        if self.m:
+            lib().gx_vdifmux_close(self.m)
+            self.m = None
 
     def __del__(self):
         try:

@@ -346,6 +346,58 @@ gx_status gx_batch_info(const gx_batch *b, int *nstreams, int *tuning, int *laun
 const char *gx_batch_last_error(const gx_batch *b);
 gx_status gx_batch_close(gx_batch *b);
 
+/* ---- Multi-thread VDIF multiplexing on the device ------------------------ */
+
+/* The reference's vdifmux (vdifio/src/vdifmux.c:496-1033), as the VDIF
+   DataStream uses it (vdiffile.cpp:495-565, 700-760): single-thread VDIF
+   frames of several threads, in one device buffer, become multi-channel
+   frames of one thread, sorted in time, in another device buffer.  Frame
+   classification and the corner turn run on the GPU; the sequential
+   decisions (duplicates, the out-of-order window nsort, the gap limit ngap,
+   the end-of-buffer back-off) run on the host over 16 bytes per frame.  The
+   input must be frame-aligned (frame k at byte k x input_frame_bytes): a
+   frame that starts but does not end with the fill pattern, or whose header
+   has another size, channel count or bit depth, is skipped whole (the
+   reference rescans it byte by byte).  Output headers, payloads of the frames
+   the reference corner-turns, the statistics and the returned byte count
+   then equal the reference's; the payload of a filler frame (invalid bit
+   set) is left as the destination held it.  Output slots past nthreads
+   (rounded up to a power of two) hold zeros.  One channel per input thread
+   (channels_per_thread must be 1: GX_ERR_UNSUPPORTED otherwise); fan-out
+   (several threads per channel) and legacy headers are not implemented. */
+typedef struct gx_vdifmux gx_vdifmux;
+#define GX_VDIFMUX_GOTOEND 0x01             /* VDIF_MUX_FLAG_GOTOEND */
+#define GX_VDIFMUX_RESPECTGRANULARITY 0x02  /* VDIF_MUX_FLAG_RESPECTGRANULARITY */
+#define GX_VDIFMUX_ENABLEVALIDITY 0x04      /* VDIF_MUX_FLAG_ENABLEVALIDITY */
+#define GX_VDIFMUX_COMPLEX 0x20             /* VDIF_MUX_FLAG_COMPLEX */
+#define GX_VDIFMUX_PROPAGATEVALIDITY 0x40   /* VDIF_MUX_FLAG_PROPAGATEVALIDITY (EDV4 output) */
+
+/* struct vdif_mux_statistics (vdifio.h:404-432): the first eleven
+   accumulate over calls (gx_vdifmux_reset_stats clears them), the rest
+   describe the last call; returned_bytes is vdifmux's return value. */
+typedef struct gx_vdifmux_stats {
+  long long valid_frames, invalid_frames, discarded_frames, wrong_thread_frames, skipped_bytes, fill_bytes,
+      duplicate_frames, bytes_processed, good_output_frames, partial_output_frames, filler_output_frames;
+  long long calls;
+  long long src_bytes, src_used, dest_bytes, dest_used, output_frames, start_frame, returned_bytes;
+  int epoch;
+} gx_vdifmux_stats;
+
+/* configurevdifmux + setvdifmuxinputchannels (vdifmux.c:107-242).  device < 0:
+   host-only (gx_vdifmux_info works, gx_vdifmux_run returns GX_ERR_STATE). */
+gx_status gx_vdifmux_open(int input_frame_bytes, int frames_per_second, int bits_per_sample, int nthreads,
+                          const int *thread_ids, int channels_per_thread, int nsort, int ngap, int flags, int device,
+                          gx_vdifmux **out);
+gx_status gx_vdifmux_info(const gx_vdifmux *m, int *output_frame_bytes, int *output_channels, int *frame_granularity);
+/* vdifmux(): src and dest are device buffers (4-byte aligned); start_frame < 0
+   starts at the lowest frame number among the first nsort usable frames.
+   Synchronises `stream` before returning. */
+gx_status gx_vdifmux_run(gx_vdifmux *m, const uint8_t *src, long long src_bytes, uint8_t *dest, long long dest_bytes,
+                         long long start_frame, gx_vdifmux_stats *stats, void *stream);
+gx_status gx_vdifmux_reset_stats(gx_vdifmux *m);
+const char *gx_vdifmux_last_error(const gx_vdifmux *m);
+gx_status gx_vdifmux_close(gx_vdifmux *m);
+
 /* Device memory a handle holds, bytes. */
 gx_status gx_device_bytes(const gx_handle *h, long long *bytes);
 

@@ -30,6 +30,7 @@ def build(reference: bool = True) -> None:
     subprocess.run(["make", "-s", "-C", HERE], check=True)
     if reference and os.path.isdir(REFERENCE_SRC):
         subprocess.run(["make", "-s", "-C", HERE, "ref", "-j8"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "vmux"], check=True)
 
 
 def reference_available() -> bool:
@@ -168,3 +169,26 @@ class Reference:
         n = self.lib.ref_unpack(self.h, station, data.ctypes.data_as(C.c_void_p), len(data), offset,
                                 out.ctypes.data_as(C.c_void_p), C.byref(w), C.byref(us))
         return out, w.value, us.value, n
+
+
+VMUX_LIB = os.path.join(HERE, "_ref", "libvdifmuxref.so")
+
+
+def vmux_available() -> bool:
+    return os.path.exists(VMUX_LIB)
+
+
+def ref_vdifmux(src: bytes, dest_bytes: int, frame_bytes: int, fps: int, bits: int, thread_ids, nsort: int,
+                ngap: int, flags: int, start_frame: int = -1, dest_init: int = 0):
+    """The reference's vdifmux on host buffers: (output bytes, stats array of 22
+    values in the order of vdifmux_harness.c)."""
+    lib = C.CDLL(VMUX_LIB)
+    dest = (C.c_ubyte * dest_bytes)(*([dest_init] * dest_bytes)) if dest_init else (C.c_ubyte * dest_bytes)()
+    srcb = (C.c_ubyte * len(src)).from_buffer_copy(src)
+    ids = (C.c_int * len(thread_ids))(*thread_ids)
+    out = (C.c_longlong * 22)()
+    rv = lib.ref_vdifmux(dest, dest_bytes, srcb, len(src), frame_bytes, fps, bits, len(thread_ids), ids, nsort, ngap,
+                         flags, C.c_longlong(start_frame), out)
+    if rv < 0:
+        raise RuntimeError(f"reference vdifmux failed: {rv}")
+    return bytes(dest), list(out)

@@ -39,7 +39,8 @@ def test_struct_layout_matches_c_compiler(tmp_path):
     import subprocess
     structs = {"gx_freq_desc": capi.gx_freq_desc, "gx_station_desc": capi.gx_station_desc,
                "gx_baseline_desc": capi.gx_baseline_desc, "gx_job_desc": capi.gx_job_desc,
-               "gx_subint_desc": capi.gx_subint_desc, "gx_layout_info": capi.gx_layout_info}
+               "gx_subint_desc": capi.gx_subint_desc, "gx_layout_info": capi.gx_layout_info,
+               "gx_vdifmux_stats": gxcorr.VdifMuxStats}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void){"]
     for name, cls in structs.items():
         lines.append(f'printf("{name} %zu\\n", sizeof({name}));')
