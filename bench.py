@@ -55,8 +55,8 @@ from difx_b200.jobfiles import JobSpec, Subband, write_job  # noqa: E402
 METRIC = "Gsamp/s correlated"
 UNIT = "Gsamp/s"
 XSTEPS = {"fp32": capi.GX_XSTEP_FP32, "tc": capi.GX_XSTEP_TC_FP16, "tc_hilo": capi.GX_XSTEP_TC_FP16_HILO}
-DEFAULT_SUBINT_MS = {"c3": 128.0, "c2": 200.0, "c1": 200.0, "c4": 0.0, "c5": 0.0}
-DEFAULT_XSTEP = {"c3": "tc_hilo", "c2": "fp32", "c1": "fp32", "c4": "tc_hilo", "c5": "tc_hilo"}
+DEFAULT_SUBINT_MS = {"c3": 128.0, "c2": 200.0, "c1": 200.0, "c4": 0.0, "c5": 0.0, "mux": 0.0}
+DEFAULT_XSTEP = {"c3": "tc_hilo", "c2": "fp32", "c1": "fp32", "c4": "tc_hilo", "c5": "tc_hilo", "mux": "fp32"}
 RHO = {"c3": 0.01, "c2": 0.02, "c1": 0.05}
 
 
@@ -467,6 +467,78 @@ def run_c4(args):
     return 0
 
 
+def mux_stream(nthreads=16, fps=4000, seconds=1, fb=8032, nbits=2, seed=77):
+    """Frame-aligned multi-thread VDIF: nthreads x fps frames per second of
+    2-bit samples, thread-interleaved in time order (as a recorder writes them)."""
+    rng = np.random.default_rng(seed)
+    n = nthreads * fps * seconds
+    buf = rng.integers(0, 256, (n, fb), dtype=np.uint8)
+    fr = np.arange(n) // nthreads
+    hdr = np.zeros((n, 8), np.uint32)
+    hdr[:, 0] = (1000 + fr // fps).astype(np.uint32)
+    hdr[:, 1] = (fr % fps).astype(np.uint32) | (40 << 24)
+    hdr[:, 2] = fb // 8
+    hdr[:, 3] = 0x4142 | ((np.arange(n) % nthreads).astype(np.uint32) << 16) | ((nbits - 1) << 26)
+    buf[:, :32] = hdr.view(np.uint8).reshape(n, 32)
+    return buf.reshape(-1)
+
+
+def run_mux(args):
+    """Device VDIF multiplexing of a 1 s, 16-thread, 2-bit stream (the VDIF
+    DataStream's corner turn): input bytes per second of device time."""
+    import torch
+    from difx_b200.gxcorr import VdifMux
+    nthreads, fps, fb, nbits = 16, 4000, 8032, 2
+    src = mux_stream(nthreads, fps, 1, fb, nbits)
+    m = VdifMux(fb, fps, nbits, list(range(nthreads)), nsort=32, ngap=fps // 4, flags=0x02 | 0x40)
+    nout = len(src) // fb // nthreads
+    dest_bytes = m.output_frame_bytes * (nout + 1)
+    d_src = torch.from_numpy(src).cuda()
+    d_dest = torch.empty(dest_bytes, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        m.run(d_src.data_ptr(), len(src), d_dest.data_ptr(), dest_bytes, -1, stream.cuda_stream)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        st = m.run(d_src.data_ptr(), len(src), d_dest.data_ptr(), dest_bytes, -1, stream.cuda_stream)
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    wall_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    peaks = load_peaks()
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    moved = len(src) + st.output_frames * m.output_frame_bytes
+    line = {"metric": "VDIF multiplex: input GB/s (device classification + corner turn, host decisions)",
+            "value": len(src) / (ms * 1e-3) / 1e9, "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8", "data": "synthetic (seeded 2-bit samples, valid headers)",
+            "config": {"workload": f"1 s of {nthreads}-thread 2-bit VDIF, {fb}-byte frames, {fps} frames/s per thread",
+                       "input_bytes": len(src), "output_frames": st.output_frames,
+                       "l2": "inputs larger than L2 (no flush)"},
+            "wall_ms_per_step": wall_ms,
+            "roofline": {"kernel": "vmux_output_kernel + vmux_classify_kernel + host decisions", "bound": "hbm",
+                         "achieved": moved / (ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                         "frac": moved / (ms * 1e-3) / 1e9 / hbm, "traffic": None,
+                         "peak_source": "of measured" if "hbm_gbs" in peaks else "of fallback"},
+            "gpu_launches": 2 * args.steps}
+    if not args.no_cpu_baseline:
+        try:
+            from oracle import pyoracle
+            if pyoracle.vmux_available():
+                _, ref = pyoracle.ref_vdifmux(src.tobytes(), dest_bytes, fb, fps, nbits, list(range(nthreads)), 32,
+                                              fps // 4, 0x02 | 0x40)
+                line["cpu_baseline"] = {"value": len(src) / (ref[22] * 1e-9) / 1e9, "unit": "GB/s", "cores": 1,
+                                        "kind": "reference",
+                                        "sample": "the reference's vdifmux (single thread, OpenMP off) on the same 1 s stream"}
+        except Exception as e:   # the baseline is reported, never required
+            line["cpu_baseline"] = {"unavailable": str(e)[:200]}
+    print(json.dumps(line))
+    return 0
+
+
 def run_c5(args):
     """Continuous batching of subint requests from 12 resident jobs through
     gx_server (device-resident inputs, HBM budget), Poisson arrivals."""
@@ -567,7 +639,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gxcorr", choices=["gxcorr", "reference"])
-    ap.add_argument("--config", default="c3", choices=["c3", "c2", "c1", "c4", "c5"])
+    ap.add_argument("--config", default="c3", choices=["c3", "c2", "c1", "c4", "c5", "mux"])
     ap.add_argument("--c4-steps", type=int, default=1, help="timed batch steps per mode (C4)")
     ap.add_argument("--c5-slots", type=int, default=4)
     ap.add_argument("--c5-seconds", type=float, default=20.0)
@@ -588,6 +660,8 @@ def main():
         return run_c5(args)
     if args.config == "c4":
         return run_c4(args)
+    if args.config == "mux":
+        return run_mux(args)
 
     import torch
     from difx_b200.gxcorr import Correlator

@@ -12,12 +12,13 @@
 //      duplicates, the out-of-order window (nSort), the gap limit (nGap), the
 //      end-of-buffer back-off, the prototype header -- producing the source
 //      slot of every (output frame, thread) and the statistics.
-//   3. vmux_output_kernel: one thread per 32-bit output word writes the
-//      output headers and corner-turns the threads' samples: output time
-//      sample s holds, at slot k of P = nThread rounded up to a power of two,
-//      the B = bits x (1|2) x channels-per-thread bits of thread k's sample s
-//      (zeros in the slots past nThread).  Reads and writes are coalesced, so
-//      the kernel streams at HBM speed.
+//   3. vmux_turn_kernel<P, B>: one thread per (output frame, input payload
+//      word) writes the output headers and corner-turns the threads' samples:
+//      output time sample s holds, at slot k of P = nThread rounded up to a
+//      power of two, the B = bits x (1|2) bits of thread k's sample s (zeros
+//      in the slots past nThread); the transpose runs in registers with
+//      constant shifts, reads and writes are coalesced.  vmux_output_kernel
+//      (one thread per output word) covers the other (P, B).
 // A slot the reference would scan byte by byte (a frame that starts with the
 // fill pattern but does not end with it, or a header of another frame size,
 // channel count or bit depth) is skipped whole here; on frame-aligned input
@@ -95,11 +96,13 @@ __global__ void vmux_output_kernel(const uint8_t *__restrict__ src, uint8_t *__r
   const int32_t *sl = slot + (long long)f * nthreads;
   const int gpw = 32 / B;                        // B-bit groups per output word
   const long long g0 = (long long)(w - kHeader / 4) * gpw;
+  int lgP = 0;
+  while ((1 << lgP) < P) lgP++;
   uint32_t v = 0;
   for (int i = 0; i < gpw; i++) {
     const long long gi = g0 + i;
-    const long long s = gi / P;                  // time sample
-    const int k = (int)(gi % P);                 // thread slot within the sample
+    const long long s = gi >> lgP;               // time sample
+    const int k = (int)(gi & (P - 1));           // thread slot within the sample
     if (k >= nthreads) continue;                 // padding slot: zeros
     const int32_t sk = sl[k];
     if (sk < 0 && !copy_missing_from_src) continue;
@@ -110,6 +113,56 @@ __global__ void vmux_output_kernel(const uint8_t *__restrict__ src, uint8_t *__r
     v |= bits << (i * B);
   }
   out[w] = v;
+}
+
+// The same corner turn for compile-time P (threads rounded up to a power of
+// two) and B (bits of a thread's time sample): one thread per (output frame,
+// input word q) loads word q of each of the P threads' payloads (coalesced
+// across the warp) and writes the P output words those 32 / B samples make;
+// every shift is a constant after unrolling, so the transpose stays in
+// registers.  Header words are written by the threads of q < 8.
+template <int P, int B>
+__global__ void __launch_bounds__(256) vmux_turn_kernel(const uint8_t *__restrict__ src, uint8_t *__restrict__ dest,
+                                                        int nout, int ofb, int ifb, int nthreads,
+                                                        const int32_t *__restrict__ slot,
+                                                        const uint32_t *__restrict__ hdr, int copy_missing_from_src)
+{
+  constexpr int G = 32 / B;                       // samples per input word
+  constexpr uint32_t M = B == 32 ? 0xFFFFFFFFu : ((1u << B) - 1u);
+  const int qwords = (ifb - kHeader) / 4;        // input payload words
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)nout * qwords) return;
+  const int f = (int)(t / qwords), q = (int)(t % qwords);
+  uint32_t *out = reinterpret_cast<uint32_t *>(dest + (long long)f * ofb);
+  const uint32_t h0 = hdr[(long long)f * 8];
+  if (q < kHeader / 4) out[q] = hdr[(long long)f * 8 + q];
+  if (h0 >> 31) return;                          // filler frame: payload left as it is
+  const int32_t *sl = slot + (long long)f * nthreads;
+  uint32_t in[P];
+#pragma unroll
+  for (int k = 0; k < P; k++) {
+    in[k] = 0u;
+    if (k < nthreads) {
+      const int32_t sk = sl[k];
+      if (sk >= 0)
+        in[k] = reinterpret_cast<const uint32_t *>(src + (long long)sk * ifb + kHeader)[q];
+      else if (copy_missing_from_src)
+        in[k] = reinterpret_cast<const uint32_t *>(src)[q];   // absent thread: the reference reads the buffer start
+    }
+  }
+  uint32_t *o = out + kHeader / 4 + (long long)q * P;
+  // output group n = s * P + k (sample s of this word, thread k) sits at bits n * B
+#pragma unroll
+  for (int j = 0; j < P; j++) {                 // output word j of this input word
+    uint32_t v = 0u;
+#pragma unroll
+    for (int i = 0; i < G; i++) {
+      const int n = j * G + i;
+      const int s = n / P, k = n % P;
+      v |= ((in[k] >> (s * B)) & M) << (i * B);
+    }
+    o[j] = v;
+  }
 }
 
 }  // namespace
@@ -428,12 +481,32 @@ gx_status gx_vdifmux_run(gx_vdifmux *m, const uint8_t *src, long long src_bytes,
     if ((r = m->cuda(cudaMemcpyAsync(m->d_hdr, hdr.data(), sizeof(uint32_t) * 8 * nout, cudaMemcpyHostToDevice, st),
                      "cudaMemcpyAsync")) != GX_OK)
       return r;
-    const long long words = nout * (long long)(m->ofb / 4);
     const int tpb = 256;
-    vmux_output_kernel<<<(unsigned)((words + tpb - 1) / tpb), tpb, 0, st>>>(src, dest, (int)nout, m->ofb, ifb, nthr,
-                                                                           m->P, m->B, m->d_slot, m->d_hdr,
-                                                                           propagate ? 1 : 0);
-    if ((r = m->cuda(cudaGetLastError(), "vmux_output_kernel")) != GX_OK) return r;
+    const long long turns = nout * (long long)((ifb - kHeader) / 4);
+    const unsigned tgrid = (unsigned)((turns + tpb - 1) / tpb);
+    bool done = false;
+#define GX_TURN(PP, BB)                                                                                     \
+    if (!done && m->P == PP && m->B == BB) {                                                                \
+      vmux_turn_kernel<PP, BB><<<tgrid, tpb, 0, st>>>(src, dest, (int)nout, m->ofb, ifb, nthr, m->d_slot,   \
+                                                     m->d_hdr, propagate ? 1 : 0);                          \
+      done = true;                                                                                          \
+    }
+    // every payload has at least 8 words, so the threads q < 8 cover the header
+    if ((ifb - kHeader) / 4 >= kHeader / 4) {
+      GX_TURN(1, 1) GX_TURN(2, 1) GX_TURN(4, 1) GX_TURN(8, 1) GX_TURN(16, 1)
+      GX_TURN(1, 2) GX_TURN(2, 2) GX_TURN(4, 2) GX_TURN(8, 2) GX_TURN(16, 2) GX_TURN(32, 2)
+      GX_TURN(1, 4) GX_TURN(2, 4) GX_TURN(4, 4) GX_TURN(8, 4) GX_TURN(16, 4) GX_TURN(32, 4)
+      GX_TURN(1, 8) GX_TURN(2, 8) GX_TURN(4, 8) GX_TURN(8, 8) GX_TURN(16, 8) GX_TURN(32, 8)
+      GX_TURN(1, 16) GX_TURN(2, 16) GX_TURN(4, 16) GX_TURN(8, 16) GX_TURN(16, 16)
+    }
+#undef GX_TURN
+    if (!done) {   // other thread counts and sample widths: one thread per output word
+      const long long words = nout * (long long)(m->ofb / 4);
+      vmux_output_kernel<<<(unsigned)((words + tpb - 1) / tpb), tpb, 0, st>>>(src, dest, (int)nout, m->ofb, ifb, nthr,
+                                                                             m->P, m->B, m->d_slot, m->d_hdr,
+                                                                             propagate ? 1 : 0);
+    }
+    if ((r = m->cuda(cudaGetLastError(), "vmux corner turn")) != GX_OK) return r;
     if ((r = m->cuda(cudaStreamSynchronize(st), "cudaStreamSynchronize")) != GX_OK) return r;
   }
 

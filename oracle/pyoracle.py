@@ -180,13 +180,14 @@ def vmux_available() -> bool:
 
 def ref_vdifmux(src: bytes, dest_bytes: int, frame_bytes: int, fps: int, bits: int, thread_ids, nsort: int,
                 ngap: int, flags: int, start_frame: int = -1, dest_init: int = 0):
-    """The reference's vdifmux on host buffers: (output bytes, stats array of 22
-    values in the order of vdifmux_harness.c)."""
+    """The reference's vdifmux on host buffers: (output bytes, array of 23
+    values in the order of vdifmux_harness.c: statistics, return value, output
+    frame bytes, nanoseconds of the call)."""
     lib = C.CDLL(VMUX_LIB)
     dest = (C.c_ubyte * dest_bytes)(*([dest_init] * dest_bytes)) if dest_init else (C.c_ubyte * dest_bytes)()
     srcb = (C.c_ubyte * len(src)).from_buffer_copy(src)
     ids = (C.c_int * len(thread_ids))(*thread_ids)
-    out = (C.c_longlong * 22)()
+    out = (C.c_longlong * 23)()
     rv = lib.ref_vdifmux(dest, dest_bytes, srcb, len(src), frame_bytes, fps, bits, len(thread_ids), ids, nsort, ngap,
                          flags, C.c_longlong(start_frame), out)
     if rv < 0:

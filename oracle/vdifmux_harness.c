@@ -3,11 +3,12 @@
  * ctypes, so that the tests can compare the device multiplexer against it. */
 #include <stdint.h>
 #include <string.h>
+#include <time.h>
 #include "vdifio.h"
 
 /* out[0..19]: the statistics in the order of gx_vdifmux_stats (accumulated
  * over this one call), out[20]: vdifmux's return value, out[21]: output frame
- * bytes. */
+ * bytes, out[22]: nanoseconds the vdifmux call took. */
 int ref_vdifmux(unsigned char *dest, int dest_bytes, const unsigned char *src, int src_bytes, int frame_bytes,
                 int frames_per_second, int bits, int nthreads, const int *thread_ids, int nsort, int ngap,
                 int flags, long long start_frame, long long *out)
@@ -17,7 +18,11 @@ int ref_vdifmux(unsigned char *dest, int dest_bytes, const unsigned char *src, i
   int rv = configurevdifmux(&vm, frame_bytes, frames_per_second, bits, nthreads, thread_ids, nsort, ngap, flags);
   if (rv < 0) return rv;
   resetvdifmuxstatistics(&st);
+  struct timespec t0, t1;
+  clock_gettime(CLOCK_MONOTONIC, &t0);
   rv = vdifmux(dest, dest_bytes, src, src_bytes, &vm, start_frame, &st);
+  clock_gettime(CLOCK_MONOTONIC, &t1);
+  out[22] = (long long)(t1.tv_sec - t0.tv_sec) * 1000000000LL + (t1.tv_nsec - t0.tv_nsec);
   out[0] = st.nValidFrame;
   out[1] = st.nInvalidFrame;
   out[2] = st.nDiscardedFrame;
