@@ -519,7 +519,7 @@ def run_mux(args):
                        "input_bytes": len(src), "output_frames": st.output_frames,
                        "l2": "inputs larger than L2 (no flush)"},
             "wall_ms_per_step": wall_ms,
-            "roofline": {"kernel": "vmux_output_kernel + vmux_classify_kernel + host decisions", "bound": "hbm",
+            "roofline": {"kernel": "vmux_turn_kernel + vmux_classify_kernel + host decisions", "bound": "hbm",
                          "achieved": moved / (ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
                          "frac": moved / (ms * 1e-3) / 1e9 / hbm, "traffic": None,
                          "peak_source": "of measured" if "hbm_gbs" in peaks else "of fallback"},

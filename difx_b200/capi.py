@@ -30,7 +30,7 @@ STATUS_NAMES = {0: "GX_OK", 1: "GX_ERR_ARG", 2: "GX_ERR_UNSUPPORTED", 3: "GX_ERR
 
 class gx_freq_desc(C.Structure):
     _fields_ = [("freq_mhz", C.c_double), ("bw_mhz", C.c_double),
-                ("lower_sideband", C.c_int), ("nchan", C.c_int)]
+                ("lower_sideband", C.c_int), ("nchan", C.c_int), ("chans_to_average", C.c_int)]
 
 
 class gx_station_desc(C.Structure):
@@ -79,7 +79,7 @@ class gx_layout_info(C.Structure):
     _fields_ = [("result_length", C.c_int64), ("nfreqs", C.c_int), ("nbaselines", C.c_int),
                 ("nstations", C.c_int), ("blocks_per_send", C.c_int), ("xmac_stride", C.c_int),
                 ("array_stride", C.c_int), ("fftchannels", C.c_int), ("nchan", C.c_int), ("xstep", C.c_int),
-                ("block_chunk", C.c_int)]
+                ("block_chunk", C.c_int), ("chans_to_average", C.c_int)]
 
 
 class JobDesc:
@@ -115,6 +115,7 @@ def job_desc_from_spec(spec: JobSpec, xstep: int = GX_XSTEP_FP32, max_data_bytes
         f.bw_mhz = sb.bw_mhz
         f.lower_sideband = 1 if sb.sideband.upper().startswith("L") else 0
         f.nchan = sb.nchan
+        f.chans_to_average = spec.chans_to_avg
         freqs.append(f)
     npol = len(spec.pols)
     stations = []

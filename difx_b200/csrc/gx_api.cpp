@@ -49,7 +49,7 @@ static void free_all(gx_handle *h)
   if (h->device < 0) return;
   void *ptrs[] = {h->d_st, h->d_tw, h->d_spec, h->d_acc, h->d_results, h->d_spec1, h->d_w, h->d_wacc, h->d_w1,
                   h->d_pairs, h->d_prods, h->d_went, h->d_sub, h->d_bp, h->d_bp1, h->d_scale, h->d_tcprods,
-                  h->d_tcrows, h->d_err};
+                  h->d_tcrows, h->d_err, h->d_full, h->d_avgtab};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->h_err) cudaFreeHost(h->h_err);
@@ -240,47 +240,88 @@ static gx_status setup(gx_handle *h)
         return h->fail(GX_ERR_ARG, "POL PRODUCTS out of range");
     }
   const int bpa = h->maxprod > 2 ? 2 : 1;
-  h->blofs.assign(d.nfreqs * (nbl ? nbl : 1), -1);
-  h->bwofs.assign(d.nfreqs * (nbl ? nbl : 1), -1);
-  h->acofs.assign(d.nstations, 0);
-  h->acwofs.assign(d.nstations, 0);
-  long long idx = 0;
+  // CHANS TO AVG (core.cpp:1819-1869, mode.cpp:1376-1401): one averaging length
+  // per job, dividing the channel count
+  int avg = 1;
   for (int f = 0; f < d.nfreqs; f++) {
-    if (!freq_used(f)) continue;
-    for (int j = 0; j < nbl; j++) {
-      int lf = bl_localfreq(d.baselines[j], f);
-      if (lf < 0) continue;
-      h->blofs[f * nbl + j] = (int)idx;
-      idx += (long long)d.baselines[j].npolprod[lf] * d.freqs[f].nchan;
+    const int a = d.freqs[f].chans_to_average > 1 ? d.freqs[f].chans_to_average : 1;
+    if (f == 0) avg = a;
+    else if (a != avg) return h->fail(GX_ERR_UNSUPPORTED, "freqs with different CHANS TO AVG");
+    if (d.freqs[f].nchan % a) return h->fail(GX_ERR_UNSUPPORTED, "CHANS TO AVG does not divide NUM CHANNELS");
+  }
+  h->avg = avg;
+  // Core result layout for records of 1 / div of the channels: crosses by
+  // freq and baseline, baseline weights, autocorrelations, their weights
+  auto build = [&](int div, std::vector<int> &blofs, std::vector<int> &bwofs, std::vector<int> &acofs,
+                   std::vector<int> &acwofs) -> long long {
+    blofs.assign(d.nfreqs * (nbl ? nbl : 1), -1);
+    bwofs.assign(d.nfreqs * (nbl ? nbl : 1), -1);
+    acofs.assign(d.nstations, 0);
+    acwofs.assign(d.nstations, 0);
+    long long idx = 0;
+    for (int f = 0; f < d.nfreqs; f++) {
+      if (!freq_used(f)) continue;
+      for (int j = 0; j < nbl; j++) {
+        int lf = bl_localfreq(d.baselines[j], f);
+        if (lf < 0) continue;
+        blofs[f * nbl + j] = (int)idx;
+        idx += (long long)d.baselines[j].npolprod[lf] * (d.freqs[f].nchan / div);
+      }
+    }
+    for (int f = 0; f < d.nfreqs; f++) {
+      if (!freq_used(f)) continue;
+      for (int j = 0; j < nbl; j++) {
+        int lf = bl_localfreq(d.baselines[j], f);
+        if (lf < 0) continue;
+        bwofs[f * nbl + j] = (int)idx;
+        int np = d.baselines[j].npolprod[lf];
+        idx += np / 2 + np % 2;
+      }
+    }
+    for (int s = 0; s < d.nstations; s++) {
+      acofs[s] = (int)idx;
+      const gx_station_desc &x = d.stations[s];
+      for (int b = 0; b < x.nbands; b++)
+        if (freq_used(x.recfreq[x.band_localfreq[b]])) idx += (long long)bpa * (J.nchan / div);
+    }
+    for (int s = 0; s < d.nstations; s++) {
+      acwofs[s] = (int)idx;
+      const gx_station_desc &x = d.stations[s];
+      int add = 0;
+      for (int b = 0; b < x.nbands; b++)
+        if (freq_used(x.recfreq[x.band_localfreq[b]])) add += bpa;
+      add = (add + 1) / 2;
+      if (add == 0) add = 1;
+      idx += add;
+    }
+    return idx;
+  };
+  // the kernels fill the full-resolution array; the averaged one is the result
+  h->rl_full = build(1, h->blofs_full, h->bwofs_full, h->acofs_full, h->acwofs_full);
+  h->rl = build(avg, h->blofs, h->bwofs, h->acofs, h->acwofs);
+  h->avgtab.clear();
+  if (avg > 1) {
+    auto add = [&](long long src, long long dst, int n, int L) { h->avgtab.push_back(AvgEntry{src, dst, n, L}); };
+    for (int f = 0; f < d.nfreqs; f++)
+      for (int j = 0; j < nbl; j++) {
+        const int lf = bl_localfreq(d.baselines[j], f);
+        if (lf < 0 || h->blofs[f * nbl + j] < 0) continue;
+        const int nf = d.freqs[f].nchan, np = d.baselines[j].npolprod[lf];
+        for (int p = 0; p < np; p++)
+          add(h->blofs_full[f * nbl + j] + (long long)p * nf, h->blofs[f * nbl + j] + (long long)p * (nf / avg),
+              nf / avg, avg);
+        add(h->bwofs_full[f * nbl + j], h->bwofs[f * nbl + j], np / 2 + np % 2, 1);
+      }
+    for (int s = 0; s < d.nstations; s++) {
+      const long long end_full = s + 1 < d.nstations ? h->acofs_full[s + 1] : h->acwofs_full[0];
+      const int nr = (int)((end_full - h->acofs_full[s]) / J.nchan);
+      for (int r = 0; r < nr; r++)
+        add(h->acofs_full[s] + (long long)r * J.nchan, h->acofs[s] + (long long)r * (J.nchan / avg), J.nchan / avg,
+            avg);
+      const long long wend_full = s + 1 < d.nstations ? h->acwofs_full[s + 1] : h->rl_full;
+      add(h->acwofs_full[s], h->acwofs[s], (int)(wend_full - h->acwofs_full[s]), 1);
     }
   }
-  for (int f = 0; f < d.nfreqs; f++) {
-    if (!freq_used(f)) continue;
-    for (int j = 0; j < nbl; j++) {
-      int lf = bl_localfreq(d.baselines[j], f);
-      if (lf < 0) continue;
-      h->bwofs[f * nbl + j] = (int)idx;
-      int np = d.baselines[j].npolprod[lf];
-      idx += np / 2 + np % 2;
-    }
-  }
-  for (int s = 0; s < d.nstations; s++) {
-    h->acofs[s] = (int)idx;
-    const gx_station_desc &x = d.stations[s];
-    for (int b = 0; b < x.nbands; b++)
-      if (freq_used(x.recfreq[x.band_localfreq[b]])) idx += (long long)bpa * J.nchan;
-  }
-  for (int s = 0; s < d.nstations; s++) {
-    h->acwofs[s] = (int)idx;
-    const gx_station_desc &x = d.stations[s];
-    int add = 0;
-    for (int b = 0; b < x.nbands; b++)
-      if (freq_used(x.recfreq[x.band_localfreq[b]])) add += bpa;
-    add = (add + 1) / 2;
-    if (add == 0) add = 1;
-    idx += add;
-  }
-  h->rl = idx;
 
   // accumulator index of the Hermitian entry (a, b) of freq f
   const XmacShape &xs = h->xs;
@@ -327,9 +368,9 @@ static gx_status setup(gx_handle *h)
         if (b1 < 0 || b1 >= d.stations[B.ds1].nbands || b2 < 0 || b2 >= d.stations[B.ds2].nbands)
           return h->fail(GX_ERR_UNSUPPORTED, "baseline band index out of range (zoom bands are not implemented)");
         int a = h->band_input[B.ds1][b1], bb = h->band_input[B.ds2][b2];
-        add_prod(h->blofs[f * nbl + j] + (long long)p * J.nchan, f, a, bb);
+        add_prod(h->blofs_full[f * nbl + j] + (long long)p * J.nchan, f, a, bb);
         WeightEntry w{};
-        w.float_index = 2LL * h->bwofs[f * nbl + j] + p;
+        w.float_index = 2LL * h->bwofs_full[f * nbl + j] + p;
         w.source = d.nstations + j;
         h->wents.push_back(w);
       }
@@ -338,8 +379,8 @@ static gx_status setup(gx_handle *h)
   const bool writecross = d.write_autocorrs && h->maxprod > 2;
   for (int s = 0; s < d.nstations; s++) {
     const gx_station_desc &x = d.stations[s];
-    long long ro = h->acofs[s];
-    long long wo = 2LL * h->acwofs[s];
+    long long ro = h->acofs_full[s];
+    long long wo = 2LL * h->acwofs_full[s];
     std::vector<int> used;
     for (int b = 0; b < x.nbands; b++)
       if (freq_used(x.recfreq[x.band_localfreq[b]])) used.push_back(b);
@@ -551,6 +592,11 @@ static gx_status setup(gx_handle *h)
   if (!h->wents.empty())
     CKR(h, cudaMemcpy(h->d_went, h->wents.data(), sizeof(WeightEntry) * h->wents.size(), cudaMemcpyHostToDevice));
   CKR(h, h->dalloc(&h->d_results, sizeof(float2) * h->rl));
+  if (h->avg > 1) {
+    CKR(h, h->dalloc(&h->d_full, sizeof(float2) * h->rl_full));
+    CKR(h, h->dalloc(&h->d_avgtab, sizeof(AvgEntry) * h->avgtab.size()));
+    CKR(h, cudaMemcpy(h->d_avgtab, h->avgtab.data(), sizeof(AvgEntry) * h->avgtab.size(), cudaMemcpyHostToDevice));
+  }
   h->ctrlstride = 3 + J.flaglen;
   h->o_len = sizeof(SubintClock);
   h->o_ptr = h->o_len + sizeof(int64_t) * d.nstations;
@@ -597,6 +643,7 @@ gx_status plan_job(const gx_job_desc *desc, JobPlan *plan, std::string &err)
   h.jd.baselines = h.bl.data();
   gx_status s = setup(&h);
   if (s != GX_OK) { err = h.err; return s; }
+  if (h.avg > 1) { err = "channel averaging is not implemented by the allocation-free entry point"; return GX_ERR_UNSUPPORTED; }
   plan->J = h.J;
   plan->J.twiddle = nullptr;
   plan->maxnrf = h.maxnrf;
@@ -690,6 +737,7 @@ gx_status gx_get_layout(const gx_handle *h, gx_layout_info *info)
   info->nchan = h->J.nchan;
   info->xstep = h->xstep;
   info->block_chunk = h->chunk;
+  info->chans_to_average = h->avg;
   return GX_OK;
 }
 
@@ -808,17 +856,24 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
     h->launches += 3;
   }
   if ((r = mark(2, true)) != GX_OK) return r;
-  CKR(h, cudaMemsetAsync(dev_results, 0, sizeof(float2) * h->rl, st));
+  // with channel averaging the finalise fills the full-resolution array first
+  float2 *fin = h->avg > 1 ? h->d_full : dev_results;
+  CKR(h, cudaMemsetAsync(fin, 0, sizeof(float2) * h->rl_full, st));
   if (h->tc) {
     CKR(h, finalise_tc_launch(h->d_tcprods, h->d_tcrows, (int)h->tcrows.size(), acc4, d.nfreqs, J.nchan,
-                              J.ninputs, h->ks, dev_results, st));
+                              J.ninputs, h->ks, fin, st));
     CKR(h, finalise_launch(nullptr, 0, h->d_acc, h->ks, h->acc_slice, J.nchan, h->d_went, (int)h->wents.size(),
-                           h->d_wacc, dev_results, st));
+                           h->d_wacc, fin, st));
   } else {
     CKR(h, finalise_launch(h->d_prods, (int)h->prods.size(), h->d_acc, h->ks, h->acc_slice, J.nchan, h->d_went,
-                           (int)h->wents.size(), h->d_wacc, dev_results, st));
+                           (int)h->wents.size(), h->d_wacc, fin, st));
   }
   h->launches += (h->prods.empty() ? 0 : 1) + (h->wents.empty() ? 0 : 1);
+  if (h->avg > 1) {
+    CKR(h, cudaMemsetAsync(dev_results, 0, sizeof(float2) * h->rl, st));
+    CKR(h, average_launch(h->d_avgtab, (int)h->avgtab.size(), h->d_full, dev_results, st));
+    h->launches += 1;
+  }
   if ((r = mark(2, false)) != GX_OK) return r;
   CKR(h, cudaMemcpyAsync(h->h_err + k, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
   return GX_OK;

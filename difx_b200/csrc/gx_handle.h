@@ -26,8 +26,14 @@ struct gx_handle {
   gx::DevJob J{};
   int maxnrf = 1, nslots = 1, chunk = 0, ks = 1, xmac_stride = 0, maxprod = 0;
   gx::XmacShape xs{};
-  long long rl = 0;
+  long long rl = 0;                          // result length (averaged layout)
   std::vector<int> blofs, bwofs, acofs, acwofs;
+  int avg = 1;                               // CHANS TO AVG
+  long long rl_full = 0;                     // the layout at full resolution (the kernels' target)
+  std::vector<int> blofs_full, bwofs_full, acofs_full, acwofs_full;
+  std::vector<gx::AvgEntry> avgtab;          // full -> averaged records
+  gx::AvgEntry *d_avgtab = nullptr;
+  float2 *d_full = nullptr;
   std::vector<std::vector<int>> band_input;  // [station][band]
   std::vector<gx::ProdEntry> prods;
   std::vector<gx::TcProdEntry> tcprods;   // sorted by (freq, a)

@@ -267,8 +267,7 @@ InputJob *read_input_job(const char *inputfile, std::string &err)
     f.lower_sideband = (sb == "L" || sb == "l" || sb == "LOWER" || sb == "lower") ? 1 : 0;
     if (in.peek("RX NAME ")) NEED(in, "RX NAME ", v);
     NEED(in, "NUM CHANNELS ", v); f.nchan = atoi(v.c_str());
-    NEED(in, "CHANS TO AVG ", v);
-    if (atoi(v.c_str()) != 1) { err = "channel averaging is not implemented"; return nullptr; }
+    NEED(in, "CHANS TO AVG ", v); f.chans_to_average = atoi(v.c_str());
     NEED(in, "OVERSAMPLE FAC. ", v);
     NEED(in, "DECIMATION FAC. ", v);
     if (atoi(v.c_str()) != 1) { err = "decimation is not implemented"; return nullptr; }

@@ -164,7 +164,7 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
   if (scan < 0 || scan >= (int)model.scans.size()) return GX_OK;               // past the last scan
   const int scanstart = (int)model.scan_start_sec(scan);
   if (sec + scanstart >= M.execute_seconds || v->nsub == 0) return GX_OK;      // writedata's early exits
-  const int nbl = d.nbaselines, N = h->J.nchan;
+  const int nbl = d.nbaselines, N = h->J.nchan / h->avg;   // output channels per record
 
   // weights: the baseline-weight and autocorrelation-weight regions of the summed array
   std::vector<float> fr(2 * (size_t)h->rl);
@@ -184,7 +184,7 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
   // Visibility::changeConfig (visibility.cpp:1314-1316)
   const double meansub = M.int_time / (((double)d.subint_ns) / 1000000000.0);
   const double ffts = meansub * h->J.blocks_per_send;
-  const float chanfactor = (float)(h->J.blocks_per_send * 2 * N * 1);   // blocks per send * 2 * nchan * chanavg
+  const float chanfactor = (float)(h->J.blocks_per_send * 2 * N * h->avg);   // blocks per send * 2 * nchan * chanavg
   auto weight_and_scale = [&](long long widx, float &w, float &scale) {
     w = (float)(fr[widx] / ffts);
     scale = w > 0.0f ? (float)(1.0 / ((double)w * meansub * (double)chanfactor)) : 0.0f;

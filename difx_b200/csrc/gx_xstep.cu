@@ -249,4 +249,29 @@ cudaError_t finalise_launch(const ProdEntry *prods, int nprods, const float2 *ac
   return cudaGetLastError();
 }
 
+// Channel averaging of the finished result array (Mode::averageFrequency,
+// mode.cpp:1376-1401, for autocorrelations; Core's averaged copy,
+// core.cpp:1819-1869, for cross products): one CTA per record.
+__global__ void average_kernel(const AvgEntry *__restrict__ tab, const float2 *__restrict__ full,
+                               float2 *__restrict__ out)
+{
+  const AvgEntry e = tab[blockIdx.x];
+  for (int c = threadIdx.x; c < e.n; c += blockDim.x) {
+    const float2 *p = full + e.src + (long long)c * e.L;
+    float2 acc = p[0];
+    for (int i = 1; i < e.L; i++) {
+      acc.x += p[i].x;
+      acc.y += p[i].y;
+    }
+    out[e.dst + c] = e.L == 1 ? acc : make_float2(acc.x / (float)e.L, acc.y / (float)e.L);   // the mean
+  }
+}
+
+cudaError_t average_launch(const AvgEntry *tab, int nent, const float2 *full, float2 *out, cudaStream_t st)
+{
+  if (nent <= 0) return cudaSuccess;
+  average_kernel<<<nent, 128, 0, st>>>(tab, full, out);
+  return cudaGetLastError();
+}
+
 }  // namespace gx

@@ -58,6 +58,13 @@ cudaError_t xmac_tc_launch(const float2 *spec, int nblk, int N, int nfreqs, int 
                            const float *scale, float4 *acc, int accumulate, int *err, cudaStream_t st);
 cudaError_t finalise_tc_launch(const TcProdEntry *prods, const TcRowEntry *rows, int nrows, const float4 *acc,
                                int nfreqs, int N, int ninputs, int ks, float2 *results, cudaStream_t st);
+// One record of channel averaging (CHANS TO AVG): n output values at dst, each
+// the mean of L consecutive values from src (L = 1: a copy, for weights).
+struct AvgEntry {
+  long long src, dst;
+  int n, L;
+};
+cudaError_t average_launch(const AvgEntry *tab, int nent, const float2 *full, float2 *out, cudaStream_t st);
 constexpr int kTcInputs = 128;   // inputs per frequency of the tensor-core X-step (the MMA M)
 
 cudaError_t finalise_launch(const ProdEntry *prods, int nprods, const float2 *acc, int ks, size_t ks_stride, int N,

@@ -74,6 +74,7 @@ class JobSpec:
     clock_rate: Sequence[float] = ()  # per-station clock rate (us/s); default 0
     uvshift_interval_ns: int = 2_000_000_000
     ac_avg_interval_ns: int = 2_000_000_000
+    chans_to_avg: int = 1             # CHANS TO AVG of every freq (output channels = nchan / this)
     poly_interval_s: int = 120
     station_names: Sequence[str] = ()
     data_files: Sequence[str] = ()
@@ -280,7 +281,7 @@ def write_job(spec: JobSpec, outdir: str) -> dict:
         L.append(_kv(f"BW (MHZ) {i}", f"{sb.bw_mhz:.11f}"))
         L.append(_kv(f"SIDEBAND {i}", sb.sideband))
         L.append(_kv(f"NUM CHANNELS {i}", sb.nchan))
-        L.append(_kv(f"CHANS TO AVG {i}", 1))
+        L.append(_kv(f"CHANS TO AVG {i}", spec.chans_to_avg))
         L.append(_kv(f"OVERSAMPLE FAC. {i}", 1))
         L.append(_kv(f"DECIMATION FAC. {i}", 1))
         L.append(_kv(f"PHASE CALS {i} OUT", 0))

@@ -79,6 +79,8 @@ typedef struct gx_freq_desc {
   double bw_mhz;           /* BW (MHZ) */
   int lower_sideband;      /* SIDEBAND L */
   int nchan;               /* NUM CHANNELS */
+  int chans_to_average;    /* CHANS TO AVG: output channels = nchan / this (0 or 1: none); the
+                              same for every freq of a job, dividing nchan */
 } gx_freq_desc;
 
 /* One datastream (DATASTREAM TABLE, configuration.cpp:1397-1850).  Only
@@ -157,6 +159,7 @@ typedef struct gx_layout_info {
   int nchan;
   int xstep;               /* X-step form in use (GX_XSTEP_AUTO resolved) */
   int block_chunk;         /* FFT blocks per device pass in use */
+  int chans_to_average;    /* output channels per record = nchan / chans_to_average */
 } gx_layout_info;
 
 /* device < 0 opens a host-only handle: layout, offsets and delay-model

@@ -125,8 +125,10 @@ def record_metric(a: np.ndarray, b: np.ndarray, offsets, nchan: int) -> float:
     return worst
 
 
-def record_offsets(jd: capi.JobDesc, blofs, acofs, spec: JobSpec):
-    """Start offsets of every cross and auto record (one per polproduct / band)."""
+def record_offsets(jd: capi.JobDesc, blofs, acofs, spec: JobSpec, nchan: int = 0):
+    """Start offsets of every cross and auto record (one per polproduct / band)
+    of records of nchan channels (default: the job's output channels)."""
+    nchan = nchan or spec.nchan // spec.chans_to_avg
     out = []
     d = jd.desc
     nbl = d.nbaselines
@@ -137,9 +139,9 @@ def record_offsets(jd: capi.JobDesc, blofs, acofs, spec: JobSpec):
                 continue
             lf = [d.baselines[j].freq[k] for k in range(d.baselines[j].nfreqs)].index(f)
             for p in range(d.baselines[j].npolprod[lf]):
-                out.append(o + p * spec.nchan)
+                out.append(o + p * nchan)
     nauto = spec.nbands * (2 if len(spec.pols) > 1 and spec.full_pol else 1)
     for s in range(d.nstations):
         for b in range(nauto):
-            out.append(acofs[s] + b * spec.nchan)
+            out.append(acofs[s] + b * nchan)
     return out

@@ -39,10 +39,10 @@ def _weight_slots(jd, bw, acw, spec):
     return np.array(idx)
 
 
-def _compare(gpu, ref, jd, spec, orc):
-    rl, bl, bw, ac, acw = orc.layout(jd)
+def _compare(gpu, ref, jd, spec, orc, layout=None):
+    rl, bl, bw, ac, acw = layout if layout is not None else orc.layout(jd)
     offs = jobs.record_offsets(jd, bl, ac, spec)
-    m = jobs.record_metric(gpu, ref, offs, spec.nchan)
+    m = jobs.record_metric(gpu, ref, offs, spec.nchan // spec.chans_to_avg)
     wi = _weight_slots(jd, bw, acw, spec)
     gf = gpu.view(np.float32) if gpu.dtype == np.complex64 else gpu.astype(np.complex64).view(np.float32)
     rf = ref.astype(np.complex64).view(np.float32)
@@ -216,3 +216,50 @@ def test_gpu_async_pipeline_matches_sync(gx):
     assert ei.value.status == 8
     np.testing.assert_array_equal(c.subint(prep.sds[1]), want[1])   # blocking calls work again
     c.close()
+
+
+AVG_CASES = {
+    "c1_avg4": lambda: (jobs.spec_c1(name="c1avg", seed=61, chans_to_avg=4), dict(invalid_frac=0.03)),
+    "cplx8_avg8": lambda: (jobs.spec_cplx8(name="cx8avg", seed=62, chans_to_avg=8), dict(invalid_frac=0.03)),
+}
+
+
+@pytest.mark.skipif(not pyoracle.reference_available(), reason="reference harness not built")
+@pytest.mark.parametrize("case", sorted(AVG_CASES))
+def test_gpu_channel_averaging_matches_reference(case, gx, oracle_lib):
+    """CHANS TO AVG (core.cpp:1819-1869, mode.cpp:1376-1401): the averaged
+    Core result array against the compiled reference reading the same .input,
+    and against the full-resolution oracle averaged here."""
+    spec, kw = AVG_CASES[case]()
+    L = spec.chans_to_avg
+    prep = jobs.prepare(spec, [100_000_000], **kw)
+    c = gx.Correlator.from_desc(prep.jd)
+    assert c.info.chans_to_average == L
+    g = c.subint(prep.sds[0])
+    r = jobs.reference_for(prep.paths["input"]).process(prep.subs[0])
+    assert g.shape == r.shape
+    m, wrel = _compare(g, r, prep.jd, spec, oracle_lib, layout=c.offsets())
+    assert m < REC_TOL and wrel < W_TOL, (m, wrel)
+    # the oracle at full resolution, averaged over groups of L channels
+    full_spec = jobs.JobSpec(**{**spec.__dict__, "chans_to_avg": 1})
+    jd_full = capi_job_desc(full_spec)
+    o = oracle_lib.subint(jd_full, prep.sds[0], _params(oracle_lib, full_spec))
+    rl_f, bl_f, bw_f, ac_f, acw_f = oracle_lib.layout(jd_full)
+    _, bl, bw, ac, acw = c.offsets()
+    full_offs = jobs.record_offsets(jd_full, bl_f, ac_f, full_spec)
+    out_offs = jobs.record_offsets(prep.jd, bl, ac, spec)
+    n = spec.nchan // L
+    worst = 0.0
+    for fo, oo in zip(full_offs, out_offs):
+        want = o[fo:fo + spec.nchan].reshape(n, L).mean(axis=1)
+        got = g[oo:oo + n]
+        den = np.mean(np.abs(want))
+        if den > 0:
+            worst = max(worst, float(np.mean(np.abs(got - want)) / den))
+    assert worst < REC_TOL, worst
+    c.close()
+
+
+def capi_job_desc(spec):
+    from difx_b200 import capi
+    return capi.job_desc_from_spec(spec)

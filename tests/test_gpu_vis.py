@@ -25,6 +25,7 @@ CASES = {
     "c1": lambda: jobs.spec_c1(name="gvis", seed=17, int_time=0.016),
     "lsb_3st": lambda: jobs.spec_lsb(name="gvisl", seed=19, int_time=0.008),
     "cplx8": lambda: jobs.spec_cplx8(name="gvisc", seed=23, int_time=0.008192),
+    "c1_avg4": lambda: jobs.spec_c1(name="gvisa", seed=29, int_time=0.016, chans_to_avg=4),
 }
 
 
@@ -75,7 +76,7 @@ def test_gx_vis_bytes_match_reference_visibility(case, tmp_path):
     b = np.fromfile(_file(theirs), np.uint8)
     assert a.size == b.size, (a.size, b.size)
     assert np.array_equal(a, b)
-    assert len(swin.read_records(_file(ours), spec.nchan)) == n
+    assert len(swin.read_records(_file(ours), spec.nchan // spec.chans_to_avg)) == n
 
 
 def test_gx_vis_end_to_end_matches_reference(tmp_path):
@@ -87,8 +88,8 @@ def test_gx_vis_end_to_end_matches_reference(tmp_path):
     ref = jobs.reference_for(prep.paths["input"])
     theirs = str(tmp_path / "ref.difx")
     ref.vis_write([ref.process(si) for si in prep.subs], 0, 0, 100_000_000, theirs)
-    ra = swin.read_records(_file(ours), spec.nchan)
-    rb = swin.read_records(_file(theirs), spec.nchan)
+    ra = swin.read_records(_file(ours), spec.nchan // spec.chans_to_avg)
+    rb = swin.read_records(_file(theirs), spec.nchan // spec.chans_to_avg)
     assert len(ra) == len(rb)
     worst = 0.0
     for (ha, da), (hb, db) in zip(ra, rb):
