@@ -19,12 +19,15 @@
 // Data path per CTA: the spectra spec[freq][block][input][chan] (float2, as the
 // F-step writes them) are read as a 4-D FP32 tensor; one TMA tile load (no
 // multicast) per 16 blocks fetches the 4 floats of the CTA's channel pair for
-// all 128 inputs ([block][input][16 bytes], blocks past the chunk read as
-// zeros) into a 4-stage FP32 ring; all threads scale each value by a power
-// of two per (input, channel), round it to FP16 and store it, transposed to
-// K-major, into the canonical no-swizzle core-matrix layout of the MMA operand
-// [Xi ; Xr] (256 rows x 16 blocks); one thread issues the MMAs and commits them
-// to an mbarrier that frees the operand stage.  In the split form the FP16
+// all 128 inputs ([block][input][16 bytes], blocks past the chunk and rows
+// past the job's inputs read as zeros) into a 4-stage FP32 ring.  The CTA's
+// warps have roles joined only by mbarriers: one lane of warp 0 issues the
+// tile loads as stages free up; eight converter warps scale each value by a
+// power of two per (input, channel), round it to FP16 and store it, transposed
+// to K-major, into the canonical no-swizzle core-matrix layout of the MMA
+// operand [Xi ; Xr] (256 rows x 16 blocks) of a 2-stage operand ring; one lane
+// of warp 1 issues the MMAs of a stage and commits them to the mbarrier that
+// frees it.  Loads, conversion and MMAs of neighbouring tiles overlap.  In the split form the FP16
 // remainder lo = fp16(x*s - hi) is kept too and the products hi*hi + hi*lo +
 // lo*hi are accumulated (lo*lo, below 2^-22 relative, is dropped).
 //
@@ -53,7 +56,7 @@ constexpr int kNI = 128;                     // inputs per frequency = MMA M
 constexpr int kKT = 16;                      // FFT blocks per K-tile = one MMA K step for FP16
 constexpr int kStages = 4;                   // FP32 staging ring depth (tile loads in flight)
 constexpr int kOpStages = 2;                 // FP16 operand stages
-constexpr int kThreads = 256;
+constexpr int kThreads = 320;                // 1 load warp, 1 MMA warp, 8 converter warps
 constexpr uint32_t kTmemCols = 512;          // 2 channels x (128 Re + 128 P) FP32 columns
 constexpr uint32_t kRowBytes = kNI * 16;     // one block of a channel pair: 128 inputs x 2 channels x float2
 constexpr uint32_t kStageBytes = kKT * kRowBytes;         // 32 KB
@@ -220,6 +223,20 @@ __device__ __forceinline__ void split2(float a, float b, uint32_t &hi, uint32_t 
   lo = *reinterpret_cast<const uint32_t *>(&l);
 }
 
+__device__ __forceinline__ void mbar_arrive(uint32_t bar)
+{
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// Warp roles: warp 0 lane 0 issues the tile loads, warp 1 lane 0 issues the
+// MMAs, warps 2..9 (kConvThreads threads) convert the staged FP32 tiles to FP16
+// operands and later run the epilogue.  The roles hand stages to each other
+// through mbarriers only, so a tile's load, conversion and MMAs overlap those
+// of its neighbours.
+constexpr int kConvThreads = 256;
+constexpr int kConvWarp0 = 2;
+constexpr int kNumBars = 2 * kStages + 2 * kOpStages + 1;   // full, empty, opfull, opempty, done
+
 template <bool HILO>
 __global__ void __launch_bounds__(kThreads, 1)
 xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, int nfreqs, int ks, int ninputs,
@@ -230,8 +247,10 @@ xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, i
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned char *staging = smem;
   unsigned char *ops = smem + kStages * kStageBytes;
-  uint64_t *bars = reinterpret_cast<uint64_t *>(ops + kOpStages * kOpStageBytes);  // [kStages] full, [kOpStages] MMA done
-  uint32_t *s_tmem = reinterpret_cast<uint32_t *>(bars + kStages + kOpStages);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(ops + kOpStages * kOpStageBytes);
+  uint64_t *full = bars, *empty = bars + kStages, *opfull = bars + 2 * kStages;
+  uint64_t *opempty = opfull + kOpStages, *done = opempty + kOpStages;
+  uint32_t *s_tmem = reinterpret_cast<uint32_t *>(bars + kNumBars);
   volatile int *s_abort = reinterpret_cast<volatile int *>(s_tmem + 1);
 
   const int p = blockIdx.x, f = blockIdx.y, z = blockIdx.z;
@@ -240,9 +259,18 @@ xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, i
   const int ntile_all = (nblk + kKT - 1) / kKT;
   const int t0 = (int)((long long)ntile_all * z / ks);
   const int nt = (int)((long long)ntile_all * (z + 1) / ks) - t0;
+  const int nconv_warps = kConvThreads / 32;
 
   if (tid == 0) {
-    for (int i = 0; i < kStages + kOpStages; i++) mbar_init(smem_u32(bars + i), 1);
+    for (int i = 0; i < kStages; i++) {
+      mbar_init(smem_u32(full + i), 1);
+      mbar_init(smem_u32(empty + i), nconv_warps);
+    }
+    for (int i = 0; i < kOpStages; i++) {
+      mbar_init(smem_u32(opfull + i), nconv_warps);
+      mbar_init(smem_u32(opempty + i), 1);
+    }
+    mbar_init(smem_u32(done), 1);
     *s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -254,36 +282,71 @@ xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, i
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *s_tmem;
-
-  // conversion role: row r of the operand, block group g (blocks 8g .. 8g+7 of a tile)
-  const int r = tid & (kNI - 1), g = tid >> 7;
-  const float s0 = scale[((size_t)f * kNI + r) * N + 2 * p];
-  const float s1 = scale[((size_t)f * kNI + r) * N + 2 * p + 1];
-  const uint32_t row_off = (uint32_t)(r >> 3) * kSBO + (uint32_t)g * kLBO + (uint32_t)(r & 7) * 16;
-
-  // tile u of this slice into staging stage u % kStages (thread 0 only): channels 2p, 2p+1
-  // (4 floats) of all 128 rows of kKT blocks; blocks past the chunk read as zeros
-  auto issue = [&](int u) {
-    const int st = u % kStages;
-    const int kb0 = (t0 + u) * kKT;
-    const uint32_t bar = smem_u32(bars + st);
-    mbar_expect_tx(bar, kStageBytes);
-    tma_load_4d(smem_u32(staging + st * kStageBytes), &spec_map, 4 * p, 0, kb0, f, bar);
+  auto abort_with = [&](int code) {
+    *s_abort = 1;
+    atomicExch(err, code);
   };
 
-  int issued = 0, t = 0;
-  if (tid == 0)
-    for (; issued < nt && issued < kStages - 1; issued++) issue(issued);
-
-  for (; t < nt; t++) {
-    if (tid == 0 && issued < nt) issue(issued++);
-    const int st = t % kStages, o = t % kOpStages;
-    bool good = mbar_wait(smem_u32(bars + st), (uint32_t)(t / kStages) & 1u);
-    if (good && t >= kOpStages) good = mbar_wait(smem_u32(bars + kStages + o), (uint32_t)(t / kOpStages - 1) & 1u);
-    if (!good) {
-      *s_abort = 1;
-      atomicExch(err, 1);
-    } else {
+  int issued = 0, mmas = 0;
+  if (warp == 0 && lane == 0) {
+    // ---- producer: tile u into stage u % kStages once its previous tile was converted
+    for (int u = 0; u < nt; u++) {
+      if (*s_abort) break;
+      const int st = u % kStages;
+      if (u >= kStages && !mbar_wait(smem_u32(empty + st), (uint32_t)(u / kStages - 1) & 1u)) {
+        abort_with(3);
+        break;
+      }
+      const uint32_t bar = smem_u32(full + st);
+      mbar_expect_tx(bar, kStageBytes);
+      tma_load_4d(smem_u32(staging + st * kStageBytes), &spec_map, 4 * p, 0, (t0 + u) * kKT, f, bar);
+      issued = u + 1;
+    }
+  } else if (warp == 1 && lane == 0) {
+    // ---- MMA issuer: operand stage t % kOpStages once converted; its commit frees the stage
+    for (int t = 0; t < nt; t++) {
+      if (*s_abort) break;
+      const int o = t % kOpStages;
+      if (!mbar_wait(smem_u32(opfull + o), (uint32_t)(t / kOpStages) & 1u)) {
+        abort_with(4);
+        break;
+      }
+      tc_fence_after();
+      const uint32_t opb = smem_u32(ops + o * kOpStageBytes);
+#pragma unroll
+      for (int e = 0; e < 2; e++) {
+        const uint32_t d = tmem + (uint32_t)e * 256u;
+        const uint32_t hb = opb + (uint32_t)e * kOpChanBytes;
+        const uint64_t xi = smem_desc(hb), xr = smem_desc(hb + kXrOffset);
+        mma_f16(d, xi, xi, idesc_f16(256), t > 0 ? 1u : 0u);
+        mma_f16(d, xr, xr, idesc_f16(128), 1u);
+        if (HILO) {
+          const uint32_t lb = opb + (2u + (uint32_t)e) * kOpChanBytes;
+          const uint64_t li = smem_desc(lb), lr = smem_desc(lb + kXrOffset);
+          mma_f16(d, xi, li, idesc_f16(256), 1u);
+          mma_f16(d, li, xi, idesc_f16(256), 1u);
+          mma_f16(d, xr, lr, idesc_f16(128), 1u);
+          mma_f16(d, lr, xr, idesc_f16(128), 1u);
+        }
+      }
+      mma_commit(smem_u32(opempty + o));
+      mmas = t + 1;
+    }
+    if (!*s_abort && mmas == nt && nt > 0) mma_commit(smem_u32(done));
+  } else if (warp >= kConvWarp0) {
+    // ---- converters: row r, block group g of each tile
+    const int ct = tid - kConvWarp0 * 32;
+    const int r = ct & (kNI - 1), g = ct >> 7;
+    const float s0 = scale[((size_t)f * kNI + r) * N + 2 * p];
+    const float s1 = scale[((size_t)f * kNI + r) * N + 2 * p + 1];
+    const uint32_t row_off = (uint32_t)(r >> 3) * kSBO + (uint32_t)g * kLBO + (uint32_t)(r & 7) * 16;
+    for (int t = 0; t < nt; t++) {
+      if (*s_abort) break;
+      const int st = t % kStages, o = t % kOpStages;
+      if (!mbar_wait(smem_u32(full + st), (uint32_t)(t / kStages) & 1u)) {
+        abort_with(1);
+        break;
+      }
       const int kv = min(kKT, nblk - (t0 + t) * kKT);
       const float4 *stg = reinterpret_cast<const float4 *>(staging + st * kStageBytes);
       uint32_t re0[4], im0[4], re1[4], im1[4];
@@ -306,6 +369,12 @@ xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, i
           im1[j] = pack_half2(a.w * s1, b.w * s1);
         }
       }
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(empty + st));   // the staging stage may be reloaded
+      if (t >= kOpStages && !mbar_wait(smem_u32(opempty + o), (uint32_t)(t / kOpStages - 1) & 1u)) {
+        abort_with(2);
+        break;
+      }
       unsigned char *op = ops + o * kOpStageBytes;
       // channel e, part q at op + (q * 2 + e) * kOpChanBytes; Xi rows 0..127, Xr rows 128..255
       *reinterpret_cast<uint4 *>(op + row_off) = make_uint4(im0[0], im0[1], im0[2], im0[3]);
@@ -320,47 +389,32 @@ xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, i
         *reinterpret_cast<uint4 *>(lo + kOpChanBytes + row_off + kXrOffset) =
             make_uint4(lre1[0], lre1[1], lre1[2], lre1[3]);
       }
-    }
-    fence_proxy_async_smem();
-    __syncthreads();
-    if (*s_abort) break;
-    if (tid == 0) {
-      tc_fence_after();
-      const uint32_t opb = smem_u32(ops + o * kOpStageBytes);
-#pragma unroll
-      for (int e = 0; e < 2; e++) {
-        const uint32_t d = tmem + (uint32_t)e * 256u;
-        const uint32_t hb = opb + (uint32_t)e * kOpChanBytes;
-        const uint64_t xi = smem_desc(hb), xr = smem_desc(hb + kXrOffset);
-        mma_f16(d, xi, xi, idesc_f16(256), t > 0 ? 1u : 0u);
-        mma_f16(d, xr, xr, idesc_f16(128), 1u);
-        if (HILO) {
-          const uint32_t lb = opb + (2u + (uint32_t)e) * kOpChanBytes;
-          const uint64_t li = smem_desc(lb), lr = smem_desc(lb + kXrOffset);
-          mma_f16(d, xi, li, idesc_f16(256), 1u);
-          mma_f16(d, li, xi, idesc_f16(256), 1u);
-          mma_f16(d, xr, lr, idesc_f16(128), 1u);
-          mma_f16(d, lr, xr, idesc_f16(128), 1u);
-        }
-      }
-      mma_commit(smem_u32(bars + kStages + o));
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(opfull + o));   // the operand stage may be multiplied
     }
   }
-
+  __syncthreads();
   // all MMAs of the slice have completed once the last commit has arrived
-  if (!*s_abort && nt > 0) {
-    const int tl = nt - 1;
-    if (!mbar_wait(smem_u32(bars + kStages + tl % kOpStages), (uint32_t)(tl / kOpStages) & 1u)) {
-      *s_abort = 1;
-      atomicExch(err, 2);
-    }
+  if (!*s_abort && nt > 0 && tid == 0 && !mbar_wait(smem_u32(done), 0u)) abort_with(5);
+  if (*s_abort) {
+    // drain: the loads this CTA issued, then the MMAs it committed (bounded)
+    if (warp == 0 && lane == 0)
+      for (int st = 0; st < kStages && st < issued; st++) {
+        const int ulast = st + ((issued - 1 - st) / kStages) * kStages;
+        mbar_wait(smem_u32(full + st), (uint32_t)(ulast / kStages) & 1u);
+      }
+    if (warp == 1 && lane == 0 && mmas > 0)
+      mbar_wait(smem_u32(opempty + (mmas - 1) % kOpStages), (uint32_t)((mmas - 1) / kOpStages) & 1u);
   }
   __syncthreads();
   tc_fence_after();
 
+  const bool ep = warp >= kConvWarp0;   // the converter warps run the epilogue
+  const int ct = tid - kConvWarp0 * 32;
   if (!*s_abort && !(nt == 0 && accumulate)) {   // an empty slice adds nothing
-    // warp w reads lanes 32 (w % 4) .. +31, i.e. row a of both accumulators
-    const int q = warp & 3, h = warp >> 2;
+    // a warp reads tensor-memory lanes 32 (warp % 4) .. +31 (its quadrant), i.e. row a of both accumulators
+    const int q = warp & 3, h = (warp - kConvWarp0) >> 2;
     const int a = 32 * q + lane;
     const uint32_t lane_addr = tmem + ((uint32_t)(32 * q) << 16);
     float4 *oblk = acc + (((size_t)z * nfreqs + f) * NP + p) * kNI * kNI;   // [a][b]
@@ -369,7 +423,9 @@ xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, i
     float *sP = reinterpret_cast<float *>(staging);                 // [2][128][kPRow]
     float *sInv = sP + 2 * kNI * kPRow;                              // [2][128]
     float4 *sV = reinterpret_cast<float4 *>(sInv + 2 * kNI);         // [128][kVRow]
-    if (nt > 0) {
+    const float s0 = ep ? scale[((size_t)f * kNI + a) * N + 2 * p] : 1.0f;
+    const float s1 = ep ? scale[((size_t)f * kNI + a) * N + 2 * p + 1] : 1.0f;
+    if (nt > 0 && ep) {
       if (h == 1) {
 #pragma unroll 1
         for (int cb = 0; cb < kNI / 16; cb++) {
@@ -394,50 +450,50 @@ xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, i
     const int ncb = (ninputs + kVCols - 1) / kVCols;
 #pragma unroll 1
     for (int cb = 0; cb < ncb; cb++) {
-      // thread (a, h) forms columns b = 8 cb + 4 h + i of row a
-      const int b0 = cb * kVCols + h * 4;
-      float r0[4] = {0.f, 0.f, 0.f, 0.f}, r1[4] = {0.f, 0.f, 0.f, 0.f};
-      if (nt > 0) {
-        tmem_ld4(lane_addr + (uint32_t)b0, r0);
-        tmem_ld4(lane_addr + 256u + (uint32_t)b0, r1);
-        tmem_ld_wait();
-      }
-#pragma unroll
-      for (int i = 0; i < 4; i++) {
-        const int b = b0 + i;
-        float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (ep) {
+        // thread (a, h) forms columns b = 8 cb + 4 h + i of row a
+        const int b0 = cb * kVCols + h * 4;
+        float r0[4] = {0.f, 0.f, 0.f, 0.f}, r1[4] = {0.f, 0.f, 0.f, 0.f};
         if (nt > 0) {
-          const float i0 = ia0 * sInv[b], i1 = ia1 * sInv[kNI + b];
-          const float im0 = sP[a * kPRow + b] - sP[b * kPRow + a];
-          const float im1 = sP[(kNI + a) * kPRow + b] - sP[(kNI + b) * kPRow + a];
-          w = make_float4(r0[i] * i0, im0 * i0, r1[i] * i1, im1 * i1);
+          tmem_ld4(lane_addr + (uint32_t)b0, r0);
+          tmem_ld4(lane_addr + 256u + (uint32_t)b0, r1);
+          tmem_ld_wait();
         }
-        sV[a * kVRow + h * 4 + i] = w;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          const int b = b0 + i;
+          float4 w = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (nt > 0) {
+            const float i0 = ia0 * sInv[b], i1 = ia1 * sInv[kNI + b];
+            const float im0 = sP[a * kPRow + b] - sP[b * kPRow + a];
+            const float im1 = sP[(kNI + a) * kPRow + b] - sP[(kNI + b) * kPRow + a];
+            w = make_float4(r0[i] * i0, im0 * i0, r1[i] * i1, im1 * i1);
+          }
+          sV[a * kVRow + h * 4 + i] = w;
+        }
       }
       __syncthreads();
       // write the slice back as whole 128-byte lines: 8 consecutive threads per row
+      if (ep) {
 #pragma unroll
-      for (int m = 0; m < kNI * kVCols / kThreads; m++) {
-        const int i = tid + kThreads * m;
-        const int row = i / kVCols, col = i % kVCols;
-        if (row >= ninputs) continue;
-        float4 w = sV[row * kVRow + col];
-        float4 *dst = oblk + (size_t)row * kNI + cb * kVCols + col;
-        if (accumulate) {
-          const float4 old = *dst;
-          w.x += old.x;
-          w.y += old.y;
-          w.z += old.z;
-          w.w += old.w;
+        for (int m = 0; m < kNI * kVCols / kConvThreads; m++) {
+          const int i = ct + kConvThreads * m;
+          const int row = i / kVCols, col = i % kVCols;
+          if (row >= ninputs) continue;
+          float4 w = sV[row * kVRow + col];
+          float4 *dst = oblk + (size_t)row * kNI + cb * kVCols + col;
+          if (accumulate) {
+            const float4 old = *dst;
+            w.x += old.x;
+            w.y += old.y;
+            w.z += old.z;
+            w.w += old.w;
+          }
+          *dst = w;
         }
-        *dst = w;
       }
       __syncthreads();
     }
-  } else if (*s_abort && tid == 0) {
-    // drain: copies issued but not consumed, then the MMAs last committed
-    for (int u = t; u < issued; u++) mbar_wait(smem_u32(bars + u % kStages), (uint32_t)(u / kStages) & 1u);
-    if (t > 0) mbar_wait(smem_u32(bars + kStages + (t - 1) % kOpStages), (uint32_t)((t - 1) / kOpStages) & 1u);
   }
   tc_fence_before();
   __syncthreads();
@@ -492,10 +548,11 @@ finalise_tc_kernel(const TcProdEntry *__restrict__ prods, const TcRowEntry *__re
 
 }  // namespace
 
+
 size_t xmac_tc_smem_bytes(bool hilo)
 {
   const size_t ops = (size_t)kOpStages * (hilo ? 2 : 1) * 2 * kOpChanBytes;
-  return (size_t)kStages * kStageBytes + ops + (kStages + kOpStages) * 8 + 16;
+  return (size_t)kStages * kStageBytes + ops + kNumBars * 8 + 16;
 }
 
 cudaError_t xmac_tc_launch(const float2 *spec, int nblk, int N, int nfreqs, int ninputs, int ks, bool hilo,
