@@ -43,7 +43,8 @@ class gx_station_desc(C.Structure):
                 ("nbands", C.c_int),
                 ("band_localfreq", C.c_int * GX_MAX_BANDS),
                 ("band_pol", C.c_char * GX_MAX_BANDS),
-                ("clock_int_seconds", C.c_int)]
+                ("clock_int_seconds", C.c_int),
+                ("phase_cal_interval_hz", C.c_longlong), ("phase_cal_base_hz", C.c_longlong)]
 
 
 class gx_baseline_desc(C.Structure):
@@ -141,6 +142,7 @@ def job_desc_from_spec(spec: JobSpec, xstep: int = GX_XSTEP_FP32, max_data_bytes
         st.band_pol = pols
         c0 = spec.clock_us[s] if s < len(spec.clock_us) else 0.0
         st.clock_int_seconds = int(math.floor(c0 / 1e6 + 0.5))
+        st.phase_cal_interval_hz = int(1e6 * spec.pcal_interval_mhz)
         stations.append(st)
     baselines = []
     for a in range(spec.nstations):

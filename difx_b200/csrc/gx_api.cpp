@@ -49,7 +49,7 @@ static void free_all(gx_handle *h)
   if (h->device < 0) return;
   void *ptrs[] = {h->d_st, h->d_tw, h->d_spec, h->d_acc, h->d_results, h->d_spec1, h->d_w, h->d_wacc, h->d_w1,
                   h->d_pairs, h->d_prods, h->d_went, h->d_sub, h->d_bp, h->d_bp1, h->d_scale, h->d_tcprods,
-                  h->d_tcrows, h->d_err, h->d_full, h->d_avgtab};
+                  h->d_tcrows, h->d_err, h->d_full, h->d_avgtab, h->d_pcal, h->d_pcalbins};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->h_err) cudaFreeHost(h->h_err);
@@ -250,6 +250,59 @@ static gx_status setup(gx_handle *h)
     if (d.freqs[f].nchan % a) return h->fail(GX_ERR_UNSUPPORTED, "CHANS TO AVG does not divide NUM CHANNELS");
   }
   h->avg = avg;
+  // Phase-cal tones per recorded band (configuration.cpp:1754-1835: integer
+  // Hz, PHASE CAL DIVISOR 1) and the extractor the reference would pick
+  // (PCal::getNew, pcal.cpp:191-260; the implicit-shift ones are built)
+  std::vector<std::vector<int>> pc_ntones(d.nstations);
+  h->pcal.clear();
+  for (int s = 0; s < d.nstations; s++) {
+    const gx_station_desc &x = d.stations[s];
+    if (x.phase_cal_interval_hz <= 0) continue;
+    const long long interval = x.phase_cal_interval_hz, base = x.phase_cal_base_hz;
+    pc_ntones[s].assign(x.nbands, 0);
+    for (int b = 0; b < x.nbands; b++) {
+      const gx_freq_desc &fq = d.freqs[x.recfreq[x.band_localfreq[b]]];
+      const double lofreq = fq.freq_mhz, bw = fq.bw_mhz;
+      const double stepmhz = interval * 1e-6;
+      long long harmonic = (long long)((lofreq - base * 1e-6) / stepmhz);
+      double tonefreq = harmonic * stepmhz + base * 1e-6;
+      int n = 0;
+      long long offset = -1;
+      if (fq.lower_sideband) {
+        if (tonefreq >= lofreq) { tonefreq -= stepmhz; harmonic -= 1; }
+        if (tonefreq >= lofreq - bw)
+          while (tonefreq - n * stepmhz >= lofreq - bw) n++;
+        if (n > 0) offset = (long long)(1e6 * lofreq) - harmonic * interval;
+      } else {
+        if (tonefreq <= lofreq) { tonefreq += stepmhz; harmonic += 1; }
+        if (tonefreq <= lofreq + bw)
+          while (tonefreq + n * stepmhz <= lofreq + bw) n++;
+        if (n > 0) offset = harmonic * interval - (long long)(1e6 * lofreq);
+      }
+      if (n == 0) n = 1;   // no tone in the band: one zero placeholder
+      pc_ntones[s][b] = n;
+      PcalBand P{};
+      P.station = s;
+      P.band = b;
+      P.ntones = n;
+      P.nbins = 0;
+      if (offset >= 0) {
+        const long long bwhz = (long long)(1e6 * bw);
+        const long long fs = cplx ? bwhz : 2 * bwhz;
+        if (offset == 0) return h->fail(GX_ERR_UNSUPPORTED, "phase-cal tone at DC (the trivial extractor) is not implemented");
+        const long long No = fs / gcdl(fs, offset), Np = fs / gcdl(fs, interval);
+        if (No % Np != 0)
+          return h->fail(GX_ERR_UNSUPPORTED, "phase-cal offsets that need the shifting extractor are not implemented");
+        long long nb = No;
+        while (fs / (2 * nb) > 1000000) nb *= 2;   // PCal::setMinFrequencyResolution(1e6), mode.cpp:403
+        if (nb > 65536) return h->fail(GX_ERR_UNSUPPORTED, "more than 65536 phase-cal bins");
+        P.nbins = (int)nb;
+        P.step = (int)std::floor((double)nb * (double)interval / (double)fs);
+        P.offset_bin = (int)std::floor((double)nb * (double)offset / (double)fs);
+      }
+      h->pcal.push_back(P);
+    }
+  }
   // Core result layout for records of 1 / div of the channels: crosses by
   // freq and baseline, baseline weights, autocorrelations, their weights
   auto build = [&](int div, std::vector<int> &blofs, std::vector<int> &bwofs, std::vector<int> &acofs,
@@ -294,11 +347,30 @@ static gx_status setup(gx_handle *h)
       if (add == 0) add = 1;
       idx += add;
     }
+    for (int s = 0; s < d.nstations; s++)   // and finally the phase-cal tones
+      for (int n : pc_ntones[s]) idx += n;
     return idx;
   };
   // the kernels fill the full-resolution array; the averaged one is the result
   h->rl_full = build(1, h->blofs_full, h->bwofs_full, h->acofs_full, h->acwofs_full);
   h->rl = build(avg, h->blofs, h->bwofs, h->acofs, h->acwofs);
+  // phase-cal section: after the autocorrelation weights, datastream by datastream, band by band
+  h->pc_off.assign((size_t)d.nstations * GX_MAX_BANDS, -1);
+  h->pc_ntones.assign((size_t)d.nstations * GX_MAX_BANDS, 0);
+  {
+    long long pos_full = h->rl_full, pos = h->rl;
+    for (int s = 0; s < d.nstations; s++)
+      for (int n : pc_ntones[s]) pos_full -= n, pos -= n;
+    size_t k = 0;
+    for (int s = 0; s < d.nstations; s++)
+      for (int b = 0; b < (int)pc_ntones[s].size(); b++) {
+        h->pcal[k++].result_offset = pos_full;
+        h->pc_off[(size_t)s * GX_MAX_BANDS + b] = (int)pos;
+        h->pc_ntones[(size_t)s * GX_MAX_BANDS + b] = pc_ntones[s][b];
+        pos_full += pc_ntones[s][b];
+        pos += pc_ntones[s][b];
+      }
+  }
   h->avgtab.clear();
   if (avg > 1) {
     auto add = [&](long long src, long long dst, int n, int L) { h->avgtab.push_back(AvgEntry{src, dst, n, L}); };
@@ -312,15 +384,20 @@ static gx_status setup(gx_handle *h)
               nf / avg, avg);
         add(h->bwofs_full[f * nbl + j], h->bwofs[f * nbl + j], np / 2 + np % 2, 1);
       }
+    long long total_pc = 0;   // the phase-cal section follows the autocorrelation weights
+    for (int q = 0; q < d.nstations; q++)
+      for (int n : pc_ntones[q]) total_pc += n;
     for (int s = 0; s < d.nstations; s++) {
       const long long end_full = s + 1 < d.nstations ? h->acofs_full[s + 1] : h->acwofs_full[0];
       const int nr = (int)((end_full - h->acofs_full[s]) / J.nchan);
       for (int r = 0; r < nr; r++)
         add(h->acofs_full[s] + (long long)r * J.nchan, h->acofs[s] + (long long)r * (J.nchan / avg), J.nchan / avg,
             avg);
-      const long long wend_full = s + 1 < d.nstations ? h->acwofs_full[s + 1] : h->rl_full;
+      const long long wend_full = s + 1 < d.nstations ? h->acwofs_full[s + 1] : h->rl_full - total_pc;
       add(h->acwofs_full[s], h->acwofs[s], (int)(wend_full - h->acwofs_full[s]), 1);
     }
+    for (const PcalBand &P : h->pcal)   // phase-cal tones are copied
+      add(P.result_offset, h->pc_off[(size_t)P.station * GX_MAX_BANDS + P.band], P.ntones, 1);
   }
 
   // accumulator index of the Hermitian entry (a, b) of freq f
@@ -592,6 +669,17 @@ static gx_status setup(gx_handle *h)
   if (!h->wents.empty())
     CKR(h, cudaMemcpy(h->d_went, h->wents.data(), sizeof(WeightEntry) * h->wents.size(), cudaMemcpyHostToDevice));
   CKR(h, h->dalloc(&h->d_results, sizeof(float2) * h->rl));
+  if (!h->pcal.empty()) {
+    h->pcal_maxbins = 1;
+    for (const PcalBand &P : h->pcal) h->pcal_maxbins = std::max(h->pcal_maxbins, P.nbins);
+    // enough CTAs for the SMs: chunks of blocks per band, at most one chunk per 16 blocks
+    h->pcal_chunks = (int)std::max<long long>(1, std::min<long long>(std::max(1, h->chunk / 16),
+                                                                      (2 * 148 + (long long)h->pcal.size() - 1) /
+                                                                          (long long)h->pcal.size()));
+    CKR(h, h->dalloc(&h->d_pcal, sizeof(PcalBand) * h->pcal.size()));
+    CKR(h, cudaMemcpy(h->d_pcal, h->pcal.data(), sizeof(PcalBand) * h->pcal.size(), cudaMemcpyHostToDevice));
+    CKR(h, h->dalloc(&h->d_pcalbins, sizeof(float2) * (size_t)h->pcal_chunks * h->pcal.size() * h->pcal_maxbins));
+  }
   if (h->avg > 1) {
     CKR(h, h->dalloc(&h->d_full, sizeof(float2) * h->rl_full));
     CKR(h, h->dalloc(&h->d_avgtab, sizeof(AvgEntry) * h->avgtab.size()));
@@ -644,6 +732,7 @@ gx_status plan_job(const gx_job_desc *desc, JobPlan *plan, std::string &err)
   gx_status s = setup(&h);
   if (s != GX_OK) { err = h.err; return s; }
   if (h.avg > 1) { err = "channel averaging is not implemented by the allocation-free entry point"; return GX_ERR_UNSUPPORTED; }
+  if (!h.pcal.empty()) { err = "phase-cal extraction is not implemented by the allocation-free entry point"; return GX_ERR_UNSUPPORTED; }
   plan->J = h.J;
   plan->J.twiddle = nullptr;
   plan->maxnrf = h.maxnrf;
@@ -738,6 +827,14 @@ gx_status gx_get_layout(const gx_handle *h, gx_layout_info *info)
   info->xstep = h->xstep;
   info->block_chunk = h->chunk;
   info->chans_to_average = h->avg;
+  return GX_OK;
+}
+
+gx_status gx_get_pcal_layout(const gx_handle *h, int *offsets, int *ntones)
+{
+  if (!h) return GX_ERR_ARG;
+  if (offsets) memcpy(offsets, h->pc_off.data(), sizeof(int) * h->pc_off.size());
+  if (ntones) memcpy(ntones, h->pc_ntones.data(), sizeof(int) * h->pc_ntones.size());
   return GX_OK;
 }
 
@@ -839,11 +936,18 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
   if (!h->tc) CKR(h, cudaMemsetAsync(h->d_acc, 0, sizeof(float2) * h->acc_slice * h->ks, st));
   CKR(h, cudaMemsetAsync(h->d_wacc, 0, sizeof(float) * (d.nstations + nbl), st));
   CKR(h, cudaMemsetAsync(h->d_err, 0, sizeof(int), st));
+  const int npc = (int)h->pcal.size();
+  if (npc)
+    CKR(h, cudaMemsetAsync(h->d_pcalbins, 0, sizeof(float2) * (size_t)h->pcal_chunks * npc * h->pcal_maxbins, st));
   gx_status r;
   for (int b0 = 0; b0 < J.blocks_per_send; b0 += h->chunk) {
     const int nb = std::min(h->chunk, J.blocks_per_send - b0);
     if ((r = mark(0, true)) != GX_OK) return r;
     CKR(h, fstep_launch(J, h->d_st, h->maxnrf, S, b0, nb, h->nslots, h->d_spec, h->d_w, h->d_bp, st));
+    if (npc) {
+      CKR(h, pcal_bins_launch(J, S, h->d_bp, nb, h->d_pcal, npc, h->pcal_chunks, h->pcal_maxbins, h->d_pcalbins, st));
+      h->launches += 1;
+    }
     if ((r = mark(0, false)) != GX_OK) return r;
     if ((r = mark(1, true)) != GX_OK) return r;
     if (h->tc)
@@ -869,6 +973,10 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
                            (int)h->wents.size(), h->d_wacc, fin, st));
   }
   h->launches += (h->prods.empty() ? 0 : 1) + (h->wents.empty() ? 0 : 1);
+  if (npc) {
+    CKR(h, pcal_tones_launch(h->d_pcal, npc, h->pcal_chunks, h->pcal_maxbins, h->d_pcalbins, fin, st));
+    h->launches += 1;
+  }
   if (h->avg > 1) {
     CKR(h, cudaMemsetAsync(dev_results, 0, sizeof(float2) * h->rl, st));
     CKR(h, average_launch(h->d_avgtab, (int)h->avgtab.size(), h->d_full, dev_results, st));

@@ -88,10 +88,27 @@ struct SubintArrays {
   const double *interp;          // [nstations][3]
 };
 
+// One recorded band with phase-cal extraction (the reference's implicit-shift
+// extractors, pcal.cpp:1032-1222 real, 1419-1600 complex): sample n of a block
+// whose absolute sample number is S goes to bin (S + n) mod nbins; tone t is
+// bin offset_bin + t * step of the bins' forward DFT (0 past nbins).
+struct PcalBand {
+  int station, band, nbins, ntones, offset_bin, step;
+  long long result_offset;   // first tone in the full-resolution result array
+};
+
 // Raises `kernel`'s dynamic shared-memory limit on the current device to at
 // least `bytes`.  Safe from several host threads at once: the limit only ever
 // grows, so a launch that opted in for its size cannot be undercut by another
 // thread opting in for a smaller one.
 cudaError_t smem_opt_in(const void *kernel, size_t bytes);
+
+// Phase-cal: bin sums of one pass of blocks (added into partial[chunk][band][bin]),
+// then the tones of all bands into the result array.
+cudaError_t pcal_bins_launch(const DevJob &J, const SubintArrays &S, const BlockParam *bp, int nblk,
+                             const PcalBand *bands, int nbands, int chunks, int maxbins, float2 *partial,
+                             cudaStream_t st);
+cudaError_t pcal_tones_launch(const PcalBand *bands, int nbands, int chunks, int maxbins, const float2 *partial,
+                              float2 *results, cudaStream_t st);
 
 }  // namespace gx

@@ -851,6 +851,96 @@ size_t fstep_smem_bytes(const DevJob &J, int nrf, int nslots)
   return b;
 }
 
+// ---------------------------------------------------------------------------
+// Phase-cal extraction (Mode::process, mode.cpp:759-774; the implicit-shift
+// extractors of pcal.cpp).  Every processed block adds its F decoded samples
+// (before any rotation, as the reference's unpacked arrays) into nbins bins
+// by absolute sample number; thread k of a CTA owns bin k (and k + 256, ...)
+// of its chunk of blocks, so every bin sum is formed in a fixed order.
+// decode_sample (above) gives the samples as the reference's unpacker does.
+
+__global__ void __launch_bounds__(256) pcal_bins_kernel(DevJob J, SubintArrays S, const BlockParam *__restrict__ bp,
+                                                        int nblk, const PcalBand *__restrict__ bands, int chunks,
+                                                        int maxbins, float2 *__restrict__ partial)
+{
+  __shared__ float s_lut[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) s_lut[i] = J.lut[i];
+  __syncthreads();
+  const int c = blockIdx.x, pb = blockIdx.y;
+  const PcalBand B = bands[pb];
+  const int s = B.station, N = B.nbins, F = J.fftlen;
+  if (N <= 0) return;
+  const uint8_t *data = S.data[s];
+  const int32_t *ctrl = S.control + (size_t)s * S.controlstride;
+  // sample number of the data buffer's start (mode.cpp:761)
+  const unsigned long long s0 =
+      (unsigned long long)(((double)ctrl[1] * 1e9 + (double)ctrl[2]) / (J.sampletime * 1e3) + 0.5);
+  const int per = (nblk + chunks - 1) / chunks;
+  const int b0 = c * per, b1 = min(nblk, b0 + per);
+  float2 *out = partial + ((size_t)c * gridDim.y + pb) * maxbins;
+  for (int k = threadIdx.x; k < N; k += blockDim.x) {
+    float2 acc = make_float2(0.f, 0.f);
+    for (int bi = b0; bi < b1; bi++) {
+      const BlockParam P = bp[(size_t)s * nblk + bi];
+      if (P.state == 0) continue;
+      const int idx0 = (int)((s0 + (unsigned long long)P.nearestsample) % (unsigned long long)N);
+      for (int n = (k - idx0 + N) % N; n < F; n += N) {
+        const float2 v = decode_sample(J, data, P, B.band, n, s_lut);
+        acc.x += v.x;
+        acc.y += v.y;
+      }
+    }
+    out[k].x += acc.x;
+    out[k].y += acc.y;
+  }
+}
+
+// Tone t of band pb: the forward DFT of the bins at bin offset_bin + t step,
+// summed in double and rounded once (the reference's DFT of its bins).
+__global__ void __launch_bounds__(128) pcal_tones_kernel(const PcalBand *__restrict__ bands, int chunks, int maxbins,
+                                                         const float2 *__restrict__ partial, float2 *__restrict__ results)
+{
+  const int pb = blockIdx.x;
+  const PcalBand B = bands[pb];
+  for (int t = threadIdx.x; t < B.ntones; t += blockDim.x) {
+    const long long bin = (long long)B.offset_bin + (long long)t * B.step;
+    double re = 0.0, im = 0.0;
+    if (B.nbins > 0 && bin < B.nbins) {
+      for (int k = 0; k < B.nbins; k++) {
+        float bx = 0.f, by = 0.f;   // the bin, summed over the chunks in order
+        for (int c = 0; c < chunks; c++) {
+          const float2 v = partial[((size_t)c * gridDim.x + pb) * maxbins + k];
+          bx += v.x;
+          by += v.y;
+        }
+        const long long m = ((long long)k * bin) % B.nbins;
+        double sn, cs;
+        sincospi(-2.0 * (double)m / (double)B.nbins, &sn, &cs);
+        re += (double)bx * cs - (double)by * sn;
+        im += (double)bx * sn + (double)by * cs;
+      }
+    }
+    results[B.result_offset + t] = make_float2((float)re, (float)im);
+  }
+}
+
+cudaError_t pcal_bins_launch(const DevJob &J, const SubintArrays &S, const BlockParam *bp, int nblk,
+                             const PcalBand *bands, int nbands, int chunks, int maxbins, float2 *partial,
+                             cudaStream_t st)
+{
+  if (nbands <= 0 || nblk <= 0) return cudaSuccess;
+  pcal_bins_kernel<<<dim3(chunks, nbands), 256, 0, st>>>(J, S, bp, nblk, bands, chunks, maxbins, partial);
+  return cudaGetLastError();
+}
+
+cudaError_t pcal_tones_launch(const PcalBand *bands, int nbands, int chunks, int maxbins, const float2 *partial,
+                              float2 *results, cudaStream_t st)
+{
+  if (nbands <= 0) return cudaSuccess;
+  pcal_tones_kernel<<<nbands, 128, 0, st>>>(bands, chunks, maxbins, partial, results);
+  return cudaGetLastError();
+}
+
 cudaError_t smem_opt_in(const void *kernel, size_t bytes)
 {
   if (bytes <= 48 * 1024) return cudaSuccess;

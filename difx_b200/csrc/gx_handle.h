@@ -34,6 +34,11 @@ struct gx_handle {
   std::vector<gx::AvgEntry> avgtab;          // full -> averaged records
   gx::AvgEntry *d_avgtab = nullptr;
   float2 *d_full = nullptr;
+  std::vector<gx::PcalBand> pcal;            // recorded bands with phase-cal extraction
+  gx::PcalBand *d_pcal = nullptr;
+  float2 *d_pcalbins = nullptr;              // [chunk][pcal band][bin] partial bin sums
+  int pcal_chunks = 0, pcal_maxbins = 0;
+  std::vector<int> pc_off, pc_ntones;        // [station * GX_MAX_BANDS + band]: result index / tones
   std::vector<std::vector<int>> band_input;  // [station][band]
   std::vector<gx::ProdEntry> prods;
   std::vector<gx::TcProdEntry> tcprods;   // sorted by (freq, a)

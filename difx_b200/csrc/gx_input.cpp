@@ -322,10 +322,14 @@ InputJob *read_input_job(const char *inputfile, std::string &err)
       if (strip(v) != "NONE") { err = "PROCESSING METHOD " + strip(v) + " is not implemented"; return nullptr; }
     }
     if (in.peek("TCAL FREQUENCY")) NEED(in, "TCAL FREQUENCY", v);
-    NEED(in, "PHASE CAL INT (MHZ)", v);
-    if (atof(v.c_str()) != 0.0) { err = "phase-cal extraction is not implemented"; return nullptr; }
-    if (in.peek("PHASE CAL DIVISOR")) NEED(in, "PHASE CAL DIVISOR", v);
-    if (in.peek("PHASE CAL BASE(MHZ)")) NEED(in, "PHASE CAL BASE(MHZ)", v);
+    NEED(in, "PHASE CAL INT (MHZ)", v); s.phase_cal_interval_hz = (long long)(1e6 * atof(v.c_str()));
+    if (in.peek("PHASE CAL DIVISOR")) {
+      NEED(in, "PHASE CAL DIVISOR", v);
+      if (atol(v.c_str()) != 1) { err = "PHASE CAL DIVISOR other than 1 is not implemented"; return nullptr; }
+    }
+    if (in.peek("PHASE CAL BASE(MHZ)")) {
+      NEED(in, "PHASE CAL BASE(MHZ)", v); s.phase_cal_base_hz = (long long)(1e6 * atof(v.c_str()));
+    }
     NEED(in, "NUM RECORDED FREQS", v); s.nrecfreqs = atoi(v.c_str());
     if (s.nrecfreqs > GX_MAX_LOCAL_FREQS) { err = "too many recorded freqs"; return nullptr; }
     int nb = 0;

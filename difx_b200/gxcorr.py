@@ -60,7 +60,7 @@ EXPORTED_SYMBOLS = ("gx_open", "gx_open_input", "gx_close", "gx_last_error", "gx
                     "gx_batch_info", "gx_batch_last_error", "gx_batch_close", "gx_vis_buffer",
                     "gx_vis_set_subints", "gx_vis_clear", "gx_subint_async", "gx_subint_wait", "gx_vdifmux_open",
                     "gx_vdifmux_info", "gx_vdifmux_run", "gx_vdifmux_reset_stats", "gx_vdifmux_last_error",
-                    "gx_vdifmux_close")
+                    "gx_vdifmux_close", "gx_get_pcal_layout")
 
 
 def subint_device_noalloc(jd: capi.JobDesc, sd: capi.SubintDesc, dev_results_ptr: int, stream_ptr: int = 0) -> None:
@@ -133,6 +133,15 @@ class Correlator:
         self._check(lib().gx_get_offsets(self.h, bl.ctypes.data_as(C.c_void_p), bw.ctypes.data_as(C.c_void_p),
                                          ac.ctypes.data_as(C.c_void_p), acw.ctypes.data_as(C.c_void_p)))
         return self.result_length, bl, bw, ac, acw
+
+    def pcal_layout(self):
+        """(offsets, ntones), each [nstations][GX_MAX_BANDS]: result index of the first
+        phase-cal tone of each recorded band (-1: none) and its number of tones."""
+        n = self.info.nstations * capi.GX_MAX_BANDS
+        off = np.zeros(n, np.int32)
+        nt = np.zeros(n, np.int32)
+        self._check(lib().gx_get_pcal_layout(self.h, off.ctypes.data_as(C.c_void_p), nt.ctypes.data_as(C.c_void_p)))
+        return off.reshape(-1, capi.GX_MAX_BANDS), nt.reshape(-1, capi.GX_MAX_BANDS)
 
     def interpolator(self, station: int, scan: int, sec: int, ns: int) -> np.ndarray:
         out = np.zeros(3, np.float64)

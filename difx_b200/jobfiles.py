@@ -75,6 +75,7 @@ class JobSpec:
     uvshift_interval_ns: int = 2_000_000_000
     ac_avg_interval_ns: int = 2_000_000_000
     chans_to_avg: int = 1             # CHANS TO AVG of every freq (output channels = nchan / this)
+    pcal_interval_mhz: int = 0        # PHASE CAL INT (MHZ) of every datastream (0: no phase-cal)
     poly_interval_s: int = 120
     station_names: Sequence[str] = ()
     data_files: Sequence[str] = ()
@@ -310,7 +311,7 @@ def write_job(spec: JobSpec, outdir: str) -> dict:
         L.append(_kv("DATA SAMPLING", samp))
         L.append(_kv("DATA SOURCE", "FILE"))
         L.append(_kv("FILTERBANK USED", "FALSE"))
-        L.append(_kv("PHASE CAL INT (MHZ)", 0))
+        L.append(_kv("PHASE CAL INT (MHZ)", spec.pcal_interval_mhz))
         L.append(_kv("NUM RECORDED FREQS", nsb))
         for j in range(nsb):
             L.append(_kv(f"REC FREQ INDEX {j}", j))

@@ -98,6 +98,8 @@ typedef struct gx_station_desc {
   int band_localfreq[GX_MAX_BANDS];                /* REC BAND i INDEX */
   char band_pol[GX_MAX_BANDS];                     /* REC BAND i POL */
   int clock_int_seconds;   /* floor(CLOCK COEFF 0 / 1e6 + 0.5), subtracted from the delay (mode.cpp:68,1526) */
+  long long phase_cal_interval_hz; /* long(1e6 x PHASE CAL INT (MHZ)); 0: no phase-cal extraction */
+  long long phase_cal_base_hz;     /* long(1e6 x PHASE CAL BASE(MHZ)); PHASE CAL DIVISOR must be 1 */
 } gx_station_desc;
 
 /* One baseline (BASELINE TABLE, configuration.cpp:1033-1180). */
@@ -400,6 +402,12 @@ gx_status gx_vdifmux_run(gx_vdifmux *m, const uint8_t *src, long long src_bytes,
 gx_status gx_vdifmux_reset_stats(gx_vdifmux *m);
 const char *gx_vdifmux_last_error(const gx_vdifmux *m);
 gx_status gx_vdifmux_close(gx_vdifmux *m);
+
+/* Phase-cal section of the Core result array (configuration.cpp:2612-2620,
+   core.cpp:1131-1164): offsets[s * GX_MAX_BANDS + b] is the result index of
+   the first tone of recorded band b of datastream s (-1 without phase-cal),
+   ntones[...] its number of tones (complex values).  Either may be NULL. */
+gx_status gx_get_pcal_layout(const gx_handle *h, int *offsets, int *ntones);
 
 /* Device memory a handle holds, bytes. */
 gx_status gx_device_bytes(const gx_handle *h, long long *bytes);

@@ -263,3 +263,44 @@ def test_gpu_channel_averaging_matches_reference(case, gx, oracle_lib):
 def capi_job_desc(spec):
     from difx_b200 import capi
     return capi.job_desc_from_spec(spec)
+
+
+PCAL_CASES = {
+    "c1_pcal": lambda: (jobs.spec_c1(name="c1pc", seed=81, pcal_interval_mhz=1), dict(invalid_frac=0.03)),
+    "lsb_pcal": lambda: (jobs.spec_lsb(name="lsbpc", seed=82, pcal_interval_mhz=1), dict(invalid_frac=0.03)),
+    "cplx8_pcal": lambda: (jobs.spec_cplx8(name="cx8pc", seed=83, pcal_interval_mhz=1), dict(invalid_frac=0.03)),
+}
+PCAL_TOL = 1e-4   # FP32 bin sums (tens of thousands of samples per bin) formed in another order
+
+
+@pytest.mark.skipif(not pyoracle.reference_available(), reason="reference harness not built")
+@pytest.mark.parametrize("case", sorted(PCAL_CASES))
+def test_gpu_phase_cal_matches_reference(case, gx, oracle_lib):
+    """Phase-cal tones (PHASE CAL INT 1 MHz; the reference's implicit-shift
+    extractors, pcal.cpp:1032-1600, called from mode.cpp:759-774 and copied by
+    core.cpp:1131-1164) in the Core result array, against the compiled
+    reference reading the same .input; the rest of the array as usual."""
+    spec, kw = PCAL_CASES[case]()
+    prep = jobs.prepare(spec, [100_000_000, 108_000_000], **kw)
+    c = gx.Correlator.from_desc(prep.jd)
+    off, nt = c.pcal_layout()
+    for i, sd in enumerate(prep.sds):
+        g = c.subint(sd)
+        r = jobs.reference_for(prep.paths["input"]).process(prep.subs[i])
+        assert g.shape == r.shape
+        m, wrel = _compare(g, r, prep.jd, spec, oracle_lib, layout=c.offsets())
+        assert m < REC_TOL and wrel < W_TOL, (m, wrel)
+        worst, nbands = 0.0, 0
+        for s in range(spec.nstations):
+            for b in range(spec.nbands):
+                o, n = int(off[s, b]), int(nt[s, b])
+                assert o >= 0 and n > 0
+                ga, ra = g[o:o + n], r[o:o + n]
+                den = np.mean(np.abs(ra))
+                if den > 0:
+                    worst = max(worst, float(np.mean(np.abs(ga - ra)) / den))
+                    nbands += 1
+                else:
+                    assert np.all(ga == 0)
+        assert nbands > 0 and worst < PCAL_TOL, (i, worst)
+    c.close()
