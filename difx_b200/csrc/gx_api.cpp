@@ -255,6 +255,8 @@ static gx_status setup(gx_handle *h)
   // (PCal::getNew, pcal.cpp:191-260; the implicit-shift ones are built)
   std::vector<std::vector<int>> pc_ntones(d.nstations);
   h->pcal.clear();
+  h->pc_tone_hz.assign((size_t)d.nstations * GX_MAX_BANDS, {});
+  h->pc_maxtones.assign(d.nstations, 0);
   for (int s = 0; s < d.nstations; s++) {
     const gx_station_desc &x = d.stations[s];
     if (x.phase_cal_interval_hz <= 0) continue;
@@ -279,7 +281,15 @@ static gx_status setup(gx_handle *h)
           while (tonefreq + n * stepmhz <= lofreq + bw) n++;
         if (n > 0) offset = harmonic * interval - (long long)(1e6 * lofreq);
       }
-      if (n == 0) n = 1;   // no tone in the band: one zero placeholder
+      // tone frequencies (configuration.cpp:1784-1786, 1818-1820) and the most per band
+      std::vector<double> &tf = h->pc_tone_hz[(size_t)s * GX_MAX_BANDS + b];
+      for (int k = 0; k < n; k++)
+        tf.push_back((double)((fq.lower_sideband ? harmonic - k : harmonic + k) * interval) + (double)base);
+      h->pc_maxtones[s] = std::max(h->pc_maxtones[s], n);
+      if (n == 0) {        // no tone in the band: one zero placeholder at 0 Hz
+        n = 1;
+        tf.push_back(0.0);
+      }
       pc_ntones[s][b] = n;
       PcalBand P{};
       P.station = s;

@@ -39,6 +39,8 @@ struct gx_handle {
   float2 *d_pcalbins = nullptr;              // [chunk][pcal band][bin] partial bin sums
   int pcal_chunks = 0, pcal_maxbins = 0;
   std::vector<int> pc_off, pc_ntones;        // [station * GX_MAX_BANDS + band]: result index / tones
+  std::vector<std::vector<double>> pc_tone_hz;   // [station * GX_MAX_BANDS + band]: tone frequencies (Hz)
+  std::vector<int> pc_maxtones;              // [station]: most tones of a band (0: phase-cal off)
   std::vector<std::vector<int>> band_input;  // [station][band]
   std::vector<gx::ProdEntry> prods;
   std::vector<gx::TcProdEntry> tcprods;   // sorted by (freq, a)

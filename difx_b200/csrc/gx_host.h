@@ -53,6 +53,7 @@ struct JobMeta {
   double int_time = 0;                 // INT TIME (SEC)
   std::vector<int> telescope;          // TELESCOPE INDEX per datastream
   std::vector<double> tsys;            // TSYS per datastream
+  std::vector<std::string> telescope_name;   // TELESCOPE NAME per telescope
 };
 
 struct InputJob {

@@ -580,6 +580,7 @@ InputJob *read_input_job(const char *inputfile, std::string &err)
   job->meta.start_seconds = job->start_seconds;
   job->meta.execute_seconds = job->execute_seconds;
   job->meta.int_time = job->int_time;
+  job->meta.telescope_name = telname;
   for (int i = 0; i < numds; i++) {
     job->meta.telescope.push_back(tel_of_cfgds[i]);
     job->meta.tsys.push_back(dstsys[dsidx[i]]);

@@ -302,9 +302,82 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
   of.close();
   if (!of) return h->fail(GX_ERR_IO, "write failed: " + v->outdir + name);
 
+  // phase-cal lines (writedata, visibility.cpp:650-675 and 985-1053): each band's
+  // tones scaled as its parallel-hand autocorrelation, one line per datastream
+  {
+    const double pcalmjd = dumpmjd + dumpseconds / 86400.0;
+    for (int s = 0; s < d.nstations; s++) {
+      const gx_station_desc &x = d.stations[s];
+      if (x.phase_cal_interval_hz <= 0) continue;
+      const int maxt = h->pc_maxtones[s];
+      char str[256];
+      snprintf(str, sizeof(str), "%s %17.11f %13.11f %d %d %d", M.telescope_name[M.telescope[s]].c_str(), pcalmjd,
+               M.int_time / 86400.0, s, x.nbands, maxt);
+      std::string line = str;
+      bool nonzero = false;
+      long long widx = 2LL * h->acwofs[s];
+      for (int b = 0; b < x.nbands; b++) {
+        const int f = x.recfreq[x.band_localfreq[b]];
+        float w = 0.0f, scale = 0.0f;
+        if (freq_used(f)) weight_and_scale(widx++, w, scale);
+        const size_t key = (size_t)s * GX_MAX_BANDS + b;
+        const int nt = h->pc_ntones[key];
+        const long long base = h->pc_off[key];
+        for (int t = 0; t < maxt; t++) {
+          if (t >= nt) {
+            line += " -1 0 0 0";
+            continue;
+          }
+          float2 v2 = v->h_buf[base + t];
+          if (w > 0.0f) {
+            v2.x *= scale;
+            v2.y *= scale;
+          }
+          const bool lsb = d.freqs[f].lower_sideband != 0;
+          snprintf(str, sizeof(str), " %.12g %c %12.5e %12.5e", 1e-6 * h->pc_tone_hz[key][t], x.band_pol[b],
+                   (double)v2.x, (double)(lsb ? v2.y : -v2.y));
+          if (v2.x != 0.0f && -v2.y != 0.0f) nonzero = true;
+          line += str;
+        }
+      }
+      if (nonzero) {
+        char pname[256];
+        snprintf(pname, sizeof(pname), "/PCAL_%05d_%06d_%s", M.start_mjd, M.start_seconds,
+                 M.telescope_name[M.telescope[s]].c_str());
+        std::ofstream pf(v->outdir + pname, std::ios::app);
+        pf << line << "\n";
+        if (!pf) return h->fail(GX_ERR_IO, "write failed: " + v->outdir + pname);
+      }
+    }
+  }
+
   CKR(h, cudaMemsetAsync(v->d_int, 0, sizeof(float2) * h->rl, v->st));
   v->nsub = 0;
   if (nrecords) *nrecords = (int)recs.size();
+  return GX_OK;
+}
+
+gx_status gx_vis_pcal_headers(gx_vis *v)
+{
+  if (!v) return GX_ERR_ARG;
+  gx_handle *h = v->h;
+  const gx_job_desc &d = h->jd;
+  const JobMeta &M = *h->meta;
+  std::vector<std::string> done;
+  for (int s = 0; s < d.nstations; s++) {
+    if (d.stations[s].phase_cal_interval_hz <= 0) continue;
+    const std::string &name = M.telescope_name[M.telescope[s]];
+    bool seen = false;
+    for (const std::string &x : done) seen = seen || x == name;
+    if (seen) continue;
+    char pname[256];
+    snprintf(pname, sizeof(pname), "/PCAL_%05d_%06d_%s", M.start_mjd, M.start_seconds, name.c_str());
+    std::ofstream pf(v->outdir + pname, std::ios::app);
+    pf << "# DiFX-derived pulse cal data\n# File version = 1\n# Start MJD = " << M.start_mjd
+       << "\n# Start seconds = " << M.start_seconds << "\n# Telescope name = " << name << "\n";
+    if (!pf) return h->fail(GX_ERR_IO, "cannot write " + v->outdir + pname);
+    done.push_back(name);
+  }
   return GX_OK;
 }
 

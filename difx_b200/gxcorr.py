@@ -60,7 +60,7 @@ EXPORTED_SYMBOLS = ("gx_open", "gx_open_input", "gx_close", "gx_last_error", "gx
                     "gx_batch_info", "gx_batch_last_error", "gx_batch_close", "gx_vis_buffer",
                     "gx_vis_set_subints", "gx_vis_clear", "gx_subint_async", "gx_subint_wait", "gx_vdifmux_open",
                     "gx_vdifmux_info", "gx_vdifmux_run", "gx_vdifmux_reset_stats", "gx_vdifmux_last_error",
-                    "gx_vdifmux_close", "gx_get_pcal_layout")
+                    "gx_vdifmux_close", "gx_get_pcal_layout", "gx_vis_pcal_headers")
 
 
 def subint_device_noalloc(jd: capi.JobDesc, sd: capi.SubintDesc, dev_results_ptr: int, stream_ptr: int = 0) -> None:
@@ -252,6 +252,10 @@ class Visibility:
 
     def clear(self) -> None:
         self.corr._check(lib().gx_vis_clear(self.v))
+
+    def pcal_headers(self) -> None:
+        """The comment lines at the top of the PCAL files (once per job)."""
+        self.corr._check(lib().gx_vis_pcal_headers(self.v))
 
     def close(self) -> None:
         if self.v:

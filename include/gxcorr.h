@@ -253,6 +253,12 @@ gx_status gx_vis_add(gx_vis *v, const float *dev_results, void *stream);
    past the end of the job or with no subints added. */
 gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords);
 gx_status gx_vis_close(gx_vis *v);
+/* With phase-cal extraction, gx_vis_write also appends each datastream's
+   scaled tones as one line to <outdir>/PCAL_<start mjd>_<start seconds>_<station>
+   (writedata, visibility.cpp:650-675, 985-1053); gx_vis_pcal_headers writes
+   the comment lines FxManager puts at the top of those files once per job
+   (Visibility::initialisePcalFiles, visibility.cpp:107-138). */
+gx_status gx_vis_pcal_headers(gx_vis *v);
 
 /* Partial integrations on several GPUs (subints shared out over ranks, as the
    FxManager shares them over Cores, fxmanager.cpp:331-336): the device

@@ -26,6 +26,8 @@ CASES = {
     "lsb_3st": lambda: jobs.spec_lsb(name="gvisl", seed=19, int_time=0.008),
     "cplx8": lambda: jobs.spec_cplx8(name="gvisc", seed=23, int_time=0.008192),
     "c1_avg4": lambda: jobs.spec_c1(name="gvisa", seed=29, int_time=0.016, chans_to_avg=4),
+    "c1_pcal": lambda: jobs.spec_c1(name="gvisp", seed=31, int_time=0.016, pcal_interval_mhz=1),
+    "lsb_pcal": lambda: jobs.spec_lsb(name="gvislp", seed=37, int_time=0.008, pcal_interval_mhz=1),
 }
 
 
@@ -53,7 +55,7 @@ def _run_gpu(prep, outdir, xstep=capi.GX_XSTEP_FP32):
 
 
 def _file(d):
-    fs = os.listdir(d)
+    fs = [f for f in os.listdir(d) if f.startswith("DIFX_")]
     assert len(fs) == 1, fs
     return os.path.join(d, fs[0])
 
@@ -145,3 +147,42 @@ def test_integration_over_ranks_single_gpu(tmp_path):
     assert np.array_equal(np.fromfile(_file(outdir), np.uint8), np.fromfile(_file(seq), np.uint8))
     v.close()
     c.close()
+
+
+@pytest.mark.parametrize("case", ["c1_pcal", "lsb_pcal"])
+def test_pcal_files_match_reference(case, tmp_path):
+    """PCAL_<mjd>_<sec>_<station> lines (tones scaled as the band's
+    autocorrelation, USB imaginary parts negated) equal the reference
+    Visibility's for the same result arrays; the header lines come from
+    gx_vis_pcal_headers as FxManager writes them once per job."""
+    spec = CASES[case]()
+    nsub = int(round(spec.int_time * 1e9 / spec.subint_ns))
+    starts = [100_000_000 + k * spec.subint_ns for k in range(nsub)]
+    prep = jobs.prepare(spec, starts, invalid_frac=0.03)
+    ours = str(tmp_path / "gx.difx")
+    os.makedirs(ours)
+    n, host = _run_gpu(prep, ours)
+    theirs = str(tmp_path / "ref.difx")
+    s0 = prep.subs[0]
+    jobs.reference_for(prep.paths["input"]).vis_write(host, s0.scan, s0.sec, s0.ns, theirs)
+    pa = sorted(f for f in os.listdir(ours) if f.startswith("PCAL_"))
+    pb = sorted(f for f in os.listdir(theirs) if f.startswith("PCAL_"))
+    assert pa == pb and len(pa) == spec.nstations, (pa, pb)
+    for f in pa:
+        a = open(os.path.join(ours, f)).read()
+        b = open(os.path.join(theirs, f)).read()
+        assert a == b, f
+        assert len(a.splitlines()) == 1 and len(a.split()) == 6 + 4 * spec.nbands * 16
+    # the header lines
+    from difx_b200.gxcorr import Correlator, Visibility
+    c = Correlator.from_input(prep.paths["input"], device=0)
+    hd = str(tmp_path / "hdr")
+    os.makedirs(hd)
+    v = Visibility(c, hd)
+    v.pcal_headers()
+    v.close()
+    c.close()
+    for f in os.listdir(hd):
+        lines = open(os.path.join(hd, f)).read().splitlines()
+        assert lines[0] == "# DiFX-derived pulse cal data" and lines[1] == "# File version = 1"
+        assert lines[4] == "# Telescope name = " + f.split("_", 3)[3]
