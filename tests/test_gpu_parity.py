@@ -62,6 +62,12 @@ CASES = {
     "cplx8_4096_lsb": lambda: (jobs.spec_long("cx8ll", 8, "COMPLEX", "L", 4096, 43), dict(invalid_frac=0.03)),
     "real2_8192": lambda: (jobs.spec_long("r2x", 2, "REAL", "U", 4096, 47), dict(invalid_frac=0.03)),
     "real2_2048_lsb": lambda: (jobs.spec_long("r2m", 2, "REAL", "L", 1024, 53), dict(invalid_frac=0.03)),
+    # other bit depths: 1-bit real (8 bands so that a time sample fills a byte), 4-bit real and complex
+    "real1_256": lambda: (jobs.spec_long("r1p", 1, "REAL", "U", 128, 57, subbands=[
+        jobs.Subband(8400.0 + 16 * i, 16.0, "U", 128) for i in range(4)]), dict(invalid_frac=0.03)),
+    "real4_1024": lambda: (jobs.spec_long("r4p", 4, "REAL", "U", 512, 59), dict(invalid_frac=0.03)),
+    "cplx4_512": lambda: (jobs.spec_long("cx4p", 4, "COMPLEX", "U", 512, 61), dict(invalid_frac=0.03)),
+    "cplx2_128": lambda: (jobs.spec_long("cx2p", 2, "COMPLEX", "U", 128, 63), dict(invalid_frac=0.03)),
 }
 
 

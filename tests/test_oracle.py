@@ -142,3 +142,25 @@ def test_correlation_is_detected(oracle_lib):
         v = o[bl[j]: bl[j] + spec.nchan]   # freq 0, RR
         coh = abs(v.mean()) / np.abs(v).mean()
         assert coh > 0.8, (j, coh)
+
+
+FORMAT_CASES = {
+    "real1": lambda: (jobs.spec_long("r1p", 1, "REAL", "U", 128, 57, subbands=[
+        jobs.Subband(8400.0 + 16 * i, 16.0, "U", 128) for i in range(4)]), dict(invalid_frac=0.03)),
+    "real4": lambda: (jobs.spec_long("r4p", 4, "REAL", "U", 512, 59), dict(invalid_frac=0.03)),
+    "cplx4": lambda: (jobs.spec_long("cx4p", 4, "COMPLEX", "U", 512, 61), dict(invalid_frac=0.03)),
+    "cplx2": lambda: (jobs.spec_long("cx2p", 2, "COMPLEX", "U", 128, 63), dict(invalid_frac=0.03)),
+}
+
+
+@needs_ref
+@pytest.mark.parametrize("case", sorted(FORMAT_CASES))
+def test_oracle_bitexact_other_bit_depths(case, oracle_lib):
+    """1-bit and 4-bit real, 2- and 4-bit complex VDIF: the oracle's Core
+    result array equals the reference's bit for bit."""
+    spec, kw = FORMAT_CASES[case]()
+    prep = jobs.prepare(spec, [100_000_000], **kw)
+    r = jobs.reference_for(prep.paths["input"]).process(prep.subs[0])
+    o = oracle_lib.subint(prep.jd, prep.sds[0], _params(oracle_lib, spec))
+    assert r.shape == o.shape
+    np.testing.assert_array_equal(o.astype(np.complex64), r)
