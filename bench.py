@@ -216,6 +216,8 @@ def run_reference_arm(args):
     v = statistics.median(steps)
     base["value"] = v
     spec = workload_spec(args.config, subint_ns=int(round(args.subint_ms * 1e6)))
+    if args.pcal_mhz:
+        spec = JobSpec(**{**spec.__dict__, "pcal_interval_mhz": args.pcal_mhz})
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": samples_per_subint(spec) / (v * 1e9) * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -234,7 +236,8 @@ def config_dict(spec: JobSpec, args):
             "stations": spec.nstations, "bands_per_station": spec.nbands, "nchan": spec.nchan,
             "fft_points": spec.fftchannels, "subint_ms": spec.subint_ns / 1e6,
             "samples_per_step": samples_per_subint(spec), "xstep": args.xstep,
-            "l2": "inputs larger than L2 (no flush)", "parallelism": f"subint-parallel x{args.gpus}"}
+            "l2": "inputs larger than L2 (no flush)", "parallelism": f"subint-parallel x{args.gpus}",
+            "phase_cal_mhz": spec.pcal_interval_mhz}
 
 
 def load_peaks():
@@ -647,6 +650,8 @@ def main():
     ap.add_argument("--xstep", default=None, choices=sorted(XSTEPS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the other X-step forms")
+    ap.add_argument("--pcal-mhz", type=int, default=0,
+                    help="PHASE CAL INT (MHZ) of every station (0: none); timing with phase-cal extraction")
     ap.add_argument("--subint-ms", type=float, default=None,
                     help="subint length; smaller values give small profiling cases")
     args = ap.parse_args()
@@ -677,6 +682,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
 
     spec = workload_spec(args.config, subint_ns=int(round(args.subint_ms * 1e6)))
+    if args.pcal_mhz:
+        spec = JobSpec(**{**spec.__dict__, "pcal_interval_mhz": args.pcal_mhz})
     d = tempfile.mkdtemp(prefix=f"gxbench{rank}_")
     paths = write_job(spec, d)
     # each rank correlates its own subint of the job

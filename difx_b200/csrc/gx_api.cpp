@@ -682,10 +682,21 @@ static gx_status setup(gx_handle *h)
   if (!h->pcal.empty()) {
     h->pcal_maxbins = 1;
     for (const PcalBand &P : h->pcal) h->pcal_maxbins = std::max(h->pcal_maxbins, P.nbins);
-    // enough CTAs for the SMs: chunks of blocks per band, at most one chunk per 16 blocks
-    h->pcal_chunks = (int)std::max<long long>(1, std::min<long long>(std::max(1, h->chunk / 16),
-                                                                      (2 * 148 + (long long)h->pcal.size() - 1) /
+    // enough CTAs for four waves of the SMs: chunks of blocks per band, at least 8 blocks a chunk
+    h->pcal_chunks = (int)std::max<long long>(1, std::min<long long>(std::max(1, h->chunk / 8),
+                                                                      (4 * 148 + (long long)h->pcal.size() - 1) /
                                                                           (long long)h->pcal.size()));
+    // one CTA per station when every station with phase-cal has the same bands
+    // and bin count (the usual case), else one per band
+    h->pcal_per_station = J.nbands;
+    for (size_t i = 0; i < h->pcal.size(); i++)
+      if (h->pcal.size() % J.nbands || h->pcal[i].nbins != h->pcal[0].nbins || h->pcal[i].nbins <= 0 ||
+          h->pcal[i].station != h->pcal[i - i % J.nbands].station)
+        h->pcal_per_station = 0;
+    if (h->pcal_per_station) {   // chunks for four waves of station CTAs
+      const long long ng = (long long)h->pcal.size() / J.nbands;
+      h->pcal_chunks = (int)std::max<long long>(1, std::min<long long>(std::max(1, h->chunk / 8), (4 * 148 + ng - 1) / ng));
+    }
     CKR(h, h->dalloc(&h->d_pcal, sizeof(PcalBand) * h->pcal.size()));
     CKR(h, cudaMemcpy(h->d_pcal, h->pcal.data(), sizeof(PcalBand) * h->pcal.size(), cudaMemcpyHostToDevice));
     CKR(h, h->dalloc(&h->d_pcalbins, sizeof(float2) * (size_t)h->pcal_chunks * h->pcal.size() * h->pcal_maxbins));
@@ -955,7 +966,8 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
     if ((r = mark(0, true)) != GX_OK) return r;
     CKR(h, fstep_launch(J, h->d_st, h->maxnrf, S, b0, nb, h->nslots, h->d_spec, h->d_w, h->d_bp, st));
     if (npc) {
-      CKR(h, pcal_bins_launch(J, S, h->d_bp, nb, h->d_pcal, npc, h->pcal_chunks, h->pcal_maxbins, h->d_pcalbins, st));
+      CKR(h, pcal_bins_launch(J, S, h->d_bp, nb, h->d_pcal, npc, h->pcal_per_station, h->pcal_chunks,
+                              h->pcal_maxbins, h->d_pcalbins, st));
       h->launches += 1;
     }
     if ((r = mark(0, false)) != GX_OK) return r;

@@ -106,8 +106,8 @@ cudaError_t smem_opt_in(const void *kernel, size_t bytes);
 // Phase-cal: bin sums of one pass of blocks (added into partial[chunk][band][bin]),
 // then the tones of all bands into the result array.
 cudaError_t pcal_bins_launch(const DevJob &J, const SubintArrays &S, const BlockParam *bp, int nblk,
-                             const PcalBand *bands, int nbands, int chunks, int maxbins, float2 *partial,
-                             cudaStream_t st);
+                             const PcalBand *bands, int nbands, int per_station, int chunks, int maxbins,
+                             float2 *partial, cudaStream_t st);
 cudaError_t pcal_tones_launch(const PcalBand *bands, int nbands, int chunks, int maxbins, const float2 *partial,
                               float2 *results, cudaStream_t st);
 

@@ -857,18 +857,56 @@ size_t fstep_smem_bytes(const DevJob &J, int nrf, int nslots)
 // (before any rotation, as the reference's unpacked arrays) into nbins bins
 // by absolute sample number; thread k of a CTA owns bin k (and k + 256, ...)
 // of its chunk of blocks, so every bin sum is formed in a fixed order.
-// decode_sample (above) gives the samples as the reference's unpacker does.
+// The samples are decoded as decode_sample (above) and the reference's unpacker do.
+
+// Sum of the decoded samples n = n0, n0 + step, ... < F of band bd of a
+// processed block, walking frame q and in-frame sample r incrementally (one
+// division per call, not per sample).
+__device__ __forceinline__ float2 sum_samples(const DevJob &J, const uint8_t *__restrict__ data,
+                                              const BlockParam &P, int bd, int n0, int step, const float *lut)
+{
+  float2 acc = make_float2(0.f, 0.f);
+  if (n0 >= J.fftlen) return acc;
+  const int fsamp = J.framesamples;
+  const int bits_ts = J.nbands * J.nbits * (J.cplx ? 2 : 1);
+  const int cmask = (1 << J.nbits) - 1;
+  const int bitband = bd * (J.cplx ? 2 : 1) * J.nbits;
+  const int smp0 = P.nearestsample + n0;
+  int q = smp0 / fsamp;
+  int r = smp0 - q * fsamp;
+  q -= P.fr0;
+  const int qstep = step / fsamp, rstep = step - qstep * fsamp;
+  for (int n = n0; n < J.fftlen; n += step) {
+    if ((P.validmask >> q) & 1ull) {
+      const uint8_t *payload = data + ((long long)P.fr0 + q) * J.framebytes + 32;
+      const int bit0 = r * bits_ts + bitband;
+      acc.x += lut[(__ldg(payload + (bit0 >> 3)) >> (bit0 & 7)) & cmask];
+      if (J.cplx) {
+        const int bit1 = bit0 + J.nbits;
+        acc.y += lut[(__ldg(payload + (bit1 >> 3)) >> (bit1 & 7)) & cmask];
+      }
+    }
+    q += qstep;
+    r += rstep;
+    if (r >= fsamp) {
+      r -= fsamp;
+      q++;
+    }
+  }
+  return acc;
+}
 
 __global__ void __launch_bounds__(256) pcal_bins_kernel(DevJob J, SubintArrays S, const BlockParam *__restrict__ bp,
                                                         int nblk, const PcalBand *__restrict__ bands, int chunks,
                                                         int maxbins, float2 *__restrict__ partial)
 {
   __shared__ float s_lut[256];
+  __shared__ float2 s_red[256];
   for (int i = threadIdx.x; i < 256; i += blockDim.x) s_lut[i] = J.lut[i];
   __syncthreads();
   const int c = blockIdx.x, pb = blockIdx.y;
   const PcalBand B = bands[pb];
-  const int s = B.station, N = B.nbins, F = J.fftlen;
+  const int s = B.station, N = B.nbins;
   if (N <= 0) return;
   const uint8_t *data = S.data[s];
   const int32_t *ctrl = S.control + (size_t)s * S.controlstride;
@@ -878,20 +916,119 @@ __global__ void __launch_bounds__(256) pcal_bins_kernel(DevJob J, SubintArrays S
   const int per = (nblk + chunks - 1) / chunks;
   const int b0 = c * per, b1 = min(nblk, b0 + per);
   float2 *out = partial + ((size_t)c * gridDim.y + pb) * maxbins;
-  for (int k = threadIdx.x; k < N; k += blockDim.x) {
+  const int tid = threadIdx.x, nth = blockDim.x;
+  if (N <= nth) {
+    // R threads per bin: thread (r, k) takes samples n = n0(k) + (r + R m) N; consecutive
+    // threads read consecutive samples
+    const int R = nth / N;
+    const int k = tid % N, r = tid / N;
     float2 acc = make_float2(0.f, 0.f);
-    for (int bi = b0; bi < b1; bi++) {
-      const BlockParam P = bp[(size_t)s * nblk + bi];
-      if (P.state == 0) continue;
-      const int idx0 = (int)((s0 + (unsigned long long)P.nearestsample) % (unsigned long long)N);
-      for (int n = (k - idx0 + N) % N; n < F; n += N) {
-        const float2 v = decode_sample(J, data, P, B.band, n, s_lut);
+    if (r < R) {
+      for (int bi = b0; bi < b1; bi++) {
+        const BlockParam P = bp[(size_t)s * nblk + bi];
+        if (P.state == 0) continue;
+        const int idx0 = (int)((s0 + (unsigned long long)P.nearestsample) % (unsigned long long)N);
+        const float2 v = sum_samples(J, data, P, B.band, (k - idx0 + N) % N + r * N, R * N, s_lut);
         acc.x += v.x;
         acc.y += v.y;
       }
     }
-    out[k].x += acc.x;
-    out[k].y += acc.y;
+    s_red[tid] = acc;
+    __syncthreads();
+    if (tid < N) {   // the R partial sums of bin k, in order
+      float2 sum = s_red[tid];
+      for (int q = 1; q < R; q++) {
+        sum.x += s_red[tid + q * N].x;
+        sum.y += s_red[tid + q * N].y;
+      }
+      out[tid].x += sum.x;
+      out[tid].y += sum.y;
+    }
+  } else {
+    for (int k = tid; k < N; k += nth) {   // more bins than threads: one thread per bin
+      float2 acc = make_float2(0.f, 0.f);
+      for (int bi = b0; bi < b1; bi++) {
+        const BlockParam P = bp[(size_t)s * nblk + bi];
+        if (P.state == 0) continue;
+        const int idx0 = (int)((s0 + (unsigned long long)P.nearestsample) % (unsigned long long)N);
+        const float2 v = sum_samples(J, data, P, B.band, (k - idx0 + N) % N, N, s_lut);
+        acc.x += v.x;
+        acc.y += v.y;
+      }
+      out[k].x += acc.x;
+      out[k].y += acc.y;
+    }
+  }
+}
+
+// The same bin sums for all nb bands of one station at once (all with N
+// bins): thread (r, k, b), b fastest, so that the threads of a warp read the
+// bands of the same time samples together -- each time sample's bytes are
+// fetched once for all its bands.
+__global__ void __launch_bounds__(512) pcal_station_kernel(DevJob J, SubintArrays S, const BlockParam *__restrict__ bp,
+                                                           int nblk, const PcalBand *__restrict__ bands, int nb,
+                                                           int chunks, int maxbins, int nbands_total,
+                                                           float2 *__restrict__ partial)
+{
+  __shared__ float s_lut[256];
+  __shared__ float2 s_red[512];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) s_lut[i] = J.lut[i];
+  __syncthreads();
+  const int c = blockIdx.x, first = blockIdx.y * nb;
+  const PcalBand B0 = bands[first];
+  const int s = B0.station, N = B0.nbins;
+  const uint8_t *data = S.data[s];
+  const int32_t *ctrl = S.control + (size_t)s * S.controlstride;
+  const unsigned long long s0 =
+      (unsigned long long)(((double)ctrl[1] * 1e9 + (double)ctrl[2]) / (J.sampletime * 1e3) + 0.5);
+  const int per = (nblk + chunks - 1) / chunks;
+  const int b0 = c * per, b1 = min(nblk, b0 + per);
+  const int tid = threadIdx.x, nth = blockDim.x, items = N * nb;
+  auto out = [&](int b, int k) -> float2 & { return partial[((size_t)c * nbands_total + first + b) * maxbins + k]; };
+  if (items <= nth) {
+    const int R = nth / items;
+    const int b = tid % nb, k = (tid / nb) % N, r = tid / items;
+    float2 acc = make_float2(0.f, 0.f);
+    if (r < R) {
+      const int bd = bands[first + b].band;
+      for (int bi = b0; bi < b1; bi++) {
+        const BlockParam P = bp[(size_t)s * nblk + bi];
+        if (P.state == 0) continue;
+        const int idx0 = (int)((s0 + (unsigned long long)P.nearestsample) % (unsigned long long)N);
+        const float2 v = sum_samples(J, data, P, bd, (k - idx0 + N) % N + r * N, R * N, s_lut);
+        acc.x += v.x;
+        acc.y += v.y;
+      }
+    }
+    s_red[tid] = acc;
+    __syncthreads();
+    if (tid < items) {   // the R partial sums of (band b, bin k), in order
+      float2 sum = s_red[tid];
+      for (int q = 1; q < R; q++) {
+        sum.x += s_red[tid + q * items].x;
+        sum.y += s_red[tid + q * items].y;
+      }
+      float2 &o = out(b, k);
+      o.x += sum.x;
+      o.y += sum.y;
+    }
+  } else {
+    for (int it = tid; it < items; it += nth) {
+      const int b = it % nb, k = it / nb;
+      const int bd = bands[first + b].band;
+      float2 acc = make_float2(0.f, 0.f);
+      for (int bi = b0; bi < b1; bi++) {
+        const BlockParam P = bp[(size_t)s * nblk + bi];
+        if (P.state == 0) continue;
+        const int idx0 = (int)((s0 + (unsigned long long)P.nearestsample) % (unsigned long long)N);
+        const float2 v = sum_samples(J, data, P, bd, (k - idx0 + N) % N, N, s_lut);
+        acc.x += v.x;
+        acc.y += v.y;
+      }
+      float2 &o = out(b, k);
+      o.x += acc.x;
+      o.y += acc.y;
+    }
   }
 }
 
@@ -925,11 +1062,15 @@ __global__ void __launch_bounds__(128) pcal_tones_kernel(const PcalBand *__restr
 }
 
 cudaError_t pcal_bins_launch(const DevJob &J, const SubintArrays &S, const BlockParam *bp, int nblk,
-                             const PcalBand *bands, int nbands, int chunks, int maxbins, float2 *partial,
-                             cudaStream_t st)
+                             const PcalBand *bands, int nbands, int per_station, int chunks, int maxbins,
+                             float2 *partial, cudaStream_t st)
 {
   if (nbands <= 0 || nblk <= 0) return cudaSuccess;
-  pcal_bins_kernel<<<dim3(chunks, nbands), 256, 0, st>>>(J, S, bp, nblk, bands, chunks, maxbins, partial);
+  if (per_station > 0)   // every station has per_station bands with the same bin count
+    pcal_station_kernel<<<dim3(chunks, nbands / per_station), 512, 0, st>>>(J, S, bp, nblk, bands, per_station,
+                                                                            chunks, maxbins, nbands, partial);
+  else
+    pcal_bins_kernel<<<dim3(chunks, nbands), 256, 0, st>>>(J, S, bp, nblk, bands, chunks, maxbins, partial);
   return cudaGetLastError();
 }
 

@@ -37,7 +37,7 @@ struct gx_handle {
   std::vector<gx::PcalBand> pcal;            // recorded bands with phase-cal extraction
   gx::PcalBand *d_pcal = nullptr;
   float2 *d_pcalbins = nullptr;              // [chunk][pcal band][bin] partial bin sums
-  int pcal_chunks = 0, pcal_maxbins = 0;
+  int pcal_chunks = 0, pcal_maxbins = 0, pcal_per_station = 0;
   std::vector<int> pc_off, pc_ntones;        // [station * GX_MAX_BANDS + band]: result index / tones
   std::vector<std::vector<double>> pc_tone_hz;   // [station * GX_MAX_BANDS + band]: tone frequencies (Hz)
   std::vector<int> pc_maxtones;              // [station]: most tones of a band (0: phase-cal off)
