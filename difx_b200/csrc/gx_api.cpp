@@ -607,6 +607,8 @@ static gx_status setup(gx_handle *h)
     else {
       double off = getenv("SYMMETRIC_8_BIT_VDIF") ? 127.5 : 128.0;
       for (int b = 0; b < 256; b++) lut[b] = (float)((b - off) / 3.3);
+      J.lut_offset = off;
+      J.lut_div = 3.3;
     }
     // Tensor-core operands: a power-of-two scale that brings the spectrum of
     // noise with the r.m.s. level of the decode table to an r.m.s. near 8, so
@@ -691,11 +693,11 @@ static gx_status setup(gx_handle *h)
     h->pcal_per_station = J.nbands;
     for (size_t i = 0; i < h->pcal.size(); i++)
       if (h->pcal.size() % J.nbands || h->pcal[i].nbins != h->pcal[0].nbins || h->pcal[i].nbins <= 0 ||
-          h->pcal[i].station != h->pcal[i - i % J.nbands].station)
+          h->pcal[i].station != h->pcal[i - i % J.nbands].station || h->pcal[i].band != (int)(i % J.nbands))
         h->pcal_per_station = 0;
-    if (h->pcal_per_station) {   // chunks for four waves of station CTAs
+    if (h->pcal_per_station) {   // chunks for about eight 256-thread CTAs per SM
       const long long ng = (long long)h->pcal.size() / J.nbands;
-      h->pcal_chunks = (int)std::max<long long>(1, std::min<long long>(std::max(1, h->chunk / 8), (4 * 148 + ng - 1) / ng));
+      h->pcal_chunks = (int)std::max<long long>(1, std::min<long long>(std::max(1, h->chunk / 8), (8 * 148 + ng - 1) / ng));
     }
     CKR(h, h->dalloc(&h->d_pcal, sizeof(PcalBand) * h->pcal.size()));
     CKR(h, cudaMemcpy(h->d_pcal, h->pcal.data(), sizeof(PcalBand) * h->pcal.size(), cudaMemcpyHostToDevice));

@@ -51,6 +51,7 @@ struct DevJob {
   double bw;              // MHz
   const float2 *twiddle;  // exp(-2 pi i m / F), m in [0, F)
   float lut[256];         // level of each sample code (VDIF decode table), staged to shared memory
+  double lut_offset, lut_div;   // 8-bit codes: level = (code - lut_offset) / lut_div
 };
 
 // Offset of (input row, channel c) inside the spectra of one (freq, block):

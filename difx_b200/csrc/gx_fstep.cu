@@ -961,19 +961,67 @@ __global__ void __launch_bounds__(256) pcal_bins_kernel(DevJob J, SubintArrays S
   }
 }
 
-// The same bin sums for all nb bands of one station at once (all with N
-// bins): thread (r, k, b), b fastest, so that the threads of a warp read the
-// bands of the same time samples together -- each time sample's bytes are
-// fetched once for all its bands.
-__global__ void __launch_bounds__(512) pcal_station_kernel(DevJob J, SubintArrays S, const BlockParam *__restrict__ bp,
+// The same bin sums for all nb bands of one station at once, for time samples
+// of W 32-bit words (W = 1: 8, 16 or 32 bits) holding bands 0..nb-1 in order.
+// Thread (r, k) reads whole time samples -- the threads of a warp read
+// consecutive ones, one wide load each -- and bins every band from registers.
+// 8-bit codes (NBITS 8; level = (code - offset) / div, an affine table) are
+// summed as integers: the fields of each word in two 16-bit lanes per
+// register (even and odd bytes), moved into 32-bit totals after each block
+// (at most 256 samples of a thread, so that no lane overflows), then
+// (sum - offset * count) / div in double once per bin.  Integer sums make the
+// result independent of the summation order.  Other widths look the level up
+// in a per-lane copy of the table (NBITS 0: width read at run time).
+constexpr int kPcalMaxBands = 16;
+
+template <int W>
+__device__ __forceinline__ uint4 load_timesample(const uint8_t *p, int align)
+{
+  if (W == 4 && align >= 16) return __ldg(reinterpret_cast<const uint4 *>(p));
+  if (W == 2 && align >= 8) {
+    const uint2 h = __ldg(reinterpret_cast<const uint2 *>(p));
+    return make_uint4(h.x, h.y, 0u, 0u);
+  }
+  uint32_t w[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+  for (int i = 0; i < W; i++)
+    w[i] = align >= 4 ? __ldg(reinterpret_cast<const uint32_t *>(p) + i)
+                      : (uint32_t)__ldg(p + 4 * i) | ((uint32_t)__ldg(p + 4 * i + 1) << 8) |
+                            ((uint32_t)__ldg(p + 4 * i + 2) << 16) | ((uint32_t)__ldg(p + 4 * i + 3) << 24);
+  return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+template <int W>
+__device__ __forceinline__ uint32_t word(const uint4 &w, int i)
+{
+  return (W > 3 && i == 3) ? w.w : (W > 2 && i == 2) ? w.z : (W > 1 && i == 1) ? w.y : w.x;
+}
+
+template <int W>
+__device__ __forceinline__ uint32_t field(const uint4 &w, int pos)
+{
+  return word<W>(w, pos >> 5) >> (pos & 31);
+}
+
+template <int W, int NBITS, int CPLX>
+__global__ void __launch_bounds__(256) pcal_station_kernel(DevJob J, SubintArrays S, const BlockParam *__restrict__ bp,
                                                            int nblk, const PcalBand *__restrict__ bands, int nb,
                                                            int chunks, int maxbins, int nbands_total,
                                                            float2 *__restrict__ partial)
 {
-  __shared__ float s_lut[256];
-  __shared__ float2 s_red[512];
-  for (int i = threadIdx.x; i < 256; i += blockDim.x) s_lut[i] = J.lut[i];
-  __syncthreads();
+  constexpr bool kInt = NBITS == 8;
+  // one copy of the decode table per lane, so that a warp's lookups of random
+  // codes never share a bank: entry v of lane l at v * 32 + l
+  extern __shared__ float s_lut32[];
+  __shared__ float2 s_red[256];
+  __shared__ int s_cnt[256];
+  const int nbits = NBITS ? NBITS : J.nbits;
+  const int cplx = NBITS ? CPLX : J.cplx;
+  if (!kInt) {
+    for (int i = threadIdx.x; i < (32 << nbits); i += blockDim.x) s_lut32[i] = J.lut[i >> 5];
+    __syncthreads();
+  }
+  const float *s_lut = s_lut32 + (threadIdx.x & 31);
   const int c = blockIdx.x, first = blockIdx.y * nb;
   const PcalBand B0 = bands[first];
   const int s = B0.station, N = B0.nbins;
@@ -983,51 +1031,134 @@ __global__ void __launch_bounds__(512) pcal_station_kernel(DevJob J, SubintArray
       (unsigned long long)(((double)ctrl[1] * 1e9 + (double)ctrl[2]) / (J.sampletime * 1e3) + 0.5);
   const int per = (nblk + chunks - 1) / chunks;
   const int b0 = c * per, b1 = min(nblk, b0 + per);
-  const int tid = threadIdx.x, nth = blockDim.x, items = N * nb;
-  auto out = [&](int b, int k) -> float2 & { return partial[((size_t)c * nbands_total + first + b) * maxbins + k]; };
-  if (items <= nth) {
-    const int R = nth / items;
-    const int b = tid % nb, k = (tid / nb) % N, r = tid / items;
-    float2 acc = make_float2(0.f, 0.f);
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int fsamp = J.framesamples, fb = J.framebytes;
+  const int bandbits = nbits * (cplx ? 2 : 1);
+  const int bits_ts = nb * bandbits;
+  const uint32_t cmask = (1u << nbits) - 1u;
+  const uint32_t tsmask = bits_ts >= 32 ? 0xffffffffu : (1u << bits_ts) - 1u;
+  // widest load every time sample start allows: the frame stride, the data
+  // base and the sample size all keep the alignment
+  int align = 16;
+  while (align > 1 && (((uintptr_t)data | (uintptr_t)fb | (uintptr_t)32) & (align - 1))) align >>= 1;
+  align = min(align, max(4, W * 4));
+  if (bits_ts < 32) align = ((uintptr_t)data & 3) || (fb & 3) ? 1 : 4;
+  for (int kb = 0; kb < N; kb += nth) {   // bins kb .. kb+nk-1 in this pass
+    const int nk = min(nth, N - kb);
+    const int R = nth / nk;
+    const int k = kb + tid % nk, r = tid / nk;
+    float ax[kPcalMaxBands], ay[kPcalMaxBands];
+    int tot[4 * W];   // 8-bit: per field (band-major, real then imaginary)
+    int cnt = 0;
+#pragma unroll
+    for (int b = 0; b < kPcalMaxBands; b++) ax[b] = ay[b] = 0.f;
+#pragma unroll
+    for (int f = 0; f < 4 * W; f++) tot[f] = 0;
     if (r < R) {
-      const int bd = bands[first + b].band;
+      const int step = R * N;
+      const int qstep = step / fsamp, rstep = step - qstep * fsamp;
       for (int bi = b0; bi < b1; bi++) {
         const BlockParam P = bp[(size_t)s * nblk + bi];
         if (P.state == 0) continue;
         const int idx0 = (int)((s0 + (unsigned long long)P.nearestsample) % (unsigned long long)N);
-        const float2 v = sum_samples(J, data, P, bd, (k - idx0 + N) % N + r * N, R * N, s_lut);
-        acc.x += v.x;
-        acc.y += v.y;
+        const int n0 = (k - idx0 + N) % N + r * N;
+        const int smp0 = P.nearestsample + n0;
+        int q = smp0 / fsamp;
+        int rr = smp0 - q * fsamp;
+        q -= P.fr0;
+        uint32_t pe[W], po[W];   // 8-bit: even / odd bytes of word i in 16-bit lanes
+#pragma unroll
+        for (int i = 0; i < W; i++) pe[i] = po[i] = 0u;
+        for (int n = n0; n < J.fftlen; n += step) {
+          if ((P.validmask >> q) & 1ull) {
+            const uint8_t *payload = data + ((long long)P.fr0 + q) * fb + 32;
+            uint4 w;
+            int sh = 0;
+            if (bits_ts < 32) {
+              const int bit = rr * bits_ts;
+              w = load_timesample<W>(payload + ((bit >> 5) << 2), align);
+              sh = bit & 31;
+            } else {
+              w = load_timesample<W>(payload + (size_t)rr * (W * 4), align);
+            }
+            if constexpr (kInt) {
+              cnt++;
+#pragma unroll
+              for (int i = 0; i < W; i++) {
+                const uint32_t x = W == 1 ? (w.x >> sh) & tsmask : word<W>(w, i);
+                pe[i] += x & 0x00ff00ffu;
+                po[i] += (x >> 8) & 0x00ff00ffu;
+              }
+            } else {
+#pragma unroll
+              for (int b = 0; b < kPcalMaxBands; b++) {
+                if (b < nb) {
+                  const int pos = b * bandbits + sh;
+                  ax[b] += s_lut[(field<W>(w, pos) & cmask) << 5];
+                  if (cplx) ay[b] += s_lut[(field<W>(w, pos + nbits) & cmask) << 5];
+                }
+              }
+            }
+          }
+          q += qstep;
+          rr += rstep;
+          if (rr >= fsamp) {
+            rr -= fsamp;
+            q++;
+          }
+        }
+        if constexpr (kInt) {   // fields 4i, 4i+2 in pe[i]; 4i+1, 4i+3 in po[i]
+#pragma unroll
+          for (int i = 0; i < W; i++) {
+            tot[4 * i] += (int)(pe[i] & 0xffffu);
+            tot[4 * i + 2] += (int)(pe[i] >> 16);
+            tot[4 * i + 1] += (int)(po[i] & 0xffffu);
+            tot[4 * i + 3] += (int)(po[i] >> 16);
+          }
+        }
       }
     }
-    s_red[tid] = acc;
-    __syncthreads();
-    if (tid < items) {   // the R partial sums of (band b, bin k), in order
-      float2 sum = s_red[tid];
-      for (int q = 1; q < R; q++) {
-        sum.x += s_red[tid + q * items].x;
-        sum.y += s_red[tid + q * items].y;
+    if constexpr (kInt) s_cnt[tid] = cnt;
+#pragma unroll
+    for (int b = 0; b < kPcalMaxBands; b++) {
+      if (b < nb) {
+        if constexpr (kInt) {
+          const int fr = b * (CPLX ? 2 : 1);   // this band's real field
+          int re = 0, im = 0;
+#pragma unroll
+          for (int f = 0; f < 4 * W; f++) {
+            if (f == fr) re = tot[f];
+            if (CPLX && f == fr + 1) im = tot[f];
+          }
+          s_red[tid] = make_float2(__int_as_float(re), __int_as_float(im));
+        } else {
+          s_red[tid] = make_float2(ax[b], ay[b]);
+        }
+        __syncthreads();
+        if (tid < nk) {   // the R partial sums of (band b, bin k), in order
+          float2 sum;
+          if constexpr (kInt) {
+            long long re = 0, im = 0, n = 0;
+            for (int qq = 0; qq < R; qq++) {
+              re += __float_as_int(s_red[tid + qq * nk].x);
+              im += __float_as_int(s_red[tid + qq * nk].y);
+              n += s_cnt[tid + qq * nk];
+            }
+            sum.x = (float)(((double)re - J.lut_offset * (double)n) / J.lut_div);
+            sum.y = CPLX ? (float)(((double)im - J.lut_offset * (double)n) / J.lut_div) : 0.f;
+          } else {
+            sum = s_red[tid];
+            for (int qq = 1; qq < R; qq++) {
+              sum.x += s_red[tid + qq * nk].x;
+              sum.y += s_red[tid + qq * nk].y;
+            }
+          }
+          float2 &o = partial[((size_t)c * nbands_total + first + b) * maxbins + k];
+          o.x += sum.x;
+          o.y += sum.y;
+        }
+        __syncthreads();
       }
-      float2 &o = out(b, k);
-      o.x += sum.x;
-      o.y += sum.y;
-    }
-  } else {
-    for (int it = tid; it < items; it += nth) {
-      const int b = it % nb, k = it / nb;
-      const int bd = bands[first + b].band;
-      float2 acc = make_float2(0.f, 0.f);
-      for (int bi = b0; bi < b1; bi++) {
-        const BlockParam P = bp[(size_t)s * nblk + bi];
-        if (P.state == 0) continue;
-        const int idx0 = (int)((s0 + (unsigned long long)P.nearestsample) % (unsigned long long)N);
-        const float2 v = sum_samples(J, data, P, bd, (k - idx0 + N) % N, N, s_lut);
-        acc.x += v.x;
-        acc.y += v.y;
-      }
-      float2 &o = out(b, k);
-      o.x += acc.x;
-      o.y += acc.y;
     }
   }
 }
@@ -1066,11 +1197,35 @@ cudaError_t pcal_bins_launch(const DevJob &J, const SubintArrays &S, const Block
                              float2 *partial, cudaStream_t st)
 {
   if (nbands <= 0 || nblk <= 0) return cudaSuccess;
-  if (per_station > 0)   // every station has per_station bands with the same bin count
-    pcal_station_kernel<<<dim3(chunks, nbands / per_station), 512, 0, st>>>(J, S, bp, nblk, bands, per_station,
-                                                                            chunks, maxbins, nbands, partial);
-  else
+  const int bits_ts = J.nbands * J.nbits * (J.cplx ? 2 : 1);
+  const dim3 grid(chunks, per_station > 0 ? nbands / per_station : 1);
+  const size_t lut_bytes = sizeof(float) * 32 * ((size_t)1 << J.nbits);   // at most 32 KB
+  // every station has per_station bands (0..per_station-1, in order) with the
+  // same bin count, and a time sample is 1, 2 or 4 words or divides a word;
+  // the 8-bit integer sums need at most 256 samples of a thread per block
+  // (the FFT length over the sample step R N, which is above 128)
+  const int W = bits_ts == 128 ? 4 : bits_ts == 64 ? 2 : (bits_ts <= 32 && 32 % bits_ts == 0) ? 1 : 0;
+  const bool station = per_station > 0 && per_station <= kPcalMaxBands && W > 0;
+  const bool i8 = J.nbits == 8 && J.fftlen <= 256 * 128;
+#define GX_PCAL_STATION(w, nbits, cplx)                                                                       \
+  pcal_station_kernel<w, nbits, cplx><<<grid, 256, nbits == 8 ? 0 : lut_bytes, st>>>(                         \
+      J, S, bp, nblk, bands, per_station, chunks, maxbins, nbands, partial)
+  if (station && i8) {
+    if (W == 4) { if (J.cplx) GX_PCAL_STATION(4, 8, 1); else GX_PCAL_STATION(4, 8, 0); }
+    else if (W == 2) { if (J.cplx) GX_PCAL_STATION(2, 8, 1); else GX_PCAL_STATION(2, 8, 0); }
+    else { if (J.cplx) GX_PCAL_STATION(1, 8, 1); else GX_PCAL_STATION(1, 8, 0); }
+  } else if (station && J.nbits == 2 && !J.cplx) {
+    if (W == 4) GX_PCAL_STATION(4, 2, 0);
+    else if (W == 2) GX_PCAL_STATION(2, 2, 0);
+    else GX_PCAL_STATION(1, 2, 0);
+  } else if (station && J.nbits != 8) {
+    if (W == 4) GX_PCAL_STATION(4, 0, 0);
+    else if (W == 2) GX_PCAL_STATION(2, 0, 0);
+    else GX_PCAL_STATION(1, 0, 0);
+  } else {
     pcal_bins_kernel<<<dim3(chunks, nbands), 256, 0, st>>>(J, S, bp, nblk, bands, chunks, maxbins, partial);
+  }
+#undef GX_PCAL_STATION
   return cudaGetLastError();
 }
 

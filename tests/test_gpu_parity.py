@@ -275,6 +275,19 @@ PCAL_CASES = {
     "c1_pcal": lambda: (jobs.spec_c1(name="c1pc", seed=81, pcal_interval_mhz=1), dict(invalid_frac=0.03)),
     "lsb_pcal": lambda: (jobs.spec_lsb(name="lsbpc", seed=82, pcal_interval_mhz=1), dict(invalid_frac=0.03)),
     "cplx8_pcal": lambda: (jobs.spec_cplx8(name="cx8pc", seed=83, pcal_interval_mhz=1), dict(invalid_frac=0.03)),
+    # 8 complex 8-bit bands: 16-byte time samples (the C3 sample format)
+    "cplx8_8band_pcal": lambda: (jobs.spec_cplx8(name="cx8pc8", seed=84, pcal_interval_mhz=1,
+                                                 subbands=[jobs.Subband(6000.0 + 16 * i, 16.0, "U", 256)
+                                                           for i in range(4)]), dict(invalid_frac=0.03)),
+    # 4-bit real and 2-bit complex: the decode width read at run time
+    "real4_pcal": lambda: (jobs.spec_long("r4pc", 4, "REAL", "U", 512, 86, pcal_interval_mhz=1),
+                           dict(invalid_frac=0.03)),
+    "cplx2_pcal": lambda: (jobs.spec_long("cx2pc", 2, "COMPLEX", "U", 128, 87, pcal_interval_mhz=1),
+                           dict(invalid_frac=0.03)),
+    # 16 2-bit real bands: 32-bit time samples
+    "real2_16band_pcal": lambda: (jobs.spec_c1(name="c1pc16", seed=85, nstations=3, pcal_interval_mhz=1,
+                                               subbands=[jobs.Subband(8400.0 + 16 * i, 16.0, "U", 128)
+                                                         for i in range(8)]), dict(invalid_frac=0.03)),
 }
 PCAL_TOL = 1e-4   # FP32 bin sums (tens of thousands of samples per bin) formed in another order
 
