@@ -289,6 +289,13 @@ def time_device(corr, sd_dev, dres, stream, steps, warmup, local, dist=None, clo
     return dev_ms, stage, launches, (clk.summary() if clk else None)
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) that ncu measured for
+# one fstep_r16_kernel launch on the C3 workload: 250 blocks x 64 stations
+# (profiles/fstep_r16_kernel_c3.md).  Traffic grows with the blocks a launch
+# processes, so a step's traffic is this per-block figure times its blocks.
+R16_C3_DRAM_BYTES_PER_BLOCK = 5.321e9 / 250
+
+
 def roofline(spec: JobSpec, xstep: str, stage, peaks):
     f_ms, x_ms, fin_ms = float(stage[0]), float(stage[1]), float(stage[2])
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
@@ -300,9 +307,13 @@ def roofline(spec: JobSpec, xstep: str, stage, peaks):
     if f_ms >= x_ms:
         k = "fstep_r16_kernel" if spec.fftchannels >= 512 else "fstep_warp_kernel"
         a = (in_bytes + spec_bytes) / (f_ms * 1e-3) / 1e9
+        traffic, tsrc = None, None
+        if spec.name == "bench_c3" and k == "fstep_r16_kernel":
+            traffic = R16_C3_DRAM_BYTES_PER_BLOCK * nblk
+            tsrc = "ncu DRAM bytes of one 250-block launch (16 ms subint), scaled to the step's blocks"
         return {"kernel": k, "bound": "hbm", "achieved": a, "peak": hbm_peak, "unit": "GB/s", "frac": a / hbm_peak,
-                "traffic": None, "peak_source": src, "algorithmic_bytes_per_step": in_bytes + spec_bytes,
-                "stage_ms": stages}
+                "traffic": traffic, "traffic_source": tsrc, "peak_source": src,
+                "algorithmic_bytes_per_step": in_bytes + spec_bytes, "stage_ms": stages}
     if xstep == "fp32":
         a = x_flops(spec) / (x_ms * 1e-3) / 1e12
         p = 148 * 128 * 2 * (peaks.get("sm_max_mhz", 1965.0) * 1e6) / 1e12

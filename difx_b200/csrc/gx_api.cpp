@@ -86,9 +86,11 @@ static gx_status setup(gx_handle *h)
   const gx_job_desc &d = h->jd;
   if (d.nstations < 1 || !d.stations || d.nfreqs < 1 || !d.freqs || d.nbaselines < 0)
     return h->fail(GX_ERR_ARG, "job descriptor: missing stations or freqs");
-  if (d.fringe_rotation_order != 1)
-    return h->fail(GX_ERR_UNSUPPORTED, "only FRINGE ROTN ORDER 1 is implemented");
+  if (d.fringe_rotation_order != 1 && d.fringe_rotation_order != 0)
+    return h->fail(GX_ERR_UNSUPPORTED, "FRINGE ROTN ORDER 2 (quadratic) is not implemented");
   const gx_station_desc &s0 = d.stations[0];
+  if (d.fringe_rotation_order == 0 && s0.is_complex)   // as the reference (mode.cpp:1131-1134)
+    return h->fail(GX_ERR_UNSUPPORTED, "post-F (0th order) fringe rotation is not supported for complex sampled data");
   for (int s = 0; s < d.nstations; s++) {
     const gx_station_desc &x = d.stations[s];
     if (x.nbits != s0.nbits || x.is_complex != s0.is_complex || x.framebytes != s0.framebytes ||
@@ -133,6 +135,7 @@ static gx_status setup(gx_handle *h)
   if (J.fftlen % J.stride) return h->fail(GX_ERR_ARG, "array stride does not divide the FFT length");
   J.nfr = J.fftlen / J.stride;
   if (J.stride & (J.stride - 1)) return h->fail(GX_ERR_UNSUPPORTED, "array stride must be a power of two");
+  J.fringe_order = d.fringe_rotation_order;
   J.lgstride = 0;
   while ((1 << J.lgstride) < J.stride) J.lgstride++;
   J.half = (cplx ? 2 * J.nfr : J.nfr) / 2;

@@ -47,6 +47,7 @@ struct DevJob {
   int blocks_per_send;
   int flaglen;
   int lgstride;           // log2(stride): FFT length, channels and stride are powers of two
+  int fringe_order;       // FRINGE ROTN ORDER: 1 pre-F linear, 0 post-F (real data)
   double sampletime;      // us
   double bw;              // MHz
   const float2 *twiddle;  // exp(-2 pi i m / F), m in [0, F)
@@ -64,7 +65,8 @@ __host__ __device__ __forceinline__ size_t spec_offset(const DevJob &J, int row,
 // Per (station, FFT block) parameters, computed in FP64 by blockparams_kernel
 // (mode.cpp:656-757, 782-799; mk5mode.cpp:94-174) and read by the F-step.
 struct __align__(16) BlockParam {
-  double a, b;                    // linear delay interpolation over the block (us), b without integer part
+  double a, b;                    // linear delay interpolation over the block (us), b without integer part;
+                                  // post-F rotation: a = 0, b = block-centre delay without its integer part
   double fracwalltime;
   unsigned long long validmask;   // bit q: frame fr0+q is valid
   int nearestsample, fr0, integerdelay, intwalltime;

@@ -186,6 +186,12 @@ __global__ void blockparams_kernel(DevJob J, SubintArrays S, int blk0, int nblk,
         if (P.weight > 0.0f) {
           P.state = 1;
           P.fracsampleerror = (float)(starttime - ns * J.sampletime);
+        }
+        if (P.weight > 0.0f && J.fringe_order == 0) {
+          // post-F: the integer part of the block-centre delay (mode.cpp:778-780)
+          P.integerdelay = (int)averagedelay;
+          P.b = averagedelay - P.integerdelay;
+        } else if (P.weight > 0.0f) {
           const double d0 = ip[0] * blk * blk + ip[1] * blk + ip[2];
           const double d1 = ip[0] * (blk + 0.5) * (blk + 0.5) + ip[1] * (blk + 0.5) + ip[2];
           const double d2 = ip[0] * (blk + 1) * (blk + 1) + ip[1] * (blk + 1) + ip[2];
@@ -211,6 +217,7 @@ __global__ void blockparams_kernel(DevJob J, SubintArrays S, int blk0, int nblk,
 __device__ __forceinline__ float2 fringe_entry(const DevJob &J, const DevStation &st, int fi, int e,
                                                const BlockParam &P)
 {
+  if (J.fringe_order == 0) return make_float2(1.0f, 0.0f);   // post-F: no rotation before the FFT
   const int Sd = J.stride, F = J.fftlen;
   const double lofreq = st.lofreq[fi];
   const double looffset = st.looff[fi];
@@ -257,7 +264,16 @@ __device__ __forceinline__ float2 frac_entry(const DevJob &J, const DevStation &
     cfreq = st.lsb[fi] ? (float)((-GX_TWO_PI * ((half - j) * Sd) * J.bw) / N)
                        : (float)((GX_TWO_PI * j * Sd * J.bw) / N);
   }
-  const float arg = __fmul_rn(cfreq, val);
+  float arg = __fmul_rn(cfreq, val);
+  if (J.fringe_order == 0 && e < Sd) {
+    // post-F fringe rotation (and LO offset) at the block centre, added to
+    // the first stride's argument for both polarisation sets (mode.cpp:1038-1049, 1085-1096)
+    const double lofreq = st.lofreq[fi];
+    double ph = P.b * lofreq;
+    if (st.fractional_lo) ph += P.integerdelay * (lofreq - (int)lofreq);
+    ph -= ((double)P.intwalltime + P.fracwalltime) * st.looff[fi];
+    arg = __fadd_rn(arg, (float)(-GX_TWO_PI * (ph - (int)ph)));
+  }
   float sn, cs;
   sincosf(arg, &sn, &cs);
   return make_float2(cs, sn);

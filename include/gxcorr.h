@@ -122,7 +122,7 @@ typedef struct gx_job_desc {
   const gx_baseline_desc *baselines;
   int subint_ns;           /* SUBINT NANOSECONDS */
   int guard_ns;            /* GUARD NANOSECONDS */
-  int fringe_rotation_order; /* FRINGE ROTN ORDER (1 supported) */
+  int fringe_rotation_order; /* FRINGE ROTN ORDER: 1 (linear, pre-F) or 0 (post-F, real-sampled data) */
   int array_stride;        /* ARRAY STRIDE LEN, 0 = automatic */
   int xmac_stride;         /* XMAC STRIDE LEN, 0 = automatic */
   int write_autocorrs;     /* WRITE AUTOCORRS (also enables cross-pol autocorrelations) */

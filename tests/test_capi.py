@@ -75,6 +75,7 @@ def test_host_only_handle_layout():
 
 @pytest.mark.parametrize("mutate,status", [
     (lambda d: setattr(d.desc, "fringe_rotation_order", 2), 2),
+    (lambda d: setattr(d.desc, "fringe_rotation_order", 3), 2),
     (lambda d: setattr(d.desc, "subint_ns", 8_000_001), 1),
     (lambda d: setattr(d._st[1], "nbits", 8), 2),
 ])
@@ -84,6 +85,16 @@ def test_bad_descriptors_are_rejected(mutate, status):
     with pytest.raises(gxcorr.GxError) as ei:
         gxcorr.Correlator.from_desc(jd, device=-1)
     assert ei.value.status == status
+
+
+def test_post_f_rotation_refused_for_complex_data():
+    """Post-F (0th order) fringe rotation is real-data only (mode.cpp:1131-1134)."""
+    jd = capi.job_desc_from_spec(jobs.spec_cplx8(fringe_rot_order=0))
+    with pytest.raises(gxcorr.GxError) as ei:
+        gxcorr.Correlator.from_desc(jd, device=-1)
+    assert ei.value.status == 2
+    c = gxcorr.Correlator.from_desc(capi.job_desc_from_spec(jobs.spec_c1(fringe_rot_order=0)), device=-1)
+    c.close()
 
 
 def test_tensor_core_xstep_limits():

@@ -224,6 +224,35 @@ def test_gpu_async_pipeline_matches_sync(gx):
     c.close()
 
 
+POSTF_CASES = {
+    # fractional-MHz LOs exercise the integer-delay term of the post-F phase
+    "c1_postf": lambda: (jobs.spec_c1(name="c1pf", seed=91, fringe_rot_order=0, subbands=[
+        jobs.Subband(8400.25 + 16 * i, 16.0, "U", 128) for i in range(4)]), dict(invalid_frac=0.02)),
+    "lsb_postf": lambda: (jobs.spec_lsb(name="lsbpf", seed=92, fringe_rot_order=0), dict(invalid_frac=0.02)),
+    "long_postf": lambda: (jobs.spec_long("r2pf", 2, "REAL", "U", 1024, 93, fringe_rot_order=0),
+                           dict(invalid_frac=0.02)),
+}
+
+
+@pytest.mark.skipif(not pyoracle.reference_available(), reason="reference harness not built")
+@pytest.mark.parametrize("case", sorted(POSTF_CASES))
+def test_gpu_post_f_fringe_rotation_matches_reference(case, gx, oracle_lib):
+    """FRINGE ROTN ORDER 0 (post-F): no rotation before the FFT, the fringe
+    phase at the block centre added to the fractional-sample rotator's first
+    stride (mode.cpp:778-780, 1038-1049, 1131-1159), against the compiled
+    reference reading the same .input, two subints."""
+    spec, kw = POSTF_CASES[case]()
+    prep = jobs.prepare(spec, [100_000_000, 108_000_000], **kw)
+    c = gx.Correlator.from_desc(prep.jd)
+    for i, sd in enumerate(prep.sds):
+        g = c.subint(sd)
+        r = jobs.reference_for(prep.paths["input"]).process(prep.subs[i])
+        assert g.shape == r.shape
+        m, wrel = _compare(g, r, prep.jd, spec, oracle_lib, layout=c.offsets())
+        assert m < REC_TOL and wrel < W_TOL, (m, wrel)
+    c.close()
+
+
 AVG_CASES = {
     "c1_avg4": lambda: (jobs.spec_c1(name="c1avg", seed=61, chans_to_avg=4), dict(invalid_frac=0.03)),
     "cplx8_avg8": lambda: (jobs.spec_cplx8(name="cx8avg", seed=62, chans_to_avg=8), dict(invalid_frac=0.03)),
