@@ -86,8 +86,8 @@ static gx_status setup(gx_handle *h)
   const gx_job_desc &d = h->jd;
   if (d.nstations < 1 || !d.stations || d.nfreqs < 1 || !d.freqs || d.nbaselines < 0)
     return h->fail(GX_ERR_ARG, "job descriptor: missing stations or freqs");
-  if (d.fringe_rotation_order != 1 && d.fringe_rotation_order != 0)
-    return h->fail(GX_ERR_UNSUPPORTED, "FRINGE ROTN ORDER 2 (quadratic) is not implemented");
+  if (d.fringe_rotation_order < 0 || d.fringe_rotation_order > 2)
+    return h->fail(GX_ERR_UNSUPPORTED, "FRINGE ROTN ORDER must be 0, 1 or 2");
   const gx_station_desc &s0 = d.stations[0];
   if (d.fringe_rotation_order == 0 && s0.is_complex)   // as the reference (mode.cpp:1131-1134)
     return h->fail(GX_ERR_UNSUPPORTED, "post-F (0th order) fringe rotation is not supported for complex sampled data");

@@ -47,7 +47,7 @@ struct DevJob {
   int blocks_per_send;
   int flaglen;
   int lgstride;           // log2(stride): FFT length, channels and stride are powers of two
-  int fringe_order;       // FRINGE ROTN ORDER: 1 pre-F linear, 0 post-F (real data)
+  int fringe_order;       // FRINGE ROTN ORDER: 1 pre-F linear, 2 pre-F quadratic, 0 post-F (real data)
   double sampletime;      // us
   double bw;              // MHz
   const float2 *twiddle;  // exp(-2 pi i m / F), m in [0, F)
@@ -66,7 +66,9 @@ __host__ __device__ __forceinline__ size_t spec_offset(const DevJob &J, int row,
 // (mode.cpp:656-757, 782-799; mk5mode.cpp:94-174) and read by the F-step.
 struct __align__(16) BlockParam {
   double a, b;                    // linear delay interpolation over the block (us), b without integer part;
-                                  // post-F rotation: a = 0, b = block-centre delay without its integer part
+                                  // post-F rotation: a = 0, b = block-centre delay without its integer part;
+                                  // quadratic: a = first-stride slope, b = delay at the block start
+  double qa, qb;                  // quadratic: curvature and slope of the delay at the block start
   double fracwalltime;
   unsigned long long validmask;   // bit q: frame fr0+q is valid
   int nearestsample, fr0, integerdelay, intwalltime;

@@ -141,7 +141,7 @@ __global__ void blockparams_kernel(DevJob J, SubintArrays S, int blk0, int nblk,
   BlockParam P;
   P.state = 0;
   P.weight = 0.0f;
-  P.a = P.b = P.fracwalltime = 0.0;
+  P.a = P.b = P.qa = P.qb = P.fracwalltime = 0.0;
   P.validmask = 0ull;
   P.nearestsample = P.fr0 = P.integerdelay = P.intwalltime = P.nframes = 0;
   P.fracsampleerror = 0.0f;
@@ -191,6 +191,19 @@ __global__ void blockparams_kernel(DevJob J, SubintArrays S, int blk0, int nblk,
           // post-F: the integer part of the block-centre delay (mode.cpp:778-780)
           P.integerdelay = (int)averagedelay;
           P.b = averagedelay - P.integerdelay;
+        } else if (P.weight > 0.0f && J.fringe_order == 2) {
+          // quadratic (mode.cpp:800-825): delay, slope and curvature at the block start
+          const double qa = ip[0];
+          const double qb = ip[1] + blk * ip[0] * 2.0;
+          double c = ip[2] + blk * ip[1] + blk * blk * ip[0];
+          const int idelay = int(c);
+          c -= idelay;
+          const double stepxoff1 = double(J.stride) / double(F);
+          P.a = qb + qa * stepxoff1;
+          P.b = c;
+          P.qa = qa;
+          P.qb = qb;
+          P.integerdelay = idelay;
         } else if (P.weight > 0.0f) {
           const double d0 = ip[0] * blk * blk + ip[1] * blk + ip[2];
           const double d1 = ip[0] * (blk + 0.5) * (blk + 0.5) + ip[1] * (blk + 0.5) + ip[2];
@@ -236,11 +249,18 @@ __device__ __forceinline__ float2 fringe_entry(const DevJob &J, const DevStation
       if (looffset < 0) fl = -fl;
       if (isfrac) ph += -fl * P.intwalltime;
     }
-  } else {
+  } else if (e < Sd + J.nfr) {
     const int j = e - Sd;
-    const double x = ((double)(j * Sd) / (double)F) * P.a;
+    const double xoff = (double)(j * Sd) / (double)F;
+    // quadratic: stepxoff b + stepxoff^2 a (mode.cpp:813-819)
+    const double x = J.fringe_order == 2 ? xoff * P.qb + (xoff * xoff) * P.qa : xoff * P.a;
     ph = x * lofreq;
     if (looff) ph += ((j * Sd * J.sampletime) / 1e6) * -looffset;
+  } else {
+    // quadratic only: the per-stride phase step of sub entry k (mode.cpp:810-812)
+    const int k = e - Sd - J.nfr;
+    const double x = ((double)k / (double)F) * (2 * P.qa * ((double)Sd / (double)F));
+    ph = x * lofreq;
   }
   const float arg = (float)(-GX_TWO_PI * (ph - (int)ph));
   float sn, cs;
@@ -498,6 +518,8 @@ fstep_cta_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays
   float2 *rstep = rsub + nrf * Sd;                           // nrf * nfr
   float2 *fsub = rstep + nrf * nfr;                          // 2 * nrf * S
   float2 *fstep = fsub + 2 * nrf * Sd;                       // 2 * nrf * half
+  float2 *rquad = fstep + 2 * nrf * (half > 0 ? half : 1);  // nrf * S (quadratic order)
+  const bool quad = J.fringe_order == 2;
 
   const int tps = kFThreads / nslots;
   const int myslot = tid / tps;
@@ -517,11 +539,13 @@ fstep_cta_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays
       }
       continue;
     }
-    for (int idx = tid; idx < nrf * (Sd + nfr); idx += blockDim.x) {
-      const int fi = idx / (Sd + nfr), e = idx % (Sd + nfr);
+    const int nfe = Sd + nfr + (quad ? Sd : 0);
+    for (int idx = tid; idx < nrf * nfe; idx += blockDim.x) {
+      const int fi = idx / nfe, e = idx % nfe;
       const float2 v = fringe_entry(J, st, fi, e, P);
       if (e < Sd) rsub[fi * Sd + e] = v;
-      else rstep[fi * nfr + e - Sd] = v;
+      else if (e < Sd + nfr) rstep[fi * nfr + e - Sd] = v;
+      else rquad[fi * Sd + e - Sd - nfr] = v;
     }
     const int npolsets = st.deltapol ? 2 : 1;
     for (int idx = tid; idx < npolsets * nrf * (Sd + half); idx += blockDim.x) {
@@ -543,10 +567,27 @@ fstep_cta_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays
         lf = st.band_localfreq[bd];
         const float2 *rs = rsub + lf * Sd;
         const float2 *rp = rstep + lf * nfr;
+        if (quad) {
+          // quadratic rotator (mode.cpp:996-1005) into bufB: stride j of entry k is
+          // sub[k] quad[k]^j step[j], the powers formed by repeated FP32 products
+          const float2 *rq = rquad + lf * Sd;
+          for (int k = lt; k < Sd; k += tps) {
+            float2 pw = rs[k];
+            for (int j = 0; j < nfr; j++) {
+              bufB[j * Sd + k] = cmul_exact(pw, rp[j]);
+              pw = cmul_exact(rq[k], pw);
+            }
+          }
+        }
+      }
+      __syncthreads();
+      if (active) {
+        const float2 *rs = rsub + lf * Sd;
+        const float2 *rp = rstep + lf * nfr;
         for (int n = lt; n < F; n += tps) {
           const float2 u = decode_sample(J, data, P, bd, n, s_lut);
           const int k = n % Sd, j = n / Sd;
-          const float2 rot = (j == 0) ? rs[k] : cmul_exact(rs[k], rp[j]);
+          const float2 rot = quad ? bufB[n] : (j == 0) ? rs[k] : cmul_exact(rs[k], rp[j]);
           bufA[n] = J.cplx ? cmul(rot, u) : make_float2(u.x * rot.x, u.x * rot.y);
         }
       }
@@ -829,7 +870,9 @@ fstep_r16_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays
 }
 
 // --------------------------------------------------------------------------
-static bool use_warp_kernel(const DevJob &J) { return J.fftlen >= 128 && J.fftlen <= 1024; }
+// The warp and radix-16 kernels hold the fringe rotator as two tables
+// (sub[k] step[j]); the quadratic order needs the full table of the CTA kernel.
+static bool use_warp_kernel(const DevJob &J) { return J.fftlen >= 128 && J.fftlen <= 1024 && J.fringe_order != 2; }
 
 static int warp_stride(const DevJob &J)
 {
@@ -842,7 +885,7 @@ static bool use_r16_kernel(const DevJob &J)
 {
   const char *e = getenv("GX_FSTEP_R16_MIN");   // smallest length routed to it (tuning runs)
   const int fmin = e ? atoi(e) : 512;
-  return J.fftlen >= fmin && J.fftlen >= 512 && J.fftlen <= 8192;
+  return J.fftlen >= fmin && J.fftlen >= 512 && J.fftlen <= 8192 && J.fringe_order != 2;
 }
 
 static int r16_tabstride(const DevJob &J)
@@ -864,6 +907,7 @@ size_t fstep_smem_bytes(const DevJob &J, int nrf, int nslots)
   size_t b = (size_t)nslots * 2 * J.fftlen * sizeof(float2);
   b += (size_t)nrf * (J.stride + J.nfr) * sizeof(float2);
   b += (size_t)2 * nrf * (J.stride + (J.half > 0 ? J.half : 1)) * sizeof(float2);
+  b += (size_t)nrf * J.stride * sizeof(float2);   // quadratic per-stride steps
   return b;
 }
 

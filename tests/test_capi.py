@@ -74,8 +74,8 @@ def test_host_only_handle_layout():
 
 
 @pytest.mark.parametrize("mutate,status", [
-    (lambda d: setattr(d.desc, "fringe_rotation_order", 2), 2),
     (lambda d: setattr(d.desc, "fringe_rotation_order", 3), 2),
+    (lambda d: setattr(d.desc, "fringe_rotation_order", -1), 2),
     (lambda d: setattr(d.desc, "subint_ns", 8_000_001), 1),
     (lambda d: setattr(d._st[1], "nbits", 8), 2),
 ])

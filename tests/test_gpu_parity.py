@@ -224,24 +224,34 @@ def test_gpu_async_pipeline_matches_sync(gx):
     c.close()
 
 
-POSTF_CASES = {
+ORDER_CASES = {
     # fractional-MHz LOs exercise the integer-delay term of the post-F phase
     "c1_postf": lambda: (jobs.spec_c1(name="c1pf", seed=91, fringe_rot_order=0, subbands=[
         jobs.Subband(8400.25 + 16 * i, 16.0, "U", 128) for i in range(4)]), dict(invalid_frac=0.02)),
     "lsb_postf": lambda: (jobs.spec_lsb(name="lsbpf", seed=92, fringe_rot_order=0), dict(invalid_frac=0.02)),
     "long_postf": lambda: (jobs.spec_long("r2pf", 2, "REAL", "U", 1024, 93, fringe_rot_order=0),
                            dict(invalid_frac=0.02)),
+    # FRINGE ROTN ORDER 2 (quadratic, pre-F)
+    "c1_quad": lambda: (jobs.spec_c1(name="c1q", seed=94, fringe_rot_order=2, subbands=[
+        jobs.Subband(8400.25 + 16 * i, 16.0, "U", 128) for i in range(4)]), dict(invalid_frac=0.02)),
+    "lsb_quad": lambda: (jobs.spec_lsb(name="lsbq", seed=95, fringe_rot_order=2), dict(invalid_frac=0.02)),
+    "cplx8_quad": lambda: (jobs.spec_cplx8(name="cx8q", seed=96, fringe_rot_order=2), dict(invalid_frac=0.02)),
+    "cplx8_4096_quad": lambda: (jobs.spec_long("cx8lq", 8, "COMPLEX", "U", 4096, 97, fringe_rot_order=2),
+                                dict(invalid_frac=0.02)),
 }
 
 
 @pytest.mark.skipif(not pyoracle.reference_available(), reason="reference harness not built")
-@pytest.mark.parametrize("case", sorted(POSTF_CASES))
-def test_gpu_post_f_fringe_rotation_matches_reference(case, gx, oracle_lib):
+@pytest.mark.parametrize("case", sorted(ORDER_CASES))
+def test_gpu_fringe_rotation_orders_match_reference(case, gx, oracle_lib):
     """FRINGE ROTN ORDER 0 (post-F): no rotation before the FFT, the fringe
     phase at the block centre added to the fractional-sample rotator's first
-    stride (mode.cpp:778-780, 1038-1049, 1131-1159), against the compiled
-    reference reading the same .input, two subints."""
-    spec, kw = POSTF_CASES[case]()
+    stride (mode.cpp:778-780, 1038-1049, 1131-1159).  ORDER 2 (quadratic):
+    delay, slope and curvature at the block start (800-825), rotator
+    sub[k] quad[k]^j step[j] with the powers as repeated FP32 products
+    (956-1005).  Against the compiled reference reading the same .input, two
+    subints."""
+    spec, kw = ORDER_CASES[case]()
     prep = jobs.prepare(spec, [100_000_000, 108_000_000], **kw)
     c = gx.Correlator.from_desc(prep.jd)
     for i, sd in enumerate(prep.sds):
