@@ -44,7 +44,8 @@ class gx_station_desc(C.Structure):
                 ("band_localfreq", C.c_int * GX_MAX_BANDS),
                 ("band_pol", C.c_char * GX_MAX_BANDS),
                 ("clock_int_seconds", C.c_int),
-                ("phase_cal_interval_hz", C.c_longlong), ("phase_cal_base_hz", C.c_longlong)]
+                ("phase_cal_interval_hz", C.c_longlong), ("phase_cal_base_hz", C.c_longlong),
+                ("interlaced", C.c_int)]
 
 
 class gx_baseline_desc(C.Structure):
@@ -143,6 +144,7 @@ def job_desc_from_spec(spec: JobSpec, xstep: int = GX_XSTEP_FP32, max_data_bytes
         c0 = spec.clock_us[s] if s < len(spec.clock_us) else 0.0
         st.clock_int_seconds = int(math.floor(c0 / 1e6 + 0.5))
         st.phase_cal_interval_hz = int(1e6 * spec.pcal_interval_mhz)
+        st.interlaced = 1 if spec.mux_threads > 0 else 0
         stations.append(st)
     baselines = []
     for a in range(spec.nstations):

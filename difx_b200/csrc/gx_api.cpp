@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <string>
 #include <vector>
@@ -204,6 +205,18 @@ static gx_status setup(gx_handle *h)
       h->band_input[s][b] = D.band_input[b];
     }
     for (int b = 0; b < x.nbands; b++) D.band_polb[b] = (D.deltapol && x.band_pol[b] != 'R') ? 1 : 0;
+  }
+  // INTERLACEDVDIF stations: one weight row per band after the station rows
+  h->interlaced_any = false;
+  h->nwrows = d.nstations;
+  for (int s = 0; s < d.nstations; s++) {
+    if (!d.stations[s].interlaced) continue;
+    if (d.stations[s].nbands > 30)   // the blanker's int-width thread masks (format_vdif.c:8509, 8530)
+      return h->fail(GX_ERR_UNSUPPORTED, "INTERLACEDVDIF with more than 30 bands is not implemented");
+    h->interlaced_any = true;
+    dst[s].interlaced = 1;
+    dst[s].wrow0 = h->nwrows;
+    h->nwrows += d.stations[s].nbands;
   }
   int ni = 0;
   for (int f = 0; f < d.nfreqs; f++) ni = count[f] > ni ? count[f] : ni;
@@ -446,8 +459,24 @@ static gx_status setup(gx_handle *h)
     const gx_baseline_desc &B = d.baselines[j];
     if (B.ds1 < 0 || B.ds1 >= d.nstations || B.ds2 < 0 || B.ds2 >= d.nstations)
       return h->fail(GX_ERR_ARG, "baseline datastream index out of range");
-    h->pairs.push_back(make_int2(B.ds1, B.ds2));
+    if (!h->interlaced_any) h->pairs.push_back(make_int2(B.ds1, B.ds2));
   }
+  // Weight sums: item i < nstations sums station row i; item nstations + k
+  // is pairs[k]: the product of rows (x, y) summed over blocks, or row x
+  // alone when y < 0.  Rows of interlaced stations are per band: the
+  // reference's getDataWeight(band) and perbandweights (core.cpp:911-912,
+  // 1039-1044; mode.cpp:1277-1284, 1342-1351).
+  std::map<std::pair<int, int>, int> witem;
+  auto wrow = [&](int s, int b) { return d.stations[s].interlaced ? dst[s].wrow0 + b : s; };
+  auto item = [&](int r1, int r2) -> int {
+    if (r2 < 0 && r1 < d.nstations) return r1;
+    auto it = witem.find({r1, r2});
+    if (it != witem.end()) return it->second;
+    const int idx = d.nstations + (int)h->pairs.size();
+    h->pairs.push_back(make_int2(r1, r2));
+    witem[{r1, r2}] = idx;
+    return idx;
+  };
   for (int f = 0; f < d.nfreqs; f++) {
     for (int j = 0; j < nbl; j++) {
       const gx_baseline_desc &B = d.baselines[j];
@@ -461,7 +490,7 @@ static gx_status setup(gx_handle *h)
         add_prod(h->blofs_full[f * nbl + j] + (long long)p * J.nchan, f, a, bb);
         WeightEntry w{};
         w.float_index = 2LL * h->bwofs_full[f * nbl + j] + p;
-        w.source = d.nstations + j;
+        w.source = h->interlaced_any ? item(wrow(B.ds1, b1), wrow(B.ds2, b2)) : d.nstations + j;
         h->wents.push_back(w);
       }
     }
@@ -481,7 +510,7 @@ static gx_status setup(gx_handle *h)
       ro += J.nchan;
       WeightEntry w{};
       w.float_index = wo++;
-      w.source = s;
+      w.source = item(wrow(s, b), -1);
       h->wents.push_back(w);
     }
     if (writecross) {
@@ -498,7 +527,7 @@ static gx_status setup(gx_handle *h)
         int partner = (b == i0) ? i1 : ((b == i1) ? i0 : -1);
         WeightEntry w{};
         w.float_index = wo++;
-        w.source = partner >= 0 ? s : -1;
+        w.source = partner < 0 ? -1 : x.interlaced ? item(wrow(s, i0), wrow(s, i1)) : s;
         h->wents.push_back(w);
         if (partner >= 0) add_prod(ro, f, h->band_input[s][b], h->band_input[s][partner]);
         ro += J.nchan;
@@ -645,8 +674,10 @@ static gx_status setup(gx_handle *h)
   CKR(h, cudaMemsetAsync(h->d_spec, 0, sizeof(float2) * spec_elems, h->stream));
   CKR(h, h->dalloc(&h->d_spec1, sizeof(float2) * (size_t)d.nfreqs * J.ninputs * J.nchan));
   CKR(h, cudaMemsetAsync(h->d_spec1, 0, sizeof(float2) * (size_t)d.nfreqs * J.ninputs * J.nchan, h->stream));
-  CKR(h, h->dalloc(&h->d_w, sizeof(float) * (size_t)d.nstations * chunk));
-  CKR(h, h->dalloc(&h->d_w1, sizeof(float) * (size_t)d.nstations));
+  CKR(h, h->dalloc(&h->d_w, sizeof(float) * (size_t)h->nwrows * chunk));
+  CKR(h, h->dalloc(&h->d_w1, sizeof(float) * (size_t)h->nwrows));
+  if (h->interlaced_any)
+    CKR(h, h->dalloc(&h->d_bandmask, sizeof(unsigned long long) * (size_t)d.nstations * chunk * J.nbands));
   CKR(h, h->dalloc(&h->d_bp, sizeof(BlockParam) * (size_t)d.nstations * chunk));
   CKR(h, h->dalloc(&h->d_bp1, sizeof(BlockParam) * (size_t)d.nstations));
   if (h->tc) {
@@ -672,10 +703,11 @@ static gx_status setup(gx_handle *h)
   CKR(h, cudaMemset(h->d_err, 0, sizeof(int)));
   CKR(h, cudaMallocHost(&h->h_err, sizeof(int) * gx_handle::kSlots));
   for (int k = 0; k < gx_handle::kSlots; k++) h->h_err[k] = 0;
-  CKR(h, h->dalloc(&h->d_wacc, sizeof(float) * (d.nstations + nbl)));
-  if (nbl) {
-    CKR(h, h->dalloc(&h->d_pairs, sizeof(int2) * nbl));
-    CKR(h, cudaMemcpy(h->d_pairs, h->pairs.data(), sizeof(int2) * nbl, cudaMemcpyHostToDevice));
+  const size_t npairs = h->pairs.size();
+  CKR(h, h->dalloc(&h->d_wacc, sizeof(float) * (d.nstations + npairs)));
+  if (npairs) {
+    CKR(h, h->dalloc(&h->d_pairs, sizeof(int2) * npairs));
+    CKR(h, cudaMemcpy(h->d_pairs, h->pairs.data(), sizeof(int2) * npairs, cudaMemcpyHostToDevice));
   }
   CKR(h, h->dalloc(&h->d_prods, sizeof(ProdEntry) * std::max<size_t>(1, h->prods.size())));
   if (!h->prods.empty())
@@ -759,6 +791,7 @@ gx_status plan_job(const gx_job_desc *desc, JobPlan *plan, std::string &err)
   if (s != GX_OK) { err = h.err; return s; }
   if (h.avg > 1) { err = "channel averaging is not implemented by the allocation-free entry point"; return GX_ERR_UNSUPPORTED; }
   if (!h.pcal.empty()) { err = "phase-cal extraction is not implemented by the allocation-free entry point"; return GX_ERR_UNSUPPORTED; }
+  if (h.interlaced_any) { err = "INTERLACEDVDIF is not implemented by the allocation-free entry point"; return GX_ERR_UNSUPPORTED; }
   plan->J = h.J;
   plan->J.twiddle = nullptr;
   plan->maxnrf = h.maxnrf;
@@ -952,6 +985,7 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
   S.control = reinterpret_cast<const int32_t *>(h->d_sub + h->o_ctrl);
   S.controlstride = h->ctrlstride;
   S.interp = reinterpret_cast<const double *>(h->d_sub + h->o_interp);
+  S.bandmask = h->d_bandmask;
   h->last = S;
   h->have_last = true;
 
@@ -960,7 +994,8 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
   auto mark = [&](int stage, bool start) -> gx_status { return timed ? record(h, st, stage, start) : GX_OK; };
   // the tensor-core X-step stores its first chunk instead of adding to it
   if (!h->tc) CKR(h, cudaMemsetAsync(h->d_acc, 0, sizeof(float2) * h->acc_slice * h->ks, st));
-  CKR(h, cudaMemsetAsync(h->d_wacc, 0, sizeof(float) * (d.nstations + nbl), st));
+  const int npairs = (int)h->pairs.size();
+  CKR(h, cudaMemsetAsync(h->d_wacc, 0, sizeof(float) * (d.nstations + npairs), st));
   CKR(h, cudaMemsetAsync(h->d_err, 0, sizeof(int), st));
   const int npc = (int)h->pcal.size();
   if (npc)
@@ -982,7 +1017,7 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
                             b0 > 0 ? 1 : 0, h->d_err, st));
     else
       CKR(h, xmac_fp32_launch(h->d_spec, nb, J.ninputs, J.nchan, d.nfreqs, h->ks, h->d_acc, st));
-    CKR(h, weights_launch(h->d_w, nb, d.nstations, h->d_pairs, nbl, h->d_wacc, st));
+    CKR(h, weights_launch(h->d_w, nb, d.nstations, h->d_pairs, npairs, h->d_wacc, st));
     if ((r = mark(1, false)) != GX_OK) return r;
     h->launches += 3;
   }

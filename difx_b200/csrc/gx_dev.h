@@ -18,6 +18,8 @@ struct DevStation {
   int nrecfreqs;
   int fractional_lo;      // Mode::fractionalLoFreq (mode.cpp:86-102)
   int deltapol;           // any CLK OFFSET delta != 0 (mode.cpp:335-343)
+  int interlaced;         // INTERLACEDVDIF: EDV4 per-band validity and weights (mk5mode.cpp:142-163)
+  int wrow0;              // interlaced: weight row of band 0 (rows wrow0 .. wrow0 + nbands - 1)
   int pad_;
   double lofreq[kMaxFreqsPerStation];      // LO used for fringe rotation (mode.cpp:872-880)
   int lsb[kMaxFreqsPerStation];
@@ -91,6 +93,9 @@ struct SubintArrays {
   const int32_t *control;        // [nstations][controlstride]
   int controlstride;
   const double *interp;          // [nstations][3]
+  // [nstations][nblk][nbands] frames (bit q: frame fr0 + q) whose samples of
+  // that band an EDV4 validity mask blanks; null when no station is interlaced
+  const unsigned long long *bandmask;
 };
 
 // One recorded band with phase-cal extraction (the reference's implicit-shift

@@ -225,6 +225,134 @@ __global__ void blockparams_kernel(DevJob J, SubintArrays S, int blk0, int nblk,
   weights[(size_t)s * nblk + bi] = P.state ? P.weight : 0.0f;
 }
 
+// EDV4 per-band validity of multiplexed VDIF (INTERLACEDVDIF; Mk5Mode::unpack,
+// mk5mode.cpp:142-163, and blank_vdif_EDV4 / _complex, format_vdif.c:8486-8660).
+// The frame geometry comes from the first frame's header in the buffer, as the
+// reference reads it: samples per header frame sph = payload bits / (channels x
+// bits), which for complex data is twice the frame's complex samples, so header
+// frame k then covers data frames [k m, (k+1) m) with m = sph / framesamples.
+// A header frame with its invalid bit clear and a validity mask other than all
+// channels blanks the samples of every band whose thread bit (band / (channels /
+// mask length)) is clear; a blanked sample counts as invalid when its decoded
+// value is not zero.  Band weight = (good - invalid[b]) / unpacksamples; block
+// weight = (good - sum invalid / nbands) / unpacksamples.  One warp per
+// (station, block); bandmask gets, per band, the data frames it blanks.
+__global__ void edv4_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays S, int nblk,
+                            BlockParam *__restrict__ bp, float *__restrict__ weights)
+{
+  __shared__ float s_lut[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) s_lut[i] = J.lut[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int bi = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  const int s = blockIdx.y;
+  if (bi >= nblk) return;
+  const DevStation &st = stations[s];
+  const int nb = J.nbands;
+  unsigned long long *bm = const_cast<unsigned long long *>(S.bandmask) + ((size_t)s * nblk + bi) * nb;
+  if (!st.interlaced) {
+    for (int b = lane; b < nb; b += 32) bm[b] = 0ull;
+    return;
+  }
+  BlockParam P = bp[(size_t)s * nblk + bi];
+  float *wb = weights + (size_t)st.wrow0 * nblk + bi;   // band b at wb[b * nblk]
+  unsigned long long mymask = 0ull;   // lane b < nb: frames blanked for band b
+  int inv = 0;                        // lane b: blanked samples with a non-zero value
+  const uint8_t *data = S.data[s];
+  const int64_t datalen = S.datalen[s];
+  if (P.state != 0 && datalen >= 32) {
+    const uint32_t *h0 = reinterpret_cast<const uint32_t *>(data);
+    const int ever = (int)(h0[4] >> 24), mlen = (int)((h0[4] >> 16) & 0xffu);
+    const int nchan = 1 << ((h0[2] >> 24) & 0x1fu);
+    const long long flen = (long long)(h0[2] & 0xffffffu) * 8;
+    const int hbits = (int)((h0[3] >> 26) & 0x1fu) + 1;
+    const long long sph = flen > 32 ? (flen - 32) * 8 / ((long long)nchan * hbits) : 0;
+    const int fs = J.framesamples;
+    const int dch = mlen > 0 ? nchan / mlen : 0;
+    if (ever == 4 && mlen >= 1 && mlen <= 64 && dch > 0 && nchan <= 62 && sph > 0 && sph % fs == 0) {
+      const int m = (int)(sph / fs);
+      const unsigned long long good_mask = (1ull << nchan) - 1ull;
+      // header frames over the window [nearestsample, + fftlen)
+      const long long k0 = (long long)P.nearestsample / sph;
+      const long long k1 = ((long long)P.nearestsample + J.fftlen - 1) / sph;
+      for (long long k = k0; k <= k1; k++) {
+        if ((k + 1) * flen > datalen) break;
+        const uint32_t *hk = reinterpret_cast<const uint32_t *>(data + k * flen);
+        const unsigned long long vmask = (unsigned long long)hk[6] | ((unsigned long long)hk[7] << 32);
+        if ((hk[0] >> 31) != 0u || vmask == good_mask) continue;
+        if (lane < nb && !((vmask >> (lane / dch)) & 1ull)) {
+          for (long long q = k * m; q < (k + 1) * m; q++) {
+            const long long rel = q - P.fr0;
+            if (rel >= 0 && rel < P.nframes) mymask |= 1ull << rel;
+          }
+        }
+      }
+      // count the non-zero samples the masks blank (decoder-valid frames only)
+      for (int b = 0; b < nb; b++) {
+        const unsigned long long bmask = __shfl_sync(0xffffffffu, mymask, b) & P.validmask;
+        if (!bmask) continue;
+        int cnt = 0;
+        for (int n = lane; n < J.fftlen; n += 32) {
+          const int smp = P.nearestsample + n;
+          const int q = smp / fs - P.fr0;
+          if (!((bmask >> q) & 1ull)) continue;
+          const int sub = J.cplx ? 2 : 1;
+          const uint8_t *payload = data + ((long long)P.fr0 + q) * J.framebytes + 32;
+          const long long bit0 = (long long)(smp % fs) * (nb * J.nbits * sub) + (long long)b * sub * J.nbits;
+          const int mask = (1 << J.nbits) - 1;
+          const float re = s_lut[(payload[bit0 >> 3] >> (bit0 & 7)) & mask];
+          float im = 0.f;
+          if (J.cplx) {
+            const long long bit1 = bit0 + J.nbits;
+            im = s_lut[(payload[bit1 >> 3] >> (bit1 & 7)) & mask];
+          }
+          if (re != 0.f || im != 0.f) cnt++;
+        }
+        for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        if (lane == b) inv = cnt;
+      }
+    }
+  }
+  // good samples of the window (as blockparams_kernel counts them)
+  int good = 0;
+  if (P.state != 0) {
+    for (int q = 0; q < P.nframes; q++) {
+      if (!((P.validmask >> q) & 1ull)) continue;
+      const long long fr = (long long)P.fr0 + q;
+      const long long lo = max((long long)P.nearestsample, fr * J.framesamples);
+      const long long hi = min((long long)P.nearestsample + J.unpacksamples, (fr + 1) * J.framesamples);
+      good += (int)(hi - lo);
+    }
+  }
+  int totalinv = inv;
+  for (int o = 16; o > 0; o >>= 1) totalinv += __shfl_xor_sync(0xffffffffu, totalinv, o);
+  if (lane < nb) {
+    bm[lane] = mymask;
+    wb[(size_t)lane * nblk] = P.state != 0 ? ((float)good - (float)inv) / (float)J.unpacksamples : 0.0f;
+  }
+  if (lane == 0 && P.state != 0 && totalinv > 0) {
+    float g = (float)good - (float)totalinv / (float)nb;
+    if (g < 0.f) g = 0.f;
+    P.weight = g / (float)J.unpacksamples;
+    if (!(P.weight > 0.0f)) {
+      P.state = 0;
+      P.weight = 0.0f;
+    }
+    bp[(size_t)s * nblk + bi] = P;
+    weights[(size_t)s * nblk + bi] = P.weight;
+  }
+}
+
+// Parameters of block bi as band bd of station s decodes it: frames an EDV4
+// validity mask blanks for this band count as invalid.
+__device__ __forceinline__ BlockParam band_param(const BlockParam *__restrict__ bp, const SubintArrays &S, int s,
+                                                 int nblk, int bi, int nbands, int bd)
+{
+  BlockParam P = bp[(size_t)s * nblk + bi];
+  if (S.bandmask) P.validmask &= ~S.bandmask[((size_t)s * nblk + bi) * nbands + bd];
+  return P;
+}
+
 // Fringe-rotator table entry e of local freq fi: e < S -> sub[e], else step[e - S]
 // (mode.cpp:882-955: FP64 phases, FP32 argument, sincos).
 __device__ __forceinline__ float2 fringe_entry(const DevJob &J, const DevStation &st, int fi, int e,
@@ -431,7 +559,7 @@ fstep_warp_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArray
   for (int it = warp; it < nitems; it += nwarps) {
     const int bi = b0 + it / J.nbands;
     const int bd = it % J.nbands;
-    const BlockParam P = bp[(size_t)s * nblk + bi];
+    const BlockParam P = band_param(bp, S, s, nblk, bi, J.nbands, bd);
     const int lf = st.band_localfreq[bd];
     const int f = st.freq_index[lf];
     float2 *dst = spec + ((size_t)f * nblk + bi) * J.ninputs * NCH;
@@ -584,8 +712,10 @@ fstep_cta_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays
       if (active) {
         const float2 *rs = rsub + lf * Sd;
         const float2 *rp = rstep + lf * nfr;
+        BlockParam Pb = P;   // this band's frames
+        if (S.bandmask) Pb.validmask &= ~S.bandmask[((size_t)s * nblk + bi) * J.nbands + bd];
         for (int n = lt; n < F; n += tps) {
-          const float2 u = decode_sample(J, data, P, bd, n, s_lut);
+          const float2 u = decode_sample(J, data, Pb, bd, n, s_lut);
           const int k = n % Sd, j = n / Sd;
           const float2 rot = quad ? bufB[n] : (j == 0) ? rs[k] : cmul_exact(rs[k], rp[j]);
           bufA[n] = J.cplx ? cmul(rot, u) : make_float2(u.x * rot.x, u.x * rot.y);
@@ -814,7 +944,7 @@ fstep_r16_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays
   for (int it = g; it < nitems; it += G) {
     const int bi = b0 + it / J.nbands;
     const int bd = it % J.nbands;
-    const BlockParam P = bp[(size_t)s * nblk + bi];
+    const BlockParam P = band_param(bp, S, s, nblk, bi, J.nbands, bd);
     const int lf = st.band_localfreq[bd];
     const int f = st.freq_index[lf];
     const int row = st.band_input[bd];
@@ -985,7 +1115,7 @@ __global__ void __launch_bounds__(256) pcal_bins_kernel(DevJob J, SubintArrays S
     float2 acc = make_float2(0.f, 0.f);
     if (r < R) {
       for (int bi = b0; bi < b1; bi++) {
-        const BlockParam P = bp[(size_t)s * nblk + bi];
+        const BlockParam P = band_param(bp, S, s, nblk, bi, J.nbands, B.band);
         if (P.state == 0) continue;
         const int idx0 = (int)((s0 + (unsigned long long)P.nearestsample) % (unsigned long long)N);
         const float2 v = sum_samples(J, data, P, B.band, (k - idx0 + N) % N + r * N, R * N, s_lut);
@@ -1008,7 +1138,7 @@ __global__ void __launch_bounds__(256) pcal_bins_kernel(DevJob J, SubintArrays S
     for (int k = tid; k < N; k += nth) {   // more bins than threads: one thread per bin
       float2 acc = make_float2(0.f, 0.f);
       for (int bi = b0; bi < b1; bi++) {
-        const BlockParam P = bp[(size_t)s * nblk + bi];
+        const BlockParam P = band_param(bp, S, s, nblk, bi, J.nbands, B.band);
         if (P.state == 0) continue;
         const int idx0 = (int)((s0 + (unsigned long long)P.nearestsample) % (unsigned long long)N);
         const float2 v = sum_samples(J, data, P, B.band, (k - idx0 + N) % N, N, s_lut);
@@ -1265,7 +1395,7 @@ cudaError_t pcal_bins_launch(const DevJob &J, const SubintArrays &S, const Block
   // the 8-bit integer sums need at most 256 samples of a thread per block
   // (the FFT length over the sample step R N, which is above 128)
   const int W = bits_ts == 128 ? 4 : bits_ts == 64 ? 2 : (bits_ts <= 32 && 32 % bits_ts == 0) ? 1 : 0;
-  const bool station = per_station > 0 && per_station <= kPcalMaxBands && W > 0;
+  const bool station = per_station > 0 && per_station <= kPcalMaxBands && W > 0 && !S.bandmask;
   const bool i8 = J.nbits == 8 && J.fftlen <= 256 * 128;
 #define GX_PCAL_STATION(w, nbits, cplx)                                                                       \
   pcal_station_kernel<w, nbits, cplx><<<grid, 256, nbits == 8 ? 0 : lut_bytes, st>>>(                         \
@@ -1320,6 +1450,10 @@ cudaError_t fstep_launch(const DevJob &J, const DevStation *stations, int maxnrf
   {
     dim3 grid((nblk + 127) / 128, J.nstations);
     blockparams_kernel<<<grid, 128, 0, st>>>(J, S, blk0, nblk, bp, weights);
+  }
+  if (S.bandmask) {   // INTERLACEDVDIF: EDV4 per-band validity, one warp per (station, block)
+    dim3 grid((nblk + 7) / 8, J.nstations);
+    edv4_kernel<<<grid, 256, 0, st>>>(J, stations, S, nblk, bp, weights);
   }
   const size_t sm = fstep_smem_bytes(J, maxnrf, nslots);
   if (use_r16_kernel(J)) {

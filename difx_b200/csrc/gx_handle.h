@@ -63,6 +63,11 @@ struct gx_handle {
   gx::BlockParam *d_bp = nullptr, *d_bp1 = nullptr;
   size_t acc_slice = 0;  // float2 per K-split slice
   int2 *d_pairs = nullptr;
+  // INTERLACEDVDIF stations: per-band weight rows after the station rows, and
+  // the per-(station, block, band) frames their EDV4 masks blank
+  bool interlaced_any = false;
+  int nwrows = 0;
+  unsigned long long *d_bandmask = nullptr;
   gx::ProdEntry *d_prods = nullptr;
   gx::WeightEntry *d_went = nullptr;
   // Per-subint tables, one block written on the host (pinned) and copied to

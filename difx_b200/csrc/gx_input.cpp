@@ -307,9 +307,21 @@ InputJob *read_input_job(const char *inputfile, std::string &err)
     NEED(in, "TELESCOPE INDEX", v); dstel[i] = atoi(v.c_str());
     NEED(in, "TSYS", v); dstsys[i] = atof(v.c_str());
     NEED(in, "DATA FORMAT", v);
-    if (strip(v) != "VDIF") { err = "DATA FORMAT " + strip(v) + " is not implemented (single-thread VDIF only)"; return nullptr; }
+    const std::string fmt = strip(v);
+    int muxthreads = 0;   // INTERLACEDVDIF/<thread>:<thread>:... (configuration.cpp:1491-1498, 2632-2651)
+    if (fmt.compare(0, 15, "INTERLACEDVDIF/") == 0 && fmt.size() > 15) {
+      muxthreads = 1;
+      for (size_t k = 15; k < fmt.size(); k++)
+        if (fmt[k] == ':') muxthreads++;
+      s.interlaced = 1;
+    } else if (fmt != "VDIF") {
+      err = "DATA FORMAT " + fmt + " is not implemented (VDIF and INTERLACEDVDIF only)";
+      return nullptr;
+    }
     NEED(in, "QUANTISATION BITS", v); s.nbits = atoi(v.c_str());
     NEED(in, "DATA FRAME SIZE", v); s.framebytes = atoi(v.c_str());
+    // the Core sees multiplexed frames: one header, every thread's payload (configuration.cpp:1686-1696)
+    if (muxthreads) s.framebytes = (s.framebytes - 32) * muxthreads + 32;
     NEED(in, "DATA SAMPLING", v);
     std::string samp = strip(v);
     if (samp == "REAL") s.is_complex = 0;

@@ -144,6 +144,9 @@ xmac_fp32_kernel(const float2 *__restrict__ spec, int nblk, int NI, int N, int n
 
 // Sum of weights over the blocks of one chunk (Core::processdata baseline
 // weights core.cpp:1005-1052; Mode autocorrelation weights mode.cpp:1277-1284).
+// Weight sums over a pass of blocks: item i < nstations sums station row i;
+// item nstations + k sums the products of rows pairs[k] (or row pairs[k].x
+// alone when pairs[k].y < 0).
 __global__ void weights_kernel(const float *__restrict__ w, int nblk, int nstations,
                                const int2 *__restrict__ pairs, int npairs, float *__restrict__ wacc)
 {
@@ -154,8 +157,12 @@ __global__ void weights_kernel(const float *__restrict__ w, int nblk, int nstati
     for (int b = threadIdx.x; b < nblk; b += blockDim.x) sum += w[(size_t)item * nblk + b];
   } else {
     const int2 pr = pairs[item - nstations];
-    for (int b = threadIdx.x; b < nblk; b += blockDim.x)
-      sum += w[(size_t)pr.x * nblk + b] * w[(size_t)pr.y * nblk + b];
+    if (pr.y < 0) {   // one row alone (a per-band weight row)
+      for (int b = threadIdx.x; b < nblk; b += blockDim.x) sum += w[(size_t)pr.x * nblk + b];
+    } else {
+      for (int b = threadIdx.x; b < nblk; b += blockDim.x)
+        sum += w[(size_t)pr.x * nblk + b] * w[(size_t)pr.y * nblk + b];
+    }
   }
   red[threadIdx.x] = sum;
   __syncthreads();

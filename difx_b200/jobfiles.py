@@ -76,6 +76,8 @@ class JobSpec:
     ac_avg_interval_ns: int = 2_000_000_000
     chans_to_avg: int = 1             # CHANS TO AVG of every freq (output channels = nchan / this)
     pcal_interval_mhz: int = 0        # PHASE CAL INT (MHZ) of every datastream (0: no phase-cal)
+    mux_threads: int = 0              # >0: INTERLACEDVDIF of this many threads, muxed frames with EDV4 headers
+    edv4_partial_frac: float = 0.0    # fraction of muxed frames whose EDV4 validity mask lacks some threads
     poly_interval_s: int = 120
     station_names: Sequence[str] = ()
     data_files: Sequence[str] = ()
@@ -148,6 +150,9 @@ class JobSpec:
         fps = self.frames_per_second
         if abs(fps - round(fps)) > 1e-9:
             raise ValueError("frames per second must be an integer")
+        if self.mux_threads > 0 and (self.payload_bytes % (8 * self.mux_threads) != 0 or
+                                     self.mux_threads > 64):
+            raise ValueError("each thread's payload must be a whole number of 8-byte words (<= 64 threads)")
         _ = self.blocks_per_send
 
     # ------------------------------------------------------------ model
@@ -305,9 +310,15 @@ def write_job(spec: JobSpec, outdir: str) -> dict:
     for i in range(nst):
         L.append(_kv("TELESCOPE INDEX", i))
         L.append(_kv("TSYS", "0.000000"))
-        L.append(_kv("DATA FORMAT", "VDIF"))
-        L.append(_kv("QUANTISATION BITS", spec.nbits))
-        L.append(_kv("DATA FRAME SIZE", spec.framebytes))
+        if spec.mux_threads > 0:
+            # per-thread frames before multiplexing; the Core sees spec.framebytes
+            L.append(_kv("DATA FORMAT", "INTERLACEDVDIF/" + ":".join(str(t) for t in range(spec.mux_threads))))
+            L.append(_kv("QUANTISATION BITS", spec.nbits))
+            L.append(_kv("DATA FRAME SIZE", spec.payload_bytes // spec.mux_threads + VDIF_HEADER_BYTES))
+        else:
+            L.append(_kv("DATA FORMAT", "VDIF"))
+            L.append(_kv("QUANTISATION BITS", spec.nbits))
+            L.append(_kv("DATA FRAME SIZE", spec.framebytes))
         L.append(_kv("DATA SAMPLING", samp))
         L.append(_kv("DATA SOURCE", "FILE"))
         L.append(_kv("FILTERBANK USED", "FALSE"))

@@ -124,7 +124,12 @@ def pack_timesamples(codes: np.ndarray, nbits: int) -> np.ndarray:
     return np.bitwise_or.reduce(flat << shifts, axis=1).astype(np.uint8)
 
 
-def vdif_header(spec: JobSpec, seconds: int, framenum: int, invalid: bool, station: int) -> bytes:
+def vdif_header(spec: JobSpec, seconds: int, framenum: int, invalid: bool, station: int,
+                validity: int = -1) -> bytes:
+    """VDIF header words 0-7.  Muxed streams (spec.mux_threads > 0) carry the
+    EDV4 fields of a multiplexed frame (vdifio.h:272-297): extended version 4,
+    mask length = threads, validity mask in words 6-7 (one bit per thread;
+    validity < 0: all threads present)."""
     nb = spec.nbands
     log2n = int(np.ceil(np.log2(nb))) if nb > 1 else 0
     w = np.zeros(8, dtype=np.uint32)
@@ -132,7 +137,37 @@ def vdif_header(spec: JobSpec, seconds: int, framenum: int, invalid: bool, stati
     w[1] = (framenum & 0xFFFFFF) | (0 << 24)
     w[2] = ((spec.framebytes // 8) & 0xFFFFFF) | (log2n << 24)
     w[3] = ((1 << 31) if spec.is_complex else 0) | ((spec.nbits - 1) << 26) | (station & 0xFFFF)
+    if spec.mux_threads > 0:
+        mt = spec.mux_threads
+        mask = ((1 << mt) - 1) if validity < 0 else validity
+        w[4] = (4 << 24) | (mt << 16)
+        w[5] = 0xACABFEED
+        w[6] = mask & 0xFFFFFFFF
+        w[7] = (mask >> 32) & 0xFFFFFFFF
     return w.tobytes()
+
+
+def edv4_masks(spec: JobSpec, station: int, seed: int, first_frame: int, nframes: int) -> np.ndarray:
+    """Validity mask of each muxed frame: all threads present, except a seeded
+    fraction spec.edv4_partial_frac of frames with one to three threads absent."""
+    mt = spec.mux_threads
+    full = (1 << mt) - 1
+    out = np.full(nframes, full, dtype=np.int64)
+    if spec.edv4_partial_frac <= 0 or mt <= 0:
+        return out
+    rng = np.random.default_rng([seed, 19, station])
+    n = first_frame + nframes
+    partial = rng.random(n) < spec.edv4_partial_frac
+    drops = rng.integers(0, mt, size=(n, 3))
+    ndrop = rng.integers(1, 4, size=n)
+    for f in range(nframes):
+        af = first_frame + f
+        if partial[af]:
+            m = full
+            for k in range(ndrop[af]):
+                m &= ~(1 << int(drops[af, k]))
+            out[f] = m
+    return out
 
 
 @dataclasses.dataclass
@@ -173,11 +208,12 @@ def make_station_stream(spec: JobSpec, station: int, first_frame: int, nframes: 
     invalid = allflags[first_frame:] < invalid_frac
     fillflags = np.random.default_rng([seed, 17, station]).random(first_frame + nframes)[first_frame:] < fill_frac
     fps = int(round(spec.frames_per_second))
+    masks = edv4_masks(spec, station, seed, first_frame, nframes)
     out = np.empty((nframes, spec.framebytes), dtype=np.uint8)
     for f in range(nframes):
         af = first_frame + f
         sec = spec.start_seconds + af // fps
-        hdr = vdif_header(spec, sec, af % fps, bool(invalid[f]), station)
+        hdr = vdif_header(spec, sec, af % fps, bool(invalid[f]), station, int(masks[f]))
         out[f, :VDIF_HEADER_BYTES] = np.frombuffer(hdr, dtype=np.uint8)
         out[f, VDIF_HEADER_BYTES:] = payload[f]
         if fillflags[f]:

@@ -100,6 +100,8 @@ typedef struct gx_station_desc {
   int clock_int_seconds;   /* floor(CLOCK COEFF 0 / 1e6 + 0.5), subtracted from the delay (mode.cpp:68,1526) */
   long long phase_cal_interval_hz; /* long(1e6 x PHASE CAL INT (MHZ)); 0: no phase-cal extraction */
   long long phase_cal_base_hz;     /* long(1e6 x PHASE CAL BASE(MHZ)); PHASE CAL DIVISOR must be 1 */
+  int interlaced;          /* DATA FORMAT INTERLACEDVDIF: framebytes is the multiplexed frame size and
+                              EDV4 validity masks blank absent threads per band (mk5mode.cpp:142-163) */
 } gx_station_desc;
 
 /* One baseline (BASELINE TABLE, configuration.cpp:1033-1180). */
@@ -122,7 +124,7 @@ typedef struct gx_job_desc {
   const gx_baseline_desc *baselines;
   int subint_ns;           /* SUBINT NANOSECONDS */
   int guard_ns;            /* GUARD NANOSECONDS */
-  int fringe_rotation_order; /* FRINGE ROTN ORDER: 1 (linear, pre-F) or 0 (post-F, real-sampled data) */
+  int fringe_rotation_order; /* FRINGE ROTN ORDER: 1 (linear), 2 (quadratic) or 0 (post-F, real data) */
   int array_stride;        /* ARRAY STRIDE LEN, 0 = automatic */
   int xmac_stride;         /* XMAC STRIDE LEN, 0 = automatic */
   int write_autocorrs;     /* WRITE AUTOCORRS (also enables cross-pol autocorrelations) */

@@ -154,3 +154,35 @@ def test_async_needs_a_device_handle():
         c.wait()
     assert ei.value.status == 8
     c.close()
+
+
+def test_interlaced_vdif_input_matches_descriptor(tmp_path):
+    """DATA FORMAT INTERLACEDVDIF/<threads> (configuration.cpp:1491-1498,
+    2632-2651): the Core sees multiplexed frames of (per-thread frame - 32) x
+    threads + 32 bytes; the .input and the descriptor give the same layout."""
+    from difx_b200.jobfiles import write_job
+    spec = jobs.spec_c1(name="mux_in", mux_threads=8)
+    paths = write_job(spec, str(tmp_path))
+    text = open(paths["input"]).read()
+    assert "INTERLACEDVDIF/0:1:2:3:4:5:6:7" in text
+    sizes = re.findall(r"^DATA FRAME SIZE:\s*(\d+)", text, re.M)
+    assert sizes and all(int(x) == spec.payload_bytes // 8 + 32 for x in sizes)
+    a = gxcorr.Correlator.from_input(paths["input"], device=-1)
+    b = gxcorr.Correlator.from_desc(capi.job_desc_from_spec(spec), device=-1)
+    assert a.info.result_length == b.info.result_length
+    for x, y in zip(a.offsets(), b.offsets()):
+        assert np.array_equal(x, y)
+    assert a.info.blocks_per_send == b.info.blocks_per_send
+    a.close()
+    b.close()
+
+
+def test_interlaced_vdif_band_limit():
+    """Per-band EDV4 masks use int-width thread bits in the reference: more
+    than 30 interlaced bands are refused."""
+    from difx_b200.jobfiles import Subband
+    spec = jobs.spec_c1(name="mux32", mux_threads=32, payload_bytes=8192,
+                        subbands=[Subband(8400.0 + 16 * i, 16.0, "U", 128) for i in range(16)])
+    with pytest.raises(gxcorr.GxError) as ei:
+        gxcorr.Correlator.from_desc(capi.job_desc_from_spec(spec), device=-1)
+    assert ei.value.status == 2

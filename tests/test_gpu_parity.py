@@ -263,6 +263,41 @@ def test_gpu_fringe_rotation_orders_match_reference(case, gx, oracle_lib):
     c.close()
 
 
+MUX_CASES = {
+    "real2_mux": lambda: (jobs.spec_c1(name="c1mx", seed=101, mux_threads=8, edv4_partial_frac=0.3),
+                          dict(invalid_frac=0.02)),
+    # 8-bit: a blanked sample whose code decodes to 0.0 does not count as invalid
+    "real8_mux": lambda: (jobs.spec_c1(name="r8mx", seed=102, nbits=8, mux_threads=8, edv4_partial_frac=0.3),
+                          dict(invalid_frac=0.02)),
+    # complex: the blanker's header geometry spans two data frames per header frame
+    "cplx8_mux": lambda: (jobs.spec_cplx8(name="cx8mx", seed=103, mux_threads=4, edv4_partial_frac=0.3),
+                          dict(invalid_frac=0.02)),
+    "lsb_mux": lambda: (jobs.spec_lsb(name="lsbmx", seed=104, mux_threads=4, edv4_partial_frac=0.3),
+                        dict(invalid_frac=0.02)),
+}
+
+
+@pytest.mark.skipif(not pyoracle.reference_available(), reason="reference harness not built")
+@pytest.mark.parametrize("case", sorted(MUX_CASES))
+def test_gpu_interlaced_vdif_matches_reference(case, gx, oracle_lib):
+    """INTERLACEDVDIF: multiplexed frames whose EDV4 validity masks lack some
+    threads; those bands' samples are blanked and every band gets its own
+    weight (mk5mode.cpp:142-163, format_vdif.c:8486-8660), used for the
+    baseline, autocorrelation and cross-pol weights (core.cpp:911-912,
+    1039-1044; mode.cpp:1277-1284, 1342-1351).  Against the compiled
+    reference reading the same .input, two subints."""
+    spec, kw = MUX_CASES[case]()
+    prep = jobs.prepare(spec, [100_000_000, 108_000_000], **kw)
+    c = gx.Correlator.from_desc(prep.jd)
+    for i, sd in enumerate(prep.sds):
+        g = c.subint(sd)
+        r = jobs.reference_for(prep.paths["input"]).process(prep.subs[i])
+        assert g.shape == r.shape
+        m, wrel = _compare(g, r, prep.jd, spec, oracle_lib, layout=c.offsets())
+        assert m < REC_TOL and wrel < W_TOL, (m, wrel)
+    c.close()
+
+
 AVG_CASES = {
     "c1_avg4": lambda: (jobs.spec_c1(name="c1avg", seed=61, chans_to_avg=4), dict(invalid_frac=0.03)),
     "cplx8_avg8": lambda: (jobs.spec_cplx8(name="cx8avg", seed=62, chans_to_avg=8), dict(invalid_frac=0.03)),
@@ -323,6 +358,9 @@ PCAL_CASES = {
                            dict(invalid_frac=0.03)),
     "cplx2_pcal": lambda: (jobs.spec_long("cx2pc", 2, "COMPLEX", "U", 128, 87, pcal_interval_mhz=1),
                            dict(invalid_frac=0.03)),
+    # multiplexed frames with EDV4 masks: phase-cal of the blanked samples
+    "mux_pcal": lambda: (jobs.spec_c1(name="c1mxpc", seed=105, pcal_interval_mhz=1, mux_threads=8,
+                                      edv4_partial_frac=0.3), dict(invalid_frac=0.02)),
     # 16 2-bit real bands: 32-bit time samples
     "real2_16band_pcal": lambda: (jobs.spec_c1(name="c1pc16", seed=85, nstations=3, pcal_interval_mhz=1,
                                                subbands=[jobs.Subband(8400.0 + 16 * i, 16.0, "U", 128)
