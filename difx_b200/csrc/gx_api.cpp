@@ -113,8 +113,15 @@ static gx_status setup(gx_handle *h)
       return h->fail(GX_ERR_UNSUPPORTED, "all freqs must share bandwidth and channel count");
   const int cplx = s0.is_complex ? 1 : 0;
   const int bits_ts = s0.nbands * s0.nbits * (cplx ? 2 : 1);
-  if (bits_ts % 8 != 0)
-    return h->fail(GX_ERR_UNSUPPORTED, "a time sample of all bands must fill whole bytes (sample granularity 1)");
+  // whole bytes per time sample, or a whole number of time samples per byte
+  // (mark5access sample granularity 8 / bits, mk5mode.cpp:100, 118-141)
+  if (bits_ts % 8 != 0 && 8 % bits_ts != 0)
+    return h->fail(GX_ERR_UNSUPPORTED, "a time sample must fill whole bytes or divide a byte");
+  // complex samples narrower than a byte: the reference's granularity erase
+  // indexes its complex unpack arrays as floats (mk5mode.cpp:118-141 over the
+  // aliased arrays of mode.cpp:152-154) and zeroes components inside the window
+  if (bits_ts < 8 && cplx)
+    return h->fail(GX_ERR_UNSUPPORTED, "complex time samples narrower than a byte are not implemented");
   const int payload = s0.framebytes - 32;
   if (payload <= 0 || (payload * 8) % bits_ts != 0 || payload % 8 != 0)
     return h->fail(GX_ERR_ARG, "DATA FRAME SIZE is not a whole number of time samples");
@@ -127,7 +134,8 @@ static gx_status setup(gx_handle *h)
   J.framebytes = s0.framebytes;
   J.framesamples = payload * 8 / (s0.nbits * s0.nbands);
   if (cplx) J.framesamples /= 2;
-  J.bytespersample = bits_ts / 8;
+  J.bps_num = bits_ts >= 8 ? bits_ts / 8 : 1;
+  J.bps_den = bits_ts >= 8 ? 1 : 8 / bits_ts;
   J.nchan = f0.nchan;
   J.fftlen = cplx ? f0.nchan : 2 * f0.nchan;
   if (J.fftlen & (J.fftlen - 1)) return h->fail(GX_ERR_UNSUPPORTED, "FFT length must be a power of two");

@@ -37,7 +37,8 @@ struct DevJob {
   int nstations;
   int nbands;             // recorded bands per station
   int nbits, cplx;
-  int framebytes, framesamples, bytespersample;
+  int framebytes, framesamples;
+  int bps_num, bps_den;   // bytes per time sample = bps_num / bps_den (mode.cpp:131-143)
   int nchan;              // N: channels per band
   int fftlen;             // F: fftchannels (2N real, N complex)
   int stride;             // S: arraystridelength

@@ -163,7 +163,7 @@ __global__ void blockparams_kernel(DevJob J, SubintArrays S, int blk0, int nblk,
                                 fftstartmicrosec / 1.0e6;
     P.intwalltime = (int)walltimesecs;
     P.fracwalltime = walltimesecs - P.intwalltime;
-    if (!(ns < -1 || (long long)(ns + F) * J.bytespersample > datalen)) {
+    if (!(ns < -1 || ((long long)(ns + F) * J.bps_num) / J.bps_den > datalen)) {
       if (ns == -1) ns = 0;
       P.nearestsample = ns;
       P.fr0 = ns / J.framesamples;

@@ -143,8 +143,8 @@ class JobSpec:
         for sb in self.subbands:
             if sb.bw_mhz != self.bw_mhz or sb.nchan != self.nchan:
                 raise ValueError("all subbands must share bandwidth and channel count")
-        if self.bits_per_timesample % 8 != 0:
-            raise ValueError("a time sample of all bands must fill whole bytes")
+        if self.bits_per_timesample % 8 != 0 and 8 % self.bits_per_timesample != 0:
+            raise ValueError("a time sample of all bands must fill whole bytes or divide a byte")
         if (self.payload_bytes * 8) % self.bits_per_timesample != 0:
             raise ValueError("payload is not a whole number of time samples")
         fps = self.frames_per_second

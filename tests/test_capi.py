@@ -186,3 +186,17 @@ def test_interlaced_vdif_band_limit():
     with pytest.raises(gxcorr.GxError) as ei:
         gxcorr.Correlator.from_desc(capi.job_desc_from_spec(spec), device=-1)
     assert ei.value.status == 2
+
+
+def test_sub_byte_time_samples():
+    """Real time samples narrower than a byte open (sample granularity 8 /
+    bits); complex ones are refused (the reference's granularity erase treats
+    its complex unpack arrays as floats, mk5mode.cpp:118-141)."""
+    from difx_b200.jobfiles import Subband
+    ok = jobs.spec_c1(name="g2", subbands=[Subband(8400.0, 16.0, "U", 128)])
+    assert ok.bits_per_timesample == 4
+    gxcorr.Correlator.from_desc(capi.job_desc_from_spec(ok), device=-1).close()
+    bad = jobs.spec_cplx8(name="gc", nbits=2, pols=("R",), subbands=[Subband(6000.0, 16.0, "U", 256)])
+    with pytest.raises(gxcorr.GxError) as ei:
+        gxcorr.Correlator.from_desc(capi.job_desc_from_spec(bad), device=-1)
+    assert ei.value.status == 2

@@ -298,6 +298,40 @@ def test_gpu_interlaced_vdif_matches_reference(case, gx, oracle_lib):
     c.close()
 
 
+GRAN_CASES = {
+    # time samples narrower than a byte (mark5access sample granularity 8 / bits)
+    "real2_2band": lambda: (jobs.spec_c1(name="g_r2x2", seed=111, subbands=[jobs.Subband(8400.0, 16.0, "U", 128)]),
+                            dict(invalid_frac=0.03)),
+    "real1_2band": lambda: (jobs.spec_c1(name="g_r1x2", seed=112, nbits=1,
+                                         subbands=[jobs.Subband(8400.0, 16.0, "U", 128)]), dict(invalid_frac=0.03)),
+    "real2_1band": lambda: (jobs.spec_c1(name="g_r2x1", seed=113, pols=("R",),
+                                         subbands=[jobs.Subband(8400.0, 16.0, "U", 128)]), dict(invalid_frac=0.03)),
+    "real2_2band_long": lambda: (jobs.spec_long("g_r2l", 2, "REAL", "U", 1024, 115, pols=("R", "L"),
+                                                subbands=[jobs.Subband(8400.0, 16.0, "U", 1024)]),
+                                 dict(invalid_frac=0.03)),
+}
+
+
+@pytest.mark.skipif(not pyoracle.reference_available(), reason="reference harness not built")
+@pytest.mark.parametrize("case", sorted(GRAN_CASES))
+def test_gpu_sub_byte_time_samples_match_reference(case, gx, oracle_lib):
+    """Time samples of 1, 2 or 4 bits (several per byte): the unpack starts on
+    a granularity boundary and the samples outside the FFT window are erased
+    from the weight (mk5mode.cpp:100, 118-141); the range check uses bytes per
+    block numerator / denominator (mode.cpp:131-143, 688).  Against the
+    compiled reference reading the same .input, two subints."""
+    spec, kw = GRAN_CASES[case]()
+    prep = jobs.prepare(spec, [100_000_000, 108_000_000], **kw)
+    c = gx.Correlator.from_desc(prep.jd)
+    for i, sd in enumerate(prep.sds):
+        g = c.subint(sd)
+        r = jobs.reference_for(prep.paths["input"]).process(prep.subs[i])
+        assert g.shape == r.shape
+        m, wrel = _compare(g, r, prep.jd, spec, oracle_lib, layout=c.offsets())
+        assert m < REC_TOL and wrel < W_TOL, (m, wrel)
+    c.close()
+
+
 AVG_CASES = {
     "c1_avg4": lambda: (jobs.spec_c1(name="c1avg", seed=61, chans_to_avg=4), dict(invalid_frac=0.03)),
     "cplx8_avg8": lambda: (jobs.spec_cplx8(name="cx8avg", seed=62, chans_to_avg=8), dict(invalid_frac=0.03)),
