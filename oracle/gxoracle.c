@@ -229,7 +229,7 @@ static inline cf cmul(cf a, cf b)
 /* State a reference Mode carries across the blocks it processes in order. */
 typedef struct { int unpackstart; } mode_state;
 
-/* Mode::process for one block (mode.cpp:634-1374), fringe rotation order 1.
+/* Mode::process for one block (mode.cpp:634-1374), fringe rotation orders 0, 1 and 2.
    Writes nbands x nchan spectra; returns the data weight (0 = zeroed block).
    FP32 path: float outputs in spec32; FP64 path: double outputs in spec64. */
 static float station_block(const gx_job_desc *d, const gx_subint_desc *s, int si, int index,
@@ -259,7 +259,13 @@ static float station_block(const gx_job_desc *d, const gx_subint_desc *s, int si
   int intwalltime = (int)walltimesecs;
   double fracwalltime = walltimesecs - intwalltime;
 
-  if (nearestsample < -1 || (long long)(nearestsample + F) * o.bytespersample > datalen) return 0.0f;
+  /* bytes per block numerator / denominator, mode.cpp:131-143, 688 */
+  {
+    int bits_ts = st->nbands * st->nbits * (o.cplx ? 2 : 1);
+    long long need = bits_ts >= 8 ? (long long)(nearestsample + F) * (bits_ts / 8)
+                                  : (long long)(nearestsample + F) / (8 / bits_ts);
+    if (nearestsample < -1 || need > datalen) return 0.0f;
+  }
 
   float dataweight = 0.0f;
   float *unp = (float *)malloc(sizeof(float) * nb * o.unpacksamples * 2);
@@ -276,19 +282,45 @@ static float station_block(const gx_job_desc *d, const gx_subint_desc *s, int si
   float fracsampleerror = (float)(starttime - nearestsampletime);
   double fracerr64 = starttime - nearestsampletime;
 
-  /* linear interpolation, mode.cpp:782-799 */
-  double d0 = interp[0] * index * index + interp[1] * index + interp[2];
-  double d1 = interp[0] * (index + 0.5) * (index + 0.5) + interp[1] * (index + 0.5) + interp[2];
-  double d2 = interp[0] * (index + 1) * (index + 1) + interp[1] * (index + 1) + interp[2];
-  double a = d2 - d0;
-  double b = d0 + (d1 - (a * 0.5 + d0)) / 3.0;
-  int integerdelay = (int)b;
-  b -= integerdelay;
-
+  /* delay interpolation by FRINGE ROTN ORDER, mode.cpp:776-826 */
+  const int order = d->fringe_rotation_order;
   double *subxval = (double *)malloc(sizeof(double) * S);
   double *stepxval = (double *)malloc(sizeof(double) * o.nfr);
-  for (int k = 0; k < S; k++) { subxval[k] = ((double)k / (double)F) * a; subxval[k] += b; }
-  for (int j = 0; j < o.nfr; j++) stepxval[j] = ((double)(j * S) / (double)F) * a;
+  double *quadxval = (double *)malloc(sizeof(double) * S);
+  int integerdelay = 0;
+  double postf_b = 0.0;   /* post-F: block-centre delay without its integer part */
+  if (order == 0) {
+    integerdelay = (int)averagedelay;
+    postf_b = averagedelay - integerdelay;
+    for (int k = 0; k < S; k++) subxval[k] = quadxval[k] = 0.0;
+    for (int j = 0; j < o.nfr; j++) stepxval[j] = 0.0;
+  } else if (order == 2) {
+    double qa = interp[0];
+    double qb = interp[1] + index * interp[0] * 2.0;
+    double c = interp[2] + index * interp[1] + index * index * interp[0];
+    integerdelay = (int)c;
+    c -= integerdelay;
+    double s1 = (double)S / (double)F;   /* stepxoff[1] */
+    for (int k = 0; k < S; k++) {
+      subxval[k] = ((double)k / (double)F) * (qb + qa * s1);
+      subxval[k] += c;
+      quadxval[k] = ((double)k / (double)F) * (2 * qa * s1);
+    }
+    for (int j = 0; j < o.nfr; j++) {
+      double x = (double)(j * S) / (double)F;
+      stepxval[j] = x * qb + (x * x) * qa;
+    }
+  } else {
+    double d0 = interp[0] * index * index + interp[1] * index + interp[2];
+    double d1 = interp[0] * (index + 0.5) * (index + 0.5) + interp[1] * (index + 0.5) + interp[2];
+    double d2 = interp[0] * (index + 1) * (index + 1) + interp[1] * (index + 1) + interp[2];
+    double a = d2 - d0;
+    double b = d0 + (d1 - (a * 0.5 + d0)) / 3.0;
+    integerdelay = (int)b;
+    b -= integerdelay;
+    for (int k = 0; k < S; k++) { subxval[k] = ((double)k / (double)F) * a; subxval[k] += b; quadxval[k] = 0.0; }
+    for (int j = 0; j < o.nfr; j++) stepxval[j] = ((double)(j * S) / (double)F) * a;
+  }
 
   cf *rot = (cf *)malloc(sizeof(cf) * F);
   cd *rot64 = (cd *)malloc(sizeof(cd) * F);
@@ -313,8 +345,17 @@ static float station_block(const gx_job_desc *d, const gx_subint_desc *s, int si
     double lofreq = fq->freq_mhz;
     if (o.cplx && lsb) lofreq = -lofreq;
 
-    /* fringe rotator, mode.cpp:831-955 */
-    if (!fp64) {
+    /* post-F fringe phase at the block centre (mode.cpp:1038-1049) */
+    double postf_ph = 0.0;
+    if (order == 0) {
+      postf_ph = postf_b * lofreq;
+      if (o.fractional_lo) postf_ph += integerdelay * (lofreq - (int)lofreq);
+      postf_ph -= walltimesecs * looffset;
+    }
+    /* fringe rotator, mode.cpp:831-1005 (none before the FFT for post-F) */
+    if (order == 0) {
+      for (int n = 0; n < F; n++) { rot[n].re = 1.0f; rot[n].im = 0.0f; rot64[n].re = 1.0; rot64[n].im = 0.0; }
+    } else if (!fp64) {
       float *subarg = (float *)malloc(sizeof(float) * S), *steparg = (float *)malloc(sizeof(float) * o.nfr);
       for (int k = 0; k < S; k++) {
         double ph = subxval[k] * lofreq;
@@ -334,13 +375,30 @@ static float station_block(const gx_job_desc *d, const gx_subint_desc *s, int si
       cf *stepc = (cf *)malloc(sizeof(cf) * o.nfr);
       for (int k = 0; k < S; k++) { rot[k].re = cosf(subarg[k]); rot[k].im = sinf(subarg[k]); }
       for (int j = 0; j < o.nfr; j++) { stepc[j].re = cosf(steparg[j]); stepc[j].im = sinf(steparg[j]); }
-      for (int j = 1; j < o.nfr; j++)
-        for (int k = 0; k < S; k++) rot[j * S + k] = cmul(rot[k], stepc[j]);
+      if (order == 2) {
+        /* piecewise rotator times step[j], then piecewise *= quad (mode.cpp:996-1005) */
+        cf *pw = (cf *)malloc(sizeof(cf) * S), *quad = (cf *)malloc(sizeof(cf) * S);
+        for (int k = 0; k < S; k++) {
+          double ph = quadxval[k] * lofreq;
+          float qarg = (float)(-TWO_PI * (ph - (int)ph));
+          quad[k].re = cosf(qarg); quad[k].im = sinf(qarg);
+          pw[k] = rot[k];
+        }
+        for (int j = 0; j < o.nfr; j++)
+          for (int k = 0; k < S; k++) {
+            rot[j * S + k] = cmul(pw[k], stepc[j]);
+            pw[k] = cmul(quad[k], pw[k]);
+          }
+        free(pw); free(quad);
+      } else {
+        for (int j = 1; j < o.nfr; j++)
+          for (int k = 0; k < S; k++) rot[j * S + k] = cmul(rot[k], stepc[j]);
+      }
       free(stepc); free(subarg); free(steparg);
     } else {
       for (int n = 0; n < F; n++) {
         int k = n % S, j = n / S;
-        double ph = (subxval[k] + stepxval[j]) * lofreq;
+        double ph = (subxval[k] + stepxval[j] + quadxval[k] * j) * lofreq;
         if (o.fractional_lo) ph += (lofreq - (int)lofreq) * (double)integerdelay;
         if (looff) {
           ph += (n * o.sampletime / 1e6) * -looffset;
@@ -359,9 +417,11 @@ static float station_block(const gx_job_desc *d, const gx_subint_desc *s, int si
         float val = (float)(fracsampleerror - st->clock_offset_us[fi] + sgn * st->clock_offset_delta_us[fi] / 2);
         cf *fr = pol == 0 ? fracA : fracB;
         cf *stepc = (cf *)malloc(sizeof(cf) * (half > 0 ? half : 1));
+        float prf = order == 0 ? (float)(-TWO_PI * (postf_ph - (int)postf_ph)) : 0.0f;
         for (int k = 0; k < S; k++) {
           float cfreq = (float)((TWO_PI * (k) * o.bw) / N);
           float arg = cfreq * val;
+          if (order == 0) arg = arg + prf;
           fr[k].re = cosf(arg); fr[k].im = sinf(arg);
         }
         for (int j = 0; j < half; j++) {
@@ -383,6 +443,7 @@ static float station_block(const gx_job_desc *d, const gx_subint_desc *s, int si
           /* every stride, the first included (mode.cpp:1071), carries step[j] */
           double sfreq = lsb ? (-TWO_PI * ((half - j) * S) * o.bw) / N : (TWO_PI * j * S * o.bw) / N;
           double arg = (cfreq + sfreq) * val;
+          if (order == 0) arg += -TWO_PI * (postf_ph - floor(postf_ph));
           fr[c].re = cos(arg); fr[c].im = sin(arg);
         }
       }
@@ -433,7 +494,7 @@ static float station_block(const gx_job_desc *d, const gx_subint_desc *s, int si
       }
     }
   }
-  free(subxval); free(stepxval); free(rot); free(rot64); free(fracA); free(fracB);
+  free(subxval); free(stepxval); free(quadxval); free(rot); free(rot64); free(fracA); free(fracB);
   free(frac64A); free(frac64B); free(buf); free(fbuf); free(unp);
   return dataweight;
 }

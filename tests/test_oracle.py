@@ -164,3 +164,52 @@ def test_oracle_bitexact_other_bit_depths(case, oracle_lib):
     o = oracle_lib.subint(prep.jd, prep.sds[0], _params(oracle_lib, spec))
     assert r.shape == o.shape
     np.testing.assert_array_equal(o.astype(np.complex64), r)
+
+
+FEATURE_CASES = {
+    # FRINGE ROTN ORDER 2 (quadratic rotator as repeated FP32 stride products)
+    "quad_real": lambda: (jobs.spec_c1(name="oq", seed=94, fringe_rot_order=2, subbands=[
+        jobs.Subband(8400.25 + 16 * i, 16.0, "U", 128) for i in range(4)]), dict(invalid_frac=0.02)),
+    "quad_cplx": lambda: (jobs.spec_cplx8(name="oqc", seed=96, fringe_rot_order=2), dict(invalid_frac=0.02)),
+    # real time samples narrower than a byte (sample granularity 2 and 4)
+    "real2_2band": lambda: (jobs.spec_c1(name="og22", seed=111, subbands=[jobs.Subband(8400.0, 16.0, "U", 128)]),
+                            dict(invalid_frac=0.03)),
+    "real1_2band": lambda: (jobs.spec_c1(name="og12", seed=112, nbits=1,
+                                         subbands=[jobs.Subband(8400.0, 16.0, "U", 128)]), dict(invalid_frac=0.03)),
+}
+
+
+@needs_ref
+@pytest.mark.parametrize("case", sorted(FEATURE_CASES))
+def test_oracle_bitexact_fringe_orders_and_granularity(case, oracle_lib):
+    """Quadratic fringe rotation and sub-byte time samples: the oracle's Core
+    result array equals the reference's bit for bit."""
+    spec, kw = FEATURE_CASES[case]()
+    prep = jobs.prepare(spec, [100_000_000], **kw)
+    r = jobs.reference_for(prep.paths["input"]).process(prep.subs[0])
+    o = oracle_lib.subint(prep.jd, prep.sds[0], _params(oracle_lib, spec))
+    assert r.shape == o.shape
+    np.testing.assert_array_equal(o.astype(np.complex64), r)
+
+
+POSTF_CASES = {
+    "postf_usb": lambda: (jobs.spec_c1(name="opf", seed=91, fringe_rot_order=0, subbands=[
+        jobs.Subband(8400.25 + 16 * i, 16.0, "U", 128) for i in range(4)]), dict(invalid_frac=0.02)),
+    "postf_lsb": lambda: (jobs.spec_lsb(name="opfl", seed=92, fringe_rot_order=0), dict(invalid_frac=0.02)),
+}
+
+
+@needs_ref
+@pytest.mark.parametrize("case", sorted(POSTF_CASES))
+def test_oracle_post_f_rotation_vs_reference(case, oracle_lib):
+    """Post-F fringe rotation: the reference transforms with a real-to-complex
+    FFT (mode.cpp:1135-1159), the oracle with a complex FFT of the same real
+    samples; records agree to 1e-6 (mean |difference| / mean |reference|)."""
+    spec, kw = POSTF_CASES[case]()
+    prep = jobs.prepare(spec, [100_000_000], **kw)
+    r = jobs.reference_for(prep.paths["input"]).process(prep.subs[0])
+    o = oracle_lib.subint(prep.jd, prep.sds[0], _params(oracle_lib, spec)).astype(np.complex64)
+    assert r.shape == o.shape
+    rl, bl, bw, ac, acw = oracle_lib.layout(prep.jd)
+    offs = jobs.record_offsets(prep.jd, bl, ac, spec)
+    assert jobs.record_metric(o, r, offs, spec.nchan) < 1e-6
