@@ -182,6 +182,53 @@ int gxo_unpack(const gx_station_desc *st, int framesamples, const unsigned char 
   return good;
 }
 
+/* EDV4 per-band blanking of multiplexed VDIF after the unpack (Mk5Mode::unpack,
+   mk5mode.cpp:142-163; blank_vdif_EDV4 / _complex, format_vdif.c:8486-8660):
+   geometry from the first header of the buffer (samples per header frame =
+   payload bits / (channels x bits), twice the complex samples for complex
+   data); a header frame with its invalid bit clear and a validity mask other
+   than all channels zeroes, in every band whose thread bit (band / (channels /
+   mask length)) is clear, the unpacked samples that are not zero, counting
+   them per band.  Without EDV4 fields nothing is blanked. */
+static void edv4_blank(const gx_station_desc *st, const unsigned char *data, long long datalen, int offset,
+                       int nsamp, float *unp, int *invalid)
+{
+  int nb = st->nbands, cplx = st->is_complex;
+  for (int b = 0; b < nb; b++) invalid[b] = 0;
+  if (datalen < 32) return;
+  const uint32_t *h0 = (const uint32_t *)data;
+  int ever = (int)(h0[4] >> 24), mlen = (int)((h0[4] >> 16) & 0xffu);
+  if (ever != 4 || mlen < 1 || mlen > 64) return;
+  int nchan = 1 << ((h0[2] >> 24) & 0x1f);
+  long long flen = (long long)(h0[2] & 0xffffffu) * 8;
+  int hbits = (int)((h0[3] >> 26) & 0x1f) + 1;
+  long long sph = (flen - 32) * 8 / ((long long)nchan * hbits);
+  int dch = nchan / mlen;
+  if (sph <= 0 || dch <= 0 || nchan > 62) return;
+  unsigned long long good_mask = (1ull << nchan) - 1ull;
+  for (long long k = offset / sph; k <= ((long long)offset + nsamp - 1) / sph; k++) {
+    if ((k + 1) * flen > datalen) break;
+    const uint32_t *hk = (const uint32_t *)(data + k * flen);
+    unsigned long long vmask = (unsigned long long)hk[6] | ((unsigned long long)hk[7] << 32);
+    if ((hk[0] >> 31) != 0u || vmask == good_mask) continue;
+    long long lo = k * sph > offset ? k * sph : offset;
+    long long hi = (k + 1) * sph < (long long)offset + nsamp ? (k + 1) * sph : (long long)offset + nsamp;
+    for (int b = 0; b < nb; b++) {
+      if ((vmask >> (b / dch)) & 1ull) continue;
+      for (long long sm = lo; sm < hi; sm++) {
+        long long o = sm - offset;
+        if (cplx) {
+          float *v = unp + (long long)b * 2 * nsamp + 2 * o;
+          if (v[0] != 0.0f || v[1] != 0.0f) { v[0] = v[1] = 0.0f; invalid[b]++; }
+        } else {
+          float *v = unp + (long long)b * nsamp + o;
+          if (*v != 0.0f) { *v = 0.0f; invalid[b]++; }
+        }
+      }
+    }
+  }
+}
+
 /* -------------------------------------------------------------- station F */
 
 typedef struct {
@@ -233,8 +280,10 @@ typedef struct { int unpackstart; } mode_state;
    Writes nbands x nchan spectra; returns the data weight (0 = zeroed block).
    FP32 path: float outputs in spec32; FP64 path: double outputs in spec64. */
 static float station_block(const gx_job_desc *d, const gx_subint_desc *s, int si, int index,
-                           int fp64, mode_state *ms, cf *spec32, cd *spec64)
+                           int fp64, mode_state *ms, cf *spec32, cd *spec64, float *bandw)
 {
+  if (bandw)   /* per-band weights reset at the start of the block (mode.cpp:646-653) */
+    for (int b = 0; b < d->stations[si].nbands; b++) bandw[b] = 0.0f;
   const gx_station_desc *st = &d->stations[si];
   stn o;
   stn_init(d, si, &o);
@@ -275,7 +324,20 @@ static float station_block(const gx_job_desc *d, const gx_subint_desc *s, int si
   if (!do_unpack) { free(unp); return 0.0f; }   /* dataweight stays 0 (mode.cpp:646) */
   ms->unpackstart = nearestsample;
   int good = gxo_unpack(st, o.framesamples, s->data[si], datalen, nearestsample, o.unpacksamples, unp);
-  dataweight = (float)good / (float)o.unpacksamples;
+  float goodsamples = (float)good;
+  if (st->interlaced) {
+    int invalid[GX_MAX_BANDS], totalinvalid = 0;
+    edv4_blank(st, s->data[si], datalen, nearestsample, o.unpacksamples, unp, invalid);
+    for (int b = 0; b < nb; b++) {
+      if (bandw) bandw[b] = (goodsamples - invalid[b]) / (float)o.unpacksamples;
+      totalinvalid += invalid[b];
+    }
+    goodsamples -= (float)totalinvalid / (float)nb;
+    if (goodsamples < 0) goodsamples = 0;
+  }
+  dataweight = goodsamples / (float)o.unpacksamples;
+  if (bandw && !st->interlaced)
+    for (int b = 0; b < nb; b++) bandw[b] = dataweight;
   if (!(dataweight > 0.0f)) { free(unp); return 0.0f; }
 
   double nearestsampletime = nearestsample * o.sampletime;
@@ -508,12 +570,12 @@ int gxo_station_block(const gx_job_desc *d, const gx_subint_desc *s, int station
   float w;
   if (p->precision == GXO_FP64) {
     cd *sp = (cd *)malloc(sizeof(cd) * st->nbands * N);
-    w = station_block(d, s, station, block, 1, &ms, 0, sp);
+    w = station_block(d, s, station, block, 1, &ms, 0, sp, 0);
     memcpy(spectra, sp, sizeof(cd) * st->nbands * N);
     free(sp);
   } else {
     cf *sp = (cf *)malloc(sizeof(cf) * st->nbands * N);
-    w = station_block(d, s, station, block, 0, &ms, sp, 0);
+    w = station_block(d, s, station, block, 0, &ms, sp, 0, 0);
     for (int i = 0; i < st->nbands * N; i++) { spectra[2 * i] = sp[i].re; spectra[2 * i + 1] = sp[i].im; }
     free(sp);
   }
@@ -560,6 +622,7 @@ int gxo_subint(const gx_job_desc *d, const gx_subint_desc *s, const gxo_params *
   cf *sp32 = (cf *)malloc(sizeof(cf) * nst * maxnb * maxN);
   cd *sp64 = (cd *)malloc(sizeof(cd) * nst * maxnb * maxN);
   float *w = (float *)malloc(sizeof(float) * nst);
+  float *wb = (float *)calloc((size_t)nst * maxnb, sizeof(float));   /* per-band weights (getDataWeight) */
   /* accumulators: cross [f][bl][p][c]; autos [st][2][band][c]; weights */
   long long crosslen = rl;
   cf *xc32 = (cf *)calloc(crosslen, sizeof(cf));
@@ -592,7 +655,7 @@ int gxo_subint(const gx_job_desc *d, const gx_subint_desc *s, const gxo_params *
           int N = d->freqs[st->recfreq[0]].nchan;
           cf *o32 = sp32 + (long long)i * maxnb * maxN;
           cd *o64 = sp64 + (long long)i * maxnb * maxN;
-          w[i] = station_block(d, s, i, blk, fp64, &ms[i], fp64 ? 0 : o32, fp64 ? o64 : 0);
+          w[i] = station_block(d, s, i, blk, fp64, &ms[i], fp64 ? 0 : o32, fp64 ? o64 : 0, wb + i * maxnb);
           if (w[i] > 0.0f) {
             /* autocorrelations and their weights, mode.cpp:1270-1284, 1333-1352 */
             for (int bd = 0; bd < st->nbands; bd++) {
@@ -607,8 +670,8 @@ int gxo_subint(const gx_job_desc *d, const gx_subint_desc *s, const gxo_params *
                   ac64[ab + c].re += a.re * a.re + a.im * a.im;
                 }
               }
-              acw32[i * 2 * maxnb + bd] += w[i];
-              acw64[i * 2 * maxnb + bd] += w[i];
+              acw32[i * 2 * maxnb + bd] += wb[i * maxnb + bd];
+              acw64[i * 2 * maxnb + bd] += wb[i * maxnb + bd];
             }
             if (d->write_autocorrs) {
               for (int fi = 0; fi < st->nrecfreqs; fi++) {
@@ -629,8 +692,10 @@ int gxo_subint(const gx_job_desc *d, const gx_subint_desc *s, const gxo_params *
                       ac64[ab + c].im += -x0.re * x1.im + x0.im * x1.re;
                     }
                   }
-                  acw32[i * 2 * maxnb + maxnb + b0] += w[i];
-                  acw64[i * 2 * maxnb + maxnb + b0] += w[i];
+                  /* interlaced: the product of the two bands' weights */
+                  float xw = st->interlaced ? wb[i * maxnb + idx[0]] * wb[i * maxnb + idx[1]] : w[i];
+                  acw32[i * 2 * maxnb + maxnb + b0] += xw;
+                  acw64[i * 2 * maxnb + maxnb + b0] += xw;
                 }
               }
             }
@@ -661,9 +726,10 @@ int gxo_subint(const gx_job_desc *d, const gx_subint_desc *s, const gxo_params *
                 }
               }
               /* baseline weight, core.cpp:1039-1044 */
-              float bwv = w[bl->ds1] * w[bl->ds2];
+              float w1 = wb[bl->ds1 * maxnb + b1], w2 = wb[bl->ds2 * maxnb + b2];
+              float bwv = w1 * w2;
               bw32[(f * nbl + j) * 4 + pp] += bwv;
-              bw64[(f * nbl + j) * 4 + pp] += (double)w[bl->ds1] * (double)w[bl->ds2];
+              bw64[(f * nbl + j) * 4 + pp] += (double)w1 * (double)w2;
             }
           }
         }
@@ -731,6 +797,6 @@ int gxo_subint(const gx_job_desc *d, const gx_subint_desc *s, const gxo_params *
   }
   for (long long e = 0; e < 2 * rl; e++) results[e] = fp64 ? r64[e] : (double)r32[e];
   free(blofs); free(bwofs); free(acofs); free(acwofs); free(r32); free(r64); free(sp32); free(sp64);
-  free(w); free(xc32); free(xc64); free(ac32); free(ac64); free(acw32); free(acw64); free(bw32); free(bw64); free(ms);
+  free(w); free(wb); free(xc32); free(xc64); free(ac32); free(ac64); free(acw32); free(acw64); free(bw32); free(bw64); free(ms);
   return 0;
 }

@@ -176,14 +176,22 @@ FEATURE_CASES = {
                             dict(invalid_frac=0.03)),
     "real1_2band": lambda: (jobs.spec_c1(name="og12", seed=112, nbits=1,
                                          subbands=[jobs.Subband(8400.0, 16.0, "U", 128)]), dict(invalid_frac=0.03)),
+    # INTERLACEDVDIF: EDV4 per-band blanking and per-band weights
+    "mux_real2": lambda: (jobs.spec_c1(name="omx2", seed=101, mux_threads=8, edv4_partial_frac=0.3),
+                          dict(invalid_frac=0.02)),
+    "mux_real8": lambda: (jobs.spec_c1(name="omx8", seed=102, nbits=8, mux_threads=8, edv4_partial_frac=0.3),
+                          dict(invalid_frac=0.02)),
+    "mux_cplx8": lambda: (jobs.spec_cplx8(name="omxc", seed=103, mux_threads=4, edv4_partial_frac=0.3),
+                          dict(invalid_frac=0.02)),
 }
 
 
 @needs_ref
 @pytest.mark.parametrize("case", sorted(FEATURE_CASES))
 def test_oracle_bitexact_fringe_orders_and_granularity(case, oracle_lib):
-    """Quadratic fringe rotation and sub-byte time samples: the oracle's Core
-    result array equals the reference's bit for bit."""
+    """Quadratic fringe rotation, sub-byte time samples and INTERLACEDVDIF
+    with EDV4 masks: the oracle's Core result array equals the reference's
+    bit for bit."""
     spec, kw = FEATURE_CASES[case]()
     prep = jobs.prepare(spec, [100_000_000], **kw)
     r = jobs.reference_for(prep.paths["input"]).process(prep.subs[0])
