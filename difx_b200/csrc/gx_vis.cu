@@ -17,8 +17,10 @@
 //                 baseline / freq / polarisation-product order, then the
 //                 autocorrelations per datastream.
 //
-// Covered: one configuration, one phase centre, no pulsar bins, no channel
-// averaging or output bands, TSYS 0 (normalised correlation coefficients).
+// Covered: one configuration, one phase centre, no pulsar bins, no output
+// bands; TSYS 0 (normalised correlation coefficients) or TSYS > 0
+// (a-priori calibration by the band-mean autocorrelations).
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -105,8 +107,6 @@ gx_status gx_vis_open(gx_handle *h, const char *outdir, gx_vis **out)
   *out = nullptr;
   if (h->device < 0) return h->fail(GX_ERR_STATE, "host-only handle (opened with device -1)");
   if (!h->model || !h->meta) return h->fail(GX_ERR_STATE, "the visibility writer needs a handle opened with gx_open_input");
-  for (double t : h->meta->tsys)
-    if (t > 0.0) return h->fail(GX_ERR_UNSUPPORTED, "TSYS > 0 (a-priori amplitude calibration) is not implemented");
   std::unique_ptr<gx_vis> v(new gx_vis());
   v->h = h;
   v->outdir = outdir;
@@ -173,6 +173,10 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
     for (int x : h->bwofs)
       if (x >= 0) bw0 = std::min<long long>(bw0, x), bw1 = std::max<long long>(bw1, x + 2);
     for (int x : h->acwofs) aw0 = std::min<long long>(aw0, x);
+    // TSYS > 0: the autocorrelations too (their band means calibrate, visibility.cpp:463-484)
+    for (double t : M.tsys)
+      if (t > 0.0)
+        for (int x : h->acofs) aw0 = std::min<long long>(aw0, x);
     if (bw1 > bw0)
       CKR(h, cudaMemcpyAsync(&fr[2 * bw0], v->d_int + bw0, sizeof(float2) * (bw1 - bw0), cudaMemcpyDeviceToHost,
                              v->st));
@@ -193,6 +197,37 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
     for (int j = 0; j < nbl; j++)
       if (gx_bl_localfreq(d.baselines[j], f) >= 0) return true;
     return false;
+  };
+  // A-priori calibration with TSYS > 0 (visibility.cpp:463-484, 505-519,
+  // 607-616): the FP32 mean of each band's summed parallel-hand
+  // autocorrelation (genericMean_32fc: a sequential sum, then a division) and
+  // the autocorrelation weights by band, as writedata forms them.
+  const int acwidth = h->maxprod > 2 ? 2 : 1;
+  std::vector<std::vector<float>> calib(d.nstations), acw0(d.nstations);
+  for (int s = 0; s < d.nstations; s++) {
+    const gx_station_desc &x = d.stations[s];
+    calib[s].assign(x.nbands, 0.0f);
+    acw0[s].assign(x.nbands, 0.0f);
+    long long widx = 2LL * h->acwofs[s];   // the parallel-hand weights come first
+    for (int b = 0; b < x.nbands; b++)
+      if (freq_used(x.recfreq[x.band_localfreq[b]])) acw0[s][b] = (float)(fr[widx++] / ffts);
+    if (!(s < (int)M.tsys.size() && M.tsys[s] > 0.0)) continue;
+    long long off = h->acofs[s];
+    for (int b = 0; b < x.nbands; b++) {
+      if (!freq_used(x.recfreq[x.band_localfreq[b]])) continue;
+      float re = 0.0f;
+      for (int c = 0; c < N; c++) re += fr[2 * (off + c)];
+      calib[s][b] = re / N;
+      off += N;
+    }
+  }
+  auto tsys = [&](int s) { return s < (int)M.tsys.size() ? M.tsys[s] : 0.0; };
+  // Mode::decorrelationpercentage (mode.cpp:1571), by bits per sample
+  static const float kDecorrelation[8] = {0.63662f, 0.88f, 0.94f, 0.96f, 0.98f, 0.99f, 0.996f, 0.998f};
+  auto matching_band = [&](const gx_station_desc &x, int b) {   // Configuration::getDMatchingBand
+    for (int i = 0; i < x.nbands; i++)
+      if (i != b && x.band_localfreq[i] == x.band_localfreq[b]) return i;
+    return -1;
   };
 
   // record table, in writeSWIN order
@@ -219,6 +254,13 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
       for (int k = 0; k < B.npolprod[lf]; k++) {
         float w, scale;
         weight_and_scale(2LL * h->bwofs[f * nbl + i] + k, w, scale);
+        if (tsys(B.ds1) > 0.0 && tsys(B.ds2) > 0.0) {
+          const int b1 = B.band1[lf][k], b2 = B.band2[lf][k];
+          const float divisor = kDecorrelation[d.stations[B.ds1].nbits - 1] * kDecorrelation[d.stations[B.ds2].nbits - 1] *
+                                calib[B.ds1][b1] * calib[B.ds2][b2] / (acw0[B.ds1][b1] * acw0[B.ds2][b2]);
+          scale = (divisor > 0.0f && w > 0.0f)
+                      ? (float)(std::sqrt(tsys(B.ds1) * tsys(B.ds2) / divisor) / w) : 0.0f;
+        }
         if (scale > 0.0f) scales.push_back(VisScale{h->blofs[f * nbl + i] + (long long)k * N, scale, 0});
         if (w > 0.0f) {
           r.freq = f;
@@ -232,7 +274,6 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
     }
   }
   if (d.write_autocorrs) {
-    const int acwidth = h->maxprod > 2 ? 2 : 1;
     for (int s = 0; s < d.nstations; s++) {
       const gx_station_desc &x = d.stations[s];
       long long off = h->acofs[s], widx = 2LL * h->acwofs[s];
@@ -242,6 +283,11 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
           if (!freq_used(f)) continue;
           float w, scale;
           weight_and_scale(widx++, w, scale);
+          if (tsys(s) > 0.0) {
+            const int m = j == 0 ? b : matching_band(x, b);
+            const float divisor = m >= 0 ? std::sqrt(calib[s][b] * calib[s][m]) : 0.0f;
+            scale = divisor > 0.0f ? (float)(tsys(s) / divisor) : 0.0f;
+          }
           if (scale > 0.0f) scales.push_back(VisScale{off, scale, 0});
           if (w > 0.0f) {
             Rec r{};

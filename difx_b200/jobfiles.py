@@ -77,6 +77,7 @@ class JobSpec:
     chans_to_avg: int = 1             # CHANS TO AVG of every freq (output channels = nchan / this)
     pcal_interval_mhz: int = 0        # PHASE CAL INT (MHZ) of every datastream (0: no phase-cal)
     mux_threads: int = 0              # >0: INTERLACEDVDIF of this many threads, muxed frames with EDV4 headers
+    tsys: float = 0.0                 # TSYS of every datastream (> 0: a-priori amplitude calibration)
     edv4_partial_frac: float = 0.0    # fraction of muxed frames whose EDV4 validity mask lacks some threads
     poly_interval_s: int = 120
     station_names: Sequence[str] = ()
@@ -309,7 +310,7 @@ def write_job(spec: JobSpec, outdir: str) -> dict:
     samp = "REAL" if not spec.is_complex else "COMPLEX"
     for i in range(nst):
         L.append(_kv("TELESCOPE INDEX", i))
-        L.append(_kv("TSYS", "0.000000"))
+        L.append(_kv("TSYS", f"{spec.tsys:.6f}"))
         if spec.mux_threads > 0:
             # per-thread frames before multiplexing; the Core sees spec.framebytes
             L.append(_kv("DATA FORMAT", "INTERLACEDVDIF/" + ":".join(str(t) for t in range(spec.mux_threads))))

@@ -28,6 +28,9 @@ CASES = {
     "c1_avg4": lambda: jobs.spec_c1(name="gvisa", seed=29, int_time=0.016, chans_to_avg=4),
     "c1_pcal": lambda: jobs.spec_c1(name="gvisp", seed=31, int_time=0.016, pcal_interval_mhz=1),
     "lsb_pcal": lambda: jobs.spec_lsb(name="gvislp", seed=37, int_time=0.008, pcal_interval_mhz=1),
+    # a-priori calibration (visibility.cpp:463-484, 505-519, 607-616)
+    "c1_tsys": lambda: jobs.spec_c1(name="gvist", seed=41, int_time=0.016, tsys=55.0),
+    "cplx8_tsys": lambda: jobs.spec_cplx8(name="gvisct", seed=43, int_time=0.008192, tsys=70.0),
 }
 
 
