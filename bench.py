@@ -171,50 +171,84 @@ class ClockSampler:
 REF_SAMPLE_NS = {"c3": 2_048_000, "c2": 4_000_000, "c1": 8_000_000}
 
 
+class ReferenceSampler:
+    """The reference's own CPU path (Core::processdata on every host core)
+    opened once over a bounded sample of the workload: one Configuration /
+    Core / Modes and one synthetic input, reused for every timed sample and
+    freed by close()."""
+
+    def __init__(self, spec_name: str):
+        from oracle import pyoracle
+        self.err = None
+        self.ref = None
+        if not pyoracle.reference_available():
+            self.err = "reference harness not built (oracle/_ref/libdifxref.so)"
+            return
+        ncores = os.cpu_count() or 1
+        self.spec = workload_spec(spec_name, subint_ns=REF_SAMPLE_NS[spec_name])
+        d = tempfile.mkdtemp(prefix="gxref_")
+        paths = write_job(self.spec, d)
+        with open(paths["threads"], "w") as f:
+            f.write(f"{'NUMBER OF CORES:':<20}1\n{ncores}\n")
+        self.ref = pyoracle.Reference(paths["input"])
+        self.si = build_input(self.spec, 100_000_000, rho=RHO[spec_name], tile_ms=2.0)
+        self.ref.process(self.si)  # warm-up: first touch of the Core's result slots and thread arrays
+
+    def rate(self, target_s: float = 15.0, max_subints: int = 50):
+        t0 = time.perf_counter()
+        n = 0
+        while True:
+            self.ref.process(self.si)
+            n += 1
+            el = time.perf_counter() - t0
+            if el >= target_s or n >= max_subints:
+                break
+        rate = n * samples_per_subint(self.spec) / el / 1e9
+        sample = (f"{n} subints of {self.spec.subint_ns / 1e6:g} ms ({self.spec.blocks_per_send} FFT blocks) of the "
+                  f"same workload, {self.ref.nthreads} process threads, {el:.1f} s")
+        return {"value": rate, "unit": UNIT, "cores": int(self.ref.nthreads), "kind": "reference", "sample": sample}
+
+    def close(self):
+        if self.ref is not None:
+            self.ref.close()
+            self.ref = None
+
+
 def reference_rate(spec_name: str, target_s: float = 15.0, max_subints: int = 50):
-    """The reference's own CPU path on every host core over a bounded sample."""
-    from oracle import pyoracle
-    if not pyoracle.reference_available():
-        return None, "reference harness not built (oracle/_ref/libdifxref.so)"
-    ncores = os.cpu_count() or 1
-    spec = workload_spec(spec_name, subint_ns=REF_SAMPLE_NS[spec_name])
-    d = tempfile.mkdtemp(prefix="gxref_")
-    paths = write_job(spec, d)
-    with open(paths["threads"], "w") as f:
-        f.write(f"{'NUMBER OF CORES:':<20}1\n{ncores}\n")
-    ref = pyoracle.Reference(paths["input"])
-    si = build_input(spec, 100_000_000, rho=RHO[spec_name], tile_ms=2.0)
-    ref.process(si)  # warm-up
-    t0 = time.perf_counter()
-    n = 0
-    while True:
-        ref.process(si)
-        n += 1
-        el = time.perf_counter() - t0
-        if el >= target_s or n >= max_subints:
-            break
-    rate = n * samples_per_subint(spec) / el / 1e9
-    sample = (f"{n} subints of {spec.subint_ns / 1e6:g} ms ({spec.blocks_per_send} FFT blocks) of the same workload, "
-              f"{ref.nthreads} process threads, {el:.1f} s")
-    return {"value": rate, "unit": UNIT, "cores": int(ref.nthreads), "kind": "reference", "sample": sample}, None
+    """One bounded timed sample of the reference's CPU path (the cpu_baseline leg)."""
+    rs = ReferenceSampler(spec_name)
+    if rs.ref is None:
+        return None, rs.err
+    try:
+        return rs.rate(target_s, max_subints), None
+    finally:
+        rs.close()
+
+
+def peak_rss_gb() -> float:
+    import resource
+    return resource.getrusage(resource.RUSAGE_SELF).ru_maxrss / 1e6
 
 
 def run_reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    steps = []
-    base, err = None, None
-    for _ in range(max(1, args.steps)):
-        base, err = reference_rate(args.config, target_s=max(3.0, 15.0 / max(1, args.steps)))
-        if base is None:
-            break
-        steps.append(base["value"])
-    if base is None:
-        print(json.dumps({"impl": "reference", "unavailable": err}))
+    rs = ReferenceSampler(args.config)
+    if rs.ref is None:
+        print(json.dumps({"impl": "reference", "unavailable": rs.err}))
         return 0
+    steps = []
+    base = None
+    try:
+        for _ in range(max(1, args.steps)):
+            base = rs.rate(target_s=max(3.0, 15.0 / max(1, args.steps)))
+            steps.append(base["value"])
+    finally:
+        rs.close()
     v = statistics.median(steps)
     base["value"] = v
+    base["peak_rss_gb"] = round(peak_rss_gb(), 2)
     spec = workload_spec(args.config, subint_ns=int(round(args.subint_ms * 1e6)))
     if args.pcal_mhz:
         spec = JobSpec(**{**spec.__dict__, "pcal_interval_mhz": args.pcal_mhz})

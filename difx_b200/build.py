@@ -12,6 +12,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -41,17 +42,23 @@ def build(verbose: bool = False, force: bool = False) -> str:
     newest = max(os.path.getmtime(p) for p in deps)
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= newest:
         return LIB
-    objs = []
     common = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-ccbin", host_cxx(),
               "-I" + os.path.join(HERE, "..", "include")]
-    for s in srcs:
+
+    def compile_one(s):
         o = os.path.join(BUILD, s + ".o")
         cmd = [nvcc()] + ARCH + common + ["-c", os.path.join(CSRC, s), "-o", o]
-        if s.endswith(".cu"):
-            cmd += ["-Xptxas", "-v"] if verbose else []
+        if s.endswith(".cu") and verbose:
+            cmd += ["-Xptxas", "-v"]
+        return s, o, cmd, subprocess.run(cmd, capture_output=True, text=True)
+
+    # one nvcc per source, in parallel (the F-step source alone takes most of a minute)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(srcs), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(compile_one, srcs))
+    objs = []
+    for s, o, cmd, r in results:
         if verbose:
             print(" ".join(cmd))
-        r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             sys.stderr.write(r.stdout + r.stderr)
             raise RuntimeError(f"nvcc failed on {s}")

@@ -22,15 +22,17 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 ORACLE_LIB = os.path.join(REF_DIR, "libgxoracle.so")
 REFERENCE_LIB = os.path.join(REF_DIR, "libdifxref.so")
-REFERENCE_SRC = "/root/reference"
+# Where the reference tree lies in the build container (DIFX_REFERENCE); the
+# GPU box has no tree and uses the prebuilt _ref/ libraries.
+REFERENCE_SRC = os.environ.get("DIFX_REFERENCE", "/root/reference")
 
 
 def build(reference: bool = True) -> None:
     """Build the oracle (and, where the reference tree exists, the reference harness)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
     if reference and os.path.isdir(REFERENCE_SRC):
-        subprocess.run(["make", "-s", "-C", HERE, "ref", "-j8"], check=True)
-        subprocess.run(["make", "-s", "-C", HERE, "vmux"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "ref", "-j8", f"REF={REFERENCE_SRC}"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "vmux", f"REF={REFERENCE_SRC}"], check=True)
 
 
 def reference_available() -> bool:
@@ -112,6 +114,21 @@ class Reference:
         self.result_length = self.lib.ref_result_length(self.h)
         self.blocks_per_send = self.lib.ref_blocks_per_send(self.h)
         self.nthreads = self.lib.ref_num_threads(self.h)
+
+    def close(self) -> None:
+        """Free the reference's Core, Modes and Configuration (many GB for large jobs)."""
+        if getattr(self, "h", None) is not None:
+            self.lib.ref_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
     def layout(self, nfreqs: int, nbaselines: int, nstations: int):
         bl = np.zeros(max(1, nfreqs * nbaselines), np.int32)

@@ -260,10 +260,46 @@ int ref_uvw(void *h, int scan, double offset, int ds1, int ds2, double *out3)
   return config->getModel()->interpolateUVW(scan, offset, a1, a2, 1, out3) ? 0 : -1;
 }
 
+// Frees everything ref_open made: per thread what Core::loopprocess frees on
+// exit (core.cpp:551-581: the Modes and the scratch vectors), the per-freq
+// baseline weight rows allocated by allocateConfigSpecificThreadArrays
+// (core.cpp:2110-2125; freed here directly, one delete per row array), then
+// the Core (core.cpp:159-186) and the Configuration.  A Core holds
+// RECEIVE_RING_LENGTH full result slots and every thread a full cross-
+// correlation accumulator, so a handle of a large job is many GB of host
+// memory.
 void ref_close(void *h)
 {
-  // The Core/Configuration destructors are not reached on the reference's
-  // own path either (processes exit); the harness simply leaks them.
-  (void)h;
+  RefJob *j = (RefJob *)h;
+  if (!j) return;
+  Configuration *cf = j->config;
+  Core *c = j->core;
+  const int nf = cf->getFreqTableLength(), nb = cf->getNumBaselines();
+  for (int t = 0; t < j->nthreads; t++) {
+    Mode **modes = j->modes[t];
+    for (int d = 0; d < j->nds; d++) delete modes[d];
+    delete[] modes;
+    Core::threadscratchspace *s = (Core::threadscratchspace *)j->scratch[t];
+    for (int f = 0; f < nf; f++) {
+      if (!cf->isFrequencyUsed(0, f) || !s->baselineweight[f]) continue;
+      for (int b = 0; b < nb; b++)
+        if (cf->getBLocalFreqIndex(0, b, f) >= 0) vectorFree(s->baselineweight[f][0][b]);
+      delete[] s->baselineweight[f][0];
+      delete[] s->baselineweight[f];
+    }
+    delete[] s->baselineweight;
+    delete[] s->baselineshiftdecorr;
+    vectorFree(s->threadcrosscorrs);
+    vectorFree(s->chanfreqs);
+    vectorFree(s->rotator);
+    vectorFree(s->rotated);
+    vectorFree(s->channelsums);
+    vectorFree(s->argument);
+    delete s;
+  }
+  for (int d = 0; d < j->nds; d++) c->procslots[0].databuffer[d] = j->origbuffers[d];
+  delete c;
+  delete cf;
+  delete j;
 }
 }
