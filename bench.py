@@ -55,9 +55,9 @@ from difx_b200.jobfiles import JobSpec, Subband, write_job  # noqa: E402
 METRIC = "Gsamp/s correlated"
 UNIT = "Gsamp/s"
 XSTEPS = {"fp32": capi.GX_XSTEP_FP32, "tc": capi.GX_XSTEP_TC_FP16, "tc_hilo": capi.GX_XSTEP_TC_FP16_HILO}
-DEFAULT_SUBINT_MS = {"c3": 128.0, "c2": 200.0, "c1": 200.0, "c4": 0.0, "c5": 0.0, "mux": 0.0}
-DEFAULT_XSTEP = {"c3": "tc_hilo", "c2": "fp32", "c1": "fp32", "c4": "tc_hilo", "c5": "tc_hilo", "mux": "fp32"}
-RHO = {"c3": 0.01, "c2": 0.02, "c1": 0.05}
+DEFAULT_SUBINT_MS = {"c3": 128.0, "c3_2bit": 128.0, "c2": 200.0, "c1": 200.0, "c4": 0.0, "c5": 0.0, "mux": 0.0}
+DEFAULT_XSTEP = {"c3": "tc_hilo", "c3_2bit": "tc_hilo", "c2": "fp32", "c1": "fp32", "c4": "tc_hilo", "c5": "tc_hilo", "mux": "fp32"}
+RHO = {"c3": 0.01, "c3_2bit": 0.01, "c2": 0.02, "c1": 0.05}
 
 
 def workload_spec(name="c3", subint_ns=None) -> JobSpec:
@@ -68,6 +68,12 @@ def workload_spec(name="c3", subint_ns=None) -> JobSpec:
                        subbands=[Subband(6000.0 + 64 * i, 64.0, "U", 4096) for i in range(4)],
                        nbits=8, sampling="COMPLEX", payload_bytes=8000, subint_ns=subint_ns, execute_seconds=20,
                        int_time=1.0, max_delay_us=20000.0, max_rate_us_per_s=3.0, seed=2027)
+    if name == "c3_2bit":
+        # the 2-bit real variant: 8192-point real transforms, 16-bit time samples
+        return JobSpec(name=f"bench_{name}", nstations=64,
+                       subbands=[Subband(6000.0 + 64 * i, 64.0, "U", 4096) for i in range(4)],
+                       nbits=2, payload_bytes=8000, subint_ns=subint_ns, execute_seconds=20,
+                       int_time=1.0, max_delay_us=20000.0, max_rate_us_per_s=3.0, seed=2028)
     if name == "c2":
         return JobSpec(name=f"bench_{name}", nstations=16,
                        subbands=[Subband(8200.0 + 32 * i, 32.0, "U", 256) for i in range(8)],
@@ -168,7 +174,7 @@ class ClockSampler:
 
 
 # subint of the bounded CPU sample per workload (whole FFT blocks)
-REF_SAMPLE_NS = {"c3": 2_048_000, "c2": 4_000_000, "c1": 8_000_000}
+REF_SAMPLE_NS = {"c3": 2_048_000, "c3_2bit": 2_048_000, "c2": 4_000_000, "c1": 8_000_000}
 
 
 class ReferenceSampler:
@@ -325,7 +331,7 @@ def time_device(corr, sd_dev, dres, stream, steps, warmup, local, dist=None, clo
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) that ncu measured for
 # one fstep_r16_kernel launch on the C3 workload: 250 blocks x 64 stations
-# (profiles/fstep_r16_kernel_c3.md).  Traffic grows with the blocks a launch
+# (a 16 ms subint captured alone).  Traffic grows with the blocks a launch
 # processes, so a step's traffic is this per-block figure times its blocks.
 R16_C3_DRAM_BYTES_PER_BLOCK = 5.321e9 / 250
 
@@ -687,7 +693,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="gxcorr", choices=["gxcorr", "reference"])
-    ap.add_argument("--config", default="c3", choices=["c3", "c2", "c1", "c4", "c5", "mux"])
+    ap.add_argument("--config", default="c3", choices=["c3", "c3_2bit", "c2", "c1", "c4", "c5", "mux"])
     ap.add_argument("--c4-steps", type=int, default=1, help="timed batch steps per mode (C4)")
     ap.add_argument("--c5-slots", type=int, default=4)
     ap.add_argument("--c5-seconds", type=float, default=20.0)
@@ -749,7 +755,7 @@ def main():
 
     # the other X-step forms first (device-resident timing only), then the headline arm
     compare = {}
-    if args.config == "c3" and not args.no_compare:
+    if args.config in ("c3", "c3_2bit") and not args.no_compare:
         for name in sorted(XSTEPS):
             if name == args.xstep:
                 continue

@@ -2,21 +2,29 @@
 // finalise kernels as gx_subint_device, for callers that cannot allocate
 // device memory.
 //
-// Who needs this: code that runs where cudaMalloc is not allowed or not
-// acceptable -- inside CUDA stream capture (cudaMalloc is not a capturable
-// operation), in real-time receive threads that must not take the implicit
-// device-wide synchronisation cudaMalloc/cudaFree can impose, and in host
-// frameworks that hand every byte of device memory to their own allocator
-// and only pass buffers in.  Such a caller passes device inputs and a device
-// result buffer; everything else this path needs -- the per-station tables,
-// twiddles, control words, spectra, accumulators and weights -- lives in
-// one fixed scratch array in device global memory, declared below.
+// Who needs this: host frameworks that hand every byte of device memory to
+// their own allocator and only pass buffers in, and threads that must not
+// call cudaMalloc/cudaFree because those calls can wait for the whole device
+// (every stream), not only for the caller's own work.  Such a caller passes
+// device inputs and a device result buffer; everything else this path needs
+// -- the per-station tables, twiddles, control words, spectra, accumulators
+// and weights -- lives in one fixed scratch array in device global memory,
+// declared below.
 //
 // The scratch array is GX_NOALLOC_SCRATCH_BYTES (64 MiB).  Every GPU on which
 // this library's device code is loaded holds that array until the process
 // exits.  Jobs whose tables and accumulators do not fit are rejected with
 // GX_ERR_UNSUPPORTED and a message giving the bytes needed; the spectra
 // buffer is sized down (fewer FFT blocks per pass) to fit what is left.
+//
+// Set-up: the first call on a device asks the runtime for the array's device
+// address on that device (cudaGetSymbolAddress, with the device current) and
+// keeps it for later calls; make that first call before any stream capture
+// begins on the device.  The kept address is not looked up again, so the
+// device must not be reset (cudaDeviceReset) while this library is in use.
+//
+// The per-call tables are copied from pageable host memory, so a call may
+// wait for work already queued on `stream` before it returns.
 //
 // All calls share the one array and each call leaves its contents behind;
 // every region that must start at zero is cleared on the caller's stream at
@@ -47,7 +55,7 @@ void *g_scratch[kMaxDevices] = {nullptr};
 
 // Device address of the scratch array on the current device.  The host-side
 // symbol is only a stand-in, so the address is asked of the runtime once per
-// device, with that device current.
+// device, with that device current (the first call on the device).
 cudaError_t scratch_address(int dev, unsigned char **out)
 {
   if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;

@@ -202,18 +202,22 @@ gx_status gx_subint_async(gx_handle *h, const gx_subint_desc *sub, float *result
 gx_status gx_subint_wait(gx_handle *h);
 
 /* No counterpart in the reference.  The same subint work as gx_subint_device
-   for callers that cannot allocate device memory (code inside CUDA stream
-   capture, real-time threads that must not take cudaMalloc's implicit
-   synchronisation, host frameworks that own all device memory and only pass
-   buffers in).  No handle: desc is planned on every call; sub->data are
-   device pointers, sub->control and sub->interp host pointers (interp is
-   required).  Everything besides the caller's inputs and dev_results lives in
-   one library-wide scratch array of GX_NOALLOC_SCRATCH_BYTES in device global
+   for callers that cannot allocate device memory (host frameworks that own
+   all device memory and only pass buffers in; threads that must not call
+   cudaMalloc/cudaFree, which can wait for every stream of the device).  No
+   handle: desc is planned on every call; sub->data are device pointers,
+   sub->control and sub->interp host pointers (interp is required).
+   Everything besides the caller's inputs and dev_results lives in one
+   library-wide scratch array of GX_NOALLOC_SCRATCH_BYTES in device global
    memory, which every GPU that loads the library holds until exit; jobs that
    do not fit return GX_ERR_UNSUPPORTED with the bytes needed in err.  The
-   call allocates no device memory.  All calls share the array: calls whose
-   work overlaps on the GPU race, so order them on one stream.  Only the FP32
-   X-step form is available on this path.  err (may be NULL) receives a
+   call allocates no device memory.  The first call on a device looks up the
+   array's device address and keeps it: make that call before any stream
+   capture begins, and do not reset the device while using this entry point.
+   Per-call tables are copied from pageable host memory, so the call may wait
+   for work already queued on `stream`.  All calls share the array: calls
+   whose work overlaps on the GPU race, so order them on one stream.  Only the
+   FP32 X-step form is available on this path.  err (may be NULL) receives a
    message of at most errlen bytes. */
 #define GX_NOALLOC_SCRATCH_BYTES (64u << 20)
 gx_status gx_subint_device_noalloc(const gx_job_desc *desc, const gx_subint_desc *sub, float *dev_results,

@@ -1,10 +1,12 @@
 """gx_subint_device_noalloc: the subint entry point for callers that cannot
-allocate device memory (stream-capture code, real-time threads that must not
-block on cudaMalloc, frameworks that own all device memory).  It keeps its
-scratch in one library-wide device array, so these checks run last: two calls
-in a row through the C ABI must each give what the allocating entry point
-(gx_subint_device on a handle) gives, and a job too large for the array must
-be refused with a clear message."""
+allocate device memory (host frameworks that own all device memory and only
+pass buffers in; threads that must not call cudaMalloc/cudaFree, which can
+wait for every stream of the device).  It keeps its scratch in one
+library-wide device array, so these checks run last: two calls in a row
+through the C ABI must each give exactly what the allocating entry point
+(gx_subint_device on a handle) gives -- the same kernels over the same pass
+length, so bit for bit -- without changing the device's free memory, and a
+job too large for the array must be refused with a clear message."""
 import ctypes as C
 
 import numpy as np
@@ -57,11 +59,17 @@ def test_noalloc_matches_allocating_entry_point():
     wslots = np.array(wslots)
 
     stream = torch.cuda.Stream()
+    outs = [torch.full((2 * rl,), float("nan"), dtype=torch.float32, device="cuda") for _ in range(2)]
+    torch.cuda.synchronize()
     for call in range(2):
-        out = torch.full((2 * rl,), float("nan"), dtype=torch.float32, device="cuda")
-        torch.cuda.synchronize()
+        out = outs[call]
+        # the array is placed on the device with the library's module (at the
+        # latest by the first call), so free memory is compared around the second
+        free0 = torch.cuda.mem_get_info()[0] if call == 1 else None
         gxcorr.subint_device_noalloc(prep.jd, sd, out.data_ptr(), stream.cuda_stream)
         stream.synchronize()
+        if call == 1:
+            assert torch.cuda.mem_get_info()[0] == free0, "the call changed the device's free memory"
         got = out.cpu().numpy().view(np.complex64)
         assert np.all(np.isfinite(got.view(np.float32))), call
         m = jobs.record_metric(got, expected, offs, spec.nchan)
@@ -69,6 +77,7 @@ def test_noalloc_matches_allocating_entry_point():
         gf, ef = got.view(np.float32), expected.view(np.float32)
         wrel = np.max(np.abs(gf[wslots] - ef[wslots]) / np.maximum(np.abs(ef[wslots]), 1e-30))
         assert wrel < W_TOL, (call, wrel)
+        assert np.array_equal(gf, ef), (call, "not bit-identical to gx_subint_device")
 
 
 def test_noalloc_rejects_jobs_over_the_scratch_limit():
