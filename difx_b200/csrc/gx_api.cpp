@@ -24,6 +24,7 @@
 #include "gx_host.h"
 #include "gx_plan.h"
 #include "gx_handle.h"
+#include "gx_fft16.h"
 
 using namespace gx;
 
@@ -35,6 +36,7 @@ int stride_length(int n)  // calcstridelength, configuration.cpp:38-50
   for (unsigned int g = (unsigned int)std::sqrt(n + 0.1);; --g)
     if (n % g == 0) return n / (int)g;
 }
+
 
 long gcdl(long a, long b)
 {
@@ -127,6 +129,7 @@ static gx_status setup(gx_handle *h)
     return h->fail(GX_ERR_ARG, "DATA FRAME SIZE is not a whole number of time samples");
 
   DevJob &J = h->J;
+  J.deltapol_any = 0;
   J.nstations = d.nstations;
   J.nbands = s0.nbands;
   J.nbits = s0.nbits;
@@ -213,6 +216,7 @@ static gx_status setup(gx_handle *h)
       h->band_input[s][b] = D.band_input[b];
     }
     for (int b = 0; b < x.nbands; b++) D.band_polb[b] = (D.deltapol && x.band_pol[b] != 'R') ? 1 : 0;
+    if (D.deltapol) J.deltapol_any = 1;
   }
   // INTERLACEDVDIF stations: one weight row per band after the station rows
   h->interlaced_any = false;
@@ -668,13 +672,9 @@ static gx_status setup(gx_handle *h)
   CKR(h, h->dalloc(&h->d_st, sizeof(DevStation) * d.nstations));
   CKR(h, cudaMemcpy(h->d_st, dst.data(), sizeof(DevStation) * d.nstations, cudaMemcpyHostToDevice));
   {
-    std::vector<float2> tw(J.fftlen);
-    for (int m = 0; m < J.fftlen; m++) {
-      double a = -2.0 * M_PI * (double)m / (double)J.fftlen;
-      tw[m] = make_float2((float)std::cos(a), (float)std::sin(a));
-    }
-    CKR(h, h->dalloc(&h->d_tw, sizeof(float2) * J.fftlen));
-    CKR(h, cudaMemcpy(h->d_tw, tw.data(), sizeof(float2) * J.fftlen, cudaMemcpyHostToDevice));
+    const std::vector<float2> tw = twiddle_table(J.fftlen);
+    CKR(h, h->dalloc(&h->d_tw, sizeof(float2) * tw.size()));
+    CKR(h, cudaMemcpy(h->d_tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice));
     J.twiddle = h->d_tw;
   }
   const size_t spec_elems = (size_t)d.nfreqs * chunk * J.ninputs * J.nchan;
@@ -781,6 +781,33 @@ static gx_status setup(gx_handle *h)
 
 namespace gx {
 
+// Twiddle table of an F-point transform (F a power of two) in the layout of
+// r16::tw_pass_offset: W_F^m, m < F, then the rows of each radix-16 pass of
+// stride 16^p and of the final radix pass.  Entries are formed in double and
+// rounded once.
+std::vector<float2> twiddle_table(int F)
+{
+  auto w = [F](long long e) {
+    const double a = -2.0 * M_PI * (double)(e % F) / (double)F;
+    return make_float2((float)std::cos(a), (float)std::sin(a));
+  };
+  std::vector<float2> tw(F >= 16 ? r16::tw_table_size(F) : F);
+  for (int m = 0; m < F; m++) tw[m] = w(m);
+  if (F < 16) return tw;
+  const int L = r16::log16_floor(F), R0 = F / r16::pow16(L);
+  for (int p = 1; p < L; p++) {
+    const int Ns = r16::pow16(p), off = r16::tw_pass_offset(F, p);
+    for (int r = 1; r < 16; r++)
+      for (int m = 0; m < Ns; m++) tw[off + (r - 1) * Ns + m] = w((long long)r * m * (F / (16 * Ns)));
+  }
+  if (R0 > 1) {
+    const int FR = F / R0, off = r16::tw_final_offset(F);
+    for (int r = 1; r < R0; r++)
+      for (int g = 0; g < FR; g++) tw[off + (r - 1) * FR + g] = w((long long)g * r);
+  }
+  return tw;
+}
+
 // The tables of a host-only open (device -1), handed to callers that place
 // them in their own device memory.
 gx_status plan_job(const gx_job_desc *desc, JobPlan *plan, std::string &err)
@@ -812,11 +839,7 @@ gx_status plan_job(const gx_job_desc *desc, JobPlan *plan, std::string &err)
   plan->prods = h.prods;
   plan->wents = h.wents;
   plan->pairs = h.pairs;
-  plan->twiddle.resize(h.J.fftlen);
-  for (int m = 0; m < h.J.fftlen; m++) {
-    double a = -2.0 * M_PI * (double)m / (double)h.J.fftlen;
-    plan->twiddle[m] = make_float2((float)std::cos(a), (float)std::sin(a));
-  }
+  plan->twiddle = twiddle_table(h.J.fftlen);
   return GX_OK;
 }
 

@@ -51,9 +51,10 @@ struct DevJob {
   int flaglen;
   int lgstride;           // log2(stride): FFT length, channels and stride are powers of two
   int fringe_order;       // FRINGE ROTN ORDER: 1 pre-F linear, 2 pre-F quadratic, 0 post-F (real data)
+  int deltapol_any;       // some station has a second (polarisation B) fractional-sample rotator
   double sampletime;      // us
   double bw;              // MHz
-  const float2 *twiddle;  // exp(-2 pi i m / F), m in [0, F)
+  const float2 *twiddle;  // exp(-2 pi i m / F), m in [0, F), then the pass rows of r16::tw_pass_offset
   float lut[256];         // level of each sample code (VDIF decode table), staged to shared memory
   double lut_offset, lut_div;   // 8-bit codes: level = (code - lut_offset) / lut_div
 };

@@ -125,8 +125,25 @@ __host__ __device__ __forceinline__ void dft16(float2 (&v)[16])
     }
 }
 
-constexpr int log16_floor(int f) { return f >= 65536 ? 4 : (f >= 4096 ? 3 : (f >= 256 ? 2 : (f >= 16 ? 1 : 0))); }
-constexpr int pow16(int l) { return l == 0 ? 1 : 16 * pow16(l - 1); }
+__host__ __device__ constexpr int log16_floor(int f) { return f >= 65536 ? 4 : (f >= 4096 ? 3 : (f >= 256 ? 2 : (f >= 16 ? 1 : 0))); }
+__host__ __device__ constexpr int pow16(int l) { return l == 0 ? 1 : 16 * pow16(l - 1); }
+
+// Twiddle table of an F-point transform as the device holds it: W_F^m for m
+// in [0, F); then one section per radix-16 pass of stride Ns = 16^p
+// (p = 1 .. L - 1), entry (r - 1) Ns + m = W_F^(r m F / (16 Ns)); then, for a
+// final radix R0 > 1, entry (r - 1) (F / R0) + g = W_F^(g r).  Each row holds
+// consecutive m (or g), so the loads of one r by a warp are contiguous.
+__host__ __device__ constexpr int tw_pass_offset(int F, int p)
+{
+  int o = F;
+  for (int q = 1; q < p; q++) o += 15 * pow16(q);
+  return o;
+}
+__host__ __device__ constexpr int tw_final_offset(int F) { return tw_pass_offset(F, log16_floor(F)); }
+__host__ __device__ constexpr int tw_table_size(int F)
+{
+  return tw_final_offset(F) + (F / pow16(log16_floor(F)) > 1 ? (F / pow16(log16_floor(F)) - 1) * pow16(log16_floor(F)) : 0);
+}
 
 template <int F>
 struct Plan {

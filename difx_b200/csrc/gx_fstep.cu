@@ -34,25 +34,11 @@
 #include <mutex>
 #include <utility>
 #include "gx_dev.h"
+#include "gx_fcommon.cuh"
 #include "gx_fft16.h"
 
 namespace gx {
 
-#define GX_TWO_PI 6.283185307179586476925286766559
-
-__device__ __forceinline__ float2 cmul_exact(float2 a, float2 b)
-{
-  // no contraction: same rounding as the reference's separate multiplies/adds
-  float2 r;
-  r.x = __fsub_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y));
-  r.y = __fadd_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x));
-  return r;
-}
-
-__device__ __forceinline__ float2 cmul(float2 a, float2 b)
-{
-  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
 
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -353,79 +339,6 @@ __device__ __forceinline__ BlockParam band_param(const BlockParam *__restrict__ 
   return P;
 }
 
-// Fringe-rotator table entry e of local freq fi: e < S -> sub[e], else step[e - S]
-// (mode.cpp:882-955: FP64 phases, FP32 argument, sincos).
-__device__ __forceinline__ float2 fringe_entry(const DevJob &J, const DevStation &st, int fi, int e,
-                                               const BlockParam &P)
-{
-  if (J.fringe_order == 0) return make_float2(1.0f, 0.0f);   // post-F: no rotation before the FFT
-  const int Sd = J.stride, F = J.fftlen;
-  const double lofreq = st.lofreq[fi];
-  const double looffset = st.looff[fi];
-  const bool looff = (looffset > 0.0 || looffset < 0.0);
-  double ph;
-  if (e < Sd) {
-    double x = ((double)e / (double)F) * P.a;
-    x += P.b;
-    ph = x * lofreq;
-    if (st.fractional_lo) ph += (lofreq - (int)lofreq) * (double)P.integerdelay;
-    if (looff) {
-      ph += ((e * J.sampletime) / 1e6) * -looffset;
-      ph += -looffset * P.fracwalltime;
-      double fl = fabs(looffset) - (int)fabs(looffset);
-      const bool isfrac = fl > (double)0.000000001f;
-      if (looffset < 0) fl = -fl;
-      if (isfrac) ph += -fl * P.intwalltime;
-    }
-  } else if (e < Sd + J.nfr) {
-    const int j = e - Sd;
-    const double xoff = (double)(j * Sd) / (double)F;
-    // quadratic: stepxoff b + stepxoff^2 a (mode.cpp:813-819)
-    const double x = J.fringe_order == 2 ? xoff * P.qb + (xoff * xoff) * P.qa : xoff * P.a;
-    ph = x * lofreq;
-    if (looff) ph += ((j * Sd * J.sampletime) / 1e6) * -looffset;
-  } else {
-    // quadratic only: the per-stride phase step of sub entry k (mode.cpp:810-812)
-    const int k = e - Sd - J.nfr;
-    const double x = ((double)k / (double)F) * (2 * P.qa * ((double)Sd / (double)F));
-    ph = x * lofreq;
-  }
-  const float arg = (float)(-GX_TWO_PI * (ph - (int)ph));
-  float sn, cs;
-  sincosf(arg, &sn, &cs);
-  return make_float2(cs, sn);
-}
-
-// Fractional-sample rotator entry e of local freq fi, polarisation set ps
-// (0: A, 1: B): e < S -> sub[e], else step[e - S] (mode.cpp:1029-1122).
-__device__ __forceinline__ float2 frac_entry(const DevJob &J, const DevStation &st, int fi, int ps, int e,
-                                             const BlockParam &P)
-{
-  const int Sd = J.stride, N = J.nchan, half = J.half;
-  const double sgn = ps == 0 ? 1.0 : -1.0;
-  const float val = (float)((double)P.fracsampleerror - st.clk[fi] + sgn * st.clkdelta[fi] / 2);
-  float cfreq;
-  if (e < Sd) {
-    cfreq = (float)((GX_TWO_PI * (e) * J.bw) / N);
-  } else {
-    const int j = e - Sd;
-    cfreq = st.lsb[fi] ? (float)((-GX_TWO_PI * ((half - j) * Sd) * J.bw) / N)
-                       : (float)((GX_TWO_PI * j * Sd * J.bw) / N);
-  }
-  float arg = __fmul_rn(cfreq, val);
-  if (J.fringe_order == 0 && e < Sd) {
-    // post-F fringe rotation (and LO offset) at the block centre, added to
-    // the first stride's argument for both polarisation sets (mode.cpp:1038-1049, 1085-1096)
-    const double lofreq = st.lofreq[fi];
-    double ph = P.b * lofreq;
-    if (st.fractional_lo) ph += P.integerdelay * (lofreq - (int)lofreq);
-    ph -= ((double)P.intwalltime + P.fracwalltime) * st.looff[fi];
-    arg = __fadd_rn(arg, (float)(-GX_TWO_PI * (ph - (int)ph)));
-  }
-  float sn, cs;
-  sincosf(arg, &sn, &cs);
-  return make_float2(cs, sn);
-}
 
 // Decoded sample n of band bd (real in .x, imaginary in .y for complex data).
 __device__ __forceinline__ float2 decode_sample(const DevJob &J, const uint8_t *__restrict__ data,
@@ -770,13 +683,6 @@ struct R16Launch {
   static constexpr int MINB = GX_R16_MINB * 256 / CTA;   // resident CTAs per SM the registers are sized for
 };
 
-template <int NT, int CTA>
-__device__ __forceinline__ void group_sync(int g)
-{
-  if constexpr (NT == 32) __syncwarp();
-  else if constexpr (NT == CTA) __syncthreads();
-  else asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(NT) : "memory");
-}
 
 // Samples x[j + NT t] (t = 0..15) of band bd of the block described by P,
 // decoded and fringe-rotated (mode.cpp:1160-1183): frame q and in-frame
@@ -892,24 +798,6 @@ __device__ __forceinline__ void r16_fft(float2 (&v)[16], int j, int g, float2 *s
   if constexpr (Pl::R0 > 1) r16::final_pass<F, Pl::R0>(v, j, tw);
 }
 
-// Sideband selection (mode.cpp:1185-1217) for bin j + NT t: false when the bin
-// is not kept; otherwise its channel c (val conjugated for complex LSB).
-template <int F, int CPLX>
-__device__ __forceinline__ bool r16_channel(int t, int j, int lsb, float2 &val, int &c)
-{
-  constexpr int NT = F / 16, NCH = CPLX ? F : F / 2;
-  const int bin = j + NT * t;
-  if (!CPLX) {
-    if (lsb ? (t < 8) : (t >= 8)) return false;   // NT * 8 = F / 2 = NCH
-    c = lsb ? bin - NCH : bin;
-  } else if (!lsb) {
-    c = bin;
-  } else {
-    c = bin == 0 ? 0 : F - bin;
-    if (bin != 0) val.y = -val.y;
-  }
-  return true;
-}
 
 template <int F, int CPLX>
 __global__ void __launch_bounds__(R16Launch<F>::CTA, R16Launch<F>::MINB)
@@ -1016,6 +904,20 @@ static bool use_r16_kernel(const DevJob &J)
   const char *e = getenv("GX_FSTEP_R16_MIN");   // smallest length routed to it (tuning runs)
   const int fmin = e ? atoi(e) : 512;
   return J.fftlen >= fmin && J.fftlen >= 512 && J.fftlen <= 8192 && J.fringe_order != 2;
+}
+
+// Station-block kernel (gx_fstep_sb.cu) for the jobs it takes; GX_FSTEP_SB=0
+// selects the per-band kernels instead (comparison runs).
+bool fstep_sb_eligible(const DevJob &J, bool interlaced);
+cudaError_t fstep_sb_launch(const DevJob &J, const DevStation *stations, int maxnrf, int deltapol,
+                            const SubintArrays &S, int nblk, const BlockParam *bp, float2 *spec, cudaStream_t st);
+size_t fstep_sb_smem_bytes(const DevJob &J, int maxnrf, int deltapol);
+
+static bool use_sb_kernel(const DevJob &J, bool interlaced)
+{
+  const char *e = getenv("GX_FSTEP_SB");
+  if (e && atoi(e) == 0) return false;
+  return fstep_sb_eligible(J, interlaced);
 }
 
 static int r16_tabstride(const DevJob &J)
@@ -1454,6 +1356,10 @@ cudaError_t fstep_launch(const DevJob &J, const DevStation *stations, int maxnrf
   if (S.bandmask) {   // INTERLACEDVDIF: EDV4 per-band validity, one warp per (station, block)
     dim3 grid((nblk + 7) / 8, J.nstations);
     edv4_kernel<<<grid, 256, 0, st>>>(J, stations, S, nblk, bp, weights);
+  }
+  if (use_sb_kernel(J, S.bandmask != nullptr)) {
+    cudaError_t e = fstep_sb_launch(J, stations, maxnrf, J.deltapol_any, S, nblk, bp, spec, st);
+    if (e != cudaErrorNotSupported) return e;
   }
   const size_t sm = fstep_smem_bytes(J, maxnrf, nslots);
   if (use_r16_kernel(J)) {

@@ -117,7 +117,7 @@ extern "C" gx_status gx_subint_device_noalloc(const gx_job_desc *desc, const gx_
   size_t off = 0;
   auto take = [&](size_t bytes) { size_t o = off; off = align256(off + bytes); return o; };
   const size_t o_st = take(sizeof(DevStation) * nst);
-  const size_t o_tw = take(sizeof(float2) * J0.fftlen);
+  const size_t o_tw = take(sizeof(float2) * plan.twiddle.size());
   const size_t o_ctrl = take(sizeof(int32_t) * plan.ctrlstride * nst);
   const size_t o_len = take(sizeof(int64_t) * nst);
   const size_t o_ptr = take(sizeof(uint8_t *) * nst);
@@ -198,7 +198,8 @@ extern "C" gx_status gx_subint_device_noalloc(const gx_job_desc *desc, const gx_
     }                                                                      \
   } while (0)
   NA_CK(cudaMemcpyAsync(d_st, plan.stations.data(), sizeof(DevStation) * nst, cudaMemcpyHostToDevice, st));
-  NA_CK(cudaMemcpyAsync((void *)J.twiddle, plan.twiddle.data(), sizeof(float2) * J.fftlen, cudaMemcpyHostToDevice, st));
+  NA_CK(cudaMemcpyAsync((void *)J.twiddle, plan.twiddle.data(), sizeof(float2) * plan.twiddle.size(),
+                        cudaMemcpyHostToDevice, st));
   NA_CK(cudaMemcpyAsync(d_ctrl, ctrl.data(), sizeof(int32_t) * ctrl.size(), cudaMemcpyHostToDevice, st));
   NA_CK(cudaMemcpyAsync(d_len, lens.data(), sizeof(int64_t) * nst, cudaMemcpyHostToDevice, st));
   NA_CK(cudaMemcpyAsync(d_ptr, sub->data, sizeof(uint8_t *) * nst, cudaMemcpyHostToDevice, st));

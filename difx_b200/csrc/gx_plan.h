@@ -15,12 +15,15 @@ struct JobPlan {
   long long result_length = 0;
   int ctrlstride = 0;
   std::vector<DevStation> stations;
-  std::vector<float2> twiddle;      // exp(-2 pi i m / F)
+  std::vector<float2> twiddle;      // twiddle_table(F)
   std::vector<ProdEntry> prods;
   std::vector<WeightEntry> wents;
   std::vector<int2> pairs;
 };
 
 gx_status plan_job(const gx_job_desc *desc, JobPlan *plan, std::string &err);
+
+// The device twiddle table of an F-point transform (layout of r16::tw_pass_offset).
+std::vector<float2> twiddle_table(int F);
 
 }  // namespace gx
