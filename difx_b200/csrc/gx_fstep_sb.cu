@@ -5,12 +5,13 @@
 // with its own gather, so a time sample of B bands crosses from L2 B times,
 // and they build the fringe rotator once per band although both
 // polarisations of a frequency share it.  Here a group
-//   1. computes the rotator tables of every local frequency of the station
-//      once (fringe: mode.cpp:882-955; fractional sample: mode.cpp:1029-1122),
-//   2. reads each of its time samples once, CHB bytes at a time with one
-//      coalesced load per time sample (consecutive threads, consecutive time
-//      samples), into registers,
-//   3. for every band held in those bytes: decodes its field through the
+//   1. stages the block's time samples into shared memory with 16-byte
+//      asynchronous copies (frame headers skipped; consecutive threads copy
+//      consecutive pieces), so the VDIF crosses from L2 once,
+//   2. meanwhile computes the rotator tables of every local frequency of the
+//      station once (fringe: mode.cpp:882-955; fractional sample:
+//      mode.cpp:1029-1122),
+//   3. for every band: decodes its field of the staged samples through the
 //      shared-memory level table (format_vdif.c:66-146), rotates
 //      (mode.cpp:1160-1183), transforms (16 points per thread, radix-16
 //      passes of gx_fft16.h with twiddle rows read from a contiguous table),
@@ -20,8 +21,9 @@
 // when one of them is invalid (samples of invalid frames decode to zero and
 // are not read).  Jobs outside this kernel's domain (other transform
 // lengths, a non-default array stride, quadratic fringe rotation,
-// INTERLACEDVDIF, time samples that are not whole bytes) use the per-band
-// kernels of gx_fstep.cu.
+// INTERLACEDVDIF, frames whose payload is not a whole number of 16-byte
+// pieces, time samples that are not whole bytes) use the per-band kernels of
+// gx_fstep.cu.
 #include <cstdint>
 #include "gx_dev.h"
 #include "gx_fcommon.cuh"
@@ -46,7 +48,7 @@ __host__ __device__ constexpr int default_stride(int n)
 
 __host__ __device__ constexpr int ilog2(int x) { return x <= 1 ? 0 : 1 + ilog2(x >> 1); }
 
-template <int F, int CPLX, int CHB>
+template <int F, int CPLX, int BPTS>
 struct Cfg {
   static constexpr int NT = F / 16;                    // threads per transform
   static constexpr int CTA = NT >= 256 ? NT : 256;
@@ -57,46 +59,21 @@ struct Cfg {
   static constexpr int NFR = F / S;                    // fringe steps
   static constexpr int HALF = N / S;                   // fractional-sample steps
   static constexpr int JSTEP = NT / S;                 // rotator step index advance per register
+  static constexpr int RAWB = F * BPTS + 32;           // staged time samples (16-byte rounding at both ends)
   static constexpr int MINB = CTA == 256 ? 2 : 1;      // resident CTAs per SM the registers are sized for
   static_assert((S & (S - 1)) == 0 && NT % S == 0, "the stride must be a power of two dividing F / 16");
 };
 
-template <int CHB>
-struct RawWord { using T = uint32_t; };
-template <>
-struct RawWord<8> { using T = uint2; };
-
-// CHB bytes at p: one load when p is aligned, bytes otherwise.
-template <int CHB>
-__device__ __forceinline__ typename RawWord<CHB>::T load_raw(const uint8_t *p, bool aligned)
+// 16-byte copy global -> shared that completes asynchronously (cp.async, L2 only).
+__device__ __forceinline__ void cp_async16(void *sdst, const void *gsrc)
 {
-  if constexpr (CHB == 8) {
-    if (aligned) return __ldg(reinterpret_cast<const uint2 *>(p));
-    uint2 w = make_uint2(0u, 0u);
-#pragma unroll
-    for (int b = 0; b < 4; b++) {
-      w.x |= (uint32_t)__ldg(p + b) << (8 * b);
-      w.y |= (uint32_t)__ldg(p + 4 + b) << (8 * b);
-    }
-    return w;
-  } else {
-    if (aligned) {
-      if constexpr (CHB == 4) return __ldg(reinterpret_cast<const uint32_t *>(p));
-      else if constexpr (CHB == 2) return (uint32_t)__ldg(reinterpret_cast<const unsigned short *>(p));
-      else return (uint32_t)__ldg(p);
-    }
-    uint32_t w = 0u;
-#pragma unroll
-    for (int b = 0; b < CHB; b++) w |= (uint32_t)__ldg(p + b) << (8 * b);
-    return w;
-  }
+  const unsigned int d = (unsigned int)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gsrc) : "memory");
 }
-
-template <int CHB>
-__device__ __forceinline__ uint32_t pick_word(const typename RawWord<CHB>::T &w, int hi)
+// Waits for this thread's outstanding cp.async copies.
+__device__ __forceinline__ void cp_async_wait_all()
 {
-  if constexpr (CHB == 8) return hi ? w.y : w.x;
-  else return w;
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
 // Radix-16 pass of stride Ns > 1 with its twiddle row from the table section
@@ -157,15 +134,15 @@ __device__ __forceinline__ void fft(float2 (&v)[16], int j, int g, float2 *xb, c
   }
 }
 
-template <int F, int CPLX, int CHB>
-__global__ void __launch_bounds__(Cfg<F, CPLX, CHB>::CTA, Cfg<F, CPLX, CHB>::MINB)
+template <int F, int CPLX, int BPTS>
+__global__ void __launch_bounds__(Cfg<F, CPLX, BPTS>::CTA, Cfg<F, CPLX, BPTS>::MINB)
 fstep_sb_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays S, const BlockParam *__restrict__ bp,
                 int nblk, int blocks_per_cta, int tabstride, float2 *__restrict__ spec)
 {
-  using C = Cfg<F, CPLX, CHB>;
+  using C = Cfg<F, CPLX, BPTS>;
   using Pl = r16::Plan<F>;
   constexpr int NT = C::NT, CTA = C::CTA, G = C::G, N = C::N, SD = C::S, LGS = C::LGS, NFR = C::NFR,
-                HALF = C::HALF;
+                HALF = C::HALF, JSTEP = C::JSTEP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ float s_lut[256];
   const int s = blockIdx.y;
@@ -174,19 +151,20 @@ fstep_sb_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays 
   for (int i = tid; i < 256; i += CTA) s_lut[i] = J.lut[i];
   __syncthreads();
 
-  float2 *xb = reinterpret_cast<float2 *>(smem_raw) + (size_t)g * (Pl::SMEM + tabstride);
+  // per group: exchange buffer, rotator tables, staged time samples
+  float2 *xb = reinterpret_cast<float2 *>(smem_raw + (size_t)g * ((Pl::SMEM + tabstride) * sizeof(float2) + C::RAWB));
   float2 *tab = xb + Pl::SMEM;
+  unsigned char *raw = reinterpret_cast<unsigned char *>(tab + tabstride);
   const int nlf = st.nrecfreqs, nps = st.deltapol ? 2 : 1;
   const int lfstride = SD + NFR + nps * (SD + HALF);
   const float2 *__restrict__ tw = J.twiddle;
 
   const uint8_t *data = S.data[s];
-  const int fsamp = J.framesamples, fbytes = J.framebytes;
-  const int bpts = J.bps_num / J.bps_den;                  // bytes per time sample (whole bytes here)
-  const int nchunk = bpts / CHB, bpc = J.nbands / nchunk;  // chunks of CHB bytes; bands per chunk
+  const int fsamp = J.framesamples, fbytes = J.framebytes, paybytes = fsamp * BPTS;
   const int fbits = J.nbits * (CPLX ? 2 : 1);
   const uint32_t cmask = (1u << J.nbits) - 1u;
-  const bool aligned = ((reinterpret_cast<uintptr_t>(data) | (uintptr_t)fbytes | (uintptr_t)bpts) & (CHB - 1)) == 0;
+  // 16-byte copies need a 16-byte aligned buffer (the frame layout is checked on the host)
+  const bool aligned = (reinterpret_cast<uintptr_t>(data) & 15) == 0;
 
   const int b0 = blockIdx.x * blocks_per_cta;
   const int nbk = min(blocks_per_cta, nblk - b0);
@@ -201,100 +179,125 @@ fstep_sb_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays 
       }
       continue;
     }
-    group_sync<NT, CTA>(g);   // the previous item is done with the tables and the exchange buffer
+    const bool allvalid = P.nframes >= 64 ? P.validmask == ~0ull : P.validmask == ((1ull << P.nframes) - 1ull);
+    group_sync<NT, CTA>(g);   // the previous item is done with the tables, samples and exchange buffer
+    // Stage the block's time samples: payload bytes [p0, pend) of the frames,
+    // headers skipped, in 16-byte pieces (a payload is whole pieces, so none
+    // straddles a frame); pieces of invalid frames are not read.
+    const long long pstart = (long long)P.nearestsample * BPTS;
+    const long long p0 = pstart & ~15ll;
+    const int npieces = (int)(((((long long)(P.nearestsample + F) * BPTS + 15) & ~15ll) - p0) >> 4);
+    {
+      const long long pos = p0 + 16 * j;
+      int q = (int)(pos / paybytes);
+      int within = (int)(pos - (long long)q * paybytes);
+      for (int k = j; k < npieces; k += NT) {
+        if (allvalid || ((P.validmask >> (q - P.fr0)) & 1ull)) {
+          const uint8_t *src = data + (long long)q * fbytes + 32 + within;
+          if (aligned) {
+            cp_async16(raw + 16 * k, src);
+          } else {
+#pragma unroll
+            for (int b = 0; b < 16; b++) raw[16 * k + b] = __ldg(src + b);
+          }
+        }
+        within += 16 * NT;
+        while (within >= paybytes) {
+          within -= paybytes;
+          q++;
+        }
+      }
+    }
+    // rotator tables of every local frequency while the copies are in flight
     for (int lf = 0; lf < nlf; lf++) {
       float2 *tl = tab + lf * lfstride;
       for (int e = j; e < SD + NFR; e += NT) tl[e] = fringe_entry(J, st, lf, e, P);
       for (int ps = 0; ps < nps; ps++)
         for (int e = j; e < SD + HALF; e += NT) tl[SD + NFR + ps * (SD + HALF) + e] = frac_entry(J, st, lf, ps, e, P);
     }
+    cp_async_wait_all();
     group_sync<NT, CTA>(g);
 
-    const bool allvalid = P.nframes >= 64 ? P.validmask == ~0ull : P.validmask == ((1ull << P.nframes) - 1ull);
-    int q0, r0;
-    {
+    // samples j + NT t of invalid frames decode to zero
+    unsigned int vmask = 0xFFFFu;
+    if (!allvalid) {
       const int smp0 = P.nearestsample + j;
-      q0 = smp0 / fsamp;
-      r0 = smp0 - q0 * fsamp;
-      q0 -= P.fr0;
-    }
-    for (int ch = 0; ch < nchunk; ch++) {
-      // time samples j + NT t of this chunk's bytes; NT <= samples per frame, so
-      // a step crosses at most one frame boundary
-      typename RawWord<CHB>::T raw[16];
-      unsigned int vmask = 0xFFFFu;
-      {
-        int q = q0, r = r0;
-        const uint8_t *fr = data + ((long long)P.fr0 + q) * fbytes + 32 + ch * CHB;
-        bool ok = allvalid || ((P.validmask >> q) & 1ull);
+      int q = smp0 / fsamp, r = smp0 - q * fsamp;
+      q -= P.fr0;
 #pragma unroll
-        for (int t = 0; t < 16; t++) {
-          if (ok) raw[t] = load_raw<CHB>(fr + r * bpts, aligned);
-          else {
-            raw[t] = typename RawWord<CHB>::T{};
-            vmask &= ~(1u << t);
-          }
-          r += NT;
-          if (r >= fsamp) {
-            r -= fsamp;
-            q++;
-            fr += fbytes;
-            ok = allvalid || (q < 64 && ((P.validmask >> q) & 1ull));
-          }
+      for (int t = 0; t < 16; t++) {
+        if (!((P.validmask >> q) & 1ull)) vmask &= ~(1u << t);
+        r += NT;
+        while (r >= fsamp) {
+          r -= fsamp;
+          q++;
         }
+        if (q > 63) q = 63;
       }
+    }
+    const unsigned char *rj = raw + (int)(pstart - p0) + j * BPTS;   // time sample j of the block
 #pragma unroll 1
-      for (int kb = 0; kb < bpc; kb++) {
-        const int bd = ch * bpc + kb;
-        const int bit0 = kb * fbits, hi = bit0 >> 5, sh = bit0 & 31;
-        const int lf = st.band_localfreq[bd];
-        const float2 *rs = tab + lf * lfstride;
-        const float2 *rp = rs + SD;
-        const float2 *fs = rp + NFR + (st.band_polb[bd] ? SD + HALF : 0);
-        const float2 *fp = fs + SD;
-        float2 v[16];
-        {
-          // decode and fringe-rotate: x[n] sub[n mod S] step[n / S]; S divides NT,
-          // so the sub entry is the same for all 16 samples of the thread
-          const float2 rsk = rs[j & (SD - 1)];
-          const float2 *rpj = rp + (j >> LGS);
+    for (int bd = 0; bd < J.nbands; bd++) {
+      const int bit0 = bd * fbits, sh = bit0 & 7;
+      const unsigned char *rb = rj + (bit0 >> 3);
+      const int lf = st.band_localfreq[bd];
+      const float2 *rs = tab + lf * lfstride;
+      const float2 *rp = rs + SD;
+      const float2 *fs = rp + NFR + (st.band_polb[bd] ? SD + HALF : 0);
+      const float2 *fp = fs + SD;
+      float2 v[16];
+      {
+        // decode and fringe-rotate: x[n] sub[n mod S] step[n / S]; S divides NT,
+        // so the sub entry is the same for all 16 samples of the thread
+        const float2 rsk = rs[j & (SD - 1)];
+        const float2 *rpj = rp + (j >> LGS);
+        if (CPLX && fbits == 16) {   // 8-bit complex: one (re, im) byte pair
 #pragma unroll
           for (int t = 0; t < 16; t++) {
-            const uint32_t w = pick_word<CHB>(raw[t], hi);
-            float2 u;
-            u.x = s_lut[(w >> sh) & cmask];
-            u.y = CPLX ? s_lut[(w >> (sh + J.nbits)) & cmask] : 0.f;
-            const float2 rot = cmul(rsk, rpj[C::JSTEP * t]);
-            v[t] = CPLX ? cmul(rot, u) : make_float2(u.x * rot.x, u.x * rot.y);
-          }
-          if (!allvalid) {
-#pragma unroll
-            for (int t = 0; t < 16; t++)
-              if (!((vmask >> t) & 1u)) v[t] = make_float2(0.f, 0.f);
-          }
-        }
-        fft<F, CTA>(v, j, g, xb, tw);
-        // register t holds bin j + NT t: sideband selection, fractional-sample
-        // correction sub[c mod S] step[c / S] (c mod S fixed per thread), store
-        const int lsb = st.lsb[lf];
-        const int f = st.freq_index[lf];
-        float2 *drow = spec + (((size_t)f * nblk + bi) * J.ninputs + st.band_input[bd]) * N;
-        const float2 fsk = fs[((CPLX && lsb) ? -j : j) & (SD - 1)];
-        auto emit = [&](int c, float2 val) { drow[c] = cmul(val, cmul(fsk, fp[c >> LGS])); };
-        if (lsb) {
-#pragma unroll
-          for (int t = 0; t < 16; t++) {
-            float2 val = v[t];
-            int c;
-            if (r16_channel<F, CPLX>(t, j, 1, val, c)) emit(c, val);
+            const uint32_t w = *reinterpret_cast<const unsigned short *>(rb + NT * BPTS * t);
+            const float2 u = make_float2(s_lut[w & 255u], s_lut[w >> 8]);
+            v[t] = cmul(cmul(rsk, rpj[JSTEP * t]), u);
           }
         } else {
 #pragma unroll
           for (int t = 0; t < 16; t++) {
-            float2 val = v[t];
-            int c;
-            if (r16_channel<F, CPLX>(t, j, 0, val, c)) emit(c, val);
+            const uint32_t w = rb[NT * BPTS * t];
+            const float2 rot = cmul(rsk, rpj[JSTEP * t]);
+            const float ux = s_lut[(w >> sh) & cmask];
+            if (CPLX) v[t] = cmul(rot, make_float2(ux, s_lut[(w >> (sh + J.nbits)) & cmask]));
+            else v[t] = make_float2(ux * rot.x, ux * rot.y);
           }
+        }
+        if (!allvalid) {
+#pragma unroll
+          for (int t = 0; t < 16; t++)
+            if (!((vmask >> t) & 1u)) v[t] = make_float2(0.f, 0.f);
+        }
+      }
+      fft<F, CTA>(v, j, g, xb, tw);
+      // register t holds bin j + NT t: sideband selection, fractional-sample
+      // correction sub[c mod S] step[c / S] (c mod S fixed per thread), store
+      const int lsb = st.lsb[lf];
+      const int f = st.freq_index[lf];
+      float2 *drow = spec + (((size_t)f * nblk + bi) * J.ninputs + st.band_input[bd]) * N;
+      if (CPLX && lsb) {
+        const float2 fsk = fs[(-j) & (SD - 1)];
+#pragma unroll
+        for (int t = 0; t < 16; t++) {
+          float2 val = v[t];
+          int c;
+          r16_channel<F, CPLX>(t, j, 1, val, c);
+          drow[c] = cmul(val, cmul(fsk, fp[c >> LGS]));
+        }
+      } else {
+        // channel c = j + NT t' with t' = t (upper sideband), t - 8 (real lower sideband)
+        const float2 fsk = fs[j & (SD - 1)];
+        const float2 *fpj = fp + (j >> LGS);
+        float2 *dj = drow + j;
+#pragma unroll
+        for (int t = 0; t < (CPLX ? 16 : 8); t++) {
+          const float2 val = (!CPLX && lsb) ? v[t + 8] : v[t];
+          dj[NT * t] = cmul(val, cmul(fsk, fpj[JSTEP * t]));
         }
       }
     }
@@ -313,49 +316,51 @@ bool fstep_sb_eligible(const DevJob &J, bool interlaced)
   const int bits_ts = J.nbands * J.nbits * (J.cplx ? 2 : 1);
   if (bits_ts % 8 || J.bps_num != bits_ts / 8 * J.bps_den) return false;
   const int bpts = bits_ts / 8;
-  const int chb = bpts >= 4 ? 4 : bpts;
-  if (bpts < chb || bpts % chb) return false;
-  const int nchunk = bpts / chb;
-  if (J.nbands % nchunk) return false;
+  if (J.cplx ? (bpts != 4 && bpts != 8 && bpts != 16) : (bpts != 1 && bpts != 2 && bpts != 4 && bpts != 8))
+    return false;
   const int fbits = J.nbits * (J.cplx ? 2 : 1);
-  if ((J.nbands / nchunk) * fbits != chb * 8) return false;   // the chunk's bands fill its bytes
-  if (F / 16 > J.framesamples) return false;
-  if (J.framebytes < 32) return false;
+  if (fbits > 8 && fbits != 16) return false;   // fields within a byte, or one (re, im) byte pair
+  const int paybytes = J.framesamples * bpts;
+  if (J.framebytes != 32 + paybytes || paybytes % 16) return false;
   return true;
+}
+
+static size_t sb_tab(const DevJob &J, int maxnrf, int deltapol)
+{
+  const int S = J.stride, nfr = J.fftlen / S, half = J.nchan / S;
+  return (size_t)((maxnrf * (S + nfr + (deltapol ? 2 : 1) * (S + half)) + 1) & ~1);
 }
 
 size_t fstep_sb_smem_bytes(const DevJob &J, int maxnrf, int deltapol)
 {
   const int F = J.fftlen, NT = F / 16, G = (NT >= 256 ? NT : 256) / NT;
-  const int S = J.stride, nfr = F / S, half = J.nchan / S;
-  const int tab = maxnrf * (S + nfr + (deltapol ? 2 : 1) * (S + half));
-  return (size_t)G * (F + F / 16 + ((tab + 1) & ~1)) * sizeof(float2);
+  const int bpts = J.nbands * J.nbits * (J.cplx ? 2 : 1) / 8;
+  return (size_t)G * ((F + F / 16 + sb_tab(J, maxnrf, deltapol)) * sizeof(float2) + (size_t)(F * bpts + 32));
 }
 
 cudaError_t fstep_sb_launch(const DevJob &J, const DevStation *stations, int maxnrf, int deltapol,
                             const SubintArrays &S, int nblk, const BlockParam *bp, float2 *spec, cudaStream_t st)
 {
   const int F = J.fftlen, NT = F / 16, G = (NT >= 256 ? NT : 256) / NT;
-  const int S_ = J.stride, nfr = F / S_, half = J.nchan / S_;
-  const int tab = maxnrf * (S_ + nfr + (deltapol ? 2 : 1) * (S_ + half));
-  const int tabstride = (tab + 1) & ~1;
+  const int tabstride = (int)sb_tab(J, maxnrf, deltapol);
   const size_t sm = fstep_sb_smem_bytes(J, maxnrf, deltapol);
+  if (sm > 227 * 1024) return cudaErrorNotSupported;
   const int bpts = J.nbands * J.nbits * (J.cplx ? 2 : 1) / 8;
-  const int chb = bpts >= 4 ? 4 : bpts;
   const int bpc = 4 * G;   // four items per group
   dim3 grid((nblk + bpc - 1) / bpc, J.nstations);
-#define GX_SB_CASE(FLV, CX, CB)                                                                         \
-  if (F == FLV && J.cplx == CX && chb == CB) {                                                          \
-    using K = sb::Cfg<FLV, CX, CB>;                                                                     \
-    cudaError_t e = smem_opt_in((const void *)sb::fstep_sb_kernel<FLV, CX, CB>, sm);                    \
+#define GX_SB_CASE(FLV, CX, BP)                                                                         \
+  if (F == FLV && J.cplx == CX && bpts == BP) {                                                         \
+    using K = sb::Cfg<FLV, CX, BP>;                                                                     \
+    cudaError_t e = smem_opt_in((const void *)sb::fstep_sb_kernel<FLV, CX, BP>, sm);                    \
     if (e != cudaSuccess) return e;                                                                     \
-    sb::fstep_sb_kernel<FLV, CX, CB><<<grid, K::CTA, sm, st>>>(J, stations, S, bp, nblk, bpc, tabstride, spec); \
+    sb::fstep_sb_kernel<FLV, CX, BP><<<grid, K::CTA, sm, st>>>(J, stations, S, bp, nblk, bpc, tabstride, spec); \
     return cudaGetLastError();                                                                          \
   }
-  GX_SB_CASE(512, 0, 1) GX_SB_CASE(1024, 0, 1) GX_SB_CASE(2048, 0, 1) GX_SB_CASE(4096, 0, 1) GX_SB_CASE(8192, 0, 1)
-  GX_SB_CASE(512, 0, 2) GX_SB_CASE(1024, 0, 2) GX_SB_CASE(2048, 0, 2) GX_SB_CASE(4096, 0, 2) GX_SB_CASE(8192, 0, 2)
-  GX_SB_CASE(512, 0, 4) GX_SB_CASE(1024, 0, 4) GX_SB_CASE(2048, 0, 4) GX_SB_CASE(4096, 0, 4) GX_SB_CASE(8192, 0, 4)
-  GX_SB_CASE(512, 1, 4) GX_SB_CASE(1024, 1, 4) GX_SB_CASE(2048, 1, 4) GX_SB_CASE(4096, 1, 4) GX_SB_CASE(8192, 1, 4)
+#define GX_SB_SIZES(CX, BP) \
+  GX_SB_CASE(512, CX, BP) GX_SB_CASE(1024, CX, BP) GX_SB_CASE(2048, CX, BP) GX_SB_CASE(4096, CX, BP) GX_SB_CASE(8192, CX, BP)
+  GX_SB_SIZES(0, 1) GX_SB_SIZES(0, 2) GX_SB_SIZES(0, 4) GX_SB_SIZES(0, 8)
+  GX_SB_SIZES(1, 4) GX_SB_SIZES(1, 8) GX_SB_SIZES(1, 16)
+#undef GX_SB_SIZES
 #undef GX_SB_CASE
   return cudaErrorNotSupported;
 }
