@@ -911,7 +911,6 @@ static bool use_r16_kernel(const DevJob &J)
 bool fstep_sb_eligible(const DevJob &J, bool interlaced);
 cudaError_t fstep_sb_launch(const DevJob &J, const DevStation *stations, int maxnrf, int deltapol,
                             const SubintArrays &S, int nblk, const BlockParam *bp, float2 *spec, cudaStream_t st);
-size_t fstep_sb_smem_bytes(const DevJob &J, int maxnrf, int deltapol);
 
 static bool use_sb_kernel(const DevJob &J, bool interlaced)
 {

@@ -35,6 +35,7 @@ cudaError_t smem_opt_in(const void *kernel, size_t bytes);
 
 namespace sb {
 
+
 // Array stride the reference derives from a channel count when the .input
 // leaves it 0 (calcstridelength, configuration.cpp:37-50).
 __host__ __device__ constexpr int default_stride(int n)
@@ -60,7 +61,8 @@ struct Cfg {
   static constexpr int HALF = N / S;                   // fractional-sample steps
   static constexpr int JSTEP = NT / S;                 // rotator step index advance per register
   static constexpr int RAWB = F * BPTS + 32;           // staged time samples (16-byte rounding at both ends)
-  static constexpr int MINB = CTA == 256 ? 2 : 1;      // resident CTAs per SM the registers are sized for
+  // two resident CTAs per SM: 128 registers a thread up to 4096 points, 64 at 8192
+  static constexpr int MINB = 2;
   static_assert((S & (S - 1)) == 0 && NT % S == 0, "the stride must be a power of two dividing F / 16");
 };
 
@@ -186,6 +188,7 @@ fstep_sb_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays 
     // straddles a frame); pieces of invalid frames are not read.
     const long long pstart = (long long)P.nearestsample * BPTS;
     const long long p0 = pstart & ~15ll;
+    const int off0 = (int)(pstart - p0);   // staged position of the block's first time sample
     const int npieces = (int)(((((long long)(P.nearestsample + F) * BPTS + 15) & ~15ll) - p0) >> 4);
     {
       const long long pos = p0 + 16 * j;
@@ -235,7 +238,7 @@ fstep_sb_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays 
         if (q > 63) q = 63;
       }
     }
-    const unsigned char *rj = raw + (int)(pstart - p0) + j * BPTS;   // time sample j of the block
+    const unsigned char *rj = raw + off0 + j * BPTS;   // time sample j of the block
 #pragma unroll 1
     for (int bd = 0; bd < J.nbands; bd++) {
       const int bit0 = bd * fbits, sh = bit0 & 7;
