@@ -43,6 +43,7 @@
 // nonzero status in *err, drains its own copies and MMAs (again bounded),
 // releases its tensor memory and returns.
 #include <cstdint>
+#include <cstdlib>
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_fp16.h>
@@ -54,12 +55,10 @@ namespace {
 
 constexpr int kNI = 128;                     // inputs per frequency = MMA M
 constexpr int kKT = 16;                      // FFT blocks per K-tile = one MMA K step for FP16
-constexpr int kStages = 4;                   // FP32 staging ring depth (tile loads in flight)
 constexpr int kOpStages = 2;                 // FP16 operand stages
 constexpr int kThreads = 320;                // 1 load warp, 1 MMA warp, 8 converter warps
 constexpr uint32_t kTmemCols = 512;          // 2 channels x (128 Re + 128 P) FP32 columns
 constexpr uint32_t kRowBytes = kNI * 16;     // one block of a channel pair: 128 inputs x 2 channels x float2
-constexpr uint32_t kStageBytes = kKT * kRowBytes;         // 32 KB
 constexpr uint32_t kLBO = 128;               // byte step between the two 8-block core matrices of a row group
 constexpr uint32_t kSBO = (kKT / 8) * 128;   // byte step between 8-row groups
 constexpr uint32_t kOpChanBytes = 2 * kNI * kKT * 2;      // [Xi ; Xr]: 256 rows x 16 FP16 = 8 KB
@@ -67,9 +66,17 @@ constexpr uint32_t kXrOffset = (kNI / 8) * kSBO;          // rows 128.. (Xr) sta
 constexpr int kPRow = kNI + 1;               // padded row of the P matrices parked in shared memory
 constexpr int kVCols = 8;                    // columns of V per epilogue slice (one 128-byte line per row)
 constexpr int kVRow = kVCols + 1;            // padded slice row, float4
-static_assert((2 * kNI * kPRow + 2 * kNI) * 4 + kNI * kVRow * 16 <=
-                  kStages * kStageBytes + kOpStages * 2 * kOpChanBytes,
-              "epilogue tables must fit in the staging ring and operand stages");
+// FP32 staging ring: RP channel pairs per tile row (RP = 2: whole 32-byte
+// sectors, half the row requests of RP = 1), as many stages as fit beside the
+// operand stages.
+template <bool HILO, int RP>
+struct TcRing {
+  static constexpr uint32_t kStageBytes = kKT * kRowBytes * RP;   // 32 or 64 KB
+  static constexpr int kStages = RP == 1 ? 4 : (HILO ? 2 : 3);
+  static constexpr uint32_t kOpStageBytes = (HILO ? 2 : 1) * 2 * kOpChanBytes;
+  static_assert((2 * kNI * kPRow + 2 * kNI) * 4 + kNI * kVRow * 16 <= kStages * kStageBytes + kOpStages * kOpStageBytes,
+                "epilogue tables must fit in the staging ring and operand stages");
+};
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
@@ -235,20 +242,22 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar)
 // of its neighbours.
 constexpr int kConvThreads = 256;
 constexpr int kConvWarp0 = 2;
-constexpr int kNumBars = 2 * kStages + 2 * kOpStages + 1;   // full, empty, opfull, opempty, done
+constexpr int kMaxStages = 4;
+constexpr int kNumBars = 2 * kMaxStages + 2 * kOpStages + 1;   // full, empty, opfull, opempty, done
 
-template <bool HILO>
+template <bool HILO, int RP>
 __global__ void __launch_bounds__(kThreads, 1)
 xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, int nfreqs, int ks, int ninputs,
                const float *__restrict__ scale, float4 *__restrict__ acc, int accumulate, int *__restrict__ err)
 {
-  constexpr uint32_t kParts = HILO ? 2 : 1;
-  constexpr uint32_t kOpStageBytes = kParts * 2 * kOpChanBytes;
+  constexpr int kStages = TcRing<HILO, RP>::kStages;
+  constexpr uint32_t kStageBytes = TcRing<HILO, RP>::kStageBytes;
+  constexpr uint32_t kOpStageBytes = TcRing<HILO, RP>::kOpStageBytes;
   extern __shared__ __align__(1024) unsigned char smem[];
   unsigned char *staging = smem;
   unsigned char *ops = smem + kStages * kStageBytes;
   uint64_t *bars = reinterpret_cast<uint64_t *>(ops + kOpStages * kOpStageBytes);
-  uint64_t *full = bars, *empty = bars + kStages, *opfull = bars + 2 * kStages;
+  uint64_t *full = bars, *empty = bars + kMaxStages, *opfull = bars + 2 * kMaxStages;
   uint64_t *opempty = opfull + kOpStages, *done = opempty + kOpStages;
   uint32_t *s_tmem = reinterpret_cast<uint32_t *>(bars + kNumBars);
   volatile int *s_abort = reinterpret_cast<volatile int *>(s_tmem + 1);
@@ -299,7 +308,7 @@ xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, i
       }
       const uint32_t bar = smem_u32(full + st);
       mbar_expect_tx(bar, kStageBytes);
-      tma_load_4d(smem_u32(staging + st * kStageBytes), &spec_map, 4 * p, 0, (t0 + u) * kKT, f, bar);
+      tma_load_4d(smem_u32(staging + st * kStageBytes), &spec_map, 4 * RP * (p / RP), 0, (t0 + u) * kKT, f, bar);
       issued = u + 1;
     }
   } else if (warp == 1 && lane == 0) {
@@ -348,15 +357,16 @@ xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, i
         break;
       }
       const int kv = min(kKT, nblk - (t0 + t) * kKT);
-      const float4 *stg = reinterpret_cast<const float4 *>(staging + st * kStageBytes);
+      // row (k, r) of the stage holds RP channel pairs; this CTA's is pair p % RP
+      const float4 *stg = reinterpret_cast<const float4 *>(staging + st * kStageBytes) + (p % RP);
       uint32_t re0[4], im0[4], re1[4], im1[4];
       uint32_t lre0[4], lim0[4], lre1[4], lim1[4];
 #pragma unroll
       for (int j = 0; j < 4; j++) {
         const int k = g * 8 + 2 * j;
         const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 a = (k < kv) ? stg[k * kNI + r] : zero;          // (c0.re, c0.im, c1.re, c1.im) at block k
-        const float4 b = (k + 1 < kv) ? stg[(k + 1) * kNI + r] : zero;
+        const float4 a = (k < kv) ? stg[(k * kNI + r) * RP] : zero;   // (c0.re, c0.im, c1.re, c1.im) at block k
+        const float4 b = (k + 1 < kv) ? stg[((k + 1) * kNI + r) * RP] : zero;
         if (HILO) {
           split2(a.x * s0, b.x * s0, re0[j], lre0[j]);
           split2(a.y * s0, b.y * s0, im0[j], lim0[j]);
@@ -549,10 +559,22 @@ finalise_tc_kernel(const TcProdEntry *__restrict__ prods, const TcRowEntry *__re
 }  // namespace
 
 
+// Channel pairs per staged tile row: 1 (16-byte rows, four stages) unless
+// GX_TC_ROW_PAIRS=2 (32-byte rows, fewer stages; measured no faster on C3).
+static int tc_row_pairs()
+{
+  const char *e = getenv("GX_TC_ROW_PAIRS");
+  return (e && atoi(e) == 2) ? 2 : 1;
+}
+
 size_t xmac_tc_smem_bytes(bool hilo)
 {
+  const int rp = tc_row_pairs();
+  const size_t ring = rp == 1 ? (size_t)TcRing<true, 1>::kStages * TcRing<true, 1>::kStageBytes
+                              : (hilo ? (size_t)TcRing<true, 2>::kStages * TcRing<true, 2>::kStageBytes
+                                      : (size_t)TcRing<false, 2>::kStages * TcRing<false, 2>::kStageBytes);
   const size_t ops = (size_t)kOpStages * (hilo ? 2 : 1) * 2 * kOpChanBytes;
-  return (size_t)kStages * kStageBytes + ops + kNumBars * 8 + 16;
+  return ring + ops + kNumBars * 8 + 16;
 }
 
 cudaError_t xmac_tc_launch(const float2 *spec, int nblk, int N, int nfreqs, int ninputs, int ks, bool hilo,
@@ -577,7 +599,8 @@ cudaError_t xmac_tc_launch(const float2 *spec, int nblk, int N, int nfreqs, int 
   const cuuint64_t dims[4] = {(cuuint64_t)(2 * N), (cuuint64_t)ninputs, (cuuint64_t)nblk, (cuuint64_t)nfreqs};
   const cuuint64_t strides[3] = {(cuuint64_t)(2 * N) * 4, (cuuint64_t)(2 * N) * 4 * ninputs,
                                  (cuuint64_t)(2 * N) * 4 * ninputs * nblk};
-  const cuuint32_t box[4] = {4, (cuuint32_t)kNI, (cuuint32_t)kKT, 1};
+  const int rp = tc_row_pairs();
+  const cuuint32_t box[4] = {(cuuint32_t)(4 * rp), (cuuint32_t)kNI, (cuuint32_t)kKT, 1};
   const cuuint32_t estr[4] = {1, 1, 1, 1};
   CUresult cr = encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float2 *>(spec), dims, strides, box, estr,
                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -585,15 +608,15 @@ cudaError_t xmac_tc_launch(const float2 *spec, int nblk, int N, int nfreqs, int 
   if (cr != CUDA_SUCCESS) return cudaErrorInvalidValue;
   const size_t sm = xmac_tc_smem_bytes(hilo);
   dim3 grid(N / 2, nfreqs, ks);
-#define GX_TC_CASE(H)                                                                                       \
-  if (hilo == H) {                                                                                          \
-    cudaError_t e = smem_opt_in((const void *)xmac_tc_kernel<H>, sm);                                       \
+#define GX_TC_CASE(H, RPV)                                                                                  \
+  if (hilo == H && rp == RPV) {                                                                             \
+    cudaError_t e = smem_opt_in((const void *)xmac_tc_kernel<H, RPV>, sm);                                  \
     if (e != cudaSuccess) return e;                                                                         \
-    xmac_tc_kernel<H><<<grid, kThreads, sm, st>>>(map, nblk, N / 2, nfreqs, ks, ninputs, scale, acc, accumulate, \
-                                                  err);                                                     \
+    xmac_tc_kernel<H, RPV><<<grid, kThreads, sm, st>>>(map, nblk, N / 2, nfreqs, ks, ninputs, scale, acc,   \
+                                                       accumulate, err);                                    \
     return cudaGetLastError();                                                                              \
   }
-  GX_TC_CASE(true) GX_TC_CASE(false)
+  GX_TC_CASE(true, 2) GX_TC_CASE(false, 2) GX_TC_CASE(true, 1) GX_TC_CASE(false, 1)
 #undef GX_TC_CASE
   return cudaErrorInvalidValue;
 }
