@@ -56,7 +56,6 @@ namespace {
 constexpr int kNI = 128;                     // inputs per frequency = MMA M
 constexpr int kKT = 16;                      // FFT blocks per K-tile = one MMA K step for FP16
 constexpr int kOpStages = 2;                 // FP16 operand stages
-constexpr int kThreads = 320;                // 1 load warp, 1 MMA warp, 8 converter warps
 constexpr uint32_t kTmemCols = 512;          // 2 channels x (128 Re + 128 P) FP32 columns
 constexpr uint32_t kRowBytes = kNI * 16;     // one block of a channel pair: 128 inputs x 2 channels x float2
 constexpr uint32_t kLBO = 128;               // byte step between the two 8-block core matrices of a row group
@@ -240,13 +239,15 @@ __device__ __forceinline__ void mbar_arrive(uint32_t bar)
 // operands and later run the epilogue.  The roles hand stages to each other
 // through mbarriers only, so a tile's load, conversion and MMAs overlap those
 // of its neighbours.
-constexpr int kConvThreads = 256;
+constexpr int kConvThreads = 256;            // converter threads that also run the epilogue
 constexpr int kConvWarp0 = 2;
+// threads of a CTA with CW converter warps: 1 load warp, 1 MMA warp, CW converters
+__host__ __device__ constexpr int tc_threads(int cw) { return 32 * (kConvWarp0 + cw); }
 constexpr int kMaxStages = 4;
 constexpr int kNumBars = 2 * kMaxStages + 2 * kOpStages + 1;   // full, empty, opfull, opempty, done
 
-template <bool HILO, int RP>
-__global__ void __launch_bounds__(kThreads, 1)
+template <bool HILO, int RP, int CW>
+__global__ void __launch_bounds__(tc_threads(CW), 1)
 xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, int nfreqs, int ks, int ninputs,
                const float *__restrict__ scale, float4 *__restrict__ acc, int accumulate, int *__restrict__ err)
 {
@@ -268,7 +269,7 @@ xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, i
   const int ntile_all = (nblk + kKT - 1) / kKT;
   const int t0 = (int)((long long)ntile_all * z / ks);
   const int nt = (int)((long long)ntile_all * (z + 1) / ks) - t0;
-  const int nconv_warps = kConvThreads / 32;
+  const int nconv_warps = CW;
 
   if (tid == 0) {
     for (int i = 0; i < kStages; i++) {
@@ -343,12 +344,15 @@ xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, i
     }
     if (!*s_abort && mmas == nt && nt > 0) mma_commit(smem_u32(done));
   } else if (warp >= kConvWarp0) {
-    // ---- converters: row r, block group g of each tile
+    // ---- converters: row r, blocks k0 .. k0 + BPT - 1 of each tile
+    constexpr int BPT = 64 / CW;   // blocks per thread: 8 (8 warps) or 4 (16 warps)
+    constexpr int NW = BPT / 2;    // half2 words per quantity
     const int ct = tid - kConvWarp0 * 32;
-    const int r = ct & (kNI - 1), g = ct >> 7;
+    const int r = ct & (kNI - 1), k0 = (ct >> 7) * BPT;
     const float s0 = scale[((size_t)f * kNI + r) * N + 2 * p];
     const float s1 = scale[((size_t)f * kNI + r) * N + 2 * p + 1];
-    const uint32_t row_off = (uint32_t)(r >> 3) * kSBO + (uint32_t)g * kLBO + (uint32_t)(r & 7) * 16;
+    const uint32_t row_off = (uint32_t)(r >> 3) * kSBO + (uint32_t)(k0 >> 3) * kLBO + (uint32_t)(r & 7) * 16 +
+                             (uint32_t)(k0 & 7) * 2;
     for (int t = 0; t < nt; t++) {
       if (*s_abort) break;
       const int st = t % kStages, o = t % kOpStages;
@@ -359,11 +363,11 @@ xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, i
       const int kv = min(kKT, nblk - (t0 + t) * kKT);
       // row (k, r) of the stage holds RP channel pairs; this CTA's is pair p % RP
       const float4 *stg = reinterpret_cast<const float4 *>(staging + st * kStageBytes) + (p % RP);
-      uint32_t re0[4], im0[4], re1[4], im1[4];
-      uint32_t lre0[4], lim0[4], lre1[4], lim1[4];
+      uint32_t re0[NW], im0[NW], re1[NW], im1[NW];
+      uint32_t lre0[NW], lim0[NW], lre1[NW], lim1[NW];
 #pragma unroll
-      for (int j = 0; j < 4; j++) {
-        const int k = g * 8 + 2 * j;
+      for (int j = 0; j < NW; j++) {
+        const int k = k0 + 2 * j;
         const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
         const float4 a = (k < kv) ? stg[(k * kNI + r) * RP] : zero;   // (c0.re, c0.im, c1.re, c1.im) at block k
         const float4 b = (k + 1 < kv) ? stg[((k + 1) * kNI + r) * RP] : zero;
@@ -387,17 +391,20 @@ xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, i
       }
       unsigned char *op = ops + o * kOpStageBytes;
       // channel e, part q at op + (q * 2 + e) * kOpChanBytes; Xi rows 0..127, Xr rows 128..255
-      *reinterpret_cast<uint4 *>(op + row_off) = make_uint4(im0[0], im0[1], im0[2], im0[3]);
-      *reinterpret_cast<uint4 *>(op + row_off + kXrOffset) = make_uint4(re0[0], re0[1], re0[2], re0[3]);
-      *reinterpret_cast<uint4 *>(op + kOpChanBytes + row_off) = make_uint4(im1[0], im1[1], im1[2], im1[3]);
-      *reinterpret_cast<uint4 *>(op + kOpChanBytes + row_off + kXrOffset) = make_uint4(re1[0], re1[1], re1[2], re1[3]);
+      auto put = [&](unsigned char *dst, const uint32_t (&w)[NW]) {
+        if constexpr (NW == 4) *reinterpret_cast<uint4 *>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
+        else *reinterpret_cast<uint2 *>(dst) = make_uint2(w[0], w[1]);
+      };
+      put(op + row_off, im0);
+      put(op + row_off + kXrOffset, re0);
+      put(op + kOpChanBytes + row_off, im1);
+      put(op + kOpChanBytes + row_off + kXrOffset, re1);
       if (HILO) {
         unsigned char *lo = op + 2 * kOpChanBytes;
-        *reinterpret_cast<uint4 *>(lo + row_off) = make_uint4(lim0[0], lim0[1], lim0[2], lim0[3]);
-        *reinterpret_cast<uint4 *>(lo + row_off + kXrOffset) = make_uint4(lre0[0], lre0[1], lre0[2], lre0[3]);
-        *reinterpret_cast<uint4 *>(lo + kOpChanBytes + row_off) = make_uint4(lim1[0], lim1[1], lim1[2], lim1[3]);
-        *reinterpret_cast<uint4 *>(lo + kOpChanBytes + row_off + kXrOffset) =
-            make_uint4(lre1[0], lre1[1], lre1[2], lre1[3]);
+        put(lo + row_off, lim0);
+        put(lo + row_off + kXrOffset, lre0);
+        put(lo + kOpChanBytes + row_off, lim1);
+        put(lo + kOpChanBytes + row_off + kXrOffset, lre1);
       }
       fence_proxy_async_smem();
       __syncwarp();
@@ -420,7 +427,8 @@ xmac_tc_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int NP, i
   __syncthreads();
   tc_fence_after();
 
-  const bool ep = warp >= kConvWarp0;   // the converter warps run the epilogue
+  // the first eight converter warps run the epilogue
+  const bool ep = warp >= kConvWarp0 && warp < kConvWarp0 + kConvThreads / 32;
   const int ct = tid - kConvWarp0 * 32;
   if (!*s_abort && !(nt == 0 && accumulate)) {   // an empty slice adds nothing
     // a warp reads tensor-memory lanes 32 (warp % 4) .. +31 (its quadrant), i.e. row a of both accumulators
@@ -607,16 +615,20 @@ cudaError_t xmac_tc_launch(const float2 *spec, int nblk, int N, int nfreqs, int 
                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (cr != CUDA_SUCCESS) return cudaErrorInvalidValue;
   const size_t sm = xmac_tc_smem_bytes(hilo);
+  // converter warps: 8 unless GX_TC_CONV_WARPS=16 (measured no faster on C3)
+  const char *ce = getenv("GX_TC_CONV_WARPS");
+  const int cw = (ce && atoi(ce) == 16) ? 16 : 8;
   dim3 grid(N / 2, nfreqs, ks);
-#define GX_TC_CASE(H, RPV)                                                                                  \
-  if (hilo == H && rp == RPV) {                                                                             \
-    cudaError_t e = smem_opt_in((const void *)xmac_tc_kernel<H, RPV>, sm);                                  \
+#define GX_TC_CASE(H, RPV, CWV)                                                                             \
+  if (hilo == H && rp == RPV && cw == CWV) {                                                                \
+    cudaError_t e = smem_opt_in((const void *)xmac_tc_kernel<H, RPV, CWV>, sm);                             \
     if (e != cudaSuccess) return e;                                                                         \
-    xmac_tc_kernel<H, RPV><<<grid, kThreads, sm, st>>>(map, nblk, N / 2, nfreqs, ks, ninputs, scale, acc,   \
-                                                       accumulate, err);                                    \
+    xmac_tc_kernel<H, RPV, CWV><<<grid, tc_threads(CWV), sm, st>>>(map, nblk, N / 2, nfreqs, ks, ninputs,   \
+                                                                    scale, acc, accumulate, err);           \
     return cudaGetLastError();                                                                              \
   }
-  GX_TC_CASE(true, 2) GX_TC_CASE(false, 2) GX_TC_CASE(true, 1) GX_TC_CASE(false, 1)
+  GX_TC_CASE(true, 1, 16) GX_TC_CASE(false, 1, 16) GX_TC_CASE(true, 1, 8) GX_TC_CASE(false, 1, 8)
+  GX_TC_CASE(true, 2, 16) GX_TC_CASE(false, 2, 16) GX_TC_CASE(true, 2, 8) GX_TC_CASE(false, 2, 8)
 #undef GX_TC_CASE
   return cudaErrorInvalidValue;
 }
