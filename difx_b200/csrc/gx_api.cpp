@@ -584,12 +584,12 @@ static gx_status setup(gx_handle *h)
     // memory is shared with other jobs: the efficient length, within the budget
     chunk = (int)std::min<size_t>({8192, efficient, std::max<size_t>(16, (size_t)d.spectra_budget_bytes / per_block)});
   } else {
-    // The tensor-core X-step moves its accumulators (128 x 128 complex per
-    // channel) through HBM once per chunk, so it gets long chunks: up to 40 GB
-    // of spectra, at most 30% of the device memory free at open.
-    size_t spec_budget = size_t(2) << 30;
-    if (h->tc) {
-      spec_budget = size_t(40) << 30;
+    // Both X-steps move their accumulators through HBM once per pass (the
+    // tensor-core form 128 x 128 complex per channel, the FP32 form its upper
+    // super-tiles), so passes are long: up to 40 GB of spectra, at most 30% of
+    // the device memory free at open.
+    size_t spec_budget = size_t(40) << 30;
+    {
       size_t fr = 0, tot = 0;
       if (h->device >= 0 && cudaSetDevice(h->device) == cudaSuccess && cudaMemGetInfo(&fr, &tot) == cudaSuccess)
         spec_budget = std::max(size_t(1) << 30, std::min(spec_budget, fr / 10 * 3));
@@ -1047,7 +1047,7 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
       CKR(h, xmac_tc_launch(h->d_spec, nb, J.nchan, d.nfreqs, J.ninputs, h->ks, h->hilo, h->d_scale, acc4,
                             b0 > 0 ? 1 : 0, h->d_err, st));
     else
-      CKR(h, xmac_fp32_launch(h->d_spec, nb, J.ninputs, J.nchan, d.nfreqs, h->ks, h->d_acc, st));
+      CKR(h, xmac_fp32_launch(h->d_spec, nb, J.ninputs, J.nchan, d.nfreqs, h->ks, h->d_acc, h->d_err, st));
     CKR(h, weights_launch(h->d_w, nb, d.nstations, h->d_pairs, npairs, h->d_wacc, st));
     if ((r = mark(1, false)) != GX_OK) return r;
     h->launches += 3;
@@ -1100,7 +1100,7 @@ static gx_status run_device(gx_handle *h, const gx_subint_desc *sub, const uint8
 static gx_status kernel_status(gx_handle *h, int k = 0)
 {
   if (h->h_err && h->h_err[k] != 0)
-    return h->fail(GX_ERR_TIMEOUT, "a tensor-core X-step wait expired (status " + std::to_string(h->h_err[k]) + ")");
+    return h->fail(GX_ERR_TIMEOUT, "an X-step wait expired (status " + std::to_string(h->h_err[k]) + ")");
   return GX_OK;
 }
 

@@ -228,7 +228,7 @@ extern "C" gx_status gx_subint_device_noalloc(const gx_job_desc *desc, const gx_
   for (int b0 = 0; b0 < J.blocks_per_send; b0 += chunk) {
     const int nb = std::min(chunk, J.blocks_per_send - b0);
     NA_CK(fstep_launch(J, d_st, plan.maxnrf, S, b0, nb, plan.nslots, d_spec, d_w, d_bp, st));
-    NA_CK(xmac_fp32_launch(d_spec, nb, J.ninputs, J.nchan, J.nfreqs, ks, d_acc, st));
+    NA_CK(xmac_fp32_launch(d_spec, nb, J.ninputs, J.nchan, J.nfreqs, ks, d_acc, nullptr, st));
     NA_CK(weights_launch(d_w, nb, nst, d_pairs, nbl, d_wacc, st));
   }
   NA_CK(finalise_launch(d_prods, (int)plan.prods.size(), d_acc, ks, acc_slice, J.nchan, d_went,

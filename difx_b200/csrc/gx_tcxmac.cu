@@ -49,6 +49,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include "gx_xstep.h"
+#include "gx_mbar.cuh"
 
 namespace gx {
 namespace {
@@ -76,65 +77,6 @@ struct TcRing {
   static_assert((2 * kNI * kPRow + 2 * kNI) * 4 + kNI * kVRow * 16 <= kStages * kStageBytes + kOpStages * kOpStageBytes,
                 "epilogue tables must fit in the staging ring and operand stages");
 };
-constexpr unsigned long long kWaitLimitNs = 2000000000ull;
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p)
-{
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ unsigned long long global_ns()
-{
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
-{
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
-{
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
-{
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// Waits for the phase of the given parity to complete; false after kWaitLimitNs.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
-{
-  if (mbar_try_wait(bar, parity)) return true;
-  const unsigned long long t0 = global_ns();
-  while (!mbar_try_wait(bar, parity))
-    if (global_ns() - t0 > kWaitLimitNs) return false;
-  return true;
-}
-
-// One tile of a 4-D tensor map (no multicast) into shared memory; coordinates innermost first.
-__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap *map, int x, int y, int zc, int w,
-                                            uint32_t bar)
-{
-  asm volatile(
-      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
-      "[%6];" ::"r"(dst),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(zc), "r"(w), "r"(bar)
-               : "memory");
-}
-
-__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
@@ -229,10 +171,6 @@ __device__ __forceinline__ void split2(float a, float b, uint32_t &hi, uint32_t 
   lo = *reinterpret_cast<const uint32_t *>(&l);
 }
 
-__device__ __forceinline__ void mbar_arrive(uint32_t bar)
-{
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
 
 // Warp roles: warp 0 lane 0 issues the tile loads, warp 1 lane 0 issues the
 // MMAs, warps 2..9 (kConvThreads threads) convert the staged FP32 tiles to FP16
@@ -567,6 +505,28 @@ finalise_tc_kernel(const TcProdEntry *__restrict__ prods, const TcRowEntry *__re
 }  // namespace
 
 
+// 4-D FP32 tensor map over a dense row-major array (innermost dimension
+// first, strides implied by the dimensions), box `box`, no swizzle, no
+// interleave; out-of-bounds elements read as zeros.
+cudaError_t tma_map_f32_4d(CUtensorMap *map, const void *base, const cuuint64_t dims[4], const cuuint32_t box[4])
+{
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess) return e;
+    if (q != cudaDriverEntryPointSuccess || !fn) return cudaErrorNotSupported;
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  const cuuint64_t strides[3] = {dims[0] * 4, dims[0] * 4 * dims[1], dims[0] * 4 * dims[1] * dims[2]};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  CUresult cr = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void *>(base), dims, strides, box, estr,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return cr == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 // Channel pairs per staged tile row: 1 (16-byte rows, four stages) unless
 // GX_TC_ROW_PAIRS=2 (32-byte rows, fewer stages; measured no faster on C3).
 static int tc_row_pairs()
@@ -594,26 +554,14 @@ cudaError_t xmac_tc_launch(const float2 *spec, int nblk, int N, int nfreqs, int 
   // {2N floats, ninputs rows, nblk blocks, nfreqs}; box {4 floats, 128 rows, kKT
   // blocks, 1}: the rows beyond the job's inputs (and blocks beyond nblk) are
   // out of bounds, so the copy fills them with zeros without reading memory
-  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-  if (!encode) {
-    void *fn = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    cudaError_t e = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
-    if (e != cudaSuccess) return e;
-    if (q != cudaDriverEntryPointSuccess || !fn) return cudaErrorNotSupported;
-    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-  }
   CUtensorMap map;
   const cuuint64_t dims[4] = {(cuuint64_t)(2 * N), (cuuint64_t)ninputs, (cuuint64_t)nblk, (cuuint64_t)nfreqs};
-  const cuuint64_t strides[3] = {(cuuint64_t)(2 * N) * 4, (cuuint64_t)(2 * N) * 4 * ninputs,
-                                 (cuuint64_t)(2 * N) * 4 * ninputs * nblk};
   const int rp = tc_row_pairs();
   const cuuint32_t box[4] = {(cuuint32_t)(4 * rp), (cuuint32_t)kNI, (cuuint32_t)kKT, 1};
-  const cuuint32_t estr[4] = {1, 1, 1, 1};
-  CUresult cr = encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float2 *>(spec), dims, strides, box, estr,
-                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (cr != CUDA_SUCCESS) return cudaErrorInvalidValue;
+  {
+    cudaError_t e = tma_map_f32_4d(&map, spec, dims, box);
+    if (e != cudaSuccess) return e;
+  }
   const size_t sm = xmac_tc_smem_bytes(hilo);
   // converter warps: 8 unless GX_TC_CONV_WARPS=16 (measured no faster on C3)
   const char *ce = getenv("GX_TC_CONV_WARPS");

@@ -16,38 +16,44 @@
 // chunk passes of a subint; finalise_kernel maps them to the Core result
 // layout (configuration.cpp:2348-2630) and sums the K-split slices.
 #include <cstdint>
+#include <cstdlib>
 #include "gx_dev.h"
 #include "gx_xstep.h"
+#include "gx_mbar.cuh"
 
 namespace gx {
 
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes)
-{
-  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+template <int T, int ST, int CT>
+__host__ __device__ constexpr int xmac_consumers() { return CT * (ST / T) * (ST / T); }
 
-template <int T, int ST, int CT, int KB, int NSTAGE>
-__global__ void __launch_bounds__(CT *(ST / T) * (ST / T))
-xmac_fp32_kernel(const float2 *__restrict__ spec, int nblk, int NI, int N, int nsuper,
-                 int ks_count, float2 *__restrict__ acc)
+// One CTA: super-tile pair blockIdx.x (upper triangle, row-major) of frequency
+// f for CT channels from c0 = blockIdx.y CT, over the blocks of K-split slice
+// ks.  One producer warp (the last) loads each stage -- KB blocks x ST rows x
+// CT channels of the I and (off the diagonal) J rows -- with one TMA tile per
+// operand into an NSTAGE ring; the consumer warps multiply from shared memory
+// and free each stage with one arrival per warp, so no CTA-wide barrier
+// separates the stages.  Every wait is bounded (kWaitLimitNs): on expiry the
+// CTA records a status in *err (when given), drains the copies it issued and
+// adds nothing.
+template <int T, int ST, int CT, int KB, int NSTAGE, int UNR = 1>
+__global__ void __launch_bounds__(xmac_consumers<T, ST, CT>() + 32, 1)
+xmac_fp32_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int N, int nsuper, int ks_count,
+                 int kper, float2 *__restrict__ acc, int *__restrict__ err)
 {
   constexpr int NT = ST / T;            // register tiles per super-tile side
-  constexpr int NTHREADS = CT * NT * NT;
+  constexpr int NC = xmac_consumers<T, ST, CT>();
+  constexpr int NCW = NC / 32;          // consumer warps
   constexpr int STAGE = KB * ST * CT;   // float2 per stage per operand
-  extern __shared__ __align__(16) float2 xsm[];
+  extern __shared__ __align__(128) float2 xsm[];
   float2 *sI = xsm;                     // [NSTAGE][KB][ST][CT]
   float2 *sJ = xsm + NSTAGE * STAGE;    // [NSTAGE][KB][ST][CT]
+  uint64_t *full = reinterpret_cast<uint64_t *>(sJ + NSTAGE * STAGE);
+  uint64_t *empty = full + NSTAGE;
+  volatile int *s_abort = reinterpret_cast<volatile int *>(empty + NSTAGE);
 
-  const int tid = threadIdx.x;
-  const int c = tid % CT;
-  const int p = tid / CT;
-  const int ti = p / NT, tj = p % NT;
-  const int c0 = blockIdx.x * CT;
-  const int stp = blockIdx.y;           // super-tile pair index (upper triangle, row-major)
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int stp = blockIdx.x;           // super-tile pair index
+  const int c0 = blockIdx.y * CT;
   const int f = blockIdx.z / ks_count;
   const int ks = blockIdx.z % ks_count;
   int SI = 0, rem = stp;
@@ -55,56 +61,79 @@ xmac_fp32_kernel(const float2 *__restrict__ spec, int nblk, int NI, int N, int n
   const int SJ = SI + rem;
   const int I0 = SI * ST, J0 = SJ * ST;
   const bool diag = (SI == SJ);
-  const float2 *sJread = diag ? sI : sJ;
 
-  const int kper = (nblk + ks_count - 1) / ks_count;
+  // slices start on stage boundaries (kper is a multiple of KB); the last
+  // stage may reach past nblk, where the copies read zeros
   const int kb0 = ks * kper, kb1 = min(nblk, kb0 + kper);
   const int nstages = (kb1 > kb0) ? (kb1 - kb0 + KB - 1) / KB : 0;
 
-  // one stage: rows [I0, I0+ST) (and [J0, J0+ST) off the diagonal) x CT channels x KB blocks,
-  // 16-byte (two-channel) pieces; missing blocks/channels are zero-filled
-  auto load_stage = [&](int st, int buf) {
-    const int k = kb0 + st * KB;
-    constexpr int PIECES = KB * ST * (CT / 2);
-    for (int e = tid; e < PIECES * (diag ? 1 : 2); e += NTHREADS) {
-      const int opnd = e / PIECES;
-      const int q = e % PIECES;
-      const int kk = q / (ST * (CT / 2));
-      const int r = (q / (CT / 2)) % ST;
-      const int cc = (q % (CT / 2)) * 2;
-      const int row = (opnd ? J0 : I0) + r;
-      const bool ok = (k + kk < kb1) && (c0 + cc < N) && (row < NI);
-      const float2 *src = ok ? spec + (((size_t)f * nblk + (k + kk)) * NI + row) * N + c0 + cc : spec;
-      float2 *dst = (opnd ? sJ : sI) + buf * STAGE + (kk * ST + r) * CT + cc;
-      cp_async16(dst, src, ok ? 16 : 0);
+  if (tid == 0) {
+    for (int i = 0; i < NSTAGE; i++) {
+      mbar_init(smem_u32(full + i), 1);
+      mbar_init(smem_u32(empty + i), NCW);
     }
-    cp_async_commit();
+    *s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto abort_with = [&](int code) {
+    *s_abort = 1;
+    if (err) atomicExch(err, code);
   };
 
+  if (warp == NCW) {
+    // ---- producer
+    if (lane == 0) {
+      const uint32_t bytes = (diag ? 1u : 2u) * (uint32_t)(STAGE * sizeof(float2));
+      int issued = 0;
+      for (int st = 0; st < nstages; st++) {
+        if (*s_abort) break;
+        const int b = st % NSTAGE;
+        if (st >= NSTAGE && !mbar_wait(smem_u32(empty + b), (uint32_t)(st / NSTAGE - 1) & 1u)) {
+          abort_with(13);
+          break;
+        }
+        const uint32_t bar = smem_u32(full + b);
+        mbar_expect_tx(bar, bytes);
+        const int k = kb0 + st * KB;
+        tma_load_4d(smem_u32(sI + b * STAGE), &spec_map, 2 * c0, I0, k, f, bar);
+        if (!diag) tma_load_4d(smem_u32(sJ + b * STAGE), &spec_map, 2 * c0, J0, k, f, bar);
+        issued = st + 1;
+      }
+      if (*s_abort) {
+        // drain: the copies this CTA issued land before it exits (bounded)
+        for (int b = 0; b < NSTAGE && b < issued; b++) {
+          const int ulast = b + ((issued - 1 - b) / NSTAGE) * NSTAGE;
+          mbar_wait(smem_u32(full + b), (uint32_t)(ulast / NSTAGE) & 1u);
+        }
+      }
+    }
+    return;
+  }
+
+  // ---- consumers: a T x T register tile of one channel
+  const int c = tid % CT;
+  const int p = tid / CT;
+  const int ti = p / NT, tj = p % NT;
+  const float2 *sJread = diag ? sI : sJ;
   float ar[T][T], ai[T][T];
 #pragma unroll
   for (int a = 0; a < T; a++)
 #pragma unroll
     for (int b = 0; b < T; b++) { ar[a][b] = 0.f; ai[a][b] = 0.f; }
-
   const bool compute = !diag || (ti <= tj);   // lower tiles of diagonal super-tiles are redundant
-
-  // NSTAGE-deep cp.async pipeline (one commit group per stage, empty groups at the tail)
-#pragma unroll
-  for (int s0 = 0; s0 < NSTAGE - 1; s0++) {
-    if (s0 < nstages) load_stage(s0, s0);
-    else cp_async_commit();
-  }
+  bool ok = true;
   for (int st = 0; st < nstages; st++) {
     const int buf = st % NSTAGE;
-    if (st + NSTAGE - 1 < nstages) load_stage(st + NSTAGE - 1, (st + NSTAGE - 1) % NSTAGE);
-    else cp_async_commit();
-    cp_async_wait<NSTAGE - 1>();
-    __syncthreads();
+    if (!mbar_wait(smem_u32(full + buf), (uint32_t)(st / NSTAGE) & 1u) || *s_abort) {
+      abort_with(14);
+      ok = false;
+      break;
+    }
     if (compute) {
       const float2 *bi_ = sI + buf * STAGE;
       const float2 *bj_ = sJread + buf * STAGE;
-#pragma unroll 2
+#pragma unroll UNR
       for (int kk = 0; kk < KB; kk++) {
         float2 xi[T], xj[T];
 #pragma unroll
@@ -124,11 +153,12 @@ xmac_fp32_kernel(const float2 *__restrict__ spec, int nblk, int NI, int N, int n
           }
       }
     }
-    __syncthreads();
+    __syncwarp();
+    if (lane == 0) mbar_arrive(smem_u32(empty + buf));   // the stage may be reloaded
   }
-  if (!compute || c0 + c >= N) return;
+  if (!ok || !compute || c0 + c >= N) return;
   const int nfreqs = gridDim.z / ks_count;
-  const size_t base = (((size_t)ks * nfreqs + f) * gridDim.y + stp) * (size_t)ST * ST;
+  const size_t base = (((size_t)ks * nfreqs + f) * gridDim.x + stp) * (size_t)ST * ST;
 #pragma unroll
   for (int a = 0; a < T; a++)
 #pragma unroll
@@ -202,18 +232,28 @@ __global__ void finalise_weights_kernel(const WeightEntry *__restrict__ we, int 
 
 // ------------------------------------------------------------------ launchers
 
-template <int T, int ST, int CT, int KB, int NSTAGE>
-static cudaError_t launch_t(const float2 *spec, int nblk, int NI, int N, int nfreqs, int ks, float2 *acc,
+template <int T, int ST, int CT, int KB, int NSTAGE, int UNR = 1>
+static cudaError_t launch_t(const float2 *spec, int nblk, int NI, int N, int nfreqs, int ks, float2 *acc, int *err,
                             cudaStream_t st)
 {
   const int nsuper = (NI + ST - 1) / ST;
   const int npairs = nsuper * (nsuper + 1) / 2;
-  const size_t sm = sizeof(float2) * 2 * NSTAGE * KB * ST * CT;
-  cudaError_t e = smem_opt_in((const void *)xmac_fp32_kernel<T, ST, CT, KB, NSTAGE>, sm);
+  const size_t sm = sizeof(float2) * 2 * NSTAGE * KB * ST * CT + 2 * NSTAGE * sizeof(uint64_t) + 16;
+  // spec[freq][block][row][channel] float2 as a 4-D FP32 tensor: {2N floats,
+  // NI rows, nblk blocks, nfreqs}; one box = KB blocks x ST rows x CT channels
+  CUtensorMap map;
+  const cuuint64_t dims[4] = {(cuuint64_t)(2 * N), (cuuint64_t)NI, (cuuint64_t)nblk, (cuuint64_t)nfreqs};
+  const cuuint32_t box[4] = {(cuuint32_t)(2 * CT), (cuuint32_t)ST, (cuuint32_t)KB, 1};
+  cudaError_t e = tma_map_f32_4d(&map, spec, dims, box);
   if (e != cudaSuccess) return e;
-  dim3 grid((N + CT - 1) / CT, npairs, nfreqs * ks);
-  xmac_fp32_kernel<T, ST, CT, KB, NSTAGE>
-      <<<grid, CT *(ST / T) * (ST / T), sm, st>>>(spec, nblk, NI, N, nsuper, ks, acc);
+  e = smem_opt_in((const void *)xmac_fp32_kernel<T, ST, CT, KB, NSTAGE, UNR>, sm);
+  if (e != cudaSuccess) return e;
+  // slices of whole stages
+  const int kper = ((nblk + ks - 1) / ks + KB - 1) / KB * KB;
+  // super-tile pairs fastest: the pairs that share a channel group's spectra run together
+  dim3 grid(npairs, (N + CT - 1) / CT, nfreqs * ks);
+  xmac_fp32_kernel<T, ST, CT, KB, NSTAGE, UNR>
+      <<<grid, xmac_consumers<T, ST, CT>() + 32, sm, st>>>(map, nblk, N, nsuper, ks, kper, acc, err);
   return cudaGetLastError();
 }
 
@@ -228,13 +268,15 @@ XmacShape xmac_shape(int NI)
   return s;
 }
 
-cudaError_t xmac_fp32_launch(const float2 *spec, int nblk, int NI, int N, int nfreqs, int ks, float2 *acc,
+cudaError_t xmac_fp32_launch(const float2 *spec, int nblk, int NI, int N, int nfreqs, int ks, float2 *acc, int *err,
                              cudaStream_t st)
 {
   XmacShape s = xmac_shape(NI);
-  if (s.ST == 8) return launch_t<4, 8, 32, 8, 3>(spec, nblk, NI, N, nfreqs, ks, acc, st);
-  if (s.ST == 16) return launch_t<4, 16, 16, 8, 3>(spec, nblk, NI, N, nfreqs, ks, acc, st);
-  return launch_t<8, 32, 16, 8, 3>(spec, nblk, NI, N, nfreqs, ks, acc, st);
+  if (s.ST == 8) return launch_t<4, 8, 32, 8, 3>(spec, nblk, NI, N, nfreqs, ks, acc, err, st);
+  if (s.ST == 16) return launch_t<4, 16, 16, 8, 3>(spec, nblk, NI, N, nfreqs, ks, acc, err, st);
+  // 8 x 8 register tiles of 32-row super-tiles, 16 channels per CTA; the
+  // block loop is not unrolled (unrolled by 2 or 4 it measured 3-9% slower)
+  return launch_t<8, 32, 16, 8, 3>(spec, nblk, NI, N, nfreqs, ks, acc, err, st);
 }
 
 cudaError_t weights_launch(const float *w, int nblk, int nstations, const int2 *pairs, int npairs, float *wacc,

@@ -2,6 +2,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include "gx_dev.h"
 
@@ -36,10 +37,15 @@ struct XmacShape {
 
 XmacShape xmac_shape(int NI);
 
+// 4-D FP32 tensor map over a dense array (dims innermost first), box `box`.
+cudaError_t tma_map_f32_4d(CUtensorMap *map, const void *base, const cuuint64_t dims[4], const cuuint32_t box[4]);
+
 size_t fstep_smem_bytes(const DevJob &J, int nrf, int nslots);cudaError_t fstep_launch(const DevJob &J, const DevStation *stations, int maxnrf, const SubintArrays &S,
                          int blk0, int nblk, int nslots, float2 *spec, float *weights, BlockParam *bp,
                          cudaStream_t st);
-cudaError_t xmac_fp32_launch(const float2 *spec, int nblk, int NI, int N, int nfreqs, int ks, float2 *acc,
+// FP32 X-step over one pass of blocks; *err (may be null) receives a nonzero
+// status if a wait of the kernel expired.
+cudaError_t xmac_fp32_launch(const float2 *spec, int nblk, int NI, int N, int nfreqs, int ks, float2 *acc, int *err,
                              cudaStream_t st);
 cudaError_t weights_launch(const float *w, int nblk, int nstations, const int2 *pairs, int npairs, float *wacc,
                            cudaStream_t st);
