@@ -87,6 +87,15 @@ def workload_spec(name="c3", subint_ns=None) -> JobSpec:
     raise ValueError(name)
 
 
+def with_nchan(spec: JobSpec, nchan: int) -> JobSpec:
+    """The workload with nchan channels per subband and a subint of the same
+    number of FFT blocks (the same per-block work of the X-step, less memory)."""
+    blocks = spec.blocks_per_send
+    sub = [Subband(s.freq_mhz, s.bw_mhz, s.sideband, nchan) for s in spec.subbands]
+    s2 = JobSpec(**{**spec.__dict__, "subbands": sub})
+    return JobSpec(**{**s2.__dict__, "subint_ns": int(round(blocks * s2.fftchannels / s2.samples_per_second * 1e9))})
+
+
 def samples_per_subint(spec: JobSpec) -> float:
     return spec.nstations * spec.nbands * spec.samples_per_second * spec.subint_ns * 1e-9
 
@@ -256,6 +265,8 @@ def run_reference_arm(args):
     base["value"] = v
     base["peak_rss_gb"] = round(peak_rss_gb(), 2)
     spec = workload_spec(args.config, subint_ns=int(round(args.subint_ms * 1e6)))
+    if args.nchan:
+        spec = with_nchan(spec, args.nchan)
     if args.pcal_mhz:
         spec = JobSpec(**{**spec.__dict__, "pcal_interval_mhz": args.pcal_mhz})
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
@@ -329,11 +340,28 @@ def time_device(corr, sd_dev, dres, stream, steps, warmup, local, dist=None, clo
     return dev_ms, stage, launches, (clk.summary() if clk else None)
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) that ncu measured for
-# one fstep_r16_kernel launch on the C3 workload: 250 blocks x 64 stations
-# (a 16 ms subint captured alone).  Traffic grows with the blocks a launch
-# processes, so a step's traffic is this per-block figure times its blocks.
-R16_C3_DRAM_BYTES_PER_BLOCK = 5.321e9 / 250
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) that ncu measured
+# for one launch of the F-step kernel, per FFT block of the launch, by
+# (workload, kernel): C3 captured at a 16 ms subint (250 blocks x 64
+# stations).  Traffic grows with the blocks a launch processes, so a step's
+# traffic is this figure times its blocks.
+F_DRAM_BYTES_PER_BLOCK = {("bench_c3", "fstep_sb_kernel"): (1.047196e9 + 4.142358e9) / 250}
+
+
+def f_kernel_name(spec: JobSpec) -> str:
+    """The F-step kernel the library runs for this job (the station-block
+    kernel's domain: 512- to 8192-point transforms, whole-byte time samples of
+    1, 2, 4 or 8 bytes (real) or 4, 8 or 16 bytes (complex), payloads of whole
+    16-byte pieces, linear fringe rotation, plain VDIF)."""
+    F = spec.fftchannels
+    bpts_bits = spec.bits_per_timesample
+    bpts = bpts_bits // 8
+    ok = (512 <= F <= 8192 and bpts_bits % 8 == 0 and
+          (bpts in (4, 8, 16) if spec.is_complex else bpts in (1, 2, 4, 8)) and
+          spec.nbits * (2 if spec.is_complex else 1) in (1, 2, 4, 8, 16) and (spec.payload_bytes % 16 == 0))
+    if ok:
+        return "fstep_sb_kernel"
+    return "fstep_r16_kernel" if F >= 512 else "fstep_warp_kernel"
 
 
 def roofline(spec: JobSpec, xstep: str, stage, peaks):
@@ -345,11 +373,11 @@ def roofline(spec: JobSpec, xstep: str, stage, peaks):
     spec_bytes = nblk * spec.nstations * spec.nbands * spec.nchan * 8
     stages = {"F": f_ms, "X": x_ms, "finalise": fin_ms}
     if f_ms >= x_ms:
-        k = "fstep_r16_kernel" if spec.fftchannels >= 512 else "fstep_warp_kernel"
+        k = f_kernel_name(spec)
         a = (in_bytes + spec_bytes) / (f_ms * 1e-3) / 1e9
         traffic, tsrc = None, None
-        if spec.name == "bench_c3" and k == "fstep_r16_kernel":
-            traffic = R16_C3_DRAM_BYTES_PER_BLOCK * nblk
+        if (spec.name, k) in F_DRAM_BYTES_PER_BLOCK:
+            traffic = F_DRAM_BYTES_PER_BLOCK[(spec.name, k)] * nblk
             tsrc = "ncu DRAM bytes of one 250-block launch (16 ms subint), scaled to the step's blocks"
         return {"kernel": k, "bound": "hbm", "achieved": a, "peak": hbm_peak, "unit": "GB/s", "frac": a / hbm_peak,
                 "traffic": traffic, "traffic_source": tsrc, "peak_source": src,
@@ -703,6 +731,8 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the other X-step forms")
     ap.add_argument("--pcal-mhz", type=int, default=0,
                     help="PHASE CAL INT (MHZ) of every station (0: none); timing with phase-cal extraction")
+    ap.add_argument("--nchan", type=int, default=0,
+                    help="channels per subband (0: the workload's); smaller values give small profiling cases")
     ap.add_argument("--subint-ms", type=float, default=None,
                     help="subint length; smaller values give small profiling cases")
     args = ap.parse_args()
@@ -733,6 +763,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
 
     spec = workload_spec(args.config, subint_ns=int(round(args.subint_ms * 1e6)))
+    if args.nchan:
+        spec = with_nchan(spec, args.nchan)
     if args.pcal_mhz:
         spec = JobSpec(**{**spec.__dict__, "pcal_interval_mhz": args.pcal_mhz})
     d = tempfile.mkdtemp(prefix=f"gxbench{rank}_")
