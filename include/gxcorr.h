@@ -133,8 +133,8 @@ typedef struct gx_job_desc {
   int block_chunk;         /* FFT blocks per device pass, 0 = automatic */
   int64_t spectra_budget_bytes; /* with block_chunk 0: > 0 caps the spectra buffer and makes passes only as
                                    long as keeps accumulator traffic under a quarter of the spectra
-                                   traffic (for many resident jobs); 0 = as long as 2 GB (FP32) or up to
-                                   40 GB (tensor cores) allow */
+                                   traffic (for many resident jobs); 0 = passes of up to 40 GB of
+                                   spectra, at most 30% of the device memory free at open */
 } gx_job_desc;
 
 /* One subint: the contents of one Core processslot (core.h:76-98). */

@@ -33,6 +33,7 @@ def build(reference: bool = True) -> None:
     if reference and os.path.isdir(REFERENCE_SRC):
         subprocess.run(["make", "-s", "-C", HERE, "ref", "-j8", f"REF={REFERENCE_SRC}"], check=True)
         subprocess.run(["make", "-s", "-C", HERE, "vmux", f"REF={REFERENCE_SRC}"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "shim", "-j8", f"REF={REFERENCE_SRC}"], check=True)
 
 
 def reference_available() -> bool:
@@ -179,6 +180,15 @@ class Reference:
                                 sp.ctypes.data_as(C.c_void_p), C.byref(w))
         return (sp[0::2] + 1j * sp[1::2]).reshape(nbands, nchan), w.value
 
+    def mode_blocks(self, si, station: int, nblocks: int, nbands: int, nchan: int):
+        """Mode::process of one datastream over blocks 0..nblocks-1: (spectra
+        [nblocks][nbands][nchan], data weights [nblocks], autocorrelations
+        [2][nbands][nchan], weights [2][nbands])."""
+        return _mode_blocks(self.lib.ref_mode_blocks, self.h, nblocks, nbands, nchan,
+                            (si.data[station].ctypes.data_as(C.c_void_p), len(si.data[station]),
+                             si.control[station].ctypes.data_as(C.c_void_p), len(si.control[station]),
+                             si.scan, si.sec, si.ns), station)
+
     def unpack(self, station: int, data: np.ndarray, offset: int, nbands: int, per: int):
         out = np.zeros(nbands * per * 2, np.float32)
         w = C.c_float(0)
@@ -186,6 +196,68 @@ class Reference:
         n = self.lib.ref_unpack(self.h, station, data.ctypes.data_as(C.c_void_p), len(data), offset,
                                 out.ctypes.data_as(C.c_void_p), C.byref(w), C.byref(us))
         return out, w.value, us.value, n
+
+
+def _mode_blocks(fn, h, nblocks, nbands, nchan, mid_args, station):
+    sp = np.zeros(2 * nblocks * nbands * nchan, np.float32)
+    dw = np.zeros(nblocks, np.float32)
+    au = np.zeros(2 * 2 * nbands * nchan, np.float32)
+    wt = np.zeros(2 * nbands, np.float32)
+    tail = (nblocks, sp.ctypes.data_as(C.c_void_p), dw.ctypes.data_as(C.c_void_p), au.ctypes.data_as(C.c_void_p),
+            wt.ctypes.data_as(C.c_void_p))
+    st = fn(h, station, *mid_args, *tail)
+    if st != 0:
+        raise RuntimeError(f"mode_blocks failed ({st})")
+    c = lambda a: a[0::2] + 1j * a[1::2]
+    return (c(sp).reshape(nblocks, nbands, nchan), dw, c(au).reshape(2, nbands, nchan), wt.reshape(2, nbands))
+
+
+SHIM_LIB = os.path.join(REF_DIR, "libgxshim.so")
+
+
+def shim_available() -> bool:
+    return os.path.exists(SHIM_LIB)
+
+
+class Binding:
+    """The DiFX-side binding (difx_b200/mpifxcorr: GpuCore, GpuMode) over the
+    reference's Configuration, driven through shim_harness.cpp."""
+
+    def __init__(self, inputfile: str, device: int = 0, xstep: int = 0):
+        if not shim_available():
+            raise RuntimeError("binding harness not built (oracle/_ref/libgxshim.so)")
+        self.lib = C.CDLL(SHIM_LIB)
+        self.lib.shim_open.restype = C.c_void_p
+        self.lib.shim_last_error.restype = C.c_char_p
+        h = self.lib.shim_open(inputfile.encode(), device, xstep)
+        if not h:
+            raise RuntimeError(f"binding could not open {inputfile}")
+        self.h = C.c_void_p(h)
+
+    def process(self, si, result_length: int) -> np.ndarray:
+        n = len(si.data)
+        datap = (C.c_void_p * n)(*[d.ctypes.data for d in si.data])
+        lens = (C.c_int * n)(*[len(d) for d in si.data])
+        ctrl = (C.c_void_p * n)(*[c.ctypes.data for c in si.control])
+        res = np.zeros(2 * result_length, np.float32)
+        st = self.lib.shim_process(self.h, si.scan, si.sec, si.ns, datap, lens, ctrl, len(si.control[0]),
+                                   res.ctypes.data_as(C.c_void_p))
+        if st != 0:
+            raise RuntimeError(f"GpuCore slot failed ({st}): {self.lib.shim_last_error(self.h).decode()}")
+        return res[0::2] + 1j * res[1::2]
+
+    def mode_blocks(self, station: int, nblocks: int, nbands: int, nchan: int):
+        """GpuMode over blocks 0..nblocks-1 of the slot process() last correlated
+        (same outputs as Reference.mode_blocks)."""
+        return _mode_blocks(self.lib.shim_mode_blocks, self.h, nblocks, nbands, nchan, (), station)
+
+    def close(self) -> None:
+        if getattr(self, "h", None) is not None:
+            self.lib.shim_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
 
 
 VMUX_LIB = os.path.join(HERE, "_ref", "libvdifmuxref.so")

@@ -205,6 +205,37 @@ int ref_mode_block(void *h, int station, const unsigned char *data, int datalen,
   return 0;
 }
 
+// Mode::process of datastream `station` over FFT blocks 0 .. nblocks-1 of
+// one subint (data, control words, slot start): per block its spectra
+// (nbands x nchan cf32) and data weight, then the autocorrelations
+// [2][nbands][nchan] cf32 and weights [2][nbands] accumulated over the blocks.
+int ref_mode_blocks(void *h, int station, const unsigned char *data, int datalen, const int *control, int controllen,
+                    int scan, int sec, int ns, int nblocks, float *spectra, float *dataweights, float *autos,
+                    float *weights)
+{
+  RefJob *j = (RefJob *)h;
+  Mode *m = j->modes[0][station];
+  std::vector<s32> flags(controllen > 3 ? controllen - 3 : 1, 0);
+  for (int i = 3; i < controllen; i++) flags[i - 3] = control[i];
+  m->zeroAutocorrelations();
+  m->setValidFlags(flags.data());
+  m->setData((u8 *)data, datalen, control[0], control[1], control[2]);
+  m->setOffsets(scan, sec, ns);
+  const int nb = m->numrecordedbands, nc = m->recordedbandchannels;
+  for (int b = 0; b < nblocks; b++) {
+    m->process(b, 0);
+    for (int k = 0; k < nb; k++)
+      memcpy(spectra + 2 * ((size_t)b * nb + k) * nc, m->getFreqs(k, 0), sizeof(cf32) * nc);
+    dataweights[b] = m->getDataWeight(0, 0);
+  }
+  for (int x = 0; x < 2; x++)
+    for (int k = 0; k < nb; k++) {
+      memcpy(autos + 2 * ((size_t)x * nb + k) * nc, m->getAutocorrelation(x == 1, k), sizeof(cf32) * nc);
+      weights[x * nb + k] = m->getWeight(x == 1, k);
+    }
+  return 0;
+}
+
 // Mk5Mode::unpack on its own: unpacked samples (nbands x unpacksamples f32,
 // or cf32 for complex data) and the returned weight.
 int ref_unpack(void *h, int station, const unsigned char *data, int datalen, int sampleoffset,

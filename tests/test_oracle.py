@@ -221,3 +221,13 @@ def test_oracle_post_f_rotation_vs_reference(case, oracle_lib):
     rl, bl, bw, ac, acw = oracle_lib.layout(prep.jd)
     offs = jobs.record_offsets(prep.jd, bl, ac, spec)
     assert jobs.record_metric(o, r, offs, spec.nchan) < 1e-6
+
+
+@pytest.mark.skipif(not pyoracle.shim_available(), reason="binding harness not built")
+def test_binding_library_builds_a_gpucore_from_the_reference_configuration():
+    """The DiFX-side binding (GpuCore over the reference's Configuration and
+    Core) loads and opens a job on the CPU; its handle opens on first use."""
+    spec = jobs.spec_c1(name="bind_cpu", seed=47)
+    prep = jobs.prepare(spec, [100_000_000])
+    b = pyoracle.Binding(prep.paths["input"])
+    b.close()
