@@ -668,49 +668,68 @@ def run_c5(args):
         srv.stats(reset=True)
         samples = [samples_per_subint(s) for s, *_ in staged]
         mean_alone_s = float(np.mean(alone)) / 1e3
-        rate = args.c5_rate if args.c5_rate > 0 else 0.7 / mean_alone_s
-        n_req = max(20, int(rate * args.c5_seconds))
-        gaps = rng.exponential(1.0 / rate, n_req)
-        picks = rng.integers(0, len(staged), n_req)
-        tickets = []
-        t0 = time.perf_counter()
-        tnext = t0
-        for g, j in zip(gaps, picks):
-            tnext += g
-            dt = tnext - time.perf_counter()
-            if dt > 0:
-                time.sleep(dt)
-            tickets.append((int(j), srv.submit(ids[j], sds[j], res[j].data_ptr(), request_bytes=0)))
-        lat = []
-        for j, t in tickets:
-            lat.append((j, srv.wait(t)))
-        wall = time.perf_counter() - t0
-        st = srv.stats()
+        subint_ms = [s.subint_ns / 1e6 for s, *_ in staged]
+
+        def run_load(rate, seconds):
+            """Poisson arrivals at `rate` requests/s for `seconds`: throughput and
+            latency, also relative to each request's subint duration."""
+            n_req = max(20, int(rate * seconds))
+            gaps = rng.exponential(1.0 / rate, n_req)
+            picks = rng.integers(0, len(staged), n_req)
+            srv.stats(reset=True)
+            tickets = []
+            t0 = time.perf_counter()
+            tnext = t0
+            for g, j in zip(gaps, picks):
+                tnext += g
+                dt = tnext - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                tickets.append((int(j), srv.submit(ids[j], sds[j], res[j].data_ptr(), request_bytes=0)))
+            lat = [(j, srv.wait(t)) for j, t in tickets]
+            wall = time.perf_counter() - t0
+            st = srv.stats()
+            rel = np.array([ms / subint_ms[j] for j, ms in lat])
+            return {"offered_load": rate * mean_alone_s, "offered_rate_req_s": rate, "requests": len(lat),
+                    "sustained_gsamp_s": sum(samples[j] for j, _ in lat) / wall / 1e9,
+                    "latency_ms": {"p50": st.p50_ms, "p95": st.p95_ms, "p99": st.p99_ms, "mean": st.mean_ms,
+                                   "max": st.max_ms},
+                    "latency_over_subint": {"p50": float(np.percentile(rel, 50)),
+                                            "p95": float(np.percentile(rel, 95)),
+                                            "p99": float(np.percentile(rel, 99))},
+                    "fraction_within_subint": float(np.mean(rel <= 1.0))}
+
+        if args.c5_rate > 0:
+            loads = [run_load(args.c5_rate, args.c5_seconds)]
+        else:
+            # offered load = arrival rate x mean one-at-a-time service time
+            loads = [run_load(f / mean_alone_s, args.c5_seconds) for f in (0.2, 0.35, 0.5, 0.7)]
         srv.close()
         for c in corrs:
             c.close()
-        done_samples = sum(samples[j] for j, _ in lat)
-        within = sum(1 for j, ms in lat if ms <= staged[j][0].subint_ns / 1e6)
-        out[form] = {"sustained_gsamp_s": done_samples / wall / 1e9, "requests": len(lat),
-                     "offered_rate_req_s": rate, "latency_ms": {"p50": st.p50_ms, "p95": st.p95_ms, "p99": st.p99_ms,
-                                                                "mean": st.mean_ms, "max": st.max_ms},
-                     "fraction_within_subint": within / len(lat), "alone_ms_mean": float(np.mean(alone)),
-                     "offered_load": rate * mean_alone_s}
+        ok = [x for x in loads if x["latency_over_subint"]["p99"] < 1.0]
+        out[form] = {"alone_ms_mean": float(np.mean(alone)), "loads": loads,
+                     "max_load_p99_within_subint": max((x["offered_load"] for x in ok), default=None),
+                     "at_max_load": max(ok, key=lambda x: x["offered_load"]) if ok else None}
     spec_rate = 50.0
-    load50 = spec_rate * float(np.mean([out["fp32"]["alone_ms_mean"] / 1e3]))
-    line = {"metric": "C5 serving: sustained Gsamp/s and subint latency", "value": out[args.xstep]["sustained_gsamp_s"],
-            "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "dtype": args.xstep,
+    load50 = spec_rate * out["fp32"]["alone_ms_mean"] / 1e3
+    head = out[args.xstep]["at_max_load"] or out[args.xstep]["loads"][0]
+    line = {"metric": "C5 serving: sustained Gsamp/s at the highest offered load with p99 latency < subint duration",
+            "value": head["sustained_gsamp_s"], "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+            "dtype": args.xstep,
             "data": "synthetic (seeded 2-bit VDIF, one stream per job shared by its stations), inputs device-resident",
             "config": {"workload": "C5: 12 real-time jobs, 4-48 stations, 2-bit real VDIF at 1-4 Gbps/station, "
-                                   "256-2048 channels, 0.2-1 s subints; Poisson arrivals",
+                                   "256-2048 channels, 0.2-1 s subints; Poisson arrivals; earliest-deadline-first "
+                                   "admission (deadline = subint duration)",
                        "jobs": [{"stations": s.nstations, "bands": s.nbands, "bw_mhz": s.bw_mhz, "nchan": s.nchan,
                                  "subint_ms": s.subint_ns / 1e6} for s, *_ in staged],
-                       "slots": args.c5_slots, "seconds": args.c5_seconds,
-                       "arrival_rate_note": (f"arrival rate set to 70% of the measured one-at-a-time capacity; the "
+                       "slots": args.c5_slots, "seconds_per_load": args.c5_seconds,
+                       "arrival_rate_note": (f"loads swept as fractions of the measured one-at-a-time capacity; the "
                                              f"specified 50 requests/s at these job sizes would offer "
                                              f"{load50:.1f}x the FP32 form's serial capacity")},
             "forms": out,
-            "tc_vs_fp32": out[args.xstep]["sustained_gsamp_s"] / out["fp32"]["sustained_gsamp_s"]}
+            "tc_vs_fp32_at_max_load": ((out[args.xstep]["at_max_load"] or {}).get("sustained_gsamp_s", 0) /
+                                       max(1e-12, (out["fp32"]["at_max_load"] or {}).get("sustained_gsamp_s", 1e-12)))}
     print(json.dumps(line))
     return 0
 
@@ -724,7 +743,7 @@ def main():
     ap.add_argument("--config", default="c3", choices=["c3", "c3_2bit", "c2", "c1", "c4", "c5", "mux"])
     ap.add_argument("--c4-steps", type=int, default=1, help="timed batch steps per mode (C4)")
     ap.add_argument("--c5-slots", type=int, default=4)
-    ap.add_argument("--c5-seconds", type=float, default=20.0)
+    ap.add_argument("--c5-seconds", type=float, default=8.0, help="seconds of arrivals per offered load")
     ap.add_argument("--c5-rate", type=float, default=0.0, help="requests per second (0: 70%% of capacity)")
     ap.add_argument("--xstep", default=None, choices=sorted(XSTEPS))
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -4,7 +4,11 @@
 // accumulators stay on the device between requests) attached to the server;
 // the device memory they hold counts against the server's HBM budget.
 // Requests -- one subint of one job -- are queued as they arrive and admitted
-// in arrival order by `slots` worker threads as soon as (a) a slot is free,
+// earliest deadline first (a request's deadline is its submission time plus
+// its job's deadline, by default the job's subint duration: a real-time
+// subint must be correlated before the next one has been recorded; requests
+// without a deadline follow in arrival order) by `slots` worker threads as
+// soon as (a) a slot is free,
 // (b) no other request of the same job is on the GPU (a job's device buffers
 // serve one subint at a time), and (c) the memory the request adds keeps the
 // total within the budget (a request is always admitted when nothing else
@@ -35,6 +39,7 @@ struct Request {
   float *results;
   long long bytes;
   Clock::time_point t_submit;
+  Clock::time_point deadline;   // time_point::max(): none
   gx_status status = GX_OK;
   double latency_ms = 0;
   bool done = false;
@@ -43,6 +48,7 @@ struct Request {
 struct Job {
   gx_handle *h;
   long long resident;
+  double deadline_ms;   // relative deadline of its requests; <= 0: none
   bool busy = false;
 };
 
@@ -87,16 +93,18 @@ struct gx_server {
   std::vector<std::thread> workers;
   bool stopping = false;
 
-  // first queued request that can start now (arrival order among the admissible)
+  // the admissible queued request with the earliest deadline (arrival order
+  // among equal deadlines and among requests without one)
   std::deque<Request *>::iterator pick()
   {
+    auto best = queue.end();
     for (auto it = queue.begin(); it != queue.end(); ++it) {
       const Request *r = *it;
       if (jobs[r->job].busy) continue;
       if (inflight > 0 && resident_total + inflight_bytes + r->bytes > budget) continue;
-      return it;
+      if (best == queue.end() || r->deadline < (*best)->deadline) best = it;
     }
-    return queue.end();
+    return best;
   }
 
   void worker()
@@ -173,9 +181,19 @@ gx_status gx_server_attach(gx_server *s, gx_handle *h, long long resident_bytes,
   const long long res = resident_bytes >= 0 ? resident_bytes : h->dev_bytes;
   std::lock_guard<std::mutex> lk(s->mu);
   if (s->resident_total + res > s->budget) return GX_ERR_NOMEM;
-  s->jobs.push_back(Job{h, res});
+  // a real-time job's subint must be done within the subint's duration
+  s->jobs.push_back(Job{h, res, h ? h->jd.subint_ns / 1e6 : 0.0});
   s->resident_total += res;
   *job = (int)s->jobs.size() - 1;
+  return GX_OK;
+}
+
+gx_status gx_server_set_deadline(gx_server *s, int job, double deadline_ms)
+{
+  if (!s) return GX_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (job < 0 || job >= (int)s->jobs.size()) return GX_ERR_ARG;
+  s->jobs[job].deadline_ms = deadline_ms;
   return GX_OK;
 }
 
@@ -201,6 +219,10 @@ gx_status gx_server_submit(gx_server *s, int job, const gx_subint_desc *sub, flo
   r->results = results;
   r->bytes = bytes;
   r->t_submit = Clock::now();
+  const double dl = s->jobs[job].deadline_ms;
+  r->deadline = dl > 0 ? r->t_submit + std::chrono::duration_cast<Clock::duration>(
+                                           std::chrono::duration<double, std::milli>(dl))
+                       : Clock::time_point::max();
   s->queue.push_back(r);
   s->reqs[r->ticket] = r;
   *ticket = r->ticket;

@@ -55,7 +55,7 @@ EXPORTED_SYMBOLS = ("gx_open", "gx_open_input", "gx_close", "gx_last_error", "gx
                     "gx_subint_device", "gx_synchronize", "gx_spectra", "gx_stage_times", "gx_launch_count",
                     "gx_subint_device_noalloc", "gx_set_tc_scales", "gx_vis_open", "gx_vis_add", "gx_vis_write",
                     "gx_vis_close", "gx_uvw", "gx_server_open", "gx_server_set_executor", "gx_server_attach",
-                    "gx_server_submit", "gx_server_wait", "gx_server_stats", "gx_server_close", "gx_device_bytes",
+                    "gx_server_submit", "gx_server_set_deadline", "gx_server_wait", "gx_server_stats", "gx_server_close", "gx_device_bytes",
                     "gx_server_last_error", "gx_batch_open", "gx_batch_run", "gx_batch_synchronize",
                     "gx_batch_info", "gx_batch_last_error", "gx_batch_close", "gx_vis_buffer",
                     "gx_vis_set_subints", "gx_vis_clear", "gx_subint_async", "gx_subint_wait", "gx_vdifmux_open",
@@ -303,6 +303,10 @@ class Server:
         self._check(lib().gx_server_attach(self.s, corr.h if corr else None, C.c_longlong(int(resident_bytes)),
                                            C.byref(job)))
         return job.value
+
+    def set_deadline(self, job: int, deadline_ms: float) -> None:
+        """Relative deadline of the job's requests (default: its subint duration; <= 0: none)."""
+        self._check(lib().gx_server_set_deadline(self.s, job, C.c_double(deadline_ms)))
 
     def submit(self, job: int, sd: capi.SubintDesc, results_ptr: int = 0, request_bytes: int = -1,
                keep=None) -> int:

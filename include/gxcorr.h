@@ -287,7 +287,9 @@ gx_status gx_uvw(gx_handle *h, int scan, double offset, int ds1, int ds2, double
 /* Opened handles are attached as jobs; their device memory (delay model,
    twiddles, tables, accumulators, input buffers) stays resident and counts
    against the server's HBM budget.  Submitted requests -- one subint of one
-   job -- are admitted in arrival order by `slots` worker threads as soon as a
+   job -- are admitted earliest deadline first (submission time plus the job's
+   deadline, by default the job's subint duration; requests without a deadline
+   in arrival order) by `slots` worker threads as soon as a
    slot is free, no other request of the same job is on the GPU, and the
    memory the request adds keeps the total within the budget (a request is
    always admitted when nothing else is in flight).  Requests of different jobs
@@ -315,6 +317,9 @@ gx_status gx_server_set_executor(gx_server *s, gx_server_executor fn, void *ctx)
 /* resident_bytes < 0: the handle's own device memory (gx_device_bytes).
    GX_ERR_NOMEM when the resident total would exceed the budget. */
 gx_status gx_server_attach(gx_server *s, gx_handle *h, long long resident_bytes, int *job);
+/* Relative deadline of the job's requests in ms (default: the subint duration
+   of the attached handle; <= 0: none, arrival order). */
+gx_status gx_server_set_deadline(gx_server *s, int job, double deadline_ms);
 /* request_bytes < 0: the growth of the job's input buffers a host-buffer
    request needs (0 with device inputs).  GX_ERR_NOMEM if it can never fit. */
 gx_status gx_server_submit(gx_server *s, int job, const gx_subint_desc *sub, float *results, long long request_bytes,

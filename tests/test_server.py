@@ -1,5 +1,6 @@
 """The request loop (gx_server_*) on the CPU, with an executor that only
-sleeps: admission in arrival order, one request per job on the GPU at a
+sleeps: admission earliest deadline first (arrival order without deadlines),
+one request per job on the GPU at a
 time, the HBM budget (resident jobs + what requests in flight add), the slot
 count, rejection of what can never fit, and the latency statistics."""
 import threading
@@ -104,3 +105,26 @@ def test_what_never_fits_is_refused():
     t = srv.submit(j, _sd(1), request_bytes=100)
     srv.wait(t)
     srv.close()
+
+
+def test_earliest_deadline_first():
+    """With one slot busy, queued requests start in order of their deadlines
+    (submission + the job's relative deadline), not of their arrival; jobs
+    without a deadline come after those with one, in arrival order."""
+    srv = gxcorr.Server(slots=1, hbm_budget_bytes=1 << 20)
+    rec = Recorder(0.03)
+    srv.set_executor(rec)
+    slow, urgent, loose, none = (srv.attach(None, 0) for _ in range(4))
+    srv.set_deadline(slow, 1000.0)
+    srv.set_deadline(urgent, 50.0)
+    srv.set_deadline(loose, 500.0)
+    t = [srv.submit(slow, _sd(0), results_ptr=1, request_bytes=0)]   # occupies the slot
+    time.sleep(0.01)
+    t.append(srv.submit(none, _sd(1), results_ptr=2, request_bytes=0))
+    t.append(srv.submit(loose, _sd(2), results_ptr=3, request_bytes=0))
+    t.append(srv.submit(slow, _sd(3), results_ptr=4, request_bytes=0))
+    t.append(srv.submit(urgent, _sd(4), results_ptr=5, request_bytes=0))
+    for x in t:
+        srv.wait(x)
+    srv.close()
+    assert [e[3] for e in rec.events] == [1, 5, 3, 4, 2]
