@@ -709,6 +709,8 @@ def run_c5(args):
             c.close()
         ok = [x for x in loads if x["latency_over_subint"]["p99"] < 1.0]
         out[form] = {"alone_ms_mean": float(np.mean(alone)), "loads": loads,
+                     # service time alone / subint duration per job: above 1 the job cannot be real time
+                     "alone_over_subint": [round(a / m, 3) for a, m in zip(alone, subint_ms)],
                      "max_load_p99_within_subint": max((x["offered_load"] for x in ok), default=None),
                      "at_max_load": max(ok, key=lambda x: x["offered_load"]) if ok else None}
     spec_rate = 50.0
@@ -728,8 +730,9 @@ def run_c5(args):
                                              f"specified 50 requests/s at these job sizes would offer "
                                              f"{load50:.1f}x the FP32 form's serial capacity")},
             "forms": out,
-            "tc_vs_fp32_at_max_load": ((out[args.xstep]["at_max_load"] or {}).get("sustained_gsamp_s", 0) /
-                                       max(1e-12, (out["fp32"]["at_max_load"] or {}).get("sustained_gsamp_s", 1e-12)))}
+            "tc_vs_fp32_at_max_load": (out[args.xstep]["at_max_load"]["sustained_gsamp_s"] /
+                                       out["fp32"]["at_max_load"]["sustained_gsamp_s"]
+                                       if out[args.xstep]["at_max_load"] and out["fp32"]["at_max_load"] else None)}
     print(json.dumps(line))
     return 0
 
