@@ -189,6 +189,14 @@ class Reference:
                              si.control[station].ctypes.data_as(C.c_void_p), len(si.control[station]),
                              si.scan, si.sec, si.ns), station)
 
+    def set_interpolator(self, station: int, interp=None) -> None:
+        """Replaces the delay interpolator Mode::setOffsets computes for
+        `station` in later mode_blocks calls (None: the model's again)."""
+        arr = None if interp is None else np.ascontiguousarray(interp, np.float64)
+        st = self.lib.ref_set_interpolator(self.h, station, None if arr is None else arr.ctypes.data_as(C.c_void_p))
+        if st != 0:
+            raise RuntimeError(f"ref_set_interpolator failed ({st})")
+
     def unpack(self, station: int, data: np.ndarray, offset: int, nbands: int, per: int):
         out = np.zeros(nbands * per * 2, np.float32)
         w = C.c_float(0)

@@ -34,6 +34,7 @@ struct RefJob {
   std::vector<void *> scratch;  // Core::threadscratchspace*
   std::vector<int> startblock, numblocks;
   std::vector<u8 *> origbuffers;
+  std::vector<std::vector<double>> interp_override;  // per datastream; empty: the model's
 };
 
 struct ThreadArg {
@@ -221,6 +222,8 @@ int ref_mode_blocks(void *h, int station, const unsigned char *data, int datalen
   m->setValidFlags(flags.data());
   m->setData((u8 *)data, datalen, control[0], control[1], control[2]);
   m->setOffsets(scan, sec, ns);
+  if (station < (int)j->interp_override.size() && j->interp_override[station].size() == 3)
+    for (int i = 0; i < 3; i++) m->interpolator[i] = j->interp_override[station][i];
   const int nb = m->numrecordedbands, nc = m->recordedbandchannels;
   for (int b = 0; b < nblocks; b++) {
     m->process(b, 0);
@@ -233,6 +236,18 @@ int ref_mode_blocks(void *h, int station, const unsigned char *data, int datalen
       memcpy(autos + 2 * ((size_t)x * nb + k) * nc, m->getAutocorrelation(x == 1, k), sizeof(cf32) * nc);
       weights[x * nb + k] = m->getWeight(x == 1, k);
     }
+  return 0;
+}
+
+// Replaces the delay interpolator that setOffsets computes for `station` in
+// later ref_mode_blocks calls (interp3 = null: the model's again).
+int ref_set_interpolator(void *h, int station, const double *interp3)
+{
+  RefJob *j = (RefJob *)h;
+  if (station < 0 || station >= j->nds) return -1;
+  if ((int)j->interp_override.size() < j->nds) j->interp_override.resize(j->nds);
+  j->interp_override[station].clear();
+  if (interp3) j->interp_override[station].assign(interp3, interp3 + 3);
   return 0;
 }
 
