@@ -13,7 +13,7 @@ from typing import List, Optional, Sequence
 
 import numpy as np
 
-from .jobfiles import JobSpec
+from .jobfiles import JobSpec, baseline_plan
 
 GX_MAX_LOCAL_FREQS = 64
 GX_MAX_BANDS = 128
@@ -45,7 +45,12 @@ class gx_station_desc(C.Structure):
                 ("band_pol", C.c_char * GX_MAX_BANDS),
                 ("clock_int_seconds", C.c_int),
                 ("phase_cal_interval_hz", C.c_longlong), ("phase_cal_base_hz", C.c_longlong),
-                ("interlaced", C.c_int)]
+                ("interlaced", C.c_int),
+                ("nzoomfreqs", C.c_int),
+                ("zoomfreq", C.c_int * GX_MAX_LOCAL_FREQS),
+                ("nzoombands", C.c_int),
+                ("zoomband_localfreq", C.c_int * GX_MAX_BANDS),
+                ("zoomband_pol", C.c_char * GX_MAX_BANDS)]
 
 
 class gx_baseline_desc(C.Structure):
@@ -108,10 +113,12 @@ class JobDesc:
 
 def job_desc_from_spec(spec: JobSpec, xstep: int = GX_XSTEP_FP32, max_data_bytes: int = 0,
                        block_chunk: int = 0, spectra_budget_bytes: int = 0) -> JobDesc:
-    """gx_job_desc for a JobSpec (all stations share the same recorded bands)."""
+    """gx_job_desc for a JobSpec: the freq table is its subbands then its zoom
+    freqs; each station records its subbands (all of them by default) in every
+    polarisation and has the zoom freqs that lie within them."""
     spec.validate()
     freqs = []
-    for sb in spec.subbands:
+    for sb in list(spec.subbands) + list(spec.zooms):
         f = gx_freq_desc()
         f.freq_mhz = sb.freq_mhz
         f.bw_mhz = sb.bw_mhz
@@ -119,52 +126,58 @@ def job_desc_from_spec(spec: JobSpec, xstep: int = GX_XSTEP_FP32, max_data_bytes
         f.nchan = sb.nchan
         f.chans_to_average = spec.chans_to_avg
         freqs.append(f)
-    npol = len(spec.pols)
+    nsb = len(spec.subbands)
     stations = []
     for s in range(spec.nstations):
         st = gx_station_desc()
         st.nbits = spec.nbits
         st.is_complex = 1 if spec.is_complex else 0
         st.framebytes = spec.framebytes
-        st.nrecfreqs = len(spec.subbands)
-        for j in range(len(spec.subbands)):
-            st.recfreq[j] = j
+        sbs = spec.station_sb(s)
+        st.nrecfreqs = len(sbs)
+        for j, g in enumerate(sbs):
+            st.recfreq[j] = g
             st.clock_offset_us[j] = 0.0
             st.clock_offset_delta_us[j] = 0.0
             st.lo_offset_hz[j] = 0.0
         st.nbands = spec.nbands
         b = 0
         pols = b""
-        for j in range(len(spec.subbands)):
+        for j in range(len(sbs)):
             for p in spec.pols:
                 st.band_localfreq[b] = j
                 pols += p.encode()
                 b += 1
         st.band_pol = pols
+        zl = spec.station_zooms(s)
+        st.nzoomfreqs = len(zl)
+        b = 0
+        pols = b""
+        for j, (k, _) in enumerate(zl):
+            st.zoomfreq[j] = nsb + k
+            for p in spec.zpols:
+                st.zoomband_localfreq[b] = j
+                pols += p.encode()
+                b += 1
+        st.nzoombands = b
+        st.zoomband_pol = pols
         c0 = spec.clock_us[s] if s < len(spec.clock_us) else 0.0
         st.clock_int_seconds = int(math.floor(c0 / 1e6 + 0.5))
         st.phase_cal_interval_hz = int(1e6 * spec.pcal_interval_mhz)
         st.interlaced = 1 if spec.mux_threads > 0 else 0
         stations.append(st)
     baselines = []
-    for a in range(spec.nstations):
-        for bb in range(a + 1, spec.nstations):
-            bl = gx_baseline_desc()
-            bl.ds1, bl.ds2 = a, bb
-            bl.nfreqs = len(spec.subbands)
-            for j in range(len(spec.subbands)):
-                bl.freq[j] = j
-                prods = []
-                for p1 in range(npol):
-                    for p2 in range(npol):
-                        if p1 == p2 or spec.full_pol:
-                            prods.append((p1, p2))
-                prods.sort(key=lambda t: (t[0] != t[1], t))
-                bl.npolprod[j] = len(prods)
-                for k, (p1, p2) in enumerate(prods):
-                    bl.band1[j][k] = j * npol + p1
-                    bl.band2[j][k] = j * npol + p2
-            baselines.append(bl)
+    for a, bb, fl in baseline_plan(spec):
+        bl = gx_baseline_desc()
+        bl.ds1, bl.ds2 = a, bb
+        bl.nfreqs = len(fl)
+        for j, (f, pairs) in enumerate(fl):
+            bl.freq[j] = f
+            bl.npolprod[j] = len(pairs)
+            for k, (b1, b2) in enumerate(pairs):
+                bl.band1[j][k] = b1
+                bl.band2[j][k] = b2
+        baselines.append(bl)
     return JobDesc(stations, freqs, baselines,
                    subint_ns=spec.subint_ns, guard_ns=spec.guard_ns,
                    fringe_rotation_order=spec.fringe_rot_order, array_stride=spec.array_stride,

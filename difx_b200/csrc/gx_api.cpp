@@ -52,7 +52,8 @@ static void free_all(gx_handle *h)
   if (h->device < 0) return;
   void *ptrs[] = {h->d_st, h->d_tw, h->d_spec, h->d_acc, h->d_results, h->d_spec1, h->d_w, h->d_wacc, h->d_w1,
                   h->d_pairs, h->d_prods, h->d_went, h->d_sub, h->d_bp, h->d_bp1, h->d_scale, h->d_tcprods,
-                  h->d_tcrows, h->d_err, h->d_full, h->d_avgtab, h->d_pcal, h->d_pcalbins};
+                  h->d_tcrows, h->d_err, h->d_full, h->d_avgtab, h->d_pcal, h->d_pcalbins, h->d_zrows,
+                  h->d_zprods, h->d_specz, h->d_accz};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->h_err) cudaFreeHost(h->h_err);
@@ -106,13 +107,28 @@ static gx_status setup(gx_handle *h)
     for (int b = 0; b < x.nbands; b++)
       if (x.band_localfreq[b] < 0 || x.band_localfreq[b] >= x.nrecfreqs)
         return h->fail(GX_ERR_ARG, "REC BAND INDEX out of range");
+    if (x.nzoomfreqs < 0 || x.nzoomfreqs > GX_MAX_LOCAL_FREQS || x.nzoombands < 0 ||
+        x.nbands + x.nzoombands > GX_MAX_BANDS)
+      return h->fail(GX_ERR_ARG, "datastream zoom freq/band count out of range");
+    for (int i = 0; i < x.nzoomfreqs; i++)
+      if (x.zoomfreq[i] < 0 || x.zoomfreq[i] >= d.nfreqs) return h->fail(GX_ERR_ARG, "ZOOM FREQ INDEX out of range");
+    for (int b = 0; b < x.nzoombands; b++)
+      if (x.zoomband_localfreq[b] < 0 || x.zoomband_localfreq[b] >= x.nzoomfreqs)
+        return h->fail(GX_ERR_ARG, "ZOOM BAND INDEX out of range");
   }
   if (s0.nbits != 1 && s0.nbits != 2 && s0.nbits != 4 && s0.nbits != 8)
     return h->fail(GX_ERR_UNSUPPORTED, "QUANTISATION BITS must be 1, 2, 4 or 8");
+  // the recorded freqs share bandwidth and channel count and come first in the
+  // freq table: their spectra and accumulators are slabs [0, nfmain)
   const gx_freq_desc &f0 = d.freqs[s0.recfreq[0]];
-  for (int f = 0; f < d.nfreqs; f++)
-    if (d.freqs[f].nchan != f0.nchan || d.freqs[f].bw_mhz != f0.bw_mhz)
-      return h->fail(GX_ERR_UNSUPPORTED, "all freqs must share bandwidth and channel count");
+  h->nfmain = 0;
+  for (int s = 0; s < d.nstations; s++)
+    for (int i = 0; i < d.stations[s].nrecfreqs; i++) {
+      const gx_freq_desc &fq = d.freqs[d.stations[s].recfreq[i]];
+      if (fq.nchan != f0.nchan || fq.bw_mhz != f0.bw_mhz)
+        return h->fail(GX_ERR_UNSUPPORTED, "all recorded freqs must share bandwidth and channel count");
+      h->nfmain = std::max(h->nfmain, d.stations[s].recfreq[i] + 1);
+    }
   const int cplx = s0.is_complex ? 1 : 0;
   const int bits_ts = s0.nbands * s0.nbits * (cplx ? 2 : 1);
   // whole bytes per time sample, or a whole number of time samples per byte
@@ -155,7 +171,7 @@ static gx_status setup(gx_handle *h)
   J.sampletime = 1.0 / (2.0 * f0.bw_mhz);
   if (cplx) J.sampletime *= 2.0;
   J.bw = f0.bw_mhz;
-  J.nfreqs = d.nfreqs;
+  J.nfreqs = h->nfmain;
   {
     double ffttime = 1000.0 * f0.nchan / f0.bw_mhz;
     double b = d.subint_ns / ffttime;
@@ -268,6 +284,138 @@ static gx_status setup(gx_handle *h)
         return h->fail(GX_ERR_ARG, "POL PRODUCTS out of range");
     }
   const int bpa = h->maxprod > 2 ? 2 : 1;
+  const bool writecross = d.write_autocorrs && h->maxprod > 2;
+
+  // Zoom freqs (configuration.cpp:1701-1753, 2774-2880; mode.cpp:184-196,
+  // 379-391): a station's zoom freq is a channel range of the recorded freq
+  // that contains it (the last one, as Configuration's search leaves it), from
+  // the channel offset Configuration computes with the first recorded freq's
+  // channel width; a zoom band takes the parent band of its polarisation.
+  // Each zoom freq gets spectra rows of its own: one per zoom band, plus the
+  // parent's cross-polarisation partner where the zoom freq lacks it (its
+  // cross-pol autocorrelation is a slice of the parent's).  Zoom freqs follow
+  // the recorded freqs in the freq table and share one channel count.
+  h->zfreq.clear();
+  h->zrows.clear();
+  h->nzchan = 0;
+  std::vector<int> zord(d.nfreqs, -1), zcount;
+  // [station][zoom band]: parent recorded band, row, row of the cross-pol partner (-1: none)
+  std::vector<std::vector<int>> zparent(d.nstations), zrow(d.nstations), zpartner(d.nstations);
+  auto partner_of = [&](const gx_station_desc &x, int b, int *i0p = nullptr, int *i1p = nullptr) {
+    // the two bands of b's local freq in band order (mode.cpp:1124-1129, 1333-1351)
+    int i0 = -1, i1 = -1;
+    for (int q = 0; q < x.nbands; q++)
+      if (x.band_localfreq[q] == x.band_localfreq[b]) {
+        if (i0 < 0) i0 = q;
+        else if (i1 < 0) i1 = q;
+      }
+    if (i0p) *i0p = i0;
+    if (i1p) *i1p = i1;
+    return (b == i0) ? i1 : ((b == i1) ? i0 : -1);
+  };
+  for (int s = 0; s < d.nstations; s++) {
+    const gx_station_desc &x = d.stations[s];
+    zparent[s].assign(x.nzoombands, -1);
+    zrow[s].assign(x.nzoombands, -1);
+    zpartner[s].assign(x.nzoombands, -1);
+    if (x.nzoombands == 0) continue;
+    std::vector<int> zpar(x.nzoomfreqs, -1), zoff(x.nzoomfreqs, 0);
+    const gx_freq_desc &r0 = d.freqs[x.recfreq[0]];
+    for (int j = 0; j < x.nzoomfreqs; j++) {
+      const int fz = x.zoomfreq[j];
+      if (fz < h->nfmain)
+        return h->fail(GX_ERR_UNSUPPORTED, "zoom freqs must follow every recorded freq in the freq table");
+      const gx_freq_desc &zq = d.freqs[fz];
+      double zlo = zq.freq_mhz, zhi = zq.freq_mhz + zq.bw_mhz;
+      if (zq.lower_sideband) { zlo -= zq.bw_mhz; zhi -= zq.bw_mhz; }
+      for (int k = 0; k < x.nrecfreqs; k++) {
+        const gx_freq_desc &pq = d.freqs[x.recfreq[k]];
+        double plo = pq.freq_mhz, phi = pq.freq_mhz + pq.bw_mhz;
+        if (pq.lower_sideband) { plo -= pq.bw_mhz; phi -= pq.bw_mhz; }
+        if (zhi <= phi && zlo >= plo) {
+          zpar[j] = k;
+          zoff[j] = (int)(((zlo - plo) / r0.bw_mhz) * r0.nchan + 0.5);
+        }
+      }
+      if (zpar[j] < 0) return h->fail(GX_ERR_ARG, "a zoom freq does not fit into any recorded freq");
+      const gx_freq_desc &pq = d.freqs[x.recfreq[zpar[j]]];
+      if (std::fabs(zq.bw_mhz / zq.nchan - pq.bw_mhz / pq.nchan) > 0.000000001)   // Mode::TINY
+        return h->fail(GX_ERR_ARG, "a zoom freq's channel width differs from its parent's");
+      if (zq.lower_sideband != pq.lower_sideband)
+        return h->fail(GX_ERR_UNSUPPORTED, "a zoom freq of the other sideband than its parent");
+      if (zoff[j] < 0 || zoff[j] + zq.nchan > pq.nchan)
+        return h->fail(GX_ERR_UNSUPPORTED, "a zoom freq's channels run past its parent's");
+      if (zq.nchan < 2 || zq.nchan % 2) return h->fail(GX_ERR_UNSUPPORTED, "zoom freqs need an even channel count");
+      if (h->nzchan == 0) h->nzchan = zq.nchan;
+      else if (zq.nchan != h->nzchan) return h->fail(GX_ERR_UNSUPPORTED, "zoom freqs with different channel counts");
+      if (zord[fz] < 0) {
+        zord[fz] = (int)h->zfreq.size();
+        h->zfreq.push_back(fz);
+        zcount.push_back(0);
+      }
+    }
+    for (int b = 0; b < x.nzoombands; b++) {
+      const int j = x.zoomband_localfreq[b];
+      int parent = -1, nmatch = 0;
+      for (int l = 0; l < x.nbands; l++)
+        if (x.band_localfreq[l] == zpar[j] && x.band_pol[l] == x.zoomband_pol[b]) { parent = l; nmatch++; }
+      if (nmatch == 0) return h->fail(GX_ERR_ARG, "a zoom band's polarisation is not recorded in its parent freq");
+      if (nmatch > 1) return h->fail(GX_ERR_UNSUPPORTED, "a zoom band's parent freq records its polarisation twice");
+      const int z = zord[x.zoomfreq[j]];
+      zparent[s][b] = parent;
+      zrow[s][b] = zcount[z]++;
+      h->zrows.push_back(ZoomRow{z, zrow[s][b], x.recfreq[zpar[j]], h->band_input[s][parent], zoff[j]});
+    }
+    if (writecross)
+      for (int b = 0; b < x.nzoombands; b++) {
+        const int pp = partner_of(x, zparent[s][b]);
+        if (pp < 0) continue;
+        const int j = x.zoomband_localfreq[b];
+        for (int b2 = 0; b2 < x.nzoombands; b2++)
+          if (x.zoomband_localfreq[b2] == j && zparent[s][b2] == pp) zpartner[s][b] = zrow[s][b2];
+        if (zpartner[s][b] < 0) {   // the partner's channels as a row of their own
+          const int z = zord[x.zoomfreq[j]];
+          zpartner[s][b] = zcount[z]++;
+          h->zrows.push_back(ZoomRow{z, zpartner[s][b], x.recfreq[zpar[j]], h->band_input[s][pp], zoff[j]});
+        }
+      }
+  }
+  {
+    int nzi = 0;
+    for (int c : zcount) nzi = std::max(nzi, c);
+    h->zxs = xmac_shape(std::max(1, nzi));
+    h->nzrows = h->zxs.nsuper * h->zxs.ST;
+  }
+  // freq of total band k of a station (recorded bands, then zoom bands: getDTotalFreqIndex)
+  auto total_freq = [&](const gx_station_desc &x, int k) {
+    return k < x.nbands ? x.recfreq[x.band_localfreq[k]] : x.zoomfreq[x.zoomband_localfreq[k - x.nbands]];
+  };
+  // Autocorrelations are kept for bands whose freq, or an equivalent one (same
+  // band edge, bandwidth, sideband-adjusted, and channel count), a baseline
+  // correlates (configuration.cpp:2299-2325; core.cpp:1273-1301)
+  auto ac_used = [&](int f) {
+    if (freq_used(f)) return true;
+    const gx_freq_desc &a = d.freqs[f];
+    for (int k = 0; k < d.nfreqs; k++) {
+      const gx_freq_desc &b = d.freqs[k];
+      double fd = a.freq_mhz - b.freq_mhz;
+      if (a.lower_sideband) fd -= a.bw_mhz;
+      if (b.lower_sideband) fd += b.bw_mhz;
+      const int aa = a.chans_to_average > 1 ? a.chans_to_average : 1, ba = b.chans_to_average > 1 ? b.chans_to_average : 1;
+      if (std::fabs(a.bw_mhz - b.bw_mhz) < 0.000000001 && std::fabs(fd) < 0.000000001 && a.nchan == b.nchan &&
+          aa == ba && freq_used(k))
+        return true;
+    }
+    return false;
+  };
+  // the total bands of a station with autocorrelations in the result, in order
+  auto ac_bands = [&](int s) {
+    const gx_station_desc &x = d.stations[s];
+    std::vector<int> v;
+    for (int k = 0; k < x.nbands + x.nzoombands; k++)
+      if (ac_used(total_freq(x, k))) v.push_back(k);
+    return v;
+  };
   // CHANS TO AVG (core.cpp:1819-1869, mode.cpp:1376-1401): one averaging length
   // per job, dividing the channel count
   int avg = 1;
@@ -372,15 +520,11 @@ static gx_status setup(gx_handle *h)
     for (int s = 0; s < d.nstations; s++) {
       acofs[s] = (int)idx;
       const gx_station_desc &x = d.stations[s];
-      for (int b = 0; b < x.nbands; b++)
-        if (freq_used(x.recfreq[x.band_localfreq[b]])) idx += (long long)bpa * (J.nchan / div);
+      for (int k : ac_bands(s)) idx += (long long)bpa * (d.freqs[total_freq(x, k)].nchan / div);
     }
     for (int s = 0; s < d.nstations; s++) {
       acwofs[s] = (int)idx;
-      const gx_station_desc &x = d.stations[s];
-      int add = 0;
-      for (int b = 0; b < x.nbands; b++)
-        if (freq_used(x.recfreq[x.band_localfreq[b]])) add += bpa;
+      int add = bpa * (int)ac_bands(s).size();
       add = (add + 1) / 2;
       if (add == 0) add = 1;
       idx += add;
@@ -426,11 +570,16 @@ static gx_status setup(gx_handle *h)
     for (int q = 0; q < d.nstations; q++)
       for (int n : pc_ntones[q]) total_pc += n;
     for (int s = 0; s < d.nstations; s++) {
-      const long long end_full = s + 1 < d.nstations ? h->acofs_full[s + 1] : h->acwofs_full[0];
-      const int nr = (int)((end_full - h->acofs_full[s]) / J.nchan);
-      for (int r = 0; r < nr; r++)
-        add(h->acofs_full[s] + (long long)r * J.nchan, h->acofs[s] + (long long)r * (J.nchan / avg), J.nchan / avg,
-            avg);
+      // parallel-hand rows of the station's bands, then (with cross-pol) the cross-hand rows
+      long long src = h->acofs_full[s], dst = h->acofs[s];
+      const std::vector<int> acb = ac_bands(s);
+      for (int rep = 0; rep < bpa; rep++)
+        for (int k : acb) {
+          const int nf = d.freqs[total_freq(d.stations[s], k)].nchan;
+          add(src, dst, nf / avg, avg);
+          src += nf;
+          dst += nf / avg;
+        }
       const long long wend_full = s + 1 < d.nstations ? h->acwofs_full[s + 1] : h->rl_full - total_pc;
       add(h->acwofs_full[s], h->acwofs[s], (int)(wend_full - h->acwofs_full[s]), 1);
     }
@@ -438,17 +587,26 @@ static gx_status setup(gx_handle *h)
       add(P.result_offset, h->pc_off[(size_t)P.station * GX_MAX_BANDS + P.band], P.ntones, 1);
   }
 
-  // accumulator index of the Hermitian entry (a, b) of freq f
+  // FP32 accumulator index of the Hermitian entry (a, b) of freq slab f (shape
+  // xs, N channels)
   const XmacShape &xs = h->xs;
-  auto acc_index = [&](int f, int a, int b, int &conj) -> long long {
+  auto shape_index = [](const XmacShape &xs, int N, int f, int a, int b, int &conj) -> long long {
     conj = 0;
     if (a / xs.T > b / xs.T) { int t = a; a = b; b = t; conj = 1; }
     int SI = a / xs.ST, SJ = b / xs.ST;
     long long stp = 0;
     for (int i = 0; i < SI; i++) stp += xs.nsuper - i;
     stp += SJ - SI;
-    return (((long long)f * xs.npairs + stp) * xs.ST * xs.ST + (long long)(a % xs.ST) * xs.ST + (b % xs.ST)) *
-           J.nchan;
+    return (((long long)f * xs.npairs + stp) * xs.ST * xs.ST + (long long)(a % xs.ST) * xs.ST + (b % xs.ST)) * N;
+  };
+  auto acc_index = [&](int f, int a, int b, int &conj) { return shape_index(xs, J.nchan, f, a, b, conj); };
+  h->zprods.clear();
+  // one zoom visibility row: result offset ro <- rows (a, b) of zoom freq z
+  auto add_zprod = [&](long long ro, int z, int a, int b) {
+    ProdEntry e{};
+    e.result_offset = ro;
+    e.acc_index = shape_index(h->zxs, h->nzchan, z, a, b, e.conj);
+    h->zprods.push_back(e);
   };
   h->prods.clear();
   h->tcprods.clear();
@@ -494,55 +652,71 @@ static gx_status setup(gx_handle *h)
       const gx_baseline_desc &B = d.baselines[j];
       int lf = bl_localfreq(B, f);
       if (lf < 0) continue;
+      const gx_station_desc &x1 = d.stations[B.ds1], &x2 = d.stations[B.ds2];
+      const int z = zord[f];
       for (int p = 0; p < B.npolprod[lf]; p++) {
         int b1 = B.band1[lf][p], b2 = B.band2[lf][p];
-        if (b1 < 0 || b1 >= d.stations[B.ds1].nbands || b2 < 0 || b2 >= d.stations[B.ds2].nbands)
-          return h->fail(GX_ERR_UNSUPPORTED, "baseline band index out of range (zoom bands are not implemented)");
-        int a = h->band_input[B.ds1][b1], bb = h->band_input[B.ds2][b2];
-        add_prod(h->blofs_full[f * nbl + j] + (long long)p * J.nchan, f, a, bb);
         WeightEntry w{};
         w.float_index = 2LL * h->bwofs_full[f * nbl + j] + p;
-        w.source = h->interlaced_any ? item(wrow(B.ds1, b1), wrow(B.ds2, b2)) : d.nstations + j;
+        if (z < 0) {
+          if (b1 < 0 || b1 >= x1.nbands || b2 < 0 || b2 >= x2.nbands)
+            return h->fail(GX_ERR_ARG, "baseline band index out of range");
+          int a = h->band_input[B.ds1][b1], bb = h->band_input[B.ds2][b2];
+          add_prod(h->blofs_full[f * nbl + j] + (long long)p * J.nchan, f, a, bb);
+          w.source = h->interlaced_any ? item(wrow(B.ds1, b1), wrow(B.ds2, b2)) : d.nstations + j;
+        } else {
+          // zoom bands: the products of their rows; weights of their parent
+          // recorded bands (datastream record band index, configuration.cpp:1203-1260)
+          const int z1 = b1 - x1.nbands, z2 = b2 - x2.nbands;
+          if (z1 < 0 || z1 >= x1.nzoombands || z2 < 0 || z2 >= x2.nzoombands || total_freq(x1, b1) != f ||
+              total_freq(x2, b2) != f)
+            return h->fail(GX_ERR_ARG, "a baseline's zoom freq product names a band of another freq");
+          add_zprod(h->blofs_full[f * nbl + j] + (long long)p * h->nzchan, z, zrow[B.ds1][z1], zrow[B.ds2][z2]);
+          w.source = h->interlaced_any ? item(wrow(B.ds1, zparent[B.ds1][z1]), wrow(B.ds2, zparent[B.ds2][z2]))
+                                       : d.nstations + j;
+        }
         h->wents.push_back(w);
       }
     }
   }
-  const bool writecross = d.write_autocorrs && h->maxprod > 2;
   for (int s = 0; s < d.nstations; s++) {
     const gx_station_desc &x = d.stations[s];
     long long ro = h->acofs_full[s];
     long long wo = 2LL * h->acwofs_full[s];
-    std::vector<int> used;
-    for (int b = 0; b < x.nbands; b++)
-      if (freq_used(x.recfreq[x.band_localfreq[b]])) used.push_back(b);
-    for (int b : used) {
-      int f = x.recfreq[x.band_localfreq[b]];
-      int a = h->band_input[s][b];
-      add_prod(ro, f, a, a);
-      ro += J.nchan;
+    // total bands: recorded, then zoom (their autocorrelations are slices of
+    // the parent band's, mode.cpp:379-391; weights the parent's, core.cpp:1317-1370)
+    const std::vector<int> used = ac_bands(s);
+    for (int k : used) {
+      const int f = total_freq(x, k);
       WeightEntry w{};
       w.float_index = wo++;
-      w.source = item(wrow(s, b), -1);
+      if (k < x.nbands) {
+        const int a = h->band_input[s][k];
+        add_prod(ro, f, a, a);
+        w.source = item(wrow(s, k), -1);
+      } else {
+        const int zb = k - x.nbands;
+        add_zprod(ro, zord[f], zrow[s][zb], zrow[s][zb]);
+        w.source = item(wrow(s, zparent[s][zb]), -1);
+      }
+      ro += d.freqs[f].nchan;
       h->wents.push_back(w);
     }
     if (writecross) {
-      for (int b : used) {
-        int lf = x.band_localfreq[b];
-        int f = x.recfreq[lf];
-        // partner: indices[0], indices[1] of this freq (mode.cpp:1124-1129, 1333-1351)
-        int i0 = -1, i1 = -1;
-        for (int q = 0; q < x.nbands; q++)
-          if (x.band_localfreq[q] == lf) {
-            if (i0 < 0) i0 = q;
-            else if (i1 < 0) i1 = q;
-          }
-        int partner = (b == i0) ? i1 : ((b == i1) ? i0 : -1);
+      for (int k : used) {
+        const int f = total_freq(x, k);
+        const int bp = k < x.nbands ? k : zparent[s][k - x.nbands];   // the recorded band
+        int i0, i1;
+        const int partner = partner_of(x, bp, &i0, &i1);
         WeightEntry w{};
         w.float_index = wo++;
         w.source = partner < 0 ? -1 : x.interlaced ? item(wrow(s, i0), wrow(s, i1)) : s;
         h->wents.push_back(w);
-        if (partner >= 0) add_prod(ro, f, h->band_input[s][b], h->band_input[s][partner]);
-        ro += J.nchan;
+        if (partner >= 0) {
+          if (k < x.nbands) add_prod(ro, f, h->band_input[s][k], h->band_input[s][partner]);
+          else add_zprod(ro, zord[f], zrow[s][k - x.nbands], zpartner[s][k - x.nbands]);
+        }
+        ro += d.freqs[f].nchan;
       }
     }
   }
@@ -565,16 +739,17 @@ static gx_status setup(gx_handle *h)
   }
 
   // chunking and K-split
-  const size_t per_block = (size_t)d.nfreqs * J.ninputs * J.nchan * sizeof(float2);
+  const size_t per_block = ((size_t)h->nfmain * J.ninputs * J.nchan +
+                           h->zfreq.size() * (size_t)h->nzrows * h->nzchan) * sizeof(float2);
   // Every pass reads and writes the accumulators once; the spectra of a block
   // are written and read once.  Passes of at least `efficient` blocks keep the
   // accumulator traffic under a quarter of the spectra traffic.
   size_t acc_pass;
   if (h->tc) {
     const size_t cols = (size_t)(ni + 7) / 8 * 8;   // written in 8-column slices
-    acc_pass = 2 * (size_t)d.nfreqs * (J.nchan / 2) * ni * cols * sizeof(float4);
+    acc_pass = 2 * (size_t)h->nfmain * (J.nchan / 2) * ni * cols * sizeof(float4);
   } else {
-    acc_pass = 2 * (size_t)d.nfreqs * xs.npairs * xs.ST * xs.ST * J.nchan * sizeof(float2);
+    acc_pass = 2 * (size_t)h->nfmain * xs.npairs * xs.ST * xs.ST * J.nchan * sizeof(float2);
   }
   const size_t efficient = std::max<size_t>(64, (4 * acc_pass + 2 * per_block - 1) / (2 * per_block));
   int chunk;
@@ -609,13 +784,13 @@ static gx_status setup(gx_handle *h)
     // adds a full accumulator write and finalise read, so the K dimension is
     // split only while the grid is under two waves of 148 SMs (at least 4
     // K-tiles per slice).
-    const long long base = (long long)(J.nchan / 2) * d.nfreqs;
+    const long long base = (long long)(J.nchan / 2) * h->nfmain;
     const int kmax = std::max(1, std::min(16, chunk / 64));
     int best = 1;
     while (best < kmax && base * best < 2 * 148) best++;
     h->ks = best;
   } else {
-    long long base = (long long)((J.nchan + xs.CT - 1) / xs.CT) * xs.npairs * d.nfreqs;
+    long long base = (long long)((J.nchan + xs.CT - 1) / xs.CT) * xs.npairs * h->nfmain;
     // K-split: enough CTAs for at least two per SM, rounded to whole waves of
     // 148 SMs where possible, keeping at least 64 blocks per slice
     const int kmax = std::max(1, std::min(16, chunk / 64));
@@ -629,6 +804,21 @@ static gx_status setup(gx_handle *h)
       if (score > best_score + 1e-9) { best_score = score; best = ks; }
     }
     h->ks = best;
+  }
+  // zoom X-step K-split: as the FP32 X-step's, over the zoom freqs
+  h->zks = 1;
+  if (!h->zfreq.empty()) {
+    const XmacShape &zx = h->zxs;
+    const long long base = (long long)((h->nzchan + zx.CT - 1) / zx.CT) * zx.npairs * (long long)h->zfreq.size();
+    const int kmax = std::max(1, std::min(16, chunk / 64));
+    double best_score = -1;
+    for (int ks = 1; ks <= kmax; ks++) {
+      const long long ctas = base * ks;
+      const double waves = std::ceil(ctas / 148.0);
+      const double score = ctas / (waves * 148.0) * std::min(1.0, ctas / 296.0);
+      if (score > best_score + 1e-9) { best_score = score; h->zks = ks; }
+    }
+    h->zacc_slice = h->zfreq.size() * (size_t)zx.npairs * zx.ST * zx.ST * h->nzchan;
   }
   // F-step concurrency: FFT slots per CTA
   {
@@ -677,11 +867,11 @@ static gx_status setup(gx_handle *h)
     CKR(h, cudaMemcpy(h->d_tw, tw.data(), sizeof(float2) * tw.size(), cudaMemcpyHostToDevice));
     J.twiddle = h->d_tw;
   }
-  const size_t spec_elems = (size_t)d.nfreqs * chunk * J.ninputs * J.nchan;
+  const size_t spec_elems = (size_t)h->nfmain * chunk * J.ninputs * J.nchan;
   CKR(h, h->dalloc(&h->d_spec, sizeof(float2) * spec_elems));
   CKR(h, cudaMemsetAsync(h->d_spec, 0, sizeof(float2) * spec_elems, h->stream));
-  CKR(h, h->dalloc(&h->d_spec1, sizeof(float2) * (size_t)d.nfreqs * J.ninputs * J.nchan));
-  CKR(h, cudaMemsetAsync(h->d_spec1, 0, sizeof(float2) * (size_t)d.nfreqs * J.ninputs * J.nchan, h->stream));
+  CKR(h, h->dalloc(&h->d_spec1, sizeof(float2) * (size_t)h->nfmain * J.ninputs * J.nchan));
+  CKR(h, cudaMemsetAsync(h->d_spec1, 0, sizeof(float2) * (size_t)h->nfmain * J.ninputs * J.nchan, h->stream));
   CKR(h, h->dalloc(&h->d_w, sizeof(float) * (size_t)h->nwrows * chunk));
   CKR(h, h->dalloc(&h->d_w1, sizeof(float) * (size_t)h->nwrows));
   if (h->interlaced_any)
@@ -690,8 +880,8 @@ static gx_status setup(gx_handle *h)
   CKR(h, h->dalloc(&h->d_bp1, sizeof(BlockParam) * (size_t)d.nstations));
   if (h->tc) {
     // [freq][chan/2][128][128] float4 (both channels of a pair) per K-split slice
-    h->acc_slice = (size_t)d.nfreqs * J.nchan * kTcInputs * kTcInputs;
-    const size_t nsc = (size_t)d.nfreqs * kTcInputs * J.nchan;
+    h->acc_slice = (size_t)h->nfmain * J.nchan * kTcInputs * kTcInputs;
+    const size_t nsc = (size_t)h->nfmain * kTcInputs * J.nchan;
     std::vector<float> sc(nsc, h->tc_scale0);
     CKR(h, h->dalloc(&h->d_scale, sizeof(float) * nsc));
     CKR(h, cudaMemcpy(h->d_scale, sc.data(), sizeof(float) * nsc, cudaMemcpyHostToDevice));
@@ -704,9 +894,21 @@ static gx_status setup(gx_handle *h)
       CKR(h, cudaMemcpy(h->d_tcrows, h->tcrows.data(), sizeof(TcRowEntry) * h->tcrows.size(),
                         cudaMemcpyHostToDevice));
   } else {
-    h->acc_slice = (size_t)d.nfreqs * xs.npairs * xs.ST * xs.ST * J.nchan;
+    h->acc_slice = (size_t)h->nfmain * xs.npairs * xs.ST * xs.ST * J.nchan;
   }
   CKR(h, h->dalloc(&h->d_acc, sizeof(float2) * h->acc_slice * h->ks));
+  if (!h->zfreq.empty()) {
+    // zoom spectra rows beyond the table's stay zero
+    const size_t nz = h->zfreq.size() * (size_t)chunk * h->nzrows * h->nzchan;
+    CKR(h, h->dalloc(&h->d_specz, sizeof(float2) * nz));
+    CKR(h, cudaMemsetAsync(h->d_specz, 0, sizeof(float2) * nz, h->stream));
+    CKR(h, h->dalloc(&h->d_accz, sizeof(float2) * h->zacc_slice * h->zks));
+    CKR(h, h->dalloc(&h->d_zrows, sizeof(ZoomRow) * h->zrows.size()));
+    CKR(h, cudaMemcpy(h->d_zrows, h->zrows.data(), sizeof(ZoomRow) * h->zrows.size(), cudaMemcpyHostToDevice));
+    CKR(h, h->dalloc(&h->d_zprods, sizeof(ProdEntry) * std::max<size_t>(1, h->zprods.size())));
+    if (!h->zprods.empty())
+      CKR(h, cudaMemcpy(h->d_zprods, h->zprods.data(), sizeof(ProdEntry) * h->zprods.size(), cudaMemcpyHostToDevice));
+  }
   CKR(h, h->dalloc(&h->d_err, sizeof(int)));
   CKR(h, cudaMemset(h->d_err, 0, sizeof(int)));
   CKR(h, cudaMallocHost(&h->h_err, sizeof(int) * gx_handle::kSlots));
@@ -827,6 +1029,7 @@ gx_status plan_job(const gx_job_desc *desc, JobPlan *plan, std::string &err)
   if (h.avg > 1) { err = "channel averaging is not implemented by the allocation-free entry point"; return GX_ERR_UNSUPPORTED; }
   if (!h.pcal.empty()) { err = "phase-cal extraction is not implemented by the allocation-free entry point"; return GX_ERR_UNSUPPORTED; }
   if (h.interlaced_any) { err = "INTERLACEDVDIF is not implemented by the allocation-free entry point"; return GX_ERR_UNSUPPORTED; }
+  if (!h.zfreq.empty()) { err = "zoom bands are not implemented by the allocation-free entry point"; return GX_ERR_UNSUPPORTED; }
   plan->J = h.J;
   plan->J.twiddle = nullptr;
   plan->maxnrf = h.maxnrf;
@@ -1025,6 +1228,8 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
   auto mark = [&](int stage, bool start) -> gx_status { return timed ? record(h, st, stage, start) : GX_OK; };
   // the tensor-core X-step stores its first chunk instead of adding to it
   if (!h->tc) CKR(h, cudaMemsetAsync(h->d_acc, 0, sizeof(float2) * h->acc_slice * h->ks, st));
+  const int nzr = (int)h->zrows.size(), nzf = (int)h->zfreq.size();
+  if (nzf) CKR(h, cudaMemsetAsync(h->d_accz, 0, sizeof(float2) * h->zacc_slice * h->zks, st));
   const int npairs = (int)h->pairs.size();
   CKR(h, cudaMemsetAsync(h->d_wacc, 0, sizeof(float) * (d.nstations + npairs), st));
   CKR(h, cudaMemsetAsync(h->d_err, 0, sizeof(int), st));
@@ -1044,10 +1249,16 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
     if ((r = mark(0, false)) != GX_OK) return r;
     if ((r = mark(1, true)) != GX_OK) return r;
     if (h->tc)
-      CKR(h, xmac_tc_launch(h->d_spec, nb, J.nchan, d.nfreqs, J.ninputs, h->ks, h->hilo, h->d_scale, acc4,
+      CKR(h, xmac_tc_launch(h->d_spec, nb, J.nchan, h->nfmain, J.ninputs, h->ks, h->hilo, h->d_scale, acc4,
                             b0 > 0 ? 1 : 0, h->d_err, st));
     else
-      CKR(h, xmac_fp32_launch(h->d_spec, nb, J.ninputs, J.nchan, d.nfreqs, h->ks, h->d_acc, h->d_err, st));
+      CKR(h, xmac_fp32_launch(h->d_spec, nb, J.ninputs, J.nchan, h->nfmain, h->ks, h->d_acc, h->d_err, st));
+    if (nzf) {   // zoom freqs: their rows of this pass's spectra, then their cross products
+      CKR(h, zoom_gather_launch(h->d_zrows, nzr, h->d_spec, J.ninputs, J.nchan, h->d_specz, h->nzrows, h->nzchan, nb,
+                                st));
+      CKR(h, xmac_fp32_launch(h->d_specz, nb, h->nzrows, h->nzchan, nzf, h->zks, h->d_accz, h->d_err, st));
+      h->launches += 2;
+    }
     CKR(h, weights_launch(h->d_w, nb, d.nstations, h->d_pairs, npairs, h->d_wacc, st));
     if ((r = mark(1, false)) != GX_OK) return r;
     h->launches += 3;
@@ -1057,7 +1268,7 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
   float2 *fin = h->avg > 1 ? h->d_full : dev_results;
   CKR(h, cudaMemsetAsync(fin, 0, sizeof(float2) * h->rl_full, st));
   if (h->tc) {
-    CKR(h, finalise_tc_launch(h->d_tcprods, h->d_tcrows, (int)h->tcrows.size(), acc4, d.nfreqs, J.nchan,
+    CKR(h, finalise_tc_launch(h->d_tcprods, h->d_tcrows, (int)h->tcrows.size(), acc4, h->nfmain, J.nchan,
                               J.ninputs, h->ks, fin, st));
     CKR(h, finalise_launch(nullptr, 0, h->d_acc, h->ks, h->acc_slice, J.nchan, h->d_went, (int)h->wents.size(),
                            h->d_wacc, fin, st));
@@ -1066,6 +1277,11 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
                            (int)h->wents.size(), h->d_wacc, fin, st));
   }
   h->launches += (h->prods.empty() ? 0 : 1) + (h->wents.empty() ? 0 : 1);
+  if (!h->zprods.empty()) {
+    CKR(h, finalise_launch(h->d_zprods, (int)h->zprods.size(), h->d_accz, h->zks, h->zacc_slice, h->nzchan, nullptr,
+                           0, nullptr, fin, st));
+    h->launches += 1;
+  }
   if (npc) {
     CKR(h, pcal_tones_launch(h->d_pcal, npc, h->pcal_chunks, h->pcal_maxbins, h->d_pcalbins, fin, st));
     h->launches += 1;

@@ -42,6 +42,19 @@ struct gx_handle {
   std::vector<std::vector<double>> pc_tone_hz;   // [station * GX_MAX_BANDS + band]: tone frequencies (Hz)
   std::vector<int> pc_maxtones;              // [station]: most tones of a band (0: phase-cal off)
   std::vector<std::vector<int>> band_input;  // [station][band]
+  // Zoom freqs (zoom bands, mode.cpp:184-196): every pass gathers their
+  // spectra rows from the parent freqs' rows, and the FP32 X-step
+  // cross-multiplies them into accumulators of their own.
+  int nfmain = 0;                            // freqs [0, nfmain) hold the recorded bands
+  std::vector<int> zfreq;                    // zoom ordinal -> freq table index
+  int nzchan = 0, nzrows = 0, zks = 1;       // zoom channels, rows per zoom freq (padded), K-split
+  gx::XmacShape zxs{};
+  std::vector<gx::ZoomRow> zrows;
+  std::vector<gx::ProdEntry> zprods;
+  size_t zacc_slice = 0;                     // float2 per zoom K-split slice
+  gx::ZoomRow *d_zrows = nullptr;
+  gx::ProdEntry *d_zprods = nullptr;
+  float2 *d_specz = nullptr, *d_accz = nullptr;
   std::vector<gx::ProdEntry> prods;
   std::vector<gx::TcProdEntry> tcprods;   // sorted by (freq, a)
   std::vector<gx::TcRowEntry> tcrows;

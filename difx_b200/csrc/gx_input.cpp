@@ -11,8 +11,8 @@
 //   .im     -- Model::readPolynomialSamples (model.cpp:596-837).
 //
 // Only the first configuration is read, and the features the device path does
-// not implement (pulsar binning, phased array, zoom bands, phase cal,
-// multiple phase centres) are rejected with a message.
+// not implement (pulsar binning, phased array, multiple phase centres,
+// PHASE CAL DIVISOR other than 1) are rejected with a message.
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -372,8 +372,20 @@ InputJob *read_input_job(const char *inputfile, std::string &err)
       NEED(in, "REC BAND ", v); s.band_pol[j] = strip(v).empty() ? 'R' : strip(v)[0];
       NEED(in, "REC BAND ", v); s.band_localfreq[j] = atoi(v.c_str());
     }
-    NEED(in, "NUM ZOOM FREQS", v);
-    if (atoi(v.c_str()) != 0) { err = "zoom bands are not implemented"; return nullptr; }
+    // zoom freqs and bands (configuration.cpp:1701-1753)
+    NEED(in, "NUM ZOOM FREQS", v); s.nzoomfreqs = atoi(v.c_str());
+    if (s.nzoomfreqs < 0 || s.nzoomfreqs > GX_MAX_LOCAL_FREQS) { err = "too many zoom freqs"; return nullptr; }
+    int nzb = 0;
+    for (int j = 0; j < s.nzoomfreqs; j++) {
+      NEED(in, "ZOOM FREQ INDEX ", v); s.zoomfreq[j] = atoi(v.c_str());
+      NEED(in, "NUM ZOOM POLS ", v); nzb += atoi(v.c_str());
+    }
+    if (nzb < 0 || nzb > GX_MAX_BANDS) { err = "too many zoom bands"; return nullptr; }
+    s.nzoombands = nzb;
+    for (int j = 0; j < nzb; j++) {
+      NEED(in, "ZOOM BAND ", v); s.zoomband_pol[j] = strip(v).empty() ? 'R' : strip(v)[0];
+      NEED(in, "ZOOM BAND ", v); s.zoomband_localfreq[j] = atoi(v.c_str());
+    }
     const std::vector<double> &cp = clockpoly[dstel[i]];
     s.clock_int_seconds = int(std::floor((cp.empty() ? 0.0 : cp[0]) / 1000000.0 + 0.5));
   }
@@ -398,8 +410,18 @@ InputJob *read_input_job(const char *inputfile, std::string &err)
         NEED(in, "D/STREAM A BAND ", v); b.band1[j][k] = atoi(v.c_str());
         NEED(in, "D/STREAM B BAND ", v); b.band2[j][k] = atoi(v.c_str());
       }
+      // the freq of the first product's band of datastream A; band indices
+      // from the recorded band count on name zoom bands (configuration.cpp:1095-1100)
       const gx_station_desc &s1 = dstab[b.ds1];
-      b.freq[j] = s1.recfreq[s1.band_localfreq[b.band1[j][0]]];
+      const int b1 = b.band1[j][0];
+      if (b1 < 0 || b1 >= s1.nbands + s1.nzoombands) { err = "baseline band index out of range"; return nullptr; }
+      if (b1 < s1.nbands) {
+        b.freq[j] = s1.recfreq[s1.band_localfreq[b1]];
+      } else {
+        const int zl = s1.zoomband_localfreq[b1 - s1.nbands];
+        if (zl < 0 || zl >= s1.nzoomfreqs) { err = "ZOOM BAND INDEX out of range"; return nullptr; }
+        b.freq[j] = s1.zoomfreq[zl];
+      }
     }
   }
 

@@ -107,6 +107,8 @@ gx_status gx_vis_open(gx_handle *h, const char *outdir, gx_vis **out)
   *out = nullptr;
   if (h->device < 0) return h->fail(GX_ERR_STATE, "host-only handle (opened with device -1)");
   if (!h->model || !h->meta) return h->fail(GX_ERR_STATE, "the visibility writer needs a handle opened with gx_open_input");
+  if (!h->zfreq.empty())   // records of the zoom freqs' own channel counts
+    return h->fail(GX_ERR_UNSUPPORTED, "the visibility writer does not implement zoom freqs");
   std::unique_ptr<gx_vis> v(new gx_vis());
   v->h = h;
   v->outdir = outdir;

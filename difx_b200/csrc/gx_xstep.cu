@@ -298,6 +298,27 @@ cudaError_t finalise_launch(const ProdEntry *prods, int nprods, const float2 *ac
   return cudaGetLastError();
 }
 
+// Zoom spectra rows: one thread per channel of one row of one block.
+__global__ void zoom_gather_kernel(const ZoomRow *__restrict__ rows, const float2 *__restrict__ spec, int NIm, int Nm,
+                                   float2 *__restrict__ specz, int NIz, int Nz, int nblk)
+{
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= Nz) return;
+  const ZoomRow r = rows[blockIdx.y];
+  const int b = blockIdx.z;
+  specz[(((size_t)r.zf * nblk + b) * NIz + r.zrow) * Nz + k] = spec[(((size_t)r.mf * nblk + b) * NIm + r.mrow) * Nm + r.off + k];
+}
+
+cudaError_t zoom_gather_launch(const ZoomRow *rows, int nrows, const float2 *spec, int NIm, int Nm, float2 *specz,
+                               int NIz, int Nz, int nblk, cudaStream_t st)
+{
+  if (nrows <= 0 || nblk <= 0) return cudaSuccess;
+  if (nrows > 65535 || nblk > 65535) return cudaErrorInvalidConfiguration;
+  dim3 grid((Nz + 127) / 128, nrows, nblk);
+  zoom_gather_kernel<<<grid, 128, 0, st>>>(rows, spec, NIm, Nm, specz, NIz, Nz, nblk);
+  return cudaGetLastError();
+}
+
 // Channel averaging of the finished result array (Mode::averageFrequency,
 // mode.cpp:1376-1401, for autocorrelations; Core's averaged copy,
 // core.cpp:1819-1869, for cross products): one CTA per record.

@@ -66,6 +66,17 @@ cudaError_t finalise_tc_launch(const TcProdEntry *prods, const TcRowEntry *rows,
                                int nfreqs, int N, int ninputs, int ks, float2 *results, cudaStream_t st);
 // One record of channel averaging (CHANS TO AVG): n output values at dst, each
 // the mean of L consecutive values from src (L = 1: a copy, for weights).
+// One spectra row of a zoom freq (Mode, mode.cpp:184-196: a zoom band's
+// spectrum is its parent recorded band's from a channel offset on): row `zrow`
+// of zoom freq `zf` takes input `mrow` of freq `mf` from channel `off`.
+struct ZoomRow {
+  int zf, zrow, mf, mrow, off;
+};
+// specz[zf][block][zrow][0 .. Nz) = spec[mf][block][mrow][off .. off + Nz)
+// for the nblk blocks of a pass (rows not in the table are left as they are).
+cudaError_t zoom_gather_launch(const ZoomRow *rows, int nrows, const float2 *spec, int NIm, int Nm, float2 *specz,
+                               int NIz, int Nz, int nblk, cudaStream_t st);
+
 struct AvgEntry {
   long long src, dst;
   int n, L;

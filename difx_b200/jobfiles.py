@@ -82,11 +82,49 @@ class JobSpec:
     poly_interval_s: int = 120
     station_names: Sequence[str] = ()
     data_files: Sequence[str] = ()
+    # per station, the indices into `subbands` it records (default: all of
+    # them); every station records the same number
+    station_subbands: Sequence[Sequence[int]] = ()
+    # zoom freqs (freq-table entries after the subbands): each station
+    # correlates each one that lies within one of its recorded subbands, in
+    # every polarisation
+    zooms: Sequence[Subband] = ()
+    zoom_only: bool = False           # baselines correlate the zoom freqs only
+    zoom_pols: Tuple[str, ...] = ()   # polarisations of the zoom bands (default: pols)
 
     # ------------------------------------------------------------ derived
+    def station_sb(self, station: int) -> List[int]:
+        """Indices into `subbands` of the subbands a station records."""
+        if self.station_subbands:
+            return list(self.station_subbands[station])
+        return list(range(len(self.subbands)))
+
+    def station_zooms(self, station: int) -> List[Tuple[int, int]]:
+        """(zoom index, local recorded freq of its parent) of each zoom freq the
+        station correlates: the last recorded subband containing it, as the
+        reference's search leaves it (configuration.cpp:1718-1737)."""
+        out = []
+        sbs = self.station_sb(station)
+        for k, z in enumerate(self.zooms):
+            zlo = z.freq_mhz - (z.bw_mhz if z.sideband == "L" else 0.0)
+            parent = -1
+            for j, i in enumerate(sbs):
+                p = self.subbands[i]
+                plo = p.freq_mhz - (p.bw_mhz if p.sideband == "L" else 0.0)
+                if zlo >= plo and zlo + z.bw_mhz <= plo + p.bw_mhz:
+                    parent = j
+            if parent >= 0:
+                out.append((k, parent))
+        return out
+
     @property
     def nbands(self) -> int:
-        return len(self.subbands) * len(self.pols)
+        """Recorded bands per station."""
+        return len(self.station_sb(0)) * len(self.pols)
+
+    @property
+    def zpols(self) -> Tuple[str, ...]:
+        return tuple(self.zoom_pols) if self.zoom_pols else tuple(self.pols)
 
     @property
     def is_complex(self) -> bool:
@@ -144,6 +182,12 @@ class JobSpec:
         for sb in self.subbands:
             if sb.bw_mhz != self.bw_mhz or sb.nchan != self.nchan:
                 raise ValueError("all subbands must share bandwidth and channel count")
+        if self.station_subbands and (len(self.station_subbands) != self.nstations or
+                                      len({len(x) for x in self.station_subbands}) != 1):
+            raise ValueError("every station must record the same number of subbands")
+        for z in self.zooms:
+            if abs(z.bw_mhz / z.nchan - self.bw_mhz / self.nchan) > 1e-9:
+                raise ValueError("a zoom freq's channel width must equal the subbands'")
         if self.bits_per_timesample % 8 != 0 and 8 % self.bits_per_timesample != 0:
             raise ValueError("a time sample of all bands must fill whole bytes or divide a byte")
         if (self.payload_bytes * 8) % self.bits_per_timesample != 0:
@@ -228,6 +272,48 @@ def delay_poly_rows(spec: JobSpec, coeffs: np.ndarray, nsamples: int) -> np.ndar
     return rows
 
 
+def baseline_plan(spec: JobSpec) -> List[Tuple[int, int, List[Tuple[int, List[Tuple[int, int]]]]]]:
+    """The baseline table: (datastream A, datastream B, [(freq-table index,
+    [(band A, band B) per polarisation product])]).  Freqs are the recorded
+    subbands both stations record (unless zoom_only), then the zoom freqs both
+    correlate; band indices count the recorded bands, then the zoom bands, as
+    the reference does (configuration.cpp:1095-1115)."""
+    npol = len(spec.pols)
+    nsb = len(spec.subbands)
+    prods = []
+    for p1 in range(npol):
+        for p2 in range(npol):
+            if p1 == p2 or spec.full_pol:
+                prods.append((p1, p2))
+    # DiFX order: parallel hands first, then cross hands (RR, LL, RL, LR)
+    prods.sort(key=lambda t: (t[0] != t[1], t))
+    out = []
+    for a in range(spec.nstations):
+        for b in range(a + 1, spec.nstations):
+            sa, sb_ = spec.station_sb(a), spec.station_sb(b)
+            za = [k for k, _ in spec.station_zooms(a)]
+            zb = [k for k, _ in spec.station_zooms(b)]
+            freqs = []
+            if not spec.zoom_only:
+                for i in range(nsb):
+                    if i in sa and i in sb_:
+                        freqs.append((i, [(sa.index(i) * npol + p1, sb_.index(i) * npol + p2) for p1, p2 in prods]))
+            zp = spec.zpols
+            nzp = len(zp)
+            zprods = []
+            for p1 in range(nzp):
+                for p2 in range(nzp):
+                    if p1 == p2 or spec.full_pol:
+                        zprods.append((p1, p2))
+            zprods.sort(key=lambda t: (t[0] != t[1], t))
+            for k in range(len(spec.zooms)):
+                if k in za and k in zb:
+                    freqs.append((nsb + k, [(spec.nbands + za.index(k) * nzp + p1, spec.nbands + zb.index(k) * nzp + p2)
+                                            for p1, p2 in zprods]))
+            out.append((a, b, freqs))
+    return out
+
+
 def write_job(spec: JobSpec, outdir: str) -> dict:
     """Write ``<name>.input/.calc/.im/.threads/.flag`` into outdir; return their paths."""
     spec.validate()
@@ -282,8 +368,8 @@ def write_job(spec: JobSpec, outdir: str) -> dict:
     L.append(_kv("RULE 0 SCAN ID", "SCAN0"))
     L.append(_kv("RULE 0 CONFIG NAME", "gxcfg"))
     L.append("\n# FREQ TABLE #######!\n")
-    L.append(_kv("FREQ ENTRIES", nsb))
-    for i, sb in enumerate(spec.subbands):
+    L.append(_kv("FREQ ENTRIES", nsb + len(spec.zooms)))
+    for i, sb in enumerate(list(spec.subbands) + list(spec.zooms)):
         L.append(_kv(f"FREQ (MHZ) {i}", f"{sb.freq_mhz:.11f}"))
         L.append(_kv(f"BW (MHZ) {i}", f"{sb.bw_mhz:.11f}"))
         L.append(_kv(f"SIDEBAND {i}", sb.sideband))
@@ -324,41 +410,42 @@ def write_job(spec: JobSpec, outdir: str) -> dict:
         L.append(_kv("DATA SOURCE", "FILE"))
         L.append(_kv("FILTERBANK USED", "FALSE"))
         L.append(_kv("PHASE CAL INT (MHZ)", spec.pcal_interval_mhz))
-        L.append(_kv("NUM RECORDED FREQS", nsb))
-        for j in range(nsb):
-            L.append(_kv(f"REC FREQ INDEX {j}", j))
+        sbs = spec.station_sb(i)
+        L.append(_kv("NUM RECORDED FREQS", len(sbs)))
+        for j, g in enumerate(sbs):
+            L.append(_kv(f"REC FREQ INDEX {j}", g))
             L.append(_kv(f"CLK OFFSET {j} (us)", "0.000000"))
             L.append(_kv(f"FREQ OFFSET {j} (Hz)", "0.000000"))
             L.append(_kv(f"NUM REC POLS {j}", npol))
         b = 0
-        for j in range(nsb):
+        for j in range(len(sbs)):
             for p in spec.pols:
                 L.append(_kv(f"REC BAND {b} POL", p))
                 L.append(_kv(f"REC BAND {b} INDEX", j))
                 b += 1
-        L.append(_kv("NUM ZOOM FREQS", 0))
+        zl = spec.station_zooms(i)
+        L.append(_kv("NUM ZOOM FREQS", len(zl)))
+        for j, (k, _) in enumerate(zl):
+            L.append(_kv(f"ZOOM FREQ INDEX {j}", nsb + k))
+            L.append(_kv(f"NUM ZOOM POLS {j}", len(spec.zpols)))
+        b = 0
+        for j in range(len(zl)):
+            for p in spec.zpols:
+                L.append(_kv(f"ZOOM BAND {b} POL", p))
+                L.append(_kv(f"ZOOM BAND {b} INDEX", j))
+                b += 1
     L.append("\n# BASELINE TABLE ###!\n")
     L.append(_kv("BASELINE ENTRIES", nbl))
-    bl = 0
-    for a in range(nst):
-        for bb in range(a + 1, nst):
-            L.append(_kv(f"D/STREAM A INDEX {bl}", a))
-            L.append(_kv(f"D/STREAM B INDEX {bl}", bb))
-            L.append(_kv(f"NUM FREQS {bl}", nsb))
-            for j in range(nsb):
-                L.append(_kv(f"TARGET FREQ {bl}/{j}", j))
-                prods = []
-                for p1 in range(npol):
-                    for p2 in range(npol):
-                        if p1 == p2 or spec.full_pol:
-                            prods.append((p1, p2))
-                # DiFX order: parallel hands first, then cross hands (RR, LL, RL, LR)
-                prods.sort(key=lambda t: (t[0] != t[1], t))
-                L.append(_kv(f"POL PRODUCTS {bl}/{j}", len(prods)))
-                for k, (p1, p2) in enumerate(prods):
-                    L.append(_kv(f"D/STREAM A BAND {k}", j * npol + p1))
-                    L.append(_kv(f"D/STREAM B BAND {k}", j * npol + p2))
-            bl += 1
+    for bl, (a, bb, freqs) in enumerate(baseline_plan(spec)):
+        L.append(_kv(f"D/STREAM A INDEX {bl}", a))
+        L.append(_kv(f"D/STREAM B INDEX {bl}", bb))
+        L.append(_kv(f"NUM FREQS {bl}", len(freqs)))
+        for j, (f, pairs) in enumerate(freqs):
+            L.append(_kv(f"TARGET FREQ {bl}/{j}", f))
+            L.append(_kv(f"POL PRODUCTS {bl}/{j}", len(pairs)))
+            for k, (b1, b2) in enumerate(pairs):
+                L.append(_kv(f"D/STREAM A BAND {k}", b1))
+                L.append(_kv(f"D/STREAM B BAND {k}", b2))
     L.append("\n# DATA TABLE #######!\n")
     for i in range(nst):
         L.append(_kv(f"D/STREAM {i} FILES", 1))

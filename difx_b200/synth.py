@@ -188,10 +188,11 @@ def make_station_stream(spec: JobSpec, station: int, first_frame: int, nframes: 
     fsamp = spec.frame_samples
     first = first_frame * fsamp
     n = nframes * fsamp
-    nsb = len(spec.subbands)
     cols = []
-    for sbi, sb in enumerate(spec.subbands):
+    for sbi in spec.station_sb(station):
+        sb = spec.subbands[sbi]
         for pi_ in range(len(spec.pols)):
+            # the common signal of a subband is the same at every station recording it
             band = sbi * len(spec.pols) + pi_
             lo = sb.freq_mhz
             x = station_band_signal(spec, station, band, lo, first, n, rho, seed)

@@ -102,6 +102,15 @@ typedef struct gx_station_desc {
   long long phase_cal_base_hz;     /* long(1e6 x PHASE CAL BASE(MHZ)); PHASE CAL DIVISOR must be 1 */
   int interlaced;          /* DATA FORMAT INTERLACEDVDIF: framebytes is the multiplexed frame size and
                               EDV4 validity masks blank absent threads per band (mk5mode.cpp:142-163) */
+  /* Zoom bands (configuration.cpp:1701-1753; Mode, mode.cpp:184-196): a zoom
+     freq is a channel range of the recorded freq that contains it, found and
+     offset as Configuration does.  Baseline band indices nbands + i name zoom
+     band i, as in the reference's total band numbering. */
+  int nzoomfreqs;          /* NUM ZOOM FREQS */
+  int zoomfreq[GX_MAX_LOCAL_FREQS];                /* ZOOM FREQ INDEX -> freq table (after the recorded freqs) */
+  int nzoombands;          /* sum of NUM ZOOM POLS */
+  int zoomband_localfreq[GX_MAX_BANDS];            /* ZOOM BAND i INDEX */
+  char zoomband_pol[GX_MAX_BANDS];                 /* ZOOM BAND i POL */
 } gx_station_desc;
 
 /* One baseline (BASELINE TABLE, configuration.cpp:1033-1180). */
