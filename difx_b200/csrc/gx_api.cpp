@@ -416,6 +416,9 @@ static gx_status setup(gx_handle *h)
       if (ac_used(total_freq(x, k))) v.push_back(k);
     return v;
   };
+  h->zparent = zparent;
+  h->acbands.resize(d.nstations);
+  for (int s = 0; s < d.nstations; s++) h->acbands[s] = ac_bands(s);
   // CHANS TO AVG (core.cpp:1819-1869, mode.cpp:1376-1401): one averaging length
   // per job, dividing the channel count
   int avg = 1;

@@ -52,6 +52,8 @@ struct gx_handle {
   std::vector<gx::ZoomRow> zrows;
   std::vector<gx::ProdEntry> zprods;
   size_t zacc_slice = 0;                     // float2 per zoom K-split slice
+  std::vector<std::vector<int>> zparent;     // [station][zoom band] parent recorded band
+  std::vector<std::vector<int>> acbands;     // [station] total bands (recorded, then zoom) with autocorrelations
   gx::ZoomRow *d_zrows = nullptr;
   gx::ProdEntry *d_zprods = nullptr;
   float2 *d_specz = nullptr, *d_accz = nullptr;

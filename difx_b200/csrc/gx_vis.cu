@@ -20,6 +20,7 @@
 // Covered: one configuration, one phase centre, no pulsar bins, no output
 // bands; TSYS 0 (normalised correlation coefficients) or TSYS > 0
 // (a-priori calibration by the band-mean autocorrelations).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -35,7 +36,7 @@ namespace {
 struct VisScale {
   long long offset;   // complex-float index of the record's first channel
   float scale;
-  int pad_;
+  int nchan;          // the record's channels
 };
 
 __global__ void vis_add4_kernel(float4 *__restrict__ acc, const float4 *__restrict__ r, size_t n)
@@ -57,10 +58,10 @@ __global__ void vis_add_kernel(float *__restrict__ acc, const float *__restrict_
     acc[i] += r[i];
 }
 
-__global__ void vis_scale_kernel(float2 *__restrict__ acc, const VisScale *__restrict__ recs, int nchan)
+__global__ void vis_scale_kernel(float2 *__restrict__ acc, const VisScale *__restrict__ recs)
 {
   const VisScale R = recs[blockIdx.y];
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nchan; c += gridDim.x * blockDim.x) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < R.nchan; c += gridDim.x * blockDim.x) {
     float2 v = acc[R.offset + c];
     v.x *= R.scale;
     v.y *= R.scale;
@@ -107,8 +108,9 @@ gx_status gx_vis_open(gx_handle *h, const char *outdir, gx_vis **out)
   *out = nullptr;
   if (h->device < 0) return h->fail(GX_ERR_STATE, "host-only handle (opened with device -1)");
   if (!h->model || !h->meta) return h->fail(GX_ERR_STATE, "the visibility writer needs a handle opened with gx_open_input");
-  if (!h->zfreq.empty())   // records of the zoom freqs' own channel counts
-    return h->fail(GX_ERR_UNSUPPORTED, "the visibility writer does not implement zoom freqs");
+  if (!h->zfreq.empty() && h->meta)
+    for (double t : h->meta->tsys)   // Configuration::getDMatchingBand reads zoom bands out of range
+      if (t > 0.0) return h->fail(GX_ERR_UNSUPPORTED, "a-priori calibration (TSYS > 0) of zoom bands is not implemented");
   std::unique_ptr<gx_vis> v(new gx_vis());
   v->h = h;
   v->outdir = outdir;
@@ -117,7 +119,7 @@ gx_status gx_vis_open(gx_handle *h, const char *outdir, gx_vis **out)
   int nrec = 0;
   for (int i = 0; i < d.nbaselines; i++)
     for (int k = 0; k < d.baselines[i].nfreqs; k++) nrec += d.baselines[i].npolprod[k];
-  for (int s = 0; s < d.nstations; s++) nrec += 2 * d.stations[s].nbands;
+  for (int s = 0; s < d.nstations; s++) nrec += 2 * (d.stations[s].nbands + d.stations[s].nzoombands);
   v->maxrec = nrec > 0 ? nrec : 1;
   CKR(h, cudaSetDevice(h->device));
   CKR(h, cudaMalloc(&v->d_int, sizeof(float2) * h->rl));
@@ -166,7 +168,8 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
   if (scan < 0 || scan >= (int)model.scans.size()) return GX_OK;               // past the last scan
   const int scanstart = (int)model.scan_start_sec(scan);
   if (sec + scanstart >= M.execute_seconds || v->nsub == 0) return GX_OK;      // writedata's early exits
-  const int nbl = d.nbaselines, N = h->J.nchan / h->avg;   // output channels per record
+  const int nbl = d.nbaselines;
+  auto nout = [&](int f) { return d.freqs[f].nchan / h->avg; };   // output channels of freq f's records
 
   // weights: the baseline-weight and autocorrelation-weight regions of the summed array
   std::vector<float> fr(2 * (size_t)h->rl);
@@ -190,15 +193,28 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
   // Visibility::changeConfig (visibility.cpp:1314-1316)
   const double meansub = M.int_time / (((double)d.subint_ns) / 1000000000.0);
   const double ffts = meansub * h->J.blocks_per_send;
-  const float chanfactor = (float)(h->J.blocks_per_send * 2 * N * h->avg);   // blocks per send * 2 * nchan * chanavg
-  auto weight_and_scale = [&](long long widx, float &w, float &scale) {
+  // blocks per send * 2 * nchan * chanavg of freq f
+  auto chanfactor = [&](int f) { return (float)(h->J.blocks_per_send * 2 * nout(f) * h->avg); };
+  auto weight_and_scale = [&](long long widx, int f, float &w, float &scale) {
     w = (float)(fr[widx] / ffts);
-    scale = w > 0.0f ? (float)(1.0 / ((double)w * meansub * (double)chanfactor)) : 0.0f;
+    scale = w > 0.0f ? (float)(1.0 / ((double)w * meansub * (double)chanfactor(f))) : 0.0f;
   };
-  auto freq_used = [&](int f) {
-    for (int j = 0; j < nbl; j++)
-      if (gx_bl_localfreq(d.baselines[j], f) >= 0) return true;
-    return false;
+  // freq and polarisation of total band k (recorded bands, then zoom bands)
+  auto total_freq = [&](const gx_station_desc &x, int k) {
+    return k < x.nbands ? x.recfreq[x.band_localfreq[k]] : x.zoomfreq[x.zoomband_localfreq[k - x.nbands]];
+  };
+  auto total_pol = [&](const gx_station_desc &x, int k) {
+    return k < x.nbands ? x.band_pol[k] : x.zoomband_pol[k - x.nbands];
+  };
+  // zoom bandwidth / parent recorded bandwidth of total band k >= nbands of
+  // station s, as the reference's FP32 `modifier` (visibility.cpp:355, 532-545, 626-631)
+  auto zoom_modifier = [&](int s, int k) {
+    const gx_station_desc &x = d.stations[s];
+    const int pf = x.recfreq[x.band_localfreq[h->zparent[s][k - x.nbands]]];
+    float modifier = 1.0f;
+    modifier *= d.freqs[total_freq(x, k)].bw_mhz;
+    modifier /= d.freqs[pf].bw_mhz;
+    return modifier;
   };
   // A-priori calibration with TSYS > 0 (visibility.cpp:463-484, 505-519,
   // 607-616): the FP32 mean of each band's summed parallel-hand
@@ -208,18 +224,17 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
   std::vector<std::vector<float>> calib(d.nstations), acw0(d.nstations);
   for (int s = 0; s < d.nstations; s++) {
     const gx_station_desc &x = d.stations[s];
-    calib[s].assign(x.nbands, 0.0f);
-    acw0[s].assign(x.nbands, 0.0f);
+    calib[s].assign(x.nbands + x.nzoombands, 0.0f);
+    acw0[s].assign(x.nbands + x.nzoombands, 0.0f);
     long long widx = 2LL * h->acwofs[s];   // the parallel-hand weights come first
-    for (int b = 0; b < x.nbands; b++)
-      if (freq_used(x.recfreq[x.band_localfreq[b]])) acw0[s][b] = (float)(fr[widx++] / ffts);
+    for (int k : h->acbands[s]) acw0[s][k] = (float)(fr[widx++] / ffts);
     if (!(s < (int)M.tsys.size() && M.tsys[s] > 0.0)) continue;
     long long off = h->acofs[s];
-    for (int b = 0; b < x.nbands; b++) {
-      if (!freq_used(x.recfreq[x.band_localfreq[b]])) continue;
+    for (int k : h->acbands[s]) {
+      const int N = nout(total_freq(x, k));
       float re = 0.0f;
       for (int c = 0; c < N; c++) re += fr[2 * (off + c)];
-      calib[s][b] = re / N;
+      calib[s][k] = re / N;
       off += N;
     }
   }
@@ -239,6 +254,7 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
     float weight;
     double uvw[3];
     long long offset;
+    int nchan;
   };
   std::vector<Rec> recs;
   std::vector<VisScale> scales;
@@ -253,9 +269,14 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
     for (int f = 0; f < d.nfreqs; f++) {
       const int lf = gx_bl_localfreq(B, f);
       if (lf < 0) continue;
+      const int N = nout(f);
       for (int k = 0; k < B.npolprod[lf]; k++) {
         float w, scale;
-        weight_and_scale(2LL * h->bwofs[f * nbl + i] + k, w, scale);
+        weight_and_scale(2LL * h->bwofs[f * nbl + i] + k, f, w, scale);
+        if (w > 0.0f) {   // zoom bands: fewer samples per channel (visibility.cpp:530-545)
+          if (B.band1[lf][k] >= d.stations[B.ds1].nbands) scale *= std::sqrt(zoom_modifier(B.ds1, B.band1[lf][k]));
+          if (B.band2[lf][k] >= d.stations[B.ds2].nbands) scale *= std::sqrt(zoom_modifier(B.ds2, B.band2[lf][k]));
+        }
         if (tsys(B.ds1) > 0.0 && tsys(B.ds2) > 0.0) {
           const int b1 = B.band1[lf][k], b2 = B.band2[lf][k];
           const float divisor = kDecorrelation[d.stations[B.ds1].nbits - 1] * kDecorrelation[d.stations[B.ds2].nbits - 1] *
@@ -263,13 +284,14 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
           scale = (divisor > 0.0f && w > 0.0f)
                       ? (float)(std::sqrt(tsys(B.ds1) * tsys(B.ds2) / divisor) / w) : 0.0f;
         }
-        if (scale > 0.0f) scales.push_back(VisScale{h->blofs[f * nbl + i] + (long long)k * N, scale, 0});
+        if (scale > 0.0f) scales.push_back(VisScale{h->blofs[f * nbl + i] + (long long)k * N, scale, N});
         if (w > 0.0f) {
           r.freq = f;
-          r.pol[0] = d.stations[B.ds1].band_pol[B.band1[lf][k]];
-          r.pol[1] = d.stations[B.ds2].band_pol[B.band2[lf][k]];
+          r.pol[0] = total_pol(d.stations[B.ds1], B.band1[lf][k]);
+          r.pol[1] = total_pol(d.stations[B.ds2], B.band2[lf][k]);
           r.weight = w;
           r.offset = h->blofs[f * nbl + i] + (long long)k * N;
+          r.nchan = N;
           recs.push_back(r);
         }
       }
@@ -280,25 +302,29 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
       const gx_station_desc &x = d.stations[s];
       long long off = h->acofs[s], widx = 2LL * h->acwofs[s];
       for (int j = 0; j < acwidth; j++)
-        for (int b = 0; b < x.nbands; b++) {
-          const int f = x.recfreq[x.band_localfreq[b]];
-          if (!freq_used(f)) continue;
+        for (int b : h->acbands[s]) {   // recorded bands, then zoom bands
+          const int f = total_freq(x, b), N = nout(f);
           float w, scale;
-          weight_and_scale(widx++, w, scale);
+          weight_and_scale(widx++, f, w, scale);
           if (tsys(s) > 0.0) {
             const int m = j == 0 ? b : matching_band(x, b);
             const float divisor = m >= 0 ? std::sqrt(calib[s][b] * calib[s][m]) : 0.0f;
             scale = divisor > 0.0f ? (float)(tsys(s) / divisor) : 0.0f;
+          } else if (b >= x.nbands && w > 0.0f) {
+            // a zoom band's autocorrelation: times zoom bandwidth / parent
+            // bandwidth, in FP32 as the reference forms it (visibility.cpp:624-633)
+            scale *= zoom_modifier(s, b);
           }
-          if (scale > 0.0f) scales.push_back(VisScale{off, scale, 0});
+          if (scale > 0.0f) scales.push_back(VisScale{off, scale, N});
           if (w > 0.0f) {
             Rec r{};
             r.baseline = 257 * (M.telescope[s] + 1);
             r.freq = f;
-            r.pol[0] = x.band_pol[b];
+            r.pol[0] = total_pol(x, b);
             r.pol[1] = j == 0 ? r.pol[0] : opposite_pol(r.pol[0]);
             r.weight = w;
             r.offset = off;
+            r.nchan = N;
             recs.push_back(r);
           }
           off += N;
@@ -310,8 +336,10 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
   if (!scales.empty()) {
     if ((int)scales.size() > v->maxrec) return h->fail(GX_ERR_ARG, "record table overflow");
     CKR(h, cudaMemcpyAsync(v->d_rec, scales.data(), sizeof(VisScale) * scales.size(), cudaMemcpyHostToDevice, v->st));
-    dim3 grid((N + 255) / 256, (unsigned)scales.size());
-    vis_scale_kernel<<<grid, 256, 0, v->st>>>(v->d_int, v->d_rec, N);
+    int maxn = 1;
+    for (const VisScale &x : scales) maxn = std::max(maxn, x.nchan);
+    dim3 grid((maxn + 255) / 256, (unsigned)scales.size());
+    vis_scale_kernel<<<grid, 256, 0, v->st>>>(v->d_int, v->d_rec);
     CKR(h, cudaGetLastError());
   }
   CKR(h, cudaMemcpyAsync(v->h_buf, v->d_int, sizeof(float2) * h->rl, cudaMemcpyDeviceToHost, v->st));
@@ -322,7 +350,11 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
   const int dumpmjd = M.start_mjd + intsec / 86400;
   const double dumpseconds = double(intsec % 86400) + ((double)ns) / 1000000000.0 + M.int_time / 2.0;
   std::vector<char> buf;
-  buf.reserve(recs.size() * (74 + sizeof(float2) * (size_t)N));
+  {
+    size_t bytes = 0;
+    for (const Rec &r : recs) bytes += 74 + sizeof(float2) * (size_t)r.nchan;
+    buf.reserve(bytes);
+  }
   for (const Rec &r : recs) {
     put(buf, (uint32_t)0xFF00FF00u);   // sync word
     put(buf, (int32_t)1);              // binary header version
@@ -340,7 +372,7 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
     put(buf, r.uvw[1]);
     put(buf, r.uvw[2]);
     const char *p = reinterpret_cast<const char *>(v->h_buf + r.offset);
-    buf.insert(buf.end(), p, p + sizeof(float2) * (size_t)N);
+    buf.insert(buf.end(), p, p + sizeof(float2) * (size_t)r.nchan);
   }
   char name[64];
   snprintf(name, sizeof(name), "/DIFX_%05d_%06d.s%04d.b%04d", M.start_mjd, M.start_seconds, 0, 0);
@@ -367,7 +399,13 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
       for (int b = 0; b < x.nbands; b++) {
         const int f = x.recfreq[x.band_localfreq[b]];
         float w = 0.0f, scale = 0.0f;
-        if (freq_used(f)) weight_and_scale(widx++, w, scale);
+        if (std::find(h->acbands[s].begin(), h->acbands[s].end(), b) != h->acbands[s].end())
+          weight_and_scale(widx++, f, w, scale);
+        if (w == 0.0f && x.nzoombands > 0) {
+          // zoom mode with no autocorrelation of the band: data contribution only (visibility.cpp:661-663)
+          w = 1.0f;
+          scale = (float)(1.0 / ((double)w * meansub * (double)chanfactor(f)));
+        }
         const size_t key = (size_t)s * GX_MAX_BANDS + b;
         const int nt = h->pc_ntones[key];
         const long long base = h->pc_off[key];

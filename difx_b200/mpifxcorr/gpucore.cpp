@@ -59,13 +59,21 @@ int GpuCore::build(int ci, Job &job)
       }
     }
     s.nbands = c->getDNumRecordedBands(ci, ds);
-    if (s.nbands > GX_MAX_BANDS || c->getDNumZoomBands(ci, ds) > 0) {
-      err = s.nbands > GX_MAX_BANDS ? "too many recorded bands" : "zoom bands are not implemented by gxcorr";
+    s.nzoomfreqs = dd.numzoomfreqs;
+    s.nzoombands = c->getDNumZoomBands(ci, ds);
+    if (s.nbands + s.nzoombands > GX_MAX_BANDS || s.nzoomfreqs > GX_MAX_LOCAL_FREQS) {
+      err = "too many recorded or zoom bands";
       return GX_ERR_UNSUPPORTED;
     }
     for (int b = 0; b < s.nbands; b++) {
       s.band_localfreq[b] = c->getDLocalRecordedFreqIndex(ci, ds, b);
       s.band_pol[b] = c->getDRecordedBandPol(ci, ds, b);
+    }
+    // zoom freqs and bands (the device finds their parents and offsets as Configuration does)
+    for (int i = 0; i < s.nzoomfreqs; i++) s.zoomfreq[i] = dd.zoomfreqtableindices[i];
+    for (int b = 0; b < s.nzoombands; b++) {
+      s.zoomband_localfreq[b] = c->getDLocalZoomFreqIndex(ci, ds, b);
+      s.zoomband_pol[b] = c->getDZoomBandPol(ci, ds, b);
     }
     s.clock_int_seconds = (int)std::floor(c->getDClockCoeff(ci, ds, 0) / 1000000.0 + 0.5);   // mode.cpp:68
     s.phase_cal_interval_hz = c->getDPhaseCalIntervalHz(ci, ds);

@@ -31,7 +31,18 @@ CASES = {
     # a-priori calibration (visibility.cpp:463-484, 505-519, 607-616)
     "c1_tsys": lambda: jobs.spec_c1(name="gvist", seed=41, int_time=0.016, tsys=55.0),
     "cplx8_tsys": lambda: jobs.spec_cplx8(name="gvisct", seed=43, int_time=0.008192, tsys=70.0),
+    # zoom freqs: records of their own channel counts, zoom autocorrelations
+    # scaled by zoom / parent bandwidth (visibility.cpp:624-633)
+    "zoom_shifted": lambda: _zoom("shifted"),
+    "zoom_mixed": lambda: _zoom("mixed"),
+    "zoom_avg": lambda: _zoom("avg"),
 }
+
+
+def _zoom(name):
+    from dataclasses import replace
+    from tests.test_zoom import _case
+    return replace(_case(name), name="gvisz_" + name, int_time=0.016)
 
 
 def _run_gpu(prep, outdir, xstep=capi.GX_XSTEP_FP32):
@@ -81,7 +92,8 @@ def test_gx_vis_bytes_match_reference_visibility(case, tmp_path):
     b = np.fromfile(_file(theirs), np.uint8)
     assert a.size == b.size, (a.size, b.size)
     assert np.array_equal(a, b)
-    assert len(swin.read_records(_file(ours), spec.nchan // spec.chans_to_avg)) == n
+    freqs = list(spec.subbands) + list(spec.zooms)
+    assert len(swin.read_records(_file(ours), lambda f: freqs[f].nchan // spec.chans_to_avg)) == n
 
 
 def test_gx_vis_end_to_end_matches_reference(tmp_path):

@@ -159,3 +159,26 @@ def test_gpu_zoom_matches_reference(name):
         print(f"\n{name} xstep {xs}: {len(recs)} records, worst record {worst:.3g}, weights {wrel:.3g}")
         assert worst <= 1e-5, (name, xs, worst)
         assert wrel <= 1e-6, (name, xs, wrel)
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not (pyoracle.reference_available() and pyoracle.shim_available()),
+                    reason="reference or binding harness not built")
+@pytest.mark.parametrize("name", ["shifted", "mixed"])
+def test_gpucore_zoom_slot_matches_core_processdata(name):
+    """The DiFX-side GpuCore passes the Configuration's zoom freqs and bands
+    to the device: a zoom job's slot against Core::processdata."""
+    from difx_b200.gxcorr import Correlator
+    spec = _case(name)
+    prep = jobs.prepare(spec, [100_000_000])
+    ref = jobs.reference_for(prep.paths["input"])
+    r = ref.process(prep.subs[0])
+    b = pyoracle.Binding(prep.paths["input"])
+    g = b.process(prep.subs[0], ref.result_length)
+    b.close()
+    c = Correlator.from_input(prep.paths["input"], device=-1)
+    recs = _records(spec, c.offsets())
+    c.close()
+    worst = max(float(np.mean(np.abs(g[o:o + n] - r[o:o + n])) / np.mean(np.abs(r[o:o + n]))) for o, n in recs)
+    print(f"\n{name}: GpuCore vs Core::processdata worst record {worst:.3g}")
+    assert worst <= 1e-5, worst
