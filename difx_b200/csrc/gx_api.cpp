@@ -30,6 +30,8 @@ using namespace gx;
 
 namespace {
 
+constexpr double kTwoPi = 6.283185307179586476925286766559;   // TWO_PI of the generic architecture
+
 int stride_length(int n)  // calcstridelength, configuration.cpp:38-50
 {
   if (n <= 16) return n;
@@ -53,7 +55,7 @@ static void free_all(gx_handle *h)
   void *ptrs[] = {h->d_st, h->d_tw, h->d_spec, h->d_acc, h->d_results, h->d_spec1, h->d_w, h->d_wacc, h->d_w1,
                   h->d_pairs, h->d_prods, h->d_went, h->d_sub, h->d_bp, h->d_bp1, h->d_scale, h->d_tcprods,
                   h->d_tcrows, h->d_err, h->d_full, h->d_avgtab, h->d_pcal, h->d_pcalbins, h->d_zrows,
-                  h->d_zprods, h->d_specz, h->d_accz};
+                  h->d_zprods, h->d_specz, h->d_accz, h->d_uvents, h->d_uvfreqs};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->h_err) cudaFreeHost(h->h_err);
@@ -118,6 +120,11 @@ static gx_status setup(gx_handle *h)
   }
   if (s0.nbits != 1 && s0.nbits != 2 && s0.nbits != 4 && s0.nbits != 8)
     return h->fail(GX_ERR_UNSUPPORTED, "QUANTISATION BITS must be 1, 2, 4 or 8");
+  // phase centres: the result records of a baseline-freq are repeated for the
+  // most phase centres of any scan (configuration.cpp:2366-2373)
+  h->maxpc = 1;
+  if (h->model)
+    for (const auto &sc : h->model->scans) h->maxpc = std::max(h->maxpc, sc.numphasecentres);
   // the recorded freqs share bandwidth and channel count and come first in the
   // freq table: their spectra and accumulators are slabs [0, nfmain)
   const gx_freq_desc &f0 = d.freqs[s0.recfreq[0]];
@@ -253,8 +260,11 @@ static gx_status setup(gx_handle *h)
   if (d.xstep == GX_XSTEP_AUTO) {
     const char *e = getenv("GX_XSTEP_AUTO_MIN_INPUTS");
     const int nmin = e ? atoi(e) : 48;
-    h->xstep = (ni >= nmin && ni <= kTcInputs && J.nchan >= 2) ? GX_XSTEP_TC_FP16_HILO : GX_XSTEP_FP32;
+    h->xstep = (ni >= nmin && ni <= kTcInputs && J.nchan >= 2 && h->maxpc == 1) ? GX_XSTEP_TC_FP16_HILO
+                                                                                : GX_XSTEP_FP32;
   }
+  if (h->maxpc > 1 && h->xstep != GX_XSTEP_FP32)
+    return h->fail(GX_ERR_UNSUPPORTED, "multiple phase centres are implemented with the FP32 X-step only");
   h->tc = h->xstep != GX_XSTEP_FP32;
   h->hilo = h->xstep == GX_XSTEP_TC_FP16_HILO;
   if (h->tc) {
@@ -380,6 +390,8 @@ static gx_status setup(gx_handle *h)
         }
       }
   }
+  if (!h->zfreq.empty() && h->maxpc > 1)
+    return h->fail(GX_ERR_UNSUPPORTED, "zoom bands with multiple phase centres are not implemented");
   {
     int nzi = 0;
     for (int c : zcount) nzi = std::max(nzi, c);
@@ -495,9 +507,10 @@ static gx_status setup(gx_handle *h)
   // Core result layout for records of 1 / div of the channels: crosses by
   // freq and baseline, baseline weights, autocorrelations, their weights
   auto build = [&](int div, std::vector<int> &blofs, std::vector<int> &bwofs, std::vector<int> &acofs,
-                   std::vector<int> &acwofs) -> long long {
+                   std::vector<int> &acwofs, std::vector<int> &bsdofs) -> long long {
     blofs.assign(d.nfreqs * (nbl ? nbl : 1), -1);
     bwofs.assign(d.nfreqs * (nbl ? nbl : 1), -1);
+    bsdofs.assign(d.nfreqs * (nbl ? nbl : 1), -1);
     acofs.assign(d.nstations, 0);
     acwofs.assign(d.nstations, 0);
     long long idx = 0;
@@ -507,7 +520,7 @@ static gx_status setup(gx_handle *h)
         int lf = bl_localfreq(d.baselines[j], f);
         if (lf < 0) continue;
         blofs[f * nbl + j] = (int)idx;
-        idx += (long long)d.baselines[j].npolprod[lf] * (d.freqs[f].nchan / div);
+        idx += (long long)h->maxpc * d.baselines[j].npolprod[lf] * (d.freqs[f].nchan / div);
       }
     }
     for (int f = 0; f < d.nfreqs; f++) {
@@ -520,6 +533,15 @@ static gx_status setup(gx_handle *h)
         idx += np / 2 + np % 2;
       }
     }
+    if (h->maxpc > 1)   // shift decorrelation factors, one float per phase centre (configuration.cpp:2548-2566)
+      for (int f = 0; f < d.nfreqs; f++) {
+        if (!freq_used(f)) continue;
+        for (int j = 0; j < nbl; j++) {
+          if (bl_localfreq(d.baselines[j], f) < 0) continue;
+          bsdofs[f * nbl + j] = (int)idx;
+          idx += h->maxpc / 2 + h->maxpc % 2;
+        }
+      }
     for (int s = 0; s < d.nstations; s++) {
       acofs[s] = (int)idx;
       const gx_station_desc &x = d.stations[s];
@@ -537,8 +559,18 @@ static gx_status setup(gx_handle *h)
     return idx;
   };
   // the kernels fill the full-resolution array; the averaged one is the result
-  h->rl_full = build(1, h->blofs_full, h->bwofs_full, h->acofs_full, h->acwofs_full);
-  h->rl = build(avg, h->blofs, h->bwofs, h->acofs, h->acwofs);
+  h->rl_full = build(1, h->blofs_full, h->bwofs_full, h->acofs_full, h->acwofs_full, h->bsdofs_full);
+  h->rl = build(avg, h->blofs, h->bwofs, h->acofs, h->acwofs, h->bsdofs);
+  h->bsd_first = h->bsd_count = 0;
+  if (h->maxpc > 1) {
+    long long lo = -1, hi = -1;
+    for (int x : h->bsdofs_full)
+      if (x >= 0) {
+        lo = lo < 0 ? x : std::min<long long>(lo, x);
+        hi = std::max<long long>(hi, x + h->maxpc / 2 + h->maxpc % 2);
+      }
+    if (lo >= 0) { h->bsd_first = lo; h->bsd_count = hi - lo; }
+  }
   // phase-cal section: after the autocorrelation weights, datastream by datastream, band by band
   h->pc_off.assign((size_t)d.nstations * GX_MAX_BANDS, -1);
   h->pc_ntones.assign((size_t)d.nstations * GX_MAX_BANDS, 0);
@@ -564,10 +596,11 @@ static gx_status setup(gx_handle *h)
         const int lf = bl_localfreq(d.baselines[j], f);
         if (lf < 0 || h->blofs[f * nbl + j] < 0) continue;
         const int nf = d.freqs[f].nchan, np = d.baselines[j].npolprod[lf];
-        for (int p = 0; p < np; p++)
+        for (int p = 0; p < h->maxpc * np; p++)   // records of every phase centre
           add(h->blofs_full[f * nbl + j] + (long long)p * nf, h->blofs[f * nbl + j] + (long long)p * (nf / avg),
               nf / avg, avg);
         add(h->bwofs_full[f * nbl + j], h->bwofs[f * nbl + j], np / 2 + np % 2, 1);
+        if (h->maxpc > 1) add(h->bsdofs_full[f * nbl + j], h->bsdofs[f * nbl + j], h->maxpc / 2 + h->maxpc % 2, 1);
       }
     long long total_pc = 0;   // the phase-cal section follows the autocorrelation weights
     for (int q = 0; q < d.nstations; q++)
@@ -612,6 +645,7 @@ static gx_status setup(gx_handle *h)
     h->zprods.push_back(e);
   };
   h->prods.clear();
+  h->uvents.clear();
   h->tcprods.clear();
   h->wents.clear();
   h->pairs.clear();
@@ -666,6 +700,8 @@ static gx_status setup(gx_handle *h)
             return h->fail(GX_ERR_ARG, "baseline band index out of range");
           int a = h->band_input[B.ds1][b1], bb = h->band_input[B.ds2][b2];
           add_prod(h->blofs_full[f * nbl + j] + (long long)p * J.nchan, f, a, bb);
+          const ProdEntry &pe = h->prods.back();
+          h->uvents.push_back(UvEntry{pe.result_offset, pe.acc_index, pe.conj, j, f, B.npolprod[lf] * J.nchan});
           w.source = h->interlaced_any ? item(wrow(B.ds1, b1), wrow(B.ds2, b2)) : d.nstations + j;
         } else {
           // zoom bands: the products of their rows; weights of their parent
@@ -696,6 +732,8 @@ static gx_status setup(gx_handle *h)
       if (k < x.nbands) {
         const int a = h->band_input[s][k];
         add_prod(ro, f, a, a);
+        const ProdEntry &pe = h->prods.back();
+        h->uvents.push_back(UvEntry{pe.result_offset, pe.acc_index, pe.conj, -1, f, 0});
         w.source = item(wrow(s, k), -1);
       } else {
         const int zb = k - x.nbands;
@@ -716,8 +754,13 @@ static gx_status setup(gx_handle *h)
         w.source = partner < 0 ? -1 : x.interlaced ? item(wrow(s, i0), wrow(s, i1)) : s;
         h->wents.push_back(w);
         if (partner >= 0) {
-          if (k < x.nbands) add_prod(ro, f, h->band_input[s][k], h->band_input[s][partner]);
-          else add_zprod(ro, zord[f], zrow[s][k - x.nbands], zpartner[s][k - x.nbands]);
+          if (k < x.nbands) {
+            add_prod(ro, f, h->band_input[s][k], h->band_input[s][partner]);
+            const ProdEntry &pe = h->prods.back();
+            h->uvents.push_back(UvEntry{pe.result_offset, pe.acc_index, pe.conj, -1, f, 0});
+          } else {
+            add_zprod(ro, zord[f], zrow[s][k - x.nbands], zpartner[s][k - x.nbands]);
+          }
         }
         ro += d.freqs[f].nchan;
       }
@@ -739,6 +782,29 @@ static gx_status setup(gx_handle *h)
       r.end = (int)i;
       h->tcrows.push_back(r);
     }
+  }
+
+  // uv-shift intervals of multi-phase-centre scans (Core::processdata,
+  // core.cpp:768-776, 984-991): maxxcblocks blocks each, a multiple of the
+  // buffered FFTs, the last one what remains of the subint
+  h->uv_nint = 0;
+  h->uvfreqs.clear();
+  if (h->maxpc > 1) {
+    const int nbuf = h->meta ? h->meta->num_buffered_ffts : 1;
+    const double blockns = (double)d.subint_ns / (double)J.blocks_per_send;
+    for (const auto &sc : h->model->scans) {
+      if (sc.numphasecentres < 2) continue;
+      int M = (int)(sc.maxns_xc / blockns);
+      M -= M % nbuf;
+      if (M == 0) M = nbuf;
+      h->uv_nint = std::max(h->uv_nint, (J.blocks_per_send + M - 1) / M);
+    }
+    h->rsl = stride_length(h->xmac_stride);   // rotatestridelen = calcstridelength(xmacstridelen)
+    if (h->rsl < 1 || h->xmac_stride % h->rsl || J.nchan % h->xmac_stride)
+      return h->fail(GX_ERR_UNSUPPORTED, "rotate stride length does not divide the xmac stride");
+    for (int f = 0; f < d.nfreqs; f++)
+      h->uvfreqs.push_back(UvFreq{d.freqs[f].freq_mhz, d.freqs[f].bw_mhz / (double)d.freqs[f].nchan,
+                                  d.freqs[f].lower_sideband ? 1 : 0, d.freqs[f].nchan});
   }
 
   // chunking and K-split
@@ -929,6 +995,13 @@ static gx_status setup(gx_handle *h)
   if (!h->wents.empty())
     CKR(h, cudaMemcpy(h->d_went, h->wents.data(), sizeof(WeightEntry) * h->wents.size(), cudaMemcpyHostToDevice));
   CKR(h, h->dalloc(&h->d_results, sizeof(float2) * h->rl));
+  if (h->maxpc > 1) {
+    CKR(h, h->dalloc(&h->d_uvents, sizeof(UvEntry) * std::max<size_t>(1, h->uvents.size())));
+    if (!h->uvents.empty())
+      CKR(h, cudaMemcpy(h->d_uvents, h->uvents.data(), sizeof(UvEntry) * h->uvents.size(), cudaMemcpyHostToDevice));
+    CKR(h, h->dalloc(&h->d_uvfreqs, sizeof(UvFreq) * h->uvfreqs.size()));
+    CKR(h, cudaMemcpy(h->d_uvfreqs, h->uvfreqs.data(), sizeof(UvFreq) * h->uvfreqs.size(), cudaMemcpyHostToDevice));
+  }
   if (!h->pcal.empty()) {
     h->pcal_maxbins = 1;
     for (const PcalBand &P : h->pcal) h->pcal_maxbins = std::max(h->pcal_maxbins, P.nbins);
@@ -961,7 +1034,11 @@ static gx_status setup(gx_handle *h)
   h->o_ptr = h->o_len + sizeof(int64_t) * d.nstations;
   h->o_interp = h->o_ptr + sizeof(uint8_t *) * d.nstations;
   h->o_ctrl = h->o_interp + sizeof(double) * 3 * d.nstations;
-  h->sub_bytes = h->o_ctrl + sizeof(int32_t) * h->ctrlstride * d.nstations;
+  // multiple phase centres: the intervals' differential delays [interval][baseline][centre]
+  // (doubles) and the shift-decorrelation section of the result (floats)
+  h->o_uvdelay = (h->o_ctrl + sizeof(int32_t) * h->ctrlstride * d.nstations + 15) & ~(size_t)15;
+  h->o_bsd = h->o_uvdelay + sizeof(double) * (size_t)h->uv_nint * d.nbaselines * h->maxpc;
+  h->sub_bytes = h->o_bsd + sizeof(float2) * (size_t)h->bsd_count;
   CKR(h, h->dalloc(&h->d_sub, h->sub_bytes));
   for (int k = 0; k < gx_handle::kSlots; k++) {
     CKR(h, cudaMallocHost(&h->h_sub[k], h->sub_bytes));
@@ -1069,12 +1146,17 @@ const char *gx_status_string(gx_status s)
   return "unknown";
 }
 
-gx_status gx_open(const gx_job_desc *desc, int device, gx_handle **out)
+// A handle for desc; model and meta (from the .input job) are in place before
+// the setup, which takes the phase centres and uv-shift intervals from them.
+static gx_status open_handle(const gx_job_desc *desc, int device, std::unique_ptr<HostModel> model,
+                             std::unique_ptr<gx::JobMeta> meta, gx_handle **out)
 {
   if (!desc || !out) return GX_ERR_ARG;
   *out = nullptr;
   gx_handle *h = new gx_handle();
   h->device = device;
+  h->model = std::move(model);
+  h->meta = std::move(meta);
   h->jd = *desc;
   if (desc->stations && desc->nstations > 0) h->st.assign(desc->stations, desc->stations + desc->nstations);
   if (desc->freqs && desc->nfreqs > 0) h->fr.assign(desc->freqs, desc->freqs + desc->nfreqs);
@@ -1092,6 +1174,11 @@ gx_status gx_open(const gx_job_desc *desc, int device, gx_handle **out)
   }
   *out = h;
   return GX_OK;
+}
+
+gx_status gx_open(const gx_job_desc *desc, int device, gx_handle **out)
+{
+  return open_handle(desc, device, nullptr, nullptr, out);
 }
 
 gx_status gx_close(gx_handle *h)
@@ -1191,6 +1278,70 @@ static gx_status stage_subint(gx_handle *h, const gx_subint_desc *sub, const uin
       if (r != GX_OK) return h->fail(r, "no delay model for this subint");
     }
   }
+  h->cur_npc[k] = 1;
+  h->cur_M[k] = 0;
+  if (h->maxpc > 1) {
+    if (sub->scan < 0 || sub->scan >= (int)h->model->scans.size()) return h->fail(GX_ERR_MODEL, "scan out of range");
+    const auto &sc = h->model->scans[sub->scan];
+    float *bsd = reinterpret_cast<float *>(b + h->o_bsd);
+    memset(bsd, 0, sizeof(float2) * h->bsd_count);
+    if (sc.numphasecentres > 1) {
+      // per uv-shift interval (its centre and width, core.cpp:984-991, 1055-1057),
+      // baseline and phase centre: the differential delay and rate against the
+      // pointing centre (core.cpp:1641-1673), and the shift decorrelation
+      // sum nswidth * time-smearing * delay-window factor (core.cpp:1894-1923)
+      const int nph = sc.numphasecentres, bps = h->J.blocks_per_send, nbl = d.nbaselines;
+      const int nbuf = h->meta ? h->meta->num_buffered_ffts : 1;
+      const double blockns = (double)d.subint_ns / (double)bps;
+      int M = (int)(sc.maxns_xc / blockns);
+      M -= M % nbuf;
+      if (M == 0) M = nbuf;
+      double *uvd = reinterpret_cast<double *>(b + h->o_uvdelay);
+      const HostModel &mdl = *h->model;
+      for (int iv = 0; iv * M < bps; iv++) {
+        const int cnt = std::min(M, bps - iv * M);
+        const double nsoffset = (iv * M + ((double)cnt) / 2.0) * blockns, nswidth = cnt * blockns;
+        const double t = sub->sec + double(sub->ns + nsoffset) / 1000000000.0;
+        for (int j = 0; j < nbl; j++) {
+          const gx_baseline_desc &B = d.baselines[j];
+          const int a1 = mdl.station_of_datastream[B.ds1], a2 = mdl.station_of_datastream[B.ds2];
+          double pc1[2], pc2[2];
+          if (!mdl.linear(sub->scan, t, a1, 0, pc1) || !mdl.linear(sub->scan, t, a2, 0, pc2))
+            return h->fail(GX_ERR_MODEL, "no delay model for a uv-shift interval");
+          for (int ph = 0; ph < nph; ph++) {
+            double p1[2], p2[2];
+            if (!mdl.linear(sub->scan, t, a1, ph + 1, p1) || !mdl.linear(sub->scan, t, a2, ph + 1, p2))
+              return h->fail(GX_ERR_MODEL, "no delay model for a phase centre");
+            double ad1 = p1[1] - pc1[1], ad2 = p2[1] - pc2[1];
+            ad1 += ad1 * pc1[0];   // the geometric rate over the shifted sample range
+            ad2 += ad2 * pc2[0];
+            const double dd1 = ad2 - ad1;
+            const double dd0 = p2[0] + pc1[0] - (p1[0] + pc2[0]);
+            uvd[((size_t)iv * nbl + j) * h->maxpc + ph] = dd1;
+            for (int f = 0; f < d.nfreqs; f++) {
+              const int o = h->bsdofs_full[f * nbl + j];
+              if (o < 0) continue;
+              double timesmeardecorr = 1.0, delaydecorr = 1.0;
+              if (std::fabs(dd0) > 1e-18) {
+                const double maxphasechange = kTwoPi * dd0 * (nswidth / 1000.0) * d.freqs[f].freq_mhz;
+                timesmeardecorr = std::sin(maxphasechange / 2.0) / (maxphasechange / 2.0);
+                if (timesmeardecorr < 0.0) timesmeardecorr = 0;
+              }
+              if (std::fabs(dd1) > 1e-18) {
+                const double delaywindow = d.freqs[f].nchan / d.freqs[f].bw_mhz;   // max lag, plus and minus
+                delaydecorr = 1.0 - std::fabs(dd1 / delaywindow);
+                if (delaydecorr < 0.0) delaydecorr = 0;
+              }
+              float &acc = bsd[2 * (o - h->bsd_first) + ph];
+              acc += nswidth * timesmeardecorr * delaydecorr;
+            }
+          }
+        }
+      }
+      h->cur_npc[k] = nph;
+      h->cur_M[k] = M;
+    }
+  }
   return GX_OK;
 }
 
@@ -1240,8 +1391,11 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
   if (npc)
     CKR(h, cudaMemsetAsync(h->d_pcalbins, 0, sizeof(float2) * (size_t)h->pcal_chunks * npc * h->pcal_maxbins, st));
   gx_status r;
-  for (int b0 = 0; b0 < J.blocks_per_send; b0 += h->chunk) {
-    const int nb = std::min(h->chunk, J.blocks_per_send - b0);
+  // with channel averaging the finalise fills the full-resolution array first
+  float2 *fin = h->avg > 1 ? h->d_full : dev_results;
+  // one pass of nb blocks from block b0: F-step (and phase-cal bins), X-step, weights
+  auto pass = [&](int b0, int nb) -> gx_status {
+    gx_status r;
     if ((r = mark(0, true)) != GX_OK) return r;
     CKR(h, fstep_launch(J, h->d_st, h->maxnrf, S, b0, nb, h->nslots, h->d_spec, h->d_w, h->d_bp, st));
     if (npc) {
@@ -1265,21 +1419,52 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
     CKR(h, weights_launch(h->d_w, nb, d.nstations, h->d_pairs, npairs, h->d_wacc, st));
     if ((r = mark(1, false)) != GX_OK) return r;
     h->launches += 3;
+    return GX_OK;
+  };
+  const int nph = h->cur_npc[k];
+  if (nph > 1) {
+    // Multiple phase centres (Core::processdata / uvshiftAndAverage,
+    // core.cpp:984-991, 1431-1938): the accumulators of each uv-shift interval
+    // are rotated per phase centre and added into the result array, the
+    // autocorrelations added as they are
+    CKR(h, cudaMemsetAsync(fin, 0, sizeof(float2) * h->rl_full, st));
+    const int M = h->cur_M[k];
+    const double *uvd = reinterpret_cast<const double *>(h->d_sub + h->o_uvdelay);
+    for (int iv = 0; iv * M < J.blocks_per_send; iv++) {
+      const int i0 = iv * M, i1 = std::min(J.blocks_per_send, i0 + M);
+      if (iv > 0) CKR(h, cudaMemsetAsync(h->d_acc, 0, sizeof(float2) * h->acc_slice * h->ks, st));
+      for (int b0 = i0; b0 < i1; b0 += h->chunk)
+        if ((r = pass(b0, std::min(h->chunk, i1 - b0))) != GX_OK) return r;
+      if ((r = mark(2, true)) != GX_OK) return r;
+      CKR(h, uvshift_launch(h->d_uvents, (int)h->uvents.size(), h->d_acc, h->ks, h->acc_slice, J.nchan,
+                            uvd + (size_t)iv * nbl * h->maxpc, nph, h->maxpc, h->d_uvfreqs, h->rsl, fin, st));
+      if ((r = mark(2, false)) != GX_OK) return r;
+      h->launches += 1;
+    }
+  } else {
+    for (int b0 = 0; b0 < J.blocks_per_send; b0 += h->chunk)
+      if ((r = pass(b0, std::min(h->chunk, J.blocks_per_send - b0))) != GX_OK) return r;
   }
   if ((r = mark(2, true)) != GX_OK) return r;
-  // with channel averaging the finalise fills the full-resolution array first
-  float2 *fin = h->avg > 1 ? h->d_full : dev_results;
-  CKR(h, cudaMemsetAsync(fin, 0, sizeof(float2) * h->rl_full, st));
-  if (h->tc) {
+  if (nph > 1) {
+    // baseline and autocorrelation weights; the shift decorrelation factors
+    CKR(h, finalise_launch(nullptr, 0, h->d_acc, h->ks, h->acc_slice, J.nchan, h->d_went, (int)h->wents.size(),
+                           h->d_wacc, fin, st));
+    CKR(h, copy_floats_launch(reinterpret_cast<const float *>(h->d_sub + h->o_bsd), 2 * h->bsd_count,
+                              reinterpret_cast<float *>(fin), 2 * h->bsd_first, st));
+    h->launches += 2;
+  } else if (h->tc) {
+    CKR(h, cudaMemsetAsync(fin, 0, sizeof(float2) * h->rl_full, st));
     CKR(h, finalise_tc_launch(h->d_tcprods, h->d_tcrows, (int)h->tcrows.size(), acc4, h->nfmain, J.nchan,
                               J.ninputs, h->ks, fin, st));
     CKR(h, finalise_launch(nullptr, 0, h->d_acc, h->ks, h->acc_slice, J.nchan, h->d_went, (int)h->wents.size(),
                            h->d_wacc, fin, st));
   } else {
+    CKR(h, cudaMemsetAsync(fin, 0, sizeof(float2) * h->rl_full, st));
     CKR(h, finalise_launch(h->d_prods, (int)h->prods.size(), h->d_acc, h->ks, h->acc_slice, J.nchan, h->d_went,
                            (int)h->wents.size(), h->d_wacc, fin, st));
   }
-  h->launches += (h->prods.empty() ? 0 : 1) + (h->wents.empty() ? 0 : 1);
+  if (nph == 1) h->launches += (h->prods.empty() ? 0 : 1) + (h->wents.empty() ? 0 : 1);
   if (!h->zprods.empty()) {
     CKR(h, finalise_launch(h->d_zprods, (int)h->zprods.size(), h->d_accz, h->zks, h->zacc_slice, h->nzchan, nullptr,
                            0, nullptr, fin, st));
@@ -1498,13 +1683,8 @@ gx_status gx_open_input(const char *inputfile, int device, int xstep, gx_handle 
     return GX_ERR_IO;
   }
   job->desc.xstep = xstep;
-  gx_handle *h = nullptr;
-  gx_status s = gx_open(&job->desc, device, &h);
-  if (s != GX_OK) return s;
-  h->model = std::move(job->model);
-  h->meta.reset(new JobMeta(job->meta));
-  *out = h;
-  return GX_OK;
+  return open_handle(&job->desc, device, std::move(job->model),
+                     std::unique_ptr<gx::JobMeta>(new gx::JobMeta(job->meta)), out);
 }
 
 }  // extern "C"

@@ -52,6 +52,19 @@ struct gx_handle {
   std::vector<gx::ZoomRow> zrows;
   std::vector<gx::ProdEntry> zprods;
   size_t zacc_slice = 0;                     // float2 per zoom K-split slice
+  // Multiple phase centres (Core::uvshiftAndAverage, core.cpp:1431-1938): the
+  // subint runs in uv-shift intervals of blocks; after each, the FP32
+  // accumulators are rotated per phase centre and added into the results.
+  int maxpc = 1;                             // most phase centres of a scan: records per baseline-freq
+  std::vector<gx::UvEntry> uvents;
+  std::vector<gx::UvFreq> uvfreqs;
+  gx::UvEntry *d_uvents = nullptr;
+  gx::UvFreq *d_uvfreqs = nullptr;
+  int uv_nint = 0, rsl = 1;                  // intervals per subint at most; rotate stride length
+  std::vector<int> bsdofs, bsdofs_full;      // [freq * nbaselines + baseline] shift-decorrelation offsets
+  long long bsd_first = 0, bsd_count = 0;    // complex-float range of that section (full layout)
+  size_t o_uvdelay = 0, o_bsd = 0;           // in the per-subint table block
+  int cur_npc[2] = {1, 1}, cur_M[2] = {0, 0};   // per slot: phase centres of the staged subint's scan, interval blocks
   std::vector<std::vector<int>> zparent;     // [station][zoom band] parent recorded band
   std::vector<std::vector<int>> acbands;     // [station] total bands (recorded, then zoom) with autocorrelations
   gx::ZoomRow *d_zrows = nullptr;

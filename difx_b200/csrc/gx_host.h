@@ -15,6 +15,8 @@ struct ModelScan {
   int nsamples = 0;
   int polystartmjd = 0, polystartseconds = 0;
   int phase_centre_source = 0;   // .calc SCAN n PHS CTR 0: source table index of the phase centre
+  int maxns_xc = 0;              // SCAN n UVSHIFT INTERVAL (NS): cross-correlation shift/average time
+  int pointing_source = 0;       // SCAN n POINTING SRC
   // delay[sample][source][station][order+1], us; source 0 = pointing centre
   std::vector<double> delay;
   std::vector<double> u, v, w;   // same indexing, metres
@@ -40,6 +42,10 @@ class HostModel {
     return sc.delay[(((size_t)sample * (sc.numphasecentres + 1) + src) * nstations + ant) * (polyorder + 1) + l];
   }
   gx_status interpolator(int datastream, int scan, int sec, int ns, double out[3]) const;
+  // Model::calculateDelayInterpolator of order 1 over 1 us with one increment
+  // (the uv-shift's delay and rate of model antenna ant, source src of the
+  // scan's table, at offsettime seconds after the scan start; core.cpp:1652-1657)
+  bool linear(int scan, double offsettime, int ant, int src, double out[2]) const;
   double scan_start_sec(int scan) const;
   // Model::interpolateUVW (model.cpp:177-217): baseline (u, v, w) of model
   // antennas ant1 - ant2 at offsettime seconds after the scan start, source
@@ -54,6 +60,7 @@ struct JobMeta {
   std::vector<int> telescope;          // TELESCOPE INDEX per datastream
   std::vector<double> tsys;            // TSYS per datastream
   std::vector<std::string> telescope_name;   // TELESCOPE NAME per telescope
+  int num_buffered_ffts = 1;           // NUM BUFFERED FFTS
 };
 
 struct InputJob {

@@ -178,6 +178,36 @@ bool HostModel::uvw(int scanindex, double offsettime, int ant1, int ant2, int sr
   return true;
 }
 
+bool HostModel::linear(int scanindex, double offsettime, int ant, int src, double out[2]) const
+{
+  if (scanindex < 0 || scanindex >= (int)scans.size()) return false;
+  const ModelScan &sc = scans[scanindex];
+  if (ant < 0 || ant >= nstations || src < 0 || src > sc.numphasecentres) return false;
+  const double timespan = 0.000001;
+  // Model::calculateDelayInterpolator, order 1 (model.cpp:232-281)
+  const int polyoffset = (modelmjd - sc.polystartmjd) * 86400 + modelstartseconds + sc.offsetseconds - sc.polystartseconds;
+  int scansample = int((offsettime + polyoffset) / double(modelincsecs));
+  if (scansample == sc.nsamples && ((offsettime + polyoffset - scansample * modelincsecs) < 1e-6)) scansample--;
+  if (scansample < 0 || scansample >= sc.nsamples) return false;
+  double tp[16];
+  double samples[3];
+  // the block-centre sample first, then the start and the end, as the reference forms them
+  const double deltas[3] = {offsettime + polyoffset - scansample * modelincsecs,
+                            offsettime + polyoffset + timespan / 2.0 - scansample * modelincsecs,
+                            offsettime + polyoffset + timespan - scansample * modelincsecs};
+  for (int q = 0; q < 3; q++) {
+    tp[0] = 1.0;
+    for (int i = 0; i < polyorder; i++) tp[i + 1] = tp[i] * deltas[q];
+    double acc = 0;
+    for (int i = 0; i < polyorder + 1; i++) acc += tp[i] * delay_at(sc, scansample, src, ant, i);
+    samples[q] = acc;
+  }
+  const int numincrements = 1;
+  out[0] = (samples[2] - samples[0]) / numincrements;
+  out[1] = samples[0] + (samples[1] - (out[0] * numincrements / 2.0 + samples[0])) / 3.0;
+  return true;
+}
+
 gx_status HostModel::interpolator(int ds, int scanindex, int sec, int ns, double out[3]) const
 {
   if (scanindex < 0 || scanindex >= (int)scans.size()) return GX_ERR_MODEL;
@@ -244,7 +274,7 @@ InputJob *read_input_job(const char *inputfile, std::string &err)
   NEED(in, "FRINGE ROTN ORDER", v); d.fringe_rotation_order = atoi(v.c_str());
   NEED(in, "ARRAY STRIDE LEN", v); d.array_stride = atoi(v.c_str());
   NEED(in, "XMAC STRIDE LEN", v); d.xmac_stride = atoi(v.c_str());
-  NEED(in, "NUM BUFFERED FFTS", v);
+  NEED(in, "NUM BUFFERED FFTS", v); job->meta.num_buffered_ffts = std::max(1, atoi(v.c_str()));
   NEED(in, "WRITE AUTOCORRS", v); d.write_autocorrs = truthy(v) ? 1 : 0;
   NEED(in, "PULSAR BINNING", v);
   if (truthy(v)) { err = "pulsar binning is not implemented"; return nullptr; }
@@ -498,8 +528,13 @@ InputJob *read_input_job(const char *inputfile, std::string &err)
     std::string pre = "SCAN " + std::to_string(i) + " ";
     if (!cget(pre + "START (S)", v)) return nullptr; m->scans[i].offsetseconds = atoi(v.c_str());
     if (!cget(pre + "DUR (S)", v)) return nullptr; m->scans[i].durationseconds = atoi(v.c_str());
+    if (!cget(pre + "UVSHIFT INTERVAL (NS)", v)) return nullptr; m->scans[i].maxns_xc = atoi(v.c_str());
+    if (!cget(pre + "POINTING SRC", v)) return nullptr; m->scans[i].pointing_source = atoi(v.c_str());
     if (!cget(pre + "NUM PHS CTRS", v)) return nullptr; m->scans[i].numphasecentres = atoi(v.c_str());
-    if (m->scans[i].numphasecentres != 1) { err = "multiple phase centres are not implemented"; return nullptr; }
+    if (m->scans[i].numphasecentres < 1 || m->scans[i].numphasecentres > 64) {
+      err = "NUM PHS CTRS out of range";
+      return nullptr;
+    }
     if (!cget(pre + "PHS CTR 0", v)) return nullptr; m->scans[i].phase_centre_source = atoi(v.c_str());
   }
   if (!cget("NUM SPACECRAFT", v)) return nullptr;

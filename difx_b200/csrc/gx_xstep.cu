@@ -15,11 +15,13 @@
 // Accumulators: acc[ks][freq][stpair][ST][ST][N] (float2), summed over the
 // chunk passes of a subint; finalise_kernel maps them to the Core result
 // layout (configuration.cpp:2348-2630) and sums the K-split slices.
+#include <algorithm>
 #include <cstdint>
 #include <cstdlib>
 #include "gx_dev.h"
 #include "gx_xstep.h"
 #include "gx_mbar.cuh"
+#include "gx_fcommon.cuh"
 
 namespace gx {
 
@@ -316,6 +318,79 @@ cudaError_t zoom_gather_launch(const ZoomRow *rows, int nrows, const float2 *spe
   if (nrows > 65535 || nblk > 65535) return cudaErrorInvalidConfiguration;
   dim3 grid((Nz + 127) / 128, nrows, nblk);
   zoom_gather_kernel<<<grid, 128, 0, st>>>(rows, spec, NIm, Nm, specz, NIz, Nz, nblk);
+  return cudaGetLastError();
+}
+
+// One interval of a multi-phase-centre subint: each thread one channel of
+// one product row.  The rotator of channel c is the reference's two-level
+// one: sub[c mod rsl] (band-edge turns included) times step[c / rsl], FP64
+// turns, FP32 arguments and sincos, FP32 products in the reference's order.
+__global__ void uvshift_kernel(const UvEntry *__restrict__ ents, const float2 *__restrict__ acc, int ks,
+                               size_t ks_stride, int N, const double *__restrict__ delays, int npc, int maxpc,
+                               const UvFreq *__restrict__ freqs, int rsl, float2 *__restrict__ results)
+{
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= N) return;
+  const UvEntry e = ents[blockIdx.y];
+  float2 v = make_float2(0.f, 0.f);
+  for (int k = 0; k < ks; k++) {
+    const float2 a = acc[(size_t)k * ks_stride + e.acc_index + c];
+    v.x += a.x;
+    v.y += a.y;
+  }
+  if (e.conj) v.y = -v.y;
+  if (e.stride == 0) {
+    float2 &r = results[e.ro + c];
+    r.x += v.x;
+    r.y += v.y;
+    return;
+  }
+  const UvFreq F = freqs[e.freq];
+  const double stepbw = rsl * F.chanbw;
+  const int cr = c % rsl, cs = c / rsl, nsteps = F.nchan / rsl;
+  const double f1 = F.lsb ? -(double)(rsl - (cr + 1)) * F.chanbw : cr * F.chanbw;
+  const double f2 = F.lsb ? -(double)(nsteps - (cs + 1)) * stepbw : cs * stepbw;
+  for (int s = 0; s < npc; s++) {
+    const double d = delays[(size_t)e.baseline * maxpc + s];
+    float2 out = v;
+    if (fabs(d) > 1.0e-20) {
+      double edgeturns = d * F.lofreq;
+      edgeturns -= floor(edgeturns);
+      const double t1 = d * f1 + edgeturns, t2 = d * f2;
+      const float a1 = (float)((t1 - floor(t1)) * GX_TWO_PI), a2 = (float)((t2 - floor(t2)) * GX_TWO_PI);
+      float s1, c1, s2, c2;
+      sincosf(a1, &s1, &c1);
+      sincosf(a2, &s2, &c2);
+      out = cmul_exact(make_float2(c1, s1), v);      // rotator x data
+      out = cmul_exact(out, make_float2(c2, s2));    // times the step rotator
+    }
+    float2 &r = results[e.ro + (size_t)s * e.stride + c];
+    r.x += out.x;
+    r.y += out.y;
+  }
+}
+
+cudaError_t uvshift_launch(const UvEntry *ents, int nents, const float2 *acc, int ks, size_t ks_stride, int N,
+                           const double *delays, int npc, int maxpc, const UvFreq *freqs, int rsl, float2 *results,
+                           cudaStream_t st)
+{
+  if (nents <= 0) return cudaSuccess;
+  if (nents > 65535) return cudaErrorInvalidConfiguration;
+  dim3 grid((N + 127) / 128, nents);
+  uvshift_kernel<<<grid, 128, 0, st>>>(ents, acc, ks, ks_stride, N, delays, npc, maxpc, freqs, rsl, results);
+  return cudaGetLastError();
+}
+
+__global__ void copy_floats_kernel(const float *__restrict__ vals, long long n, float *__restrict__ out)
+{
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = vals[i];
+}
+
+cudaError_t copy_floats_launch(const float *vals, long long n, float *results_f, long long first, cudaStream_t st)
+{
+  if (n <= 0) return cudaSuccess;
+  copy_floats_kernel<<<(unsigned)std::min<long long>((n + 255) / 256, 1024), 256, 0, st>>>(vals, n, results_f + first);
   return cudaGetLastError();
 }
 

@@ -77,6 +77,32 @@ struct ZoomRow {
 cudaError_t zoom_gather_launch(const ZoomRow *rows, int nrows, const float2 *spec, int NIm, int Nm, float2 *specz,
                                int NIz, int Nz, int nblk, cudaStream_t st);
 
+// Multiple phase centres (Core::uvshiftAndAverageBaselineFreq,
+// core.cpp:1605-1938): one product row of the FP32 accumulators.  A cross
+// product (stride > 0) is rotated by each phase centre's differential delay
+// and added at result offset ro + s * stride; an autocorrelation (stride 0)
+// is added once.
+struct UvEntry {
+  long long ro;          // result offset of phase centre 0
+  long long acc_index;   // accumulator index (ks = 0 slice)
+  int conj;
+  int baseline, freq;
+  int stride;            // complex floats between phase centres' records; 0: autocorrelation
+};
+// Per freq: band edge (MHz), channel width (MHz), sideband, channels.
+struct UvFreq {
+  double lofreq, chanbw;
+  int lsb, nchan;
+};
+// Adds one interval's accumulators into the result array.  delays[bl][s]
+// (us): the differential delay of phase centre s on baseline bl; rsl: the
+// rotate stride length (the two-level rotator of core.cpp:1690-1766).
+cudaError_t uvshift_launch(const UvEntry *ents, int nents, const float2 *acc, int ks, size_t ks_stride, int N,
+                           const double *delays, int npc, int maxpc, const UvFreq *freqs, int rsl, float2 *results,
+                           cudaStream_t st);
+// results_f[first + i] = vals[i], i < n (floats)
+cudaError_t copy_floats_launch(const float *vals, long long n, float *results_f, long long first, cudaStream_t st);
+
 struct AvgEntry {
   long long src, dst;
   int n, L;

@@ -91,6 +91,13 @@ class JobSpec:
     zooms: Sequence[Subband] = ()
     zoom_only: bool = False           # baselines correlate the zoom freqs only
     zoom_pols: Tuple[str, ...] = ()   # polarisations of the zoom bands (default: pols)
+    # phase centres: with more than one, source 0 is the (uncorrelated)
+    # pointing centre and sources 1..n the phase centres, each with a seeded
+    # delay offset of up to max_pc_offset_us and rate of up to
+    # max_pc_rate_us_per_s relative to the pointing centre
+    phase_centres: int = 1
+    max_pc_offset_us: float = 0.02
+    max_pc_rate_us_per_s: float = 0.002
 
     # ------------------------------------------------------------ derived
     def station_sb(self, station: int) -> List[int]:
@@ -215,6 +222,17 @@ class JobSpec:
             c0 = rng.uniform(-1, 1) * (self.max_delay_us - abs(c1) * span - abs(c2) * span * span)
             c[s] = (c0, c1, c2)
         return c
+
+
+def phase_centre_offsets(spec: JobSpec) -> np.ndarray:
+    """Per phase centre and station (offset us, rate us/s) added to the
+    pointing centre's delay model."""
+    rng = np.random.default_rng(spec.seed * 31337 + 5)
+    out = np.zeros((max(1, spec.phase_centres), spec.nstations, 2))
+    if spec.phase_centres > 1:
+        out[..., 0] = rng.uniform(-1, 1, out.shape[:2]) * spec.max_pc_offset_us
+        out[..., 1] = rng.uniform(-1, 1, out.shape[:2]) * spec.max_pc_rate_us_per_s
+    return out
 
 
 def uvw_poly_rows(spec: JobSpec, nsamp: int) -> np.ndarray:
@@ -493,12 +511,15 @@ def write_job(spec: JobSpec, outdir: str) -> dict:
         C.append(_kv(f"TELESCOPE {i} Y (m)", f"{xyz[1]:.6f}"))
         C.append(_kv(f"TELESCOPE {i} Z (m)", f"{xyz[2]:.6f}"))
         C.append(_kv(f"TELESCOPE {i} SHELF", "NONE"))
-    C.append(_kv("NUM SOURCES", 1))
-    C.append(_kv("SOURCE 0 NAME", "SYNTH"))
-    C.append(_kv("SOURCE 0 RA", " 1.0000000000000000"))
-    C.append(_kv("SOURCE 0 DEC", " 0.5000000000000000"))
-    C.append(_kv("SOURCE 0 CALCODE", " "))
-    C.append(_kv("SOURCE 0 QUAL", 0))
+    npc = max(1, spec.phase_centres)
+    srcnames = ["SYNTH"] + ([f"PC{j}" for j in range(npc)] if npc > 1 else [])
+    C.append(_kv("NUM SOURCES", len(srcnames)))
+    for j, nm in enumerate(srcnames):
+        C.append(_kv(f"SOURCE {j} NAME", nm))
+        C.append(_kv(f"SOURCE {j} RA", f" {1.0 + 1e-5 * j:.16f}"))
+        C.append(_kv(f"SOURCE {j} DEC", f" {0.5 + 1e-5 * j:.16f}"))
+        C.append(_kv(f"SOURCE {j} CALCODE", " "))
+        C.append(_kv(f"SOURCE {j} QUAL", 0))
     C.append(_kv("NUM SCANS", 1))
     C.append(_kv("SCAN 0 IDENTIFIER", "SCAN0"))
     C.append(_kv("SCAN 0 START (S)", 0))
@@ -507,8 +528,9 @@ def write_job(spec: JobSpec, outdir: str) -> dict:
     C.append(_kv("SCAN 0 UVSHIFT INTERVAL (NS)", spec.uvshift_interval_ns))
     C.append(_kv("SCAN 0 AC AVG INTERVAL (NS)", spec.ac_avg_interval_ns))
     C.append(_kv("SCAN 0 POINTING SRC", 0))
-    C.append(_kv("SCAN 0 NUM PHS CTRS", 1))
-    C.append(_kv("SCAN 0 PHS CTR 0", 0))
+    C.append(_kv("SCAN 0 NUM PHS CTRS", npc))
+    for j in range(npc):
+        C.append(_kv(f"SCAN 0 PHS CTR {j}", j + 1 if npc > 1 else 0))
     C.append(_kv("NUM EOPS", 0))
     C.append(_kv("NUM SPACECRAFT", 0))
     C.append(_kv("IM FILENAME", paths["im"]))
@@ -537,17 +559,23 @@ def write_job(spec: JobSpec, outdir: str) -> dict:
         I.append(_kv(f"TELESCOPE {i} NAME", names[i]))
     I.append(_kv("NUM SCANS", 1))
     I.append(_kv("SCAN 0 POINTING SRC", "SYNTH"))
-    I.append(_kv("SCAN 0 NUM PHS CTRS", 1))
-    I.append(_kv("SCAN 0 PHS CTR 0 SRC", "SYNTH"))
+    I.append(_kv("SCAN 0 NUM PHS CTRS", npc))
+    for j in range(npc):
+        I.append(_kv(f"SCAN 0 PHS CTR {j} SRC", srcnames[j + 1] if npc > 1 else "SYNTH"))
     I.append(_kv("SCAN 0 NUM POLY", nsamp))
     uvw = uvw_poly_rows(spec, nsamp)
     for k in range(nsamp):
         t = spec.start_seconds + k * spec.poly_interval_s
         I.append(_kv(f"SCAN 0 POLY {k} MJD", spec.start_mjd + t // 86400))
         I.append(_kv(f"SCAN 0 POLY {k} SEC", t % 86400))
-        for src in range(2):
+        pco = phase_centre_offsets(spec)
+        for src in range(npc + 1):
             for s in range(nst):
-                vals = "\t ".join(f"{v:.16e}" for v in rows[k, s])
+                row = rows[k, s].copy()
+                if npc > 1 and src > 0:   # phase centre src: offset + rate (t from the poly start)
+                    row[0] += pco[src - 1, s, 0] + pco[src - 1, s, 1] * k * spec.poly_interval_s
+                    row[1] += pco[src - 1, s, 1]
+                vals = "\t ".join(f"{v:.16e}" for v in row)
                 I.append(_kv(f"SRC {src} ANT {s} DELAY (us)", vals))
                 for c, name in enumerate("UVW"):
                     I.append(_kv(f"SRC {src} ANT {s} {name} (m)", "\t ".join(f"{v:.16e}" for v in uvw[k, s, c])))
