@@ -17,6 +17,7 @@ struct ModelScan {
   int phase_centre_source = 0;   // .calc SCAN n PHS CTR 0: source table index of the phase centre
   int maxns_xc = 0;              // SCAN n UVSHIFT INTERVAL (NS): cross-correlation shift/average time
   int pointing_source = 0;       // SCAN n POINTING SRC
+  std::vector<int> phase_centre_sources;   // SCAN n PHS CTR j: source table index of phase centre j
   // delay[sample][source][station][order+1], us; source 0 = pointing centre
   std::vector<double> delay;
   std::vector<double> u, v, w;   // same indexing, metres

@@ -535,7 +535,11 @@ InputJob *read_input_job(const char *inputfile, std::string &err)
       err = "NUM PHS CTRS out of range";
       return nullptr;
     }
-    if (!cget(pre + "PHS CTR 0", v)) return nullptr; m->scans[i].phase_centre_source = atoi(v.c_str());
+    for (int j = 0; j < m->scans[i].numphasecentres; j++) {
+      if (!cget(pre + "PHS CTR " + std::to_string(j), v)) return nullptr;
+      m->scans[i].phase_centre_sources.push_back(atoi(v.c_str()));
+    }
+    m->scans[i].phase_centre_source = m->scans[i].phase_centre_sources[0];
   }
   if (!cget("NUM SPACECRAFT", v)) return nullptr;
   if (atoi(v.c_str()) != 0) { err = "spacecraft models are not implemented"; return nullptr; }

@@ -108,8 +108,6 @@ gx_status gx_vis_open(gx_handle *h, const char *outdir, gx_vis **out)
   *out = nullptr;
   if (h->device < 0) return h->fail(GX_ERR_STATE, "host-only handle (opened with device -1)");
   if (!h->model || !h->meta) return h->fail(GX_ERR_STATE, "the visibility writer needs a handle opened with gx_open_input");
-  if (h->maxpc > 1)   // records per phase centre go to files of their own (visibility.cpp:1056-1091)
-    return h->fail(GX_ERR_UNSUPPORTED, "the visibility writer does not implement multiple phase centres");
   if (!h->zfreq.empty() && h->meta)
     for (double t : h->meta->tsys)   // Configuration::getDMatchingBand reads zoom bands out of range
       if (t > 0.0) return h->fail(GX_ERR_UNSUPPORTED, "a-priori calibration (TSYS > 0) of zoom bands is not implemented");
@@ -120,7 +118,7 @@ gx_status gx_vis_open(gx_handle *h, const char *outdir, gx_vis **out)
   const gx_job_desc &d = h->jd;
   int nrec = 0;
   for (int i = 0; i < d.nbaselines; i++)
-    for (int k = 0; k < d.baselines[i].nfreqs; k++) nrec += d.baselines[i].npolprod[k];
+    for (int k = 0; k < d.baselines[i].nfreqs; k++) nrec += h->maxpc * d.baselines[i].npolprod[k];
   for (int s = 0; s < d.nstations; s++) nrec += 2 * (d.stations[s].nbands + d.stations[s].nzoombands);
   v->maxrec = nrec > 0 ? nrec : 1;
   CKR(h, cudaSetDevice(h->device));
@@ -179,6 +177,8 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
     long long bw0 = h->rl, bw1 = 0, aw0 = h->rl;
     for (int x : h->bwofs)
       if (x >= 0) bw0 = std::min<long long>(bw0, x), bw1 = std::max<long long>(bw1, x + 2);
+    for (int x : h->bsdofs)   // and the shift decorrelation factors that follow them
+      if (x >= 0) bw1 = std::max<long long>(bw1, x + h->maxpc / 2 + h->maxpc % 2);
     for (int x : h->acwofs) aw0 = std::min<long long>(aw0, x);
     // TSYS > 0: the autocorrelations too (their band means calibrate, visibility.cpp:463-484)
     for (double t : M.tsys)
@@ -257,21 +257,34 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
     double uvw[3];
     long long offset;
     int nchan;
+    int file;     // phase centre: output file DIFX_..s<file>.b0000
+    int source;   // source table index in the header
   };
   std::vector<Rec> recs;
   std::vector<VisScale> scales;
-  const int srcindex = model.scans[scan].phase_centre_source;
+  const ModelScan &scn = model.scans[scan];
+  const int nph = scn.numphasecentres;
+  // shift decorrelation factor of phase centre ph: the interval sums over the
+  // integration's nanoseconds, in FP32 (visibility.cpp:428-441)
+  auto shiftdecorr = [&](int f, int i, int ph) {
+    return (float)(fr[2LL * h->bsdofs[f * nbl + i] + ph] / (1000000000.0 * M.int_time));
+  };
   const double scanoffset = sec + ((double)ns) / 1e9 + M.int_time / 2.0;
   for (int i = 0; i < nbl; i++) {
     const gx_baseline_desc &B = d.baselines[i];
-    Rec r{};
-    r.baseline = (M.telescope[B.ds1] + 1) * 256 + (M.telescope[B.ds2] + 1);
-    if (!model.uvw(scan, scanoffset, model.station_of_datastream[B.ds1], model.station_of_datastream[B.ds2], 1, r.uvw))
-      return h->fail(GX_ERR_MODEL, "no (u, v, w) model for this integration");
     for (int f = 0; f < d.nfreqs; f++) {
       const int lf = gx_bl_localfreq(B, f);
       if (lf < 0) continue;
       const int N = nout(f);
+      for (int ph = 0; ph < nph; ph++) {   // records of every phase centre, each to its own file
+      Rec r{};
+      r.baseline = (M.telescope[B.ds1] + 1) * 256 + (M.telescope[B.ds2] + 1);
+      r.file = ph;
+      r.source = scn.phase_centre_sources[ph];
+      if (!model.uvw(scan, scanoffset, model.station_of_datastream[B.ds1], model.station_of_datastream[B.ds2], ph + 1,
+                     r.uvw))
+        return h->fail(GX_ERR_MODEL, "no (u, v, w) model for this integration");
+      const long long base = h->blofs[f * nbl + i] + (long long)ph * B.npolprod[lf] * N;
       for (int k = 0; k < B.npolprod[lf]; k++) {
         float w, scale;
         weight_and_scale(2LL * h->bwofs[f * nbl + i] + k, f, w, scale);
@@ -286,16 +299,22 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
           scale = (divisor > 0.0f && w > 0.0f)
                       ? (float)(std::sqrt(tsys(B.ds1) * tsys(B.ds2) / divisor) / w) : 0.0f;
         }
-        if (scale > 0.0f) scales.push_back(VisScale{h->blofs[f * nbl + i] + (long long)k * N, scale, N});
+        float sd = 1.0f;
+        if (nph > 1) {   // further scaled by the decorrelation of the uv shift (visibility.cpp:554-557)
+          sd = shiftdecorr(f, i, ph);
+          scale /= sd;
+        }
+        if (scale > 0.0f) scales.push_back(VisScale{base + (long long)k * N, scale, N});
         if (w > 0.0f) {
           r.freq = f;
           r.pol[0] = total_pol(d.stations[B.ds1], B.band1[lf][k]);
           r.pol[1] = total_pol(d.stations[B.ds2], B.band2[lf][k]);
-          r.weight = w;
-          r.offset = h->blofs[f * nbl + i] + (long long)k * N;
+          r.weight = nph > 1 ? w * sd : w;   // the weight times the decorrelation (visibility.cpp:869-872)
+          r.offset = base + (long long)k * N;
           r.nchan = N;
           recs.push_back(r);
         }
+      }
       }
     }
   }
@@ -321,6 +340,8 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
           if (w > 0.0f) {
             Rec r{};
             r.baseline = 257 * (M.telescope[s] + 1);
+            r.file = 0;   // the autocorrelations follow the first file's crosses (visibility.cpp:895-948)
+            r.source = nph == 1 ? scn.phase_centre_sources[0] : scn.pointing_source;
             r.freq = f;
             r.pol[0] = total_pol(x, b);
             r.pol[1] = j == 0 ? r.pol[0] : opposite_pol(r.pol[0]);
@@ -351,20 +372,22 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
   const int intsec = M.start_seconds + scanstart + sec;
   const int dumpmjd = M.start_mjd + intsec / 86400;
   const double dumpseconds = double(intsec % 86400) + ((double)ns) / 1000000000.0 + M.int_time / 2.0;
-  std::vector<char> buf;
+  // one file per phase centre (flushBuffersToDisk, visibility.cpp:1056-1091)
+  std::vector<std::vector<char>> bufs(nph);
   {
-    size_t bytes = 0;
-    for (const Rec &r : recs) bytes += 74 + sizeof(float2) * (size_t)r.nchan;
-    buf.reserve(bytes);
+    std::vector<size_t> bytes(nph, 0);
+    for (const Rec &r : recs) bytes[r.file] += 74 + sizeof(float2) * (size_t)r.nchan;
+    for (int q = 0; q < nph; q++) bufs[q].reserve(bytes[q]);
   }
   for (const Rec &r : recs) {
+    std::vector<char> &buf = bufs[r.file];
     put(buf, (uint32_t)0xFF00FF00u);   // sync word
     put(buf, (int32_t)1);              // binary header version
     put(buf, (int32_t)r.baseline);
     put(buf, (int32_t)dumpmjd);
     put(buf, dumpseconds);
     put(buf, (int32_t)0);              // configuration index
-    put(buf, (int32_t)srcindex);
+    put(buf, (int32_t)r.source);
     put(buf, (int32_t)r.freq);
     buf.push_back(r.pol[0]);
     buf.push_back(r.pol[1]);
@@ -376,13 +399,15 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
     const char *p = reinterpret_cast<const char *>(v->h_buf + r.offset);
     buf.insert(buf.end(), p, p + sizeof(float2) * (size_t)r.nchan);
   }
-  char name[64];
-  snprintf(name, sizeof(name), "/DIFX_%05d_%06d.s%04d.b%04d", M.start_mjd, M.start_seconds, 0, 0);
-  std::ofstream of(v->outdir + name, std::ios::app | std::ios::binary);
-  if (!of) return h->fail(GX_ERR_IO, "cannot open " + v->outdir + name);
-  of.write(buf.data(), (std::streamsize)buf.size());
-  of.close();
-  if (!of) return h->fail(GX_ERR_IO, "write failed: " + v->outdir + name);
+  for (int q = 0; q < nph; q++) {
+    char name[64];
+    snprintf(name, sizeof(name), "/DIFX_%05d_%06d.s%04d.b%04d", M.start_mjd, M.start_seconds, q, 0);
+    std::ofstream of(v->outdir + name, std::ios::app | std::ios::binary);
+    if (!of) return h->fail(GX_ERR_IO, "cannot open " + v->outdir + name);
+    of.write(bufs[q].data(), (std::streamsize)bufs[q].size());
+    of.close();
+    if (!of) return h->fail(GX_ERR_IO, "write failed: " + v->outdir + name);
+  }
 
   // phase-cal lines (writedata, visibility.cpp:650-675 and 985-1053): each band's
   // tones scaled as its parallel-hand autocorrelation, one line per datastream

@@ -36,7 +36,17 @@ CASES = {
     "zoom_shifted": lambda: _zoom("shifted"),
     "zoom_mixed": lambda: _zoom("mixed"),
     "zoom_avg": lambda: _zoom("avg"),
+    # multiple phase centres: one file per centre, weights times the shift
+    # decorrelation, scales divided by it (visibility.cpp:428-441, 554-557, 860-890)
+    "pc3": lambda: _pc("pc3"),
+    "pc2_avg": lambda: _pc("pc2_avg"),
 }
+
+
+def _pc(name):
+    from dataclasses import replace
+    from tests.test_phase_centres import _case
+    return replace(_case(name), name="gvispc_" + name, int_time=0.016)
 
 
 def _zoom(name):
@@ -88,12 +98,18 @@ def test_gx_vis_bytes_match_reference_visibility(case, tmp_path):
     theirs = str(tmp_path / "ref.difx")
     s0 = prep.subs[0]
     ref.vis_write(host, s0.scan, s0.sec, s0.ns, theirs)
-    a = np.fromfile(_file(ours), np.uint8)
-    b = np.fromfile(_file(theirs), np.uint8)
-    assert a.size == b.size, (a.size, b.size)
-    assert np.array_equal(a, b)
+    fa = sorted(f for f in os.listdir(ours) if f.startswith("DIFX_"))
+    fb = sorted(f for f in os.listdir(theirs) if f.startswith("DIFX_"))
+    assert fa == fb and len(fa) == max(1, spec.phase_centres), (fa, fb)
     freqs = list(spec.subbands) + list(spec.zooms)
-    assert len(swin.read_records(_file(ours), lambda f: freqs[f].nchan // spec.chans_to_avg)) == n
+    nrec = 0
+    for f in fa:
+        a = np.fromfile(os.path.join(ours, f), np.uint8)
+        b = np.fromfile(os.path.join(theirs, f), np.uint8)
+        assert a.size == b.size, (f, a.size, b.size)
+        assert np.array_equal(a, b), f
+        nrec += len(swin.read_records(os.path.join(ours, f), lambda q: freqs[q].nchan // spec.chans_to_avg))
+    assert nrec == n
 
 
 def test_gx_vis_end_to_end_matches_reference(tmp_path):
