@@ -16,6 +16,7 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <type_traits>
 #include <vector>
 #include <cuda_runtime.h>
 #include "../../include/gxcorr.h"
@@ -55,7 +56,9 @@ static void free_all(gx_handle *h)
   void *ptrs[] = {h->d_st, h->d_tw, h->d_spec, h->d_acc, h->d_results, h->d_spec1, h->d_w, h->d_wacc, h->d_w1,
                   h->d_pairs, h->d_prods, h->d_went, h->d_sub, h->d_bp, h->d_bp1, h->d_scale, h->d_tcprods,
                   h->d_tcrows, h->d_err, h->d_full, h->d_avgtab, h->d_pcal, h->d_pcalbins, h->d_zrows,
-                  h->d_zprods, h->d_specz, h->d_accz, h->d_uvents, h->d_uvfreqs};
+                  h->d_zprods, h->d_specz, h->d_accz, h->d_uvents, h->d_uvfreqs, h->d_binents, h->d_binitems,
+                  h->d_binwout, h->d_autoprods, h->d_autowents, h->d_binphase, h->d_binweight, h->d_accb,
+                  h->d_wbins};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->h_err) cudaFreeHost(h->h_err);
@@ -125,6 +128,15 @@ static gx_status setup(gx_handle *h)
   h->maxpc = 1;
   if (h->model)
     for (const auto &sc : h->model->scans) h->maxpc = std::max(h->maxpc, sc.numphasecentres);
+  // pulsar binning: records per bin unless scrunched (configuration.cpp:2455-2470)
+  h->nbins = 0;
+  h->binloop = 1;
+  h->scrunch = false;
+  if (h->meta && h->meta->pulsar) {
+    h->nbins = h->meta->pulsar->nbins;
+    h->scrunch = h->meta->pulsar->scrunch;
+    h->binloop = h->scrunch ? 1 : h->nbins;
+  }
   // the recorded freqs share bandwidth and channel count and come first in the
   // freq table: their spectra and accumulators are slabs [0, nfmain)
   const gx_freq_desc &f0 = d.freqs[s0.recfreq[0]];
@@ -260,11 +272,17 @@ static gx_status setup(gx_handle *h)
   if (d.xstep == GX_XSTEP_AUTO) {
     const char *e = getenv("GX_XSTEP_AUTO_MIN_INPUTS");
     const int nmin = e ? atoi(e) : 48;
-    h->xstep = (ni >= nmin && ni <= kTcInputs && J.nchan >= 2 && h->maxpc == 1) ? GX_XSTEP_TC_FP16_HILO
-                                                                                : GX_XSTEP_FP32;
+    h->xstep = (ni >= nmin && ni <= kTcInputs && J.nchan >= 2 && h->maxpc == 1 && h->nbins == 0)
+                   ? GX_XSTEP_TC_FP16_HILO : GX_XSTEP_FP32;
   }
   if (h->maxpc > 1 && h->xstep != GX_XSTEP_FP32)
     return h->fail(GX_ERR_UNSUPPORTED, "multiple phase centres are implemented with the FP32 X-step only");
+  if (h->nbins > 0) {
+    if (h->xstep != GX_XSTEP_FP32)
+      return h->fail(GX_ERR_UNSUPPORTED, "pulsar binning is implemented with the FP32 X-step only");
+    if (h->maxpc > 1) return h->fail(GX_ERR_UNSUPPORTED, "pulsar binning with multiple phase centres is not implemented");
+    if (h->interlaced_any) return h->fail(GX_ERR_UNSUPPORTED, "pulsar binning of INTERLACEDVDIF is not implemented");
+  }
   h->tc = h->xstep != GX_XSTEP_FP32;
   h->hilo = h->xstep == GX_XSTEP_TC_FP16_HILO;
   if (h->tc) {
@@ -392,6 +410,8 @@ static gx_status setup(gx_handle *h)
   }
   if (!h->zfreq.empty() && h->maxpc > 1)
     return h->fail(GX_ERR_UNSUPPORTED, "zoom bands with multiple phase centres are not implemented");
+  if (!h->zfreq.empty() && h->nbins > 0)
+    return h->fail(GX_ERR_UNSUPPORTED, "zoom bands with pulsar binning are not implemented");
   {
     int nzi = 0;
     for (int c : zcount) nzi = std::max(nzi, c);
@@ -520,7 +540,7 @@ static gx_status setup(gx_handle *h)
         int lf = bl_localfreq(d.baselines[j], f);
         if (lf < 0) continue;
         blofs[f * nbl + j] = (int)idx;
-        idx += (long long)h->maxpc * d.baselines[j].npolprod[lf] * (d.freqs[f].nchan / div);
+        idx += (long long)h->maxpc * h->binloop * d.baselines[j].npolprod[lf] * (d.freqs[f].nchan / div);
       }
     }
     for (int f = 0; f < d.nfreqs; f++) {
@@ -529,7 +549,7 @@ static gx_status setup(gx_handle *h)
         int lf = bl_localfreq(d.baselines[j], f);
         if (lf < 0) continue;
         bwofs[f * nbl + j] = (int)idx;
-        int np = d.baselines[j].npolprod[lf];
+        int np = h->binloop * d.baselines[j].npolprod[lf];   // a weight per bin and product
         idx += np / 2 + np % 2;
       }
     }
@@ -596,10 +616,11 @@ static gx_status setup(gx_handle *h)
         const int lf = bl_localfreq(d.baselines[j], f);
         if (lf < 0 || h->blofs[f * nbl + j] < 0) continue;
         const int nf = d.freqs[f].nchan, np = d.baselines[j].npolprod[lf];
-        for (int p = 0; p < h->maxpc * np; p++)   // records of every phase centre
+        for (int p = 0; p < h->maxpc * h->binloop * np; p++)   // records of every phase centre and bin
           add(h->blofs_full[f * nbl + j] + (long long)p * nf, h->blofs[f * nbl + j] + (long long)p * (nf / avg),
               nf / avg, avg);
-        add(h->bwofs_full[f * nbl + j], h->bwofs[f * nbl + j], np / 2 + np % 2, 1);
+        const int nw = h->binloop * np;
+        add(h->bwofs_full[f * nbl + j], h->bwofs[f * nbl + j], nw / 2 + nw % 2, 1);
         if (h->maxpc > 1) add(h->bsdofs_full[f * nbl + j], h->bsdofs[f * nbl + j], h->maxpc / 2 + h->maxpc % 2, 1);
       }
     long long total_pc = 0;   // the phase-cal section follows the autocorrelation weights
@@ -646,6 +667,11 @@ static gx_status setup(gx_handle *h)
   };
   h->prods.clear();
   h->uvents.clear();
+  h->binents.clear();
+  h->binitems.clear();
+  h->binwout.clear();
+  h->autoprods.clear();
+  h->autowents.clear();
   h->tcprods.clear();
   h->wents.clear();
   h->pairs.clear();
@@ -703,6 +729,15 @@ static gx_status setup(gx_handle *h)
           const ProdEntry &pe = h->prods.back();
           h->uvents.push_back(UvEntry{pe.result_offset, pe.acc_index, pe.conj, j, f, B.npolprod[lf] * J.nchan});
           w.source = h->interlaced_any ? item(wrow(B.ds1, b1), wrow(B.ds2, b2)) : d.nstations + j;
+          if (h->nbins > 0) {
+            // binned: one weight sum per (freq, baseline), the same for its products
+            if (p == 0) h->binitems.push_back(BinWeightItem{f, B.ds1, B.ds2});
+            const int fj = (int)h->binitems.size() - 1;
+            h->binents.push_back(BinEntry{h->blofs_full[f * nbl + j], f, a, bb, p, B.npolprod[lf], fj});
+            for (int b = 0; b < h->binloop; b++)
+              h->binwout.push_back(BinWeightOut{2LL * h->bwofs_full[f * nbl + j] + b * B.npolprod[lf] + p, fj, b});
+            continue;   // no unbinned weight entry
+          }
         } else {
           // zoom bands: the products of their rows; weights of their parent
           // recorded bands (datastream record band index, configuration.cpp:1203-1260)
@@ -718,6 +753,7 @@ static gx_status setup(gx_handle *h)
       }
     }
   }
+  const size_t ncross_prods = h->prods.size();   // the autocorrelation rows follow
   for (int s = 0; s < d.nstations; s++) {
     const gx_station_desc &x = d.stations[s];
     long long ro = h->acofs_full[s];
@@ -766,6 +802,8 @@ static gx_status setup(gx_handle *h)
       }
     }
   }
+
+  if (h->nbins > 0) h->autoprods.assign(h->prods.begin() + ncross_prods, h->prods.end());
 
   // tensor-core finalising pass: entries grouped by (freq, a) row
   h->tcrows.clear();
@@ -846,6 +884,12 @@ static gx_status setup(gx_handle *h)
     // equal chunks: no short tail pass
     const int nch = (J.blocks_per_send + chunk - 1) / chunk;
     chunk = (J.blocks_per_send + nch - 1) / nch;
+  }
+  if (h->nbins > 0) {
+    // passes of whole buffered-FFT groups: the binned weights are summed in
+    // the reference's group order (core.cpp:784-800, 943-950)
+    const int nbuf = h->meta ? h->meta->num_buffered_ffts : 1;
+    chunk = std::min(J.blocks_per_send, (chunk + nbuf - 1) / nbuf * nbuf);
   }
   h->chunk = chunk;
   if (h->tc) {
@@ -995,6 +1039,24 @@ static gx_status setup(gx_handle *h)
   if (!h->wents.empty())
     CKR(h, cudaMemcpy(h->d_went, h->wents.data(), sizeof(WeightEntry) * h->wents.size(), cudaMemcpyHostToDevice));
   CKR(h, h->dalloc(&h->d_results, sizeof(float2) * h->rl));
+  if (h->nbins > 0) {
+    const PulsarConfig &P = *h->meta->pulsar;
+    auto up = [&](auto **dst, const auto &vec) -> gx_status {
+      using T = typename std::remove_reference<decltype(vec)>::type::value_type;
+      CKR(h, h->dalloc(dst, sizeof(T) * std::max<size_t>(1, vec.size())));
+      if (!vec.empty()) CKR(h, cudaMemcpy(*dst, vec.data(), sizeof(T) * vec.size(), cudaMemcpyHostToDevice));
+      return GX_OK;
+    };
+    gx_status r;
+    if ((r = up(&h->d_binents, h->binents)) != GX_OK) return r;
+    if ((r = up(&h->d_binitems, h->binitems)) != GX_OK) return r;
+    if ((r = up(&h->d_binwout, h->binwout)) != GX_OK) return r;
+    if ((r = up(&h->d_autoprods, h->autoprods)) != GX_OK) return r;
+    if ((r = up(&h->d_binphase, P.binphaseends)) != GX_OK) return r;
+    if ((r = up(&h->d_binweight, P.binweights)) != GX_OK) return r;
+    CKR(h, h->dalloc(&h->d_accb, sizeof(float2) * std::max<size_t>(1, h->binents.size()) * h->nbins * J.nchan));
+    CKR(h, h->dalloc(&h->d_wbins, sizeof(float) * std::max<size_t>(1, h->binitems.size()) * h->nbins));
+  }
   if (h->maxpc > 1) {
     CKR(h, h->dalloc(&h->d_uvents, sizeof(UvEntry) * std::max<size_t>(1, h->uvents.size())));
     if (!h->uvents.empty())
@@ -1038,7 +1100,11 @@ static gx_status setup(gx_handle *h)
   // (doubles) and the shift-decorrelation section of the result (floats)
   h->o_uvdelay = (h->o_ctrl + sizeof(int32_t) * h->ctrlstride * d.nstations + 15) & ~(size_t)15;
   h->o_bsd = h->o_uvdelay + sizeof(double) * (size_t)h->uv_nint * d.nbaselines * h->maxpc;
-  h->sub_bytes = h->o_bsd + sizeof(float2) * (size_t)h->bsd_count;
+  // pulsar binning: the mean pulse phase of every block and the dispersion
+  // phase offset of every channel (doubles)
+  h->o_avgphase = (h->o_bsd + sizeof(float2) * (size_t)h->bsd_count + 15) & ~(size_t)15;
+  h->o_dmoff = h->o_avgphase + (h->nbins > 0 ? sizeof(double) * (size_t)J.blocks_per_send : 0);
+  h->sub_bytes = h->o_dmoff + (h->nbins > 0 ? sizeof(double) * (size_t)h->nfmain * J.nchan : 0);
   CKR(h, h->dalloc(&h->d_sub, h->sub_bytes));
   for (int k = 0; k < gx_handle::kSlots; k++) {
     CKR(h, cudaMallocHost(&h->h_sub[k], h->sub_bytes));
@@ -1278,6 +1344,51 @@ static gx_status stage_subint(gx_handle *h, const gx_subint_desc *sub, const uin
       if (r != GX_OK) return h->fail(r, "no delay model for this subint");
     }
   }
+  if (h->nbins > 0) {
+    // Pulsar binning: the polyco covering the subint start (Core::loopprocess,
+    // core.cpp:496-507; Polyco::setTime and calculateDMPhaseOffsets,
+    // polyco.cpp:291-342, 368-387), the dispersion phase offset of every
+    // channel (setFrequencyValues, polyco.cpp:226-251, with the FP32 band
+    // edges and widths it keeps) and the mean phase of every block
+    // (getBins, polyco.cpp:177-190)
+    const PulsarConfig &P = *h->meta->pulsar;
+    const JobMeta &M = *h->meta;
+    const double sec = double(M.start_seconds + (int)h->model->scan_start_sec(sub->scan) + sub->sec) +
+                       ((double)sub->ns) / 1000000000.0;
+    const int pi = P.current(M.start_mjd, sec / 86400.0);
+    if (pi < 0) return h->fail(GX_ERR_MODEL, "no polyco covers this subint");
+    const PolycoEntry &Q = P.polycos[pi];
+    const int nco = (int)Q.phasecoef.size();
+    const double dt0 = (M.start_mjd - Q.mjd) * 1440 + (sec / 86400.0 - Q.mjdfraction) * 1440.0;
+    const double calclengthmins = double(d.subint_ns) / 60000000000.0;
+    double tp[64];
+    tp[0] = 1.0;
+    auto dot = [&](double dt, const std::vector<double> &c) {
+      for (int i = 1; i < nco; i++) tp[i] = dt * tp[i - 1];
+      double acc = 0;
+      for (int i = 0; i < nco; i++) acc += tp[i] * c[i];
+      return acc;
+    };
+    const double currentfreq = dot(dt0 + calclengthmins / 2, Q.freqcoef);
+    const double DMC = 1.0 / 0.000241;   // Polyco::DM_CONSTANT_SECS
+    double *dmoff = reinterpret_cast<double *>(b + h->o_dmoff);
+    const int N = h->J.nchan;
+    for (int f = 0; f < h->nfmain; f++) {
+      const gx_freq_desc &fq = d.freqs[f];
+      double lo = fq.freq_mhz;
+      if (fq.lower_sideband) lo -= ((double)(fq.nchan - 1)) * fq.bw_mhz / ((double)fq.nchan);
+      const float lof = (float)lo, bwf = (float)fq.bw_mhz;
+      for (int c = 0; c < N; c++) {
+        const double cf = lof + ((float)c * bwf) / double(fq.nchan);
+        const double dmdelay = -Q.dm * DMC / (cf * cf) + Q.dm * DMC / (Q.obsfreq * Q.obsfreq);
+        dmoff[(size_t)f * N + c] = dmdelay * currentfreq;
+      }
+    }
+    double *avgphase = reinterpret_cast<double *>(b + h->o_avgphase);
+    const double blockns = ((double)d.subint_ns) / ((double)h->J.blocks_per_send);
+    for (int i = 0; i < h->J.blocks_per_send; i++)
+      avgphase[i] = dot(dt0 + ((double)i) * blockns / 60000000000.0, Q.phasecoef);
+  }
   h->cur_npc[k] = 1;
   h->cur_M[k] = 0;
   if (h->maxpc > 1) {
@@ -1384,6 +1495,10 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
   if (!h->tc) CKR(h, cudaMemsetAsync(h->d_acc, 0, sizeof(float2) * h->acc_slice * h->ks, st));
   const int nzr = (int)h->zrows.size(), nzf = (int)h->zfreq.size();
   if (nzf) CKR(h, cudaMemsetAsync(h->d_accz, 0, sizeof(float2) * h->zacc_slice * h->zks, st));
+  if (h->nbins > 0) {
+    CKR(h, cudaMemsetAsync(h->d_accb, 0, sizeof(float2) * h->binents.size() * h->nbins * J.nchan, st));
+    CKR(h, cudaMemsetAsync(h->d_wbins, 0, sizeof(float) * h->binitems.size() * h->nbins, st));
+  }
   const int npairs = (int)h->pairs.size();
   CKR(h, cudaMemsetAsync(h->d_wacc, 0, sizeof(float) * (d.nstations + npairs), st));
   CKR(h, cudaMemsetAsync(h->d_err, 0, sizeof(int), st));
@@ -1410,6 +1525,16 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
                             b0 > 0 ? 1 : 0, h->d_err, st));
     else
       CKR(h, xmac_fp32_launch(h->d_spec, nb, J.ninputs, J.nchan, h->nfmain, h->ks, h->d_acc, h->d_err, st));
+    if (h->nbins > 0) {   // pulsar binning: the binned cross products and weights of this pass
+      const double *avgphase = reinterpret_cast<const double *>(h->d_sub + h->o_avgphase);
+      const double *dmoff = reinterpret_cast<const double *>(h->d_sub + h->o_dmoff);
+      CKR(h, binned_xmac_launch(h->d_binents, (int)h->binents.size(), h->d_spec, J.ninputs, J.nchan, nb, b0, avgphase,
+                                dmoff, h->d_binphase, h->nbins, h->d_accb, st));
+      CKR(h, binned_weights_launch(h->d_binitems, (int)h->binitems.size(), h->d_w, nb, b0, J.nchan,
+                                   h->meta->num_buffered_ffts, h->xmac_stride, avgphase, dmoff, h->d_binphase,
+                                   h->d_binweight, h->nbins, h->scrunch ? 1 : 0, h->d_wbins, st));
+      h->launches += 2;
+    }
     if (nzf) {   // zoom freqs: their rows of this pass's spectra, then their cross products
       CKR(h, zoom_gather_launch(h->d_zrows, nzr, h->d_spec, J.ninputs, J.nchan, h->d_specz, h->nzrows, h->nzchan, nb,
                                 st));
@@ -1459,6 +1584,15 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
                               J.ninputs, h->ks, fin, st));
     CKR(h, finalise_launch(nullptr, 0, h->d_acc, h->ks, h->acc_slice, J.nchan, h->d_went, (int)h->wents.size(),
                            h->d_wacc, fin, st));
+  } else if (h->nbins > 0) {
+    // the autocorrelations and their weights as usual, the crosses from the bins
+    CKR(h, cudaMemsetAsync(fin, 0, sizeof(float2) * h->rl_full, st));
+    CKR(h, finalise_launch(h->d_autoprods, (int)h->autoprods.size(), h->d_acc, h->ks, h->acc_slice, J.nchan,
+                           h->d_went, (int)h->wents.size(), h->d_wacc, fin, st));
+    CKR(h, binned_finalise_launch(h->d_binents, (int)h->binents.size(), h->d_accb, J.nchan, h->nbins,
+                                  h->scrunch ? 1 : 0, h->d_binweight, h->d_binwout, (int)h->binwout.size(), h->d_wbins,
+                                  fin, st));
+    h->launches += 1;
   } else {
     CKR(h, cudaMemsetAsync(fin, 0, sizeof(float2) * h->rl_full, st));
     CKR(h, finalise_launch(h->d_prods, (int)h->prods.size(), h->d_acc, h->ks, h->acc_slice, J.nchan, h->d_went,

@@ -65,6 +65,25 @@ struct gx_handle {
   long long bsd_first = 0, bsd_count = 0;    // complex-float range of that section (full layout)
   size_t o_uvdelay = 0, o_bsd = 0;           // in the per-subint table block
   int cur_npc[2] = {1, 1}, cur_M[2] = {0, 0};   // per slot: phase centres of the staged subint's scan, interval blocks
+  // Pulsar binning (core.cpp:803-811, 913-958): cross products accumulated
+  // per pulse-phase bin by their own kernel, the autocorrelations through the
+  // FP32 X-step as usual.
+  int nbins = 0, binloop = 1;                // bins (0: no binning); records per baseline-freq
+  bool scrunch = false;
+  std::vector<gx::BinEntry> binents;
+  std::vector<gx::BinWeightItem> binitems;
+  std::vector<gx::BinWeightOut> binwout;
+  std::vector<gx::ProdEntry> autoprods;      // the autocorrelation rows of prods
+  std::vector<gx::WeightEntry> autowents;    // and their weight entries
+  gx::BinEntry *d_binents = nullptr;
+  gx::BinWeightItem *d_binitems = nullptr;
+  gx::BinWeightOut *d_binwout = nullptr;
+  gx::ProdEntry *d_autoprods = nullptr;
+  gx::WeightEntry *d_autowents = nullptr;
+  double *d_binphase = nullptr, *d_binweight = nullptr;
+  float2 *d_accb = nullptr;                  // [entry][bin][chan]
+  float *d_wbins = nullptr;                  // [item][bin]
+  size_t o_avgphase = 0, o_dmoff = 0;        // per-subint tables: mean phase per block, dispersion phase offsets
   std::vector<std::vector<int>> zparent;     // [station][zoom band] parent recorded band
   std::vector<std::vector<int>> acbands;     // [station] total bands (recorded, then zoom) with autocorrelations
   gx::ZoomRow *d_zrows = nullptr;

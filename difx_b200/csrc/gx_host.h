@@ -54,6 +54,27 @@ class HostModel {
   bool uvw(int scan, double offsettime, int ant1, int ant2, int src, double out[3]) const;
 };
 
+// One polyco (Polyco::loadPolycoFile, polyco.cpp:399-524): pulse phase and
+// frequency as polynomials in minutes from its centre time.
+struct PolycoEntry {
+  int mjd = 0;
+  double mjdfraction = 0, dm = 0, f0 = 0, refphase = 0, obsfreq = 0;
+  int timespan = 0;                     // minutes
+  std::vector<double> phasecoef, freqcoef;
+};
+
+// PULSAR CONFIG FILE of a configuration (Configuration::processPulsarConfig,
+// configuration.cpp:3400-3498) and the polycos of its files.
+struct PulsarConfig {
+  int nbins = 0;
+  bool scrunch = false;
+  std::vector<double> binphaseends, binweights;
+  std::vector<PolycoEntry> polycos;
+  // Polyco::getCurrentPolyco (polyco.cpp:349-366): the first whose span
+  // (plus a second) covers mjd + mjdfraction; -1: none
+  int current(int mjd, double mjdfraction) const;
+};
+
 // Job-level .input facts the visibility writer needs (Configuration).
 struct JobMeta {
   int start_mjd = 0, start_seconds = 0, execute_seconds = 0;
@@ -62,6 +83,7 @@ struct JobMeta {
   std::vector<double> tsys;            // TSYS per datastream
   std::vector<std::string> telescope_name;   // TELESCOPE NAME per telescope
   int num_buffered_ffts = 1;           // NUM BUFFERED FFTS
+  std::shared_ptr<PulsarConfig> pulsar;   // PULSAR BINNING: the bins and polycos
 };
 
 struct InputJob {

@@ -132,6 +132,59 @@ std::string resolve(const std::string &file, const std::string &relto)
   return dir_of(relto) + f;
 }
 
+// Polycos of one file, in order (Polyco::loadPolycoFile, polyco.cpp:399-524):
+// two header lines, then the coefficients three to a line, D exponents allowed.
+bool read_polycos(const std::string &path, std::vector<PolycoEntry> &out, std::string &err)
+{
+  std::ifstream in(path);
+  if (!in) { err = "cannot open polyco file " + path; return false; }
+  std::vector<std::string> lines;
+  std::string line;
+  while (std::getline(in, line))
+    if (line.find_first_not_of(" \t\r\n") != std::string::npos) lines.push_back(line);
+  size_t i = 0;
+  while (i + 2 <= lines.size()) {
+    PolycoEntry P;
+    std::istringstream a(lines[i]), b(lines[i + 1]);
+    std::string name, date, utc;
+    double mjdd = 0;
+    if (!(a >> name >> date >> utc >> mjdd >> P.dm)) { err = "polyco header line 1: " + path; return false; }
+    P.mjd = int(mjdd);
+    P.mjdfraction = mjdd - P.mjd;
+    std::string obs;
+    int ncoef = 0;
+    if (!(b >> P.refphase >> P.f0 >> obs >> P.timespan >> ncoef >> P.obsfreq) || ncoef < 2 || ncoef > 64) {
+      err = "polyco header line 2: " + path;
+      return false;
+    }
+    P.refphase = P.refphase - std::floor(P.refphase);
+    i += 2;
+    std::vector<double> c;
+    while ((int)c.size() < ncoef) {
+      if (i >= lines.size()) { err = "polyco coefficients: " + path; return false; }
+      std::istringstream cs(lines[i++]);
+      std::string tok;
+      while ((int)c.size() < ncoef && cs >> tok) {
+        for (char &ch : tok)
+          if (ch == 'D' || ch == 'd') ch = 'E';
+        c.push_back(atof(tok.c_str()));
+      }
+    }
+    // frequency and phase coefficients (polyco.cpp:506-515)
+    P.freqcoef.assign(ncoef, 0.0);
+    P.freqcoef[0] = P.f0 + c[1] / 60.0;
+    P.freqcoef[ncoef - 1] = 0.0;
+    for (int k = 1; k < ncoef - 1; k++) P.freqcoef[k] = (k + 1) * c[k + 1] / 60.0;
+    P.phasecoef.assign(ncoef, 0.0);
+    P.phasecoef[0] = P.refphase + c[0];
+    P.phasecoef[1] = 60.0 * P.f0 + c[1];
+    for (int k = 2; k < ncoef; k++) P.phasecoef[k] = c[k];
+    out.push_back(P);
+  }
+  if (out.empty()) { err = "no polycos in " + path; return false; }
+  return true;
+}
+
 #define NEED(kv, key, var)          \
   do {                              \
     if (!(kv).get((key), (var))) {  \
@@ -176,6 +229,17 @@ bool HostModel::uvw(int scanindex, double offsettime, int ant1, int ant2, int sr
     out[c] = a - b;
   }
   return true;
+}
+
+int PulsarConfig::current(int mjd, double mjdfraction) const
+{
+  for (size_t i = 0; i < polycos.size(); i++) {
+    const PolycoEntry &P = polycos[i];
+    const double differencemins = (mjd - P.mjd) * 1440 + (mjdfraction - P.mjdfraction) * 1440;
+    const double rangemins = double(P.timespan) / 2.0 + 1.0 / 60.0;   // an extra second against roundoff
+    if (differencemins <= rangemins && differencemins >= -rangemins) return (int)i;
+  }
+  return -1;
 }
 
 bool HostModel::linear(int scanindex, double offsettime, int ant, int src, double out[2]) const
@@ -277,7 +341,34 @@ InputJob *read_input_job(const char *inputfile, std::string &err)
   NEED(in, "NUM BUFFERED FFTS", v); job->meta.num_buffered_ffts = std::max(1, atoi(v.c_str()));
   NEED(in, "WRITE AUTOCORRS", v); d.write_autocorrs = truthy(v) ? 1 : 0;
   NEED(in, "PULSAR BINNING", v);
-  if (truthy(v)) { err = "pulsar binning is not implemented"; return nullptr; }
+  if (truthy(v)) {
+    // the bin configuration and its polycos (configuration.cpp:1368-1372, 3400-3498)
+    NEED(in, "PULSAR CONFIG FILE", v);
+    KVFile bc;
+    if (!bc.load(resolve(v, inputfile))) { err = bc.err; return nullptr; }
+    std::shared_ptr<PulsarConfig> pc(new PulsarConfig());
+    std::string w;
+    if (!bc.get("NUM POLYCO FILES", w)) { err = bc.err; return nullptr; }
+    const int nfiles = atoi(w.c_str());
+    for (int i = 0; i < nfiles; i++) {
+      if (!bc.get("POLYCO FILE", w)) { err = bc.err; return nullptr; }
+      if (!read_polycos(resolve(w, inputfile), pc->polycos, err)) return nullptr;
+    }
+    if (!bc.get("NUM PULSAR BINS", w)) { err = bc.err; return nullptr; }
+    pc->nbins = atoi(w.c_str());
+    if (pc->nbins < 1 || pc->nbins > 1024) { err = "NUM PULSAR BINS out of range"; return nullptr; }
+    if (!bc.get("SCRUNCH OUTPUT", w)) { err = bc.err; return nullptr; }
+    pc->scrunch = truthy(w);
+    for (int i = 0; i < pc->nbins; i++) {
+      if (!bc.get("BIN PHASE END", w)) { err = bc.err; return nullptr; }
+      pc->binphaseends.push_back(atof(w.c_str()));
+      if (!bc.get("BIN WEIGHT", w)) { err = bc.err; return nullptr; }
+      pc->binweights.push_back(atof(w.c_str()));
+    }
+    for (int i = 1; i < pc->nbins; i++)
+      if (pc->binphaseends[i] < pc->binphaseends[i - 1]) { err = "bin phase ends not ascending"; return nullptr; }
+    job->meta.pulsar = pc;
+  }
   NEED(in, "PHASED ARRAY", v);
   if (truthy(v)) { err = "phased-array mode is not implemented"; return nullptr; }
   std::vector<int> dsidx(numds), blidx(numbl);

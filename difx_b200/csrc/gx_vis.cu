@@ -108,6 +108,8 @@ gx_status gx_vis_open(gx_handle *h, const char *outdir, gx_vis **out)
   *out = nullptr;
   if (h->device < 0) return h->fail(GX_ERR_STATE, "host-only handle (opened with device -1)");
   if (!h->model || !h->meta) return h->fail(GX_ERR_STATE, "the visibility writer needs a handle opened with gx_open_input");
+  if (h->nbins > 0)   // per-bin files, weights over the bin widths (visibility.cpp:402-420)
+    return h->fail(GX_ERR_UNSUPPORTED, "the visibility writer does not implement pulsar binning");
   if (!h->zfreq.empty() && h->meta)
     for (double t : h->meta->tsys)   // Configuration::getDMatchingBand reads zoom bands out of range
       if (t > 0.0) return h->fail(GX_ERR_UNSUPPORTED, "a-priori calibration (TSYS > 0) of zoom bands is not implemented");

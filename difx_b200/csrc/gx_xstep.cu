@@ -394,6 +394,157 @@ cudaError_t copy_floats_launch(const float *vals, long long n, float *results_f,
   return cudaGetLastError();
 }
 
+// The pulsar bin of a channel (Polyco::getBins, polyco.cpp:196-222): the
+// fractional part of the mean phase plus the channel's dispersion offset,
+// bin 0 outside [first end, last end), else the bin whose phase range holds it.
+__device__ __forceinline__ int pulsar_bin(double avgphase, double dmoff, const double *__restrict__ bp, int nbins)
+{
+  const double ap = dmoff + avgphase;
+  const double m = ap - floor(ap);
+  if (m < bp[0] || m >= bp[nbins - 1]) return 0;
+  int bin = 0;
+  for (int k = nbins - 1; k > 0; k--)
+    if (m < bp[k] && m >= bp[k - 1]) bin = k;
+  return bin;
+}
+
+__global__ void binned_xmac_kernel(const BinEntry *__restrict__ ents, const float2 *__restrict__ spec, int NI, int N,
+                                   int nblk, int b0, const double *__restrict__ avgphase,
+                                   const double *__restrict__ dmoff, const double *__restrict__ bp, int nbins,
+                                   float2 *__restrict__ acc)
+{
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= N) return;
+  const BinEntry e = ents[blockIdx.y];
+  const size_t bstride = (size_t)NI * N;
+  const float2 *xa = spec + ((size_t)e.f * nblk * NI + e.a) * N + c;
+  const float2 *xb = spec + ((size_t)e.f * nblk * NI + e.b) * N + c;
+  const double dm = dmoff[(size_t)e.f * N + c];
+  float2 *row = acc + (size_t)blockIdx.y * nbins * N + c;
+  // the current bin's accumulator is carried in registers: the same additions,
+  // in block order, as adding into it in memory block by block (core.cpp:943-950)
+  int cur = -1;
+  float2 sum = make_float2(0.f, 0.f);
+  for (int k = 0; k < nblk; k++) {
+    const int bin = pulsar_bin(avgphase[b0 + k], dm, bp, nbins);
+    if (bin != cur) {
+      if (cur >= 0) row[(size_t)cur * N] = sum;
+      cur = bin;
+      sum = row[(size_t)cur * N];
+    }
+    const float2 x1 = xa[k * bstride], x2 = xb[k * bstride];
+    const float2 p = cmul_exact(x1, make_float2(x2.x, -x2.y));   // vis1 x conj(vis2) (vectorMul_cf32)
+    sum.x = __fadd_rn(sum.x, p.x);
+    sum.y = __fadd_rn(sum.y, p.y);
+  }
+  if (cur >= 0) row[(size_t)cur * N] = sum;
+}
+
+cudaError_t binned_xmac_launch(const BinEntry *ents, int nents, const float2 *spec, int NI, int N, int nblk, int b0,
+                               const double *avgphase, const double *dmoff, const double *binphases, int nbins,
+                               float2 *acc, cudaStream_t st)
+{
+  if (nents <= 0 || nblk <= 0) return cudaSuccess;
+  if (nents > 65535) return cudaErrorInvalidConfiguration;
+  dim3 grid((N + 127) / 128, nents);
+  binned_xmac_kernel<<<grid, 128, 0, st>>>(ents, spec, NI, N, nblk, b0, avgphase, dmoff, binphases, nbins, acc);
+  return cudaGetLastError();
+}
+
+// One thread per (item, bin); the scrunched sum is bin 0's thread.
+__global__ void binned_weights_kernel(const BinWeightItem *__restrict__ items, int nitems, const float *__restrict__ w,
+                                      int nblk, int b0, int N, int nbuf, int xstride, const double *__restrict__ avgphase,
+                                      const double *__restrict__ dmoff, const double *__restrict__ bp,
+                                      const double *__restrict__ bw, int nbins, int scrunch, float *__restrict__ wbins)
+{
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int fj = t / nbins, mybin = t % nbins;
+  if (fj >= nitems || (scrunch && mybin != 0)) return;
+  const BinWeightItem it = items[fj];
+  const double *dm = dmoff + (size_t)it.f * N;
+  float acc = wbins[t];
+  const int nstr = (N + xstride - 1) / xstride;
+  // buffered-FFT groups of the subint (core.cpp:784-800), xmac strides, blocks, channels
+  for (int g0 = 0; g0 < nblk; g0 += nbuf) {
+    const int g1 = min(nblk, g0 + nbuf);
+    for (int x = 0; x < nstr; x++) {
+      const int c0 = x * xstride, c1 = min(N, c0 + xstride);
+      for (int k = g0; k < g1; k++) {
+        const float bweight = w[(size_t)it.s1 * nblk + k] * w[(size_t)it.s2 * nblk + k] / N;
+        const double ap = avgphase[b0 + k];
+        for (int c = c0; c < c1; c++) {
+          const int bin = pulsar_bin(ap, dm[c], bp, nbins);
+          if (scrunch) {
+            if (bw[bin] > 0.0) acc = (float)((double)acc + bweight * bw[bin]);
+          } else if (bin == mybin) {
+            acc = __fadd_rn(acc, bweight);
+          }
+        }
+      }
+    }
+  }
+  wbins[t] = acc;
+}
+
+cudaError_t binned_weights_launch(const BinWeightItem *items, int nitems, const float *w, int nblk, int b0, int N,
+                                  int nbuf, int xmacstride, const double *avgphase, const double *dmoff,
+                                  const double *binphases, const double *binweights, int nbins, int scrunch,
+                                  float *wbins, cudaStream_t st)
+{
+  if (nitems <= 0 || nblk <= 0) return cudaSuccess;
+  const int n = nitems * nbins;
+  binned_weights_kernel<<<(n + 63) / 64, 64, 0, st>>>(items, nitems, w, nblk, b0, N, nbuf, xmacstride, avgphase, dmoff,
+                                                      binphases, binweights, nbins, scrunch, wbins);
+  return cudaGetLastError();
+}
+
+__global__ void binned_finalise_kernel(const BinEntry *__restrict__ ents, const float2 *__restrict__ acc, int N,
+                                       int nbins, int scrunch, const double *__restrict__ bw,
+                                       float2 *__restrict__ results)
+{
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= N) return;
+  const BinEntry e = ents[blockIdx.y];
+  const float2 *row = acc + (size_t)blockIdx.y * nbins * N + c;
+  if (!scrunch) {
+    for (int b = 0; b < nbins; b++) results[e.ro + (size_t)(b * e.npol + e.p) * N + c] = row[(size_t)b * N];
+    return;
+  }
+  // each bin scaled by its (FP32) weight, then added in bin order (core.cpp:1439-1470, 1808-1823)
+  float2 s = make_float2(0.f, 0.f);
+  for (int b = 0; b < nbins; b++) {
+    const float wf = (float)bw[b];
+    const float2 v = row[(size_t)b * N];
+    s.x = __fadd_rn(s.x, __fmul_rn(v.x, wf));
+    s.y = __fadd_rn(s.y, __fmul_rn(v.y, wf));
+  }
+  results[e.ro + (size_t)e.p * N + c] = s;
+}
+
+__global__ void binned_weights_out_kernel(const BinWeightOut *__restrict__ wo, int n, const float *__restrict__ wbins,
+                                          int nbins, float *__restrict__ results_f)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const BinWeightOut x = wo[i];
+  results_f[x.float_index] = wbins[(size_t)x.fj * nbins + x.bin];
+}
+
+cudaError_t binned_finalise_launch(const BinEntry *ents, int nents, const float2 *acc, int N, int nbins, int scrunch,
+                                   const double *binweights, const BinWeightOut *wout, int nwout, const float *wbins,
+                                   float2 *results, cudaStream_t st)
+{
+  if (nents > 65535) return cudaErrorInvalidConfiguration;
+  if (nents > 0) {
+    dim3 grid((N + 127) / 128, nents);
+    binned_finalise_kernel<<<grid, 128, 0, st>>>(ents, acc, N, nbins, scrunch, binweights, results);
+  }
+  if (nwout > 0)
+    binned_weights_out_kernel<<<(nwout + 255) / 256, 256, 0, st>>>(wout, nwout, wbins, nbins,
+                                                                   reinterpret_cast<float *>(results));
+  return cudaGetLastError();
+}
+
 // Channel averaging of the finished result array (Mode::averageFrequency,
 // mode.cpp:1376-1401, for autocorrelations; Core's averaged copy,
 // core.cpp:1819-1869, for cross products): one CTA per record.

@@ -103,6 +103,43 @@ cudaError_t uvshift_launch(const UvEntry *ents, int nents, const float2 *acc, in
 // results_f[first + i] = vals[i], i < n (floats)
 cudaError_t copy_floats_launch(const float *vals, long long n, float *results_f, long long first, cudaStream_t st);
 
+// Pulsar binning (core.cpp:803-811, 913-958; Polyco::getBins,
+// polyco.cpp:177-224).  One cross product row: inputs a x conj(b) of freq f,
+// product p of npol; its bin-b record starts at ro + (b * npol + p) * N
+// (scrunched: ro + p * N); fj indexes its (freq, baseline) weight sums.
+struct BinEntry {
+  long long ro;
+  int f, a, b, p, npol, fj;
+};
+// (freq, baseline stations) of a binned weight sum
+struct BinWeightItem {
+  int f, s1, s2;
+};
+// result float index <- the weight sum of item fj, bin b
+struct BinWeightOut {
+  long long float_index;
+  int fj, bin;
+};
+// One pass of nblk blocks starting at subint block b0: acc[e][bin][c] +=
+// spec[f][blk][a][c] * conj(spec[f][blk][b][c]) in block order, the bin of
+// (block, channel) from the block's mean pulse phase and the channel's
+// dispersion phase offset (dmoff[f][c]).
+cudaError_t binned_xmac_launch(const BinEntry *ents, int nents, const float2 *spec, int NI, int N, int nblk, int b0,
+                               const double *avgphase, const double *dmoff, const double *binphases, int nbins,
+                               float2 *acc, cudaStream_t st);
+// The binned baseline weights of one pass, in the reference's order
+// (buffered FFT groups, xmac strides, blocks, channels): per bin the sum of
+// w1 w2 / nchan over the channels in the bin; scrunched (scrunch != 0), one
+// sum of w1 w2 / nchan x the bin's weight over channels of positive-weight bins.
+cudaError_t binned_weights_launch(const BinWeightItem *items, int nitems, const float *w, int nblk, int b0, int N,
+                                  int nbuf, int xmacstride, const double *avgphase, const double *dmoff,
+                                  const double *binphases, const double *binweights, int nbins, int scrunch,
+                                  float *wbins, cudaStream_t st);
+// The binned records (or their weighted sum when scrunched) and weights into the result array.
+cudaError_t binned_finalise_launch(const BinEntry *ents, int nents, const float2 *acc, int N, int nbins, int scrunch,
+                                   const double *binweights, const BinWeightOut *wout, int nwout, const float *wbins,
+                                   float2 *results, cudaStream_t st);
+
 struct AvgEntry {
   long long src, dst;
   int n, L;

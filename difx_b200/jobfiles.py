@@ -98,6 +98,13 @@ class JobSpec:
     phase_centres: int = 1
     max_pc_offset_us: float = 0.02
     max_pc_rate_us_per_s: float = 0.002
+    # pulsar binning: bins (0: none) of equal phase width, their weights
+    # (default 1), scrunched output, and a synthetic pulsar's polyco
+    pulsar_bins: int = 0
+    pulsar_bin_weights: Sequence[float] = ()
+    pulsar_scrunch: bool = False
+    pulsar_f0: float = 503.7          # Hz
+    pulsar_dm: float = 500.0          # pc cm^-3
 
     # ------------------------------------------------------------ derived
     def station_sb(self, station: int) -> List[int]:
@@ -332,12 +339,48 @@ def baseline_plan(spec: JobSpec) -> List[Tuple[int, int, List[Tuple[int, List[Tu
     return out
 
 
+def _fortran_d(x: float) -> str:
+    return f"{x:25.17E}".replace("E", "D")
+
+
+def write_polyco(spec: JobSpec, path: str) -> None:
+    """A one-entry TEMPO-style polyco (the layout Configuration counts entries
+    by and Polyco::loadPolycoFile reads, polyco.cpp:399-524): a 2-hour span
+    centred on the job, the phase polynomial in minutes from that centre."""
+    mjd_mid = spec.start_mjd + (spec.start_seconds + spec.execute_seconds / 2.0) / 86400.0
+    frac = mjd_mid - int(mjd_mid)
+    hh = int(frac * 24)
+    mm = int((frac * 24 - hh) * 60)
+    ss = ((frac * 24 - hh) * 60 - mm) * 60
+    coeffs = [0.137, 2.0e-3, 1.5e-5, -2.0e-8] + [0.0] * 8
+    utc = f"{hh:02d}{mm:02d}{ss:05.2f}"
+    l1 = f"{'J0000+00':<10s}{'01-JAN-15':>10s}{utc:>12s}{mjd_mid:20.11f}{spec.pulsar_dm:21.6f}{0.0:7.3f}{-6.0:7.3f}"
+    l2 = f"{0.25:20.6f}{spec.pulsar_f0:18.12f}{'    7':>5s}{120:5d}{len(coeffs):5d}{8400.0:10.3f}"
+    lines = [l1, l2]
+    for k in range(0, len(coeffs), 3):
+        lines.append("".join(_fortran_d(c) for c in coeffs[k:k + 3]))
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")
+
+
 def write_job(spec: JobSpec, outdir: str) -> dict:
     """Write ``<name>.input/.calc/.im/.threads/.flag`` into outdir; return their paths."""
     spec.validate()
     os.makedirs(outdir, exist_ok=True)
     base = os.path.join(outdir, spec.name)
     paths = {k: base + "." + k for k in ("input", "calc", "im", "threads", "flag")}
+    if spec.pulsar_bins > 0:
+        paths["binconfig"] = base + ".binconfig"
+        paths["polyco"] = base + ".polyco"
+        write_polyco(spec, paths["polyco"])
+        B = [_kv("NUM POLYCO FILES", 1), _kv("POLYCO FILE 0", paths["polyco"]),
+             _kv("NUM PULSAR BINS", spec.pulsar_bins), _kv("SCRUNCH OUTPUT", "TRUE" if spec.pulsar_scrunch else "FALSE")]
+        for k in range(spec.pulsar_bins):
+            w = spec.pulsar_bin_weights[k] if k < len(spec.pulsar_bin_weights) else 1.0
+            B.append(_kv(f"BIN PHASE END {k}", f"{(k + 1) / spec.pulsar_bins:.6f}"))
+            B.append(_kv(f"BIN WEIGHT {k}", f"{w:.6f}"))
+        with open(paths["binconfig"], "w") as f:
+            f.write("".join(B))
     names = spec.names()
     nst = spec.nstations
     nsb = len(spec.subbands)
@@ -375,7 +418,11 @@ def write_job(spec: JobSpec, outdir: str) -> dict:
     L.append(_kv("XMAC STRIDE LENGTH", spec.xmac_stride))
     L.append(_kv("NUM BUFFERED FFTS", spec.num_buffered_ffts))
     L.append(_kv("WRITE AUTOCORRS", "TRUE" if spec.write_autocorrs else "FALSE"))
-    L.append(_kv("PULSAR BINNING", "FALSE"))
+    if spec.pulsar_bins > 0:
+        L.append(_kv("PULSAR BINNING", "TRUE"))
+        L.append(_kv("PULSAR CONFIG FILE", paths["binconfig"]))
+    else:
+        L.append(_kv("PULSAR BINNING", "FALSE"))
     L.append(_kv("PHASED ARRAY", "FALSE"))
     for i in range(nst):
         L.append(_kv(f"DATASTREAM {i} INDEX", i))

@@ -35,6 +35,9 @@ struct RefJob {
   std::vector<int> startblock, numblocks;
   std::vector<u8 *> origbuffers;
   std::vector<std::vector<double>> interp_override;  // per datastream; empty: the model's
+  std::vector<Polyco **> polycos;      // per thread (pulsar binning), as Core::updateconfig gives them
+  std::vector<int> npolycos;
+  std::vector<Polyco *> curpolyco;     // per thread, set for the slot being processed
 };
 
 struct ThreadArg {
@@ -48,7 +51,7 @@ void *worker(void *p)
   RefJob *j = a->job;
   Core *c = j->core;
   pthread_mutex_lock(&(c->procslots[0].slotlocks[a->t]));
-  c->processdata(0, a->t, j->startblock[a->t], j->numblocks[a->t], j->modes[a->t], 0,
+  c->processdata(0, a->t, j->startblock[a->t], j->numblocks[a->t], j->modes[a->t], j->curpolyco[a->t],
                  (Core::threadscratchspace *)j->scratch[a->t]);
   pthread_mutex_unlock(&(c->procslots[1].slotlocks[a->t]));
   return 0;
@@ -99,11 +102,22 @@ void *ref_open(const char *inputfile)
     s->rotated = vectorAlloc_cf32(maxchan);
     s->channelsums = vectorAlloc_cf32(maxchan);
     s->argument = vectorAlloc_f32(3 * maxrot);
+    // pulsar binning scratch (core.cpp:437-458)
+    const bool psr = config->pulsarBinOn(0);
+    if (psr) {
+      s->pulsarscratchspace = vectorAlloc_cf32(config->getXmacStrideLength(0));
+      if (config->scrunchOutputOn(0)) s->pulsaraccumspace = new cf32 ******[config->getFreqTableLength()]();
+      c->createPulsarVaryingSpace(s->pulsaraccumspace, &(s->bins), 0, -1, t);
+    }
     c->allocateConfigSpecificThreadArrays(s->baselineweight, s->baselineshiftdecorr, 0, -1, t);
     Mode **modes = new Mode *[j->nds];
     int sb = 0, nb = 0, npoly = 0;
     bool pb = false;
-    c->updateconfig(0, 0, t, sb, nb, npoly, pb, modes, 0, true);
+    Polyco **polys = psr ? new Polyco *[config->getNumPolycos(0)] : 0;
+    c->updateconfig(0, 0, t, sb, nb, npoly, pb, modes, polys, true);
+    j->polycos.push_back(polys);
+    j->npolycos.push_back(npoly);
+    j->curpolyco.push_back(0);
     j->modes.push_back(modes);
     j->scratch.push_back(s);
     j->startblock.push_back(sb);
@@ -172,6 +186,19 @@ int ref_process(void *h, int scan, int sec, int ns, const unsigned char **data, 
   }
   int rl = j->config->getCoreResultLength(0);
   vectorZero_cf32(slot->results, rl);
+  if (j->config->pulsarBinOn(0)) {
+    // the polyco of the slot's time (Core::loopprocess, core.cpp:496-507)
+    Configuration *cf = j->config;
+    const int startmjd = cf->getStartMJD(), startseconds = cf->getStartSeconds();
+    const double secs = double(startseconds + c->model->getScanStartSec(scan, startmjd, startseconds) + sec) +
+                        ((double)ns) / 1000000000.0;
+    for (int t = 0; t < j->nthreads; t++) {
+      Polyco *p = Polyco::getCurrentPolyco(0, startmjd, secs / 86400.0, j->polycos[t], j->npolycos[t], false);
+      if (!p) return -2;
+      p->setTime(startmjd, secs / 86400.0);
+      j->curpolyco[t] = p;
+    }
+  }
   std::vector<pthread_t> th(j->nthreads);
   std::vector<ThreadArg> args(j->nthreads);
   for (int t = 0; t < j->nthreads; t++) {
