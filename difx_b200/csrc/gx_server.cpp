@@ -15,8 +15,12 @@
 // is in flight, so an oversized request cannot stall the loop).  Requests of
 // different jobs therefore run concurrently, each on its job's stream, and a
 // request that arrives while others are on the GPU starts as soon as a slot
-// and memory free up.  Each request's latency runs from submission to the
-// moment its results are in the caller's buffer.
+// and memory free up.  With device inputs, a request runs on a stream whose
+// CUDA priority follows its deadline's rank among the requests on the GPU
+// when it is admitted (the earliest deadline on the highest priority), so
+// that the GPU's block scheduler serves urgent requests first when several
+// share it.  Each request's latency runs from submission to the moment its
+// results are in the caller's buffer.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -67,6 +71,16 @@ gx_status run_device_inputs(void *, gx_handle *h, int, const gx_subint_desc *sub
   return gx_synchronize(h);
 }
 
+// The same on a given stream (a priority stream of the loop).
+gx_status run_device_inputs_on(gx_handle *h, const gx_subint_desc *sub, float *results, cudaStream_t st)
+{
+  gx_status s = gx_subint_device(h, sub, reinterpret_cast<float *>(h->d_results), st);
+  if (s != GX_OK) return s;
+  CKR(h, cudaMemcpyAsync(results, h->d_results, sizeof(float2) * h->rl, cudaMemcpyDeviceToHost, st));
+  CKR(h, cudaStreamSynchronize(st));
+  return gx_synchronize(h);
+}
+
 }  // namespace
 
 struct gx_server {
@@ -92,6 +106,31 @@ struct gx_server {
   std::condition_variable cv_work, cv_done;
   std::vector<std::thread> workers;
   bool stopping = false;
+  // priority streams (device inputs): [worker][level], level 0 the highest priority
+  std::vector<std::vector<cudaStream_t>> pstreams;
+  std::vector<Clock::time_point> running_deadline;   // deadlines of the requests on the GPU
+  bool streams_tried = false;
+
+  // per worker, one stream per priority level of the device (the inputs' device)
+  void make_streams(const gx_handle *h)
+  {
+    streams_tried = true;
+    if (!h || h->device < 0 || cudaSetDevice(h->device) != cudaSuccess) return;
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) return;
+    const int nlev = std::min(4, least - greatest + 1);
+    if (nlev < 2) return;
+    pstreams.assign(slots, {});
+    for (int w = 0; w < slots; w++)
+      for (int l = 0; l < nlev; l++) {
+        cudaStream_t st = nullptr;
+        if (cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, greatest + l) != cudaSuccess) {
+          pstreams.clear();
+          return;
+        }
+        pstreams[w].push_back(st);
+      }
+  }
 
   // the admissible queued request with the earliest deadline (arrival order
   // among equal deadlines and among requests without one)
@@ -107,7 +146,7 @@ struct gx_server {
     return best;
   }
 
-  void worker()
+  void worker(int wid)
   {
     std::unique_lock<std::mutex> lk(mu);
     for (;;) {
@@ -120,10 +159,24 @@ struct gx_server {
       J.busy = true;
       inflight++;
       inflight_bytes += r->bytes;
+      // the request's priority level: how many requests on the GPU have an earlier deadline
+      cudaStream_t pst = nullptr;
+      if (exec == run_device_inputs) {
+        if (!streams_tried) make_streams(J.h);
+        if (!pstreams.empty()) {
+          int rank = 0;
+          for (const auto &dl : running_deadline)
+            if (dl < r->deadline) rank++;
+          pst = pstreams[wid][std::min(rank, (int)pstreams[wid].size() - 1)];
+        }
+      }
+      running_deadline.push_back(r->deadline);
       lk.unlock();
-      const gx_status st = exec(exec_ctx, J.h, r->job, &r->sub, r->results);
+      const gx_status st = pst ? run_device_inputs_on(J.h, &r->sub, r->results, pst)
+                               : exec(exec_ctx, J.h, r->job, &r->sub, r->results);
       const double ms = std::chrono::duration<double, std::milli>(Clock::now() - r->t_submit).count();
       lk.lock();
+      running_deadline.erase(std::find(running_deadline.begin(), running_deadline.end(), r->deadline));
       J.busy = false;
       inflight--;
       inflight_bytes -= r->bytes;
@@ -146,7 +199,7 @@ struct gx_server {
   {
     if (started) return;
     started = true;
-    for (int i = 0; i < slots; i++) workers.emplace_back([this] { worker(); });
+    for (int i = 0; i < slots; i++) workers.emplace_back([this, i] { worker(i); });
   }
 };
 
@@ -287,6 +340,8 @@ gx_status gx_server_close(gx_server *s)
     s->cv_work.notify_all();
   }
   for (auto &t : s->workers) t.join();
+  for (auto &v : s->pstreams)
+    for (cudaStream_t st : v) cudaStreamDestroy(st);
   for (auto &kv : s->reqs) delete kv.second;
   delete s;
   return GX_OK;
