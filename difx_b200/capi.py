@@ -18,6 +18,7 @@ from .jobfiles import JobSpec, baseline_plan
 GX_MAX_LOCAL_FREQS = 64
 GX_MAX_BANDS = 128
 GX_MAX_POLPRODUCTS = 4
+GX_MAX_MUX_THREADS = 64
 
 GX_XSTEP_FP32 = 0
 GX_XSTEP_TC_FP16 = 1
@@ -50,7 +51,9 @@ class gx_station_desc(C.Structure):
                 ("zoomfreq", C.c_int * GX_MAX_LOCAL_FREQS),
                 ("nzoombands", C.c_int),
                 ("zoomband_localfreq", C.c_int * GX_MAX_BANDS),
-                ("zoomband_pol", C.c_char * GX_MAX_BANDS)]
+                ("zoomband_pol", C.c_char * GX_MAX_BANDS),
+                ("nmuxthreads", C.c_int),
+                ("muxthread", C.c_int * GX_MAX_MUX_THREADS)]
 
 
 class gx_baseline_desc(C.Structure):
@@ -165,6 +168,9 @@ def job_desc_from_spec(spec: JobSpec, xstep: int = GX_XSTEP_FP32, max_data_bytes
         st.clock_int_seconds = int(math.floor(c0 / 1e6 + 0.5))
         st.phase_cal_interval_hz = int(1e6 * spec.pcal_interval_mhz)
         st.interlaced = 1 if spec.mux_threads > 0 else 0
+        st.nmuxthreads = spec.mux_threads
+        for t in range(spec.mux_threads):
+            st.muxthread[t] = t
         stations.append(st)
     baselines = []
     for a, bb, fl in baseline_plan(spec):

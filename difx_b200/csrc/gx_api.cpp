@@ -1104,7 +1104,8 @@ static gx_status setup(gx_handle *h)
   // phase offset of every channel (doubles)
   h->o_avgphase = (h->o_bsd + sizeof(float2) * (size_t)h->bsd_count + 15) & ~(size_t)15;
   h->o_dmoff = h->o_avgphase + (h->nbins > 0 ? sizeof(double) * (size_t)J.blocks_per_send : 0);
-  h->sub_bytes = h->o_dmoff + (h->nbins > 0 ? sizeof(double) * (size_t)h->nfmain * J.nchan : 0);
+  h->o_ring = (h->o_dmoff + (h->nbins > 0 ? sizeof(double) * (size_t)h->nfmain * J.nchan : 0) + 15) & ~(size_t)15;
+  h->sub_bytes = h->o_ring + sizeof(double) * 3 * d.nstations;
   CKR(h, h->dalloc(&h->d_sub, h->sub_bytes));
   for (int k = 0; k < gx_handle::kSlots; k++) {
     CKR(h, cudaMallocHost(&h->h_sub[k], h->sub_bytes));
@@ -1476,6 +1477,12 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
   if (timed) {
     CKR(h, cudaEventRecord(h->ev_sub[k], st));
     h->ev_sub_pending[k] = true;
+  }
+  if (h->ring_req) {
+    // station data from the rings: the walk fills in the data pointers,
+    // lengths and control words of the tables just copied
+    gx_status rr = gx_ring_enqueue_control(h->ring_req, h, st);
+    if (rr != GX_OK) return rr;
   }
   SubintArrays S{};
   S.clock = reinterpret_cast<const SubintClock *>(h->d_sub);

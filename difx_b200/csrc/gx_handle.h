@@ -127,6 +127,11 @@ struct gx_handle {
   int slot = 0;                    // slot of the subint being staged and enqueued
   unsigned char *h_sub[kSlots] = {}, *d_sub = nullptr;
   size_t sub_bytes = 0, o_len = 0, o_ptr = 0, o_interp = 0, o_ctrl = 0;
+  // data ring subints (gx_ring_subint_device): [nstations][3] span delays in
+  // the block, and the ring whose walk runs right after the block's copy
+  size_t o_ring = 0;
+  struct gx_ring *ring_req = nullptr;
+  int ring_scan = 0, ring_sec = 0, ring_ns = 0;
   cudaEvent_t ev_sub[kSlots] = {}; // recorded after a block's copy (host may rewrite it once passed)
   bool ev_sub_pending[kSlots] = {};
   int ctrlstride = 0;
@@ -186,3 +191,5 @@ int gx_bl_localfreq(const gx_baseline_desc &b, int f);
 // host (capturable into a CUDA graph when h->untimed is set).
 gx_status gx_stage_subint(gx_handle *h, const gx_subint_desc *sub, const uint8_t *const *devdata);
 gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st);
+// The ring walk of h->ring_req over the copied tables (gx_ring.cu).
+gx_status gx_ring_enqueue_control(struct gx_ring *r, gx_handle *h, cudaStream_t st);

@@ -35,6 +35,7 @@ class HostModel {
   std::vector<ModelScan> scans;
   std::vector<int> station_of_datastream;   // model antenna index per datastream
   std::vector<int> intclockseconds;         // per datastream
+  std::vector<double> maxrate;              // per model antenna: Model::getMaxRate (us/s)
   double timespan_s = 0;                    // blockspersend * fftchannels * sampletime / 1e6
   int blocks_per_send = 0;
 
@@ -48,6 +49,11 @@ class HostModel {
   // scan's table, at offsettime seconds after the scan start; core.cpp:1652-1657)
   bool linear(int scan, double offsettime, int ant, int src, double out[2]) const;
   double scan_start_sec(int scan) const;
+  // Model::calculateDelayInterpolator of order 0 (model.cpp:232-248): the
+  // delay (us, clock included) of datastream ds at offsettime seconds after
+  // the scan start, for the source DataStream::calculateControlParams asks
+  // for (datastream.cpp:375-377); false outside the scan's model samples.
+  bool delay0(int ds, int scan, double offsettime, double *out) const;
   // Model::interpolateUVW (model.cpp:177-217): baseline (u, v, w) of model
   // antennas ant1 - ant2 at offsettime seconds after the scan start, source
   // src of the scan's table (1: first phase centre).
@@ -83,6 +89,7 @@ struct JobMeta {
   std::vector<double> tsys;            // TSYS per datastream
   std::vector<std::string> telescope_name;   // TELESCOPE NAME per telescope
   int num_buffered_ffts = 1;           // NUM BUFFERED FFTS
+  int data_buffer_factor = 0, num_data_segments = 0;   // DATA BUFFER FACTOR, NUM DATA SEGMENTS
   std::shared_ptr<PulsarConfig> pulsar;   // PULSAR BINNING: the bins and polycos
 };
 

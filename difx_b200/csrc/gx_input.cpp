@@ -272,6 +272,27 @@ bool HostModel::linear(int scanindex, double offsettime, int ant, int src, doubl
   return true;
 }
 
+bool HostModel::delay0(int ds, int scanindex, double offsettime, double *out) const
+{
+  if (scanindex < 0 || scanindex >= (int)scans.size()) return false;
+  const ModelScan &sc = scans[scanindex];
+  const int ant = station_of_datastream[ds];
+  const int srcindex = (sc.numphasecentres == 1) ? 1 : 0;
+  const int polyoffset = (modelmjd - sc.polystartmjd) * 86400 + modelstartseconds + sc.offsetseconds - sc.polystartseconds;
+  int scansample = int((offsettime + polyoffset) / double(modelincsecs));
+  if (scansample == sc.nsamples && ((offsettime + polyoffset - scansample * modelincsecs) < 1e-6)) scansample--;
+  if (scansample < 0 || scansample >= sc.nsamples) return false;
+  // a zero time span: the polynomial at offsettime itself
+  const double dt = offsettime + polyoffset + 0.0 / 2.0 - scansample * modelincsecs;
+  double tp[16];
+  tp[0] = 1.0;
+  for (int i = 0; i < polyorder; i++) tp[i + 1] = tp[i] * dt;
+  double acc = 0;
+  for (int i = 0; i < polyorder + 1; i++) acc += tp[i] * delay_at(sc, scansample, srcindex, ant, i);
+  *out = acc;
+  return true;
+}
+
 gx_status HostModel::interpolator(int ds, int scanindex, int sec, int ns, double out[3]) const
 {
   if (scanindex < 0 || scanindex >= (int)scans.size()) return GX_ERR_MODEL;
@@ -417,8 +438,8 @@ InputJob *read_input_job(const char *inputfile, std::string &err)
   if (!in.seek_section("# DATASTREAM TABLE")) { err = in.err; return nullptr; }
   NEED(in, "DATASTREAM ENTRIES", v);
   const int nds_table = atoi(v.c_str());
-  NEED(in, "DATA BUFFER FACTOR", v);
-  NEED(in, "NUM DATA SEGMENTS", v);
+  NEED(in, "DATA BUFFER FACTOR", v); job->meta.data_buffer_factor = atoi(v.c_str());
+  NEED(in, "NUM DATA SEGMENTS", v); job->meta.num_data_segments = atoi(v.c_str());
   std::vector<gx_station_desc> dstab(nds_table);
   std::vector<int> dstel(nds_table);
   std::vector<double> dstsys(nds_table, 0.0);
@@ -431,9 +452,16 @@ InputJob *read_input_job(const char *inputfile, std::string &err)
     const std::string fmt = strip(v);
     int muxthreads = 0;   // INTERLACEDVDIF/<thread>:<thread>:... (configuration.cpp:1491-1498, 2632-2651)
     if (fmt.compare(0, 15, "INTERLACEDVDIF/") == 0 && fmt.size() > 15) {
-      muxthreads = 1;
-      for (size_t k = 15; k < fmt.size(); k++)
-        if (fmt[k] == ':') muxthreads++;
+      // the thread ids, read with atoi per ':'-separated field
+      size_t a = 15;
+      while (true) {
+        const size_t e = fmt.find(':', a);
+        if (muxthreads == GX_MAX_MUX_THREADS) { err = "more than 64 VDIF threads"; return nullptr; }
+        s.muxthread[muxthreads++] = atoi(fmt.substr(a, e == std::string::npos ? std::string::npos : e - a).c_str());
+        if (e == std::string::npos) break;
+        a = e + 1;
+      }
+      s.nmuxthreads = muxthreads;
       s.interlaced = 1;
     } else if (fmt != "VDIF") {
       err = "DATA FORMAT " + fmt + " is not implemented (VDIF and INTERLACEDVDIF only)";
@@ -687,6 +715,18 @@ InputJob *read_input_job(const char *inputfile, std::string &err)
         }
       }
     }
+  }
+  // the largest delay rate of every antenna over the polynomials as read
+  // (before the clock terms), skipping rows of negative delay (model.cpp:762-765)
+  m->maxrate.assign(m->nstations, 0.0);
+  if (m->polyorder >= 1) {
+    for (const auto &sc : m->scans)
+      for (int k = 0; k < sc.nsamples; k++)
+        for (int p = 0; p < sc.numphasecentres + 1; p++)
+          for (int a = 0; a < m->nstations; a++) {
+            const double *d = &sc.delay[(((size_t)k * (sc.numphasecentres + 1) + p) * m->nstations + a) * (m->polyorder + 1)];
+            if (std::fabs(d[1]) > std::fabs(m->maxrate[a]) && d[0] > 0.0) m->maxrate[a] = std::fabs(d[1]);
+          }
   }
   // clock terms (Model::addClockTerms, model.cpp:291-352, with isupdate = false)
   std::vector<std::vector<double>> binom(m->polyorder + 1);

@@ -237,10 +237,6 @@ gx_status gx_vdifmux_open(int input_frame_bytes, int frames_per_second, int bits
   if (flags & ~(GX_VDIFMUX_GOTOEND | GX_VDIFMUX_RESPECTGRANULARITY | GX_VDIFMUX_ENABLEVALIDITY | GX_VDIFMUX_COMPLEX |
                 GX_VDIFMUX_PROPAGATEVALIDITY))
     return GX_ERR_UNSUPPORTED;   // legacy headers are not implemented by the reference either
-  // Several channels per thread (setvdifmuxinputchannels) make the reference's
-  // output frames channels-per-thread times longer than the data the threads
-  // carry (vdifmux.c:73-80, 167); that mode is not reproduced.
-  if (channels_per_thread != 1) return GX_ERR_UNSUPPORTED;
   std::unique_ptr<gx_vdifmux> m(new gx_vdifmux());
   m->device = device;
   m->ifb = input_frame_bytes;
@@ -259,12 +255,16 @@ gx_status gx_vdifmux_open(int input_frame_bytes, int frames_per_second, int bits
     m->ids[i] = thread_ids[i];
   }
   while (m->P < nthreads) m->P *= 2;
-  m->B = bits_per_sample * m->cf * channels_per_thread;
+  // Several channels per thread (setvdifmuxinputchannels, vdifmux.c:202-242):
+  // a thread's time sample holds all its channels, the header counts P x
+  // channels, and the output payload stays P input payloads (outputDataSize
+  // is fixed at configuration, vdifmux.c:167-171).  One thread: a plain copy.
+  m->B = m->P == 1 ? 32 : bits_per_sample * m->cf * channels_per_thread;
   if (32 % m->B) return GX_ERR_UNSUPPORTED;   // a thread's time sample must pack into 32-bit words
   m->nout_chan = m->P * channels_per_thread;
   m->ids_bytes = input_frame_bytes - kHeader;
   if (m->ids_bytes % 4) return GX_ERR_ARG;
-  m->ofb = m->ids_bytes * m->nout_chan + kHeader;
+  m->ofb = m->ids_bytes * m->P + kHeader;
   m->granularity = (int)(frames_per_second / gcdll(frames_per_second, 1000000000LL));
   if (device >= 0) {
     if (cudaSetDevice(device) != cudaSuccess) return GX_ERR_CUDA;
@@ -498,6 +498,7 @@ gx_status gx_vdifmux_run(gx_vdifmux *m, const uint8_t *src, long long src_bytes,
       GX_TURN(1, 4) GX_TURN(2, 4) GX_TURN(4, 4) GX_TURN(8, 4) GX_TURN(16, 4) GX_TURN(32, 4)
       GX_TURN(1, 8) GX_TURN(2, 8) GX_TURN(4, 8) GX_TURN(8, 8) GX_TURN(16, 8) GX_TURN(32, 8)
       GX_TURN(1, 16) GX_TURN(2, 16) GX_TURN(4, 16) GX_TURN(8, 16) GX_TURN(16, 16)
+      GX_TURN(1, 32)
     }
 #undef GX_TURN
     if (!done) {   // other thread counts and sample widths: one thread per output word

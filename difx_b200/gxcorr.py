@@ -42,9 +42,10 @@ def lib():
         L.gx_server_last_error.restype = C.c_char_p
         L.gx_batch_last_error.restype = C.c_char_p
         L.gx_vdifmux_last_error.restype = C.c_char_p
+        L.gx_ring_last_error.restype = C.c_char_p
         for name in EXPORTED_SYMBOLS:
             if name not in ("gx_last_error", "gx_status_string", "gx_server_last_error", "gx_batch_last_error",
-                            "gx_vdifmux_last_error"):
+                            "gx_vdifmux_last_error", "gx_ring_last_error"):
                 getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -60,7 +61,10 @@ EXPORTED_SYMBOLS = ("gx_open", "gx_open_input", "gx_close", "gx_last_error", "gx
                     "gx_batch_info", "gx_batch_last_error", "gx_batch_close", "gx_vis_buffer",
                     "gx_vis_set_subints", "gx_vis_clear", "gx_subint_async", "gx_subint_wait", "gx_vdifmux_open",
                     "gx_vdifmux_info", "gx_vdifmux_run", "gx_vdifmux_reset_stats", "gx_vdifmux_last_error",
-                    "gx_vdifmux_close", "gx_get_pcal_layout", "gx_vis_pcal_headers")
+                    "gx_vdifmux_close", "gx_get_pcal_layout", "gx_vis_pcal_headers", "gx_ring_open",
+                    "gx_ring_geometry_get", "gx_ring_buffer", "gx_ring_read", "gx_ring_set_segment",
+                    "gx_ring_get_segment", "gx_ring_control_host", "gx_ring_subint_device", "gx_ring_last_control",
+                    "gx_ring_reset", "gx_ring_last_error", "gx_ring_close")
 
 
 def subint_device_noalloc(jd: capi.JobDesc, sd: capi.SubintDesc, dev_results_ptr: int, stream_ptr: int = 0) -> None:
@@ -437,6 +441,103 @@ class VdifMux:
         if self.m:
             lib().gx_vdifmux_close(self.m)
             self.m = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class RingGeometry(C.Structure):
+    _fields_ = [(n, C.c_int) for n in (
+        "bufferbytes", "readbytes", "numsegments", "overflowbytes", "sendbytes", "blockspersend", "controllength",
+        "blockbytes", "bytespersamplenum", "bytespersampledenom", "bytesbetweenintegerns", "nsinc", "framebytes",
+        "payloadbytes", "framespersecond", "framegranularity", "intclockseconds")] + [
+        ("sampletimens", C.c_double), ("dataspanns", C.c_longlong)]
+
+
+class RingSegment(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("scan", "scanseconds", "scanns", "validbytes", "readto", "configindex")]
+
+    def astuple(self):
+        return (self.scan, self.scanseconds, self.scanns, self.validbytes, self.readto, self.configindex)
+
+
+class Ring:
+    """Per-station data rings of a Correlator with control words computed on
+    the device (gx_ring_*): the DataStream's segmented buffer, filled by the
+    device multiplexer, walked by a kernel for every subint."""
+
+    def __init__(self, corr: Correlator, databufferfactor: int = 0, numdatasegments: int = 0):
+        self.corr = corr
+        self.r = C.c_void_p()
+        st = lib().gx_ring_open(corr.h, databufferfactor, numdatasegments, C.byref(self.r))
+        if st != 0:
+            raise GxError(st, lib().gx_last_error(corr.h).decode())
+        self.nst = corr.info.nstations if hasattr(corr, "info") else None
+
+    def _check(self, st: int):
+        if st != 0:
+            raise GxError(st, lib().gx_ring_last_error(self.r).decode())
+
+    def geometry(self, station: int) -> RingGeometry:
+        g = RingGeometry()
+        self._check(lib().gx_ring_geometry_get(self.r, station, C.byref(g)))
+        return g
+
+    def buffer_ptr(self, station: int) -> int:
+        p = C.c_void_p()
+        self._check(lib().gx_ring_buffer(self.r, station, C.byref(p)))
+        return p.value
+
+    def read(self, station: int, segment: int, scan: int, raw_ptr: int, raw_bytes: int, stream_ptr: int = 0) -> int:
+        used = C.c_longlong(0)
+        self._check(lib().gx_ring_read(self.r, station, segment, scan, C.c_void_p(raw_ptr), C.c_longlong(raw_bytes),
+                                       C.byref(used), C.c_void_p(stream_ptr) if stream_ptr else None))
+        return used.value
+
+    def set_segment(self, station: int, segment: int, seg) -> None:
+        s = RingSegment(*seg) if not isinstance(seg, RingSegment) else seg
+        self._check(lib().gx_ring_set_segment(self.r, station, segment, C.byref(s)))
+
+    def segment(self, station: int, segment: int) -> RingSegment:
+        s = RingSegment()
+        self._check(lib().gx_ring_get_segment(self.r, station, segment, C.byref(s)))
+        return s
+
+    def control_host(self, station: int, scan: int, sec: int, ns: int):
+        n = self.geometry(station).controllength
+        cw = np.zeros(n, np.int32)
+        sp = C.c_int(0)
+        st = lib().gx_ring_control_host(self.r, station, scan, sec, ns, cw.ctypes.data_as(C.c_void_p), C.byref(sp))
+        if st not in (0, 8):
+            self._check(st)
+        return cw, sp.value, st == 8
+
+    def subint_device(self, scan: int, sec: int, ns: int, scan_start_sec: float, dev_results_ptr: int,
+                      stream_ptr: int = 0) -> None:
+        st = lib().gx_ring_subint_device(self.corr.h, self.r, scan, sec, ns, C.c_double(scan_start_sec),
+                                         C.c_void_p(dev_results_ptr), C.c_void_p(stream_ptr) if stream_ptr else None)
+        if st != 0:
+            raise GxError(st, lib().gx_last_error(self.corr.h).decode())
+
+    def last_control(self, nstations: int):
+        n = self.geometry(0).controllength
+        cw = np.zeros((nstations, n), np.int32)
+        sp = np.zeros(nstations, np.int32)
+        st = lib().gx_ring_last_control(self.r, cw.ctypes.data_as(C.c_void_p), sp.ctypes.data_as(C.c_void_p))
+        if st not in (0, 8):
+            self._check(st)
+        return cw, sp, st == 8
+
+    def reset(self) -> None:
+        self._check(lib().gx_ring_reset(self.r))
+
+    def close(self) -> None:
+        if self.r:
+            lib().gx_ring_close(self.r)
+            self.r = None
 
     def __del__(self):
         try:

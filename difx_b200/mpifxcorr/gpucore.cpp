@@ -75,6 +75,15 @@ int GpuCore::build(int ci, Job &job)
       s.zoomband_localfreq[b] = c->getDLocalZoomFreqIndex(ci, ds, b);
       s.zoomband_pol[b] = c->getDZoomBandPol(ci, ds, b);
     }
+    // the VDIF threads (setDatastreamMuxInfo, configuration.cpp:2632-2651), for a ring's multiplexer
+    if (s.interlaced) {
+      s.nmuxthreads = c->getDNumMuxThreads(ci, ds);
+      if (s.nmuxthreads > GX_MAX_MUX_THREADS) {
+        err = "more than 64 VDIF threads";
+        return GX_ERR_UNSUPPORTED;
+      }
+      for (int t = 0; t < s.nmuxthreads; t++) s.muxthread[t] = c->getDMuxThreadMap(ci, ds)[t];
+    }
     s.clock_int_seconds = (int)std::floor(c->getDClockCoeff(ci, ds, 0) / 1000000.0 + 0.5);   // mode.cpp:68
     s.phase_cal_interval_hz = c->getDPhaseCalIntervalHz(ci, ds);
     s.phase_cal_base_hz = c->getDPhaseCalBaseHz(ci, ds);

@@ -49,6 +49,7 @@ extern "C" {
 #define GX_MAX_LOCAL_FREQS 64
 #define GX_MAX_BANDS 128
 #define GX_MAX_POLPRODUCTS 4
+#define GX_MAX_MUX_THREADS 64
 
 typedef enum gx_status {
   GX_OK = 0,
@@ -111,6 +112,11 @@ typedef struct gx_station_desc {
   int nzoombands;          /* sum of NUM ZOOM POLS */
   int zoomband_localfreq[GX_MAX_BANDS];            /* ZOOM BAND i INDEX */
   char zoomband_pol[GX_MAX_BANDS];                 /* ZOOM BAND i POL */
+  /* VDIF threads the station's frames arrive on (DATA FORMAT
+     INTERLACEDVDIF/<id>:<id>:..., configuration.cpp:2632-2651); 0: plain
+     VDIF, one thread of id 0.  Only gx_ring reads them (its multiplexer). */
+  int nmuxthreads;
+  int muxthread[GX_MAX_MUX_THREADS];
 } gx_station_desc;
 
 /* One baseline (BASELINE TABLE, configuration.cpp:1033-1180). */
@@ -428,6 +434,89 @@ gx_status gx_vdifmux_run(gx_vdifmux *m, const uint8_t *src, long long src_bytes,
 gx_status gx_vdifmux_reset_stats(gx_vdifmux *m);
 const char *gx_vdifmux_last_error(const gx_vdifmux *m);
 gx_status gx_vdifmux_close(gx_vdifmux *m);
+
+/* ---- Station data ring and control words computed on the device ---------- */
+
+/* The DataStream's segmented data buffer (DataStream::initialise and
+   updateConfig, datastream.cpp:116-230, 733-763, in the VDIF form of
+   vdiffile.cpp:475-493) held in device memory, one per station: DATA BUFFER
+   FACTOR x the largest data bytes of a subint, cut into NUM DATA SEGMENTS
+   segments, then the overflow region a send runs into when it wraps.
+   Segments are filled from raw single-thread VDIF frames by the device
+   multiplexer (gx_ring_read, as VDIFDataStream::dataRead, vdiffile.cpp:668-
+   860) or described by the caller (gx_ring_set_segment).  gx_ring_subint_device
+   then correlates one subint straight out of the rings: one kernel finds each
+   station's segment and send start from the device-resident segment table
+   and writes the subint's control words (first-sample time and the per-block
+   valid flags, DataStream::calculateControlParams, datastream.cpp:368-627,
+   aligned to whole multiplexed frames as VDIFDataStream::calculateControlParams
+   does, vdiffile.cpp:348-470) and data pointers into the device tables the
+   F-step reads; a second copies the wrapped part of a send into the overflow
+   region (DataStream::execute, datastream.cpp:296-305).  No host round trip
+   sits between the segment table and the F-step.  The only host inputs per
+   subint are the geometric delays at the two ends of the data span
+   (Model::calculateDelayInterpolator of order 0), from the handle's model.
+   A ring belongs to one handle and is used on one stream at a time; a
+   segment must not be refilled while a subint that reads it is in flight
+   (the reference's segment locks). */
+typedef struct gx_ring gx_ring;
+
+/* One segment (readinfo, datastream.h): the time of its first multiplexed
+   frame relative to the start of its scan, and how many bytes it holds. */
+typedef struct gx_ring_segment {
+  int scan, scanseconds, scanns;
+  int validbytes;
+  int readto;          /* nonzero once filled */
+  int configindex;     /* 0; < 0: a segment without configuration (the frame
+                          alignment then looks at the next segments) */
+} gx_ring_segment;
+
+/* Per-station quantities the DataStream derives from the configuration. */
+typedef struct gx_ring_geometry {
+  int bufferbytes, readbytes, numsegments, overflowbytes;
+  int sendbytes, blockspersend, controllength, blockbytes;
+  int bytespersamplenum, bytespersampledenom, bytesbetweenintegerns, nsinc;
+  int framebytes;        /* multiplexed frame */
+  int payloadbytes;      /* multiplexed frame payload */
+  int framespersecond;   /* multiplexed frames per second */
+  int framegranularity;  /* frames per integer nanosecond (vdifmux) */
+  int intclockseconds;
+  double sampletimens;
+  long long dataspanns;
+} gx_ring_geometry;
+
+/* Rings for every station of a handle opened with a delay model
+   (gx_open_input); buffers are zeroed as the reference's are. */
+gx_status gx_ring_open(gx_handle *h, int databufferfactor, int numdatasegments, gx_ring **out);
+gx_status gx_ring_geometry_get(const gx_ring *r, int station, gx_ring_geometry *g);
+/* Device address of a station's buffer (segment k at k x readbytes). */
+gx_status gx_ring_buffer(const gx_ring *r, int station, uint8_t **dev_buffer);
+/* VDIFDataStream::dataRead for one segment: multiplex raw single-thread
+   frames (device memory, frame-aligned) of `scan` into the segment, continuing
+   the frame numbering of the station's previous read, and set the segment's
+   time and valid bytes from the first output frame.  *consumed: raw bytes
+   used (the next read starts there).  Synchronises `stream`. */
+gx_status gx_ring_read(gx_ring *r, int station, int segment, int scan, const uint8_t *dev_raw, long long raw_bytes,
+                       long long *consumed, void *stream);
+gx_status gx_ring_set_segment(gx_ring *r, int station, int segment, const gx_ring_segment *seg);
+gx_status gx_ring_get_segment(const gx_ring *r, int station, int segment, gx_ring_segment *seg);
+/* The control words and send start of one station for a subint, computed on
+   the host from the host copy of the segment table with the host's own
+   segment position (the CPU form of the device kernel's bookkeeping).
+   control: geometry.controllength words. */
+gx_status gx_ring_control_host(gx_ring *r, int station, int scan, int sec, int ns, int32_t *control, int *startpos);
+/* One subint of the handle from the rings, results into dev_results as
+   gx_subint_device writes them; the segment positions advance on the device. */
+gx_status gx_ring_subint_device(gx_handle *h, gx_ring *r, int scan, int sec, int ns, double scan_start_sec,
+                                float *dev_results, void *stream);
+/* The control words [nstations][controllength] and send starts the last
+   gx_ring_subint_device computed (synchronises its stream).  GX_ERR_STATE if
+   a station's subint lay past every filled segment. */
+gx_status gx_ring_last_control(gx_ring *r, int32_t *control, int *startpos);
+/* Both segment positions (host and device) back to segment 0. */
+gx_status gx_ring_reset(gx_ring *r);
+const char *gx_ring_last_error(const gx_ring *r);
+gx_status gx_ring_close(gx_ring *r);
 
 /* Phase-cal section of the Core result array (configuration.cpp:2612-2620,
    core.cpp:1131-1164): offsets[s * GX_MAX_BANDS + b] is the result index of

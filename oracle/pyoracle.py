@@ -206,6 +206,68 @@ class Reference:
         return out, w.value, us.value, n
 
 
+class RefDataStream:
+    """The reference's VDIF DataStream of one datastream of a Reference
+    (ds_harness.cpp): raw frames of one scan file, dataRead per segment,
+    calculateControlParams per subint."""
+
+    GEOM = ("bufferbytes", "readbytes", "numsegments", "overflowbytes", "sendbytes", "blockspersend",
+            "controllength", "bytespersamplenum", "bytespersampledenom", "bytesbetweenintegerns", "nsinc",
+            "framegranularity", "slotbytes", "framespersecond")
+
+    def __init__(self, ref: "Reference", ds: int, raw: bytes):
+        self.ref = ref
+        self.lib = ref.lib
+        self.lib.ref_ds_open.restype = C.c_void_p
+        self.lib.ref_ds_buffer.restype = C.c_void_p
+        self._raw = (C.c_ubyte * len(raw)).from_buffer_copy(raw)
+        p = self.lib.ref_ds_open(ref.h, ds, self._raw, C.c_longlong(len(raw)))
+        if not p:
+            raise RuntimeError("reference DataStream could not take these bytes")
+        self.p = C.c_void_p(p)
+        g = (C.c_longlong * 14)()
+        d = (C.c_double * 1)()
+        self.lib.ref_ds_geometry(self.p, g, d)
+        self.geometry = dict(zip(self.GEOM, list(g)))
+        self.geometry["sampletimens"] = d[0]
+
+    def read(self, segment: int):
+        """dataRead(segment): ((raw offset, window bytes, dest bytes, start
+        frame), (scan, scanseconds, scanns, validbytes, readto)), or None once
+        the data has ended."""
+        win = (C.c_longlong * 4)()
+        seg = (C.c_int * 5)()
+        if self.lib.ref_ds_read(self.p, segment, win, seg) != 0:
+            return None
+        return tuple(win), tuple(seg)
+
+    def set_segment(self, segment: int, seg) -> None:
+        a = (C.c_int * 5)(*seg[:5])
+        self.lib.ref_ds_set_segment(self.p, segment, a)
+
+    def control(self, scan: int, sec: int, ns: int):
+        """calculateControlParams + the wrap copy: (control words, send start,
+        segment, bytes sent)."""
+        n = self.geometry["controllength"]
+        cw = np.zeros(n, np.int32)
+        info = (C.c_int * 3)()
+        self.lib.ref_ds_control(self.p, scan, sec, ns, cw.ctypes.data_as(C.c_void_p), info)
+        return cw, info[0], info[1], info[2]
+
+    def data(self, start: int, nbytes: int) -> np.ndarray:
+        """A copy of the data buffer's bytes [start, start + nbytes)."""
+        base = self.lib.ref_ds_buffer(self.p)
+        return np.ctypeslib.as_array((C.c_ubyte * nbytes).from_address(base + start)).copy()
+
+    def close(self) -> None:
+        if getattr(self, "p", None) is not None:
+            self.lib.ref_ds_close(self.p)
+            self.p = None
+
+    def __del__(self):
+        self.close()
+
+
 def _mode_blocks(fn, h, nblocks, nbands, nchan, mid_args, station):
     sp = np.zeros(2 * nblocks * nbands * nchan, np.float32)
     dw = np.zeros(nblocks, np.float32)
@@ -276,7 +338,7 @@ def vmux_available() -> bool:
 
 
 def ref_vdifmux(src: bytes, dest_bytes: int, frame_bytes: int, fps: int, bits: int, thread_ids, nsort: int,
-                ngap: int, flags: int, start_frame: int = -1, dest_init: int = 0):
+                ngap: int, flags: int, start_frame: int = -1, dest_init: int = 0, channels_per_thread: int = 1):
     """The reference's vdifmux on host buffers: (output bytes, array of 23
     values in the order of vdifmux_harness.c: statistics, return value, output
     frame bytes, nanoseconds of the call)."""
@@ -285,8 +347,8 @@ def ref_vdifmux(src: bytes, dest_bytes: int, frame_bytes: int, fps: int, bits: i
     srcb = (C.c_ubyte * len(src)).from_buffer_copy(src)
     ids = (C.c_int * len(thread_ids))(*thread_ids)
     out = (C.c_longlong * 23)()
-    rv = lib.ref_vdifmux(dest, dest_bytes, srcb, len(src), frame_bytes, fps, bits, len(thread_ids), ids, nsort, ngap,
-                         flags, C.c_longlong(start_frame), out)
+    rv = lib.ref_vdifmux_channels(dest, dest_bytes, srcb, len(src), frame_bytes, fps, bits, len(thread_ids), ids,
+                                  nsort, ngap, flags, C.c_longlong(start_frame), channels_per_thread, out)
     if rv < 0:
         raise RuntimeError(f"reference vdifmux failed: {rv}")
     return bytes(dest), list(out)

@@ -126,6 +126,7 @@ void *ref_open(const char *inputfile)
   return j;
 }
 
+Configuration *ref_job_config(void *h) { return ((RefJob *)h)->config; }
 int ref_num_threads(void *h) { return ((RefJob *)h)->nthreads; }
 int ref_result_length(void *h) { return ((RefJob *)h)->config->getCoreResultLength(0); }
 int ref_blocks_per_send(void *h) { return ((RefJob *)h)->config->getBlocksPerSend(0); }

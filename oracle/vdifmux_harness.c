@@ -9,14 +9,17 @@
 /* out[0..19]: the statistics in the order of gx_vdifmux_stats (accumulated
  * over this one call), out[20]: vdifmux's return value, out[21]: output frame
  * bytes, out[22]: nanoseconds the vdifmux call took. */
-int ref_vdifmux(unsigned char *dest, int dest_bytes, const unsigned char *src, int src_bytes, int frame_bytes,
-                int frames_per_second, int bits, int nthreads, const int *thread_ids, int nsort, int ngap,
-                int flags, long long start_frame, long long *out)
+int ref_vdifmux_channels(unsigned char *dest, int dest_bytes, const unsigned char *src, int src_bytes,
+                         int frame_bytes, int frames_per_second, int bits, int nthreads, const int *thread_ids,
+                         int nsort, int ngap, int flags, long long start_frame, int channels_per_thread,
+                         long long *out)
 {
   struct vdif_mux vm;
   struct vdif_mux_statistics st;
   int rv = configurevdifmux(&vm, frame_bytes, frames_per_second, bits, nthreads, thread_ids, nsort, ngap, flags);
   if (rv < 0) return rv;
+  /* several recorded bands per thread, as VDIFDataStream::initialiseFile sets them (vdiffile.cpp:533-546) */
+  if (channels_per_thread > 1 && (rv = setvdifmuxinputchannels(&vm, channels_per_thread)) < 0) return rv;
   resetvdifmuxstatistics(&st);
   struct timespec t0, t1;
   clock_gettime(CLOCK_MONOTONIC, &t0);
@@ -46,4 +49,12 @@ int ref_vdifmux(unsigned char *dest, int dest_bytes, const unsigned char *src, i
   out[20] = rv;
   out[21] = vm.outputFrameSize;
   return rv < 0 ? rv : 0;
+}
+
+int ref_vdifmux(unsigned char *dest, int dest_bytes, const unsigned char *src, int src_bytes, int frame_bytes,
+                int frames_per_second, int bits, int nthreads, const int *thread_ids, int nsort, int ngap,
+                int flags, long long start_frame, long long *out)
+{
+  return ref_vdifmux_channels(dest, dest_bytes, src, src_bytes, frame_bytes, frames_per_second, bits, nthreads,
+                              thread_ids, nsort, ngap, flags, start_frame, 1, out);
 }

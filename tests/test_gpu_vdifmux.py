@@ -28,6 +28,11 @@ CASES = {
     # (24 threads: the reference's presence mask is built with int shifts, vdifmux.c:742-750, so it
     # cannot describe thread 31 and above)
     "24thr_1bit": dict(ids=list(range(24)), nbits=1, flags=DS_FLAGS, pert=PERTURB),
+    # several recorded bands per thread (setvdifmuxinputchannels, as the VDIF
+    # DataStream sets it when bands outnumber threads): one thread of 8 bands
+    # (a plain copy) and 2 threads of 2 bands (4-bit time samples per thread)
+    "1thr_8ch_2bit": dict(ids=[0], nbits=2, flags=DS_FLAGS, pert=PERTURB, chans=8),
+    "2thr_2ch_2bit": dict(ids=[0, 1], nbits=2, flags=DS_FLAGS, pert=PERTURB, chans=2),
 }
 
 FIELDS = ["valid_frames", "invalid_frames", "discarded_frames", "wrong_thread_frames", "skipped_bytes", "fill_bytes",
@@ -43,9 +48,11 @@ def test_device_mux_matches_reference(case, dest_frames):
     from difx_b200.gxcorr import VdifMux
     c = CASES[case]
     fb, fps, nsort, ngap = 1032, 1000, 16, 250
-    ids, nbits, cplx = c["ids"], c["nbits"], c.get("cplx", False)
-    src = vs.stream(ids, 60, fb, fps, nbits, seed=11 + sorted(CASES).index(case), start_frame=7, cplx=cplx, **c["pert"])
-    m = VdifMux(fb, fps, nbits, ids, nsort=nsort, ngap=ngap, flags=c["flags"])
+    ids, nbits, cplx, chans = c["ids"], c["nbits"], c.get("cplx", False), c.get("chans", 1)
+    # enough frames that every perturbation occurs with few threads too
+    src = vs.stream(ids, max(60, 240 // len(ids)), fb, fps, nbits, seed=11 + sorted(CASES).index(case), start_frame=7,
+                    cplx=cplx, chans=chans, **c["pert"])
+    m = VdifMux(fb, fps, nbits, ids, nsort=nsort, ngap=ngap, flags=c["flags"], channels_per_thread=chans)
     ofb = m.output_frame_bytes
     dest_bytes = ofb * dest_frames
     d_src = torch.frombuffer(bytearray(src), dtype=torch.uint8).cuda()
@@ -55,13 +62,14 @@ def test_device_mux_matches_reference(case, dest_frames):
     P = 1
     while P < len(ids):
         P *= 2
-    B = nbits * (2 if cplx else 1)
+    B = nbits * (2 if cplx else 1) * chans
     pad_bits = P != len(ids)   # some corner turners leave the padding slots untouched (scratch stays there)
     for call in range(4):
         if idx >= len(src) - fb:
             break
         chunk = src[idx:idx + window]
-        ref_out, ref = pyoracle.ref_vdifmux(chunk, dest_bytes, fb, fps, nbits, ids, nsort, ngap, c["flags"], start)
+        ref_out, ref = pyoracle.ref_vdifmux(chunk, dest_bytes, fb, fps, nbits, ids, nsort, ngap, c["flags"], start,
+                                            channels_per_thread=chans)
         d_dest.zero_()
         st = m.run(d_src.data_ptr() + idx, len(chunk), d_dest.data_ptr(), dest_bytes, start)
         # the reference's statistics accumulate only within its call here

@@ -50,8 +50,15 @@ def test_open_arguments_and_geometry():
     m = gxcorr.VdifMux(1032, 3, 8, [0, 1], device=-1)
     assert m.frame_granularity == 3
     m.close()
-    with pytest.raises(gxcorr.GxError) as ei:
-        gxcorr.VdifMux(1032, 1000, 2, [0, 1], channels_per_thread=2, device=-1)
+    # several channels per thread: the header counts them, the payload stays P input payloads
+    m = gxcorr.VdifMux(1032, 1000, 2, [0, 1], channels_per_thread=2, device=-1)
+    assert m.output_channels == 4 and m.output_frame_bytes == 1000 * 2 + 32
+    m.close()
+    m = gxcorr.VdifMux(8032, 4000, 8, [0], channels_per_thread=8, device=-1)
+    assert m.output_channels == 8 and m.output_frame_bytes == 8032
+    m.close()
+    with pytest.raises(gxcorr.GxError) as ei:   # 8 x 8-bit bands per thread do not pack into 32-bit words
+        gxcorr.VdifMux(1032, 1000, 8, [0, 1], channels_per_thread=8, device=-1)
     assert ei.value.status == 2
     with pytest.raises(gxcorr.GxError) as ei:
         gxcorr.VdifMux(1032, 1000, 2, [0, 1], flags=0x08, device=-1)   # legacy input headers

@@ -9,17 +9,20 @@ import numpy as np
 FILL = 0x11223344
 
 
-def header(seconds, frame, thread, nbits, frame_bytes, invalid=False, epoch=40, station=0x4142, cplx=False):
+def header(seconds, frame, thread, nbits, frame_bytes, invalid=False, epoch=40, station=0x4142, cplx=False,
+           log2chans=0):
     w0 = (seconds & 0x3FFFFFFF) | (int(invalid) << 31)
     w1 = (frame & 0xFFFFFF) | (epoch << 24)
-    w2 = (frame_bytes // 8) & 0xFFFFFF            # one channel, version 0
+    w2 = ((frame_bytes // 8) & 0xFFFFFF) | (log2chans << 24)   # version 0
     w3 = (station & 0xFFFF) | ((thread & 1023) << 16) | ((nbits - 1) << 26) | (int(cplx) << 31)
     return struct.pack("<8I", w0, w1, w2, w3, 0, 0, 0, 0)
 
 
 def stream(thread_ids, nframes, frame_bytes, fps, nbits, seed, start_sec=1000, start_frame=0, invalid_frac=0.0,
-           drop_frac=0.0, dup_frac=0.0, swap_frac=0.0, fill_frac=0.0, stray_frac=0.0, cplx=False):
-    """Bytes of nframes frame times of every thread, perturbed as asked."""
+           drop_frac=0.0, dup_frac=0.0, swap_frac=0.0, fill_frac=0.0, stray_frac=0.0, cplx=False, chans=1):
+    """Bytes of nframes frame times of every thread (chans channels each, a
+    power of two), perturbed as asked."""
+    lc = chans.bit_length() - 1
     rng = np.random.default_rng(seed)
     payload = frame_bytes - 32
     frames = []
@@ -31,12 +34,12 @@ def stream(thread_ids, nframes, frame_bytes, fps, nbits, seed, start_sec=1000, s
                 continue
             body = rng.integers(0, 256, payload, dtype=np.uint8).tobytes()
             inv = rng.random() < invalid_frac
-            frames.append(header(sec, fr, t, nbits, frame_bytes, inv, cplx=cplx) + body)
+            frames.append(header(sec, fr, t, nbits, frame_bytes, inv, cplx=cplx, log2chans=lc) + body)
             if rng.random() < dup_frac:   # a second copy with other samples: the first must win
-                frames.append(header(sec, fr, t, nbits, frame_bytes, False, cplx=cplx) +
+                frames.append(header(sec, fr, t, nbits, frame_bytes, False, cplx=cplx, log2chans=lc) +
                               rng.integers(0, 256, payload, dtype=np.uint8).tobytes())
             if rng.random() < stray_frac:
-                frames.append(header(sec, fr, 1000, nbits, frame_bytes, False, cplx=cplx) + body)
+                frames.append(header(sec, fr, 1000, nbits, frame_bytes, False, cplx=cplx, log2chans=lc) + body)
     for i in range(len(frames) - 1):
         if rng.random() < swap_frac:
             frames[i], frames[i + 1] = frames[i + 1], frames[i]
