@@ -58,7 +58,7 @@ static void free_all(gx_handle *h)
                   h->d_tcrows, h->d_err, h->d_full, h->d_avgtab, h->d_pcal, h->d_pcalbins, h->d_zrows,
                   h->d_zprods, h->d_specz, h->d_accz, h->d_uvents, h->d_uvfreqs, h->d_binents, h->d_binitems,
                   h->d_binwout, h->d_autoprods, h->d_autowents, h->d_binphase, h->d_binweight, h->d_accb,
-                  h->d_wbins};
+                  h->d_wbins, h->d_pcalrot};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->h_err) cudaFreeHost(h->h_err);
@@ -466,6 +466,7 @@ static gx_status setup(gx_handle *h)
   // (PCal::getNew, pcal.cpp:191-260; the implicit-shift ones are built)
   std::vector<std::vector<int>> pc_ntones(d.nstations);
   h->pcal.clear();
+  h->pcal_rot.clear();
   h->pc_tone_hz.assign((size_t)d.nstations * GX_MAX_BANDS, {});
   h->pc_maxtones.assign(d.nstations, 0);
   for (int s = 0; s < d.nstations; s++) {
@@ -507,19 +508,62 @@ static gx_status setup(gx_handle *h)
       P.band = b;
       P.ntones = n;
       P.nbins = 0;
+      P.nextract = n;
       if (offset >= 0) {
+        // the extractor PCal::getNew picks (pcal.cpp:191-260): offset and
+        // spacing periods No and Np (No at least the 1 MHz resolution,
+        // PCal::setMinFrequencyResolution, mode.cpp:403), tones per PCal::calcNumTones
         const long long bwhz = (long long)(1e6 * bw);
         const long long fs = cplx ? bwhz : 2 * bwhz;
-        if (offset == 0) return h->fail(GX_ERR_UNSUPPORTED, "phase-cal tone at DC (the trivial extractor) is not implemented");
-        const long long No = fs / gcdl(fs, offset), Np = fs / gcdl(fs, interval);
-        if (No % Np != 0)
-          return h->fail(GX_ERR_UNSUPPORTED, "phase-cal offsets that need the shifting extractor are not implemented");
-        long long nb = No;
-        while (fs / (2 * nb) > 1000000) nb *= 2;   // PCal::setMinFrequencyResolution(1e6), mode.cpp:403
+        long long No = fs / gcdl(fs, offset);
+        const long long Np = fs / gcdl(fs, interval);
+        while (fs / (2 * No) > 1000000) No *= 2;
+        int nt = 0;   // PCal::calcNumTones (pcal.cpp:317-335): tones in [offset, bw], a DC tone and a top-edge one counted once
+        long long ftone = offset;
+        while (ftone <= bwhz) {
+          nt++;
+          ftone += interval;
+        }
+        if (offset == 0 && ftone - interval == bwhz) nt--;
+        long long nb = 0;
+        if (nt == 0) {
+          nb = 0;   // PCalExtractorDummy: zeros
+        } else if (!cplx && offset == 0) {
+          // PCalExtractorTrivial (pcal.cpp:427-575): bins of the spacing period, tone i at bin (i + 1) step
+          nb = fs / gcdl(fs, interval);
+          P.step = (int)(interval / gcdl(fs, interval));
+          P.offset_bin = P.step;
+          P.nextract = nt - 1;
+        } else if (No % Np == 0) {
+          // the implicit-shift extractors (pcal.cpp:1032-1222, 1419-1600)
+          nb = fs / gcdl(fs, offset);
+          while (fs / (2 * nb) > 1000000) nb *= 2;
+          P.step = (int)std::floor((double)nb * (double)interval / (double)fs);
+          P.offset_bin = (int)std::floor((double)nb * (double)offset / (double)fs);
+          P.nextract = nt;
+        } else {
+          // the shifting extractors (pcal.cpp:583-800 real, 806-1025 complex): the
+          // samples mixed down by the offset with an FP32 oscillator table, bins
+          // of the spacing period, tone i at bin i step
+          nb = fs / gcdl(fs, interval);
+          if (cplx)
+            while (fs / (2 * nb) > 1000000) nb *= 2;
+          const long long lo = fs / gcdl(fs, offset);
+          const long long L = nb * lo / gcdl(lo, nb);
+          if (L > (1LL << 22)) return h->fail(GX_ERR_UNSUPPORTED, "phase-cal oscillator period above 4M samples");
+          P.step = (int)std::floor((double)nb * (double)interval / (double)fs);
+          P.offset_bin = 0;
+          P.nextract = nt;
+          P.rotlen = (int)L;
+          P.rot0 = (long long)h->pcal_rot.size();
+          const double dphi = -2 * M_PI * (double)offset / (double)fs;
+          for (long long m = 0; m < 2 * L; m++) {
+            const double arg = dphi * double(m);
+            h->pcal_rot.push_back(make_float2((float)std::cos(arg), (float)std::sin(arg)));
+          }
+        }
         if (nb > 65536) return h->fail(GX_ERR_UNSUPPORTED, "more than 65536 phase-cal bins");
         P.nbins = (int)nb;
-        P.step = (int)std::floor((double)nb * (double)interval / (double)fs);
-        P.offset_bin = (int)std::floor((double)nb * (double)offset / (double)fs);
       }
       h->pcal.push_back(P);
     }
@@ -1076,6 +1120,7 @@ static gx_status setup(gx_handle *h)
     h->pcal_per_station = J.nbands;
     for (size_t i = 0; i < h->pcal.size(); i++)
       if (h->pcal.size() % J.nbands || h->pcal[i].nbins != h->pcal[0].nbins || h->pcal[i].nbins <= 0 ||
+          h->pcal[i].rotlen > 0 ||
           h->pcal[i].station != h->pcal[i - i % J.nbands].station || h->pcal[i].band != (int)(i % J.nbands))
         h->pcal_per_station = 0;
     if (h->pcal_per_station) {   // chunks for about eight 256-thread CTAs per SM
@@ -1084,6 +1129,10 @@ static gx_status setup(gx_handle *h)
     }
     CKR(h, h->dalloc(&h->d_pcal, sizeof(PcalBand) * h->pcal.size()));
     CKR(h, cudaMemcpy(h->d_pcal, h->pcal.data(), sizeof(PcalBand) * h->pcal.size(), cudaMemcpyHostToDevice));
+    if (!h->pcal_rot.empty()) {
+      CKR(h, h->dalloc(&h->d_pcalrot, sizeof(float2) * h->pcal_rot.size()));
+      CKR(h, cudaMemcpy(h->d_pcalrot, h->pcal_rot.data(), sizeof(float2) * h->pcal_rot.size(), cudaMemcpyHostToDevice));
+    }
     CKR(h, h->dalloc(&h->d_pcalbins, sizeof(float2) * (size_t)h->pcal_chunks * h->pcal.size() * h->pcal_maxbins));
   }
   if (h->avg > 1) {
@@ -1521,7 +1570,7 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
     if ((r = mark(0, true)) != GX_OK) return r;
     CKR(h, fstep_launch(J, h->d_st, h->maxnrf, S, b0, nb, h->nslots, h->d_spec, h->d_w, h->d_bp, st));
     if (npc) {
-      CKR(h, pcal_bins_launch(J, S, h->d_bp, nb, h->d_pcal, npc, h->pcal_per_station, h->pcal_chunks,
+      CKR(h, pcal_bins_launch(J, S, h->d_bp, nb, h->d_pcal, h->d_pcalrot, npc, h->pcal_per_station, h->pcal_chunks,
                               h->pcal_maxbins, h->d_pcalbins, st));
       h->launches += 1;
     }

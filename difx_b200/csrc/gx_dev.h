@@ -104,9 +104,14 @@ struct SubintArrays {
 // extractors, pcal.cpp:1032-1222 real, 1419-1600 complex): sample n of a block
 // whose absolute sample number is S goes to bin (S + n) mod nbins; tone t is
 // bin offset_bin + t * step of the bins' forward DFT (0 past nbins).
+// Shifting extractors (rotlen > 0): each sample is first multiplied by
+// rot[rot0 + (S mod rotlen) + (n mod rotlen)], the FP32 oscillator of the
+// reference (2 rotlen entries).  Tones t >= nextract stay zero.
 struct PcalBand {
   int station, band, nbins, ntones, offset_bin, step;
   long long result_offset;   // first tone in the full-resolution result array
+  int nextract, rotlen;
+  long long rot0;
 };
 
 // Raises `kernel`'s dynamic shared-memory limit on the current device to at
@@ -118,7 +123,8 @@ cudaError_t smem_opt_in(const void *kernel, size_t bytes);
 // Phase-cal: bin sums of one pass of blocks (added into partial[chunk][band][bin]),
 // then the tones of all bands into the result array.
 cudaError_t pcal_bins_launch(const DevJob &J, const SubintArrays &S, const BlockParam *bp, int nblk,
-                             const PcalBand *bands, int nbands, int per_station, int chunks, int maxbins,
+                             const PcalBand *bands, const float2 *rot, int nbands, int per_station, int chunks,
+                             int maxbins,
                              float2 *partial, cudaStream_t st);
 cudaError_t pcal_tones_launch(const PcalBand *bands, int nbands, int chunks, int maxbins, const float2 *partial,
                               float2 *results, cudaStream_t st);

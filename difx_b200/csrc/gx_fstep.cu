@@ -987,9 +987,58 @@ __device__ __forceinline__ float2 sum_samples(const DevJob &J, const uint8_t *__
   return acc;
 }
 
+// The shifting extractors' form (pcal.cpp:692-740, 906-955): every sample
+// times the oscillator entry (S mod L) + (n mod L) of the reference's table of
+// 2 L FP32 values, then summed; S: the block's absolute sample number.
+__device__ __forceinline__ float2 sum_samples_rot(const DevJob &J, const uint8_t *__restrict__ data,
+                                                  const BlockParam &P, int bd, int n0, int step, const float *lut,
+                                                  const float2 *__restrict__ rot, int L, int sl)
+{
+  float2 acc = make_float2(0.f, 0.f);
+  if (n0 >= J.fftlen) return acc;
+  const int fsamp = J.framesamples;
+  const int bits_ts = J.nbands * J.nbits * (J.cplx ? 2 : 1);
+  const int cmask = (1 << J.nbits) - 1;
+  const int bitband = bd * (J.cplx ? 2 : 1) * J.nbits;
+  const int smp0 = P.nearestsample + n0;
+  int q = smp0 / fsamp;
+  int r = smp0 - q * fsamp;
+  q -= P.fr0;
+  const int qstep = step / fsamp, rstep = step - qstep * fsamp;
+  const int lstep = step % L;
+  int nl = n0 % L;
+  for (int n = n0; n < J.fftlen; n += step) {
+    if ((P.validmask >> q) & 1ull) {
+      const uint8_t *payload = data + ((long long)P.fr0 + q) * J.framebytes + 32;
+      const int bit0 = r * bits_ts + bitband;
+      const float xr = lut[(__ldg(payload + (bit0 >> 3)) >> (bit0 & 7)) & cmask];
+      const float2 o = __ldg(rot + sl + nl);
+      if (J.cplx) {
+        const int bit1 = bit0 + J.nbits;
+        const float xi = lut[(__ldg(payload + (bit1 >> 3)) >> (bit1 & 7)) & cmask];
+        acc.x += xr * o.x - xi * o.y;
+        acc.y += xr * o.y + xi * o.x;
+      } else {
+        acc.x += xr * o.x;
+        acc.y += xr * o.y;
+      }
+    }
+    q += qstep;
+    r += rstep;
+    if (r >= fsamp) {
+      r -= fsamp;
+      q++;
+    }
+    nl += lstep;
+    if (nl >= L) nl -= L;
+  }
+  return acc;
+}
+
 __global__ void __launch_bounds__(256) pcal_bins_kernel(DevJob J, SubintArrays S, const BlockParam *__restrict__ bp,
-                                                        int nblk, const PcalBand *__restrict__ bands, int chunks,
-                                                        int maxbins, float2 *__restrict__ partial)
+                                                        int nblk, const PcalBand *__restrict__ bands,
+                                                        const float2 *__restrict__ rot, int chunks, int maxbins,
+                                                        float2 *__restrict__ partial)
 {
   __shared__ float s_lut[256];
   __shared__ float2 s_red[256];
@@ -1018,8 +1067,13 @@ __global__ void __launch_bounds__(256) pcal_bins_kernel(DevJob J, SubintArrays S
       for (int bi = b0; bi < b1; bi++) {
         const BlockParam P = band_param(bp, S, s, nblk, bi, J.nbands, B.band);
         if (P.state == 0) continue;
-        const int idx0 = (int)((s0 + (unsigned long long)P.nearestsample) % (unsigned long long)N);
-        const float2 v = sum_samples(J, data, P, B.band, (k - idx0 + N) % N + r * N, R * N, s_lut);
+        const unsigned long long sb = s0 + (unsigned long long)P.nearestsample;
+        const int idx0 = (int)(sb % (unsigned long long)N);
+        const float2 v =
+            B.rotlen > 0
+                ? sum_samples_rot(J, data, P, B.band, (k - idx0 + N) % N + r * N, R * N, s_lut, rot + B.rot0, B.rotlen,
+                                  (int)(sb % (unsigned long long)B.rotlen))
+                : sum_samples(J, data, P, B.band, (k - idx0 + N) % N + r * N, R * N, s_lut);
         acc.x += v.x;
         acc.y += v.y;
       }
@@ -1041,8 +1095,11 @@ __global__ void __launch_bounds__(256) pcal_bins_kernel(DevJob J, SubintArrays S
       for (int bi = b0; bi < b1; bi++) {
         const BlockParam P = band_param(bp, S, s, nblk, bi, J.nbands, B.band);
         if (P.state == 0) continue;
-        const int idx0 = (int)((s0 + (unsigned long long)P.nearestsample) % (unsigned long long)N);
-        const float2 v = sum_samples(J, data, P, B.band, (k - idx0 + N) % N, N, s_lut);
+        const unsigned long long sb = s0 + (unsigned long long)P.nearestsample;
+        const int idx0 = (int)(sb % (unsigned long long)N);
+        const float2 v = B.rotlen > 0 ? sum_samples_rot(J, data, P, B.band, (k - idx0 + N) % N, N, s_lut, rot + B.rot0,
+                                                        B.rotlen, (int)(sb % (unsigned long long)B.rotlen))
+                                      : sum_samples(J, data, P, B.band, (k - idx0 + N) % N, N, s_lut);
         acc.x += v.x;
         acc.y += v.y;
       }
@@ -1264,7 +1321,7 @@ __global__ void __launch_bounds__(128) pcal_tones_kernel(const PcalBand *__restr
   for (int t = threadIdx.x; t < B.ntones; t += blockDim.x) {
     const long long bin = (long long)B.offset_bin + (long long)t * B.step;
     double re = 0.0, im = 0.0;
-    if (B.nbins > 0 && bin < B.nbins) {
+    if (B.nbins > 0 && bin < B.nbins && t < B.nextract) {
       for (int k = 0; k < B.nbins; k++) {
         float bx = 0.f, by = 0.f;   // the bin, summed over the chunks in order
         for (int c = 0; c < chunks; c++) {
@@ -1284,7 +1341,8 @@ __global__ void __launch_bounds__(128) pcal_tones_kernel(const PcalBand *__restr
 }
 
 cudaError_t pcal_bins_launch(const DevJob &J, const SubintArrays &S, const BlockParam *bp, int nblk,
-                             const PcalBand *bands, int nbands, int per_station, int chunks, int maxbins,
+                             const PcalBand *bands, const float2 *rot, int nbands, int per_station, int chunks,
+                             int maxbins,
                              float2 *partial, cudaStream_t st)
 {
   if (nbands <= 0 || nblk <= 0) return cudaSuccess;
@@ -1314,7 +1372,7 @@ cudaError_t pcal_bins_launch(const DevJob &J, const SubintArrays &S, const Block
     else if (W == 2) GX_PCAL_STATION(2, 0, 0);
     else GX_PCAL_STATION(1, 0, 0);
   } else {
-    pcal_bins_kernel<<<dim3(chunks, nbands), 256, 0, st>>>(J, S, bp, nblk, bands, chunks, maxbins, partial);
+    pcal_bins_kernel<<<dim3(chunks, nbands), 256, 0, st>>>(J, S, bp, nblk, bands, rot, chunks, maxbins, partial);
   }
 #undef GX_PCAL_STATION
   return cudaGetLastError();

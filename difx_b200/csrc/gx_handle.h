@@ -36,6 +36,8 @@ struct gx_handle {
   float2 *d_full = nullptr;
   std::vector<gx::PcalBand> pcal;            // recorded bands with phase-cal extraction
   gx::PcalBand *d_pcal = nullptr;
+  std::vector<float2> pcal_rot;              // shifting extractors' oscillator tables (2 rotlen each)
+  float2 *d_pcalrot = nullptr;
   float2 *d_pcalbins = nullptr;              // [chunk][pcal band][bin] partial bin sums
   int pcal_chunks = 0, pcal_maxbins = 0, pcal_per_station = 0;
   std::vector<int> pc_off, pc_ntones;        // [station * GX_MAX_BANDS + band]: result index / tones

@@ -399,6 +399,13 @@ PCAL_CASES = {
     "real2_16band_pcal": lambda: (jobs.spec_c1(name="c1pc16", seed=85, nstations=3, pcal_interval_mhz=1,
                                                subbands=[jobs.Subband(8400.0 + 16 * i, 16.0, "U", 128)
                                                          for i in range(8)]), dict(invalid_frac=0.03)),
+    # 3 MHz tones: the subbands' first-tone offsets (1, 2 and 3 MHz) make the
+    # reference pick the implicit-shift extractor for some bands and the
+    # shifting one (the samples mixed down by the offset, pcal.cpp:583-1025)
+    # for others: real USB, real LSB, complex
+    "c1_pcal3": lambda: (jobs.spec_c1(name="c1pc3", seed=88, pcal_interval_mhz=3), dict(invalid_frac=0.03)),
+    "lsb_pcal3": lambda: (jobs.spec_lsb(name="lsbpc3", seed=89, pcal_interval_mhz=3), dict(invalid_frac=0.03)),
+    "cplx8_pcal3": lambda: (jobs.spec_cplx8(name="cx8pc3", seed=90, pcal_interval_mhz=3), dict(invalid_frac=0.03)),
 }
 PCAL_TOL = 1e-4   # FP32 bin sums (tens of thousands of samples per bin) formed in another order
 
@@ -406,10 +413,11 @@ PCAL_TOL = 1e-4   # FP32 bin sums (tens of thousands of samples per bin) formed 
 @pytest.mark.skipif(not pyoracle.reference_available(), reason="reference harness not built")
 @pytest.mark.parametrize("case", sorted(PCAL_CASES))
 def test_gpu_phase_cal_matches_reference(case, gx, oracle_lib):
-    """Phase-cal tones (PHASE CAL INT 1 MHz; the reference's implicit-shift
-    extractors, pcal.cpp:1032-1600, called from mode.cpp:759-774 and copied by
-    core.cpp:1131-1164) in the Core result array, against the compiled
-    reference reading the same .input; the rest of the array as usual."""
+    """Phase-cal tones (PHASE CAL INT 1 or 3 MHz; the reference's
+    implicit-shift and shifting extractors, pcal.cpp:583-1600, called from
+    mode.cpp:759-774 and copied by core.cpp:1131-1164) in the Core result
+    array, against the compiled reference reading the same .input; the rest
+    of the array as usual."""
     spec, kw = PCAL_CASES[case]()
     prep = jobs.prepare(spec, [100_000_000, 108_000_000], **kw)
     c = gx.Correlator.from_desc(prep.jd)
