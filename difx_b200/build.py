@@ -20,7 +20,7 @@ LIB = os.path.join(HERE, "libgxcorr.so")
 BUILD = os.path.join(HERE, "_build")
 
 SOURCES = ["gx_fstep.cu", "gx_fstep_sb.cu", "gx_xstep.cu", "gx_tcxmac.cu", "gx_noalloc.cu", "gx_vis.cu", "gx_api.cpp", "gx_input.cpp",
-           "gx_server.cpp", "gx_batch.cpp", "gx_vdifmux.cu", "gx_ring.cu"]
+           "gx_server.cpp", "gx_batch.cpp", "gx_vdifmux.cu", "gx_ring.cu", "gx_monitor.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

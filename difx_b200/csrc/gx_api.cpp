@@ -625,6 +625,21 @@ static gx_status setup(gx_handle *h)
   // the kernels fill the full-resolution array; the averaged one is the result
   h->rl_full = build(1, h->blofs_full, h->bwofs_full, h->acofs_full, h->acwofs_full, h->bsdofs_full);
   h->rl = build(avg, h->blofs, h->bwofs, h->acofs, h->acwofs, h->bsdofs);
+  // each recorded band's autocorrelation record and weight (for gx_sta)
+  h->sta_acoff.assign((size_t)d.nstations * GX_MAX_BANDS, -1);
+  h->sta_acw.assign((size_t)d.nstations * GX_MAX_BANDS, -1);
+  for (int s = 0; s < d.nstations; s++) {
+    long long o = h->acofs[s];
+    int p = 0;
+    for (int k : ac_bands(s)) {
+      if (k < d.stations[s].nbands) {
+        h->sta_acoff[(size_t)s * GX_MAX_BANDS + k] = (int)o;
+        h->sta_acw[(size_t)s * GX_MAX_BANDS + k] = p;
+      }
+      o += d.freqs[total_freq(d.stations[s], k)].nchan / avg;
+      p++;
+    }
+  }
   h->bsd_first = h->bsd_count = 0;
   if (h->maxpc > 1) {
     long long lo = -1, hi = -1;
@@ -1305,6 +1320,7 @@ gx_status gx_close(gx_handle *h)
     if (h->stream) cudaStreamSynchronize(h->stream);
   }
   free_all(h);
+  if (h->kurt) gx_kurtosis_free(h->kurt);
   delete h;
   return GX_OK;
 }
@@ -1569,6 +1585,7 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
     gx_status r;
     if ((r = mark(0, true)) != GX_OK) return r;
     CKR(h, fstep_launch(J, h->d_st, h->maxnrf, S, b0, nb, h->nslots, h->d_spec, h->d_w, h->d_bp, st));
+    if (h->kurt && (r = gx_kurtosis_pass(h, nb, st)) != GX_OK) return r;
     if (npc) {
       CKR(h, pcal_bins_launch(J, S, h->d_bp, nb, h->d_pcal, h->d_pcalrot, npc, h->pcal_per_station, h->pcal_chunks,
                               h->pcal_maxbins, h->d_pcalbins, st));
@@ -1603,6 +1620,7 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
     return GX_OK;
   };
   const int nph = h->cur_npc[k];
+  if (h->kurt && (r = gx_kurtosis_begin(h, st)) != GX_OK) return r;
   if (nph > 1) {
     // Multiple phase centres (Core::processdata / uvshiftAndAverage,
     // core.cpp:984-991, 1431-1938): the accumulators of each uv-shift interval
@@ -1626,6 +1644,7 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
     for (int b0 = 0; b0 < J.blocks_per_send; b0 += h->chunk)
       if ((r = pass(b0, std::min(h->chunk, J.blocks_per_send - b0))) != GX_OK) return r;
   }
+  if (h->kurt && (r = gx_kurtosis_end(h, st)) != GX_OK) return r;
   if ((r = mark(2, true)) != GX_OK) return r;
   if (nph > 1) {
     // baseline and autocorrelation weights; the shift decorrelation factors

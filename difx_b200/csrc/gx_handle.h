@@ -151,6 +151,8 @@ struct gx_handle {
   std::vector<int> ev_stage;
   int launches = 0;
 
+  std::vector<int> sta_acoff, sta_acw;   // [station * GX_MAX_BANDS + recorded band]: autocorrelation record, weight (-1: none)
+  struct gx_kurtosis_state *kurt = nullptr;   // gx_set_kurtosis
   std::unique_ptr<HostModel> model;  // only for gx_open_input
   std::unique_ptr<gx::JobMeta> meta; // only for gx_open_input
   std::vector<gx::DevStation> dst;   // host copy of the per-station device constants
@@ -195,3 +197,9 @@ gx_status gx_stage_subint(gx_handle *h, const gx_subint_desc *sub, const uint8_t
 gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st);
 // The ring walk of h->ring_req over the copied tables (gx_ring.cu).
 gx_status gx_ring_enqueue_control(struct gx_ring *r, gx_handle *h, cudaStream_t st);
+// Spectral kurtosis of the recorded bands (gx_monitor.cu): zero the sums,
+// add one pass of spectra, finish the subint.
+gx_status gx_kurtosis_begin(gx_handle *h, cudaStream_t st);
+gx_status gx_kurtosis_pass(gx_handle *h, int nblk, cudaStream_t st);
+gx_status gx_kurtosis_end(gx_handle *h, cudaStream_t st);
+void gx_kurtosis_free(struct gx_kurtosis_state *k);

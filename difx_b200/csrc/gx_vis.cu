@@ -17,7 +17,7 @@
 //                 baseline / freq / polarisation-product order, then the
 //                 autocorrelations per datastream.
 //
-// Covered: one configuration, one phase centre, no pulsar bins, no output
+// Covered: one configuration, phase centres, pulsar bins, no output
 // bands; TSYS 0 (normalised correlation coefficients) or TSYS > 0
 // (a-priori calibration by the band-mean autocorrelations).
 #include <algorithm>
@@ -108,8 +108,6 @@ gx_status gx_vis_open(gx_handle *h, const char *outdir, gx_vis **out)
   *out = nullptr;
   if (h->device < 0) return h->fail(GX_ERR_STATE, "host-only handle (opened with device -1)");
   if (!h->model || !h->meta) return h->fail(GX_ERR_STATE, "the visibility writer needs a handle opened with gx_open_input");
-  if (h->nbins > 0)   // per-bin files, weights over the bin widths (visibility.cpp:402-420)
-    return h->fail(GX_ERR_UNSUPPORTED, "the visibility writer does not implement pulsar binning");
   if (!h->zfreq.empty() && h->meta)
     for (double t : h->meta->tsys)   // Configuration::getDMatchingBand reads zoom bands out of range
       if (t > 0.0) return h->fail(GX_ERR_UNSUPPORTED, "a-priori calibration (TSYS > 0) of zoom bands is not implemented");
@@ -120,7 +118,7 @@ gx_status gx_vis_open(gx_handle *h, const char *outdir, gx_vis **out)
   const gx_job_desc &d = h->jd;
   int nrec = 0;
   for (int i = 0; i < d.nbaselines; i++)
-    for (int k = 0; k < d.baselines[i].nfreqs; k++) nrec += h->maxpc * d.baselines[i].npolprod[k];
+    for (int k = 0; k < d.baselines[i].nfreqs; k++) nrec += h->maxpc * h->binloop * d.baselines[i].npolprod[k];
   for (int s = 0; s < d.nstations; s++) nrec += 2 * (d.stations[s].nbands + d.stations[s].nzoombands);
   v->maxrec = nrec > 0 ? nrec : 1;
   CKR(h, cudaSetDevice(h->device));
@@ -199,8 +197,27 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
   const double ffts = meansub * h->J.blocks_per_send;
   // blocks per send * 2 * nchan * chanavg of freq f
   auto chanfactor = [&](int f) { return (float)(h->J.blocks_per_send * 2 * nout(f) * h->avg); };
-  auto weight_and_scale = [&](long long widx, int f, float &w, float &scale) {
-    w = (float)(fr[widx] / ffts);
+  // pulsar binning (visibility.cpp:402-415, 1376-1393): a bin's baseline
+  // weights over the bin's phase width, scrunched ones over the FP32 sum of
+  // weight x width of every bin
+  const int binloop = h->binloop;
+  std::vector<double> binwidth(binloop, 1.0);
+  float scrunchdiv = 0.0f;
+  if (h->nbins > 0) {
+    const PulsarConfig &P = *M.pulsar;
+    const int nb = (int)P.binphaseends.size();
+    auto width = [&](int b) {
+      const double w = P.binphaseends[b] - P.binphaseends[(b + nb - 1) % nb];
+      return w < 0.0 ? 1.0 + w : w;
+    };
+    if (binloop > 1)
+      for (int b = 0; b < binloop; b++) binwidth[b] = width(b);
+    for (int b = 0; b < nb; b++) scrunchdiv += P.binweights[b] * width(b);
+  }
+  auto weight_and_scale = [&](long long widx, int f, float &w, float &scale, int bin = -1) {
+    if (bin >= 0 && binloop > 1) w = (float)(fr[widx] / (ffts * binwidth[bin]));
+    else if (bin >= 0 && h->nbins > 0) w = (float)(fr[widx] / (ffts * scrunchdiv));
+    else w = (float)(fr[widx] / ffts);
     scale = w > 0.0f ? (float)(1.0 / ((double)w * meansub * (double)chanfactor(f))) : 0.0f;
   };
   // freq and polarisation of total band k (recorded bands, then zoom bands)
@@ -259,8 +276,9 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
     double uvw[3];
     long long offset;
     int nchan;
-    int file;     // phase centre: output file DIFX_..s<file>.b0000
+    int file;     // phase centre x bins + bin: output file DIFX_..s<centre>.b<bin>
     int source;   // source table index in the header
+    int bin;      // pulsar bin in the header
   };
   std::vector<Rec> recs;
   std::vector<VisScale> scales;
@@ -278,18 +296,20 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
       const int lf = gx_bl_localfreq(B, f);
       if (lf < 0) continue;
       const int N = nout(f);
-      for (int ph = 0; ph < nph; ph++) {   // records of every phase centre, each to its own file
+      for (int ph = 0; ph < nph; ph++) {   // records of every phase centre and bin, each to its own file
+      for (int bin = 0; bin < binloop; bin++) {
       Rec r{};
       r.baseline = (M.telescope[B.ds1] + 1) * 256 + (M.telescope[B.ds2] + 1);
-      r.file = ph;
+      r.file = ph * binloop + bin;
+      r.bin = bin;
       r.source = scn.phase_centre_sources[ph];
       if (!model.uvw(scan, scanoffset, model.station_of_datastream[B.ds1], model.station_of_datastream[B.ds2], ph + 1,
                      r.uvw))
         return h->fail(GX_ERR_MODEL, "no (u, v, w) model for this integration");
-      const long long base = h->blofs[f * nbl + i] + (long long)ph * B.npolprod[lf] * N;
+      const long long base = h->blofs[f * nbl + i] + ((long long)ph * binloop + bin) * B.npolprod[lf] * N;
       for (int k = 0; k < B.npolprod[lf]; k++) {
         float w, scale;
-        weight_and_scale(2LL * h->bwofs[f * nbl + i] + k, f, w, scale);
+        weight_and_scale(2LL * h->bwofs[f * nbl + i] + (long long)bin * B.npolprod[lf] + k, f, w, scale, bin);
         if (w > 0.0f) {   // zoom bands: fewer samples per channel (visibility.cpp:530-545)
           if (B.band1[lf][k] >= d.stations[B.ds1].nbands) scale *= std::sqrt(zoom_modifier(B.ds1, B.band1[lf][k]));
           if (B.band2[lf][k] >= d.stations[B.ds2].nbands) scale *= std::sqrt(zoom_modifier(B.ds2, B.band2[lf][k]));
@@ -316,6 +336,7 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
           r.nchan = N;
           recs.push_back(r);
         }
+      }
       }
       }
     }
@@ -374,12 +395,13 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
   const int intsec = M.start_seconds + scanstart + sec;
   const int dumpmjd = M.start_mjd + intsec / 86400;
   const double dumpseconds = double(intsec % 86400) + ((double)ns) / 1000000000.0 + M.int_time / 2.0;
-  // one file per phase centre (flushBuffersToDisk, visibility.cpp:1056-1091)
-  std::vector<std::vector<char>> bufs(nph);
+  // one file per phase centre and bin (flushBuffersToDisk, visibility.cpp:1056-1091)
+  const int nfiles = nph * binloop;
+  std::vector<std::vector<char>> bufs(nfiles);
   {
-    std::vector<size_t> bytes(nph, 0);
+    std::vector<size_t> bytes(nfiles, 0);
     for (const Rec &r : recs) bytes[r.file] += 74 + sizeof(float2) * (size_t)r.nchan;
-    for (int q = 0; q < nph; q++) bufs[q].reserve(bytes[q]);
+    for (int q = 0; q < nfiles; q++) bufs[q].reserve(bytes[q]);
   }
   for (const Rec &r : recs) {
     std::vector<char> &buf = bufs[r.file];
@@ -393,7 +415,7 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
     put(buf, (int32_t)r.freq);
     buf.push_back(r.pol[0]);
     buf.push_back(r.pol[1]);
-    put(buf, (int32_t)0);              // pulsar bin
+    put(buf, (int32_t)r.bin);          // pulsar bin
     put(buf, (double)r.weight);
     put(buf, r.uvw[0]);
     put(buf, r.uvw[1]);
@@ -401,9 +423,9 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
     const char *p = reinterpret_cast<const char *>(v->h_buf + r.offset);
     buf.insert(buf.end(), p, p + sizeof(float2) * (size_t)r.nchan);
   }
-  for (int q = 0; q < nph; q++) {
+  for (int q = 0; q < nfiles; q++) {
     char name[64];
-    snprintf(name, sizeof(name), "/DIFX_%05d_%06d.s%04d.b%04d", M.start_mjd, M.start_seconds, q, 0);
+    snprintf(name, sizeof(name), "/DIFX_%05d_%06d.s%04d.b%04d", M.start_mjd, M.start_seconds, q / binloop, q % binloop);
     std::ofstream of(v->outdir + name, std::ios::app | std::ios::binary);
     if (!of) return h->fail(GX_ERR_IO, "cannot open " + v->outdir + name);
     of.write(bufs[q].data(), (std::streamsize)bufs[q].size());

@@ -64,7 +64,8 @@ EXPORTED_SYMBOLS = ("gx_open", "gx_open_input", "gx_close", "gx_last_error", "gx
                     "gx_vdifmux_close", "gx_get_pcal_layout", "gx_vis_pcal_headers", "gx_ring_open",
                     "gx_ring_geometry_get", "gx_ring_buffer", "gx_ring_read", "gx_ring_set_segment",
                     "gx_ring_get_segment", "gx_ring_control_host", "gx_ring_subint_device", "gx_ring_last_control",
-                    "gx_ring_reset", "gx_ring_last_error", "gx_ring_close")
+                    "gx_ring_reset", "gx_ring_last_error", "gx_ring_close", "gx_set_kurtosis", "gx_kurtosis",
+                    "gx_sta")
 
 
 def subint_device_noalloc(jd: capi.JobDesc, sd: capi.SubintDesc, dev_results_ptr: int, stream_ptr: int = 0) -> None:
@@ -210,6 +211,34 @@ class Correlator:
         sd, out = self._inflight.pop(0) if getattr(self, "_inflight", None) else (None, None)
         self._check(st)
         return out
+
+    def set_kurtosis(self, dump_channels: int) -> None:
+        """Spectral kurtosis accumulation on (dump channels) or off (0)."""
+        self._check(lib().gx_set_kurtosis(self.h, dump_channels))
+        self._kdump = dump_channels
+
+    def kurtosis(self):
+        """(sk [nstations, GX_MAX_BANDS, dump], nchan [nstations, GX_MAX_BANDS], valid [nstations])
+        of the last subint."""
+        n = self.info.nstations
+        d = self._kdump
+        sk = np.zeros((n, capi.GX_MAX_BANDS, d), np.float32)
+        nch = np.zeros((n, capi.GX_MAX_BANDS), np.int32)
+        valid = np.zeros(n, np.int32)
+        self._check(lib().gx_kurtosis(self.h, sk.ctypes.data_as(C.c_void_p), nch.ctypes.data_as(C.c_void_p),
+                                      valid.ctypes.data_as(C.c_void_p)))
+        return sk, nch, valid
+
+    def sta(self, results: np.ndarray, dump_channels: int):
+        """STA dump of a Core result array (complex64, host): (sta, nchan, sent)."""
+        n = self.info.nstations
+        res = np.ascontiguousarray(results, dtype=np.complex64)
+        out = np.zeros((n, capi.GX_MAX_BANDS, dump_channels), np.float32)
+        nch = np.zeros((n, capi.GX_MAX_BANDS), np.int32)
+        sent = np.zeros((n, capi.GX_MAX_BANDS), np.int32)
+        self._check(lib().gx_sta(self.h, res.ctypes.data_as(C.c_void_p), dump_channels, out.ctypes.data_as(C.c_void_p),
+                                 nch.ctypes.data_as(C.c_void_p), sent.ctypes.data_as(C.c_void_p)))
+        return out, nch, sent
 
     def set_tc_scales(self, station: int, band: int, scales) -> None:
         """Per-channel operand scales of the tensor-core X-step for one station band

@@ -518,6 +518,38 @@ gx_status gx_ring_reset(gx_ring *r);
 const char *gx_ring_last_error(const gx_ring *r);
 gx_status gx_ring_close(gx_ring *r);
 
+/* ---- Monitoring spectra: spectral kurtosis and STA dumps -------------------- */
+
+/* The reference's Core sends two monitoring products on its message bus when
+   an operator asks for them: the spectral kurtosis of every recorded band
+   (Mode accumulates |X|^2 and |X|^4 of each channel over its FFT blocks,
+   mode.cpp:1237-1254, and turns them into n s2 / s1^2 - 1, debiased and
+   averaged to the dump channel count, mode.cpp:1403-1454;
+   Core::averageAndSendKurtosis, core.cpp:1378-1430), and the STA dump, each
+   band's autocorrelation normalised to power spectral density and averaged
+   to the dump channels (Core::averageAndSendAutocorrs, core.cpp:1180-1255).
+   Both are given here for one subint (the reference's records of a Core with
+   one process thread); sending them is the caller's. */
+
+/* Kurtosis accumulation on (dump_channels > 0, the STA DUMP CHANNELS value)
+   or off (0) for the following subints.  The sums read the spectra in
+   device memory after each pass of the F-step. */
+gx_status gx_set_kurtosis(gx_handle *h, int dump_channels);
+/* The kurtosis of the last subint: sk[(station * GX_MAX_BANDS + band) *
+   dump_channels + j] for recorded bands, nchan[station * GX_MAX_BANDS + band]
+   the channels each holds, valid[station] whether the reference would send
+   that station's records (its last band had data; a band without data keeps
+   its previous values, as the reference's arrays do).  nchan, valid may be
+   NULL.  Synchronises the subint's stream. */
+gx_status gx_kurtosis(gx_handle *h, float *sk, int *nchan, int *valid);
+/* The STA dump of a subint from its Core result array (host memory, complex
+   interleaved): sta[(station * GX_MAX_BANDS + band) * dump_channels + j],
+   nchan[...] the channels of each record, sent[...] whether the reference
+   sends it (the band's weight reaches a third of a full subint's,
+   Core::MINIMUM_FILTERBANK_WEIGHT).  GX_ERR_UNSUPPORTED when the dump needs
+   more channels than the averaged records keep. */
+gx_status gx_sta(const gx_handle *h, const float *results, int dump_channels, float *sta, int *nchan, int *sent);
+
 /* Phase-cal section of the Core result array (configuration.cpp:2612-2620,
    core.cpp:1131-1164): offsets[s * GX_MAX_BANDS + b] is the result index of
    the first tone of recorded band b of datastream s (-1 without phase-cal),

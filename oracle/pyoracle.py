@@ -165,6 +165,30 @@ class Reference:
         if st != 0:
             raise RuntimeError(f"ref_vis_write failed ({st})")
 
+    def set_monitor(self, sta: bool, kurtosis: bool, channels: int) -> None:
+        """STA / kurtosis dumps on for the following process() calls."""
+        self.lib.ref_set_monitor(self.h, int(sta), int(kurtosis), channels)
+
+    def take_monitor_records(self):
+        """The STA and kurtosis records (DifxMessageSTARecord, difxmessage.h:637-652)
+        the reference sent since the last call: a list of dicts with the type
+        (STA_AUTOCORRELATION 1, STA_KURTOSIS 3), datastream,
+        band, nChan, times and the float data."""
+        buf = (C.c_char * (1 << 22))()
+        n = self.lib.ref_take_messages(self.h, buf, len(buf))
+        raw = bytes(buf[:n])
+        out, o = [], 0
+        hdr = 10 * 4 + 32
+        while o + hdr <= n:
+            v = np.frombuffer(raw[o:o + 40], "<i4")
+            nchan = int(v[9])
+            data = np.frombuffer(raw[o + hdr:o + hdr + 4 * nchan], "<f4").copy()
+            out.append(dict(type=int(v[0]), scan=int(v[1]), sec=int(v[2]), ns=int(v[3]), nswidth=int(v[4]),
+                            ds=int(v[5]), core=int(v[6]), thread=int(v[7]), band=int(v[8]), nchan=nchan,
+                            ident=raw[o + 40:o + hdr].split(b"\0")[0].decode(), data=data))
+            o += hdr + 4 * nchan
+        return out
+
     def uvw(self, scan: int, offset_s: float, ds1: int, ds2: int) -> np.ndarray:
         out = np.zeros(3, np.float64)
         if self.lib.ref_uvw(self.h, scan, C.c_double(offset_s), ds1, ds2, out.ctypes.data_as(C.c_void_p)) != 0:

@@ -127,6 +127,33 @@ void *ref_open(const char *inputfile)
 }
 
 Configuration *ref_job_config(void *h) { return ((RefJob *)h)->config; }
+
+int gx_stub_binary_take(char *out, int max);
+
+// STA and kurtosis dumps on or off for the following slots, as an operator
+// message sets them (Configuration's flags) and Core::loopprocess hands them
+// to each thread's scratch space with a record buffer of one MTU
+// (core.cpp:510-525).
+void ref_set_monitor(void *h, int sta, int kurtosis, int channels)
+{
+  RefJob *j = (RefJob *)h;
+  j->config->dumpsta = sta != 0;
+  j->config->dumpkurtosis = kurtosis != 0;
+  j->config->stadumpchannels = channels;
+  for (void *p : j->scratch) {
+    Core::threadscratchspace *s = (Core::threadscratchspace *)p;
+    s->dumpsta = sta != 0;
+    s->dumpkurtosis = kurtosis != 0;
+    if ((sta || kurtosis) && !s->starecordbuffer) s->starecordbuffer = (DifxMessageSTARecord *)malloc(j->config->getMTU());
+  }
+}
+
+// The binary messages the reference sent since the last call.
+int ref_take_messages(void *h, char *out, int max)
+{
+  (void)h;
+  return gx_stub_binary_take(out, max);
+}
 int ref_num_threads(void *h) { return ((RefJob *)h)->nthreads; }
 int ref_result_length(void *h) { return ((RefJob *)h)->config->getCoreResultLength(0); }
 int ref_blocks_per_send(void *h) { return ((RefJob *)h)->config->getBlocksPerSend(0); }

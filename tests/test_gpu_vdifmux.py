@@ -102,7 +102,8 @@ def test_device_mux_matches_reference(case, dest_frames):
     if c["pert"]:
         assert acc["duplicate_frames"] > 0 and acc["fill_bytes"] > 0 and acc["wrong_thread_frames"] > 0
         if c["flags"] & 0x40:
-            assert acc["partial_output_frames"] > 0
+            # one thread: an output frame is whole or absent, never partial
+            assert acc["partial_output_frames"] > 0 or len(ids) == 1
         else:
             assert acc["filler_output_frames"] > 0
     m.close()

@@ -40,7 +40,18 @@ CASES = {
     # decorrelation, scales divided by it (visibility.cpp:428-441, 554-557, 860-890)
     "pc3": lambda: _pc("pc3"),
     "pc2_avg": lambda: _pc("pc2_avg"),
+    # pulsar binning: one file per bin, baseline weights over the bin's phase
+    # width; scrunched: one file, weights over the summed weight x width
+    # (visibility.cpp:402-415, 1056-1091, 1376-1393)
+    "psr8": lambda: _psr("bins8"),
+    "psr_scrunch": lambda: _psr("scrunch4"),
 }
+
+
+def _psr(name):
+    from dataclasses import replace
+    from tests.test_pulsar import _case
+    return replace(_case(name), name="gvispsr_" + name, int_time=0.016)
 
 
 def _pc(name):
@@ -100,7 +111,8 @@ def test_gx_vis_bytes_match_reference_visibility(case, tmp_path):
     ref.vis_write(host, s0.scan, s0.sec, s0.ns, theirs)
     fa = sorted(f for f in os.listdir(ours) if f.startswith("DIFX_"))
     fb = sorted(f for f in os.listdir(theirs) if f.startswith("DIFX_"))
-    assert fa == fb and len(fa) == max(1, spec.phase_centres), (fa, fb)
+    nbinfiles = spec.pulsar_bins if spec.pulsar_bins and not spec.pulsar_scrunch else 1
+    assert fa == fb and len(fa) == max(1, spec.phase_centres) * nbinfiles, (fa, fb)
     freqs = list(spec.subbands) + list(spec.zooms)
     nrec = 0
     for f in fa:
