@@ -507,6 +507,19 @@ def run_c4(args):
     modes["per_job_launches"] = {"gsamp_s": samples * steps / (ms * 1e-3) / 1e9, "device_ms_per_step": ms / steps,
                                  "wall_ms_per_step": wall / steps, "gpu_launches_per_step": b.info()[2]}
     b.close()
+    # launch shapes per shape class (X-step channel tile and stage depth,
+    # F-step blocks per CTA), from the default shapes' graph step to the tuned one
+    b = Batch(corrs, ptrs, mode="graph", nstreams=16)
+    timed(b, 1)
+    ms_default, _ = timed(b, steps)
+    t_tile = time.perf_counter()
+    nclasses = b.tune_tiles(subs, reps=2)
+    tile_tune_s = time.perf_counter() - t_tile
+    tiles = {}
+    for c in corrs:
+        t = c.tiles()
+        tiles[f"x{t[0]}_f{t[1]}"] = tiles.get(f"x{t[0]}_f{t[1]}", 0) + 1
+    b.close()
     # branch streams replayed as one graph; the branch count is tuned on the first steps
     with ClockSampler(0) as clk:
         b = Batch(corrs, ptrs, mode="graph", nstreams=0)
@@ -521,7 +534,9 @@ def run_c4(args):
     clocks = clk.summary()
     modes["graph"] = {"gsamp_s": samples * steps / (ms * 1e-3) / 1e9, "device_ms_per_step": ms / steps,
                       "wall_ms_per_step": wall / steps, "branches": k, "tuning_ms": tune,
-                      "gpu_launches_per_step": launches, "host_launches_per_step": 1}
+                      "gpu_launches_per_step": launches, "host_launches_per_step": 1,
+                      "tile_tuner": {"shape_classes": nclasses, "tuning_s": tile_tune_s, "chosen": tiles,
+                                     "default_tiles_device_ms_per_step_16_branches": ms_default / steps}}
     # the same schedule issued stream by stream (no graph)
     b = Batch(corrs, ptrs, mode="streams", nstreams=k)
     timed(b, 1)

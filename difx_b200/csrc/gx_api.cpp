@@ -1353,6 +1353,24 @@ gx_status gx_get_pcal_layout(const gx_handle *h, int *offsets, int *ntones)
   return GX_OK;
 }
 
+gx_status gx_set_tiles(gx_handle *h, int xmac_variant, int fstep_items)
+{
+  if (!h) return GX_ERR_ARG;
+  if (xmac_variant < 0 || xmac_variant >= kXmacVariants || fstep_items < 0 || fstep_items > 64)
+    return h->fail(GX_ERR_ARG, "tile choice out of range");
+  h->xvar = xmac_variant;
+  h->J.sb_items = fstep_items;
+  return GX_OK;
+}
+
+gx_status gx_get_tiles(const gx_handle *h, int *xmac_variant, int *fstep_items)
+{
+  if (!h) return GX_ERR_ARG;
+  if (xmac_variant) *xmac_variant = h->xvar;
+  if (fstep_items) *fstep_items = h->J.sb_items > 0 ? h->J.sb_items : 4;
+  return GX_OK;
+}
+
 gx_status gx_get_offsets(const gx_handle *h, int *blofs, int *bwofs, int *acofs, int *acwofs)
 {
   if (!h) return GX_ERR_ARG;
@@ -1597,7 +1615,7 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
       CKR(h, xmac_tc_launch(h->d_spec, nb, J.nchan, h->nfmain, J.ninputs, h->ks, h->hilo, h->d_scale, acc4,
                             b0 > 0 ? 1 : 0, h->d_err, st));
     else
-      CKR(h, xmac_fp32_launch(h->d_spec, nb, J.ninputs, J.nchan, h->nfmain, h->ks, h->d_acc, h->d_err, st));
+      CKR(h, xmac_fp32_launch(h->d_spec, nb, J.ninputs, J.nchan, h->nfmain, h->ks, h->d_acc, h->d_err, st, h->xvar));
     if (h->nbins > 0) {   // pulsar binning: the binned cross products and weights of this pass
       const double *avgphase = reinterpret_cast<const double *>(h->d_sub + h->o_avgphase);
       const double *dmoff = reinterpret_cast<const double *>(h->d_sub + h->o_dmoff);

@@ -18,10 +18,13 @@
 // every step still producing its results) and the fastest is kept.
 #include <algorithm>
 #include <cmath>
+#include <map>
 #include <numeric>
+#include <tuple>
 #include <string>
 #include <vector>
 #include "gx_handle.h"
+#include "gx_xstep.h"
 
 namespace {
 
@@ -310,6 +313,74 @@ gx_status gx_batch_info(const gx_batch *b, int *nstreams, int *tuning, int *laun
   if (nstreams) *nstreams = b->tuning ? 0 : b->nbranch;
   if (tuning) *tuning = b->tuning ? 1 : 0;
   if (launches) *launches = b->launches;
+  return GX_OK;
+}
+
+// Launch-shape tuner: jobs whose kernels take the same template instances
+// (X-step form and register/super-tile shape, transform length, sample
+// format, band count) form a class; the class's costliest job runs its
+// subint under every candidate (X-step variant x F-step items per group),
+// timed alone by events, and the fastest candidate goes to every job of the
+// class.  The candidates leave the results unchanged, so tuning steps are
+// ordinary steps.
+gx_status gx_batch_tune_tiles(gx_batch *b, const gx_subint_desc *const *subs, int reps, int *nclasses)
+{
+  if (!b || !subs || reps < 1) return GX_ERR_ARG;
+  gx_status r;
+  if ((r = b->cuda(cudaSetDevice(b->device), "cudaSetDevice")) != GX_OK) return r;
+  if ((r = b->finish()) != GX_OK) return r;
+  for (auto &g : b->graph)   // graphs hold the launch shapes they captured
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+  struct Key {
+    int tc, T, ST, F, nbits, cplx, nbands;
+    bool operator<(const Key &o) const
+    {
+      return std::tie(tc, T, ST, F, nbits, cplx, nbands) < std::tie(o.tc, o.T, o.ST, o.F, o.nbits, o.cplx, o.nbands);
+    }
+  };
+  std::map<Key, std::vector<int>> classes;
+  for (size_t j = 0; j < b->jobs.size(); j++) {
+    const gx_handle *h = b->jobs[j];
+    const Key k{h->tc ? 1 : 0, h->tc ? 0 : h->xs.T, h->tc ? 0 : h->xs.ST, h->J.fftlen, h->J.nbits, h->J.cplx, h->J.nbands};
+    classes[k].push_back((int)j);
+  }
+  const int items[] = {2, 4, 8};
+  for (auto &kv : classes) {
+    const std::vector<int> &members = kv.second;
+    int jb = members[0];
+    for (int j : members)
+      if (b->cost[j] > b->cost[jb]) jb = j;
+    gx_handle *h = b->jobs[jb];
+    const int nxv = h->tc ? 1 : gx::kXmacVariants;
+    double best = 1e30;
+    int bx = 0, bf = 4;
+    for (int xv = 0; xv < nxv; xv++)
+      for (int fi : items) {
+        if ((r = gx_set_tiles(h, xv, fi)) != GX_OK) return b->fail(r, h->err);
+        float ms = 1e30f;
+        for (int rep = 0; rep < reps; rep++) {
+          if ((r = gx_stage_subint(h, subs[jb], subs[jb]->data)) != GX_OK) return b->fail(r, h->err);
+          if ((r = b->cuda(cudaEventRecord(b->ev0, b->origin), "cudaEventRecord")) != GX_OK) return r;
+          if ((r = b->enqueue_job(jb, b->origin)) != GX_OK) return r;
+          if ((r = b->cuda(cudaEventRecord(b->ev1, b->origin), "cudaEventRecord")) != GX_OK) return r;
+          if ((r = b->cuda(cudaEventSynchronize(b->ev1), "cudaEventSynchronize")) != GX_OK) return r;
+          float t = 0.f;
+          if ((r = b->cuda(cudaEventElapsedTime(&t, b->ev0, b->ev1), "cudaEventElapsedTime")) != GX_OK) return r;
+          ms = std::min(ms, t);
+        }
+        if (ms < best) {
+          best = ms;
+          bx = xv;
+          bf = fi;
+        }
+      }
+    for (int j : members)
+      if ((r = gx_set_tiles(b->jobs[j], bx, bf)) != GX_OK) return b->fail(r, b->jobs[j]->err);
+  }
+  if (nclasses) *nclasses = (int)classes.size();
   return GX_OK;
 }
 

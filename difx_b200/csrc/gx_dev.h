@@ -48,6 +48,7 @@ struct DevJob {
   int ninputs;            // NI: padded spectra rows per freq
   int nfreqs;
   int blocks_per_send;
+  int sb_items;           // station-block F-step: FFT blocks per group and CTA (0: 4)
   int flaglen;
   int lgstride;           // log2(stride): FFT length, channels and stride are powers of two
   int fringe_order;       // FRINGE ROTN ORDER: 1 pre-F linear, 2 pre-F quadratic, 0 post-F (real data)

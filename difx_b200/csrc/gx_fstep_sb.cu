@@ -349,7 +349,7 @@ cudaError_t fstep_sb_launch(const DevJob &J, const DevStation *stations, int max
   const size_t sm = fstep_sb_smem_bytes(J, maxnrf, deltapol);
   if (sm > 227 * 1024) return cudaErrorNotSupported;
   const int bpts = J.nbands * J.nbits * (J.cplx ? 2 : 1) / 8;
-  const int bpc = 4 * G;   // four items per group
+  const int bpc = (J.sb_items > 0 ? J.sb_items : 4) * G;   // items per group (four unless tuned)
   dim3 grid((nblk + bpc - 1) / bpc, J.nstations);
 #define GX_SB_CASE(FLV, CX, BP)                                                                         \
   if (F == FLV && J.cplx == CX && bpts == BP) {                                                         \

@@ -153,6 +153,7 @@ struct gx_handle {
 
   std::vector<int> sta_acoff, sta_acw;   // [station * GX_MAX_BANDS + recorded band]: autocorrelation record, weight (-1: none)
   struct gx_kurtosis_state *kurt = nullptr;   // gx_set_kurtosis
+  int xvar = 0;                              // FP32 X-step launch variant (gx_set_tiles)
   std::unique_ptr<HostModel> model;  // only for gx_open_input
   std::unique_ptr<gx::JobMeta> meta; // only for gx_open_input
   std::vector<gx::DevStation> dst;   // host copy of the per-station device constants

@@ -175,8 +175,13 @@ gx_status gx_vis_write(gx_vis *v, int scan, int sec, int ns, int *nrecords)
   std::vector<float> fr(2 * (size_t)h->rl);
   {
     long long bw0 = h->rl, bw1 = 0, aw0 = h->rl;
-    for (int x : h->bwofs)
-      if (x >= 0) bw0 = std::min<long long>(bw0, x), bw1 = std::max<long long>(bw1, x + 2);
+    for (int f = 0; f < d.nfreqs; f++)   // each baseline-freq's weights: bins x products floats
+      for (int i = 0; i < nbl; i++) {
+        const int x = h->bwofs[f * nbl + i], lf = gx_bl_localfreq(d.baselines[i], f);
+        if (x < 0 || lf < 0) continue;
+        bw0 = std::min<long long>(bw0, x);
+        bw1 = std::max<long long>(bw1, x + (h->binloop * d.baselines[i].npolprod[lf] + 1) / 2);
+      }
     for (int x : h->bsdofs)   // and the shift decorrelation factors that follow them
       if (x >= 0) bw1 = std::max<long long>(bw1, x + h->maxpc / 2 + h->maxpc % 2);
     for (int x : h->acwofs) aw0 = std::min<long long>(aw0, x);

@@ -271,14 +271,22 @@ XmacShape xmac_shape(int NI)
 }
 
 cudaError_t xmac_fp32_launch(const float2 *spec, int nblk, int NI, int N, int nfreqs, int ks, float2 *acc, int *err,
-                             cudaStream_t st)
+                             cudaStream_t st, int variant)
 {
+  // every variant keeps the register tile T and super-tile ST of the shape
+  // (the accumulator layout) and 192 KB of stages; variant 1 trades channels
+  // per CTA against blocks per stage (or doubles the channels)
   XmacShape s = xmac_shape(NI);
-  if (s.ST == 8) return launch_t<4, 8, 32, 8, 3>(spec, nblk, NI, N, nfreqs, ks, acc, err, st);
-  if (s.ST == 16) return launch_t<4, 16, 16, 8, 3>(spec, nblk, NI, N, nfreqs, ks, acc, err, st);
+  if (s.ST == 8)
+    return variant == 1 ? launch_t<4, 8, 64, 8, 3>(spec, nblk, NI, N, nfreqs, ks, acc, err, st)
+                        : launch_t<4, 8, 32, 8, 3>(spec, nblk, NI, N, nfreqs, ks, acc, err, st);
+  if (s.ST == 16)
+    return variant == 1 ? launch_t<4, 16, 32, 8, 3>(spec, nblk, NI, N, nfreqs, ks, acc, err, st)
+                        : launch_t<4, 16, 16, 8, 3>(spec, nblk, NI, N, nfreqs, ks, acc, err, st);
   // 8 x 8 register tiles of 32-row super-tiles, 16 channels per CTA; the
   // block loop is not unrolled (unrolled by 2 or 4 it measured 3-9% slower)
-  return launch_t<8, 32, 16, 8, 3>(spec, nblk, NI, N, nfreqs, ks, acc, err, st);
+  return variant == 1 ? launch_t<8, 32, 8, 16, 3>(spec, nblk, NI, N, nfreqs, ks, acc, err, st)
+                      : launch_t<8, 32, 16, 8, 3>(spec, nblk, NI, N, nfreqs, ks, acc, err, st);
 }
 
 cudaError_t weights_launch(const float *w, int nblk, int nstations, const int2 *pairs, int npairs, float *wacc,

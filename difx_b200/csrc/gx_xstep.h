@@ -44,9 +44,12 @@ size_t fstep_smem_bytes(const DevJob &J, int nrf, int nslots);cudaError_t fstep_
                          int blk0, int nblk, int nslots, float2 *spec, float *weights, BlockParam *bp,
                          cudaStream_t st);
 // FP32 X-step over one pass of blocks; *err (may be null) receives a nonzero
-// status if a wait of the kernel expired.
+// status if a wait of the kernel expired.  variant: the launch shape (0: the
+// default channel tile and stage depth; 1: the other one of the shape class,
+// kXmacVariants in all); the sums are the same for every variant.
+constexpr int kXmacVariants = 2;
 cudaError_t xmac_fp32_launch(const float2 *spec, int nblk, int NI, int N, int nfreqs, int ks, float2 *acc, int *err,
-                             cudaStream_t st);
+                             cudaStream_t st, int variant = 0);
 cudaError_t weights_launch(const float *w, int nblk, int nstations, const int2 *pairs, int npairs, float *wacc,
                            cudaStream_t st);
 // Entries [start, end) of the tensor-core product table (sorted by freq, then a)

@@ -65,7 +65,7 @@ EXPORTED_SYMBOLS = ("gx_open", "gx_open_input", "gx_close", "gx_last_error", "gx
                     "gx_ring_geometry_get", "gx_ring_buffer", "gx_ring_read", "gx_ring_set_segment",
                     "gx_ring_get_segment", "gx_ring_control_host", "gx_ring_subint_device", "gx_ring_last_control",
                     "gx_ring_reset", "gx_ring_last_error", "gx_ring_close", "gx_set_kurtosis", "gx_kurtosis",
-                    "gx_sta")
+                    "gx_sta", "gx_set_tiles", "gx_get_tiles", "gx_batch_tune_tiles")
 
 
 def subint_device_noalloc(jd: capi.JobDesc, sd: capi.SubintDesc, dev_results_ptr: int, stream_ptr: int = 0) -> None:
@@ -211,6 +211,15 @@ class Correlator:
         sd, out = self._inflight.pop(0) if getattr(self, "_inflight", None) else (None, None)
         self._check(st)
         return out
+
+    def set_tiles(self, xmac_variant: int, fstep_items: int) -> None:
+        """Launch shapes (results do not depend on them)."""
+        self._check(lib().gx_set_tiles(self.h, xmac_variant, fstep_items))
+
+    def tiles(self):
+        x, f = C.c_int(0), C.c_int(0)
+        self._check(lib().gx_get_tiles(self.h, C.byref(x), C.byref(f)))
+        return x.value, f.value
 
     def set_kurtosis(self, dump_channels: int) -> None:
         """Spectral kurtosis accumulation on (dump channels) or off (0)."""
@@ -411,6 +420,13 @@ class Batch:
         ms = C.c_float(0)
         self._check(lib().gx_batch_synchronize(self.b, C.byref(ms)))
         return ms.value
+
+    def tune_tiles(self, subs: Sequence[capi.SubintDesc], reps: int = 2) -> int:
+        """Per shape class, the fastest launch shapes (gx_batch_tune_tiles); returns the class count."""
+        arr = (C.c_void_p * self.n)(*[C.addressof(sd.desc) for sd in subs])
+        n = C.c_int(0)
+        self._check(lib().gx_batch_tune_tiles(self.b, arr, int(reps), C.byref(n)))
+        return n.value
 
     def info(self):
         """(branch streams in use (0 while tuning), tuning, kernel launches of the last step)."""

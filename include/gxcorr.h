@@ -380,6 +380,12 @@ gx_status gx_batch_synchronize(gx_batch *b, float *device_ms);
 /* Branch count in use (0 while tuning), whether tuning is still on, and the
    kernel launches of the last step. */
 gx_status gx_batch_info(const gx_batch *b, int *nstreams, int *tuning, int *launches);
+/* Tunes the launch shapes (gx_set_tiles) of a batch's jobs per shape class:
+   the class's costliest job runs its subint of `subs` under every candidate,
+   `reps` times each, timed alone on the device, and the fastest goes to every
+   job of the class.  Graphs captured before are dropped (the next graph step
+   captures the tuned shapes).  *nclasses: the classes found. */
+gx_status gx_batch_tune_tiles(gx_batch *b, const gx_subint_desc *const *subs, int reps, int *nclasses);
 const char *gx_batch_last_error(const gx_batch *b);
 gx_status gx_batch_close(gx_batch *b);
 
@@ -549,6 +555,12 @@ gx_status gx_kurtosis(gx_handle *h, float *sk, int *nchan, int *valid);
    Core::MINIMUM_FILTERBANK_WEIGHT).  GX_ERR_UNSUPPORTED when the dump needs
    more channels than the averaged records keep. */
 gx_status gx_sta(const gx_handle *h, const float *results, int dump_channels, float *sta, int *nchan, int *sent);
+
+/* Launch shapes a tuner may choose per job; results do not depend on them.
+   xmac_variant: the FP32 X-step's channel tile and stage depth (0 or 1);
+   fstep_items: FFT blocks a station-block F-step group takes per CTA (0: 4). */
+gx_status gx_set_tiles(gx_handle *h, int xmac_variant, int fstep_items);
+gx_status gx_get_tiles(const gx_handle *h, int *xmac_variant, int *fstep_items);
 
 /* Phase-cal section of the Core result array (configuration.cpp:2612-2620,
    core.cpp:1131-1164): offsets[s * GX_MAX_BANDS + b] is the result index of

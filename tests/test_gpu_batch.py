@@ -90,3 +90,33 @@ def test_batch_matches_alone(batch_jobs, mode, nstreams):
     b.close()
     for c in corrs:
         c.close()
+
+
+def test_tile_tuner_keeps_results(batch_jobs):
+    """gx_batch_tune_tiles times every launch-shape candidate per shape class
+    and sets the fastest; the shapes change no bit of any job's results
+    (every candidate of every job is checked here too)."""
+    import torch
+    from difx_b200 import gxcorr
+    out, alone = batch_jobs
+    corrs = [gxcorr.Correlator.from_desc(jd) for _, jd, _ in out]
+    bufs = [torch.zeros((2 * c.result_length,), dtype=torch.float32, device="cuda") for c in corrs]
+    for j, c in enumerate(corrs):
+        for xv in (0, 1):
+            for fi in (2, 4, 8):
+                c.set_tiles(xv, fi)
+                c.subint_device(out[j][2][0][0], bufs[j].data_ptr())
+                c.synchronize()
+                np.testing.assert_array_equal(bufs[j].cpu().numpy().view(np.complex64), alone[j][0],
+                                              err_msg=f"job {j} tiles {xv}/{fi}")
+        c.set_tiles(0, 0)
+    b = gxcorr.Batch(corrs, [x.data_ptr() for x in bufs], mode="graph", nstreams=2)
+    n = b.tune_tiles([subs[0][0] for _, _, subs in out], reps=1)
+    assert 1 <= n <= len(out)
+    b.run([subs[1][0] for _, _, subs in out])
+    b.synchronize()
+    for j in range(len(out)):
+        np.testing.assert_array_equal(bufs[j].cpu().numpy().view(np.complex64), alone[j][1])
+    b.close()
+    for c in corrs:
+        c.close()
