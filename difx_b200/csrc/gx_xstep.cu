@@ -250,8 +250,10 @@ static cudaError_t launch_t(const float2 *spec, int nblk, int NI, int N, int nfr
   if (e != cudaSuccess) return e;
   e = smem_opt_in((const void *)xmac_fp32_kernel<T, ST, CT, KB, NSTAGE, UNR>, sm);
   if (e != cudaSuccess) return e;
-  // slices of whole stages
-  const int kper = ((nblk + ks - 1) / ks + KB - 1) / KB * KB;
+  // slices of whole stages, on 16-block boundaries for every variant (KB 8
+  // or 16), so that the variants add the same blocks into each slice
+  static_assert(16 % KB == 0, "slice boundaries must be whole stages");
+  const int kper = ((nblk + ks - 1) / ks + 15) / 16 * 16;
   // super-tile pairs fastest: the pairs that share a channel group's spectra run together
   dim3 grid(npairs, (N + CT - 1) / CT, nfreqs * ks);
   xmac_fp32_kernel<T, ST, CT, KB, NSTAGE, UNR>
