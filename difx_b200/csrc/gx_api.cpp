@@ -1015,6 +1015,19 @@ static gx_status setup(gx_handle *h)
       for (int b = 0; b < 256; b++) lut[b] = (float)((b - off) / 3.3);
       J.lut_offset = off;
       J.lut_div = 3.3;
+      // The same levels without a table lookup: 1 / 3.3 as a two-float sum and
+      // one fused multiply-add, used only if it reproduces every entry.
+      const double bias = 8388608.0 + off;
+      const float hi = (float)(1.0 / 3.3), lo = (float)(1.0 / 3.3 - (double)hi);
+      bool ok = (double)(float)bias == bias;
+      for (int b = 0; ok && b < 256; b++) {
+        const float x = (float)(8388608.0 + b) - (float)bias;
+        ok = std::fma(x, hi, x * lo) == lut[b];
+      }
+      J.lut_affine = ok ? 1 : 0;
+      J.lut_bias = (float)bias;
+      J.lut_hi = hi;
+      J.lut_lo = lo;
     }
     // Tensor-core operands: a power-of-two scale that brings the spectrum of
     // noise with the r.m.s. level of the decode table to an r.m.s. near 8, so

@@ -58,6 +58,11 @@ struct DevJob {
   const float2 *twiddle;  // exp(-2 pi i m / F), m in [0, F), then the pass rows of r16::tw_pass_offset
   float lut[256];         // level of each sample code (VDIF decode table), staged to shared memory
   double lut_offset, lut_div;   // 8-bit codes: level = (code - lut_offset) / lut_div
+  // 8-bit codes by arithmetic: level = fma(x, lut_hi, x * lut_lo) with
+  // x = float(2^23 + code) - lut_bias; set only when the host has checked that
+  // this equals lut[code] for all 256 codes (lut_affine = 1)
+  int lut_affine;
+  float lut_bias, lut_hi, lut_lo;
 };
 
 // Offset of (input row, channel c) inside the spectra of one (freq, block):

@@ -14,7 +14,8 @@
 //   3. for every band: decodes its field of the staged samples through the
 //      shared-memory level table (format_vdif.c:66-146), rotates
 //      (mode.cpp:1160-1183), transforms (16 points per thread, radix-16
-//      passes of gx_fft16.h with twiddle rows read from a contiguous table),
+//      passes of gx_fft16.h with the twiddle rows of the stride-16 and
+//      stride-256 passes in shared memory),
 //      selects the sideband, applies the fractional-sample correction
 //      (mode.cpp:1185-1261) and writes the channels with coalesced stores.
 // Frames a block spans are checked against the block's validity mask only
@@ -78,17 +79,6 @@ __device__ __forceinline__ void cp_async_wait_all()
   asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
 }
 
-// Radix-16 pass of stride Ns > 1 with its twiddle row from the table section
-// at `sec` (entry (r - 1) Ns + m), then the 16-point transform.
-template <int F>
-__device__ __forceinline__ void pass16_tab(float2 (&v)[16], int j, int Ns, const float2 *__restrict__ sec)
-{
-  const float2 *row = sec + (j & (Ns - 1));
-#pragma unroll
-  for (int r = 1; r < 16; r++) v[r] = r16::mul(v[r], __ldg(row + (r - 1) * Ns));
-  r16::dft16(v);
-}
-
 // Final radix-R0 pass (stride F / R0) with twiddles from the final section
 // (entry (r - 1) (F / R0) + g, g = j + NT mm).
 template <int F, int R0>
@@ -109,13 +99,55 @@ __device__ __forceinline__ void final_pass_tab(float2 (&v)[16], int j, const flo
   }
 }
 
+// Twiddle rows of the radix-16 passes held in shared memory, 15 x 16 entries
+// each, entry (r - 1) 16 + m:
+//   A: W_256^(r m)  -- the stride-16 pass's whole table,
+//   B: W_4096^(r m) -- the low digit of the stride-256 pass, whose twiddle
+//      W_4096^(r m) for m < 256 is B[r][m mod 16] A[r][m / 16].
+// The full stride-256 table (3840 entries, 30 KB) is larger than what L1 keeps
+// beside two CTAs' shared memory, so reading it per pass went to L2.
+constexpr int kTwRow = 16 * 15;
+
+// Fills A and B from the device twiddle table (group-independent; the caller
+// synchronises before the first transform).
+template <int F>
+__device__ __forceinline__ void load_tw_rows(float2 *twA, float2 *twB, const float2 *__restrict__ tw, int tid, int nthr)
+{
+  using Pl = r16::Plan<F>;
+  const float2 *s1 = tw + r16::tw_pass_offset(F, 1);
+  for (int i = tid; i < kTwRow; i += nthr) twA[i] = s1[i];
+  if constexpr (Pl::L >= 3) {
+    const float2 *s2 = tw + r16::tw_pass_offset(F, 2);
+    for (int i = tid; i < kTwRow; i += nthr) twB[i] = s2[(i >> 4) * 256 + (i & 15)];
+  }
+}
+
+// Radix-16 pass of stride 16 (p = 1) or 256 (p = 2) with twiddles from the rows.
+template <int P>
+__device__ __forceinline__ void pass16_rows(float2 (&v)[16], int j, const float2 *twA, const float2 *twB)
+{
+  if constexpr (P == 1) {
+    const float2 *a = twA + (j & 15);
+#pragma unroll
+    for (int r = 1; r < 16; r++) v[r] = r16::mul(v[r], a[(r - 1) * 16]);
+  } else {
+    const float2 *a = twA + ((j >> 4) & 15);
+    const float2 *b = twB + (j & 15);
+#pragma unroll
+    for (int r = 1; r < 16; r++) v[r] = r16::mul(v[r], r16::mul(b[(r - 1) * 16], a[(r - 1) * 16]));
+  }
+  r16::dft16(v);
+}
+
 // Forward transform of the group's F points (16 per thread): register t ends
 // holding bin j + NT t.
 template <int F, int CTA>
-__device__ __forceinline__ void fft(float2 (&v)[16], int j, int g, float2 *xb, const float2 *__restrict__ tw)
+__device__ __forceinline__ void fft(float2 (&v)[16], int j, int g, float2 *xb, const float2 *__restrict__ tw,
+                                    const float2 *twA, const float2 *twB)
 {
   using Pl = r16::Plan<F>;
   constexpr int NT = Pl::NT;
+  static_assert(Pl::L <= 3, "shared twiddle rows cover strides 16 and 256");
   r16::dft16(v);   // stride-1 pass: no twiddles
 #pragma unroll
   for (int p = 1; p < Pl::L; p++) {
@@ -124,7 +156,8 @@ __device__ __forceinline__ void fft(float2 (&v)[16], int j, int g, float2 *xb, c
     r16::store16(v, j, Ns, xb);
     group_sync<NT, CTA>(g);
     r16::load16<F>(v, j, xb);
-    pass16_tab<F>(v, j, r16::pow16(p), tw + r16::tw_pass_offset(F, p));
+    if (p == 1) pass16_rows<1>(v, j, twA, twB);
+    else pass16_rows<2>(v, j, twA, twB);
   }
   if constexpr (Pl::R0 > 1) {
     // the last radix-16 pass leaves its outputs for a pass of stride F / R0
@@ -150,11 +183,16 @@ fstep_sb_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays 
   const int s = blockIdx.y;
   const int tid = threadIdx.x, g = tid / NT, j = tid % NT;
   const DevStation &st = stations[s];
+  // CTA-wide twiddle rows, then per group: exchange buffer, rotator tables,
+  // staged time samples
+  float2 *twA = reinterpret_cast<float2 *>(smem_raw);
+  float2 *twB = twA + kTwRow;
   for (int i = tid; i < 256; i += CTA) s_lut[i] = J.lut[i];
+  load_tw_rows<F>(twA, twB, J.twiddle, tid, CTA);
   __syncthreads();
 
-  // per group: exchange buffer, rotator tables, staged time samples
-  float2 *xb = reinterpret_cast<float2 *>(smem_raw + (size_t)g * ((Pl::SMEM + tabstride) * sizeof(float2) + C::RAWB));
+  float2 *xb = reinterpret_cast<float2 *>(smem_raw + 2 * kTwRow * sizeof(float2) +
+                                          (size_t)g * ((Pl::SMEM + tabstride) * sizeof(float2) + C::RAWB));
   float2 *tab = xb + Pl::SMEM;
   unsigned char *raw = reinterpret_cast<unsigned char *>(tab + tabstride);
   const int nlf = st.nrecfreqs, nps = st.deltapol ? 2 : 1;
@@ -239,6 +277,7 @@ fstep_sb_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays 
       }
     }
     const unsigned char *rj = raw + off0 + j * BPTS;   // time sample j of the block
+    uint32_t wpair[16];   // 8-bit complex: the words of the current band pair
 #pragma unroll 1
     for (int bd = 0; bd < J.nbands; bd++) {
       const int bit0 = bd * fbits, sh = bit0 & 7;
@@ -254,7 +293,26 @@ fstep_sb_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays 
         // so the sub entry is the same for all 16 samples of the thread
         const float2 rsk = rs[j & (SD - 1)];
         const float2 *rpj = rp + (j >> LGS);
-        if (CPLX && fbits == 16) {   // 8-bit complex: one (re, im) byte pair
+        if (CPLX && fbits == 16 && J.lut_affine) {   // 8-bit complex, levels by arithmetic
+          // Bands 2k and 2k + 1 share a 4-byte word of the time sample (the
+          // complex 8-bit domain has 2, 4 or 8 bands); it is read once for the
+          // pair, halving the bank-conflicted reads of the 16-byte-stride samples.
+          const unsigned int h = bd & 1;
+          if (h == 0) {
+#pragma unroll
+            for (int t = 0; t < 16; t++) wpair[t] = *reinterpret_cast<const uint32_t *>(rb + NT * BPTS * t);
+          }
+          const unsigned int sre = 0x7650u + 2u * h, sim = sre + 1u;
+          const float bias = J.lut_bias, hi = J.lut_hi, lo = J.lut_lo;
+#pragma unroll
+          for (int t = 0; t < 16; t++) {
+            // code c as the float 2^23 + c (byte placed under the exponent 0x4B)
+            const float xr = __uint_as_float(__byte_perm(wpair[t], 0x4B000000u, sre)) - bias;
+            const float xi = __uint_as_float(__byte_perm(wpair[t], 0x4B000000u, sim)) - bias;
+            const float2 u = make_float2(fmaf(xr, hi, xr * lo), fmaf(xi, hi, xi * lo));
+            v[t] = cmul(cmul(rsk, rpj[JSTEP * t]), u);
+          }
+        } else if (CPLX && fbits == 16) {   // 8-bit complex: one (re, im) byte pair
 #pragma unroll
           for (int t = 0; t < 16; t++) {
             const uint32_t w = *reinterpret_cast<const unsigned short *>(rb + NT * BPTS * t);
@@ -277,7 +335,7 @@ fstep_sb_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays 
             if (!((vmask >> t) & 1u)) v[t] = make_float2(0.f, 0.f);
         }
       }
-      fft<F, CTA>(v, j, g, xb, tw);
+      fft<F, CTA>(v, j, g, xb, tw, twA, twB);
       // register t holds bin j + NT t: sideband selection, fractional-sample
       // correction sub[c mod S] step[c / S] (c mod S fixed per thread), store
       const int lsb = st.lsb[lf];
@@ -338,7 +396,8 @@ size_t fstep_sb_smem_bytes(const DevJob &J, int maxnrf, int deltapol)
 {
   const int F = J.fftlen, NT = F / 16, G = (NT >= 256 ? NT : 256) / NT;
   const int bpts = J.nbands * J.nbits * (J.cplx ? 2 : 1) / 8;
-  return (size_t)G * ((F + F / 16 + sb_tab(J, maxnrf, deltapol)) * sizeof(float2) + (size_t)(F * bpts + 32));
+  return 2 * sb::kTwRow * sizeof(float2) +
+         (size_t)G * ((F + F / 16 + sb_tab(J, maxnrf, deltapol)) * sizeof(float2) + (size_t)(F * bpts + 32));
 }
 
 cudaError_t fstep_sb_launch(const DevJob &J, const DevStation *stations, int maxnrf, int deltapol,
