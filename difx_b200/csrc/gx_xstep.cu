@@ -118,11 +118,11 @@ xmac_fp32_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int N, 
   const int p = tid / CT;
   const int ti = p / NT, tj = p % NT;
   const float2 *sJread = diag ? sI : sJ;
-  float ar[T][T], ai[T][T];
+  float2 acc2[T][T];   // (Re, Im) of each product sum, one register pair for the f32x2 FMAs
 #pragma unroll
   for (int a = 0; a < T; a++)
 #pragma unroll
-    for (int b = 0; b < T; b++) { ar[a][b] = 0.f; ai[a][b] = 0.f; }
+    for (int b = 0; b < T; b++) acc2[a][b] = make_float2(0.f, 0.f);
   const bool compute = !diag || (ti <= tj);   // lower tiles of diagonal super-tiles are redundant
   bool ok = true;
   for (int st = 0; st < nstages; st++) {
@@ -143,15 +143,22 @@ xmac_fp32_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int N, 
           xi[r] = bi_[(kk * ST + ti * T + r) * CT + c];
           xj[r] = bj_[(kk * ST + tj * T + r) * CT + c];
         }
+        // xi * conj(xj) as two paired FMAs (one f32x2 instruction each on
+        // sm_100): Re += xi.x xj.x then xi.y xj.y; Im += xi.y xj.x then -xi.x xj.y,
+        // the same operations in the same order as four scalar FMAs.
+        float2 xs[T], bx[T], by[T];
+#pragma unroll
+        for (int r = 0; r < T; r++) {
+          xs[r] = make_float2(xi[r].y, -xi[r].x);
+          bx[r] = make_float2(xj[r].x, xj[r].x);
+          by[r] = make_float2(xj[r].y, xj[r].y);
+        }
 #pragma unroll
         for (int a = 0; a < T; a++)
 #pragma unroll
           for (int b = 0; b < T; b++) {
-            // xi * conj(xj)
-            ar[a][b] = fmaf(xi[a].x, xj[b].x, ar[a][b]);
-            ar[a][b] = fmaf(xi[a].y, xj[b].y, ar[a][b]);
-            ai[a][b] = fmaf(xi[a].y, xj[b].x, ai[a][b]);
-            ai[a][b] = fmaf(-xi[a].x, xj[b].y, ai[a][b]);
+            acc2[a][b] = __ffma2_rn(xi[a], bx[b], acc2[a][b]);
+            acc2[a][b] = __ffma2_rn(xs[a], by[b], acc2[a][b]);
           }
       }
     }
@@ -168,8 +175,8 @@ xmac_fp32_kernel(const __grid_constant__ CUtensorMap spec_map, int nblk, int N, 
       const int ii = ti * T + a, jj = tj * T + b;
       float2 *dst = acc + (base + (size_t)ii * ST + jj) * N + c0 + c;
       float2 v = *dst;
-      v.x += ar[a][b];
-      v.y += ai[a][b];
+      v.x += acc2[a][b].x;
+      v.y += acc2[a][b].y;
       *dst = v;
     }
 }
