@@ -345,7 +345,7 @@ def time_device(corr, sd_dev, dres, stream, steps, warmup, local, dist=None, clo
 # (workload, kernel): C3 captured at a 16 ms subint (250 blocks x 64
 # stations).  Traffic grows with the blocks a launch processes, so a step's
 # traffic is this figure times its blocks.
-F_DRAM_BYTES_PER_BLOCK = {("bench_c3", "fstep_sb_kernel"): (1.047196e9 + 4.142358e9) / 250}
+F_DRAM_BYTES_PER_BLOCK = {("bench_c3", "fstep_sb_kernel"): (1.047047e9 + 4.136257e9) / 250}
 
 
 def f_kernel_name(spec: JobSpec) -> str:
