@@ -58,7 +58,7 @@ static void free_all(gx_handle *h)
                   h->d_tcrows, h->d_err, h->d_full, h->d_avgtab, h->d_pcal, h->d_pcalbins, h->d_zrows,
                   h->d_zprods, h->d_specz, h->d_accz, h->d_uvents, h->d_uvfreqs, h->d_binents, h->d_binitems,
                   h->d_binwout, h->d_autoprods, h->d_autowents, h->d_binphase, h->d_binweight, h->d_accb,
-                  h->d_wbins, h->d_pcalrot};
+                  h->d_wbins, h->d_pcalrot, h->d_pcalfirst};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (h->h_err) cudaFreeHost(h->h_err);
@@ -1161,6 +1161,25 @@ static gx_status setup(gx_handle *h)
       CKR(h, h->dalloc(&h->d_pcalrot, sizeof(float2) * h->pcal_rot.size()));
       CKR(h, cudaMemcpy(h->d_pcalrot, h->pcal_rot.data(), sizeof(float2) * h->pcal_rot.size(), cudaMemcpyHostToDevice));
     }
+    // The station-block F-step forms the bin sums itself when each thread's
+    // samples share a bin (nbins divides F / 16); it then needs one slot of
+    // partial sums per CTA group of the longest pass.
+    h->pcal_fuse_bins = 0;
+    if (h->pcal_per_station && fstep_sb_eligible(J, false)) {
+      const int NT = J.fftlen / 16, G = (NT >= 256 ? NT : 256) / NT, nbins = h->pcal[0].nbins;
+      if (nbins <= NT && NT % nbins == 0) {
+        const int bpc = (J.sb_items > 0 ? J.sb_items : 4) * G;
+        const long long slots = (long long)((h->chunk + bpc - 1) / bpc) * G;
+        if (slots * (long long)h->pcal.size() * h->pcal_maxbins <= (64ll << 20)) {   // at most 512 MB of sums
+          std::vector<int> first(d.nstations, -1);
+          for (size_t i = 0; i < h->pcal.size(); i += J.nbands) first[h->pcal[i].station] = (int)i;
+          CKR(h, h->dalloc(&h->d_pcalfirst, sizeof(int) * first.size()));
+          CKR(h, cudaMemcpy(h->d_pcalfirst, first.data(), sizeof(int) * first.size(), cudaMemcpyHostToDevice));
+          h->pcal_chunks = (int)std::max<long long>(h->pcal_chunks, slots);
+          h->pcal_fuse_bins = nbins;
+        }
+      }
+    }
     CKR(h, h->dalloc(&h->d_pcalbins, sizeof(float2) * (size_t)h->pcal_chunks * h->pcal.size() * h->pcal_maxbins));
   }
   if (h->avg > 1) {
@@ -1615,9 +1634,12 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
   auto pass = [&](int b0, int nb) -> gx_status {
     gx_status r;
     if ((r = mark(0, true)) != GX_OK) return r;
-    CKR(h, fstep_launch(J, h->d_st, h->maxnrf, S, b0, nb, h->nslots, h->d_spec, h->d_w, h->d_bp, st));
+    const PcalFuse pf{h->d_pcalbins, h->d_pcalfirst, h->pcal_fuse_bins, h->pcal_maxbins, npc, h->pcal_chunks};
+    bool pcal_done = false;
+    CKR(h, fstep_launch(J, h->d_st, h->maxnrf, S, b0, nb, h->nslots, h->d_spec, h->d_w, h->d_bp, st,
+                        npc && h->pcal_fuse_bins ? &pf : nullptr, &pcal_done));
     if (h->kurt && (r = gx_kurtosis_pass(h, nb, st)) != GX_OK) return r;
-    if (npc) {
+    if (npc && !pcal_done) {
       CKR(h, pcal_bins_launch(J, S, h->d_bp, nb, h->d_pcal, h->d_pcalrot, npc, h->pcal_per_station, h->pcal_chunks,
                               h->pcal_maxbins, h->d_pcalbins, st));
       h->launches += 1;
@@ -1711,8 +1733,9 @@ gx_status gx_enqueue_subint(gx_handle *h, float2 *dev_results, cudaStream_t st)
     h->launches += 1;
   }
   if (npc) {
-    CKR(h, pcal_tones_launch(h->d_pcal, npc, h->pcal_chunks, h->pcal_maxbins, h->d_pcalbins, fin, st));
-    h->launches += 1;
+    CKR(h, pcal_fold_launch(h->d_pcalbins, h->pcal_chunks, (long long)npc * h->pcal_maxbins, st));
+    CKR(h, pcal_tones_launch(h->d_pcal, npc, 1, h->pcal_maxbins, h->d_pcalbins, fin, st));
+    h->launches += h->pcal_chunks > 1 ? 2 : 1;
   }
   if (h->avg > 1) {
     CKR(h, cudaMemsetAsync(dev_results, 0, sizeof(float2) * h->rl, st));

@@ -120,6 +120,20 @@ struct PcalBand {
   long long rot0;
 };
 
+// Phase-cal bin sums formed inside the station-block F-step (the block's
+// samples are decoded there anyway) instead of by a second read of the VDIF.
+// Taken when every station with phase-cal has one implicit-shift band per
+// recorded band, all with nbins bins, and nbins divides the transform's
+// threads per group (F / 16): the 16 samples a thread decodes then share one
+// bin.  Group g of F-step CTA x adds its sums into partial[x G + g][band][bin]
+// (slots partial slots in all); first[s] is station s's first band in the
+// phase-cal band list (-1: none).
+struct PcalFuse {
+  float2 *partial;
+  const int *first;
+  int nbins, maxbins, nbands_total, slots;
+};
+
 // Raises `kernel`'s dynamic shared-memory limit on the current device to at
 // least `bytes`.  Safe from several host threads at once: the limit only ever
 // grows, so a launch that opted in for its size cannot be undercut by another
@@ -134,5 +148,8 @@ cudaError_t pcal_bins_launch(const DevJob &J, const SubintArrays &S, const Block
                              float2 *partial, cudaStream_t st);
 cudaError_t pcal_tones_launch(const PcalBand *bands, int nbands, int chunks, int maxbins, const float2 *partial,
                               float2 *results, cudaStream_t st);
+// Adds chunks 1 .. chunks-1 of partial ([chunk][n]) into chunk 0, in chunk
+// order, so that the tones can be formed from one chunk.
+cudaError_t pcal_fold_launch(float2 *partial, int chunks, long long n, cudaStream_t st);
 
 }  // namespace gx

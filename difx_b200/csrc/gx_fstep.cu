@@ -910,7 +910,8 @@ static bool use_r16_kernel(const DevJob &J)
 // selects the per-band kernels instead (comparison runs).
 bool fstep_sb_eligible(const DevJob &J, bool interlaced);
 cudaError_t fstep_sb_launch(const DevJob &J, const DevStation *stations, int maxnrf, int deltapol,
-                            const SubintArrays &S, int nblk, const BlockParam *bp, float2 *spec, cudaStream_t st);
+                            const SubintArrays &S, int nblk, const BlockParam *bp, float2 *spec, cudaStream_t st,
+                            const PcalFuse *pf, bool *pcal_done);
 
 static bool use_sb_kernel(const DevJob &J, bool interlaced)
 {
@@ -1378,6 +1379,30 @@ cudaError_t pcal_bins_launch(const DevJob &J, const SubintArrays &S, const Block
   return cudaGetLastError();
 }
 
+// Sum of the chunks' partial bin sums into chunk 0, in chunk order (the order
+// the tones kernel would add them in): one thread per (band, bin), loads
+// coalesced across threads.
+__global__ void __launch_bounds__(256) pcal_fold_kernel(float2 *__restrict__ partial, int chunks, long long n)
+{
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float bx = 0.f, by = 0.f;
+#pragma unroll 8
+  for (int c = 0; c < chunks; c++) {
+    const float2 v = partial[(size_t)c * n + i];
+    bx += v.x;
+    by += v.y;
+  }
+  partial[i] = make_float2(bx, by);
+}
+
+cudaError_t pcal_fold_launch(float2 *partial, int chunks, long long n, cudaStream_t st)
+{
+  if (chunks <= 1 || n <= 0) return cudaSuccess;
+  pcal_fold_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(partial, chunks, n);
+  return cudaGetLastError();
+}
+
 cudaError_t pcal_tones_launch(const PcalBand *bands, int nbands, int chunks, int maxbins, const float2 *partial,
                               float2 *results, cudaStream_t st)
 {
@@ -1404,8 +1429,9 @@ cudaError_t smem_opt_in(const void *kernel, size_t bytes)
 
 cudaError_t fstep_launch(const DevJob &J, const DevStation *stations, int maxnrf, const SubintArrays &S,
                          int blk0, int nblk, int nslots, float2 *spec, float *weights, BlockParam *bp,
-                         cudaStream_t st)
+                         cudaStream_t st, const PcalFuse *pf, bool *pcal_done)
 {
+  if (pcal_done) *pcal_done = false;
   {
     dim3 grid((nblk + 127) / 128, J.nstations);
     blockparams_kernel<<<grid, 128, 0, st>>>(J, S, blk0, nblk, bp, weights);
@@ -1415,8 +1441,9 @@ cudaError_t fstep_launch(const DevJob &J, const DevStation *stations, int maxnrf
     edv4_kernel<<<grid, 256, 0, st>>>(J, stations, S, nblk, bp, weights);
   }
   if (use_sb_kernel(J, S.bandmask != nullptr)) {
-    cudaError_t e = fstep_sb_launch(J, stations, maxnrf, J.deltapol_any, S, nblk, bp, spec, st);
+    cudaError_t e = fstep_sb_launch(J, stations, maxnrf, J.deltapol_any, S, nblk, bp, spec, st, pf, pcal_done);
     if (e != cudaErrorNotSupported) return e;
+    if (pcal_done) *pcal_done = false;
   }
   const size_t sm = fstep_smem_bytes(J, maxnrf, nslots);
   if (use_r16_kernel(J)) {

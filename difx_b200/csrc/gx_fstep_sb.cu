@@ -140,10 +140,11 @@ __device__ __forceinline__ void pass16_rows(float2 (&v)[16], int j, const float2
 }
 
 // Forward transform of the group's F points (16 per thread): register t ends
-// holding bin j + NT t.
-template <int F, int CTA>
+// holding bin j + NT t.  `mid` runs once, after the group's first barrier
+// (everything the group wrote to shared memory before the call is visible).
+template <int F, int CTA, typename Mid>
 __device__ __forceinline__ void fft(float2 (&v)[16], int j, int g, float2 *xb, const float2 *__restrict__ tw,
-                                    const float2 *twA, const float2 *twB)
+                                    const float2 *twA, const float2 *twB, Mid &&mid)
 {
   using Pl = r16::Plan<F>;
   constexpr int NT = Pl::NT;
@@ -153,6 +154,7 @@ __device__ __forceinline__ void fft(float2 (&v)[16], int j, int g, float2 *xb, c
   for (int p = 1; p < Pl::L; p++) {
     const int Ns = r16::pow16(p - 1);
     group_sync<NT, CTA>(g);
+    if (p == 1) mid();
     r16::store16(v, j, Ns, xb);
     group_sync<NT, CTA>(g);
     r16::load16<F>(v, j, xb);
@@ -169,10 +171,15 @@ __device__ __forceinline__ void fft(float2 (&v)[16], int j, int g, float2 *xb, c
   }
 }
 
-template <int F, int CPLX, int BPTS>
+// Pad slot of thread j in the exchange buffer: position 17 k + 16 is never an
+// element (pad(i) = i + i / 16 skips it), so a thread's phase-cal sum parks
+// there while the transform uses the buffer.
+__device__ __forceinline__ int pc_slot(int j) { return 17 * j + 16; }
+
+template <int F, int CPLX, int BPTS, bool PC>
 __global__ void __launch_bounds__(Cfg<F, CPLX, BPTS>::CTA, Cfg<F, CPLX, BPTS>::MINB)
 fstep_sb_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays S, const BlockParam *__restrict__ bp,
-                int nblk, int blocks_per_cta, int tabstride, float2 *__restrict__ spec)
+                int nblk, int blocks_per_cta, int tabstride, float2 *__restrict__ spec, PcalFuse pf)
 {
   using C = Cfg<F, CPLX, BPTS>;
   using Pl = r16::Plan<F>;
@@ -205,6 +212,18 @@ fstep_sb_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays 
   const uint32_t cmask = (1u << J.nbits) - 1u;
   // 16-byte copies need a 16-byte aligned buffer (the frame layout is checked on the host)
   const bool aligned = (reinterpret_cast<uintptr_t>(data) & 15) == 0;
+  // phase-cal (PC): this station's first band in the phase-cal list, the
+  // absolute sample number of the subint start (as the binning kernels form
+  // it) and this group's slot of partial sums
+  const int pcfirst = PC ? pf.first[s] : -1;
+  unsigned long long pcs0 = 0;
+  if (PC && pcfirst >= 0) {
+    const int32_t *ctrl = S.control + (size_t)s * S.controlstride;
+    pcs0 = (unsigned long long)(((double)ctrl[1] * 1e9 + (double)ctrl[2]) / (J.sampletime * 1e3) + 0.5);
+  }
+  float2 *pcout = PC && pcfirst >= 0
+                      ? pf.partial + ((size_t)(blockIdx.x * G + g) * pf.nbands_total + pcfirst) * pf.maxbins
+                      : nullptr;
 
   const int b0 = blockIdx.x * blocks_per_cta;
   const int nbk = min(blocks_per_cta, nblk - b0);
@@ -278,6 +297,13 @@ fstep_sb_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays 
     }
     const unsigned char *rj = raw + off0 + j * BPTS;   // time sample j of the block
     uint32_t wpair[16];   // 8-bit complex: the words of the current band pair
+    // phase-cal: sample n of the block is absolute sample pcs0 + nearestsample + n,
+    // bin (that) mod nbins; nbins divides NT, so thread j's samples j + NT t
+    // all fall in bin pcbin, and threads j < nbins own one bin each
+    const int pcn = PC ? pf.nbins : 1;
+    const int pcbin = PC ? (int)((pcs0 + (unsigned long long)P.nearestsample + (unsigned long long)j) %
+                                 (unsigned long long)pcn)
+                         : 0;
 #pragma unroll 1
     for (int bd = 0; bd < J.nbands; bd++) {
       const int bit0 = bd * fbits, sh = bit0 & 7;
@@ -288,6 +314,7 @@ fstep_sb_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays 
       const float2 *fs = rp + NFR + (st.band_polb[bd] ? SD + HALF : 0);
       const float2 *fp = fs + SD;
       float2 v[16];
+      float2 ps = make_float2(0.f, 0.f);   // phase-cal: sum of this thread's valid samples
       {
         // decode and fringe-rotate: x[n] sub[n mod S] step[n / S]; S divides NT,
         // so the sub entry is the same for all 16 samples of the thread
@@ -311,6 +338,7 @@ fstep_sb_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays 
             const float xi = __uint_as_float(__byte_perm(wpair[t], 0x4B000000u, sim)) - bias;
             const float2 u = make_float2(fmaf(xr, hi, xr * lo), fmaf(xi, hi, xi * lo));
             v[t] = cmul(cmul(rsk, rpj[JSTEP * t]), u);
+            if (PC && (allvalid || ((vmask >> t) & 1u))) ps = make_float2(ps.x + u.x, ps.y + u.y);
           }
         } else if (CPLX && fbits == 16) {   // 8-bit complex: one (re, im) byte pair
 #pragma unroll
@@ -318,6 +346,7 @@ fstep_sb_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays 
             const uint32_t w = *reinterpret_cast<const unsigned short *>(rb + NT * BPTS * t);
             const float2 u = make_float2(s_lut[w & 255u], s_lut[w >> 8]);
             v[t] = cmul(cmul(rsk, rpj[JSTEP * t]), u);
+            if (PC && (allvalid || ((vmask >> t) & 1u))) ps = make_float2(ps.x + u.x, ps.y + u.y);
           }
         } else {
 #pragma unroll
@@ -325,8 +354,10 @@ fstep_sb_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays 
             const uint32_t w = rb[NT * BPTS * t];
             const float2 rot = cmul(rsk, rpj[JSTEP * t]);
             const float ux = s_lut[(w >> sh) & cmask];
-            if (CPLX) v[t] = cmul(rot, make_float2(ux, s_lut[(w >> (sh + J.nbits)) & cmask]));
+            const float uy = CPLX ? s_lut[(w >> (sh + J.nbits)) & cmask] : 0.f;
+            if (CPLX) v[t] = cmul(rot, make_float2(ux, uy));
             else v[t] = make_float2(ux * rot.x, ux * rot.y);
+            if (PC && (allvalid || ((vmask >> t) & 1u))) ps = make_float2(ps.x + ux, ps.y + uy);
           }
         }
         if (!allvalid) {
@@ -335,7 +366,22 @@ fstep_sb_kernel(DevJob J, const DevStation *__restrict__ stations, SubintArrays 
             if (!((vmask >> t) & 1u)) v[t] = make_float2(0.f, 0.f);
         }
       }
-      fft<F, CTA>(v, j, g, xb, tw, twA, twB);
+      if (PC) xb[pc_slot(j)] = ps;
+      fft<F, CTA>(v, j, g, xb, tw, twA, twB, [&]() {
+        if (PC && pcout && j < pcn) {
+          // bin (pcbin of thread j) collects threads j, j + nbins, ...: fixed
+          // order; one thread per bin and item, items ordered by the group's
+          // barriers, so the sums do not depend on timing
+          float2 a = make_float2(0.f, 0.f);
+          for (int m = j; m < NT; m += pcn) {
+            const float2 q = xb[pc_slot(m)];
+            a = make_float2(a.x + q.x, a.y + q.y);
+          }
+          float2 *o = pcout + (size_t)bd * pf.maxbins + pcbin;
+          atomicAdd(&o->x, a.x);
+          if (CPLX) atomicAdd(&o->y, a.y);
+        }
+      });
       // register t holds bin j + NT t: sideband selection, fractional-sample
       // correction sub[c mod S] step[c / S] (c mod S fixed per thread), store
       const int lsb = st.lsb[lf];
@@ -400,8 +446,19 @@ size_t fstep_sb_smem_bytes(const DevJob &J, int maxnrf, int deltapol)
          (size_t)G * ((F + F / 16 + sb_tab(J, maxnrf, deltapol)) * sizeof(float2) + (size_t)(F * bpts + 32));
 }
 
+// Whether the kernel can form the phase-cal sums of pf for this job and
+// launch shape: bins dividing the threads of a transform, one slot per group.
+bool fstep_sb_pcal_fits(const DevJob &J, const PcalFuse &pf, int nblk)
+{
+  const int F = J.fftlen, NT = F / 16, G = (NT >= 256 ? NT : 256) / NT;
+  const int bpc = (J.sb_items > 0 ? J.sb_items : 4) * G;
+  return pf.partial && pf.first && pf.nbins > 0 && pf.nbins <= NT && NT % pf.nbins == 0 &&
+         (long long)((nblk + bpc - 1) / bpc) * G <= pf.slots;
+}
+
 cudaError_t fstep_sb_launch(const DevJob &J, const DevStation *stations, int maxnrf, int deltapol,
-                            const SubintArrays &S, int nblk, const BlockParam *bp, float2 *spec, cudaStream_t st)
+                            const SubintArrays &S, int nblk, const BlockParam *bp, float2 *spec, cudaStream_t st,
+                            const PcalFuse *pf, bool *pcal_done)
 {
   const int F = J.fftlen, NT = F / 16, G = (NT >= 256 ? NT : 256) / NT;
   const int tabstride = (int)sb_tab(J, maxnrf, deltapol);
@@ -410,13 +467,24 @@ cudaError_t fstep_sb_launch(const DevJob &J, const DevStation *stations, int max
   const int bpts = J.nbands * J.nbits * (J.cplx ? 2 : 1) / 8;
   const int bpc = (J.sb_items > 0 ? J.sb_items : 4) * G;   // items per group (four unless tuned)
   dim3 grid((nblk + bpc - 1) / bpc, J.nstations);
-#define GX_SB_CASE(FLV, CX, BP)                                                                         \
-  if (F == FLV && J.cplx == CX && bpts == BP) {                                                         \
-    using K = sb::Cfg<FLV, CX, BP>;                                                                     \
-    cudaError_t e = smem_opt_in((const void *)sb::fstep_sb_kernel<FLV, CX, BP>, sm);                    \
-    if (e != cudaSuccess) return e;                                                                     \
-    sb::fstep_sb_kernel<FLV, CX, BP><<<grid, K::CTA, sm, st>>>(J, stations, S, bp, nblk, bpc, tabstride, spec); \
-    return cudaGetLastError();                                                                          \
+  const bool pc = pf && fstep_sb_pcal_fits(J, *pf, nblk);
+  const PcalFuse pfv = pc ? *pf : PcalFuse{};
+#define GX_SB_CASE(FLV, CX, BP)                                                                          \
+  if (F == FLV && J.cplx == CX && bpts == BP) {                                                          \
+    using K = sb::Cfg<FLV, CX, BP>;                                                                      \
+    const void *kf = pc ? (const void *)sb::fstep_sb_kernel<FLV, CX, BP, true>                           \
+                        : (const void *)sb::fstep_sb_kernel<FLV, CX, BP, false>;                         \
+    cudaError_t e = smem_opt_in(kf, sm);                                                                 \
+    if (e != cudaSuccess) return e;                                                                      \
+    if (pc)                                                                                              \
+      sb::fstep_sb_kernel<FLV, CX, BP, true><<<grid, K::CTA, sm, st>>>(J, stations, S, bp, nblk, bpc,     \
+                                                                        tabstride, spec, pfv);           \
+    else                                                                                                 \
+      sb::fstep_sb_kernel<FLV, CX, BP, false><<<grid, K::CTA, sm, st>>>(J, stations, S, bp, nblk, bpc,    \
+                                                                         tabstride, spec, pfv);          \
+    e = cudaGetLastError();                                                                              \
+    if (e == cudaSuccess && pcal_done) *pcal_done = pc;                                                  \
+    return e;                                                                                            \
   }
 #define GX_SB_SIZES(CX, BP) \
   GX_SB_CASE(512, CX, BP) GX_SB_CASE(1024, CX, BP) GX_SB_CASE(2048, CX, BP) GX_SB_CASE(4096, CX, BP) GX_SB_CASE(8192, CX, BP)

@@ -40,6 +40,10 @@ struct gx_handle {
   float2 *d_pcalrot = nullptr;
   float2 *d_pcalbins = nullptr;              // [chunk][pcal band][bin] partial bin sums
   int pcal_chunks = 0, pcal_maxbins = 0, pcal_per_station = 0;
+  // bin sums formed inside the station-block F-step (gx::PcalFuse): station
+  // -> first phase-cal band (-1: none), on the device; 0 bins when not offered
+  int *d_pcalfirst = nullptr;
+  int pcal_fuse_bins = 0;
   std::vector<int> pc_off, pc_ntones;        // [station * GX_MAX_BANDS + band]: result index / tones
   std::vector<std::vector<double>> pc_tone_hz;   // [station * GX_MAX_BANDS + band]: tone frequencies (Hz)
   std::vector<int> pc_maxtones;              // [station]: most tones of a band (0: phase-cal off)

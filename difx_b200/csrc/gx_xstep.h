@@ -40,9 +40,15 @@ XmacShape xmac_shape(int NI);
 // 4-D FP32 tensor map over a dense array (dims innermost first), box `box`.
 cudaError_t tma_map_f32_4d(CUtensorMap *map, const void *base, const cuuint64_t dims[4], const cuuint32_t box[4]);
 
-size_t fstep_smem_bytes(const DevJob &J, int nrf, int nslots);cudaError_t fstep_launch(const DevJob &J, const DevStation *stations, int maxnrf, const SubintArrays &S,
+size_t fstep_smem_bytes(const DevJob &J, int nrf, int nslots);
+// Whether the station-block F-step (gx_fstep_sb.cu) takes this job.
+bool fstep_sb_eligible(const DevJob &J, bool interlaced);
+// F-step of one pass of blocks.  With pf, the station-block kernel also forms
+// the phase-cal bin sums when it takes the job; *pcal_done (if given) tells
+// whether it did (else the caller runs pcal_bins_launch).
+cudaError_t fstep_launch(const DevJob &J, const DevStation *stations, int maxnrf, const SubintArrays &S,
                          int blk0, int nblk, int nslots, float2 *spec, float *weights, BlockParam *bp,
-                         cudaStream_t st);
+                         cudaStream_t st, const PcalFuse *pf = nullptr, bool *pcal_done = nullptr);
 // FP32 X-step over one pass of blocks; *err (may be null) receives a nonzero
 // status if a wait of the kernel expired.  variant: the launch shape (0: the
 // default channel tile and stage depth; 1: the other one of the shape class,

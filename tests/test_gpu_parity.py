@@ -392,6 +392,13 @@ PCAL_CASES = {
                            dict(invalid_frac=0.03)),
     "cplx2_pcal": lambda: (jobs.spec_long("cx2pc", 2, "COMPLEX", "U", 128, 87, pcal_interval_mhz=1),
                            dict(invalid_frac=0.03)),
+    # the C3 sample format (8 complex 8-bit bands, 16-byte time samples) with
+    # 4096-point transforms: the station-block F-step forms the bin sums
+    # (16 bins divide its 256 threads per transform); real4_pcal takes that
+    # path with four transform groups per CTA (32 bins, 64 threads)
+    "cplx8_4096_pcal": lambda: (jobs.spec_long("cx8pcl", 8, "COMPLEX", "U", 4096, 91, pcal_interval_mhz=1,
+                                               subbands=[jobs.Subband(6000.0 + 16 * i, 16.0, "U", 4096)
+                                                         for i in range(4)]), dict(invalid_frac=0.03)),
     # multiplexed frames with EDV4 masks: phase-cal of the blanked samples
     "mux_pcal": lambda: (jobs.spec_c1(name="c1mxpc", seed=105, pcal_interval_mhz=1, mux_threads=8,
                                       edv4_partial_frac=0.3), dict(invalid_frac=0.02)),
