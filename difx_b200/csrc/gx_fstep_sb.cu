@@ -11,13 +11,18 @@
 //   2. meanwhile computes the rotator tables of every local frequency of the
 //      station once (fringe: mode.cpp:882-955; fractional sample:
 //      mode.cpp:1029-1122),
-//   3. for every band: decodes its field of the staged samples through the
-//      shared-memory level table (format_vdif.c:66-146), rotates
+//   3. for every band: decodes its field of the staged samples (8-bit codes
+//      by an exact two-term FMA, other widths through the shared-memory level
+//      table; format_vdif.c:66-146), rotates
 //      (mode.cpp:1160-1183), transforms (16 points per thread, radix-16
 //      passes of gx_fft16.h with the twiddle rows of the stride-16 and
 //      stride-256 passes in shared memory),
 //      selects the sideband, applies the fractional-sample correction
-//      (mode.cpp:1185-1261) and writes the channels with coalesced stores.
+//      (mode.cpp:1185-1261) and writes the channels with coalesced stores;
+//   4. with phase-cal (PC, gx::PcalFuse), also adds the decoded samples of
+//      each band into their phase-cal bins (mode.cpp:759-774; the
+//      implicit-shift extractors of pcal.cpp:1032-1222 and 1419-1600), so
+//      the samples are not read and decoded a second time.
 // Frames a block spans are checked against the block's validity mask only
 // when one of them is invalid (samples of invalid frames decode to zero and
 // are not read).  Jobs outside this kernel's domain (other transform
