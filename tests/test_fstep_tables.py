@@ -75,3 +75,29 @@ def test_8bit_symmetric_offset_keeps_table():
     bias = 8388608.0 + 127.5
     assert float(np.float32(bias)) != bias
     assert float(np.float32(8388608.0 + 128.0)) == 8388608.0 + 128.0
+
+
+def test_phase_cal_pad_slots_are_free():
+    # The exchange buffer holds element i of a transform at pad(i) = i + i // 16
+    # (F + F / 16 entries); thread j parks its phase-cal sum at 17 j + 16,
+    # j < F / 16.  Those slots must lie inside the buffer and never be an
+    # element position, so the transform's stores and loads cannot touch them.
+    for F in (512, 1024, 2048, 4096, 8192):
+        used = {i + i // 16 for i in range(F)}
+        slots = {17 * j + 16 for j in range(F // 16)}
+        assert len(slots) == F // 16
+        assert not (used & slots)
+        assert max(slots) < F + F // 16 and max(used) < F + F // 16
+
+
+def test_phase_cal_bins_of_a_thread():
+    # Sample j + (F / 16) t of a block whose first sample is absolute sample S
+    # falls in bin (S + j) mod nbins for every t when nbins divides F / 16.
+    rng = np.random.default_rng(5)
+    for F in (512, 4096, 8192):
+        NT = F // 16
+        for nbins in [d for d in (1, 2, 4, 8, 16, 32, 64, 128, 256, 512) if NT % d == 0]:
+            S = int(rng.integers(0, 2**40))
+            for j in rng.integers(0, NT, 8):
+                bins = {(S + int(j) + NT * t) % nbins for t in range(16)}
+                assert bins == {(S + int(j)) % nbins}
