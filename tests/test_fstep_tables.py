@@ -7,7 +7,9 @@ and decodes 8-bit VDIF codes (format_vdif.c: level = (b - 128) / 3.3) by
 fma(x, hi, x * lo) with 1/3.3 = hi + lo when the host finds that equal to the
 level table.  These tests restate both in numpy: the factorised twiddle stays
 within a few FP32 ulps of the exact one, and the two-term FMA reproduces every
-entry of the reference's table.
+entry of the reference's table.  They also check the index arithmetic of the
+phase-cal sums the kernel forms: the exchange-buffer pad slots it parks them
+in, and the one bin a thread's samples share.
 """
 import numpy as np
 
